@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Benchmark: semi-Lagrangian level-set updates/s at 256^3 on B200.
+
+Workload (one "step"): one SL step of a 256^3 FP32 signed distance (sphere
+r = 0.15 at (0.35, 0.35, 0.35)) in LeVeque's time-reversing deformation
+field (T = 3, dt at CFL 0.5), midpoint backtrace, Catmull-Rom tricubic
+reconstruction with the coefficient solve as a split-BF16 tcgen05 GEMM --
+every one of the 16,777,216 grid points is updated.  Inputs are synthetic
+(formulas), resident in HBM, larger than L2 (no flush needed).
+
+Also measured in the same run: the plain FP32 CUDA-core step (1331-nnz
+coefficient form) and the separable FP32 step, the error of the TC step vs
+the FP64 GPU oracle in the |phi| < 3h band, the end-to-end rate through the
+reference-facing C ABI with FP64 host buffers, and the CPU oracle port.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (torchrun): every rank advects its own independent 256^3 level set
+(independent DCells, no collective on the data path) -> weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 256
+BYTES_PER_UPDATE = 20          # FP32: read phi0 4 B + u,v,w 12 B, write phi 4 B
+TC_FLOP_PER_UPDATE = 16384     # 2 * 64 * 64 per split term, hi + lo
+T_PERIOD = 3.0
+METRIC = "SL level-set updates/s @256^3: split-BF16 TC vs plain FP32 GPU at <=1e-5 err"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the TC kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "sl_tc_kernel_256.md")
+    try:
+        for ln in open(path):
+            if ln.startswith("dram_bytes_per_launch_256:"):
+                return float(ln.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.rows.append([c.strip() for c in ln.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(N, dev):
+    import torch
+
+    from dcell_b200 import fields
+    h = 1.0 / N
+    phi = fields.sphere_sdf(N, device=dev).float().contiguous()
+    vel = fields.deformation_velocity(N, device=dev).float().contiguous()
+    dt = fields.cfl_dt((2.0, 1.0, 1.0), h)
+    return h, phi, vel, dt, torch
+
+
+def dt_at(step, dt):
+    """velocity factor cos(pi t/T) at the step's mid time, folded into dt"""
+    return dt * math.cos(math.pi * (step + 0.5) * dt / T_PERIOD)
+
+
+def timed_steps(L, torch, phi, vel, h, dt, interp, K, W, dist=None):
+    a, b = phi.clone(), phi.clone()
+    for s in range(W):
+        L.sl_step(a, vel, dt_at(s, dt), h, interp=interp, backtrace="midpoint", out=b)
+        a, b = b, a
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for s in range(K):
+        L.sl_step(a, vel, dt_at(W + s, dt), h, interp=interp, backtrace="midpoint", out=b)
+        a, b = b, a
+    e1.record(st)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    return e0.elapsed_time(e1)
+
+
+def cpu_oracle_rate(phi, vel, h, dt, nplanes=24, threads=1):
+    """FP64 oracle port (tricubic, midpoint) on `nplanes` z-planes of the grid."""
+    import numpy as np
+
+    import oracle
+    N = phi.shape[0]
+    p64 = phi.double().cpu().numpy()
+    v64 = vel.double().cpu().numpy()
+    z0 = N // 2 - nplanes // 2
+    zs, ys, xs = np.meshgrid(np.arange(z0, z0 + nplanes), np.arange(N), np.arange(N), indexing="ij")
+    pts = np.stack([xs.ravel(), ys.ravel(), zs.ravel()], 1).astype(np.int32)
+    chunks = np.array_split(pts, threads)
+    t0 = time.perf_counter()
+    if threads == 1:
+        oracle.sl_step(p64, v64, dt, h, band=pts, interp="cubic", backtrace="midpoint")
+    else:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(threads) as ex:  # ctypes releases the GIL
+            list(ex.map(lambda c: oracle.sl_step(p64, v64, dt, h, band=c, interp="cubic", backtrace="midpoint"),
+                        chunks))
+    t = time.perf_counter() - t0
+    return len(pts) / t, len(pts), t
+
+
+def reference_linear_rate(phi, vel, h, dt, nplanes=24):
+    """The reference's own LevelSetAdvectSL_3D (linear, Euler, FP64) on `nplanes` planes."""
+    import numpy as np
+
+    from oracle import reference as R
+    if not R.available():
+        return None
+    N = phi.shape[0]
+    ls = R.RefLevelSet.create(h, (0, 0, 0), (N, N, N))
+    ls.set_phi(phi.double().cpu().numpy())
+    z0 = N // 2 - nplanes // 2
+    zs, ys, xs = np.meshgrid(np.arange(z0, z0 + nplanes), np.arange(N), np.arange(N), indexing="ij")
+    ls.set_band(np.stack([xs.ravel(), ys.ravel(), zs.ravel()], 1).astype(np.int32))
+    ls.set_velocity(vel.double().cpu().numpy())
+    ls.copy_phi_to_phi0()
+    t0 = time.perf_counter()
+    ls.advect_sl(dt)
+    t = time.perf_counter() - t0
+    ls.close()
+    return xs.size / t
+
+
+def e2e_rate(phi, vel, h, dt, K, torch):
+    """Through the reference-facing C ABI with pinned FP64 host buffers
+    (reference Grid layout): H2D of phi0 + velocity, TC step, D2H of phi,
+    per step; synchronous calls timed by the host clock."""
+    from dcell_b200 import _lib
+    L = _lib.lib()
+    N = phi.shape[0]
+    p0 = phi.double().cpu().pin_memory()
+    v0 = vel.double().cpu().pin_memory()
+    out = torch.empty_like(p0).pin_memory()
+    sess = ctypes.c_void_p()
+    _lib.check(L.dcell_session_create(torch.cuda.current_device(), ctypes.byref(sess)))
+    g = _lib.geom((N, N, N), h)
+    args = lambda s: (sess, ctypes.byref(g), ctypes.c_void_p(p0.data_ptr()), ctypes.c_void_p(v0.data_ptr()), None, 0,
+                      dt_at(s, dt), _lib.CUBIC_TC, _lib.MIDPOINT, _lib.F32, ctypes.c_void_p(out.data_ptr()))
+    _lib.check(L.dcell_ls_advect_sl(*args(0)))  # warm-up (device buffers allocated)
+    t0 = time.perf_counter()
+    for s in range(K):
+        _lib.check(L.dcell_ls_advect_sl(*args(s)))
+    t = time.perf_counter() - t0
+    L.dcell_session_destroy(sess)
+    n = N ** 3
+    return n * K / t, {"h2d_bytes_per_step": n * 8 + n * 24, "d2h_bytes_per_step": n * 8}
+
+
+def error_check(L, torch, phi, vel, h, dt):
+    a = L.sl_step(phi, vel, dt_at(0, dt), h, interp="cubic_tc", backtrace="midpoint").double()
+    ref = L.sl_step(phi.double(), vel.double(), dt_at(0, dt), h, interp="cubic_plain", backtrace="midpoint")
+    plain = L.sl_step(phi, vel, dt_at(0, dt), h, interp="cubic_plain", backtrace="midpoint").double()
+    band = ref.abs() < 3 * h
+    e_tc, e_pl = (a - ref).abs()[band], (plain - ref).abs()[band]
+    vol_ref = float(L.volume(ref, h, 1.5 * h).item())
+    vol_tc = float(L.volume(a, h, 1.5 * h).item())
+    return {"max_err_band_tc": float(e_tc.max()), "l2_err_band_tc": float(e_tc.pow(2).mean().sqrt()),
+            "max_err_band_plain_fp32": float(e_pl.max()), "volume_rel_err_tc": abs(vol_tc - vol_ref) / vol_ref,
+            "band_points": int(band.sum())}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU implementation of the path on the host cores."""
+    if rank != 0:
+        return
+    import torch
+    h, phi, vel, dt, _ = workload(args.size, "cpu")
+    threads = os.cpu_count() or 1
+    nplanes = 16
+    rates = []
+    for s in range(args.warmup + args.steps):
+        r, npts, t = cpu_oracle_rate(phi, vel, h, dt_at(s, dt), nplanes=nplanes, threads=threads)
+        if s >= args.warmup:
+            rates.append(r)
+    value = statistics.median(rates)
+    n = args.size ** 3
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"sphere r=0.15 in LeVeque deformation, {args.size}^3, tricubic, midpoint SL",
+                       "sample": f"{nplanes} z-planes ({nplanes * args.size ** 2} points) per step"},
+            "cpu_baseline": {"value": value, "unit": "updates/s", "cores": threads, "kind": "port",
+                             "sample": f"{nplanes} of {args.size} z-planes per step; the reference has no tricubic "
+                                       "SL, so its FP64 restatement (oracle/sl_oracle.c) is timed"},
+            "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=N_DEFAULT)
+    ap.add_argument("--no-extras", action="store_true", help="skip comparators, e2e and CPU baseline")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    from dcell_b200 import levelset as L
+    h, phi, vel, dt, _ = workload(args.size, dev)
+    n = args.size ** 3
+    K, W = args.steps, args.warmup
+
+    with ClockSampler(local) as clk:
+        ms_tc = timed_steps(L, torch, phi, vel, h, dt, "cubic_tc", K, W, dist)
+    ms = ms_tc
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n * K * world / (ms / 1e3)
+
+    hbm, bf16, src = peaks()
+    t_launch = ms_tc / K / 1e3
+    achieved = BYTES_PER_UPDATE * n / t_launch / 1e9
+    traffic = profiled_traffic()
+    line = {"metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (bf16x2 split operands, f32 accumulate)", "data": "synthetic",
+            "config": {"workload": f"sphere r=0.15 in LeVeque deformation field, {args.size}^3 dense, tricubic "
+                                   "(split-BF16 tcgen05 coefficient GEMM), midpoint SL backtrace, CFL 0.5",
+                       "grid": [args.size] * 3, "points_per_step": n, "l2": "inputs 268 MB > 126 MB L2, no flush",
+                       "parallelism": f"independent level set per GPU x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic, "peak_source": src, "bytes_per_update": BYTES_PER_UPDATE,
+                         "tensor_tflops": TC_FLOP_PER_UPDATE * n / t_launch / 1e12,
+                         "tensor_frac": TC_FLOP_PER_UPDATE * n / t_launch / 1e12 / bf16},
+            "gpu_launches": K, "clocks": clk.summary()}
+
+    if not args.no_extras:
+        ms_pl = timed_steps(L, torch, phi, vel, h, dt, "cubic_plain", K, W)
+        ms_sep = timed_steps(L, torch, phi, vel, h, dt, "cubic_separable", K, W)
+        ms_lin = timed_steps(L, torch, phi, vel, h, dt, "linear", K, W)
+        line["comparators"] = {
+            "plain_fp32_updates_per_s": n * K / (ms_pl / 1e3),
+            "separable_fp32_updates_per_s": n * K / (ms_sep / 1e3),
+            "linear_fp32_updates_per_s": n * K / (ms_lin / 1e3),
+            "tc_over_plain_fp32": ms_pl / ms_tc,
+            "tc_over_separable_fp32": ms_sep / ms_tc}
+        line["accuracy"] = error_check(L, torch, phi, vel, h, dt)
+        if rank == 0:
+            e2e, by = e2e_rate(phi, vel, h, dt, min(K, 5), torch)
+            line["e2e"] = {"value": e2e * world, "unit": "updates/s", **by,
+                           "how": "dcell_ls_advect_sl (C ABI) on pinned FP64 host buffers, FP32 TC compute, "
+                                  "host clock around synchronous calls"}
+            if world == 1:
+                rate, npts, t = cpu_oracle_rate(phi, vel, h, dt, nplanes=24, threads=1)
+                line["cpu_baseline"] = {"value": rate, "unit": "updates/s", "cores": 1, "kind": "port",
+                                        "sample": f"{npts} points (24 z-planes) of the 256^3 step, FP64 "
+                                                  f"oracle restatement, {t:.1f} s"}
+                ref_lin = reference_linear_rate(phi, vel, h, dt, nplanes=24)
+                if ref_lin:
+                    line["cpu_baseline"]["reference_linear_advectsl_updates_per_s"] = ref_lin
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,111 @@
+"""ctypes binding of ``lib/libdcell_ls.so`` (the C ABI in include/dcell_ls.h).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libdcell_ls.so")
+
+OK, ERR_ARG, ERR_CUDA, ERR_DEPARTURE, ERR_NONFINITE, ERR_TIMEOUT, ERR_CAPACITY, ERR_UNSUPPORTED, ERR_NOMEM = range(9)
+F32, F64 = 0, 1
+LINEAR, CUBIC_PLAIN, CUBIC_SEPARABLE, CUBIC_TC = 0, 1, 2, 3
+EULER, MIDPOINT = 0, 1
+FLAG_DEPARTURE_CLAMPED, FLAG_NONFINITE, FLAG_CAPACITY, FLAG_WAIT_TIMEOUT = 1, 2, 4, 8
+
+INTERP = {"linear": LINEAR, "cubic": CUBIC_PLAIN, "cubic_plain": CUBIC_PLAIN, "cubic_separable": CUBIC_SEPARABLE,
+          "cubic_tc": CUBIC_TC}
+BACKTRACE = {"euler": EULER, "midpoint": MIDPOINT}
+
+
+class DcellError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"dcell error {code}: {msg}")
+        self.code = code
+
+
+class Geom(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int * 3), ("p", ctypes.c_int * 3), ("h", ctypes.c_double * 3)]
+
+
+class IrregularNode(ctypes.Structure):
+    _fields_ = [("pos", ctypes.c_int * 3), ("axis", ctypes.c_int), ("shift", ctypes.c_int),
+                ("signCenter", ctypes.c_int), ("signFace", ctypes.c_int), ("pad", ctypes.c_int),
+                ("d", ctypes.c_double), ("X", ctypes.c_double * 3), ("op", ctypes.c_double * 3),
+                ("n", ctypes.c_double * 3), ("k", ctypes.c_double)]
+
+
+NODE_DTYPE = np.dtype([("pos", "<i4", 3), ("axis", "<i4"), ("shift", "<i4"), ("signCenter", "<i4"),
+                       ("signFace", "<i4"), ("pad", "<i4"), ("d", "<f8"), ("X", "<f8", 3), ("op", "<f8", 3),
+                       ("n", "<f8", 3), ("k", "<f8")])
+assert NODE_DTYPE.itemsize == ctypes.sizeof(IrregularNode) == 120
+
+
+def geom(shape, h, origin=(0, 0, 0)) -> Geom:
+    """Geom from a phi shape ((nz, ny, nx) or (ny, nx)), spacing and global origin."""
+    if len(shape) == 2:
+        ny, nx = shape
+        nz = 1
+    else:
+        nz, ny, nx = shape
+    hh = np.broadcast_to(np.asarray(h, dtype=np.float64), (3,))
+    o = tuple(int(v) for v in origin) + (0,) * (3 - len(origin))
+    g = Geom()
+    g.n[:] = [int(nx), int(ny), int(nz)]
+    g.p[:] = [o[0], o[1], o[2] if nz > 1 else 0]
+    g.h[:] = [float(hh[0]), float(hh[1]), float(hh[2])]
+    return g
+
+
+_LIB = None
+
+
+def lib():
+    """The loaded C-ABI library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m dcell_b200.build` "
+                          "(the level-set kernels have no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i, d, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+    G = ctypes.POINTER(Geom)
+    L.dcell_last_error.restype = ctypes.c_char_p
+    L.dcell_version.restype = i
+    L.dcell_sl_step.argtypes = [G, i, vp, vp, d, vp, i, i, i, vp, vp, vp]
+    L.dcell_irregular_nodes_scratch_bytes.argtypes = [i]
+    L.dcell_irregular_nodes_scratch_bytes.restype = sz
+    L.dcell_irregular_nodes.argtypes = [G, i, vp, vp, i, i, vp, i, vp, vp, sz, vp, vp]
+    L.dcell_max_velocity.argtypes = [G, i, vp, vp, vp, i, vp, vp]
+    L.dcell_volume_scratch_bytes.restype = sz
+    L.dcell_volume.argtypes = [G, i, vp, d, vp, vp, sz, vp]
+    L.dcell_session_create.argtypes = [i, ctypes.POINTER(vp)]
+    L.dcell_session_destroy.argtypes = [vp]
+    L.dcell_ls_advect_sl.argtypes = [vp, G, vp, vp, vp, i, d, i, i, i, vp]
+    L.dcell_ls_update_irregular_nodes.argtypes = [vp, G, vp, vp, i, i, i, vp, i, vp]
+    L.dcell_ls_max_velocity.argtypes = [vp, G, vp, vp, i, vp]
+    L.dcell_tc_gemm_check.argtypes = [vp, vp, vp, vp]
+    for name in ("dcell_sl_step", "dcell_irregular_nodes", "dcell_max_velocity", "dcell_volume",
+                 "dcell_session_create", "dcell_session_destroy", "dcell_ls_advect_sl",
+                 "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_tc_gemm_check"):
+        getattr(L, name).restype = i
+    _LIB = L
+    return L
+
+
+def check(rc: int):
+    if rc != OK:
+        raise DcellError(rc, lib().dcell_last_error().decode(errors="replace"))
+
+
+def exported_symbols():
+    """Names the public header declares (for the load/export test)."""
+    hdr = os.path.join(os.path.dirname(PKG), "include", "dcell_ls.h")
+    import re
+    return re.findall(r"^DCELL_API [^(]*?\b(dcell_\w+)\(", open(hdr).read(), flags=re.M)

@@ -1,0 +1,381 @@
+// C ABI of the level-set transport path (include/dcell_ls.h).
+//
+// Validates arguments, maps them onto the kernel launchers and converts
+// device status flags into status codes.  The dcell_ls_* entry points are the
+// host-buffer drop-in for the reference's LevelSetAdvectSL,
+// LevelSetUpdateIrregularNodeList and LevelSet_MaxVelocity: they copy the
+// reference's FP64 arrays in, run the kernels and copy the results back.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
+#include "dcell_common.cuh"
+#include "dcell_kernels.h"
+
+int launch_tc_gemm_check(const float *A, float *D, int *flags, cudaStream_t st);
+
+namespace {
+thread_local char g_err[1024] = "";
+}
+
+extern "C" void dcell_set_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  int n = snprintf(g_err, sizeof(g_err), "[dcell %d] ", code);
+  if (n < 0) n = 0;
+  vsnprintf(g_err + n, sizeof(g_err) - (size_t)n, fmt, ap);
+  va_end(ap);
+}
+
+#define FAIL(code, ...)                  \
+  do {                                   \
+    dcell_set_error((code), __VA_ARGS__); \
+    return (code);                       \
+  } while (0)
+
+static int check_geom(const dcell_geom *g) {
+  if (!g) FAIL(DCELL_ERR_ARG, "geometry is NULL");
+  if (g->n[0] < 1 || g->n[1] < 1 || g->n[2] < 0)
+    FAIL(DCELL_ERR_ARG, "grid extents must be positive (got %d %d %d)", g->n[0], g->n[1], g->n[2]);
+  if (!(g->h[0] > 0) || !(g->h[1] > 0) || (g->n[2] > 1 && !(g->h[2] > 0)))
+    FAIL(DCELL_ERR_ARG, "grid spacing must be positive");
+  const long long n = (long long)g->n[0] * g->n[1] * (g->n[2] > 1 ? g->n[2] : 1);
+  if (n > (1LL << 40)) FAIL(DCELL_ERR_ARG, "grid too large");
+  return DCELL_OK;
+}
+
+static long long grid_points(const dcell_geom *g) {
+  return (long long)g->n[0] * g->n[1] * (g->n[2] > 1 ? g->n[2] : 1);
+}
+
+
+extern "C" {
+
+DCELL_API const char *dcell_last_error(void) { return g_err; }
+DCELL_API int dcell_version(void) { return DCELL_LS_VERSION; }
+
+DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt,
+                            const int *band, int nband, int interp, int backtrace, void *phi, int *flags,
+                            void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (interp < DCELL_LINEAR || interp > DCELL_CUBIC_TC) FAIL(DCELL_ERR_ARG, "unknown interpolation %d", interp);
+  if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+  if (!phi0 || !vel || !phi) FAIL(DCELL_ERR_ARG, "phi0, vel and phi must be device pointers");
+  if (band && nband < 0) FAIL(DCELL_ERR_ARG, "nband must be >= 0");
+  if (!(dt == dt)) FAIL(DCELL_ERR_NONFINITE, "dt is NaN");
+  const dcell::Geom G = dcell::to_geom(g);
+  const long long npts = band ? (long long)nband : grid_points(g);
+  if (npts == 0) return DCELL_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (interp == DCELL_LINEAR) return launch_sl_linear(G, dtype, phi0, vel, dt, band, npts, backtrace, phi, flags, st);
+  if (interp == DCELL_CUBIC_TC) {
+    if (dtype != DCELL_F32) FAIL(DCELL_ERR_UNSUPPORTED, "DCELL_CUBIC_TC computes in FP32 only");
+    if (G.nz == 1) FAIL(DCELL_ERR_UNSUPPORTED, "DCELL_CUBIC_TC is 3D only");
+    return launch_sl_tc(G, (const float *)phi0, (const float *)vel, dt, band, npts, backtrace, (float *)phi, flags,
+                        st);
+  }
+  return launch_sl_cubic(G, dtype, phi0, vel, dt, band, npts, interp, backtrace, phi, flags, st);
+}
+
+DCELL_API size_t dcell_irregular_nodes_scratch_bytes(int nband) { return irregular_scratch_bytes(nband < 0 ? 0 : nband); }
+
+DCELL_API int dcell_irregular_nodes(const dcell_geom *g, int dtype, const void *phi, const int *band, int nband,
+                                    int with_surface, dcell_irregular_node *nodes, int capacity, int *count,
+                                    void *scratch, size_t scratch_bytes, int *flags, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (!phi || !count || nband < 0 || (nband > 0 && !band)) FAIL(DCELL_ERR_ARG, "phi, band and count are required");
+  if (capacity < 0 || (capacity > 0 && !nodes)) FAIL(DCELL_ERR_ARG, "invalid node buffer");
+  if (nband > 0 && (!scratch || scratch_bytes < irregular_scratch_bytes(nband)))
+    FAIL(DCELL_ERR_ARG, "scratch must hold %zu bytes", irregular_scratch_bytes(nband));
+  return launch_irregular(dcell::to_geom(g), dtype, phi, band, nband, with_surface, nodes, capacity, count, scratch,
+                          flags, (cudaStream_t)stream);
+}
+
+DCELL_API int dcell_max_velocity(const dcell_geom *g, int dtype, const void *vel, const dcell_irregular_node *nodes,
+                                 const int *count, int capacity, double *maxvel, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (!vel || !count || !maxvel || capacity < 0 || (capacity > 0 && !nodes)) FAIL(DCELL_ERR_ARG, "missing pointer");
+  return launch_max_velocity(dcell::to_geom(g), dtype, vel, nodes, count, capacity, maxvel, (cudaStream_t)stream);
+}
+
+DCELL_API size_t dcell_volume_scratch_bytes(void) { return volume_scratch_bytes(); }
+
+DCELL_API int dcell_volume(const dcell_geom *g, int dtype, const void *phi, double eps, double *volume, void *scratch,
+                           size_t scratch_bytes, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (!phi || !volume) FAIL(DCELL_ERR_ARG, "phi and volume are required");
+  if (!(eps > 0)) FAIL(DCELL_ERR_ARG, "eps must be positive");
+  if (!scratch || scratch_bytes < volume_scratch_bytes())
+    FAIL(DCELL_ERR_ARG, "scratch must hold %zu bytes", volume_scratch_bytes());
+  return launch_volume(dcell::to_geom(g), dtype, phi, eps, volume, (double *)scratch, (cudaStream_t)stream);
+}
+
+DCELL_API int dcell_tc_gemm_check(const float *a, float *d, int *flags, void *stream) {
+  if (!a || !d) FAIL(DCELL_ERR_ARG, "a and d are required");
+  return launch_tc_gemm_check(a, d, flags, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Host-buffer session
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return DCELL_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      FAIL(DCELL_ERR_NOMEM, "cudaMalloc of %zu bytes failed", bytes);
+    }
+    cap = bytes;
+    return DCELL_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct dcell_session {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevBuf phi0_64, vel_64, phi_64, phi0_32, vel_32, phi_32, stage32, band, vals, nodes, scratch, small;
+  std::vector<double> host_vals;
+};
+
+#define ENSURE(buf, bytes)             \
+  do {                                 \
+    int _r = (buf).ensure(bytes);      \
+    if (_r) return _r;                 \
+  } while (0)
+
+static int session_flags_status(dcell_session *s, int flags) {
+  if (flags & DCELL_FLAG_WAIT_TIMEOUT) FAIL(DCELL_ERR_TIMEOUT, "a device-side wait timed out");
+  if (flags & DCELL_FLAG_CAPACITY) FAIL(DCELL_ERR_CAPACITY, "node capacity exceeded");
+  if (flags & DCELL_FLAG_DEPARTURE_CLAMPED)
+    FAIL(DCELL_ERR_DEPARTURE, "a departure point left the grid; its sample was clamped to the grid");
+  (void)s;
+  return DCELL_OK;
+}
+
+static size_t band_index(const dcell_geom *g, const int *b) {
+  const int nz = g->n[2] > 1 ? g->n[2] : 1;
+  const int x = b[0] - g->p[0], y = b[1] - g->p[1], z = nz == 1 ? 0 : b[2] - g->p[2];
+  return ((size_t)z * g->n[1] + (size_t)y) * g->n[0] + (size_t)x;
+}
+
+static int check_band_host(const dcell_geom *g, const int *band, int nband) {
+  const int nz = g->n[2] > 1 ? g->n[2] : 1;
+  for (int b = 0; b < nband; ++b) {
+    const int *c = band + 3 * b;
+    if (c[0] < g->p[0] || c[0] >= g->p[0] + g->n[0] || c[1] < g->p[1] || c[1] >= g->p[1] + g->n[1] ||
+        (nz > 1 && (c[2] < g->p[2] || c[2] >= g->p[2] + nz)))
+      FAIL(DCELL_ERR_ARG, "band entry %d (%d,%d,%d) lies outside the grid", b, c[0], c[1], c[2]);
+  }
+  return DCELL_OK;
+}
+
+extern "C" {
+
+DCELL_API int dcell_session_create(int device, dcell_session **out) {
+  if (!out) FAIL(DCELL_ERR_ARG, "out is NULL");
+  *out = nullptr;
+  DCELL_CUDA_CHECK(cudaSetDevice(device));
+  dcell_session *s = new dcell_session();
+  s->device = device;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete s;
+    FAIL(DCELL_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  int rc = s->small.ensure(256);
+  if (rc) {
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return rc;
+  }
+  *out = s;
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_session_destroy(dcell_session *s) {
+  if (!s) return DCELL_OK;
+  cudaSetDevice(s->device);
+  cudaStreamSynchronize(s->stream);
+  for (DevBuf *b : {&s->phi0_64, &s->vel_64, &s->phi_64, &s->phi0_32, &s->vel_32, &s->phi_32, &s->stage32, &s->band, &s->vals,
+                    &s->nodes, &s->scratch, &s->small})
+    b->release();
+  cudaStreamDestroy(s->stream);
+  delete s;
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const double *phi0, const double *vel,
+                                 const int *band, int nband, double dt, int interp, int backtrace, int precision,
+                                 double *phi) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (!phi0 || !vel || !phi) FAIL(DCELL_ERR_ARG, "phi0, vel and phi are required");
+  if (precision != DCELL_F32 && precision != DCELL_F64) FAIL(DCELL_ERR_ARG, "precision must be F32 or F64");
+  if (band && nband < 0) FAIL(DCELL_ERR_ARG, "nband must be >= 0");
+  if (band) {
+    rc = check_band_host(g, band, nband);
+    if (rc) return rc;
+  }
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  const long long n = grid_points(g);
+  const int dof = g->n[2] > 1 ? 3 : 2;
+  const long long npts = band ? nband : n;
+  cudaStream_t st = s->stream;
+  ENSURE(s->phi0_64, n * sizeof(double));
+  ENSURE(s->vel_64, n * dof * sizeof(double));
+  int *dflags = (int *)s->small.p;
+  DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi0_64.p, phi0, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->vel_64.p, vel, n * dof * sizeof(double), cudaMemcpyHostToDevice, st));
+  const int *dband = nullptr;
+  if (band && nband > 0) {
+    ENSURE(s->band, (size_t)nband * 3 * sizeof(int));
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->band.p, band, (size_t)nband * 3 * sizeof(int), cudaMemcpyHostToDevice, st));
+    dband = (const int *)s->band.p;
+  }
+  const void *dphi0 = s->phi0_64.p, *dvel = s->vel_64.p;
+  void *dphi;
+  int dtype = precision;
+  if (precision == DCELL_F32) {
+    ENSURE(s->phi0_32, n * sizeof(float));
+    ENSURE(s->vel_32, n * dof * sizeof(float));
+    ENSURE(s->phi_32, n * sizeof(float));
+    if ((rc = launch_convert(s->phi0_64.p, DCELL_F64, s->phi0_32.p, DCELL_F32, n, st))) return rc;
+    if ((rc = launch_convert(s->vel_64.p, DCELL_F64, s->vel_32.p, DCELL_F32, n * dof, st))) return rc;
+    dphi0 = s->phi0_32.p;
+    dvel = s->vel_32.p;
+    dphi = s->phi_32.p;
+  } else {
+    ENSURE(s->phi_64, n * sizeof(double));
+    dphi = s->phi_64.p;
+  }
+  if (npts > 0) {
+    rc = dcell_sl_step(g, dtype, dphi0, dvel, dt, dband, band ? nband : 0, interp, backtrace, dphi, dflags, st);
+    if (rc) return rc;
+  }
+  // results back: band values (gathered) or the whole grid
+  if (band) {
+    if (nband > 0) {
+      ENSURE(s->vals, (size_t)nband * sizeof(double));
+      if (precision == DCELL_F32) {
+        // gather the FP32 band values, then widen them into vals
+        ENSURE(s->stage32, (size_t)nband * sizeof(float));
+        float *stage = (float *)s->stage32.p;
+        if ((rc = launch_gather_band(dcell::to_geom(g), DCELL_F32, s->phi_32.p, dband, nband, stage, st))) return rc;
+        if ((rc = launch_convert(stage, DCELL_F32, s->vals.p, DCELL_F64, nband, st))) return rc;
+      } else {
+        if ((rc = launch_gather_band(dcell::to_geom(g), DCELL_F64, s->phi_64.p, dband, nband, s->vals.p, st)))
+          return rc;
+      }
+      s->host_vals.resize((size_t)nband);
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(s->host_vals.data(), s->vals.p, (size_t)nband * sizeof(double),
+                                       cudaMemcpyDeviceToHost, st));
+    }
+  } else {
+    if (precision == DCELL_F32) {
+      if ((rc = launch_convert(s->phi_32.p, DCELL_F32, s->phi0_64.p, DCELL_F64, n, st))) return rc;
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(phi, s->phi0_64.p, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    } else {
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(phi, s->phi_64.p, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+  }
+  int hflags = 0;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(&hflags, dflags, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  if (band)
+    for (int b = 0; b < nband; ++b) phi[band_index(g, band + 3 * b)] = s->host_vals[(size_t)b];
+  return session_flags_status(s, hflags);
+}
+
+DCELL_API int dcell_ls_update_irregular_nodes(dcell_session *s, const dcell_geom *g, const double *phi,
+                                              const int *band, int nband, int with_surface, int precision,
+                                              dcell_irregular_node *nodes, int capacity, int *count) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (!phi || !count || nband < 0 || (nband > 0 && !band)) FAIL(DCELL_ERR_ARG, "phi, band and count are required");
+  if (capacity < 0 || (capacity > 0 && !nodes)) FAIL(DCELL_ERR_ARG, "invalid node buffer");
+  if (precision != DCELL_F32 && precision != DCELL_F64) FAIL(DCELL_ERR_ARG, "precision must be F32 or F64");
+  if ((rc = check_band_host(g, band, nband))) return rc;
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long n = grid_points(g);
+  ENSURE(s->phi_64, n * sizeof(double));
+  int *dflags = (int *)s->small.p;
+  int *dcount = dflags + 1;
+  DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, 2 * sizeof(int), st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi_64.p, phi, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  const void *dphi = s->phi_64.p;
+  if (precision == DCELL_F32) {
+    ENSURE(s->phi_32, n * sizeof(float));
+    if ((rc = launch_convert(s->phi_64.p, DCELL_F64, s->phi_32.p, DCELL_F32, n, st))) return rc;
+    dphi = s->phi_32.p;
+  }
+  if (nband > 0) {
+    ENSURE(s->band, (size_t)nband * 3 * sizeof(int));
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->band.p, band, (size_t)nband * 3 * sizeof(int), cudaMemcpyHostToDevice, st));
+  }
+  const size_t sb = irregular_scratch_bytes(nband);
+  ENSURE(s->scratch, sb);
+  ENSURE(s->nodes, (size_t)(capacity > 0 ? capacity : 1) * sizeof(dcell_irregular_node));
+  rc = dcell_irregular_nodes(g, precision, dphi, (const int *)s->band.p, nband, with_surface,
+                             (dcell_irregular_node *)s->nodes.p, capacity, dcount, s->scratch.p, sb, dflags, st);
+  if (rc) return rc;
+  int hv[2] = {0, 0};
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(hv, dflags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  *count = hv[1];
+  const int ncopy = hv[1] < capacity ? hv[1] : capacity;
+  if (ncopy > 0)
+    DCELL_CUDA_CHECK(cudaMemcpy(nodes, s->nodes.p, (size_t)ncopy * sizeof(dcell_irregular_node), cudaMemcpyDeviceToHost));
+  return session_flags_status(s, hv[0]);
+}
+
+DCELL_API int dcell_ls_max_velocity(dcell_session *s, const dcell_geom *g, const double *vel,
+                                    const dcell_irregular_node *nodes, int count, double *maxvel) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (!vel || !maxvel || count < 0 || (count > 0 && !nodes)) FAIL(DCELL_ERR_ARG, "vel, nodes and maxvel are required");
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long n = grid_points(g);
+  const int dof = g->n[2] > 1 ? 3 : 2;
+  ENSURE(s->vel_64, n * dof * sizeof(double));
+  ENSURE(s->nodes, (size_t)(count > 0 ? count : 1) * sizeof(dcell_irregular_node));
+  int *dcount = (int *)s->small.p + 1;
+  double *dmax = (double *)((char *)s->small.p + 64);
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->vel_64.p, vel, n * dof * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (count > 0)
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->nodes.p, nodes, (size_t)count * sizeof(dcell_irregular_node),
+                                     cudaMemcpyHostToDevice, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(dcount, &count, sizeof(int), cudaMemcpyHostToDevice, st));
+  rc = dcell_max_velocity(g, DCELL_F64, s->vel_64.p, (const dcell_irregular_node *)s->nodes.p, dcount, count, dmax, st);
+  if (rc) return rc;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(maxvel, dmax, sizeof(double), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  return DCELL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,27 @@
+// Internal launcher interface between the CUDA translation units and the
+// C ABI (capi.cu).  Not part of the public header.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "dcell_common.cuh"
+
+int launch_sl_linear(const dcell::Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
+                     long long npts, int backtrace, void *phi, int *flags, cudaStream_t st);
+int launch_sl_cubic(const dcell::Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
+                    long long npts, int interp, int backtrace, void *phi, int *flags, cudaStream_t st);
+int launch_sl_tc(const dcell::Geom &g, const float *phi0, const float *vel, double dt, const int *band,
+                 long long npts, int backtrace, float *phi, int *flags, cudaStream_t st);
+
+size_t irregular_scratch_bytes(int nband);
+int launch_irregular(const dcell::Geom &g, int dtype, const void *phi, const int *band, int nband, int with_surface,
+                     dcell_irregular_node *nodes, int cap, int *count, void *scratch, int *flags, cudaStream_t st);
+int launch_max_velocity(const dcell::Geom &g, int dtype, const void *vel, const dcell_irregular_node *nodes,
+                        const int *count, int cap, double *out, cudaStream_t st);
+size_t volume_scratch_bytes();
+int launch_volume(const dcell::Geom &g, int dtype, const void *phi, double eps, double *out, double *partial,
+                  cudaStream_t st);
+
+int launch_convert(const void *src, int src_dtype, void *dst, int dst_dtype, long long n, cudaStream_t st);
+int launch_gather_band(const dcell::Geom &g, int dtype, const void *phi, const int *band, int nband, void *out,
+                       cudaStream_t st);

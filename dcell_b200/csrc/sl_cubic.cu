@@ -1,0 +1,190 @@
+// Cubic semi-Lagrangian kernels on CUDA cores (FP32 and FP64).
+//
+// Reconstruction at the departure point is the Catmull-Rom tricubic
+// (bicubic in 2D) of the reference's TricubicInverse.h /
+// OrthogonalProjection.c:48-63, which is the tensor product C (x) C (x) C of
+// the 1-D Keys a=-1/2 matrix.  Two forms of the same interpolant:
+//
+//   PLAIN      per point: gather the 4^3 stencil, form the 64 coefficients
+//              with the 1331 non-zeros of the 64x64 operator, evaluate the
+//              64-term polynomial -- the reference's own arithmetic shape and
+//              the "plain FP32 CUDA SL step";
+//   SEPARABLE  per point: 4-tap weights per axis, 64 + 16 + 4 multiply-adds.
+//
+// Band structure and backtrace follow LevelSetAdvectSL_2D/_3D
+// (LevelSetMethod/AdvectSL.c:23-89).  The FP64 instantiation of PLAIN is
+// the GPU FP64 oracle used to measure errors on grids too large for the CPU.
+#include "dcell_common.cuh"
+#include "dcell_kernels.h"
+#include "sl_device.cuh"
+#include "catmull_rom_ops.inc"
+
+namespace dcell {
+
+template <typename T, int DIM>
+__device__ __forceinline__ T cubic_plain(const Geom &g, const T *__restrict__ phi0, const int c[3], const T f[3]) {
+  if (DIM == 3) {
+    T s[64];
+#pragma unroll
+    for (int z = 0; z < 4; ++z)
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+#pragma unroll
+        for (int x = 0; x < 4; ++x) s[x + 4 * y + 16 * z] = phi0[gidx(g, c[0] - 1 + x, c[1] - 1 + y, c[2] - 1 + z)];
+    // a = M s with M = C (x) C (x) C: the 1331 non-zeros as straight-line code
+    T a[64];
+    DCELL_CR_COEFS3(s, a);
+    // p = sum a[i + 4j + 16k] x^i y^j z^k, Horner per axis
+    T pz = T(0);
+#pragma unroll
+    for (int k = 3; k >= 0; --k) {
+      T py = T(0);
+#pragma unroll
+      for (int j = 3; j >= 0; --j) {
+        const T *r = a + 4 * j + 16 * k;
+        const T px = ((r[3] * f[0] + r[2]) * f[0] + r[1]) * f[0] + r[0];
+        py = py * f[1] + px;
+      }
+      pz = pz * f[2] + py;
+    }
+    return pz;
+  } else {
+    T s[16];
+#pragma unroll
+    for (int y = 0; y < 4; ++y)
+#pragma unroll
+      for (int x = 0; x < 4; ++x) s[x + 4 * y] = phi0[gidx(g, c[0] - 1 + x, c[1] - 1 + y, 0)];
+    T a[16];
+    DCELL_CR_COEFS2(s, a);
+    T py = T(0);
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+      const T *r = a + 4 * j;
+      const T px = ((r[3] * f[0] + r[2]) * f[0] + r[1]) * f[0] + r[0];
+      py = py * f[1] + px;
+    }
+    return py;
+  }
+}
+
+template <typename T, int DIM>
+__device__ __forceinline__ T cubic_separable(const Geom &g, const T *__restrict__ phi0, const int c[3], const T f[3]) {
+  T wx[4], wy[4];
+  cr_weights<T>(f[0], wx);
+  cr_weights<T>(f[1], wy);
+  if (DIM == 3) {
+    T wz[4];
+    cr_weights<T>(f[2], wz);
+    T acc = T(0);
+#pragma unroll
+    for (int z = 0; z < 4; ++z) {
+      T accy = T(0);
+#pragma unroll
+      for (int y = 0; y < 4; ++y) {
+        T accx = T(0);
+#pragma unroll
+        for (int x = 0; x < 4; ++x) accx += wx[x] * phi0[gidx(g, c[0] - 1 + x, c[1] - 1 + y, c[2] - 1 + z)];
+        accy += wy[y] * accx;
+      }
+      acc += wz[z] * accy;
+    }
+    return acc;
+  } else {
+    T acc = T(0);
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+      T accx = T(0);
+#pragma unroll
+      for (int x = 0; x < 4; ++x) accx += wx[x] * phi0[gidx(g, c[0] - 1 + x, c[1] - 1 + y, 0)];
+      acc += wy[y] * accx;
+    }
+    return acc;
+  }
+}
+
+template <typename T, int DIM, bool SEPARABLE>
+__global__ void __launch_bounds__(256) sl_cubic_kernel(Geom g, const T *__restrict__ phi0, const T *__restrict__ vel,
+                                                       T dt, const int *__restrict__ band, long long npts,
+                                                       int backtrace, T *__restrict__ phi, int *flags) {
+  const T dth[3] = {dt / (T)g.hx, dt / (T)g.hy, dt / (T)g.hz};
+  bool clamped = false;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npts;
+       q += (long long)gridDim.x * blockDim.x) {
+    int x, y, z, c[3];
+    T f[3];
+    arrival(g, band, q, x, y, z);
+    clamped |= departure_cell<T, DIM>(g, vel, dth, backtrace, x, y, z, c, f);
+    phi[gidx(g, x, y, z)] = SEPARABLE ? cubic_separable<T, DIM>(g, phi0, c, f) : cubic_plain<T, DIM>(g, phi0, c, f);
+  }
+  if (clamped) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);
+}
+
+// FP64 <-> FP32 conversion and band gathers for the host-buffer entry points.
+template <typename S, typename D>
+__global__ void convert_kernel(const S *__restrict__ src, D *__restrict__ dst, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    dst[q] = (D)src[q];
+}
+
+template <typename T>
+__global__ void gather_band_kernel(Geom g, const T *__restrict__ phi, const int *__restrict__ band, int nband,
+                                   T *__restrict__ out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nband) out[b] = phi[gidx(g, band[3 * b], band[3 * b + 1], g.nz == 1 ? 0 : band[3 * b + 2])];
+}
+
+}  // namespace dcell
+
+using namespace dcell;
+
+static inline int blocks_for(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  if (b > 148LL * 32) b = 148LL * 32;
+  return (int)(b < 1 ? 1 : b);
+}
+
+template <typename T>
+static void cubic_dispatch(const Geom &g, const T *phi0, const T *vel, T dt, const int *band, long long npts,
+                           int interp, int backtrace, T *phi, int *flags, cudaStream_t st) {
+  const int threads = 256, blocks = blocks_for(npts, threads);
+  const bool sep = interp == DCELL_CUBIC_SEPARABLE;
+  if (g.nz == 1) {
+    if (sep) sl_cubic_kernel<T, 2, true><<<blocks, threads, 0, st>>>(g, phi0, vel, dt, band, npts, backtrace, phi, flags);
+    else sl_cubic_kernel<T, 2, false><<<blocks, threads, 0, st>>>(g, phi0, vel, dt, band, npts, backtrace, phi, flags);
+  } else {
+    if (sep) sl_cubic_kernel<T, 3, true><<<blocks, threads, 0, st>>>(g, phi0, vel, dt, band, npts, backtrace, phi, flags);
+    else sl_cubic_kernel<T, 3, false><<<blocks, threads, 0, st>>>(g, phi0, vel, dt, band, npts, backtrace, phi, flags);
+  }
+}
+
+int launch_sl_cubic(const Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
+                    long long npts, int interp, int backtrace, void *phi, int *flags, cudaStream_t st) {
+  if (dtype == DCELL_F64)
+    cubic_dispatch<double>(g, (const double *)phi0, (const double *)vel, dt, band, npts, interp, backtrace,
+                           (double *)phi, flags, st);
+  else
+    cubic_dispatch<float>(g, (const float *)phi0, (const float *)vel, (float)dt, band, npts, interp, backtrace,
+                          (float *)phi, flags, st);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_convert(const void *src, int src_dtype, void *dst, int dst_dtype, long long n, cudaStream_t st) {
+  const int threads = 256, blocks = blocks_for(n, threads);
+  if (src_dtype == DCELL_F64 && dst_dtype == DCELL_F32)
+    convert_kernel<double, float><<<blocks, threads, 0, st>>>((const double *)src, (float *)dst, n);
+  else if (src_dtype == DCELL_F32 && dst_dtype == DCELL_F64)
+    convert_kernel<float, double><<<blocks, threads, 0, st>>>((const float *)src, (double *)dst, n);
+  else
+    return DCELL_ERR_ARG;
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_gather_band(const Geom &g, int dtype, const void *phi, const int *band, int nband, void *out,
+                       cudaStream_t st) {
+  if (nband <= 0) return DCELL_OK;
+  if (dtype == DCELL_F64)
+    gather_band_kernel<double><<<(nband + 255) / 256, 256, 0, st>>>(g, (const double *)phi, band, nband, (double *)out);
+  else
+    gather_band_kernel<float><<<(nband + 255) / 256, 256, 0, st>>>(g, (const float *)phi, band, nband, (float *)out);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}

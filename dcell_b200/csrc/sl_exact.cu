@@ -1,0 +1,931 @@
+// Reference-exact kernels of the level-set transport path.
+//
+// This translation unit is compiled with -fmad=false: every expression keeps
+// the reference's operation order with one rounding per operation, so in
+// FP64 the results are bit-identical to the reference's x86 double
+// arithmetic (Common/Grid.c, Grid3D.c, InterpolateVelocity.c, AdvectSL.c,
+// IrregularNodes*.c).  The FP32 instantiations follow the same order.
+//
+// Kernels:
+//   sl_linear_kernel     LevelSetAdvectSL_2D/_3D (AdvectSL.c:23-89)
+//   irr_count/irr_write  LevelSetUpdateIrregularNodeList_2D/_3D
+//   ortho_kernel         OrthogonalProjection2D/3D (8 threads per node)
+//   surface_kernel       IIMUpdateSurfaceQuantities normal + curvature
+//   maxvel_kernel        LevelSet_MaxVelocity (Advect.c:70-111)
+//   volume kernels       smoothed-Heaviside volume, deterministic FP64 sum
+#include <math.h>
+
+#include "dcell_common.cuh"
+#include "dcell_kernels.h"
+
+namespace dcell {
+
+// ---------------------------------------------------------------------------
+// MAC velocity interpolation: InterpolateVelocity2D/3D
+// (Common/InterpolateVelocity.c:7-67), same loop and operation order.
+template <typename T>
+__device__ __forceinline__ void interp_vel3(const Geom &g, const T *__restrict__ vel, const T X[3], T V[3]) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const T tx = d == 0 ? T(0.5) : T(0), ty = d == 1 ? T(0.5) : T(0), tz = d == 2 ? T(0.5) : T(0);
+    const int xs = (int)floor(X[0] + tx), ys = (int)floor(X[1] + ty), zs = (int)floor(X[2] + tz);
+    const T sx = X[0] - (T)xs + tx, sy = X[1] - (T)ys + ty, sz = X[2] - (T)zs + tz;
+    T sum = 0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+          sum += ((1 - sx) * (T)(1 - i) + (T)i * sx) * ((1 - sy) * (T)(1 - j) + (T)j * sy) *
+                 ((1 - sz) * (T)(1 - k) + (T)k * sz) * vel[gidx(g, xs + i, ys + j, zs + k) * 3 + d];
+    V[d] = sum;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void interp_vel2(const Geom &g, const T *__restrict__ vel, const T X[3], T V[3]) {
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    const T tx = d == 0 ? T(0.5) : T(0), ty = d == 1 ? T(0.5) : T(0);
+    const int xs = (int)floor(X[0] + tx), ys = (int)floor(X[1] + ty);
+    const T sx = X[0] - (T)xs + tx, sy = X[1] - (T)ys + ty;
+    T sum = 0;
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+        sum += ((1 - sx) * (T)(1 - i) + (T)i * sx) * ((1 - sy) * (T)(1 - j) + (T)j * sy) *
+               vel[gidx(g, xs + i, ys + j, 0) * 2 + d];
+    V[d] = sum;
+  }
+  V[2] = 0;
+}
+
+// Bilinear3D(GridFunction3D_Identity) (Grid3D.c:4-36).
+template <typename T>
+__device__ __forceinline__ T trilinear_ref(const Geom &g, const T *__restrict__ f, const T S[3]) {
+  const int xs = (int)floor(S[0]), ys = (int)floor(S[1]), zs = (int)floor(S[2]);
+  const T sx = S[0] - (T)xs, sy = S[1] - (T)ys, sz = S[2] - (T)zs;
+  T sum = 0;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const T xb = (T)i * sx + (T)(1 - i) * (1 - sx);
+        const T yb = (T)j * sy + (T)(1 - j) * (1 - sy);
+        const T zb = (T)k * sz + (T)(1 - k) * (1 - sz);
+        sum += f[gidx(g, xs + i, ys + j, zs + k)] * xb * yb * zb;
+      }
+  return sum;
+}
+
+// Bilinear2D(GridFunction2D_Identity) (Grid.c:190-217).
+template <typename T>
+__device__ __forceinline__ T bilinear_ref(const Geom &g, const T *__restrict__ f, T x, T y) {
+  const int xi = (int)floor(x), yi = (int)floor(y);
+  const T xf = (T(2.) * (x - (T)xi) - T(1.)), yf = (T(2.) * (y - (T)yi) - T(1.));
+  T sum = 0;
+#pragma unroll
+  for (int k = 0; k < 2; ++k)
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      const T xb = T(1.) + (T(2.) * (T)k - T(1.)) * xf;
+      const T yb = T(1.) + (T(2.) * (T)l - T(1.)) * yf;
+      sum += f[gidx(g, xi + k, yi + l, 0)] * xb * yb;
+    }
+  sum /= T(4.);
+  return sum;
+}
+
+template <typename T>
+__device__ __forceinline__ bool outside(const Geom &g, const T S[3]) {
+  return S[0] < (T)g.px || S[0] > (T)(g.px + g.nx - 1) || S[1] < (T)g.py || S[1] > (T)(g.py + g.ny - 1) ||
+         (g.nz > 1 && (S[2] < (T)g.pz || S[2] > (T)(g.pz + g.nz - 1)));
+}
+
+// Departure point of arrival X (AdvectSL.c:44-47 / :78-82; midpoint variant).
+template <typename T, int DIM>
+__device__ __forceinline__ void departure(const Geom &g, const T *__restrict__ vel, T dt, T hx, T hy, T hz,
+                                          int backtrace, const T X[3], T S[3]) {
+  T V[3];
+  if (DIM == 3) interp_vel3<T>(g, vel, X, V); else interp_vel2<T>(g, vel, X, V);
+  if (backtrace == DCELL_MIDPOINT) {
+    const T half = T(0.5) * dt;
+    T Xm[3] = {X[0] - V[0] * half / hx, X[1] - V[1] * half / hy, DIM == 3 ? X[2] - V[2] * half / hz : T(0)};
+    if (DIM == 3) interp_vel3<T>(g, vel, Xm, V); else interp_vel2<T>(g, vel, Xm, V);
+  }
+  S[0] = X[0] - V[0] * dt / hx;
+  S[1] = X[1] - V[1] * dt / hy;
+  S[2] = DIM == 3 ? X[2] - V[2] * dt / hz : T(0);
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) sl_linear_kernel(Geom g, const T *__restrict__ phi0, const T *__restrict__ vel,
+                                                        T dt, const int *__restrict__ band, long long npts, int backtrace,
+                                                        T *__restrict__ phi, int *flags) {
+  const T hx = (T)g.hx, hy = (T)g.hy, hz = (T)g.hz;
+  bool clamped = false;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npts;
+       q += (long long)gridDim.x * blockDim.x) {
+    int x, y, z;
+    arrival(g, band, q, x, y, z);
+    const T X[3] = {(T)x, (T)y, (T)z};
+    T S[3];
+    departure<T, DIM>(g, vel, dt, hx, hy, hz, backtrace, X, S);
+    clamped |= outside<T>(g, S);
+    phi[gidx(g, x, y, z)] = DIM == 3 ? trilinear_ref<T>(g, phi0, S) : bilinear_ref<T>(g, phi0, S[0], S[1]);
+  }
+  if (clamped) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);
+}
+
+// ---------------------------------------------------------------------------
+// Catmull-Rom operator (TricubicInverse.h == C (x) C (x) C; OrthogonalProjection.c:48-63 == C (x) C).
+__device__ __constant__ double kCR[4][4] = {
+    {0, 1, 0, 0}, {-0.5, 0, 0.5, 0}, {1, -2.5, 2, -0.5}, {-0.5, 1.5, -1.5, 0.5}};
+
+template <typename T>
+__device__ void cubic_coefs3(const T *s, T *a) {
+  for (int pz = 0; pz < 4; ++pz)
+    for (int py = 0; py < 4; ++py)
+      for (int px = 0; px < 4; ++px) {
+        T acc = 0;
+        for (int sz = 0; sz < 4; ++sz) {
+          const double cz = kCR[pz][sz];
+          if (cz == 0.0) continue;
+          for (int sy = 0; sy < 4; ++sy) {
+            const double cy = kCR[py][sy];
+            if (cy == 0.0) continue;
+            for (int sx = 0; sx < 4; ++sx) {
+              const double cx = kCR[px][sx];
+              if (cx == 0.0) continue;
+              acc += (T)(cz * cy * cx) * s[sx + 4 * sy + 16 * sz];
+            }
+          }
+        }
+        a[px + 4 * py + 16 * pz] = acc;
+      }
+}
+
+template <typename T>
+__device__ void cubic_coefs2(const T *s, T *a) {
+  for (int py = 0; py < 4; ++py)
+    for (int px = 0; px < 4; ++px) {
+      T acc = 0;
+      for (int sy = 0; sy < 4; ++sy) {
+        const double cy = kCR[py][sy];
+        if (cy == 0.0) continue;
+        for (int sx = 0; sx < 4; ++sx) {
+          const double cx = kCR[px][sx];
+          if (cx == 0.0) continue;
+          acc += (T)(cy * cx) * s[sx + 4 * sy];
+        }
+      }
+      a[px + 4 * py] = acc;
+    }
+}
+
+template <typename T>
+__device__ void cubic_eval3(const T *a, T x, T y, T z, T &p, T &gx, T &gy, T &gz) {
+  const T X[4] = {1, x, x * x, x * x * x}, Y[4] = {1, y, y * y, y * y * y}, Z[4] = {1, z, z * z, z * z * z};
+  const T dX[4] = {0, 1, 2 * x, 3 * x * x}, dY[4] = {0, 1, 2 * y, 3 * y * y}, dZ[4] = {0, 1, 2 * z, 3 * z * z};
+  T v = 0, vx = 0, vy = 0, vz = 0;
+  for (int k = 0; k < 4; ++k)
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const T c = a[i + 4 * j + 16 * k];
+        v += c * X[i] * Y[j] * Z[k];
+        vx += c * dX[i] * Y[j] * Z[k];
+        vy += c * X[i] * dY[j] * Z[k];
+        vz += c * X[i] * Y[j] * dZ[k];
+      }
+  p = v; gx = vx; gy = vy; gz = vz;
+}
+
+template <typename T>
+__device__ void cubic_eval2(const T *a, T x, T y, T &p, T &gx, T &gy) {
+  const T X[4] = {1, x, x * x, x * x * x}, Y[4] = {1, y, y * y, y * y * y};
+  const T dX[4] = {0, 1, 2 * x, 3 * x * x}, dY[4] = {0, 1, 2 * y, 3 * y * y};
+  T v = 0, vx = 0, vy = 0;
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const T c = a[i + 4 * j];
+      v += c * X[i] * Y[j];
+      vx += c * dX[i] * Y[j];
+      vy += c * X[i] * dY[j];
+    }
+  p = v; gx = vx; gy = vy;
+}
+
+// ---------------------------------------------------------------------------
+// Irregular nodes (IrregularNodes.c:32-141, IrregularNodes3D.c:6-117).
+// STAGGERED_GRID (Common.h:42-47): CELL_CENTER {0,0,0}, U {-1,0,0}, V {0,-1,0}, W {0,0,-1}.
+__device__ __forceinline__ int stag(int face, int axis) { return (face == axis + 1) ? -1 : 0; }
+
+// Visits the nodes of one band point in the reference's emission order.
+// EMIT(kind, args...) is a functor: kind 0 = projection node, 1 = cell-face
+// node (axis), 2 = velocity-face node (face, axis, hi, lo).
+template <typename T, int DIM, typename F>
+__device__ __forceinline__ void visit_point(const Geom &g, const T *__restrict__ phi, int i, int j, int k, F &emit) {
+  if (DIM == 3) {
+    T s[3][3][3];
+#pragma unroll
+    for (int K = 0; K < 3; ++K)
+#pragma unroll
+      for (int J = 0; J < 3; ++J)
+#pragma unroll
+        for (int I = 0; I < 3; ++I) s[K][J][I] = phi[gidx(g, i + I - 1, j + J - 1, k + K - 1)];
+    const T c = s[1][1][1];
+    // STAR order (Common.h:49-51): +x, -x, +y, -y, +z, -z; first sign change only.
+    const int star[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      if (c * s[1 + star[m][2]][1 + star[m][1]][1 + star[m][0]] <= T(0.)) {
+        emit.projection(c);
+        break;
+      }
+    }
+#pragma unroll
+    for (int f = 1; f <= 3; ++f) {
+      const T nb = s[1 + stag(f, 2)][1 + stag(f, 1)][1 + stag(f, 0)];
+      if (c * nb <= T(0.)) emit.cell_face(f - 1, c, nb);
+    }
+#pragma unroll
+    for (int face = 1; face <= 3; ++face) {
+      const T hi = (s[1 + stag(face, 2)][1 + stag(face, 1)][1 + stag(face, 0)] + c) / T(2.);
+#pragma unroll
+      for (int axis = 1; axis <= 3; ++axis) {
+        if (face == axis) continue;
+        const T lo = (s[1 + stag(face, 2) + stag(axis, 2)][1 + stag(face, 1) + stag(axis, 1)]
+                       [1 + stag(face, 0) + stag(axis, 0)] +
+                      s[1 + stag(axis, 2)][1 + stag(axis, 1)][1 + stag(axis, 0)]) /
+                     T(2.);
+        if (hi * lo <= T(0.)) emit.vel_face(face, axis - 1, hi, lo);
+      }
+    }
+  } else {
+    T s[3][3];
+#pragma unroll
+    for (int J = 0; J < 3; ++J)
+#pragma unroll
+      for (int I = 0; I < 3; ++I) s[J][I] = phi[gidx(g, i + I - 1, j + J - 1, 0)];
+    const T c = s[1][1];
+    const int nei[4][2] = {{1, 0}, {-1, 0}, {0, -1}, {0, 1}};  // IrregularNodes.c:36
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (c * s[1 + nei[m][1]][1 + nei[m][0]] <= T(0.)) {
+        emit.projection(c);
+        break;
+      }
+    }
+#pragma unroll
+    for (int f = 1; f <= 2; ++f) {
+      const T nb = s[1 + stag(f, 1)][1 + stag(f, 0)];
+      if (c * nb <= T(0.)) emit.cell_face(f - 1, c, nb);
+    }
+    // U-velocity Laplacian (IrregularNodes.c:108-122), V (:124-138)
+    T hi = (s[1][0] + s[1][1]) / T(2.), lo = (s[0][0] + s[0][1]) / T(2.);
+    if (hi * lo <= T(0.)) emit.vel_face(1, 1, hi, lo);
+    hi = (s[0][1] + s[1][1]) / T(2.);
+    lo = (s[0][0] + s[1][0]) / T(2.);
+    if (hi * lo <= T(0.)) emit.vel_face(2, 0, hi, lo);
+  }
+}
+
+struct CountEmit {
+  int n = 0;
+  template <typename T> __device__ void projection(T) { ++n; }
+  template <typename T> __device__ void cell_face(int, T, T) { ++n; }
+  template <typename T> __device__ void vel_face(int, int, T, T) { ++n; }
+};
+
+template <typename T, int DIM>
+struct WriteEmit {
+  dcell_irregular_node *out;
+  long long slot;
+  long long cap;
+  int i, j, k;
+  __device__ dcell_irregular_node *next() {
+    if (slot >= cap) { ++slot; return nullptr; }
+    dcell_irregular_node *r = out + slot++;
+    return r;
+  }
+  __device__ void base(dcell_irregular_node &r) {
+    r.pos[0] = i; r.pos[1] = j; r.pos[2] = k;
+    r.pad = 0;
+    r.d = 0; r.X[0] = r.X[1] = r.X[2] = 0; r.op[0] = r.op[1] = r.op[2] = 0;
+    r.n[0] = r.n[1] = r.n[2] = 0; r.k = 0;
+    r.signFace = 0;
+  }
+  __device__ void projection(T c) {
+    dcell_irregular_node *r = next();
+    if (!r) return;
+    dcell_irregular_node t; base(t);
+    t.axis = -1; t.shift = -1; t.signCenter = c > T(0.) ? 1 : -1;
+    t.X[0] = i; t.X[1] = j; t.X[2] = DIM == 3 ? k : 0;  // op (and X) filled by the projection kernel
+    *r = t;
+  }
+  __device__ void cell_face(int axis, T c, T nb) {
+    dcell_irregular_node *r = next();
+    if (!r) return;
+    dcell_irregular_node t; base(t);
+    const T d = c / (c - nb);
+    t.d = (double)d;
+    t.signCenter = c > T(0.) ? 1 : -1;
+    t.signFace = d < T(0.5) ? -t.signCenter : t.signCenter;
+    t.shift = 0; t.axis = axis;
+    // X = pos + d * STAGGERED_GRID[axis+1]  (the -1 component only)
+    t.X[0] = (double)((T)i + d * (T)stag(axis + 1, 0));
+    t.X[1] = (double)((T)j + d * (T)stag(axis + 1, 1));
+    t.X[2] = DIM == 3 ? (double)((T)k + d * (T)stag(axis + 1, 2)) : 0.0;
+    *r = t;
+  }
+  __device__ void vel_face(int face, int axis, T hi, T lo) {
+    dcell_irregular_node *r = next();
+    if (!r) return;
+    dcell_irregular_node t; base(t);
+    T d = hi / (hi - lo);
+    if (DIM == 3 && d != d) d = 0;
+    t.d = (double)d;
+    t.signCenter = hi > T(0.) ? 1 : -1;
+    t.signFace = d < T(0.5) ? -t.signCenter : t.signCenter;
+    t.shift = face; t.axis = axis;
+    if (DIM == 3) {
+      t.X[0] = (double)((T)i + (T)stag(face, 0) / T(2.) + d * (T)stag(axis + 1, 0));
+      t.X[1] = (double)((T)j + (T)stag(face, 1) / T(2.) + d * (T)stag(axis + 1, 1));
+      t.X[2] = (double)((T)k + (T)stag(face, 2) / T(2.) + d * (T)stag(axis + 1, 2));
+    } else if (face == 1) {  // U: X = (x - 1/2, y - d)
+      t.X[0] = (double)((T)i + (T)stag(1, 0) / T(2.));
+      t.X[1] = (double)((T)j + (T)stag(1, 1) / T(2.) - d);
+    } else {                 // V: X = (x - d, y - 1/2)
+      t.X[0] = (double)((T)i + (T)stag(2, 0) / T(2.) - d);
+      t.X[1] = (double)((T)j + (T)stag(2, 1) / T(2.));
+    }
+    *r = t;
+  }
+};
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) irr_count_kernel(Geom g, const T *__restrict__ phi, const int *__restrict__ band,
+                                                        int nband, int *__restrict__ counts) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nband) return;
+  CountEmit e;
+  visit_point<T, DIM>(g, phi, band[3 * b], band[3 * b + 1], DIM == 3 ? band[3 * b + 2] : 0, e);
+  counts[b] = e.n;
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) irr_write_kernel(Geom g, const T *__restrict__ phi, const int *__restrict__ band,
+                                                        int nband, const int *__restrict__ offsets,
+                                                        dcell_irregular_node *__restrict__ out, int cap) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nband) return;
+  WriteEmit<T, DIM> e;
+  e.out = out; e.slot = offsets[b]; e.cap = cap;
+  e.i = band[3 * b]; e.j = band[3 * b + 1]; e.k = DIM == 3 ? band[3 * b + 2] : band[3 * b + 2];
+  visit_point<T, DIM>(g, phi, e.i, e.j, DIM == 3 ? e.k : 0, e);
+}
+
+// ---------------------------------------------------------------------------
+// Block-level exclusive scan of int counts (3 passes): offsets[b], total.
+constexpr int SCAN_BLOCK = 1024;
+
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_blocks_kernel(const int *__restrict__ in, int n,
+                                                                 int *__restrict__ out, int *__restrict__ partial) {
+  __shared__ int warp_sums[SCAN_BLOCK / 32];
+  const int b = blockIdx.x * SCAN_BLOCK + threadIdx.x;
+  const int v = b < n ? in[b] : 0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += t;
+  }
+  if (lane == 31) warp_sums[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int y = warp_sums[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, y, o);
+      if (lane >= o) y += t;
+    }
+    warp_sums[lane] = y;
+  }
+  __syncthreads();
+  const int incl = x + (w > 0 ? warp_sums[w - 1] : 0);
+  if (b < n) out[b] = incl - v;
+  if (threadIdx.x == SCAN_BLOCK - 1) partial[blockIdx.x] = incl;
+}
+
+// Single block: exclusive scan of the per-block totals in place; total at partial[nblk].
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_partials_kernel(int *__restrict__ partial, int nblk) {
+  __shared__ int warp_sums[SCAN_BLOCK / 32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int base = 0; base < nblk; base += SCAN_BLOCK) {
+    const int b = base + threadIdx.x;
+    const int v = b < nblk ? partial[b] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += t;
+    }
+    if (lane == 31) warp_sums[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      int y = warp_sums[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= o) y += t;
+      }
+      warp_sums[lane] = y;
+    }
+    __syncthreads();
+    const int incl = x + (w > 0 ? warp_sums[w - 1] : 0);
+    const int c = carry;
+    if (b < nblk) partial[b] = c + incl - v;
+    __syncthreads();
+    if (threadIdx.x == SCAN_BLOCK - 1) carry = c + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[nblk] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) scan_add_kernel(int *__restrict__ out, int n,
+                                                              const int *__restrict__ partial, int nblk,
+                                                              int *__restrict__ total, int cap, int *flags) {
+  const int b = blockIdx.x * SCAN_BLOCK + threadIdx.x;
+  if (b < n) out[b] += partial[blockIdx.x];
+  if (b == 0) {
+    *total = partial[nblk];
+    if (partial[nblk] > cap) raise_flag(flags, FLAG_CAPACITY);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Orthogonal projection (OrthogonalProjection.c, OrthogonalProjection3D.c):
+// 8 threads per projection node, thread s = sub-cell (i,j,k) of the 2x2x2
+// (2D: 2x2) patches; the closest converged in-cell root wins (ties resolve to
+// the lowest sub-cell index, the reference's loop order).
+template <typename T>
+__device__ void ortho_quadratic3(const T s[3][3][3], T op[3]);
+template <typename T>
+__device__ void ortho_linear3(const T s[3][3][3], T op[3]) {
+  const int star[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  T mindist = 2;
+  for (int i = 0; i < 6; ++i) {
+    const T nb = s[star[i][2] + 1][star[i][1] + 1][star[i][0] + 1];
+    if (s[1][1][1] * nb <= 0) {
+      const T dist = s[1][1][1] / (s[1][1][1] - nb);
+      if (dist < mindist) {
+        mindist = dist;
+        op[0] = dist * (T)star[i][0];
+        op[1] = dist * (T)star[i][1];
+        op[2] = dist * (T)star[i][2];
+      }
+    }
+  }
+}
+template <typename T>
+__device__ void ortho_quadratic3(const T s[3][3][3], T op[3]) {
+  const T p = s[1][1][1];
+  const T px = (s[1][1][2] - s[1][1][0]) / T(2.), py = (s[1][2][1] - s[1][0][1]) / T(2.),
+          pz = (s[2][1][1] - s[0][1][1]) / T(2.);
+  const T px2 = px * px, py2 = py * py, pz2 = pz * pz;
+  const T pxx = (s[1][1][2] - T(2.) * p + s[1][1][0]);
+  const T pyy = (s[1][2][1] - T(2.) * p + s[1][0][1]);
+  const T pzz = (s[2][1][1] - T(2.) * p + s[0][1][1]);
+  const T pxy = (s[1][0][0] + s[1][2][2] - s[1][2][0] - s[1][0][2]) / T(4.);
+  const T pxz = (s[0][1][0] + s[2][1][2] - s[2][1][0] - s[0][1][2]) / T(4.);
+  const T pyz = (s[0][0][1] + s[2][2][1] - s[2][0][1] - s[0][2][1]) / T(4.);
+  const T pn = sqrt(px2 + py2 + pz2);
+  const T c = (px2 * pxx + py2 * pyy + pz2 * pzz + T(2) * px * py * pxy + T(2) * px * pz * pxz +
+               T(2) * py * pz * pyz) /
+              (px2 + py2 + pz2);
+  T a = 0;
+  for (int m = 0; m < 5; ++m) {
+    const T f = p + pn * a + T(0.5) * a * a * c;
+    const T df = pn + a * c;
+    a = a - f / df;
+  }
+  if (fabs(a) < T(1)) {
+    op[0] = a * px / pn;
+    op[1] = a * py / pn;
+    op[2] = a * pz / pn;
+  } else {
+    ortho_linear3<T>(s, op);
+  }
+}
+
+template <typename T>
+__device__ void ortho_linear2(const T s[3][3], T op[3], T &mindist) {
+  const int star[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+  mindist = 2;
+  for (int i = 0; i < 4; ++i) {
+    const T nb = s[star[i][1] + 1][star[i][0] + 1];
+    if (s[1][1] * nb <= 0) {
+      const T dist = s[1][1] / (s[1][1] - nb);
+      if (dist < mindist) {
+        mindist = dist;
+        op[0] = dist * (T)star[i][0];
+        op[1] = dist * (T)star[i][1];
+      }
+    }
+  }
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) ortho_kernel(Geom g, const T *__restrict__ phi,
+                                                    dcell_irregular_node *__restrict__ nodes,
+                                                    const int *__restrict__ count, int cap) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long node = tid >> 3;
+  const int sub = (int)(tid & 7);
+  const int n = min(*count, cap);
+  const bool active = node < n && nodes[node].axis == -1 && (DIM == 3 || sub < 4);
+  const T TOL = T(1e-3), TOL2 = TOL * TOL;
+  const double BIG = 1.7976931348623157e308;
+  double dist = BIG;
+  T res[3] = {0, 0, 0};
+  int ci = 0, cj = 0, ck = 0;
+  if (active) {
+    ci = nodes[node].pos[0]; cj = nodes[node].pos[1]; ck = DIM == 3 ? nodes[node].pos[2] : 0;
+    const int i = sub & 1, j = (sub >> 1) & 1, k = (sub >> 2) & 1;
+    T x0[3] = {(T)(1 - i), (T)(1 - j), (T)(1 - k)}, x = x0[0], y = x0[1], z = x0[2];
+    int m;
+    if (DIM == 3) {
+      T s[64], a[64];
+      for (int zz = 0; zz < 4; ++zz)
+        for (int yy = 0; yy < 4; ++yy)
+          for (int xx = 0; xx < 4; ++xx)
+            s[xx + 4 * yy + 16 * zz] = phi[gidx(g, ci - 2 + i + xx, cj - 2 + j + yy, ck - 2 + k + zz)];
+      cubic_coefs3<T>(s, a);
+      for (m = 0; m < 20; ++m) {
+        T p, gx, gy, gz;
+        cubic_eval3<T>(a, x, y, z, p, gx, gy, gz);
+        const T pp = gx * gx + gy * gy + gz * gz;
+        const T d1x = -p * gx / pp, d1y = -p * gy / pp, d1z = -p * gz / pp;
+        const T xp = (x0[0] - x) * gx + (x0[1] - y) * gy + (x0[2] - z) * gz;
+        const T d2x = (x0[0] - x) - xp / pp * gx, d2y = (x0[1] - y) - xp / pp * gy, d2z = (x0[2] - z) - xp / pp * gz;
+        x += d1x + T(0.5) * d2x;
+        y += d1y + T(0.5) * d2y;
+        z += d1z + T(0.5) * d2z;
+        const T norm = d1x * d1x + d1y * d1y + d1z * d1z + d2x * d2x + d2y * d2y + d2z * d2z;
+        if (norm < TOL2) break;
+      }
+      if (m < 20 && !(x < -TOL || 1 + TOL < x || y < -TOL || 1 + TOL < y || z < -TOL || 1 + TOL < z))
+        dist = (double)sqrt((x - x0[0]) * (x - x0[0]) + (y - x0[1]) * (y - x0[1]) + (z - x0[2]) * (z - x0[2]));
+      res[0] = x + (T)i - 1; res[1] = y + (T)j - 1; res[2] = z + (T)k - 1;
+    } else {
+      T s[16], a[16];
+      for (int yy = 0; yy < 4; ++yy)
+        for (int xx = 0; xx < 4; ++xx) s[xx + 4 * yy] = phi[gidx(g, ci - 2 + i + xx, cj - 2 + j + yy, 0)];
+      cubic_coefs2<T>(s, a);
+      for (m = 0; m < 20; ++m) {
+        T p, gx, gy;
+        cubic_eval2<T>(a, x, y, p, gx, gy);
+        const T pp = gx * gx + gy * gy;
+        const T d1x = -p * gx / pp, d1y = -p * gy / pp;
+        const T xp = (x0[0] - x) * gx + (x0[1] - y) * gy;
+        const T d2x = (x0[0] - x) - xp / pp * gx, d2y = (x0[1] - y) - xp / pp * gy;
+        x += d1x + T(0.5) * d2x;
+        y += d1y + T(0.5) * d2y;
+        const T norm = d1x * d1x + d1y * d1y + d2x * d2x + d2y * d2y;
+        if (norm < TOL2) break;
+      }
+      if (m < 20 && !(x < -TOL || 1 + TOL < x || y < -TOL || 1 + TOL < y))
+        dist = (double)sqrt((x - x0[0]) * (x - x0[0]) + (y - x0[1]) * (y - x0[1]));
+      res[0] = x + (T)i - 1; res[1] = y + (T)j - 1; res[2] = 0;
+    }
+  }
+  // min over the 8 sub-cells of this node (lanes 8q..8q+7), lowest index on ties
+  int best = sub;
+  double bd = dist;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    const double od = __shfl_xor_sync(0xffffffffu, bd, o, 8);
+    const int ob = __shfl_xor_sync(0xffffffffu, best, o, 8);
+    if (od < bd || (od == bd && ob < best)) { bd = od; best = ob; }
+  }
+  T w0 = __shfl_sync(0xffffffffu, res[0], best, 8);
+  T w1 = __shfl_sync(0xffffffffu, res[1], best, 8);
+  T w2 = __shfl_sync(0xffffffffu, res[2], best, 8);
+  if (!active || sub != 0) return;
+  T op[3] = {w0, w1, w2};
+  if (DIM == 3) {
+    if (bd == BIG) {  // no sub-cell converged: quadratic, then linear fallback
+      T s3[3][3][3];
+      for (int K = 0; K < 3; ++K)
+        for (int J = 0; J < 3; ++J)
+          for (int I = 0; I < 3; ++I) s3[K][J][I] = phi[gidx(g, ci + I - 1, cj + J - 1, ck + K - 1)];
+      op[0] = op[1] = op[2] = 0;
+      ortho_quadratic3<T>(s3, op);
+    }
+  } else {
+    T s3[3][3], opl[3] = {0, 0, 0}, dl;
+    for (int J = 0; J < 3; ++J)
+      for (int I = 0; I < 3; ++I) s3[J][I] = phi[gidx(g, ci + I - 1, cj + J - 1, 0)];
+    ortho_linear2<T>(s3, opl, dl);
+    if (!(bd < (double)dl)) { op[0] = opl[0]; op[1] = opl[1]; op[2] = 0; }
+  }
+  dcell_irregular_node &r = nodes[node];
+  r.op[0] = (double)op[0]; r.op[1] = (double)op[1]; r.op[2] = (double)op[2];
+  r.X[0] = (double)((T)ci + op[0]);
+  r.X[1] = (double)((T)cj + op[1]);
+  r.X[2] = DIM == 3 ? (double)((T)ck + op[2]) : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Grid functions (GridFunction2D_* Grid.c:214-254, GridFunction3D_* Grid3D.c:33-108).
+template <typename T>
+__device__ __forceinline__ T gf3(const Geom &g, const T *__restrict__ p, int fn, int i, int j, int k, T dx, T dy, T dz) {
+#define P(a, b, c) p[gidx(g, (a), (b), (c))]
+  switch (fn) {
+    case 0: return P(i, j, k);
+    case 1: return (P(i + 1, j, k) - P(i - 1, j, k)) / (T(2.0) * dx);
+    case 2: return (P(i, j + 1, k) - P(i, j - 1, k)) / (T(2.0) * dy);
+    case 3: return (P(i, j, k + 1) - P(i, j, k - 1)) / (T(2.0) * dz);
+    default: {
+      const T px = (P(i + 1, j, k) - P(i - 1, j, k)) / (T(2.0) * dx);
+      const T py = (P(i, j + 1, k) - P(i, j - 1, k)) / (T(2.0) * dy);
+      const T pz = (P(i, j, k + 1) - P(i, j, k - 1)) / (T(2.0) * dz);
+      const T px2 = px * px, py2 = py * py, pz2 = pz * pz;
+      const T ppp = px2 + py2 + pz2;
+      const T pxx = (P(i - 1, j, k) - T(2.) * P(i, j, k) + P(i + 1, j, k)) / (dx * dx);
+      const T pyy = (P(i, j - 1, k) - T(2.) * P(i, j, k) + P(i, j + 1, k)) / (dy * dy);
+      const T pzz = (P(i, j, k - 1) - T(2.) * P(i, j, k) + P(i, j, k + 1)) / (dz * dz);
+      const T pxy = (P(i - 1, j - 1, k) + P(i + 1, j + 1, k) - P(i - 1, j + 1, k) - P(i + 1, j - 1, k)) / (T(4.) * dx * dy);
+      const T pxz = (P(i - 1, j, k - 1) + P(i + 1, j, k + 1) - P(i - 1, j, k + 1) - P(i + 1, j, k - 1)) / (T(4.) * dx * dz);
+      const T pyz = (P(i, j - 1, k - 1) + P(i, j + 1, k + 1) - P(i, j - 1, k + 1) - P(i, j + 1, k - 1)) / (T(4.) * dy * dz);
+      T c = px2 * (pyy + pzz) + py2 * (pxx + pzz) + pz2 * (pxx + pyy);
+      c -= T(2.) * (px * py * pxy + px * pz * pxz + py * pz * pyz);
+      c /= sqrt(ppp * ppp * ppp);
+      if (c != c) c = 0;
+      return c;
+    }
+  }
+#undef P
+}
+
+template <typename T>
+__device__ __forceinline__ T gf2(const Geom &g, const T *__restrict__ p, int fn, int i, int j, T dx, T dy) {
+#define P(a, b) p[gidx(g, (a), (b), 0)]
+  switch (fn) {
+    case 0: return P(i, j);
+    case 1: return (P(i + 1, j) - P(i - 1, j)) / (T(2.) * dx);
+    case 2: return (P(i, j + 1) - P(i, j - 1)) / (T(2.) * dy);
+    case 3: return 0;
+    default: {
+      const T px = (P(i + 1, j) - P(i - 1, j)) / (T(2.) * dx);
+      const T py = (P(i, j + 1) - P(i, j - 1)) / (T(2.) * dy);
+      const T px2 = px * px, py2 = py * py;
+      const T pxx = (P(i - 1, j) - T(2.) * P(i, j) + P(i + 1, j)) / (dx * dx);
+      const T pyy = (P(i, j - 1) - T(2.) * P(i, j) + P(i, j + 1)) / (dy * dy);
+      const T pxy = (P(i - 1, j - 1) + P(i + 1, j + 1) - P(i - 1, j + 1) - P(i + 1, j - 1)) / (T(4.) * dx * dy);
+      T k = (pxx * py2 - T(2.) * px * py * pxy + pyy * px2) / sqrt((px2 + py2) * (px2 + py2) * (px2 + py2));
+      if (k != k) k = 0;
+      return k;
+    }
+  }
+#undef P
+}
+
+// Bilinear3D / Bilinear2D of grid function fn at X.
+template <typename T, int DIM>
+__device__ T sample_gf(const Geom &g, const T *__restrict__ p, int fn, const T X[3]) {
+  const T dx = (T)g.hx, dy = (T)g.hy, dz = (T)g.hz;
+  if (DIM == 2) {
+    const int xi = (int)floor(X[0]), yi = (int)floor(X[1]);
+    const T xf = (T(2.) * (X[0] - (T)xi) - T(1.)), yf = (T(2.) * (X[1] - (T)yi) - T(1.));
+    T sum = 0;
+    for (int k = 0; k < 2; ++k)
+      for (int l = 0; l < 2; ++l) {
+        const T xb = T(1.) + (T(2.) * (T)k - T(1.)) * xf;
+        const T yb = T(1.) + (T(2.) * (T)l - T(1.)) * yf;
+        sum += gf2<T>(g, p, fn, xi + k, yi + l, dx, dy) * xb * yb;
+      }
+    sum /= T(4.);
+    return sum;
+  }
+  const int xs = (int)floor(X[0]), ys = (int)floor(X[1]), zs = (int)floor(X[2]);
+  const T sx = X[0] - (T)xs, sy = X[1] - (T)ys, sz = X[2] - (T)zs;
+  T sum = 0;
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j)
+      for (int k = 0; k < 2; ++k) {
+        const T xb = (T)i * sx + (T)(1 - i) * (1 - sx);
+        const T yb = (T)j * sy + (T)(1 - j) * (1 - sy);
+        const T zb = (T)k * sz + (T)(1 - k) * (1 - sz);
+        sum += gf3<T>(g, p, fn, xs + i, ys + j, zs + k, dx, dy, dz) * xb * yb * zb;
+      }
+  return sum;
+}
+
+// Normal and curvature at node X (IIM/SurfaceQuantities.c 2D:48-56, 3D:83-89,111).
+template <typename T, int DIM>
+__global__ void __launch_bounds__(128) surface_kernel(Geom g, const T *__restrict__ phi,
+                                                      dcell_irregular_node *__restrict__ nodes,
+                                                      const int *__restrict__ count, int cap) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int n = min(*count, cap);
+  if (q >= n) return;
+  dcell_irregular_node &r = nodes[q];
+  const T X[3] = {(T)r.X[0], (T)r.X[1], (T)r.X[2]};
+  if (DIM == 2) {
+    const T nx = sample_gf<T, 2>(g, phi, 1, X), ny = sample_gf<T, 2>(g, phi, 2, X);
+    const T h = sqrt(nx * nx + ny * ny);
+    r.n[0] = (double)(nx / h); r.n[1] = (double)(ny / h); r.n[2] = 0.0;
+    r.k = (double)sample_gf<T, 2>(g, phi, 4, X);
+  } else {
+    T nx = sample_gf<T, 3>(g, phi, 1, X), ny = sample_gf<T, 3>(g, phi, 2, X), nz = sample_gf<T, 3>(g, phi, 3, X);
+    const T h = sqrt(nx * nx + ny * ny + nz * nz);
+    nx /= h; ny /= h; nz /= h;
+    r.n[0] = (double)nx; r.n[1] = (double)ny; r.n[2] = (double)nz;
+    r.k = (double)sample_gf<T, 3>(g, phi, 4, X);
+  }
+}
+
+// LevelSet_MaxVelocity: max |V(pos)| over nodes; non-negative doubles order
+// like their bit patterns, so an integer atomicMax is exact and deterministic.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) maxvel_kernel(Geom g, const T *__restrict__ vel,
+                                                     const dcell_irregular_node *__restrict__ nodes,
+                                                     const int *__restrict__ count, int cap,
+                                                     unsigned long long *__restrict__ out) {
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int n = min(*count, cap);
+  double mag = 0.0;
+  if (q < n) {
+    const T X[3] = {(T)nodes[q].pos[0], (T)nodes[q].pos[1], DIM == 3 ? (T)nodes[q].pos[2] : T(0)};
+    T V[3];
+    if (DIM == 3) {
+      interp_vel3<T>(g, vel, X, V);
+      mag = (double)sqrt(V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+    } else {
+      interp_vel2<T>(g, vel, X, V);
+      mag = (double)sqrt(V[0] * V[0] + V[1] * V[1]);
+    }
+  }
+  unsigned long long bits = (unsigned long long)__double_as_longlong(mag);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long t = __shfl_xor_sync(0xffffffffu, bits, o);
+    bits = t > bits ? t : bits;
+  }
+  if ((threadIdx.x & 31) == 0 && bits) atomicMax(out, bits);
+}
+
+// Smoothed-Heaviside volume: fixed grid, fixed per-thread strides and a fixed
+// reduction tree -> bitwise reproducible.
+constexpr int VOL_BLOCKS = 148 * 4;
+constexpr int VOL_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(VOL_THREADS) volume_partial_kernel(const T *__restrict__ phi, long long n, double eps,
+                                                                     double *__restrict__ partial) {
+  __shared__ double ws[VOL_THREADS / 32];
+  const double pi = 3.14159265358979323846264;
+  double acc = 0.0;
+  for (long long q = blockIdx.x * (long long)VOL_THREADS + threadIdx.x; q < n; q += (long long)VOL_BLOCKS * VOL_THREADS) {
+    const double p = (double)phi[q];
+    double H;
+    if (p < -eps) H = 0.0;
+    else if (p > eps) H = 1.0;
+    else H = 0.5 * (1.0 + p / eps + sin(pi * p / eps) / pi);
+    acc += 1.0 - H;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < VOL_THREADS / 32; ++w) s += ws[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+__global__ void __launch_bounds__(32) volume_final_kernel(const double *__restrict__ partial, double cell,
+                                                          double *__restrict__ out) {
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < VOL_BLOCKS; b += 32) acc += partial[b];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (threadIdx.x == 0) *out = acc * cell;
+}
+
+}  // namespace dcell
+
+// ===========================================================================
+// Launchers (declared in dcell_kernels.h)
+using namespace dcell;
+
+static inline int grid_for(long long n, int threads) {
+  long long b = (n + threads - 1) / threads;
+  if (b > 148LL * 64) b = 148LL * 64;
+  return (int)(b < 1 ? 1 : b);
+}
+
+int launch_sl_linear(const Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
+                     long long npts, int backtrace, void *phi, int *flags, cudaStream_t st) {
+  const int threads = 256, blocks = grid_for(npts, threads);
+  const bool is2d = g.nz == 1;
+  if (dtype == DCELL_F64) {
+    if (is2d)
+      sl_linear_kernel<double, 2><<<blocks, threads, 0, st>>>(g, (const double *)phi0, (const double *)vel, dt, band,
+                                                              npts, backtrace, (double *)phi, flags);
+    else
+      sl_linear_kernel<double, 3><<<blocks, threads, 0, st>>>(g, (const double *)phi0, (const double *)vel, dt, band,
+                                                              npts, backtrace, (double *)phi, flags);
+  } else {
+    if (is2d)
+      sl_linear_kernel<float, 2><<<blocks, threads, 0, st>>>(g, (const float *)phi0, (const float *)vel, (float)dt,
+                                                             band, npts, backtrace, (float *)phi, flags);
+    else
+      sl_linear_kernel<float, 3><<<blocks, threads, 0, st>>>(g, (const float *)phi0, (const float *)vel, (float)dt,
+                                                             band, npts, backtrace, (float *)phi, flags);
+  }
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+size_t irregular_scratch_bytes(int nband) {
+  const size_t nblk = ((size_t)nband + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  return sizeof(int) * ((size_t)nband + 1 + nblk + 1) + 256;
+}
+
+template <typename T, int DIM>
+static void irr_launch(const Geom &g, const T *phi, const int *band, int nband, int with_surface,
+                       dcell_irregular_node *nodes, int cap, int *count, int *offsets, int *partial, int *flags,
+                       cudaStream_t st) {
+  const int nblk = (nband + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  irr_count_kernel<T, DIM><<<(nband + 255) / 256, 256, 0, st>>>(g, phi, band, nband, offsets);
+  scan_blocks_kernel<<<nblk, SCAN_BLOCK, 0, st>>>(offsets, nband, offsets, partial);
+  scan_partials_kernel<<<1, SCAN_BLOCK, 0, st>>>(partial, nblk);
+  scan_add_kernel<<<nblk, SCAN_BLOCK, 0, st>>>(offsets, nband, partial, nblk, count, cap, flags);
+  irr_write_kernel<T, DIM><<<(nband + 255) / 256, 256, 0, st>>>(g, phi, band, nband, offsets, nodes, cap);
+  // projection nodes: 8 threads each; bounded by the capacity
+  const long long nthreads = 8LL * cap;
+  ortho_kernel<T, DIM><<<(int)((nthreads + 255) / 256), 256, 0, st>>>(g, phi, nodes, count, cap);
+  if (with_surface) surface_kernel<T, DIM><<<(cap + 127) / 128, 128, 0, st>>>(g, phi, nodes, count, cap);
+}
+
+int launch_irregular(const Geom &g, int dtype, const void *phi, const int *band, int nband, int with_surface,
+                     dcell_irregular_node *nodes, int cap, int *count, void *scratch, int *flags, cudaStream_t st) {
+  int *offsets = (int *)scratch;
+  int *partial = offsets + nband + 1;
+  if (nband == 0) {
+    cudaMemsetAsync(count, 0, sizeof(int), st);
+    return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+  }
+  const bool is2d = g.nz == 1;
+  if (dtype == DCELL_F64) {
+    if (is2d) irr_launch<double, 2>(g, (const double *)phi, band, nband, with_surface, nodes, cap, count, offsets, partial, flags, st);
+    else irr_launch<double, 3>(g, (const double *)phi, band, nband, with_surface, nodes, cap, count, offsets, partial, flags, st);
+  } else {
+    if (is2d) irr_launch<float, 2>(g, (const float *)phi, band, nband, with_surface, nodes, cap, count, offsets, partial, flags, st);
+    else irr_launch<float, 3>(g, (const float *)phi, band, nband, with_surface, nodes, cap, count, offsets, partial, flags, st);
+  }
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_max_velocity(const Geom &g, int dtype, const void *vel, const dcell_irregular_node *nodes,
+                        const int *count, int cap, double *out, cudaStream_t st) {
+  cudaMemsetAsync(out, 0, sizeof(double), st);
+  if (cap <= 0) return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+  const int blocks = (cap + 255) / 256;
+  unsigned long long *o = (unsigned long long *)out;
+  const bool is2d = g.nz == 1;
+  if (dtype == DCELL_F64) {
+    if (is2d) maxvel_kernel<double, 2><<<blocks, 256, 0, st>>>(g, (const double *)vel, nodes, count, cap, o);
+    else maxvel_kernel<double, 3><<<blocks, 256, 0, st>>>(g, (const double *)vel, nodes, count, cap, o);
+  } else {
+    if (is2d) maxvel_kernel<float, 2><<<blocks, 256, 0, st>>>(g, (const float *)vel, nodes, count, cap, o);
+    else maxvel_kernel<float, 3><<<blocks, 256, 0, st>>>(g, (const float *)vel, nodes, count, cap, o);
+  }
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+size_t volume_scratch_bytes() { return sizeof(double) * VOL_BLOCKS; }
+
+int launch_volume(const Geom &g, int dtype, const void *phi, double eps, double *out, double *partial,
+                  cudaStream_t st) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  const double cell = g.hx * g.hy * (g.nz == 1 ? 1.0 : g.hz);
+  if (dtype == DCELL_F64)
+    volume_partial_kernel<double><<<VOL_BLOCKS, VOL_THREADS, 0, st>>>((const double *)phi, n, eps, partial);
+  else
+    volume_partial_kernel<float><<<VOL_BLOCKS, VOL_THREADS, 0, st>>>((const float *)phi, n, eps, partial);
+  volume_final_kernel<<<1, 32, 0, st>>>(partial, cell, out);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}

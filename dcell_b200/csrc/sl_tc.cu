@@ -1,0 +1,359 @@
+// Split-BF16 tensor-core tricubic semi-Lagrangian step (sm_100a, tcgen05).
+//
+// Per departure point the 64 Catmull-Rom coefficients are a = M s, with s the
+// 4^3 stencil of phi0 around the departure cell and M the fixed 64x64
+// operator of the reference's TricubicInverse.h (= C (x) C (x) C, every entry
+// exact in BF16).  The kernel batches that contraction over 128 points per
+// MMA:
+//
+//     D[128 points x 64 coefs] = A[128 x 128] * B[128 x 64]
+//       A row p = [ bf16_hi(s_p - r_p) | bf16_lo(s_p - r_p) ]   (K = 64 + 64)
+//       B       = [ M^T ; M^T ]                                  (BF16, exact)
+//       D       = FP32 accumulator in tensor memory
+//
+// r_p = phi0 at the departure cell (stencil entry (1,1,1)); subtracting it
+// shrinks the dynamic range before the split and is exact algebraically
+// (M maps the constant stencil to the constant monomial).  hi + lo carry
+// ~16 significant bits of each stencil difference.
+//
+// Data path per CTA (128 threads = 4 warps, thread t <-> TMEM lane t):
+//   1. each thread backtraces its point (integer cell + FP32 fraction),
+//      gathers its 64 stencil values, splits them and writes its A row into
+//      TMEM with tcgen05.st (A is the MMA's TMEM operand, no shared-memory
+//      staging of the gathered stencils);
+//   2. one thread issues 8 tcgen05.mma (M=128, N=64, K=16; 4 K-steps for hi,
+//      4 for lo, B from shared memory) and a tcgen05.commit to an mbarrier;
+//   3. every thread waits (bounded) on the mbarrier, reads its 64
+//      coefficients with tcgen05.ld, evaluates the tricubic polynomial at its
+//      fraction (Horner) and adds r back.
+// Several CTAs per SM (128 TMEM columns each) overlap one CTA's gathers with
+// another's MMA.  Band structure and backtrace follow LevelSetAdvectSL_3D
+// (LevelSetMethod/AdvectSL.c:56-89).
+#include <cuda_bf16.h>
+
+#include "dcell_common.cuh"
+#include "dcell_kernels.h"
+#include "sl_device.cuh"
+
+namespace dcell {
+namespace tc {
+
+constexpr int kTile = 128;       // points per MMA (M)
+constexpr int kCoef = 64;        // coefficients (N)
+constexpr int kTmemCols = 128;   // A: 64 columns (hi 32 + lo 32), D: 64 columns
+constexpr int kBBytes = kCoef * 64 * 2;  // B: 64 rows x 64 K of bf16 (reused for hi and lo)
+constexpr int kDynSmem = 56 * 1024;      // caps residency at 4 CTAs/SM = 512 TMEM columns
+constexpr unsigned kWaitLimit = 1u << 20;  // bounded mbarrier polls (a normal MMA completes in microseconds)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle: 8-row x 16-byte core
+// matrices; LBO = byte stride between K-adjacent core matrices, SBO = byte
+// stride between 8-row groups; version 1 (sm_100) in bits 46-47.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: D F32, A/B BF16, both K-major, N, M.
+__host__ __device__ constexpr uint32_t instr_desc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Byte offset of element (row n, k) of a K-major no-swizzle operand with K = 64.
+__device__ __forceinline__ int b_offset(int n, int k) {
+  return (((n >> 3) * 8 + (k >> 3)) * 128) + (n & 7) * 16 + (k & 7) * 2;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Bounded wait for phase `parity` of the mbarrier; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (unsigned it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, int ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, int ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+#define DCELL_R8(b) "r"(v[b + 0]), "r"(v[b + 1]), "r"(v[b + 2]), "r"(v[b + 3]), "r"(v[b + 4]), "r"(v[b + 5]), \
+                    "r"(v[b + 6]), "r"(v[b + 7])
+// 32 consecutive 32-bit columns of this thread's lane <- v[0..31]
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t *v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+      DCELL_R8(0), DCELL_R8(8), DCELL_R8(16), DCELL_R8(24)
+      : "memory");
+}
+#undef DCELL_R8
+
+#define DCELL_W8(b) "=r"(v[b + 0]), "=r"(v[b + 1]), "=r"(v[b + 2]), "=r"(v[b + 3]), "=r"(v[b + 4]), "=r"(v[b + 5]), \
+                    "=r"(v[b + 6]), "=r"(v[b + 7])
+// v[0..31] <- 32 consecutive 32-bit columns of this thread's lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : DCELL_W8(0), DCELL_W8(8), DCELL_W8(16), DCELL_W8(24)
+      : "r"(taddr)
+      : "memory");
+}
+#undef DCELL_W8
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// Shared state and one-time set-up of a CTA: B operand, mbarrier, TMEM.
+struct Ctx {
+  uint32_t tmem;      // base TMEM address (lane 0, first column)
+  uint32_t lane_off;  // this warp's lane quarter, in TMEM address units
+  uint64_t bdesc;     // descriptor of B at K-step 0
+};
+
+__device__ __forceinline__ void setup(uint8_t *sB, uint64_t *bar, uint32_t *tmem_slot, Ctx &c) {
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int e = tid; e < kCoef * 64; e += blockDim.x) {
+    const int n = e >> 6, k = e & 63;  // B[n][k] = M[n][k]: coefficient n from stencil entry k
+    const float w = cr_coef(n >> 4, k >> 4) * cr_coef((n >> 2) & 3, (k >> 2) & 3) * cr_coef(n & 3, k & 3);
+    *reinterpret_cast<__nv_bfloat16 *>(sB + b_offset(n, k)) = __float2bfloat16_rn(w);
+  }
+  if (tid == 0) mbar_init(bar, 1);
+  if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  fence_before();
+  __syncthreads();
+  fence_after();
+  c.tmem = *tmem_slot;
+  c.lane_off = (uint32_t)(warp * 32) << 16;
+  c.bdesc = smem_desc(smem_u32(sB), 128, 1024);
+}
+
+// Pack hi/lo BF16 halves of 64 values (already centred) into 2 x 32 columns.
+__device__ __forceinline__ void split_bf16(const float *s, uint32_t *hi, uint32_t *lo) {
+#pragma unroll
+  for (int e = 0; e < 32; ++e) {
+    const float v0 = s[2 * e], v1 = s[2 * e + 1];
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);  // .x (low half) = element 2e
+    const __nv_bfloat162 l = __floats2bfloat162_rn(v0 - __low2float(h), v1 - __high2float(h));
+    hi[e] = *reinterpret_cast<const uint32_t *>(&h);
+    lo[e] = *reinterpret_cast<const uint32_t *>(&l);
+  }
+}
+
+// A (this lane) -> TMEM, barrier, MMA by thread 0, bounded wait, D -> regs.
+// Returns false (CTA-uniformly) when the wait timed out.
+__device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t parity, const uint32_t *hi,
+                                         const uint32_t *lo, float *coef) {
+  tmem_st32(c.tmem + c.lane_off + 0, hi);
+  tmem_st32(c.tmem + c.lane_off + 32, lo);
+  tmem_wait_st();
+  fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    fence_after();
+    constexpr uint32_t idesc = instr_desc_bf16(kTile, kCoef);
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      const uint32_t a_tmem = c.tmem + (uint32_t)(kk * 8);               // 8 columns = 16 bf16 of K
+      const uint64_t bdesc = c.bdesc + (uint64_t)(((kk & 3) * 256) >> 4);  // K-step of B (2 core matrices)
+      mma_bf16(c.tmem + 64, a_tmem, bdesc, idesc, kk > 0 ? 1u : 0u);
+    }
+    mma_commit(bar);
+  }
+  const bool ok = mbar_wait(bar, parity);
+  const int all_ok = __syncthreads_and(ok ? 1 : 0);
+  if (!all_ok) return false;
+  fence_after();
+  uint32_t *u = reinterpret_cast<uint32_t *>(coef);
+  tmem_ld32(c.tmem + c.lane_off + 64, u);
+  tmem_ld32(c.tmem + c.lane_off + 96, u + 32);
+  tmem_wait_ld();
+  fence_before();
+  return true;
+}
+
+__device__ __forceinline__ float horner3(const float *a, const float f[3]) {
+  float pz = 0.f;
+#pragma unroll
+  for (int k = 3; k >= 0; --k) {
+    float py = 0.f;
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+      const float *r = a + 4 * j + 16 * k;
+      const float px = fmaf(fmaf(fmaf(r[3], f[0], r[2]), f[0], r[1]), f[0], r[0]);
+      py = fmaf(py, f[1], px);
+    }
+    pz = fmaf(pz, f[2], py);
+  }
+  return pz;
+}
+
+__global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__restrict__ phi0,
+                                                         const float *__restrict__ vel, float dt,
+                                                         const int *__restrict__ band, long long npts, int backtrace,
+                                                         float *__restrict__ phi, int *flags) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sB = smem;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kBBytes);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kBBytes + 8);
+  Ctx c;
+  setup(sB, bar, tmem_slot, c);
+
+  const float dth[3] = {dt / (float)g.hx, dt / (float)g.hy, dt / (float)g.hz};
+  const long long ntiles = (npts + kTile - 1) / kTile;
+  uint32_t parity = 0;
+  bool clamped = false, timeout = false;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long q = tile * kTile + threadIdx.x;
+    const bool valid = q < npts;
+    int x = 0, y = 0, z = 0, cc[3] = {0, 0, 0};
+    float f[3] = {0.f, 0.f, 0.f}, r = 0.f;
+    uint32_t hi[32], lo[32];
+    {
+      float s[64];
+      if (valid) {
+        arrival(g, band, q, x, y, z);
+        clamped |= departure_cell<float, 3>(g, vel, dth, backtrace, x, y, z, cc, f);
+#pragma unroll
+        for (int zz = 0; zz < 4; ++zz)
+#pragma unroll
+          for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int xx = 0; xx < 4; ++xx)
+              s[xx + 4 * yy + 16 * zz] = phi0[gidx(g, cc[0] - 1 + xx, cc[1] - 1 + yy, cc[2] - 1 + zz)];
+        r = s[21];
+#pragma unroll
+        for (int e = 0; e < 64; ++e) s[e] -= r;
+      } else {
+#pragma unroll
+        for (int e = 0; e < 64; ++e) s[e] = 0.f;
+      }
+      split_bf16(s, hi, lo);
+    }
+    float a[64];
+    if (!mma_tile(c, bar, parity, hi, lo, a)) {
+      timeout = true;
+      break;
+    }
+    parity ^= 1u;
+    if (valid) phi[gidx(g, x, y, z)] = horner3(a, f) + r;
+  }
+  if (clamped) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);
+  if (timeout && threadIdx.x == 0) raise_flag(flags, FLAG_WAIT_TIMEOUT);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if ((threadIdx.x >> 5) == 0) tmem_dealloc(c.tmem, kTmemCols);
+}
+
+// D = bf16(A) * M^T on the same tensor-core path (hi half only): a check of
+// the operand layouts against a host GEMM.  A: 128 x 64 row-major, D: 128 x 64.
+__global__ void __launch_bounds__(kTile, 1) tc_gemm_check_kernel(const float *__restrict__ A, float *__restrict__ D,
+                                                                 int *flags) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sB = smem;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kBBytes);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kBBytes + 8);
+  Ctx c;
+  setup(sB, bar, tmem_slot, c);
+  float s[64];
+  for (int e = 0; e < 64; ++e) s[e] = A[threadIdx.x * 64 + e];
+  uint32_t hi[32], lo[32];
+  split_bf16(s, hi, lo);
+  for (int e = 0; e < 32; ++e) lo[e] = 0u;  // hi only: D = bf16(A) M^T
+  float a[64];
+  if (mma_tile(c, bar, 0, hi, lo, a)) {
+    for (int e = 0; e < 64; ++e) D[threadIdx.x * 64 + e] = a[e];
+  } else if (threadIdx.x == 0) {
+    raise_flag(flags, FLAG_WAIT_TIMEOUT);
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if ((threadIdx.x >> 5) == 0) tmem_dealloc(c.tmem, kTmemCols);
+}
+
+}  // namespace tc
+}  // namespace dcell
+
+using namespace dcell;
+
+static int tc_grid(long long npts) {
+  static int num_sms = 0;
+  if (!num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (num_sms <= 0) num_sms = 148;
+  }
+  const long long ntiles = (npts + tc::kTile - 1) / tc::kTile;
+  long long grid = 4LL * num_sms;
+  if (grid > ntiles) grid = ntiles;
+  return (int)(grid < 1 ? 1 : grid);
+}
+
+int launch_sl_tc(const Geom &g, const float *phi0, const float *vel, double dt, const int *band, long long npts,
+                 int backtrace, float *phi, int *flags, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    DCELL_CUDA_CHECK(
+        cudaFuncSetAttribute(tc::sl_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kDynSmem));
+    DCELL_CUDA_CHECK(
+        cudaFuncSetAttribute(tc::tc_gemm_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kDynSmem));
+    configured = true;
+  }
+  if (npts <= 0) return DCELL_OK;
+  tc::sl_tc_kernel<<<tc_grid(npts), tc::kTile, tc::kDynSmem, st>>>(g, phi0, vel, (float)dt, band, npts, backtrace,
+                                                                   phi, flags);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_tc_gemm_check(const float *A, float *D, int *flags, cudaStream_t st) {
+  DCELL_CUDA_CHECK(
+      cudaFuncSetAttribute(tc::tc_gemm_check_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kDynSmem));
+  tc::tc_gemm_check_kernel<<<1, tc::kTile, tc::kDynSmem, st>>>(A, D, flags);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}

@@ -1,0 +1,258 @@
+"""Host-side mirror of the reference's LevelSet interface over the C ABI.
+
+Device memory comes from torch (CUDA tensors); every computation is a
+kernel of ``libdcell_ls.so`` launched on torch's current stream.  Names and
+argument meanings follow LevelSetMethod/LevelSetMethod.h:57-94:
+
+    LevelSetCreate(dh, pos, size)                  LevelSet.c:6-37
+    LevelSetAdvectSL(ls, velgrid, dt)              AdvectSL.c:6-19
+    LevelSetAdvectSLRK2HalfStep / FullStep         AdvectRK2.c:5-26
+    LevelSetUpdateIrregularNodeList(ls)            IrregularNodes.c:9-28
+    LevelSetCFLIncrement / LevelSet_MaxVelocity    Advect.c:54-111
+    LevelSetAdvectAndReinit(ls, velgrid, dt)       Advect.c:33-50
+
+Errors raise :class:`dcell_b200.DcellError` (the reference returns a
+PetscErrorCode).  Reinitialisation stays the reference's CPU fast marching:
+``LevelSetAdvectAndReinit`` calls ``ls.Reinitialize(ls)``, a hook the caller
+supplies, when the reference's thresholds trigger.
+
+Layout: phi tensors are (nz, ny, nx) or (ny, nx); velocity grids append the
+MAC components (3 or 2) innermost; bands are (nb, 3) int32 GLOBAL indices.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Callable, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import BACKTRACE, INTERP, NODE_DTYPE, DcellError, check, geom, lib
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dtype_code(t: torch.Tensor) -> int:
+    if t.dtype == torch.float32:
+        return _lib.F32
+    if t.dtype == torch.float64:
+        return _lib.F64
+    raise DcellError(_lib.ERR_ARG, f"unsupported dtype {t.dtype} (float32 or float64)")
+
+
+def _require_cuda(*ts):
+    for t in ts:
+        if t is None:
+            continue
+        if not t.is_cuda:
+            raise DcellError(_lib.ERR_ARG, "tensors must live on a CUDA device (no CPU fallback)")
+        if not t.is_contiguous():
+            raise DcellError(_lib.ERR_ARG, "tensors must be contiguous")
+
+
+def sl_step(phi0: torch.Tensor, vel: torch.Tensor, dt: float, h, origin=(0, 0, 0), band=None,
+            interp="linear", backtrace="euler", out: Optional[torch.Tensor] = None,
+            flags: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """One semi-Lagrangian step phi[X] = interp(phi0, S(X)) on the band (or everywhere).
+
+    ``out`` (default: a copy of phi0) is updated in place at the advected points."""
+    _require_cuda(phi0, vel, band, out, flags)
+    dof = 3 if phi0.dim() == 3 else 2
+    if tuple(vel.shape) != tuple(phi0.shape) + (dof,):
+        raise DcellError(_lib.ERR_ARG, f"velocity shape {tuple(vel.shape)} != {tuple(phi0.shape) + (dof,)}")
+    if vel.dtype != phi0.dtype:
+        raise DcellError(_lib.ERR_ARG, "phi0 and velocity dtypes differ")
+    if out is None:
+        out = phi0.clone()
+    if band is not None and (band.dtype != torch.int32 or band.dim() != 2 or band.shape[1] != 3):
+        raise DcellError(_lib.ERR_ARG, "band must be an (nb, 3) int32 tensor")
+    g = geom(phi0.shape, h, origin)
+    nb = int(band.shape[0]) if band is not None else 0
+    check(lib().dcell_sl_step(ctypes.byref(g), _dtype_code(phi0), _ptr(phi0), _ptr(vel), float(dt), _ptr(band), nb,
+                              INTERP[interp] if isinstance(interp, str) else int(interp),
+                              BACKTRACE[backtrace] if isinstance(backtrace, str) else int(backtrace),
+                              _ptr(out), _ptr(flags), _stream()))
+    return out
+
+
+def nodes_to_numpy(raw: torch.Tensor, count: int) -> np.ndarray:
+    """Device node buffer (uint8, 120 B/node) -> numpy structured array."""
+    n = int(count)
+    return np.frombuffer(raw[: n * NODE_DTYPE.itemsize].cpu().numpy().tobytes(), dtype=NODE_DTYPE)
+
+
+def nodes_to_rows(nodes: np.ndarray) -> np.ndarray:
+    """Structured nodes -> (n, 18) float64 rows: pos, axis, shift, signCenter,
+    signFace, d, X, op, n, k (the oracle's record layout)."""
+    r = np.zeros((len(nodes), 18))
+    r[:, 0:3] = nodes["pos"]
+    r[:, 3] = nodes["axis"]
+    r[:, 4] = nodes["shift"]
+    r[:, 5] = nodes["signCenter"]
+    r[:, 6] = nodes["signFace"]
+    r[:, 7] = nodes["d"]
+    r[:, 8:11] = nodes["X"]
+    r[:, 11:14] = nodes["op"]
+    r[:, 14:17] = nodes["n"]
+    r[:, 17] = nodes["k"]
+    return r
+
+
+def irregular_nodes(phi: torch.Tensor, h, band: torch.Tensor, origin=(0, 0, 0), with_surface=True,
+                    capacity: Optional[int] = None, flags: Optional[torch.Tensor] = None):
+    """Irregular-node pass; returns (raw uint8 node buffer, device int32 count tensor)."""
+    _require_cuda(phi, band, flags)
+    nb = int(band.shape[0])
+    cap = capacity if capacity is not None else max(16, (10 if phi.dim() == 3 else 5) * nb)
+    dev = phi.device
+    raw = torch.empty(max(cap, 1) * NODE_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    count = torch.zeros(1, dtype=torch.int32, device=dev)
+    sb = lib().dcell_irregular_nodes_scratch_bytes(nb)
+    scratch = torch.empty(max(int(sb), 16), dtype=torch.uint8, device=dev)
+    g = geom(phi.shape, h, origin)
+    check(lib().dcell_irregular_nodes(ctypes.byref(g), _dtype_code(phi), _ptr(phi), _ptr(band), nb,
+                                      1 if with_surface else 0, _ptr(raw), cap, _ptr(count), _ptr(scratch),
+                                      scratch.numel(), _ptr(flags), _stream()))
+    return raw, count
+
+
+def max_velocity(vel: torch.Tensor, h, raw_nodes: torch.Tensor, count: torch.Tensor, origin=(0, 0, 0)):
+    _require_cuda(vel, raw_nodes, count)
+    shape = tuple(vel.shape[:-1])
+    g = geom(shape, h, origin)
+    out = torch.zeros(1, dtype=torch.float64, device=vel.device)
+    cap = raw_nodes.numel() // NODE_DTYPE.itemsize
+    check(lib().dcell_max_velocity(ctypes.byref(g), _dtype_code(vel), _ptr(vel), _ptr(raw_nodes), _ptr(count), cap,
+                                   _ptr(out), _stream()))
+    return out
+
+
+def volume(phi: torch.Tensor, h, eps: float):
+    """Enclosed volume through the smoothed Heaviside (FP64, deterministic)."""
+    _require_cuda(phi)
+    g = geom(phi.shape, h)
+    out = torch.zeros(1, dtype=torch.float64, device=phi.device)
+    sb = int(lib().dcell_volume_scratch_bytes())
+    scratch = torch.empty(sb, dtype=torch.uint8, device=phi.device)
+    check(lib().dcell_volume(ctypes.byref(g), _dtype_code(phi), _ptr(phi), float(eps), _ptr(out), _ptr(scratch), sb,
+                             _stream()))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# LevelSet object and the reference-named entry points
+@dataclass
+class LevelSet:
+    """Mirror of struct _LevelSet (LevelSetMethod.h:10-26) with device grids."""
+    phi: torch.Tensor
+    phi0: torch.Tensor
+    h: tuple
+    origin: tuple
+    band: torch.Tensor
+    bandWidth: float = 6.0
+    PHI_INF: float = 7.5
+    CFLthres: float = 3.0
+    CFLcount: float = 0.0
+    AdvectThres: int = 1000
+    AdvectCount: int = 0
+    maxVel: float = 0.0
+    interp: str = "linear"
+    backtrace: str = "euler"
+    irregularNodes: Optional[torch.Tensor] = None
+    irregularCount: Optional[torch.Tensor] = None
+    Advect: Optional[Callable] = None
+    Reinitialize: Optional[Callable] = None
+    flags: Optional[torch.Tensor] = field(default=None)
+
+    @property
+    def is2D(self) -> bool:
+        return self.phi.dim() == 2
+
+
+def LevelSetCreate(dh, pos, size, dtype=torch.float32, device="cuda") -> LevelSet:
+    """LevelSetCreate (LevelSet.c:6-37): zeroed phi/phi0 on [pos, pos+size), bandwidth 6."""
+    nx, ny, nz = (int(v) for v in size)
+    shape = (ny, nx) if nz < 2 else (nz, ny, nx)
+    phi = torch.zeros(shape, dtype=dtype, device=device)
+    ls = LevelSet(phi=phi, phi0=phi.clone(), h=tuple(np.broadcast_to(np.asarray(dh, float), (3,))),
+                  origin=tuple(int(v) for v in pos), band=torch.zeros((0, 3), dtype=torch.int32, device=device))
+    LevelSetSetBandWidth(ls, 6.0)
+    ls.Advect = LevelSetAdvectAndReinit
+    ls.flags = torch.zeros(1, dtype=torch.int32, device=device)
+    return ls
+
+
+def LevelSetSetBandWidth(ls: LevelSet, bandwidth: float):
+    """LevelSetSetBandWidth (LevelSet.c:60-66): PHI_INF = bandWidth + 1.5."""
+    ls.bandWidth = float(bandwidth)
+    ls.PHI_INF = ls.bandWidth + 1.5
+
+
+def LevelSetAdvectSL(ls: LevelSet, velgrid: torch.Tensor, dt: float):
+    """phi[band] <- SL(phi0, velgrid, dt) (AdvectSL.c:6-89)."""
+    sl_step(ls.phi0, velgrid, dt, ls.h, ls.origin, band=ls.band, interp=ls.interp, backtrace=ls.backtrace,
+            out=ls.phi, flags=ls.flags)
+
+
+def LevelSetUpdateIrregularNodeList(ls: LevelSet, with_surface: bool = False):
+    raw, count = irregular_nodes(ls.phi, ls.h, ls.band, ls.origin, with_surface=with_surface, flags=ls.flags)
+    ls.irregularNodes, ls.irregularCount = raw, count
+
+
+def LevelSetAdvectSLRK2HalfStep(ls: LevelSet, velgrid: torch.Tensor, dt: float):
+    """AdvectRK2.c:5-14: phi0 <- phi; SL(dt); irregular nodes."""
+    ls.phi0.copy_(ls.phi)
+    LevelSetAdvectSL(ls, velgrid, dt)
+    LevelSetUpdateIrregularNodeList(ls)
+
+
+def LevelSetAdvectSLRK2FullStep(ls: LevelSet, velgrid: torch.Tensor, dt: float):
+    """AdvectRK2.c:18-26: SL(dt) from the same phi0; irregular nodes."""
+    LevelSetAdvectSL(ls, velgrid, dt)
+    LevelSetUpdateIrregularNodeList(ls)
+
+
+def LevelSet_MaxVelocity(ls: LevelSet, velgrid: torch.Tensor) -> float:
+    """Advect.c:70-111: max |V| over the irregular nodes' positions."""
+    if ls.irregularNodes is None:
+        ls.maxVel = 0.0
+        return 0.0
+    ls.maxVel = float(max_velocity(velgrid, ls.h, ls.irregularNodes, ls.irregularCount, ls.origin).item())
+    return ls.maxVel
+
+
+def LevelSetCFLIncrement(ls: LevelSet, velgrid: torch.Tensor, dt: float):
+    """Advect.c:54-66."""
+    LevelSet_MaxVelocity(ls, velgrid)
+    ls.CFLcount += dt * ls.maxVel / ls.h[0]
+    ls.AdvectCount += 1
+
+
+def LevelSetAdvectAndReinit(ls: LevelSet, velgrid: torch.Tensor, dt: float):
+    """Advect.c:33-50: copy, SL, CFL bookkeeping, irregular nodes, reinit trigger."""
+    ls.phi0.copy_(ls.phi)
+    LevelSetAdvectSL(ls, velgrid, dt)
+    LevelSetCFLIncrement(ls, velgrid, dt)
+    LevelSetUpdateIrregularNodeList(ls)
+    if ls.AdvectCount > ls.AdvectThres or ls.CFLcount > ls.CFLthres:
+        ls.CFLcount = 0.0
+        ls.AdvectCount = 0
+        if ls.Reinitialize is None:
+            raise DcellError(_lib.ERR_UNSUPPORTED, "reinitialisation threshold reached but no Reinitialize hook is "
+                             "set (fast marching stays the reference's CPU LevelSetReinitialize)")
+        ls.Reinitialize(ls)
+
+
+def status(ls: LevelSet) -> int:
+    """Read and clear the device status flags of ``ls`` (DCELL_FLAG_* bits)."""
+    v = int(ls.flags.item())
+    ls.flags.zero_()
+    return v

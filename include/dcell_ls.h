@@ -1,0 +1,190 @@
+/*
+ * dcell_ls.h -- C ABI of the B200 (sm_100a) level-set transport path.
+ *
+ * Drop-in boundary for adrielb/DCell's LevelSetMethod hot path.  Plain C
+ * types, plain pointers and sizes; no C++ or torch types.  All functions
+ * return a status (DCELL_OK == 0, like the reference's PetscErrorCode) and
+ * never exit; dcell_last_error() gives the message of the last failure on
+ * the calling thread.
+ *
+ * Two layers:
+ *  - device-resident entry points (dcell_sl_step, dcell_irregular_nodes, ...)
+ *    take DEVICE pointers and a cudaStream_t (passed as void*), enqueue work
+ *    and return without synchronising;
+ *  - host-buffer entry points (dcell_ls_*) take the reference's own FP64
+ *    host arrays (Grid.v1, Array data of LevelSet.band) through a session,
+ *    copy in, compute, copy out and synchronise -- what a LevelSet C host
+ *    calls from LevelSetAdvectSL & co.
+ *
+ * Grid convention (reference Common/Grid.c:69-93, Common/Grid.h:8-22): a grid
+ * covers global indices [p, p+n) per axis, x fastest; velocity grids keep dof
+ * (2 or 3) values innermost, u at x-face i-1/2, v at y-face j-1/2, w at z-face
+ * k-1/2 (Common/Common.h:26-30, Tensor1).  2D grids have n[2] <= 1.  The band
+ * is an array of iCoor {x, y, z} int triples in GLOBAL indices
+ * (LevelSetMethod.h:23, Common/Common.h:22-24).
+ */
+#ifndef DCELL_LS_H_
+#define DCELL_LS_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DCELL_LS_VERSION 1
+
+#if defined(__GNUC__)
+#define DCELL_API __attribute__((visibility("default")))
+#else
+#define DCELL_API
+#endif
+
+/* status codes (reference: PetscErrorCode, 0 = success) */
+enum {
+  DCELL_OK = 0,
+  DCELL_ERR_ARG = 1,          /* invalid argument (SETERRQ ... ARG_OUTOFRANGE in Array.c:92-95) */
+  DCELL_ERR_CUDA = 2,         /* CUDA runtime error */
+  DCELL_ERR_DEPARTURE = 3,    /* a departure point left the grid (sample clamped) */
+  DCELL_ERR_NONFINITE = 4,    /* non-finite input or result */
+  DCELL_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+  DCELL_ERR_CAPACITY = 6,     /* caller buffer too small */
+  DCELL_ERR_UNSUPPORTED = 7,  /* combination not implemented */
+  DCELL_ERR_NOMEM = 8         /* device allocation failed */
+};
+
+enum { DCELL_F32 = 0, DCELL_F64 = 1 };
+
+/* reconstruction at the departure point */
+enum {
+  DCELL_LINEAR = 0,          /* reference Bilinear2D/Bilinear3D (Grid.c:190, Grid3D.c:4) */
+  DCELL_CUBIC_PLAIN = 1,     /* Catmull-Rom, 64 (16) coefficients by the 1331 (121) non-zeros
+                                of TricubicInverse.h (OrthogonalProjection.c:48-63 in 2D) */
+  DCELL_CUBIC_SEPARABLE = 2, /* same interpolant as 3 (2) passes of 4-tap filters */
+  DCELL_CUBIC_TC = 3         /* same interpolant, coefficient solve as a split-BF16 tcgen05
+                                GEMM with FP32 accumulation (3D, FP32 only) */
+};
+
+/* departure-point backtrace */
+enum {
+  DCELL_EULER = 0,    /* S = X - V(X) dt/h, V at the arrival point (AdvectSL.c:44-47, :78-82) */
+  DCELL_MIDPOINT = 1  /* Xm = X - V(X) dt/(2h);  S = X - V(Xm) dt/h */
+};
+
+/* Grid geometry: the n / p / d fields of struct _Grid (Grid.h:8-22). */
+typedef struct dcell_geom {
+  int n[3];
+  int p[3];
+  double h[3];
+} dcell_geom;
+
+/* One irregular node: the fields of struct _IrregularNode
+ * (LevelSetMethod.h:29-54) that the transport path writes. */
+typedef struct dcell_irregular_node {
+  int pos[3];      /* node index (global) */
+  int axis;        /* 0/1/2 or -1 for an orthogonal-projection node */
+  int shift;       /* VelFace: CELL_CENTER 0, U_FACE 1, V_FACE 2, W_FACE 3; -1 for projection nodes */
+  int signCenter;
+  int signFace;
+  int pad;
+  double d;        /* crossing fraction along the axis */
+  double X[3];     /* index-space position of the interface point */
+  double op[3];    /* orthogonal projection relative to pos (projection nodes) */
+  double n[3];     /* unit normal at X (with_surface) */
+  double k;        /* curvature at X (with_surface) */
+} dcell_irregular_node;
+
+/* Text of the last error on this thread ("" if none). */
+DCELL_API const char *dcell_last_error(void);
+DCELL_API int dcell_version(void);
+
+/* ------------------------------------------------------------------------
+ * Device-resident entry points
+ * ---------------------------------------------------------------------- */
+
+/* One semi-Lagrangian step: for each band point X (or every grid point when
+ * band == NULL), phi[X] = interp(phi0, S(X)).
+ * Replaces LevelSetAdvectSL / _2D / _3D (LevelSetMethod/AdvectSL.c:6-89).
+ * phi0, phi: dtype grids of n[0]*n[1]*n[2] values; vel: dtype, dof innermost;
+ * band: int32 [nband][3] or NULL; dt is the step the velocity is multiplied
+ * by (fold any scalar time factor of the field into it).  phi is written at
+ * the updated points only.  flags (optional int on the device) receives
+ * DCELL_FLAG_* bits.  DCELL_CUBIC_TC requires dtype F32 and a 3D grid. */
+#define DCELL_FLAG_DEPARTURE_CLAMPED 1
+#define DCELL_FLAG_NONFINITE 2
+#define DCELL_FLAG_CAPACITY 4
+#define DCELL_FLAG_WAIT_TIMEOUT 8
+DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
+                  int nband, int interp, int backtrace, void *phi, int *flags, void *stream);
+
+/* Irregular-node pass over the band: replaces LevelSetUpdateIrregularNodeList
+ * (LevelSetMethod/IrregularNodes.c:9-141, IrregularNodes3D.c:6-117) including
+ * OrthogonalProjection2D/3D (OrthogonalProjection*.c).  Nodes are written in
+ * the reference's order (band order; per point: projection node, cell-face
+ * nodes, velocity-face nodes).  With with_surface != 0 also fills n and k as
+ * IIMUpdateSurfaceQuantities_2D/3D does (IIM/SurfaceQuantities.c:48-56,
+ * :83-89, :111).  *count (device int) receives the total node count even if
+ * it exceeds capacity (then DCELL_FLAG_CAPACITY is raised).  scratch is a
+ * device buffer of at least dcell_irregular_nodes_scratch_bytes(nband). */
+DCELL_API size_t dcell_irregular_nodes_scratch_bytes(int nband);
+DCELL_API int dcell_irregular_nodes(const dcell_geom *g, int dtype, const void *phi, const int *band, int nband,
+                          int with_surface, dcell_irregular_node *nodes, int capacity, int *count, void *scratch,
+                          size_t scratch_bytes, int *flags, void *stream);
+
+/* max |V| over the integer positions of the irregular nodes
+ * (LevelSet_MaxVelocity, LevelSetMethod/Advect.c:70-111).  count and maxvel
+ * are device pointers; *maxvel is overwritten. */
+DCELL_API int dcell_max_velocity(const dcell_geom *g, int dtype, const void *vel, const dcell_irregular_node *nodes,
+                       const int *count, int capacity, double *maxvel, void *stream);
+
+/* Enclosed volume (2D: area) sum (1 - H_eps(phi)) * cell volume with the
+ * smoothed Heaviside whose derivative is the reference's smoothed delta
+ * (LevelSetDiracDelta2D/3D, NormalDirection.c:36-57); FP64 accumulation,
+ * deterministic.  *volume is a device double.  scratch: at least
+ * dcell_volume_scratch_bytes() bytes. */
+DCELL_API size_t dcell_volume_scratch_bytes(void);
+DCELL_API int dcell_volume(const dcell_geom *g, int dtype, const void *phi, double eps, double *volume, void *scratch,
+                 size_t scratch_bytes, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Host-buffer drop-in entry points (reference FP64 layout)
+ * ---------------------------------------------------------------------- */
+typedef struct dcell_session dcell_session;
+
+/* A session owns device mirrors (grow-only) and a stream on one device. */
+DCELL_API int dcell_session_create(int device, dcell_session **out);
+DCELL_API int dcell_session_destroy(dcell_session *s);
+
+/* LevelSetAdvectSL(ls, velgrid, dt) with ls->phi0->v1 = phi0, velgrid->v1 =
+ * vel, ls->band = band and ls->phi->v1 = phi (updated in place at the band
+ * points, or everywhere when band == NULL).  precision: DCELL_F64 computes in
+ * FP64 (the reference's arithmetic, bit-identical for DCELL_LINEAR +
+ * DCELL_EULER), DCELL_F32 in FP32.  Returns DCELL_ERR_DEPARTURE (after
+ * writing the clamped result) if a departure point left the grid. */
+DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const double *phi0, const double *vel, const int *band,
+                       int nband, double dt, int interp, int backtrace, int precision, double *phi);
+
+/* LevelSetUpdateIrregularNodeList(ls) on host phi; *count = node count. */
+DCELL_API int dcell_ls_update_irregular_nodes(dcell_session *s, const dcell_geom *g, const double *phi, const int *band,
+                                    int nband, int with_surface, int precision, dcell_irregular_node *nodes,
+                                    int capacity, int *count);
+
+/* LevelSet_MaxVelocity(ls, velgrid) on host arrays. */
+DCELL_API int dcell_ls_max_velocity(dcell_session *s, const dcell_geom *g, const double *vel,
+                          const dcell_irregular_node *nodes, int count, double *maxvel);
+
+/* ------------------------------------------------------------------------
+ * Diagnostics
+ * ---------------------------------------------------------------------- */
+
+/* D = bf16(A) * M^T on the tensor-core path of DCELL_CUBIC_TC, where M is
+ * the 64x64 Catmull-Rom operator of TricubicInverse.h; A (128 x 64) and D
+ * (128 x 64) are row-major FP32 device arrays.  Checks the MMA operand
+ * layouts on the running GPU against a host product. */
+DCELL_API int dcell_tc_gemm_check(const float *a, float *d, int *flags, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DCELL_LS_H_ */

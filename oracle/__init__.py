@@ -1,0 +1,199 @@
+"""CPU oracle for the level-set transport path -- TEST INFRASTRUCTURE ONLY.
+
+Two libraries sit behind this module:
+
+* ``liboracle.so`` -- our FP64 C restatement of the reference's hot path
+  (``oracle/sl_oracle.c``; every function cites the reference file:line it
+  follows).
+* ``_ref/libdcell_ref.so`` -- the reference's OWN C sources compiled against
+  ``oracle/shim`` (see ``oracle/Makefile``); present only where the reference
+  tree was available at build time.  ``oracle.reference`` wraps it.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may use this package, and only as the checker / the timed CPU baseline.
+The product path (``dcell_b200``) never imports it.
+
+Array conventions: phi is (nz, ny, nx) or (ny, nx) float64, x fastest;
+velocity is (nz, ny, nx, 3) or (ny, nx, 2) with the MAC components innermost
+(u at x-face i-1/2, v at y-face j-1/2, w at z-face k-1/2); band is an
+(nb, 3) int32 array of GLOBAL (x, y, z) indices; ``origin`` is the global
+index of element 0 (the reference Grid's ``p``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+NODE_FIELDS = ("px", "py", "pz", "axis", "shift", "signCenter", "signFace", "d",
+               "Xx", "Xy", "Xz", "opx", "opy", "opz", "nx", "ny", "nz", "k")
+NODE_W = len(NODE_FIELDS)
+
+
+class Geom(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("px", ctypes.c_int), ("py", ctypes.c_int), ("pz", ctypes.c_int),
+                ("hx", ctypes.c_double), ("hy", ctypes.c_double), ("hz", ctypes.c_double)]
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def lib():
+    """Load liboracle.so, compiling it with gcc first if it is missing."""
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        src = os.path.join(HERE, "sl_oracle.c")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+        L = ctypes.CDLL(path)
+        vp, i, d, l = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long
+        L.orc_sl_step.argtypes = [vp, vp, vp, d, vp, i, i, i, vp]
+        L.orc_sl_step.restype = i
+        L.orc_interp_velocity.argtypes = [vp, vp, vp, i, vp]
+        L.orc_tricubic_coefs.argtypes = [vp, vp]
+        L.orc_bicubic_coefs.argtypes = [vp, vp]
+        L.orc_sample.argtypes = [vp, vp, i, d, d, d]
+        L.orc_sample.restype = d
+        L.orc_ortho2d.argtypes = [vp, vp, vp]
+        L.orc_ortho3d.argtypes = [vp, vp, vp]
+        L.orc_irregular_nodes.argtypes = [vp, vp, vp, i, vp, l]
+        L.orc_irregular_nodes.restype = l
+        L.orc_node_surface.argtypes = [vp, vp, vp, l]
+        L.orc_max_velocity.argtypes = [vp, vp, vp, l]
+        L.orc_max_velocity.restype = d
+        L.orc_volume.argtypes = [vp, vp, d]
+        L.orc_volume.restype = d
+        _LIB = L
+    return _LIB
+
+
+def geom(shape, h, origin=(0, 0, 0)):
+    """Geom from a phi shape ((nz,ny,nx) or (ny,nx)), spacing and origin."""
+    if len(shape) == 2:
+        ny, nx = shape
+        nz = 1
+    else:
+        nz, ny, nx = shape
+    h = np.broadcast_to(np.asarray(h, dtype=np.float64), (3,))
+    o = tuple(origin) + (0,) * (3 - len(origin))
+    return Geom(int(nx), int(ny), int(nz), int(o[0]), int(o[1]), int(0 if nz == 1 else o[2]),
+                float(h[0]), float(h[1]), float(h[2]))
+
+
+def _band(band):
+    if band is None:
+        return None, 0
+    b = np.ascontiguousarray(band, dtype=np.int32).reshape(-1, 3)
+    return b, b.shape[0]
+
+
+def sl_step(phi0, vel, dt, h, origin=(0, 0, 0), band=None, interp="linear", backtrace="euler", phi=None):
+    """One semi-Lagrangian step (AdvectSL.c:23-89 for linear/euler)."""
+    phi0 = np.ascontiguousarray(phi0, dtype=np.float64)
+    vel = np.ascontiguousarray(vel, dtype=np.float64)
+    out = phi0.copy() if phi is None else np.ascontiguousarray(phi, dtype=np.float64).copy()
+    g = geom(phi0.shape, h, origin)
+    b, nb = _band(band)
+    rc = lib().orc_sl_step(ctypes.byref(g), _ptr(phi0), _ptr(vel), float(dt), _ptr(b), nb,
+                           {"linear": 0, "cubic": 1}[interp], {"euler": 0, "midpoint": 1}[backtrace],
+                           _ptr(out))
+    assert rc == 0
+    return out
+
+
+def interp_velocity(vel, X, h=1.0, origin=(0, 0, 0)):
+    vel = np.ascontiguousarray(vel, dtype=np.float64)
+    shape = vel.shape[:-1]
+    X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 3)
+    V = np.zeros_like(X)
+    g = geom(shape, h, origin)
+    lib().orc_interp_velocity(ctypes.byref(g), _ptr(vel), _ptr(X), X.shape[0], _ptr(V))
+    return V
+
+
+def tricubic_coefs(stencil64):
+    s = np.ascontiguousarray(stencil64, dtype=np.float64).reshape(64)
+    a = np.zeros(64)
+    lib().orc_tricubic_coefs(_ptr(s), _ptr(a))
+    return a
+
+
+def bicubic_coefs(stencil16):
+    s = np.ascontiguousarray(stencil16, dtype=np.float64).reshape(16)
+    a = np.zeros(16)
+    lib().orc_bicubic_coefs(_ptr(s), _ptr(a))
+    return a
+
+
+def catmull_rom_operator(dim=3):
+    """Dense (4^dim x 4^dim) matrix M with a = M @ stencil (a[px+4py+16pz])."""
+    n = 4 ** dim
+    M = np.zeros((n, n))
+    f = tricubic_coefs if dim == 3 else bicubic_coefs
+    for s in range(n):
+        e = np.zeros(n)
+        e[s] = 1.0
+        M[:, s] = f(e)
+    return M
+
+
+def sample(phi, fn, X, h, origin=(0, 0, 0)):
+    """Bilinear/trilinear sample of a grid function at index-space points X.
+    fn: 0 identity, 1-3 d/dx,d/dy,d/dz, 4 curvature, 5 smoothed delta."""
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    g = geom(phi.shape, h, origin)
+    X = np.asarray(X, dtype=np.float64).reshape(-1, 3)
+    return np.array([lib().orc_sample(ctypes.byref(g), _ptr(phi), int(fn), *map(float, x)) for x in X])
+
+
+def ortho3d(phi3, phi5):
+    a3 = np.ascontiguousarray(phi3, dtype=np.float64).reshape(27)
+    a5 = np.ascontiguousarray(phi5, dtype=np.float64).reshape(125)
+    op = np.zeros(3)
+    lib().orc_ortho3d(_ptr(a3), _ptr(a5), _ptr(op))
+    return op
+
+
+def ortho2d(phi3, phi5):
+    a3 = np.ascontiguousarray(phi3, dtype=np.float64).reshape(9)
+    a5 = np.ascontiguousarray(phi5, dtype=np.float64).reshape(25)
+    op = np.zeros(3)
+    lib().orc_ortho2d(_ptr(a3), _ptr(a5), _ptr(op))
+    return op
+
+
+def irregular_nodes(phi, h, band, origin=(0, 0, 0), surface=True):
+    """Irregular-node list (IrregularNodes.c:32-141 / IrregularNodes3D.c:6-117),
+    optionally with normals and curvature; (n, 18) float64, NODE_FIELDS order."""
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    g = geom(phi.shape, h, origin)
+    b, nb = _band(band)
+    cap = max(16, 13 * nb)
+    out = np.zeros((cap, NODE_W))
+    n = lib().orc_irregular_nodes(ctypes.byref(g), _ptr(phi), _ptr(b), nb, _ptr(out), cap)
+    assert n <= cap
+    out = np.ascontiguousarray(out[:n])
+    if surface and n:
+        lib().orc_node_surface(ctypes.byref(g), _ptr(phi), _ptr(out), n)
+    return out
+
+
+def max_velocity(vel, nodes, h=1.0, origin=(0, 0, 0)):
+    vel = np.ascontiguousarray(vel, dtype=np.float64)
+    g = geom(vel.shape[:-1], h, origin)
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    return lib().orc_max_velocity(ctypes.byref(g), _ptr(vel), _ptr(nodes), nodes.shape[0])
+
+
+def volume(phi, h, eps):
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    g = geom(phi.shape, h)
+    return lib().orc_volume(ctypes.byref(g), _ptr(phi), float(eps))

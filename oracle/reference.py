@@ -1,0 +1,225 @@
+"""ctypes wrapper over the reference's own level-set C (oracle/_ref) --
+TEST INFRASTRUCTURE ONLY.
+
+``_ref/libdcell_ref.so`` is the reference's unmodified hot-path sources plus
+``oracle/ref_driver.c``, compiled by ``make -C oracle ref`` where the
+reference tree is present.  ``available()`` says whether it was built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import NODE_W
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PATH = os.path.join(HERE, "_ref", "libdcell_ref.so")
+_L = None
+
+
+def available() -> bool:
+    return os.path.exists(PATH)
+
+
+def lib():
+    global _L
+    if _L is None:
+        L = ctypes.CDLL(PATH)
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.dref_ls_create.restype = vp
+        L.dref_ls_create.argtypes = [d, d, d, i, i, i, i, i, i]
+        L.dref_ls_destroy.argtypes = [vp]
+        L.dref_ls_geometry.argtypes = [vp, vp, vp]
+        L.dref_ls_set_phi.argtypes = [vp, vp, i]
+        L.dref_ls_get_phi.argtypes = [vp, vp, i]
+        L.dref_ls_set_band.argtypes = [vp, vp, i]
+        L.dref_ls_band_length.argtypes = [vp]
+        L.dref_ls_get_band.argtypes = [vp, vp]
+        L.dref_ls_param.argtypes = [vp, i]
+        L.dref_ls_param.restype = d
+        L.dref_vel_create.restype = vp
+        L.dref_vel_create.argtypes = [vp, vp]
+        L.dref_vel_destroy.argtypes = [vp]
+        for f in ("dref_advect_sl", "dref_rk2_half", "dref_rk2_full", "dref_advect_and_reinit",
+                  "dref_cfl_increment"):
+            getattr(L, f).argtypes = [vp, vp, d]
+        L.dref_copy_phi_to_phi0.argtypes = [vp]
+        L.dref_max_velocity.argtypes = [vp, vp]
+        L.dref_max_velocity.restype = d
+        L.dref_update_irregular.argtypes = [vp]
+        L.dref_reinitialize.argtypes = [vp]
+        L.dref_get_irregular.argtypes = [vp, vp, i]
+        L.dref_init_sphere.restype = vp
+        L.dref_init_sphere.argtypes = [d, d, d, d, d]
+        L.dref_init_circle.restype = vp
+        L.dref_init_circle.argtypes = [d, d, d, d]
+        L.dref_sample.argtypes = [vp, i, d, d, d]
+        L.dref_sample.restype = d
+        L.dref_interp_velocity.argtypes = [vp, d, d, d, vp]
+        L.dref_ortho3d.argtypes = [vp, vp, vp]
+        L.dref_ortho2d.argtypes = [vp, vp, vp]
+        L.dref_tricubic_coefs.argtypes = [vp, vp]
+        _L = L
+    return _L
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class RefLevelSet:
+    """A reference ``LevelSet`` (LevelSetMethod.h:10-26) driven from numpy."""
+
+    def __init__(self, handle):
+        self.h = handle
+        self._vel = None
+
+    @classmethod
+    def create(cls, h, origin, shape):
+        """LevelSetCreate (LevelSet.c:6-37); shape (nz,ny,nx) or (ny,nx)."""
+        if len(shape) == 2:
+            ny, nx = shape
+            nz = 0
+        else:
+            nz, ny, nx = shape
+        o = tuple(origin) + (0,) * (3 - len(origin))
+        hh = np.broadcast_to(np.asarray(h, dtype=np.float64), (3,))
+        return cls(lib().dref_ls_create(*map(float, hh), *map(int, o), int(nx), int(ny), int(nz)))
+
+    @classmethod
+    def sphere(cls, h, center, r):
+        return cls(lib().dref_init_sphere(float(h), *map(float, center), float(r)))
+
+    @classmethod
+    def circle(cls, h, center, r):
+        return cls(lib().dref_init_circle(float(h), *map(float, center), float(r)))
+
+    def close(self):
+        if self._vel:
+            lib().dref_vel_destroy(self._vel)
+            self._vel = None
+        if self.h:
+            lib().dref_ls_destroy(self.h)
+            self.h = None
+
+    def geometry(self):
+        p = (ctypes.c_int * 3)()
+        n = (ctypes.c_int * 3)()
+        lib().dref_ls_geometry(self.h, p, n)
+        return tuple(p), tuple(n)
+
+    @property
+    def shape(self):
+        _, n = self.geometry()
+        return (n[1], n[0]) if n[2] < 2 else (n[2], n[1], n[0])
+
+    @property
+    def origin(self):
+        return self.geometry()[0]
+
+    def get_phi(self, which=0):
+        out = np.zeros(self.shape)
+        lib().dref_ls_get_phi(self.h, _p(out), which)
+        return out
+
+    def set_phi(self, phi, which=0):
+        a = np.ascontiguousarray(phi, dtype=np.float64)
+        assert a.shape == self.shape
+        assert lib().dref_ls_set_phi(self.h, _p(a), which) == 0
+
+    def band(self):
+        nb = lib().dref_ls_band_length(self.h)
+        out = np.zeros((nb, 3), dtype=np.int32)
+        lib().dref_ls_get_band(self.h, _p(out))
+        return out
+
+    def set_band(self, band):
+        b = np.ascontiguousarray(band, dtype=np.int32).reshape(-1, 3)
+        assert lib().dref_ls_set_band(self.h, _p(b), b.shape[0]) == 0
+
+    def set_velocity(self, vel):
+        if self._vel:
+            lib().dref_vel_destroy(self._vel)
+        v = np.ascontiguousarray(vel, dtype=np.float64)
+        self._vel = lib().dref_vel_create(self.h, _p(v))
+
+    def param(self, which):
+        return lib().dref_ls_param(self.h, {"bandWidth": 0, "PHI_INF": 1, "CFLcount": 2,
+                                            "AdvectCount": 3, "maxVel": 4}[which])
+
+    def copy_phi_to_phi0(self):
+        assert lib().dref_copy_phi_to_phi0(self.h) == 0
+
+    def advect_sl(self, dt):
+        """LevelSetAdvectSL (AdvectSL.c:6): phi[band] <- SL(phi0, vel, dt)."""
+        assert lib().dref_advect_sl(self.h, self._vel, float(dt)) == 0
+
+    def rk2_half(self, dt):
+        assert lib().dref_rk2_half(self.h, self._vel, float(dt)) == 0
+
+    def rk2_full(self, dt):
+        assert lib().dref_rk2_full(self.h, self._vel, float(dt)) == 0
+
+    def advect_and_reinit(self, dt):
+        assert lib().dref_advect_and_reinit(self.h, self._vel, float(dt)) == 0
+
+    def cfl_increment(self, dt):
+        assert lib().dref_cfl_increment(self.h, self._vel, float(dt)) == 0
+
+    def max_velocity(self):
+        return lib().dref_max_velocity(self.h, self._vel)
+
+    def update_irregular(self):
+        n = lib().dref_update_irregular(self.h)
+        assert n >= 0
+        return n
+
+    def irregular_nodes(self, surface=True):
+        n = lib().dref_update_irregular(self.h)
+        out = np.zeros((max(n, 1), NODE_W))
+        lib().dref_get_irregular(self.h, _p(out), 1 if surface else 0)
+        return out[:n]
+
+    def nodes_no_update(self, n, surface=True):
+        out = np.zeros((max(n, 1), NODE_W))
+        lib().dref_get_irregular(self.h, _p(out), 1 if surface else 0)
+        return out[:n]
+
+    def reinitialize(self):
+        assert lib().dref_reinitialize(self.h) == 0
+
+    def sample(self, fn, X):
+        return np.array([lib().dref_sample(self.h, int(fn), *map(float, x)) for x in np.reshape(X, (-1, 3))])
+
+    def interp_velocity(self, X):
+        out = np.zeros(3)
+        res = []
+        for x in np.reshape(X, (-1, 3)):
+            lib().dref_interp_velocity(self._vel, *map(float, x), _p(out))
+            res.append(out.copy())
+        return np.array(res)
+
+
+def tricubic_coefs(stencil64):
+    s = np.ascontiguousarray(stencil64, dtype=np.float64).reshape(64)
+    a = np.zeros(64)
+    lib().dref_tricubic_coefs(_p(s), _p(a))
+    return a
+
+
+def ortho3d(phi3, phi5):
+    a3 = np.ascontiguousarray(phi3, dtype=np.float64).reshape(27)
+    a5 = np.ascontiguousarray(phi5, dtype=np.float64).reshape(125)
+    op = np.zeros(3)
+    lib().dref_ortho3d(_p(a3), _p(a5), _p(op))
+    return op
+
+
+def ortho2d(phi3, phi5):
+    a3 = np.ascontiguousarray(phi3, dtype=np.float64).reshape(9)
+    a5 = np.ascontiguousarray(phi5, dtype=np.float64).reshape(25)
+    op = np.zeros(3)
+    lib().dref_ortho2d(_p(a3), _p(a5), _p(op))
+    return op

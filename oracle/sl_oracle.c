@@ -1,0 +1,741 @@
+/*
+ * FP64 CPU restatement of the level-set transport path -- the ORACLE.
+ *
+ * Test infrastructure only: tests/, the smoke check and the bench's CPU
+ * baseline call it to check or time the CUDA path; the product never does.
+ *
+ * Every function names the reference code it restates (paths relative to the
+ * reference tree).  The linear paths keep the reference's exact floating
+ * point operation order (compiled with -ffp-contract=off) so they reproduce
+ * the reference bit for bit; tests pin that against the reference compiled
+ * from its own sources (oracle/_ref) and against tests/golden fixtures.
+ *
+ * Grid convention (Common/Grid.c:69-93): a grid covers global indices
+ * [p, p+n) per axis, x fastest; a velocity grid has dof values innermost.
+ * 2D grids have nz == 1 and pz == 0.  Index gathers are clamped to the grid
+ * (the reference reads out of bounds instead; it never does so for band
+ * points that sit >= bandWidth+1 cells inside the grid, Resize.c:13-43).
+ */
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_EXPORT __attribute__((visibility("default")))
+
+typedef struct {
+  int nx, ny, nz;    /* extents (nz == 1 in 2D) */
+  int px, py, pz;    /* global index of element 0 */
+  double hx, hy, hz; /* spacing */
+} orc_geom;
+
+static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+static inline size_t gidx(const orc_geom *g, int i, int j, int k) {
+  i = clampi(i, g->px, g->px + g->nx - 1);
+  j = clampi(j, g->py, g->py + g->ny - 1);
+  k = clampi(k, g->pz, g->pz + g->nz - 1);
+  return ((size_t)(k - g->pz) * g->ny + (size_t)(j - g->py)) * g->nx + (size_t)(i - g->px);
+}
+
+/* Staggering of the MAC components: Common/Common.h:26-30 (Tensor1). */
+static const double kStag[3][3] = {{0.5, 0, 0}, {0, 0.5, 0}, {0, 0, 0.5}};
+
+/* InterpolateVelocity3D, Common/InterpolateVelocity.c:35-67 (same order). */
+static void interp_vel3d(const orc_geom *g, const double *vel, const double X[3], double V[3]) {
+  for (int d = 0; d < 3; ++d) {
+    int xs = (int)floor(X[0] + kStag[d][0]);
+    int ys = (int)floor(X[1] + kStag[d][1]);
+    int zs = (int)floor(X[2] + kStag[d][2]);
+    double sx = X[0] - xs + kStag[d][0];
+    double sy = X[1] - ys + kStag[d][1];
+    double sz = X[2] - zs + kStag[d][2];
+    double sum = 0;
+    for (int k = 0; k < 2; ++k)
+      for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i)
+          sum += ((1 - sx) * (1 - i) + i * sx) * ((1 - sy) * (1 - j) + j * sy) * ((1 - sz) * (1 - k) + k * sz) *
+                 vel[gidx(g, xs + i, ys + j, zs + k) * 3 + d];
+    V[d] = sum;
+  }
+}
+
+/* InterpolateVelocity2D, Common/InterpolateVelocity.c:7-33. */
+static void interp_vel2d(const orc_geom *g, const double *vel, const double X[2], double V[2]) {
+  for (int d = 0; d < 2; ++d) {
+    int xs = (int)floor(X[0] + kStag[d][0]);
+    int ys = (int)floor(X[1] + kStag[d][1]);
+    double sx = X[0] - xs + kStag[d][0];
+    double sy = X[1] - ys + kStag[d][1];
+    double sum = 0;
+    for (int j = 0; j < 2; ++j)
+      for (int i = 0; i < 2; ++i)
+        sum += ((1 - sx) * (1 - i) + i * sx) * ((1 - sy) * (1 - j) + j * sy) * vel[gidx(g, xs + i, ys + j, 0) * 2 + d];
+    V[d] = sum;
+  }
+}
+
+/* Bilinear3D with GridFunction3D_Identity, Common/Grid3D.c:4-36
+ * (loop order i, j, k with k innermost; weights i*s + (1-i)*(1-s)). */
+static double trilinear_ref(const orc_geom *g, const double *f, const double S[3]) {
+  int xs = (int)floor(S[0]), ys = (int)floor(S[1]), zs = (int)floor(S[2]);
+  double sx = S[0] - xs, sy = S[1] - ys, sz = S[2] - zs, sum = 0.0;
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j)
+      for (int k = 0; k < 2; ++k) {
+        double xb = i * sx + (1 - i) * (1 - sx);
+        double yb = j * sy + (1 - j) * (1 - sy);
+        double zb = k * sz + (1 - k) * (1 - sz);
+        sum += f[gidx(g, xs + i, ys + j, zs + k)] * xb * yb * zb;
+      }
+  return sum;
+}
+
+/* Bilinear2D with GridFunction2D_Identity, Common/Grid.c:190-217
+ * (weights (1 + (2k-1)(2(x-xi)-1)) / 4, x outer loop). */
+static double bilinear_ref(const orc_geom *g, const double *f, double x, double y) {
+  int xi = (int)floor(x), yi = (int)floor(y);
+  double xf = (2. * (x - xi) - 1.), yf = (2. * (y - yi) - 1.), sum = 0.;
+  for (int k = 0; k < 2; ++k)
+    for (int l = 0; l < 2; ++l) {
+      double xb = 1. + (2. * k - 1.) * xf;
+      double yb = 1. + (2. * l - 1.) * yf;
+      sum += f[gidx(g, xi + k, yi + l, 0)] * xb * yb;
+    }
+  sum /= 4.;
+  return sum;
+}
+
+/* ---- Catmull-Rom (Keys a = -1/2) cubic: the operator of the reference's
+ * TricubicInverse.h / OrthogonalProjection.c:48-63, which equals the tensor
+ * product C (x) C (x) C of this 4x4 matrix (rows: power 0..3, columns:
+ * stencil offsets -1..2).  Pinned against the compiled reference header. */
+static const double kCR[4][4] = {
+    {0, 1, 0, 0}, {-0.5, 0, 0.5, 0}, {1, -2.5, 2, -0.5}, {-0.5, 1.5, -1.5, 0.5}};
+
+/* a[px + 4py + 16pz] = sum C[pz][sz] C[py][sy] C[px][sx] s[sx + 4sy + 16sz] */
+ORC_EXPORT void orc_tricubic_coefs(const double *s, double *a) {
+  for (int pz = 0; pz < 4; ++pz)
+    for (int py = 0; py < 4; ++py)
+      for (int px = 0; px < 4; ++px) {
+        double acc = 0.0;
+        for (int sz = 0; sz < 4; ++sz)
+          for (int sy = 0; sy < 4; ++sy)
+            for (int sx = 0; sx < 4; ++sx) {
+              double w = kCR[pz][sz] * kCR[py][sy] * kCR[px][sx];
+              if (w != 0.0) acc += w * s[sx + 4 * sy + 16 * sz];
+            }
+        a[px + 4 * py + 16 * pz] = acc;
+      }
+}
+
+ORC_EXPORT void orc_bicubic_coefs(const double *s, double *a) {
+  for (int py = 0; py < 4; ++py)
+    for (int px = 0; px < 4; ++px) {
+      double acc = 0.0;
+      for (int sy = 0; sy < 4; ++sy)
+        for (int sx = 0; sx < 4; ++sx) {
+          double w = kCR[py][sy] * kCR[px][sx];
+          if (w != 0.0) acc += w * s[sx + 4 * sy];
+        }
+      a[px + 4 * py] = acc;
+    }
+}
+
+/* p, dp/dx, dp/dy, dp/dz of sum a[i+4j+16k] x^i y^j z^k (TricubicInterpolation.h:1-4). */
+static void tricubic_eval(const double *a, double x, double y, double z, double *p, double *gx, double *gy,
+                          double *gz) {
+  double X[4] = {1, x, x * x, x * x * x}, Y[4] = {1, y, y * y, y * y * y}, Z[4] = {1, z, z * z, z * z * z};
+  double dX[4] = {0, 1, 2 * x, 3 * x * x}, dY[4] = {0, 1, 2 * y, 3 * y * y}, dZ[4] = {0, 1, 2 * z, 3 * z * z};
+  double v = 0, vx = 0, vy = 0, vz = 0;
+  for (int k = 0; k < 4; ++k)
+    for (int j = 0; j < 4; ++j)
+      for (int i = 0; i < 4; ++i) {
+        double c = a[i + 4 * j + 16 * k];
+        v += c * X[i] * Y[j] * Z[k];
+        vx += c * dX[i] * Y[j] * Z[k];
+        vy += c * X[i] * dY[j] * Z[k];
+        vz += c * X[i] * Y[j] * dZ[k];
+      }
+  *p = v;
+  if (gx) *gx = vx;
+  if (gy) *gy = vy;
+  if (gz) *gz = vz;
+}
+
+static void bicubic_eval(const double *a, double x, double y, double *p, double *gx, double *gy) {
+  double X[4] = {1, x, x * x, x * x * x}, Y[4] = {1, y, y * y, y * y * y};
+  double dX[4] = {0, 1, 2 * x, 3 * x * x}, dY[4] = {0, 1, 2 * y, 3 * y * y};
+  double v = 0, vx = 0, vy = 0;
+  for (int j = 0; j < 4; ++j)
+    for (int i = 0; i < 4; ++i) {
+      double c = a[i + 4 * j];
+      v += c * X[i] * Y[j];
+      vx += c * dX[i] * Y[j];
+      vy += c * X[i] * dY[j];
+    }
+  *p = v;
+  if (gx) *gx = vx;
+  if (gy) *gy = vy;
+}
+
+/* Tricubic sample of f at index-space point S: 4^3 stencil around floor(S),
+ * 64 coefficients, polynomial at the fractional offset. */
+static double tricubic_sample(const orc_geom *g, const double *f, const double S[3]) {
+  int c[3];
+  double fr[3], s[64], a[64], p;
+  for (int d = 0; d < 3; ++d) {
+    c[d] = (int)floor(S[d]);
+    fr[d] = S[d] - c[d];
+  }
+  for (int z = 0; z < 4; ++z)
+    for (int y = 0; y < 4; ++y)
+      for (int x = 0; x < 4; ++x) s[x + 4 * y + 16 * z] = f[gidx(g, c[0] - 1 + x, c[1] - 1 + y, c[2] - 1 + z)];
+  orc_tricubic_coefs(s, a);
+  tricubic_eval(a, fr[0], fr[1], fr[2], &p, NULL, NULL, NULL);
+  return p;
+}
+
+static double bicubic_sample(const orc_geom *g, const double *f, double x, double y) {
+  int cx = (int)floor(x), cy = (int)floor(y);
+  double s[16], a[16], p;
+  for (int j = 0; j < 4; ++j)
+    for (int i = 0; i < 4; ++i) s[i + 4 * j] = f[gidx(g, cx - 1 + i, cy - 1 + j, 0)];
+  orc_bicubic_coefs(s, a);
+  bicubic_eval(a, x - cx, y - cy, &p, NULL, NULL);
+  return p;
+}
+
+enum { ORC_LINEAR = 0, ORC_CUBIC = 1 };
+enum { ORC_EULER = 0, ORC_MIDPOINT = 1 };
+
+/* One SL step over the band (or every grid point when band == NULL).
+ * Euler backtrace = LevelSetAdvectSL_2D/_3D, LevelSetMethod/AdvectSL.c:23-89:
+ *   V = MAC velocity at the arrival point X;  S = X - V*dt/h  (index space);
+ *   phi[X] = interpolant(phi0, S).
+ * Midpoint backtrace (new): Xm = X - V(X)*dt/(2h), S = X - V(Xm)*dt/h. */
+ORC_EXPORT int orc_sl_step(const orc_geom *g, const double *phi0, const double *vel, double dt, const int *band,
+                           int nband, int interp, int backtrace, double *phi) {
+  const int is2D = g->nz == 1;
+  const long npts = band ? nband : (long)g->nx * g->ny * g->nz;
+  for (long b = 0; b < npts; ++b) {
+    int xi, yi, zi;
+    if (band) {
+      xi = band[3 * b]; yi = band[3 * b + 1]; zi = band[3 * b + 2];
+    } else {
+      xi = g->px + (int)(b % g->nx);
+      yi = g->py + (int)((b / g->nx) % g->ny);
+      zi = g->pz + (int)(b / ((long)g->nx * g->ny));
+    }
+    double X[3] = {xi, yi, is2D ? 0.0 : zi}, V[3] = {0, 0, 0}, S[3];
+    if (is2D) interp_vel2d(g, vel, X, V); else interp_vel3d(g, vel, X, V);
+    if (backtrace == ORC_MIDPOINT) {
+      double Xm[3] = {X[0] - V[0] * (0.5 * dt) / g->hx, X[1] - V[1] * (0.5 * dt) / g->hy,
+                      is2D ? 0.0 : X[2] - V[2] * (0.5 * dt) / g->hz};
+      if (is2D) interp_vel2d(g, vel, Xm, V); else interp_vel3d(g, vel, Xm, V);
+    }
+    S[0] = X[0] - V[0] * dt / g->hx;
+    S[1] = X[1] - V[1] * dt / g->hy;
+    S[2] = is2D ? 0.0 : X[2] - V[2] * dt / g->hz;
+    double out;
+    if (interp == ORC_LINEAR)
+      out = is2D ? bilinear_ref(g, phi0, S[0], S[1]) : trilinear_ref(g, phi0, S);
+    else
+      out = is2D ? bicubic_sample(g, phi0, S[0], S[1]) : tricubic_sample(g, phi0, S);
+    phi[gidx(g, xi, yi, zi)] = out;
+  }
+  return 0;
+}
+
+/* MAC velocity at arbitrary index-space points (InterpolateVelocity2D/3D). */
+ORC_EXPORT int orc_interp_velocity(const orc_geom *g, const double *vel, const double *X, int n, double *V) {
+  for (int i = 0; i < n; ++i) {
+    if (g->nz == 1) {
+      interp_vel2d(g, vel, X + 3 * i, V + 3 * i);
+      V[3 * i + 2] = 0.0;
+    } else {
+      interp_vel3d(g, vel, X + 3 * i, V + 3 * i);
+    }
+  }
+  return 0;
+}
+
+/* ---------------- finite-difference grid functions ----------------------
+ * GridFunction2D_* Common/Grid.c:214-254, GridFunction3D_* Grid3D.c:33-108,
+ * same operation order.  fn: 0 identity, 1 d/dx, 2 d/dy, 3 d/dz, 4 curvature */
+static double gf3(const orc_geom *g, const double *p, int fn, int i, int j, int k) {
+#define P(a, b, c) p[gidx(g, (a), (b), (c))]
+  const double dx = g->hx, dy = g->hy, dz = g->hz;
+  switch (fn) {
+    case 0: return P(i, j, k);
+    case 1: return (P(i + 1, j, k) - P(i - 1, j, k)) / (2.0 * dx);
+    case 2: return (P(i, j + 1, k) - P(i, j - 1, k)) / (2.0 * dy);
+    case 3: return (P(i, j, k + 1) - P(i, j, k - 1)) / (2.0 * dz);
+    default: {
+      double px = (P(i + 1, j, k) - P(i - 1, j, k)) / (2.0 * dx);
+      double py = (P(i, j + 1, k) - P(i, j - 1, k)) / (2.0 * dy);
+      double pz = (P(i, j, k + 1) - P(i, j, k - 1)) / (2.0 * dz);
+      double px2 = px * px, py2 = py * py, pz2 = pz * pz;
+      double ppp = px2 + py2 + pz2;
+      double pxx = (P(i - 1, j, k) - 2. * P(i, j, k) + P(i + 1, j, k)) / (dx * dx);
+      double pyy = (P(i, j - 1, k) - 2. * P(i, j, k) + P(i, j + 1, k)) / (dy * dy);
+      double pzz = (P(i, j, k - 1) - 2. * P(i, j, k) + P(i, j, k + 1)) / (dz * dz);
+      double pxy = (P(i - 1, j - 1, k) + P(i + 1, j + 1, k) - P(i - 1, j + 1, k) - P(i + 1, j - 1, k)) / (4. * dx * dy);
+      double pxz = (P(i - 1, j, k - 1) + P(i + 1, j, k + 1) - P(i - 1, j, k + 1) - P(i + 1, j, k - 1)) / (4. * dx * dz);
+      double pyz = (P(i, j - 1, k - 1) + P(i, j + 1, k + 1) - P(i, j - 1, k + 1) - P(i, j + 1, k - 1)) / (4. * dy * dz);
+      double c = px2 * (pyy + pzz) + py2 * (pxx + pzz) + pz2 * (pxx + pyy);
+      c -= 2. * (px * py * pxy + px * pz * pxz + py * pz * pyz);
+      c /= sqrt(ppp * ppp * ppp);
+      if (c != c) c = 0;
+      return c;
+    }
+  }
+#undef P
+}
+
+static double gf2(const orc_geom *g, const double *p, int fn, int i, int j) {
+#define P(a, b) p[gidx(g, (a), (b), 0)]
+  const double dx = g->hx, dy = g->hy;
+  switch (fn) {
+    case 0: return P(i, j);
+    case 1: return (P(i + 1, j) - P(i - 1, j)) / (2. * dx);
+    case 2: return (P(i, j + 1) - P(i, j - 1)) / (2. * dy);
+    case 3: return 0.0;
+    default: {
+      double px = (P(i + 1, j) - P(i - 1, j)) / (2. * dx);
+      double py = (P(i, j + 1) - P(i, j - 1)) / (2. * dy);
+      double px2 = px * px, py2 = py * py;
+      double pxx = (P(i - 1, j) - 2. * P(i, j) + P(i + 1, j)) / (dx * dx);
+      double pyy = (P(i, j - 1) - 2. * P(i, j) + P(i, j + 1)) / (dy * dy);
+      double pxy = (P(i - 1, j - 1) + P(i + 1, j + 1) - P(i - 1, j + 1) - P(i + 1, j - 1)) / (4. * dx * dy);
+      double k = (pxx * py2 - 2. * px * py * pxy + pyy * px2) / sqrt((px2 + py2) * (px2 + py2) * (px2 + py2));
+      if (k != k) k = 0;
+      return k;
+    }
+  }
+#undef P
+}
+
+/* Bilinear3D / Bilinear2D of grid function fn at index-space point X. */
+static double sample_gf(const orc_geom *g, const double *p, int fn, const double X[3]) {
+  if (g->nz == 1) {
+    int xi = (int)floor(X[0]), yi = (int)floor(X[1]);
+    double xf = (2. * (X[0] - xi) - 1.), yf = (2. * (X[1] - yi) - 1.), sum = 0.;
+    for (int k = 0; k < 2; ++k)
+      for (int l = 0; l < 2; ++l) {
+        double xb = 1. + (2. * k - 1.) * xf;
+        double yb = 1. + (2. * l - 1.) * yf;
+        sum += gf2(g, p, fn, xi + k, yi + l) * xb * yb;
+      }
+    sum /= 4.;
+    return sum;
+  }
+  int xs = (int)floor(X[0]), ys = (int)floor(X[1]), zs = (int)floor(X[2]);
+  double sx = X[0] - xs, sy = X[1] - ys, sz = X[2] - zs, sum = 0.0;
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j)
+      for (int k = 0; k < 2; ++k) {
+        double xb = i * sx + (1 - i) * (1 - sx);
+        double yb = j * sy + (1 - j) * (1 - sy);
+        double zb = k * sz + (1 - k) * (1 - sz);
+        sum += gf3(g, p, fn, xs + i, ys + j, zs + k) * xb * yb * zb;
+      }
+  return sum;
+}
+
+ORC_EXPORT double orc_sample(const orc_geom *g, const double *p, int fn, double x, double y, double z) {
+  double X[3] = {x, y, z};
+  if (fn == 5) { /* LevelSetDiracDelta2D/3D, LevelSetMethod/NormalDirection.c:36-57 */
+    const double eps = 1.5;
+    const double phival = sample_gf(g, p, 0, X);
+    if (phival < -eps || phival > eps) return 0;
+    const double px = sample_gf(g, p, 1, X), py = sample_gf(g, p, 2, X);
+    double gradmag;
+    if (g->nz == 1) {
+      gradmag = sqrt(px * px + py * py);
+    } else {
+      const double pz = sample_gf(g, p, 3, X);
+      gradmag = sqrt(px * px + py * py + pz * pz);
+    }
+    return gradmag * (1 + cos(3.14159265358979323846264 * phival / eps)) / (2 * eps);
+  }
+  return sample_gf(g, p, fn, X);
+}
+
+/* ---------------- orthogonal projection ---------------------------------- */
+#define ORC_MAXREAL 1.7976931348623157e308
+
+/* OrthogonalProjection2D_Linear, LevelSetMethod/OrthogonalProjection.c:175-195 */
+static void ortho2d_linear(const double phi[3][3], double op[3], double *mindist) {
+  static const int star[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+  *mindist = 2;
+  for (int i = 0; i < 4; ++i) {
+    int x = star[i][0] + 1, y = star[i][1] + 1;
+    if (phi[1][1] * phi[y][x] <= 0) {
+      double dist = phi[1][1] / (phi[1][1] - phi[y][x]);
+      if (dist < *mindist) {
+        *mindist = dist;
+        op[0] = dist * star[i][0];
+        op[1] = dist * star[i][1];
+      }
+    }
+  }
+}
+
+/* OrthogonalProjection2D_Bicubic, OrthogonalProjection.c:30-125: per sub-cell
+ * (i,j) in {0,1}^2 a bicubic patch on phi[j..j+3][i..i+3], damped Newton
+ * x += d1 + d2/2 from the node corner, TOL 1e-3, <= 20 iterations. */
+static void ortho2d_bicubic(const double phi[5][5], double op[3], double *minDist) {
+  const double TOL = 1e-3, TOL2 = TOL * TOL;
+  const int MAXITER = 20;
+  double mindist = ORC_MAXREAL;
+  for (int j = 0; j <= 1; ++j)
+    for (int i = 0; i <= 1; ++i) {
+      double s[16], a[16];
+      for (int y = 0; y < 4; ++y)
+        for (int x = 0; x < 4; ++x) s[x + 4 * y] = phi[j + y][i + x];
+      orc_bicubic_coefs(s, a);
+      double x0x = 1 - i, x0y = 1 - j, x = x0x, y = x0y, dist;
+      int m;
+      for (m = 0; m < MAXITER; ++m) {
+        double p, px, py;
+        bicubic_eval(a, x, y, &p, &px, &py);
+        double pp = px * px + py * py;
+        double d1x = -p * px / pp, d1y = -p * py / pp;
+        double xp = (x0x - x) * px + (x0y - y) * py;
+        double d2x = (x0x - x) - xp / pp * px, d2y = (x0y - y) - xp / pp * py;
+        x += d1x + 0.5 * d2x;
+        y += d1y + 0.5 * d2y;
+        double norm = d1x * d1x + d1y * d1y + d2x * d2x + d2y * d2y;
+        if (norm < TOL2) break;
+      }
+      if (m == MAXITER) dist = ORC_MAXREAL;
+      else if (x < -TOL || 1 + TOL < x || y < -TOL || 1 + TOL < y) dist = ORC_MAXREAL;
+      else dist = sqrt((x - x0x) * (x - x0x) + (y - x0y) * (y - x0y));
+      if (dist < mindist) {
+        mindist = dist;
+        op[0] = x + i - 1;
+        op[1] = y + j - 1;
+        op[2] = 0;
+      }
+    }
+  *minDist = mindist;
+}
+
+/* OrthogonalProjection2D, OrthogonalProjection.c:6-23 */
+ORC_EXPORT void orc_ortho2d(const double *phi3_in, const double *phi5_in, double *op) {
+  double phi3[3][3], phi5[5][5], opB[3] = {0, 0, 0}, opL[3] = {0, 0, 0}, dB, dL;
+  memcpy(phi3, phi3_in, sizeof(phi3));
+  memcpy(phi5, phi5_in, sizeof(phi5));
+  ortho2d_bicubic(phi5, opB, &dB);
+  ortho2d_linear(phi3, opL, &dL);
+  if (dB < dL) memcpy(op, opB, sizeof(opB));
+  else { op[0] = opL[0]; op[1] = opL[1]; op[2] = 0; }
+}
+
+/* OrthogonalProjection3D_Linear, OrthogonalProjection3D.c:187-208 */
+static void ortho3d_linear(const double phi[3][3][3], double op[3]) {
+  static const int star[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  double mindist = 2, dist;
+  for (int i = 0; i < 6; ++i) {
+    int x = star[i][0] + 1, y = star[i][1] + 1, z = star[i][2] + 1;
+    if (phi[1][1][1] * phi[z][y][x] <= 0) {
+      dist = phi[1][1][1] / (phi[1][1][1] - phi[z][y][x]);
+      if (dist < mindist) {
+        mindist = dist;
+        op[0] = dist * star[i][0];
+        op[1] = dist * star[i][1];
+        op[2] = dist * star[i][2];
+      }
+    }
+  }
+}
+
+/* OrthogonalProjection3D_Quadratic, OrthogonalProjection3D.c:131-183 */
+static void ortho3d_quadratic(const double phi[3][3][3], double op[3]) {
+  const int i = 1, j = 1, k = 1;
+  double p = phi[k][j][i];
+  double px = (phi[k][j][i + 1] - phi[k][j][i - 1]) / 2.;
+  double py = (phi[k][j + 1][i] - phi[k][j - 1][i]) / 2.;
+  double pz = (phi[k + 1][j][i] - phi[k - 1][j][i]) / 2.;
+  double px2 = px * px, py2 = py * py, pz2 = pz * pz;
+  double pxx = (phi[k][j][i + 1] - 2. * p + phi[k][j][i - 1]);
+  double pyy = (phi[k][j + 1][i] - 2. * p + phi[k][j - 1][i]);
+  double pzz = (phi[k + 1][j][i] - 2. * p + phi[k - 1][j][i]);
+  double pxy = (phi[k][j - 1][i - 1] + phi[k][j + 1][i + 1] - phi[k][j + 1][i - 1] - phi[k][j - 1][i + 1]) / 4.;
+  double pxz = (phi[k - 1][j][i - 1] + phi[k + 1][j][i + 1] - phi[k + 1][j][i - 1] - phi[k - 1][j][i + 1]) / 4.;
+  double pyz = (phi[k - 1][j - 1][i] + phi[k + 1][j + 1][i] - phi[k + 1][j - 1][i] - phi[k - 1][j + 1][i]) / 4.;
+  double pn = sqrt(px2 + py2 + pz2);
+  double c = (px2 * pxx + py2 * pyy + pz2 * pzz + 2 * px * py * pxy + 2 * px * pz * pxz + 2 * py * pz * pyz) /
+             (px2 + py2 + pz2);
+  double a = 0;
+  for (int m = 0; m < 5; ++m) {
+    double f = p + pn * a + 0.5 * a * a * c;
+    double df = pn + a * c;
+    a = a - f / df;
+  }
+  if (fabs(a) < 1) {
+    op[0] = a * px / pn;
+    op[1] = a * py / pn;
+    op[2] = a * pz / pn;
+  } else {
+    ortho3d_linear(phi, op);
+  }
+}
+
+/* OrthogonalProjection3D, OrthogonalProjection3D.c:6-127: 8 tricubic
+ * sub-cell patches, damped Newton, closest converged in-cell root wins;
+ * quadratic (then linear) fallback when none converges. */
+ORC_EXPORT void orc_ortho3d(const double *phi3_in, const double *phi5_in, double *op) {
+  double phi3[3][3][3], phi5[5][5][5];
+  memcpy(phi3, phi3_in, sizeof(phi3));
+  memcpy(phi5, phi5_in, sizeof(phi5));
+  const double TOL = 1e-3, TOL2 = TOL * TOL;
+  const int MAXITER = 20;
+  double mindist = ORC_MAXREAL;
+  for (int k = 0; k <= 1; ++k)
+    for (int j = 0; j <= 1; ++j)
+      for (int i = 0; i <= 1; ++i) {
+        double s[64], a[64];
+        for (int z = 0; z < 4; ++z)
+          for (int y = 0; y < 4; ++y)
+            for (int x = 0; x < 4; ++x) s[x + 4 * y + 16 * z] = phi5[k + z][j + y][i + x];
+        orc_tricubic_coefs(s, a);
+        double x0[3] = {1 - i, 1 - j, 1 - k}, x = x0[0], y = x0[1], z = x0[2], dist;
+        int m;
+        for (m = 0; m < MAXITER; ++m) {
+          double p, px, py, pz;
+          tricubic_eval(a, x, y, z, &p, &px, &py, &pz);
+          double pp = px * px + py * py + pz * pz;
+          double d1x = -p * px / pp, d1y = -p * py / pp, d1z = -p * pz / pp;
+          double xp = (x0[0] - x) * px + (x0[1] - y) * py + (x0[2] - z) * pz;
+          double d2x = (x0[0] - x) - xp / pp * px, d2y = (x0[1] - y) - xp / pp * py, d2z = (x0[2] - z) - xp / pp * pz;
+          x += d1x + 0.5 * d2x;
+          y += d1y + 0.5 * d2y;
+          z += d1z + 0.5 * d2z;
+          double norm = d1x * d1x + d1y * d1y + d1z * d1z + d2x * d2x + d2y * d2y + d2z * d2z;
+          if (norm < TOL2) break;
+        }
+        if (m == MAXITER) dist = ORC_MAXREAL;
+        else if (x < -TOL || 1 + TOL < x || y < -TOL || 1 + TOL < y || z < -TOL || 1 + TOL < z) dist = ORC_MAXREAL;
+        else dist = sqrt((x - x0[0]) * (x - x0[0]) + (y - x0[1]) * (y - x0[1]) + (z - x0[2]) * (z - x0[2]));
+        if (dist < mindist) {
+          mindist = dist;
+          op[0] = x + i - 1;
+          op[1] = y + j - 1;
+          op[2] = z + k - 1;
+        }
+      }
+  if (fabs(mindist - ORC_MAXREAL) < 1) ortho3d_quadratic(phi3, op);
+}
+
+/* ---------------- irregular nodes ----------------------------------------
+ * Record layout (18 doubles per node, the same as the reference driver's
+ * export):  pos xyz, axis, shift, signCenter, signFace, d, X xyz, op xyz,
+ * n xyz, k.  Order = band order, and within one band point the reference's
+ * emission order (IrregularNodes.c:69-138 / IrregularNodes3D.c:294-360). */
+#define NODE_W 18
+
+static double *node_new(double *out, long *cnt, long cap) {
+  if (*cnt >= cap) { (*cnt)++; return NULL; }
+  double *r = out + NODE_W * (*cnt)++;
+  memset(r, 0, sizeof(double) * NODE_W);
+  return r;
+}
+
+static const int kFace[4][3] = {{0, 0, 0}, {-1, 0, 0}, {0, -1, 0}, {0, 0, -1}}; /* STAGGERED_GRID */
+
+ORC_EXPORT long orc_irregular_nodes(const orc_geom *g, const double *phi, const int *band, int nband, double *out,
+                                    long cap) {
+  long cnt = 0;
+  const int is2D = g->nz == 1;
+  for (int b = 0; b < nband; ++b) {
+    const int i = band[3 * b], j = band[3 * b + 1], k = is2D ? 0 : band[3 * b + 2];
+    double *n;
+    if (is2D) {
+      double sten[3][3], local[5][5];
+      for (int J = -2; J <= 2; ++J)
+        for (int I = -2; I <= 2; ++I) local[J + 2][I + 2] = phi[gidx(g, I + i, J + j, 0)];
+      for (int J = -1; J <= 1; ++J)
+        for (int I = -1; I <= 1; ++I) sten[J + 1][I + 1] = phi[gidx(g, I + i, J + j, 0)];
+      static const int nei[4][2] = {{1, 0}, {-1, 0}, {0, -1}, {0, 1}};
+      for (int m = 0; m < 4; ++m) {
+        int ni = 1 + nei[m][0], nj = 1 + nei[m][1];
+        if (sten[1][1] * sten[nj][ni] <= 0.) {
+          if ((n = node_new(out, &cnt, cap))) {
+            double op[3] = {0, 0, 0};
+            orc_ortho2d(&sten[0][0], &local[0][0], op);
+            n[0] = i; n[1] = j; n[2] = band[3 * b + 2];
+            n[3] = -1; n[4] = -1; n[5] = sten[1][1] > 0. ? 1 : -1;
+            n[11] = op[0]; n[12] = op[1]; n[13] = op[2];
+            n[8] = n[0] + op[0]; n[9] = n[1] + op[1];
+          }
+          break;
+        }
+      }
+      for (int f = 1; f <= 2; ++f) {
+        int ni = 1 + kFace[f][0], nj = 1 + kFace[f][1];
+        if (sten[1][1] * sten[nj][ni] <= 0.) {
+          if ((n = node_new(out, &cnt, cap))) {
+            n[7] = sten[1][1] / (sten[1][1] - sten[nj][ni]);
+            n[5] = sten[1][1] > 0. ? 1 : -1;
+            n[6] = n[7] < 0.5 ? -n[5] : n[5];
+            n[0] = i; n[1] = j; n[2] = band[3 * b + 2];
+            n[4] = 0; n[3] = f - 1;
+            n[8] = n[0] + n[7] * kFace[f][0];
+            n[9] = n[1] + n[7] * kFace[f][1];
+          }
+        }
+      }
+      /* U-velocity Laplacian (IrregularNodes.c:108-122) */
+      double hi = (sten[1][0] + sten[1][1]) / 2., lo = (sten[0][0] + sten[0][1]) / 2.;
+      if (hi * lo <= 0.) {
+        if ((n = node_new(out, &cnt, cap))) {
+          n[7] = hi / (hi - lo);
+          n[5] = hi > 0. ? 1 : -1;
+          n[6] = n[7] < 0.5 ? -n[5] : n[5];
+          n[0] = i; n[1] = j; n[2] = band[3 * b + 2];
+          n[4] = 1; n[3] = 1;
+          n[8] = n[0] + kFace[1][0] / 2.;
+          n[9] = n[1] + kFace[1][1] / 2. - n[7];
+        }
+      }
+      /* V-velocity Laplacian (IrregularNodes.c:124-138) */
+      hi = (sten[0][1] + sten[1][1]) / 2.;
+      lo = (sten[0][0] + sten[1][0]) / 2.;
+      if (hi * lo <= 0.) {
+        if ((n = node_new(out, &cnt, cap))) {
+          n[7] = hi / (hi - lo);
+          n[5] = hi > 0. ? 1 : -1;
+          n[6] = n[7] < 0.5 ? -n[5] : n[5];
+          n[0] = i; n[1] = j; n[2] = band[3 * b + 2];
+          n[4] = 2; n[3] = 0;
+          n[8] = n[0] + kFace[2][0] / 2. - n[7];
+          n[9] = n[1] + kFace[2][1] / 2.;
+        }
+      }
+    } else {
+      double sten[3][3][3], local[5][5][5];
+      for (int K = -2; K <= 2; ++K)
+        for (int J = -2; J <= 2; ++J)
+          for (int I = -2; I <= 2; ++I) local[K + 2][J + 2][I + 2] = phi[gidx(g, I + i, J + j, K + k)];
+      for (int K = -1; K <= 1; ++K)
+        for (int J = -1; J <= 1; ++J)
+          for (int I = -1; I <= 1; ++I) sten[K + 1][J + 1][I + 1] = phi[gidx(g, I + i, J + j, K + k)];
+      static const int star[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+      for (int m = 0; m < 6; ++m) {
+        int ni = 1 + star[m][0], nj = 1 + star[m][1], nk = 1 + star[m][2];
+        if (sten[1][1][1] * sten[nk][nj][ni] <= 0.) {
+          if ((n = node_new(out, &cnt, cap))) {
+            double op[3] = {0, 0, 0};
+            orc_ortho3d(&sten[0][0][0], &local[0][0][0], op);
+            n[0] = i; n[1] = j; n[2] = k;
+            n[3] = -1; n[4] = -1; n[5] = sten[1][1][1] > 0. ? 1 : -1;
+            n[11] = op[0]; n[12] = op[1]; n[13] = op[2];
+            n[8] = n[0] + op[0]; n[9] = n[1] + op[1]; n[10] = n[2] + op[2];
+          }
+          break;
+        }
+      }
+      for (int f = 1; f <= 3; ++f) {
+        int ni = 1 + kFace[f][0], nj = 1 + kFace[f][1], nk = 1 + kFace[f][2];
+        if (sten[1][1][1] * sten[nk][nj][ni] <= 0.) {
+          if ((n = node_new(out, &cnt, cap))) {
+            n[7] = sten[1][1][1] / (sten[1][1][1] - sten[nk][nj][ni]);
+            n[5] = sten[1][1][1] > 0. ? 1 : -1;
+            n[6] = n[7] < 0.5 ? -n[5] : n[5];
+            n[0] = i; n[1] = j; n[2] = k;
+            n[4] = 0; n[3] = f - 1;
+            n[8] = n[0] + n[7] * kFace[f][0];
+            n[9] = n[1] + n[7] * kFace[f][1];
+            n[10] = n[2] + n[7] * kFace[f][2];
+          }
+        }
+      }
+      /* velocity-face nodes (IrregularNodes3D.c:337-360) */
+      for (int face = 1; face <= 3; ++face) {
+        const int *gg = kFace[face];
+        double hi = (sten[1 + gg[2]][1 + gg[1]][1 + gg[0]] + sten[1][1][1]) / 2.;
+        for (int axis = 1; axis <= 3; ++axis) {
+          if (face == axis) continue;
+          const int *lo3 = kFace[axis];
+          double lo = (sten[1 + gg[2] + lo3[2]][1 + gg[1] + lo3[1]][1 + gg[0] + lo3[0]] +
+                       sten[1 + lo3[2]][1 + lo3[1]][1 + lo3[0]]) / 2.;
+          if (hi * lo <= 0.) {
+            if ((n = node_new(out, &cnt, cap))) {
+              n[7] = hi / (hi - lo);
+              if (n[7] != n[7]) n[7] = 0;
+              n[5] = hi > 0. ? 1 : -1;
+              n[6] = n[7] < 0.5 ? -n[5] : n[5];
+              n[0] = i; n[1] = j; n[2] = k;
+              n[4] = face; n[3] = axis - 1;
+              n[8] = n[0] + kFace[face][0] / 2. + n[7] * kFace[axis][0];
+              n[9] = n[1] + kFace[face][1] / 2. + n[7] * kFace[axis][1];
+              n[10] = n[2] + kFace[face][2] / 2. + n[7] * kFace[axis][2];
+            }
+          }
+        }
+      }
+    }
+  }
+  return cnt;
+}
+
+/* Surface quantities at node positions X (IIM/SurfaceQuantities.c 2D:48-56,
+ * 3D:83-89,111): normal = normalised bilinear FD gradient, k = bilinear
+ * curvature.  Writes fields 14-17 of each record. */
+ORC_EXPORT void orc_node_surface(const orc_geom *g, const double *phi, double *nodes, long n) {
+  for (long q = 0; q < n; ++q) {
+    double *r = nodes + NODE_W * q;
+    double X[3] = {r[8], r[9], r[10]};
+    if (g->nz == 1) {
+      double nx = sample_gf(g, phi, 1, X), ny = sample_gf(g, phi, 2, X);
+      double h = sqrt(nx * nx + ny * ny);
+      r[14] = nx / h; r[15] = ny / h; r[16] = 0;
+    } else {
+      double nx = sample_gf(g, phi, 1, X), ny = sample_gf(g, phi, 2, X), nz = sample_gf(g, phi, 3, X);
+      double h = sqrt(nx * nx + ny * ny + nz * nz);
+      nx /= h; ny /= h; nz /= h;
+      r[14] = nx; r[15] = ny; r[16] = nz;
+    }
+    r[17] = sample_gf(g, phi, 4, X);
+  }
+}
+
+/* LevelSet_MaxVelocity, LevelSetMethod/Advect.c:70-111: max |V| over the
+ * integer positions of the irregular nodes. */
+ORC_EXPORT double orc_max_velocity(const orc_geom *g, const double *vel, const double *nodes, long n) {
+  double maxv = 0;
+  for (long q = 0; q < n; ++q) {
+    const double *r = nodes + NODE_W * q;
+    double X[3] = {r[0], r[1], r[2]}, V[3] = {0, 0, 0}, mag;
+    if (g->nz == 1) {
+      interp_vel2d(g, vel, X, V);
+      mag = sqrt(V[0] * V[0] + V[1] * V[1]);
+    } else {
+      interp_vel3d(g, vel, X, V);
+      mag = sqrt(V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+    }
+    maxv = mag > maxv ? mag : maxv;
+  }
+  return maxv;
+}
+
+/* Enclosed volume (area in 2D) through the smoothed Heaviside
+ * H_eps(phi) = 0 | 1 | (1 + phi/eps + sin(pi phi/eps)/pi)/2, eps in the units of
+ * phi; inside = sum (1 - H) * cell volume.  The integral of the reference's
+ * smoothed delta (NormalDirection.c:36-57). */
+ORC_EXPORT double orc_volume(const orc_geom *g, const double *phi, double eps) {
+  const double pi = 3.14159265358979323846264;
+  double cell = g->hx * g->hy * (g->nz == 1 ? 1.0 : g->hz), acc = 0.0;
+  size_t npts = (size_t)g->nx * g->ny * g->nz;
+  for (size_t q = 0; q < npts; ++q) {
+    double p = phi[q], H;
+    if (p < -eps) H = 0.0;
+    else if (p > eps) H = 1.0;
+    else H = 0.5 * (1.0 + p / eps + sin(pi * p / eps) / pi);
+    acc += 1.0 - H;
+  }
+  return acc * cell;
+}

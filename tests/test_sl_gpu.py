@@ -1,0 +1,183 @@
+"""GPU parity of the semi-Lagrangian step against the reference and the oracle.
+
+* FP64 linear/Euler (the reference's own AdvectSL arithmetic) must reproduce
+  the reference's outputs bit for bit (golden fixtures from its compiled C).
+* FP32 paths: within FP32 rounding of the FP64 results.
+* Cubic paths: against the oracle's FP64 Catmull-Rom restatement.
+* Split-BF16 tensor-core path: max |error| <= 1e-5 (physical units) in the
+  |phi| < 3h band on a smooth signed distance, vs the FP64 oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from dcell_b200 import _lib, fields
+from dcell_b200 import levelset as L
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a, dev, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=dev)
+
+
+def _run(g, dev, dtype, interp="linear", backtrace="euler", vel_key="vel", dt=None, phi_in=None):
+    phi0 = _t(g["phi0"], dev, dtype)
+    vel = _t(g[vel_key], dev, dtype)
+    band = torch.as_tensor(g["band"], dtype=torch.int32, device=dev)
+    out = phi0.clone() if phi_in is None else _t(phi_in, dev, dtype)
+    flags = torch.zeros(1, dtype=torch.int32, device=dev)
+    L.sl_step(phi0, vel, float(g["dt"]) if dt is None else dt, float(g["h"]), tuple(g["origin"]), band=band,
+              interp=interp, backtrace=backtrace, out=out, flags=flags)
+    torch.cuda.synchronize()
+    assert int(flags.item()) == 0
+    return out.cpu().numpy().astype(np.float64)
+
+
+@pytest.mark.parametrize("case", ["sl3d_linear", "sl2d_linear"])
+def test_linear_fp64_bit_exact_vs_reference(golden, cuda, case):
+    g = golden(case)
+    out = _run(g, cuda, torch.float64)
+    assert np.array_equal(out, g["phi"])
+
+
+@pytest.mark.parametrize("case", ["sl3d_linear", "sl2d_linear"])
+def test_linear_fp32_vs_reference(golden, cuda, case):
+    g = golden(case)
+    out = _run(g, cuda, torch.float32)
+    scale = np.abs(g["phi"]).max()
+    assert np.abs(out - g["phi"]).max() <= 4e-7 * scale
+
+
+def test_rk2_half_full_fp64_bit_exact(golden, cuda):
+    """AdvectRK2.c: HalfStep(dt/2, u^n) then FullStep(dt, u^{n+1/2}) from the same phi0."""
+    g = golden("sl3d_rk2")
+    dt = float(g["dt"])
+    half = _run(g, cuda, torch.float64, dt=dt / 2)
+    assert np.array_equal(half, g["phi_half"])
+    full = _run(g, cuda, torch.float64, vel_key="vel_half", dt=dt, phi_in=half)
+    assert np.array_equal(full, g["phi_full"])
+
+
+@pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
+@pytest.mark.parametrize("case", ["sl3d_linear", "sl2d_linear"])
+def test_cubic_fp64_vs_oracle(golden, cuda, case, backtrace):
+    g = golden(case)
+    ref = oracle.sl_step(g["phi0"], g["vel"], float(g["dt"]), float(g["h"]), origin=g["origin"], band=g["band"],
+                         interp="cubic", backtrace=backtrace, phi=g["phi0"])
+    for interp in ("cubic_plain", "cubic_separable"):
+        out = _run(g, cuda, torch.float64, interp=interp, backtrace=backtrace)
+        assert np.abs(out - ref).max() < 1e-12, interp
+
+
+def test_linear_midpoint_fp64_vs_oracle(golden, cuda):
+    g = golden("sl3d_linear")
+    ref = oracle.sl_step(g["phi0"], g["vel"], float(g["dt"]), float(g["h"]), origin=g["origin"], band=g["band"],
+                         interp="linear", backtrace="midpoint", phi=g["phi0"])
+    out = _run(g, cuda, torch.float64, backtrace="midpoint")
+    assert np.abs(out - ref).max() < 1e-12
+
+
+@pytest.mark.parametrize("interp", ["cubic_plain", "cubic_separable", "cubic_tc"])
+def test_cubic_fp32_vs_oracle_golden_case(golden, cuda, interp):
+    """Cell-unit signed distance (|phi| up to ~12): FP32 relative accuracy."""
+    g = golden("sl3d_linear")
+    ref = oracle.sl_step(g["phi0"], g["vel"], float(g["dt"]), float(g["h"]), origin=g["origin"], band=g["band"],
+                         interp="cubic", phi=g["phi0"])
+    out = _run(g, cuda, torch.float32, interp=interp)
+    tol = 2e-5 if interp == "cubic_tc" else 4e-6
+    assert np.abs(out - ref).max() <= tol * np.abs(ref).max(), np.abs(out - ref).max()
+
+
+def _sphere_case(N, dev):
+    h = 1.0 / N
+    phi = fields.sphere_sdf(N, device=dev)
+    vel = fields.deformation_velocity(N, device=dev)
+    dt = fields.cfl_dt((2.0, 1.0, 1.0), h) * fields.deformation_time_factor(0.37)
+    return h, phi, vel, dt
+
+
+@pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
+def test_tensor_core_dense_error_budget(cuda, backtrace):
+    """Dense 64^3 sphere in the deformation field: split-BF16 TC and plain FP32
+    vs the FP64 GPU oracle (itself checked against the CPU oracle on a sample)."""
+    N = 64
+    h, phi, vel, dt = _sphere_case(N, cuda)
+    ref = L.sl_step(phi, vel, dt, h, interp="cubic_plain", backtrace=backtrace)
+    # FP64 GPU oracle == CPU oracle
+    cpu = oracle.sl_step(phi.cpu().numpy(), vel.cpu().numpy(), dt, h, interp="cubic", backtrace=backtrace)
+    assert np.abs(ref.cpu().numpy() - cpu).max() < 1e-13
+    band = (ref.abs() < 3 * h)
+    p32, v32 = phi.float().contiguous(), vel.float().contiguous()
+    for interp, tol in (("cubic_tc", 1e-5), ("cubic_plain", 1e-6), ("cubic_separable", 1e-6)):
+        out = L.sl_step(p32, v32, dt, h, interp=interp, backtrace=backtrace).double()
+        err = (out - ref).abs()
+        assert float(err[band].max()) <= tol, (interp, float(err[band].max()))
+        assert float(err.max()) <= 10 * tol, (interp, float(err.max()))
+
+
+def test_tensor_core_band_mode_matches_dense(cuda):
+    N = 48
+    h, phi, vel, dt = _sphere_case(N, cuda)
+    p32, v32 = phi.float().contiguous(), vel.float().contiguous()
+    dense = L.sl_step(p32, v32, dt, h, interp="cubic_tc")
+    band = fields.band_of(phi, 6 * h).to(cuda)
+    banded = L.sl_step(p32, v32, dt, h, band=band, interp="cubic_tc", out=p32.clone())
+    sel = torch.zeros_like(phi, dtype=torch.bool)
+    sel[band[:, 2].long(), band[:, 1].long(), band[:, 0].long()] = True
+    assert torch.equal(banded[sel], dense[sel])
+    assert torch.equal(banded[~sel], p32[~sel])
+
+
+def test_tc_gemm_layout(cuda):
+    """The tensor-core operand layouts: D = bf16(A) M^T against a host product."""
+    rng = np.random.default_rng(3)
+    A = rng.normal(size=(128, 64)).astype(np.float32)
+    Ab = torch.as_tensor(A).to(torch.bfloat16).float().numpy().astype(np.float64)
+    M = oracle.catmull_rom_operator(3)
+    a = torch.as_tensor(A, device=cuda)
+    d = torch.zeros((128, 64), dtype=torch.float32, device=cuda)
+    flags = torch.zeros(1, dtype=torch.int32, device=cuda)
+    import ctypes
+    _lib.check(_lib.lib().dcell_tc_gemm_check(ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(d.data_ptr()),
+                                              ctypes.c_void_p(flags.data_ptr()),
+                                              ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    assert int(flags.item()) == 0
+    expect = Ab @ M.T
+    assert np.abs(d.cpu().numpy() - expect).max() < 1e-4 * np.abs(expect).max()
+
+
+def test_departure_outside_grid_is_flagged(cuda):
+    N = 16
+    phi = torch.zeros((N, N, N), dtype=torch.float32, device=cuda)
+    vel = torch.full((N, N, N, 3), 4.0, dtype=torch.float32, device=cuda)
+    flags = torch.zeros(1, dtype=torch.int32, device=cuda)
+    for interp in ("linear", "cubic_plain", "cubic_tc"):
+        flags.zero_()
+        L.sl_step(phi, vel, 1.0, 1.0, interp=interp, flags=flags)
+        torch.cuda.synchronize()
+        assert int(flags.item()) & _lib.FLAG_DEPARTURE_CLAMPED
+
+
+def test_zero_velocity_is_identity(cuda):
+    N = 24
+    phi = fields.sphere_sdf(N, device=cuda).float()
+    vel = torch.zeros((N, N, N, 3), dtype=torch.float32, device=cuda)
+    for interp in ("linear", "cubic_plain", "cubic_separable", "cubic_tc"):
+        out = L.sl_step(phi, vel, 0.1, 1.0 / N, interp=interp)
+        tol = 0 if interp != "cubic_tc" else 1e-7
+        assert float((out - phi).abs().max()) <= tol, interp
+
+
+def test_integer_shift_is_exact_translation(cuda):
+    """u = 1 cell/step along x: departure = X - 1 exactly (fraction 0)."""
+    N = 20
+    phi = fields.sphere_sdf(N, device=cuda).float()
+    vel = torch.zeros((N, N, N, 3), dtype=torch.float32, device=cuda)
+    vel[..., 0] = 1.0
+    for interp in ("linear", "cubic_plain", "cubic_separable", "cubic_tc"):
+        out = L.sl_step(phi, vel, 1.0 / N, 1.0 / N, interp=interp)
+        tol = 0 if interp != "cubic_tc" else 1e-7
+        assert float((out[:, :, 1:] - phi[:, :, :-1]).abs().max()) <= tol, interp
