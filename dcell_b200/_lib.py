@@ -16,7 +16,7 @@ OK, ERR_ARG, ERR_CUDA, ERR_DEPARTURE, ERR_NONFINITE, ERR_TIMEOUT, ERR_CAPACITY, 
 F32, F64 = 0, 1
 LINEAR, CUBIC_PLAIN, CUBIC_SEPARABLE, CUBIC_TC = 0, 1, 2, 3
 EULER, MIDPOINT = 0, 1
-FLAG_DEPARTURE_CLAMPED, FLAG_NONFINITE, FLAG_CAPACITY, FLAG_WAIT_TIMEOUT = 1, 2, 4, 8
+FLAG_DEPARTURE_CLAMPED, FLAG_NONFINITE, FLAG_CAPACITY, FLAG_WAIT_TIMEOUT, FLAG_BAD_BAND = 1, 2, 4, 8, 16
 
 INTERP = {"linear": LINEAR, "cubic": CUBIC_PLAIN, "cubic_plain": CUBIC_PLAIN, "cubic_separable": CUBIC_SEPARABLE,
           "cubic_tc": CUBIC_TC}

@@ -42,7 +42,7 @@ static int check_geom(const dcell_geom *g) {
   if (!(g->h[0] > 0) || !(g->h[1] > 0) || (g->n[2] > 1 && !(g->h[2] > 0)))
     FAIL(DCELL_ERR_ARG, "grid spacing must be positive");
   const long long n = (long long)g->n[0] * g->n[1] * (g->n[2] > 1 ? g->n[2] : 1);
-  if (n > (1LL << 40)) FAIL(DCELL_ERR_ARG, "grid too large");
+  if (3 * n >= (1LL << 31)) FAIL(DCELL_ERR_ARG, "grid too large (3 * points must stay below 2^31)");
   return DCELL_OK;
 }
 
@@ -167,6 +167,7 @@ struct dcell_session {
 static int session_flags_status(dcell_session *s, int flags) {
   if (flags & DCELL_FLAG_WAIT_TIMEOUT) FAIL(DCELL_ERR_TIMEOUT, "a device-side wait timed out");
   if (flags & DCELL_FLAG_CAPACITY) FAIL(DCELL_ERR_CAPACITY, "node capacity exceeded");
+  if (flags & DCELL_FLAG_BAD_BAND) FAIL(DCELL_ERR_ARG, "a band entry lies outside the grid");
   if (flags & DCELL_FLAG_DEPARTURE_CLAMPED)
     FAIL(DCELL_ERR_DEPARTURE, "a departure point left the grid; its sample was clamped to the grid");
   (void)s;

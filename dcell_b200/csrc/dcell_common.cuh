@@ -60,12 +60,30 @@ __device__ __forceinline__ void arrival(const Geom &g, const int *__restrict__ b
   }
 }
 
+// Local (origin-relative) arrival point of number q; false when a band entry
+// lies outside the grid (the point is then skipped and flagged).
+__device__ __forceinline__ bool arrival_local(const Geom &g, const int *__restrict__ band, long long q, int &x,
+                                              int &y, int &z) {
+  if (band) {
+    x = band[3 * q] - g.px;
+    y = band[3 * q + 1] - g.py;
+    z = g.nz == 1 ? 0 : band[3 * q + 2] - g.pz;
+    return (unsigned)x < (unsigned)g.nx && (unsigned)y < (unsigned)g.ny && (unsigned)z < (unsigned)g.nz;
+  }
+  const int n = (int)q;
+  x = n % g.nx;
+  y = (n / g.nx) % g.ny;
+  z = n / (g.nx * g.ny);
+  return true;
+}
+
 // Status bits a kernel may raise in its optional device flags word.
 enum : int {
   FLAG_DEPARTURE_CLAMPED = 1,  // a departure point fell outside the grid
   FLAG_NONFINITE = 2,          // a non-finite value was produced
   FLAG_CAPACITY = 4,           // output list capacity exceeded
   FLAG_WAIT_TIMEOUT = 8,       // a bounded device wait gave up
+  FLAG_BAD_BAND = 16,          // a band entry lies outside the grid (skipped)
 };
 
 __device__ __forceinline__ void raise_flag(int *flags, int bit) {

@@ -25,12 +25,7 @@ template <typename T, int DIM>
 __device__ __forceinline__ T cubic_plain(const Geom &g, const T *__restrict__ phi0, const int c[3], const T f[3]) {
   if (DIM == 3) {
     T s[64];
-#pragma unroll
-    for (int z = 0; z < 4; ++z)
-#pragma unroll
-      for (int y = 0; y < 4; ++y)
-#pragma unroll
-        for (int x = 0; x < 4; ++x) s[x + 4 * y + 16 * z] = phi0[gidx(g, c[0] - 1 + x, c[1] - 1 + y, c[2] - 1 + z)];
+    gather_stencil<T, 3>(g, phi0, c, s);
     // a = M s with M = C (x) C (x) C: the 1331 non-zeros as straight-line code
     T a[64];
     DCELL_CR_COEFS3(s, a);
@@ -50,10 +45,7 @@ __device__ __forceinline__ T cubic_plain(const Geom &g, const T *__restrict__ ph
     return pz;
   } else {
     T s[16];
-#pragma unroll
-    for (int y = 0; y < 4; ++y)
-#pragma unroll
-      for (int x = 0; x < 4; ++x) s[x + 4 * y] = phi0[gidx(g, c[0] - 1 + x, c[1] - 1 + y, 0)];
+    gather_stencil<T, 2>(g, phi0, c, s);
     T a[16];
     DCELL_CR_COEFS2(s, a);
     T py = T(0);
@@ -72,6 +64,8 @@ __device__ __forceinline__ T cubic_separable(const Geom &g, const T *__restrict_
   T wx[4], wy[4];
   cr_weights<T>(f[0], wx);
   cr_weights<T>(f[1], wy);
+  T s[DIM == 3 ? 64 : 16];
+  gather_stencil<T, DIM>(g, phi0, c, s);
   if (DIM == 3) {
     T wz[4];
     cr_weights<T>(f[2], wz);
@@ -83,7 +77,7 @@ __device__ __forceinline__ T cubic_separable(const Geom &g, const T *__restrict_
       for (int y = 0; y < 4; ++y) {
         T accx = T(0);
 #pragma unroll
-        for (int x = 0; x < 4; ++x) accx += wx[x] * phi0[gidx(g, c[0] - 1 + x, c[1] - 1 + y, c[2] - 1 + z)];
+        for (int x = 0; x < 4; ++x) accx += wx[x] * s[x + 4 * y + 16 * z];
         accy += wy[y] * accx;
       }
       acc += wz[z] * accy;
@@ -95,7 +89,7 @@ __device__ __forceinline__ T cubic_separable(const Geom &g, const T *__restrict_
     for (int y = 0; y < 4; ++y) {
       T accx = T(0);
 #pragma unroll
-      for (int x = 0; x < 4; ++x) accx += wx[x] * phi0[gidx(g, c[0] - 1 + x, c[1] - 1 + y, 0)];
+      for (int x = 0; x < 4; ++x) accx += wx[x] * s[x + 4 * y];
       acc += wy[y] * accx;
     }
     return acc;
@@ -107,16 +101,21 @@ __global__ void __launch_bounds__(256) sl_cubic_kernel(Geom g, const T *__restri
                                                        T dt, const int *__restrict__ band, long long npts,
                                                        int backtrace, T *__restrict__ phi, int *flags) {
   const T dth[3] = {dt / (T)g.hx, dt / (T)g.hy, dt / (T)g.hz};
-  bool clamped = false;
+  bool clamped = false, bad = false;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npts;
        q += (long long)gridDim.x * blockDim.x) {
     int x, y, z, c[3];
     T f[3];
-    arrival(g, band, q, x, y, z);
+    if (!arrival_local(g, band, q, x, y, z)) {
+      bad = true;
+      continue;
+    }
     clamped |= departure_cell<T, DIM>(g, vel, dth, backtrace, x, y, z, c, f);
-    phi[gidx(g, x, y, z)] = SEPARABLE ? cubic_separable<T, DIM>(g, phi0, c, f) : cubic_plain<T, DIM>(g, phi0, c, f);
+    phi[(z * g.ny + y) * g.nx + x] =
+        SEPARABLE ? cubic_separable<T, DIM>(g, phi0, c, f) : cubic_plain<T, DIM>(g, phi0, c, f);
   }
-  if (clamped) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);
+  if (clamped && band) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);  // dense grids: the edge is the domain boundary
+  if (bad) raise_flag(flags, FLAG_BAD_BAND);
 }
 
 // FP64 <-> FP32 conversion and band gathers for the host-buffer entry points.

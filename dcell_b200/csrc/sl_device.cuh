@@ -11,65 +11,71 @@
 
 namespace dcell {
 
-// MAC velocity at integer node (x, y, z): each component is the mean of its
-// two faces around the node -- InterpolateVelocity3D/2D
+// Index math of this path is 32-bit: the C ABI rejects grids with 3 * points
+// >= 2^31.  Gathers take LOCAL indices (origin subtracted) and clamp only on
+// the slow path, when a stencil touches the grid edge.
+
+// MAC velocity at local node (x, y, z): each component is the mean of its two
+// faces around the node -- InterpolateVelocity3D/2D
 // (Common/InterpolateVelocity.c:35-67) at an integer point, where the
 // off-axis trilinear weights vanish.
 template <typename T, int DIM>
 __device__ __forceinline__ void mac_vel_node(const Geom &g, const T *__restrict__ vel, int x, int y, int z, T V[3]) {
+  const int q = (z * g.ny + y) * g.nx + x;
+  const T *c = vel + DIM * q;
+  const int dx = x + 1 < g.nx ? DIM : 0, dy = y + 1 < g.ny ? DIM * g.nx : 0;
+  V[0] = T(0.5) * __ldg(c) + T(0.5) * __ldg(c + dx);
+  V[1] = T(0.5) * __ldg(c + 1) + T(0.5) * __ldg(c + dy + 1);
   if (DIM == 3) {
-    V[0] = T(0.5) * vel[gidx(g, x, y, z) * 3 + 0] + T(0.5) * vel[gidx(g, x + 1, y, z) * 3 + 0];
-    V[1] = T(0.5) * vel[gidx(g, x, y, z) * 3 + 1] + T(0.5) * vel[gidx(g, x, y + 1, z) * 3 + 1];
-    V[2] = T(0.5) * vel[gidx(g, x, y, z) * 3 + 2] + T(0.5) * vel[gidx(g, x, y, z + 1) * 3 + 2];
+    const int dz = z + 1 < g.nz ? 3 * g.nx * g.ny : 0;
+    V[2] = T(0.5) * __ldg(c + 2) + T(0.5) * __ldg(c + dz + 2);
   } else {
-    V[0] = T(0.5) * vel[gidx(g, x, y, 0) * 2 + 0] + T(0.5) * vel[gidx(g, x + 1, y, 0) * 2 + 0];
-    V[1] = T(0.5) * vel[gidx(g, x, y, 0) * 2 + 1] + T(0.5) * vel[gidx(g, x, y + 1, 0) * 2 + 1];
     V[2] = T(0);
   }
 }
 
-// MAC velocity at node + delta (|delta| small), trilinear per component with
-// the component's half-cell stagger (Tensor1, Common/Common.h:26-30).
+// MAC velocity at local node + delta (|delta| small), trilinear per component
+// with the component's half-cell stagger (Tensor1, Common/Common.h:26-30).
 template <typename T, int DIM>
 __device__ __forceinline__ void mac_vel_rel(const Geom &g, const T *__restrict__ vel, int x, int y, int z,
                                             const T dl[3], T V[3]) {
+  const int X[3] = {x, y, z}, n[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
     int b[3];
     T s[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
+      if (a == 2 && DIM == 2) { b[2] = 0; s[2] = T(0); continue; }
       const T t = dl[a] + (a == d ? T(0.5) : T(0));
       const T f = floor(t);
-      b[a] = (a == 0 ? x : a == 1 ? y : z) + (int)f;
+      b[a] = X[a] + (int)f;
       s[a] = t - f;
     }
-    T sum = 0;
+    // offsets of the +1 neighbour per axis (0 when clamped at the upper edge)
+    int o[3], bc[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      bc[a] = clampi(b[a], 0, n[a] - 1);
+      const int up = clampi(b[a] + 1, 0, n[a] - 1) - bc[a];
+      o[a] = up * (a == 0 ? DIM : a == 1 ? DIM * g.nx : DIM * g.nx * g.ny);
+    }
+    const T *c = vel + DIM * ((bc[2] * g.ny + bc[1]) * g.nx + bc[0]) + d;
+    const T wx0 = 1 - s[0], wy0 = 1 - s[1];
+    T sum = (wx0 * __ldg(c) + s[0] * __ldg(c + o[0])) * wy0 +
+            (wx0 * __ldg(c + o[1]) + s[0] * __ldg(c + o[1] + o[0])) * s[1];
     if (DIM == 3) {
-#pragma unroll
-      for (int k = 0; k < 2; ++k)
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int i = 0; i < 2; ++i) {
-            const T w = (i ? s[0] : 1 - s[0]) * (j ? s[1] : 1 - s[1]) * (k ? s[2] : 1 - s[2]);
-            sum += w * vel[gidx(g, b[0] + i, b[1] + j, b[2] + k) * 3 + d];
-          }
-    } else {
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const T w = (i ? s[0] : 1 - s[0]) * (j ? s[1] : 1 - s[1]);
-          sum += w * vel[gidx(g, b[0] + i, b[1] + j, 0) * 2 + d];
-        }
+      const T *c2 = c + o[2];
+      const T top = (wx0 * __ldg(c2) + s[0] * __ldg(c2 + o[0])) * wy0 +
+                    (wx0 * __ldg(c2 + o[1]) + s[0] * __ldg(c2 + o[1] + o[0])) * s[1];
+      sum = sum * (1 - s[2]) + top * s[2];
     }
     V[d] = sum;
   }
   if (DIM == 2) V[2] = T(0);
 }
 
-// Departure cell (global indices) and fraction for arrival node (x, y, z).
+// Departure cell (LOCAL indices) and fraction for local arrival node (x, y, z).
 // dth[a] = dt / h[a].  Returns true if the departure point left the grid.
 template <typename T, int DIM>
 __device__ __forceinline__ bool departure_cell(const Geom &g, const T *__restrict__ vel, const T dth[3], int backtrace,
@@ -80,13 +86,12 @@ __device__ __forceinline__ bool departure_cell(const Geom &g, const T *__restric
     const T dl[3] = {T(-0.5) * V[0] * dth[0], T(-0.5) * V[1] * dth[1], DIM == 3 ? T(-0.5) * V[2] * dth[2] : T(0)};
     mac_vel_rel<T, DIM>(g, vel, x, y, z, dl, V);
   }
-  const int X[3] = {x, y, z};
+  const int X[3] = {x, y, z}, n[3] = {g.nx, g.ny, g.nz};
   bool out = false;
-  const int lo[3] = {g.px, g.py, g.pz}, n[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     if (a == 2 && DIM == 2) {
-      c[2] = z;
+      c[2] = 0;
       f[2] = T(0);
       continue;
     }
@@ -94,9 +99,43 @@ __device__ __forceinline__ bool departure_cell(const Geom &g, const T *__restric
     const T fl = floor(t);
     c[a] = X[a] + (int)fl;
     f[a] = t - fl;
-    out |= c[a] < lo[a] || c[a] + (f[a] > T(0) ? 1 : 0) > lo[a] + n[a] - 1;
+    out |= c[a] < 0 || c[a] + (f[a] > T(0) ? 1 : 0) > n[a] - 1;
   }
   return out;
+}
+
+// 4^3 (DIM 3) or 4^2 stencil of f around local cell c: s[x + 4y + 16z] =
+// f[c - 1 + (x, y, z)], clamped to the grid.
+template <typename T, int DIM>
+__device__ __forceinline__ void gather_stencil(const Geom &g, const T *__restrict__ f, const int c[3], T *s) {
+  const int x0 = c[0] - 1, y0 = c[1] - 1, z0 = DIM == 3 ? c[2] - 1 : 0;
+  const int sy = g.nx, sz = g.nx * g.ny;
+  const bool inside = x0 >= 0 && y0 >= 0 && x0 + 3 < g.nx && y0 + 3 < g.ny && (DIM == 2 || (z0 >= 0 && z0 + 3 < g.nz));
+  if (inside) {
+    const T *p = f + ((z0 * g.ny + y0) * g.nx + x0);
+#pragma unroll
+    for (int z = 0; z < (DIM == 3 ? 4 : 1); ++z)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) {
+        const T *r = p + z * sz + y * sy;
+#pragma unroll
+        for (int x = 0; x < 4; ++x) s[x + 4 * y + 16 * z] = __ldg(r + x);
+      }
+  } else {
+    int xi[4], yo[4], zo[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      xi[i] = clampi(x0 + i, 0, g.nx - 1);
+      yo[i] = clampi(y0 + i, 0, g.ny - 1) * sy;
+      zo[i] = DIM == 3 ? clampi(z0 + i, 0, g.nz - 1) * sz : 0;
+    }
+#pragma unroll
+    for (int z = 0; z < (DIM == 3 ? 4 : 1); ++z)
+#pragma unroll
+      for (int y = 0; y < 4; ++y)
+#pragma unroll
+        for (int x = 0; x < 4; ++x) s[x + 4 * y + 16 * z] = __ldg(f + zo[z] + yo[y] + xi[x]);
+  }
 }
 
 // Catmull-Rom (Keys a = -1/2) cubic, the 1-D factor of the reference's

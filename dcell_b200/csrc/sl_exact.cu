@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256) sl_linear_kernel(Geom g, const T *__restr
     clamped |= outside<T>(g, S);
     phi[gidx(g, x, y, z)] = DIM == 3 ? trilinear_ref<T>(g, phi0, S) : bilinear_ref<T>(g, phi0, S[0], S[1]);
   }
-  if (clamped) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);
+  if (clamped && band) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);  // dense grids: the edge is the domain boundary
 }
 
 // ---------------------------------------------------------------------------

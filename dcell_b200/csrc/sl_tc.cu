@@ -245,25 +245,22 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__
   const float dth[3] = {dt / (float)g.hx, dt / (float)g.hy, dt / (float)g.hz};
   const long long ntiles = (npts + kTile - 1) / kTile;
   uint32_t parity = 0;
-  bool clamped = false, timeout = false;
+  bool clamped = false, timeout = false, bad = false;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long long q = tile * kTile + threadIdx.x;
-    const bool valid = q < npts;
     int x = 0, y = 0, z = 0, cc[3] = {0, 0, 0};
+    bool valid = q < npts;
+    if (valid && !arrival_local(g, band, q, x, y, z)) {
+      valid = false;
+      bad = true;
+    }
     float f[3] = {0.f, 0.f, 0.f}, r = 0.f;
     uint32_t hi[32], lo[32];
     {
       float s[64];
       if (valid) {
-        arrival(g, band, q, x, y, z);
         clamped |= departure_cell<float, 3>(g, vel, dth, backtrace, x, y, z, cc, f);
-#pragma unroll
-        for (int zz = 0; zz < 4; ++zz)
-#pragma unroll
-          for (int yy = 0; yy < 4; ++yy)
-#pragma unroll
-            for (int xx = 0; xx < 4; ++xx)
-              s[xx + 4 * yy + 16 * zz] = phi0[gidx(g, cc[0] - 1 + xx, cc[1] - 1 + yy, cc[2] - 1 + zz)];
+        gather_stencil<float, 3>(g, phi0, cc, s);
         r = s[21];
 #pragma unroll
         for (int e = 0; e < 64; ++e) s[e] -= r;
@@ -279,9 +276,10 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__
       break;
     }
     parity ^= 1u;
-    if (valid) phi[gidx(g, x, y, z)] = horner3(a, f) + r;
+    if (valid) phi[(z * g.ny + y) * g.nx + x] = horner3(a, f) + r;
   }
-  if (clamped) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);
+  if (clamped && band) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);  // dense grids: the edge is the domain boundary
+  if (bad) raise_flag(flags, FLAG_BAD_BAND);
   if (timeout && threadIdx.x == 0) raise_flag(flags, FLAG_WAIT_TIMEOUT);
   fence_before();
   __syncthreads();

@@ -108,12 +108,20 @@ DCELL_API int dcell_version(void);
  * phi0, phi: dtype grids of n[0]*n[1]*n[2] values; vel: dtype, dof innermost;
  * band: int32 [nband][3] or NULL; dt is the step the velocity is multiplied
  * by (fold any scalar time factor of the field into it).  phi is written at
- * the updated points only.  flags (optional int on the device) receives
- * DCELL_FLAG_* bits.  DCELL_CUBIC_TC requires dtype F32 and a 3D grid. */
+ * the updated points only.  Samples outside the grid are clamped to it: for a
+ * dense step (band == NULL) that is the boundary condition (constant
+ * extrapolation at the domain edge); for a band step it means the band came
+ * too close to the grid edge (the reference would read out of bounds) and
+ * DCELL_FLAG_DEPARTURE_CLAMPED is raised.  Band entries outside the grid are
+ * skipped and raise DCELL_FLAG_BAD_BAND.  Grids are limited to
+ * 3 * points < 2^31.  flags (optional int on the device) receives
+ * DCELL_FLAG_* bits.  DCELL_CUBIC_TC requires dtype F32 and a 3D
+ * grid. */
 #define DCELL_FLAG_DEPARTURE_CLAMPED 1
 #define DCELL_FLAG_NONFINITE 2
 #define DCELL_FLAG_CAPACITY 4
 #define DCELL_FLAG_WAIT_TIMEOUT 8
+#define DCELL_FLAG_BAD_BAND 16
 DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
                   int nband, int interp, int backtrace, void *phi, int *flags, void *stream);
 

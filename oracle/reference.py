@@ -16,17 +16,18 @@ from . import NODE_W
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PATH = os.path.join(HERE, "_ref", "libdcell_ref.so")
-_L = None
+# the same reference sources linked with the B200 drop-in (make -C oracle dropin)
+DROPIN_PATH = os.path.join(HERE, "_ref", "libdcell_ref_b200.so")
+_LIBS = {}
 
 
-def available() -> bool:
-    return os.path.exists(PATH)
+def available(path=PATH) -> bool:
+    return os.path.exists(path)
 
 
-def lib():
-    global _L
-    if _L is None:
-        L = ctypes.CDLL(PATH)
+def lib(path=PATH):
+    if path not in _LIBS:
+        L = ctypes.CDLL(path)
         vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
         L.dref_ls_create.restype = vp
         L.dref_ls_create.argtypes = [d, d, d, i, i, i, i, i, i]
@@ -61,8 +62,8 @@ def lib():
         L.dref_ortho3d.argtypes = [vp, vp, vp]
         L.dref_ortho2d.argtypes = [vp, vp, vp]
         L.dref_tricubic_coefs.argtypes = [vp, vp]
-        _L = L
-    return _L
+        _LIBS[path] = L
+    return _LIBS[path]
 
 
 def _p(a):
@@ -72,12 +73,13 @@ def _p(a):
 class RefLevelSet:
     """A reference ``LevelSet`` (LevelSetMethod.h:10-26) driven from numpy."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, path=PATH):
         self.h = handle
         self._vel = None
+        self.L = lib(path)
 
     @classmethod
-    def create(cls, h, origin, shape):
+    def create(cls, h, origin, shape, path=PATH):
         """LevelSetCreate (LevelSet.c:6-37); shape (nz,ny,nx) or (ny,nx)."""
         if len(shape) == 2:
             ny, nx = shape
@@ -86,28 +88,28 @@ class RefLevelSet:
             nz, ny, nx = shape
         o = tuple(origin) + (0,) * (3 - len(origin))
         hh = np.broadcast_to(np.asarray(h, dtype=np.float64), (3,))
-        return cls(lib().dref_ls_create(*map(float, hh), *map(int, o), int(nx), int(ny), int(nz)))
+        return cls(lib(path).dref_ls_create(*map(float, hh), *map(int, o), int(nx), int(ny), int(nz)), path)
 
     @classmethod
-    def sphere(cls, h, center, r):
-        return cls(lib().dref_init_sphere(float(h), *map(float, center), float(r)))
+    def sphere(cls, h, center, r, path=PATH):
+        return cls(lib(path).dref_init_sphere(float(h), *map(float, center), float(r)), path)
 
     @classmethod
-    def circle(cls, h, center, r):
-        return cls(lib().dref_init_circle(float(h), *map(float, center), float(r)))
+    def circle(cls, h, center, r, path=PATH):
+        return cls(lib(path).dref_init_circle(float(h), *map(float, center), float(r)), path)
 
     def close(self):
         if self._vel:
-            lib().dref_vel_destroy(self._vel)
+            self.L.dref_vel_destroy(self._vel)
             self._vel = None
         if self.h:
-            lib().dref_ls_destroy(self.h)
+            self.L.dref_ls_destroy(self.h)
             self.h = None
 
     def geometry(self):
         p = (ctypes.c_int * 3)()
         n = (ctypes.c_int * 3)()
-        lib().dref_ls_geometry(self.h, p, n)
+        self.L.dref_ls_geometry(self.h, p, n)
         return tuple(p), tuple(n)
 
     @property
@@ -121,83 +123,83 @@ class RefLevelSet:
 
     def get_phi(self, which=0):
         out = np.zeros(self.shape)
-        lib().dref_ls_get_phi(self.h, _p(out), which)
+        self.L.dref_ls_get_phi(self.h, _p(out), which)
         return out
 
     def set_phi(self, phi, which=0):
         a = np.ascontiguousarray(phi, dtype=np.float64)
         assert a.shape == self.shape
-        assert lib().dref_ls_set_phi(self.h, _p(a), which) == 0
+        assert self.L.dref_ls_set_phi(self.h, _p(a), which) == 0
 
     def band(self):
-        nb = lib().dref_ls_band_length(self.h)
+        nb = self.L.dref_ls_band_length(self.h)
         out = np.zeros((nb, 3), dtype=np.int32)
-        lib().dref_ls_get_band(self.h, _p(out))
+        self.L.dref_ls_get_band(self.h, _p(out))
         return out
 
     def set_band(self, band):
         b = np.ascontiguousarray(band, dtype=np.int32).reshape(-1, 3)
-        assert lib().dref_ls_set_band(self.h, _p(b), b.shape[0]) == 0
+        assert self.L.dref_ls_set_band(self.h, _p(b), b.shape[0]) == 0
 
     def set_velocity(self, vel):
         if self._vel:
-            lib().dref_vel_destroy(self._vel)
+            self.L.dref_vel_destroy(self._vel)
         v = np.ascontiguousarray(vel, dtype=np.float64)
-        self._vel = lib().dref_vel_create(self.h, _p(v))
+        self._vel = self.L.dref_vel_create(self.h, _p(v))
 
     def param(self, which):
-        return lib().dref_ls_param(self.h, {"bandWidth": 0, "PHI_INF": 1, "CFLcount": 2,
+        return self.L.dref_ls_param(self.h, {"bandWidth": 0, "PHI_INF": 1, "CFLcount": 2,
                                             "AdvectCount": 3, "maxVel": 4}[which])
 
     def copy_phi_to_phi0(self):
-        assert lib().dref_copy_phi_to_phi0(self.h) == 0
+        assert self.L.dref_copy_phi_to_phi0(self.h) == 0
 
     def advect_sl(self, dt):
         """LevelSetAdvectSL (AdvectSL.c:6): phi[band] <- SL(phi0, vel, dt)."""
-        assert lib().dref_advect_sl(self.h, self._vel, float(dt)) == 0
+        assert self.L.dref_advect_sl(self.h, self._vel, float(dt)) == 0
 
     def rk2_half(self, dt):
-        assert lib().dref_rk2_half(self.h, self._vel, float(dt)) == 0
+        assert self.L.dref_rk2_half(self.h, self._vel, float(dt)) == 0
 
     def rk2_full(self, dt):
-        assert lib().dref_rk2_full(self.h, self._vel, float(dt)) == 0
+        assert self.L.dref_rk2_full(self.h, self._vel, float(dt)) == 0
 
     def advect_and_reinit(self, dt):
-        assert lib().dref_advect_and_reinit(self.h, self._vel, float(dt)) == 0
+        assert self.L.dref_advect_and_reinit(self.h, self._vel, float(dt)) == 0
 
     def cfl_increment(self, dt):
-        assert lib().dref_cfl_increment(self.h, self._vel, float(dt)) == 0
+        assert self.L.dref_cfl_increment(self.h, self._vel, float(dt)) == 0
 
     def max_velocity(self):
-        return lib().dref_max_velocity(self.h, self._vel)
+        return self.L.dref_max_velocity(self.h, self._vel)
 
     def update_irregular(self):
-        n = lib().dref_update_irregular(self.h)
+        n = self.L.dref_update_irregular(self.h)
         assert n >= 0
         return n
 
     def irregular_nodes(self, surface=True):
-        n = lib().dref_update_irregular(self.h)
+        n = self.L.dref_update_irregular(self.h)
         out = np.zeros((max(n, 1), NODE_W))
-        lib().dref_get_irregular(self.h, _p(out), 1 if surface else 0)
+        self.L.dref_get_irregular(self.h, _p(out), 1 if surface else 0)
         return out[:n]
 
     def nodes_no_update(self, n, surface=True):
         out = np.zeros((max(n, 1), NODE_W))
-        lib().dref_get_irregular(self.h, _p(out), 1 if surface else 0)
+        self.L.dref_get_irregular(self.h, _p(out), 1 if surface else 0)
         return out[:n]
 
     def reinitialize(self):
-        assert lib().dref_reinitialize(self.h) == 0
+        assert self.L.dref_reinitialize(self.h) == 0
 
     def sample(self, fn, X):
-        return np.array([lib().dref_sample(self.h, int(fn), *map(float, x)) for x in np.reshape(X, (-1, 3))])
+        return np.array([self.L.dref_sample(self.h, int(fn), *map(float, x)) for x in np.reshape(X, (-1, 3))])
 
     def interp_velocity(self, X):
         out = np.zeros(3)
         res = []
         for x in np.reshape(X, (-1, 3)):
-            lib().dref_interp_velocity(self._vel, *map(float, x), _p(out))
+            self.L.dref_interp_velocity(self._vel, *map(float, x), _p(out))
             res.append(out.copy())
         return np.array(res)
 

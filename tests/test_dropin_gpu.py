@@ -1,0 +1,89 @@
+"""The drop-in: the reference's own C host with dcell_b200/host/levelset_b200.c
+linked in place of its CPU LevelSetAdvectSL / LevelSetUpdateIrregularNodeList /
+LevelSet_MaxVelocity (oracle/_ref/libdcell_ref_b200.so, built by
+`make -C oracle dropin`), driven through the very same reference call
+sequence as the unmodified reference library.  FP64 linear is bit-identical.
+"""
+import numpy as np
+import pytest
+
+from oracle import reference as R
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (R.available() and R.available(R.DROPIN_PATH)),
+                                 reason="reference libraries (oracle/_ref) not built")]
+
+EXACT = [0, 1, 2, 3, 4, 5, 6, 7]
+
+
+def _pair(g, key="phi0"):
+    out = []
+    for path in (R.PATH, R.DROPIN_PATH):
+        ls = R.RefLevelSet.create(float(g["h"]), tuple(g["origin"]), g[key].shape, path=path)
+        ls.set_phi(g[key])
+        ls.set_band(g["band"])
+        ls.set_velocity(g["vel"])
+        out.append(ls)
+    return out
+
+
+@pytest.mark.parametrize("case", ["sl3d_linear", "sl2d_linear"])
+def test_dropin_advect_irregular_maxvel(golden, cuda, case):
+    g = golden(case)
+    ref, b200 = _pair(g)
+    for ls in (ref, b200):
+        ls.copy_phi_to_phi0()
+        ls.advect_sl(float(g["dt"]))
+    assert np.array_equal(ref.get_phi(), b200.get_phi())
+    assert np.array_equal(b200.get_phi(), g["phi"])
+    nr, nb = ref.irregular_nodes(surface=False), b200.irregular_nodes(surface=False)
+    assert nr.shape == nb.shape
+    assert np.array_equal(nr[:, EXACT], nb[:, EXACT])
+    assert np.abs(nr[:, 8:14] - nb[:, 8:14]).max() < 1e-11
+    face = nr[:, 3] != -1
+    assert np.array_equal(nr[face, 8:11], nb[face, 8:11])
+    assert ref.max_velocity() == b200.max_velocity() == float(g["maxvel"])
+    for ls in (ref, b200):
+        ls.cfl_increment(float(g["dt"]))
+    assert ref.param("CFLcount") == b200.param("CFLcount")
+    ref.close()
+    b200.close()
+
+
+def test_dropin_rk2_half_full(golden, cuda):
+    """AdvectRK2.c unchanged: its LevelSetAdvectSL / irregular-node calls land on the GPU."""
+    g = golden("sl3d_rk2")
+    ref, b200 = _pair(g)
+    dt = float(g["dt"])
+    for ls in (ref, b200):
+        ls.rk2_half(dt / 2)
+    assert np.array_equal(ref.get_phi(), b200.get_phi())
+    for ls in (ref, b200):
+        ls.set_velocity(g["vel_half"])
+        ls.rk2_full(dt)
+    assert np.array_equal(ref.get_phi(), b200.get_phi())
+    assert np.array_equal(b200.get_phi(), g["phi_full"])
+    ref.close()
+    b200.close()
+
+
+def test_dropin_advect_and_reinit_sequence(cuda):
+    """Reference initialiser + LevelSetAdvectAndReinit steps (CPU fast marching
+    in between, triggered by the reference's CFL threshold)."""
+    rng = np.random.default_rng(7)
+    h = 1.0 / 40
+    libs = [R.RefLevelSet.sphere(h, (0.5, 0.5, 0.5), 0.16, path=p) for p in (R.PATH, R.DROPIN_PATH)]
+    ref, b200 = libs
+    # the initialiser already ran the (GPU resp. CPU) irregular-node pass and FMM
+    assert ref.shape == b200.shape
+    assert np.abs(ref.get_phi() - b200.get_phi()).max() < 1e-11
+    vel = np.ascontiguousarray(rng.uniform(-1, 1, size=ref.shape + (3,)).astype(np.float32).astype(np.float64))
+    for ls in libs:
+        ls.set_velocity(vel)
+    for step in range(6):
+        for ls in libs:
+            ls.advect_and_reinit(0.45 * h)
+        assert ref.band().shape == b200.band().shape
+        assert np.abs(ref.get_phi() - b200.get_phi()).max() < 1e-9, step
+    ref.close()
+    b200.close()

@@ -150,15 +150,24 @@ def test_tc_gemm_layout(cuda):
 
 
 def test_departure_outside_grid_is_flagged(cuda):
+    """Band points whose departure leaves the grid raise the flag; a dense
+    step treats the grid edge as the domain boundary and does not."""
     N = 16
     phi = torch.zeros((N, N, N), dtype=torch.float32, device=cuda)
     vel = torch.full((N, N, N, 3), 4.0, dtype=torch.float32, device=cuda)
     flags = torch.zeros(1, dtype=torch.int32, device=cuda)
+    band = torch.tensor([[8, 8, 8], [2, 3, 2]], dtype=torch.int32, device=cuda)
+    inner = torch.tensor([[8, 8, 8]], dtype=torch.int32, device=cuda)
     for interp in ("linear", "cubic_plain", "cubic_tc"):
         flags.zero_()
+        L.sl_step(phi, vel, 1.0, 1.0, band=band, interp=interp, flags=flags)
+        torch.cuda.synchronize()
+        assert int(flags.item()) & _lib.FLAG_DEPARTURE_CLAMPED, interp
+        flags.zero_()
+        L.sl_step(phi, vel, 1.0, 1.0, band=inner, interp=interp, flags=flags)
         L.sl_step(phi, vel, 1.0, 1.0, interp=interp, flags=flags)
         torch.cuda.synchronize()
-        assert int(flags.item()) & _lib.FLAG_DEPARTURE_CLAMPED
+        assert int(flags.item()) == 0, interp
 
 
 def test_zero_velocity_is_identity(cuda):
