@@ -26,7 +26,6 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -63,50 +62,55 @@ def profiled_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """SM clock, power and clock-event (throttle) reasons sampled through NVML
+    every 5 ms while the timed region runs (reads only; changes nothing)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index):
-        self.index, self.rows, self.proc = index, [], None
+    def __init__(self, cuda_index):
+        self.cuda_index, self.samples, self.max_mhz, self.stop = cuda_index, [], None, threading.Event()
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as N
+            import torch
+            N.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            try:
+                self.h = N.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                self.h = N.nvmlDeviceGetHandleByIndex(self.cuda_index)
+            self.N = N
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(self.h, N.NVML_CLOCK_SM)
+            getr = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                N.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def run():
+                while not self.stop.is_set():
+                    try:
+                        self.samples.append((N.nvmlDeviceGetClockInfo(self.h, N.NVML_CLOCK_SM), getr(self.h),
+                                             N.nvmlDeviceGetPowerUsage(self.h) / 1000.0))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.005)
+            self.t = threading.Thread(target=run, daemon=True)
             self.t.start()
-        except OSError:
-            self.proc = None
+        except Exception:
+            self.N = None
         return self
 
-    def _read(self):
-        for ln in self.proc.stdout:
-            self.rows.append([c.strip() for c in ln.split(",")])
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self.stop.set()
+        if self.N is not None:
+            self.t.join(timeout=2)
 
     def summary(self):
-        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            if len(r) > 8:
-                for nm, v in zip(names, r[5:9]):
-                    if v.strip().lower() == "active":
-                        reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted({name for s in self.samples for bit, name in self.REASONS.items() if s[1] & bit})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "power_w_max": max((s[2] for s in self.samples), default=None), "samples": len(sm),
+                "source": "nvml, 5 ms period, during the timed region"}
 
 
 def workload(N, dev):
