@@ -82,6 +82,7 @@ def lib():
     L.dcell_irregular_nodes_scratch_bytes.argtypes = [i]
     L.dcell_irregular_nodes_scratch_bytes.restype = sz
     L.dcell_irregular_nodes.argtypes = [G, i, vp, vp, i, i, vp, i, vp, vp, sz, vp, vp]
+    L.dcell_irregular_nodes_noalloc.argtypes = [G, i, vp, vp, i, i, vp, i, vp, vp, vp]
     L.dcell_max_velocity.argtypes = [G, i, vp, vp, vp, i, vp, vp]
     L.dcell_volume_scratch_bytes.restype = sz
     L.dcell_volume.argtypes = [G, i, vp, d, vp, vp, sz, vp]
@@ -91,7 +92,8 @@ def lib():
     L.dcell_ls_update_irregular_nodes.argtypes = [vp, G, vp, vp, i, i, i, vp, i, vp]
     L.dcell_ls_max_velocity.argtypes = [vp, G, vp, vp, i, vp]
     L.dcell_tc_gemm_check.argtypes = [vp, vp, vp, vp]
-    for name in ("dcell_sl_step", "dcell_irregular_nodes", "dcell_max_velocity", "dcell_volume",
+    for name in ("dcell_sl_step", "dcell_irregular_nodes", "dcell_irregular_nodes_noalloc", "dcell_max_velocity",
+                 "dcell_volume",
                  "dcell_session_create", "dcell_session_destroy", "dcell_ls_advect_sl",
                  "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_tc_gemm_check"):
         getattr(L, name).restype = i

@@ -15,6 +15,7 @@
 #include "dcell_kernels.h"
 
 int launch_tc_gemm_check(const float *A, float *D, int *flags, cudaStream_t st);
+static_assert(DCELL_NOALLOC_MAX_BAND == kNoAllocMaxBand, "header and kernel limits differ");
 
 namespace {
 thread_local char g_err[1024] = "";
@@ -95,6 +96,20 @@ DCELL_API int dcell_irregular_nodes(const dcell_geom *g, int dtype, const void *
     FAIL(DCELL_ERR_ARG, "scratch must hold %zu bytes", irregular_scratch_bytes(nband));
   return launch_irregular(dcell::to_geom(g), dtype, phi, band, nband, with_surface, nodes, capacity, count, scratch,
                           flags, (cudaStream_t)stream);
+}
+
+DCELL_API int dcell_irregular_nodes_noalloc(const dcell_geom *g, int dtype, const void *phi, const int *band,
+                                            int nband, int with_surface, dcell_irregular_node *nodes, int capacity,
+                                            int *count, int *flags, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (nband > DCELL_NOALLOC_MAX_BAND)
+    FAIL(DCELL_ERR_ARG, "band of %d points exceeds the allocation-free maximum of %d", nband, DCELL_NOALLOC_MAX_BAND);
+  if (!phi || !count || nband < 0 || (nband > 0 && !band)) FAIL(DCELL_ERR_ARG, "phi, band and count are required");
+  if (capacity < 0 || (capacity > 0 && !nodes)) FAIL(DCELL_ERR_ARG, "invalid node buffer");
+  return launch_irregular_noalloc(dcell::to_geom(g), dtype, phi, band, nband, with_surface, nodes, capacity, count,
+                                  flags, (cudaStream_t)stream);
 }
 
 DCELL_API int dcell_max_velocity(const dcell_geom *g, int dtype, const void *vel, const dcell_irregular_node *nodes,

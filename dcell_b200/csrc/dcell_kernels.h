@@ -18,6 +18,13 @@ int launch_irregular(const dcell::Geom &g, int dtype, const void *phi, const int
                      dcell_irregular_node *nodes, int cap, int *count, void *scratch, int *flags, cudaStream_t st);
 int launch_max_velocity(const dcell::Geom &g, int dtype, const void *vel, const dcell_irregular_node *nodes,
                         const int *count, int cap, double *out, cudaStream_t st);
+// Allocation-free irregular-node pass: scratch in a static device array.
+constexpr int kNoAllocMaxBand = 1 << 20;
+constexpr int kNoAllocScratchInts = kNoAllocMaxBand + 1 + (kNoAllocMaxBand + 1023) / 1024 + 1;
+constexpr int kNoAllocMaxDevices = 64;
+int launch_irregular_noalloc(const dcell::Geom &g, int dtype, const void *phi, const int *band, int nband,
+                             int with_surface, dcell_irregular_node *nodes, int cap, int *count, int *flags,
+                             cudaStream_t st);
 size_t volume_scratch_bytes();
 int launch_volume(const dcell::Geom &g, int dtype, const void *phi, double eps, double *out, double *partial,
                   cudaStream_t st);

@@ -15,6 +15,8 @@
 //   volume kernels       smoothed-Heaviside volume, deterministic FP64 sum
 #include <math.h>
 
+#include <mutex>
+
 #include "dcell_common.cuh"
 #include "dcell_kernels.h"
 
@@ -928,4 +930,65 @@ int launch_volume(const Geom &g, int dtype, const void *phi, double eps, double 
     volume_partial_kernel<float><<<VOL_BLOCKS, VOL_THREADS, 0, st>>>((const float *)phi, n, eps, partial);
   volume_final_kernel<<<1, 32, 0, st>>>(partial, cell, out);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the irregular-node pass.
+//
+// The scan scratch of launch_irregular lives in this file-scope device array
+// instead of a caller buffer.  Every GPU that loads the library holds it
+// (about 4 MiB) until the process exits; all calls on a device share it, so
+// calls that overlap on the GPU race.  Every scratch entry is written before
+// it is read, so nothing needs clearing between calls.  The host cannot use
+// the array's name as a device address: its address is looked up once per
+// device with cudaGetSymbolAddress, on the first call made with that device
+// current.
+static_assert(kNoAllocScratchInts >= kNoAllocMaxBand + 1 + (kNoAllocMaxBand + SCAN_BLOCK - 1) / SCAN_BLOCK + 1,
+              "allocation-free scratch smaller than the scan layout of launch_irregular");
+static __device__ __align__(256) int g_irr_noalloc_scratch[kNoAllocScratchInts];
+
+namespace {
+std::mutex g_noalloc_mu;
+int *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+static int noalloc_scratch(int **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    dcell_set_error(DCELL_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+    return DCELL_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    dcell_set_error(DCELL_ERR_UNSUPPORTED, "device %d beyond the %d devices the allocation-free path tracks", dev,
+                    kNoAllocMaxDevices);
+    return DCELL_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_irr_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      dcell_set_error(DCELL_ERR_CUDA, "cudaGetSymbolAddress of the allocation-free scratch failed: %s",
+                      cudaGetErrorString(e));
+      return DCELL_ERR_CUDA;
+    }
+    g_noalloc_ptr[dev] = (int *)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return DCELL_OK;
+}
+
+int launch_irregular_noalloc(const Geom &g, int dtype, const void *phi, const int *band, int nband,
+                             int with_surface, dcell_irregular_node *nodes, int cap, int *count, int *flags,
+                             cudaStream_t st) {
+  if (nband > kNoAllocMaxBand) {
+    dcell_set_error(DCELL_ERR_ARG, "band of %d points exceeds the allocation-free maximum of %d", nband,
+                    kNoAllocMaxBand);
+    return DCELL_ERR_ARG;
+  }
+  int *scratch = nullptr;
+  const int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  return launch_irregular(g, dtype, phi, band, nband, with_surface, nodes, cap, count, scratch, flags, st);
 }

@@ -139,6 +139,27 @@ DCELL_API int dcell_irregular_nodes(const dcell_geom *g, int dtype, const void *
                           int with_surface, dcell_irregular_node *nodes, int capacity, int *count, void *scratch,
                           size_t scratch_bytes, int *flags, void *stream);
 
+/* Allocation-free variant of dcell_irregular_nodes.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory -- a
+ * host whose device memory is all owned by another runtime's allocator or a
+ * fixed-size pool, or one that must not call cudaMalloc because that call can
+ * synchronise the device and stall its other streams.  Same inputs, outputs
+ * and results as dcell_irregular_nodes, but it takes no scratch: the scan
+ * scratch lives in a static array of the library (about 4 MiB, held on every
+ * GPU that loads the library until the process exits).  Limits and rules:
+ *   - nband <= DCELL_NOALLOC_MAX_BAND, else DCELL_ERR_ARG and no work;
+ *   - the first call on a device (made with that device current) looks up the
+ *     array's device address; make that first call before any stream capture;
+ *   - all calls on a device share the array, so calls that overlap on the GPU
+ *     (different streams, or a second call before the first one finished)
+ *     race; serialise them;
+ *   - it allocates nothing (no cudaMalloc, cudaFree or allocating library
+ *     call).  The caller still provides nodes, count and flags. */
+#define DCELL_NOALLOC_MAX_BAND (1 << 20)
+DCELL_API int dcell_irregular_nodes_noalloc(const dcell_geom *g, int dtype, const void *phi, const int *band,
+                                            int nband, int with_surface, dcell_irregular_node *nodes, int capacity,
+                                            int *count, int *flags, void *stream);
+
 /* max |V| over the integer positions of the irregular nodes
  * (LevelSet_MaxVelocity, LevelSetMethod/Advect.c:70-111).  count and maxvel
  * are device pointers; *maxvel is overwritten. */
