@@ -30,6 +30,7 @@ UNITS = {
     "sl_exact.cu": ["-fmad=false"],
     "sl_cubic.cu": [],
     "sl_tc.cu": [],
+    "sl_adjoint.cu": [],
     "capi.cu": [],
 }
 

@@ -82,6 +82,21 @@ DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, co
   return launch_sl_cubic(G, dtype, phi0, vel, dt, band, npts, interp, backtrace, phi, flags, st);
 }
 
+DCELL_API int dcell_sl_adjoint(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt,
+                               int interp, int backtrace, const void *grad_phi, void *grad_phi0, void *grad_vel,
+                               void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (g->n[2] < 2) FAIL(DCELL_ERR_UNSUPPORTED, "the adjoint step is 3D only");
+  if (interp < DCELL_LINEAR || interp > DCELL_CUBIC_TC) FAIL(DCELL_ERR_ARG, "unknown interpolation %d", interp);
+  if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+  if (!phi0 || !vel || !grad_phi || !grad_phi0 || !grad_vel) FAIL(DCELL_ERR_ARG, "all arrays are required");
+  if (!(dt == dt)) FAIL(DCELL_ERR_NONFINITE, "dt is NaN");
+  return launch_sl_adjoint(dcell::to_geom(g), dtype, phi0, vel, dt, interp, backtrace, grad_phi, grad_phi0, grad_vel,
+                           (cudaStream_t)stream);
+}
+
 DCELL_API size_t dcell_irregular_nodes_scratch_bytes(int nband) { return irregular_scratch_bytes(nband < 0 ? 0 : nband); }
 
 DCELL_API int dcell_irregular_nodes(const dcell_geom *g, int dtype, const void *phi, const int *band, int nband,
@@ -133,6 +148,49 @@ DCELL_API int dcell_volume(const dcell_geom *g, int dtype, const void *phi, doub
   if (!scratch || scratch_bytes < volume_scratch_bytes())
     FAIL(DCELL_ERR_ARG, "scratch must hold %zu bytes", volume_scratch_bytes());
   return launch_volume(dcell::to_geom(g), dtype, phi, eps, volume, (double *)scratch, (cudaStream_t)stream);
+}
+
+DCELL_API int dcell_batch_plan(const dcell_cell *cells, int ncells, int tx, int ty, int tz, dcell_tile *tiles,
+                               int capacity, int *ntiles) {
+  if (!cells || ncells < 0 || !ntiles || capacity < 0 || (capacity > 0 && !tiles))
+    FAIL(DCELL_ERR_ARG, "cells, tiles and ntiles are required");
+  if (tx < 1 || ty < 1 || tz < 1) FAIL(DCELL_ERR_ARG, "tile extents must be positive");
+  long long k = 0;
+  for (int c = 0; c < ncells; ++c) {
+    const dcell_cell &C = cells[c];
+    if (C.n[0] < 1 || C.n[1] < 1 || C.n[2] < 1 || C.offset < 0) FAIL(DCELL_ERR_ARG, "cell %d has an empty grid", c);
+    if (3LL * C.n[0] * C.n[1] * C.n[2] >= (1LL << 31)) FAIL(DCELL_ERR_ARG, "cell %d grid too large", c);
+    for (int z = 0; z < C.n[2]; z += tz)
+      for (int y = 0; y < C.n[1]; y += ty)
+        for (int x = 0; x < C.n[0]; x += tx) {
+          if (k < capacity) tiles[k] = dcell_tile{c, x, y, z};
+          ++k;
+        }
+  }
+  if (k > (1LL << 31) - 1) FAIL(DCELL_ERR_ARG, "too many tiles");
+  *ntiles = (int)k;
+  if (k > capacity) FAIL(DCELL_ERR_CAPACITY, "the plan needs %lld tiles, capacity %d", k, capacity);
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_batch_sl_step(const dcell_cell *cells, int ncells, const dcell_tile *tiles, int ntiles, int tx,
+                                  int ty, int tz, int ctas_per_sm, const float *phi0, const float *vel, float *phi,
+                                  int interp, int backtrace, int *flags, void *stream) {
+  if (!cells || ncells < 0 || ntiles < 0 || (ntiles > 0 && !tiles)) FAIL(DCELL_ERR_ARG, "cells and tiles are required");
+  if (!phi0 || !vel || !phi) FAIL(DCELL_ERR_ARG, "phi0, vel and phi must be device pointers");
+  if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+  if (tx < 1 || ty < 1 || tz < 1) FAIL(DCELL_ERR_ARG, "tile extents must be positive");
+  const int threads = tx * ty * tz;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (interp == DCELL_CUBIC_TC) {
+    if (threads != 128) FAIL(DCELL_ERR_ARG, "DCELL_CUBIC_TC tiles must hold 128 points (got %d)", threads);
+    return launch_batch_tc(cells, tiles, ntiles, tx, ty, ctas_per_sm, phi0, vel, backtrace, phi, flags, st);
+  }
+  if (interp != DCELL_LINEAR && interp != DCELL_CUBIC_PLAIN && interp != DCELL_CUBIC_SEPARABLE)
+    FAIL(DCELL_ERR_ARG, "unknown interpolation %d", interp);
+  if (threads < 32 || threads > 1024) FAIL(DCELL_ERR_ARG, "tiles must hold 32..1024 points (got %d)", threads);
+  return launch_batch_cuda_core(cells, tiles, ntiles, tx, ty, tz, ctas_per_sm, phi0, vel, interp, backtrace, phi,
+                                flags, st);
 }
 
 DCELL_API int dcell_tc_gemm_check(const float *a, float *d, int *flags, void *stream) {

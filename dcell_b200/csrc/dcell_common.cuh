@@ -14,10 +14,32 @@
 
 namespace dcell {
 
+// Unsigned 32-bit division by an invariant divisor d >= 1 (multiply-high and
+// shifts, Granlund-Montgomery / Hacker's Delight 10-8): n / d for all n < 2^32.
+struct FastDiv {
+  uint32_t m, s1, s2;
+};
+
+static inline FastDiv make_fastdiv(uint32_t d) {
+  uint32_t l = 0;
+  while ((1ull << l) < d) ++l;
+  FastDiv f;
+  f.m = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+  f.s1 = l < 1 ? l : 1;
+  f.s2 = l > 1 ? l - 1 : 0;
+  return f;
+}
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f) {
+  const uint32_t t = __umulhi(f.m, n);
+  return (t + ((n - t) >> f.s1)) >> f.s2;
+}
+
 struct Geom {
   int nx, ny, nz;
   int px, py, pz;
   double hx, hy, hz;
+  FastDiv div_nx, div_nxny;  // dense-index decode
 };
 
 static inline Geom to_geom(const dcell_geom *g) {
@@ -25,6 +47,8 @@ static inline Geom to_geom(const dcell_geom *g) {
   r.nx = g->n[0]; r.ny = g->n[1]; r.nz = g->n[2] < 1 ? 1 : g->n[2];
   r.px = g->p[0]; r.py = g->p[1]; r.pz = r.nz == 1 ? 0 : g->p[2];
   r.hx = g->h[0]; r.hy = g->h[1]; r.hz = g->h[2];
+  r.div_nx = make_fastdiv((uint32_t)r.nx);
+  r.div_nxny = make_fastdiv((uint32_t)r.nx * (uint32_t)r.ny);
   return r;
 }
 
@@ -70,10 +94,11 @@ __device__ __forceinline__ bool arrival_local(const Geom &g, const int *__restri
     z = g.nz == 1 ? 0 : band[3 * q + 2] - g.pz;
     return (unsigned)x < (unsigned)g.nx && (unsigned)y < (unsigned)g.ny && (unsigned)z < (unsigned)g.nz;
   }
-  const int n = (int)q;
-  x = n % g.nx;
-  y = (n / g.nx) % g.ny;
-  z = n / (g.nx * g.ny);
+  const uint32_t n = (uint32_t)q, zq = fdiv(n, g.div_nxny), rem = n - zq * (uint32_t)(g.nx * g.ny);
+  const uint32_t yq = fdiv(rem, g.div_nx);
+  x = (int)(rem - yq * (uint32_t)g.nx);
+  y = (int)yq;
+  z = (int)zq;
   return true;
 }
 

@@ -13,6 +13,15 @@ int launch_sl_cubic(const dcell::Geom &g, int dtype, const void *phi0, const voi
 int launch_sl_tc(const dcell::Geom &g, const float *phi0, const float *vel, double dt, const int *band,
                  long long npts, int backtrace, float *phi, int *flags, cudaStream_t st);
 
+int launch_batch_tc(const dcell_cell *cells, const dcell_tile *tiles, int ntiles, int tx, int ty, int ctas_per_sm,
+                    const float *phi0, const float *vel, int backtrace, float *phi, int *flags, cudaStream_t st);
+int launch_batch_cuda_core(const dcell_cell *cells, const dcell_tile *tiles, int ntiles, int tx, int ty, int tz,
+                           int ctas_per_sm, const float *phi0, const float *vel, int interp, int backtrace, float *phi,
+                           int *flags, cudaStream_t st);
+
+int launch_sl_adjoint(const dcell::Geom &g, int dtype, const void *phi0, const void *vel, double dt, int interp,
+                      int backtrace, const void *gphi, void *gphi0, void *gvel, cudaStream_t st);
+
 size_t irregular_scratch_bytes(int nband);
 int launch_irregular(const dcell::Geom &g, int dtype, const void *phi, const int *band, int nband, int with_surface,
                      dcell_irregular_node *nodes, int cap, int *count, void *scratch, int *flags, cudaStream_t st);

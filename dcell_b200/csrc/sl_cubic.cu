@@ -118,6 +118,49 @@ __global__ void __launch_bounds__(256) sl_cubic_kernel(Geom g, const T *__restri
   if (bad) raise_flag(flags, FLAG_BAD_BAND);
 }
 
+// Trilinear sample on the production gather (batched linear mode).
+template <typename T>
+__device__ __forceinline__ T trilinear_fast(const Geom &g, const T *__restrict__ f, const int c[3], const T fr[3]) {
+  T s[64];  // s[21] holds cell c itself (stencil origin c - 1)
+  gather_stencil<T, 3>(g, f, c, s);
+  const T x0 = 1 - fr[0], y0 = 1 - fr[1], z0 = 1 - fr[2];
+  const T a = (x0 * s[21] + fr[0] * s[22]) * y0 + (x0 * s[25] + fr[0] * s[26]) * fr[1];
+  const T b = (x0 * s[37] + fr[0] * s[38]) * y0 + (x0 * s[41] + fr[0] * s[42]) * fr[1];
+  return a * z0 + b * fr[2];
+}
+
+// Batched cells on CUDA cores: one thread per point of a tile, a persistent
+// grid walking the packed tile queue (see dcell_batch_sl_step).
+template <int MODE>
+__global__ void __launch_bounds__(1024) batch_cubic_kernel(const dcell_cell *__restrict__ cells,
+                                                           const dcell_tile *__restrict__ tiles, int ntiles, int tx,
+                                                           int ty, const float *__restrict__ phi0,
+                                                           const float *__restrict__ vel, int backtrace,
+                                                           float *__restrict__ phi) {
+  const int lx = threadIdx.x % tx, ly = (threadIdx.x / tx) % ty, lz = threadIdx.x / (tx * ty);
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const dcell_tile T = tiles[t];
+    const dcell_cell C = cells[T.cell];
+    Geom g;
+    g.nx = C.n[0]; g.ny = C.n[1]; g.nz = C.n[2];
+    g.px = g.py = g.pz = 0;
+    g.hx = C.h[0]; g.hy = C.h[1]; g.hz = C.h[2];
+    const int x = T.x0 + lx, y = T.y0 + ly, z = T.z0 + lz;
+    if (x >= g.nx || y >= g.ny || z >= g.nz) continue;
+    const float dtf = (float)C.dt;  // same rounding as the single-grid kernels
+    const float dth[3] = {dtf / (float)C.h[0], dtf / (float)C.h[1], dtf / (float)C.h[2]};
+    const float *p0 = phi0 + C.offset;
+    int c[3];
+    float f[3];
+    departure_cell<float, 3>(g, vel + 3 * C.offset, dth, backtrace, x, y, z, c, f);
+    float out;
+    if (MODE == DCELL_CUBIC_SEPARABLE) out = cubic_separable<float, 3>(g, p0, c, f);
+    else if (MODE == DCELL_CUBIC_PLAIN) out = cubic_plain<float, 3>(g, p0, c, f);
+    else out = trilinear_fast<float>(g, p0, c, f);
+    phi[C.offset + (z * g.ny + y) * g.nx + x] = out;
+  }
+}
+
 // FP64 <-> FP32 conversion and band gathers for the host-buffer entry points.
 template <typename S, typename D>
 __global__ void convert_kernel(const S *__restrict__ src, D *__restrict__ dst, long long n) {
@@ -185,5 +228,28 @@ int launch_gather_band(const Geom &g, int dtype, const void *phi, const int *ban
     gather_band_kernel<double><<<(nband + 255) / 256, 256, 0, st>>>(g, (const double *)phi, band, nband, (double *)out);
   else
     gather_band_kernel<float><<<(nband + 255) / 256, 256, 0, st>>>(g, (const float *)phi, band, nband, (float *)out);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_batch_cuda_core(const dcell_cell *cells, const dcell_tile *tiles, int ntiles, int tx, int ty, int tz,
+                           int ctas_per_sm, const float *phi0, const float *vel, int interp, int backtrace, float *phi,
+                           int *flags, cudaStream_t st) {
+  (void)flags;
+  if (ntiles <= 0) return DCELL_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int threads = tx * ty * tz;
+  const int per = ctas_per_sm < 1 ? 1 : (ctas_per_sm > 8 ? 8 : ctas_per_sm);
+  const int grid = per * sms < ntiles ? per * sms : ntiles;
+  if (interp == DCELL_CUBIC_SEPARABLE)
+    batch_cubic_kernel<DCELL_CUBIC_SEPARABLE><<<grid, threads, 0, st>>>(cells, tiles, ntiles, tx, ty, phi0, vel,
+                                                                       backtrace, phi);
+  else if (interp == DCELL_CUBIC_PLAIN)
+    batch_cubic_kernel<DCELL_CUBIC_PLAIN><<<grid, threads, 0, st>>>(cells, tiles, ntiles, tx, ty, phi0, vel,
+                                                                   backtrace, phi);
+  else
+    batch_cubic_kernel<DCELL_LINEAR><<<grid, threads, 0, st>>>(cells, tiles, ntiles, tx, ty, phi0, vel, backtrace,
+                                                              phi);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }

@@ -203,7 +203,8 @@ __device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t p
     }
     mma_commit(bar);
   }
-  const bool ok = mbar_wait(bar, parity);
+  // only the issuing thread polls the mbarrier; the others sleep in the barrier
+  const bool ok = threadIdx.x == 0 ? mbar_wait(bar, parity) : true;
   const int all_ok = __syncthreads_and(ok ? 1 : 0);
   if (!all_ok) return false;
   fence_after();
@@ -231,6 +232,27 @@ __device__ __forceinline__ float horner3(const float *a, const float f[3]) {
   return pz;
 }
 
+// Per-point front half: backtrace, stencil gather, centring, hi/lo split.
+// Invalid lanes contribute a zero A row.
+__device__ __forceinline__ void tc_prepare(const Geom &g, const float *__restrict__ phi0,
+                                           const float *__restrict__ vel, const float dth[3], int backtrace,
+                                           bool valid, int x, int y, int z, float f[3], float &r, uint32_t *hi,
+                                           uint32_t *lo, bool &clamped) {
+  float s[64];
+  if (valid) {
+    int cc[3];
+    clamped |= departure_cell<float, 3>(g, vel, dth, backtrace, x, y, z, cc, f);
+    gather_stencil<float, 3>(g, phi0, cc, s);
+    r = s[21];
+#pragma unroll
+    for (int e = 0; e < 64; ++e) s[e] -= r;
+  } else {
+#pragma unroll
+    for (int e = 0; e < 64; ++e) s[e] = 0.f;
+  }
+  split_bf16(s, hi, lo);
+}
+
 __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__restrict__ phi0,
                                                          const float *__restrict__ vel, float dt,
                                                          const int *__restrict__ band, long long npts, int backtrace,
@@ -248,7 +270,7 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__
   bool clamped = false, timeout = false, bad = false;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long long q = tile * kTile + threadIdx.x;
-    int x = 0, y = 0, z = 0, cc[3] = {0, 0, 0};
+    int x = 0, y = 0, z = 0;
     bool valid = q < npts;
     if (valid && !arrival_local(g, band, q, x, y, z)) {
       valid = false;
@@ -256,20 +278,7 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__
     }
     float f[3] = {0.f, 0.f, 0.f}, r = 0.f;
     uint32_t hi[32], lo[32];
-    {
-      float s[64];
-      if (valid) {
-        clamped |= departure_cell<float, 3>(g, vel, dth, backtrace, x, y, z, cc, f);
-        gather_stencil<float, 3>(g, phi0, cc, s);
-        r = s[21];
-#pragma unroll
-        for (int e = 0; e < 64; ++e) s[e] -= r;
-      } else {
-#pragma unroll
-        for (int e = 0; e < 64; ++e) s[e] = 0.f;
-      }
-      split_bf16(s, hi, lo);
-    }
+    tc_prepare(g, phi0, vel, dth, backtrace, valid, x, y, z, f, r, hi, lo, clamped);
     float a[64];
     if (!mma_tile(c, bar, parity, hi, lo, a)) {
       timeout = true;
@@ -280,6 +289,52 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__
   }
   if (clamped && band) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);  // dense grids: the edge is the domain boundary
   if (bad) raise_flag(flags, FLAG_BAD_BAND);
+  if (timeout && threadIdx.x == 0) raise_flag(flags, FLAG_WAIT_TIMEOUT);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if ((threadIdx.x >> 5) == 0) tmem_dealloc(c.tmem, kTmemCols);
+}
+
+// Batched cells: a persistent CTA walks a packed queue of 128-point tiles
+// (tx x ty x tz boxes of one cell's grid) over many uneven cell grids.
+__global__ void __launch_bounds__(kTile, 4) batch_tc_kernel(const dcell_cell *__restrict__ cells,
+                                                            const dcell_tile *__restrict__ tiles, int ntiles, int tx,
+                                                            int ty, const float *__restrict__ phi0,
+                                                            const float *__restrict__ vel, int backtrace,
+                                                            float *__restrict__ phi, int *flags) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sB = smem;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kBBytes);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kBBytes + 8);
+  Ctx c;
+  setup(sB, bar, tmem_slot, c);
+  const int lx = threadIdx.x % tx, ly = (threadIdx.x / tx) % ty, lz = threadIdx.x / (tx * ty);
+  uint32_t parity = 0;
+  bool clamped = false, timeout = false;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const dcell_tile T = tiles[t];
+    const dcell_cell C = cells[T.cell];
+    Geom g;
+    g.nx = C.n[0]; g.ny = C.n[1]; g.nz = C.n[2];
+    g.px = g.py = g.pz = 0;
+    g.hx = C.h[0]; g.hy = C.h[1]; g.hz = C.h[2];
+    const float dtf = (float)C.dt;  // same rounding as the single-grid kernels
+    const float dth[3] = {dtf / (float)C.h[0], dtf / (float)C.h[1], dtf / (float)C.h[2]};
+    const int x = T.x0 + lx, y = T.y0 + ly, z = T.z0 + lz;
+    const bool valid = x < g.nx && y < g.ny && z < g.nz;
+    float f[3] = {0.f, 0.f, 0.f}, r = 0.f;
+    uint32_t hi[32], lo[32];
+    tc_prepare(g, phi0 + C.offset, vel + 3 * C.offset, dth, backtrace, valid, x, y, z, f, r, hi, lo, clamped);
+    float a[64];
+    if (!mma_tile(c, bar, parity, hi, lo, a)) {
+      timeout = true;
+      break;
+    }
+    parity ^= 1u;
+    if (valid) phi[C.offset + (z * g.ny + y) * g.nx + x] = horner3(a, f) + r;
+  }
+  (void)clamped;  // dense cells: the grid edge is the cell's domain boundary
   if (timeout && threadIdx.x == 0) raise_flag(flags, FLAG_WAIT_TIMEOUT);
   fence_before();
   __syncthreads();
@@ -346,6 +401,25 @@ int launch_sl_tc(const Geom &g, const float *phi0, const float *vel, double dt, 
   if (npts <= 0) return DCELL_OK;
   tc::sl_tc_kernel<<<tc_grid(npts), tc::kTile, tc::kDynSmem, st>>>(g, phi0, vel, (float)dt, band, npts, backtrace,
                                                                    phi, flags);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_batch_tc(const dcell_cell *cells, const dcell_tile *tiles, int ntiles, int tx, int ty, int ctas_per_sm,
+                    const float *phi0, const float *vel, int backtrace, float *phi, int *flags, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    DCELL_CUDA_CHECK(
+        cudaFuncSetAttribute(tc::batch_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kDynSmem));
+    configured = true;
+  }
+  if (ntiles <= 0) return DCELL_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int per = ctas_per_sm < 1 ? 1 : (ctas_per_sm > 4 ? 4 : ctas_per_sm);
+  const int grid = per * sms < ntiles ? per * sms : ntiles;
+  tc::batch_tc_kernel<<<grid, tc::kTile, tc::kDynSmem, st>>>(cells, tiles, ntiles, tx, ty, phi0, vel, backtrace, phi,
+                                                            flags);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 

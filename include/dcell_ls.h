@@ -125,6 +125,18 @@ DCELL_API int dcell_version(void);
 DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
                   int nband, int interp, int backtrace, void *phi, int *flags, void *stream);
 
+/* Adjoint of one dense 3D SL step (dcell_sl_step with band == NULL): given
+ * grad_phi = dL/dphi, ACCUMULATES dL/dphi0 into grad_phi0 and dL/dvel into
+ * grad_vel (same layouts as phi0 / vel; zero them first for a fresh
+ * gradient).  The transpose of the interpolation weights is scattered with
+ * global atomics; the velocity sensitivity goes through the departure point
+ * (and, for DCELL_MIDPOINT, through the midpoint).  interp DCELL_LINEAR or
+ * any cubic mode (they share one interpolant).  No counterpart in the
+ * reference, which has no derivatives. */
+DCELL_API int dcell_sl_adjoint(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt,
+                               int interp, int backtrace, const void *grad_phi, void *grad_phi0, void *grad_vel,
+                               void *stream);
+
 /* Irregular-node pass over the band: replaces LevelSetUpdateIrregularNodeList
  * (LevelSetMethod/IrregularNodes.c:9-141, IrregularNodes3D.c:6-117) including
  * OrthogonalProjection2D/3D (OrthogonalProjection*.c).  Nodes are written in
@@ -174,6 +186,48 @@ DCELL_API int dcell_max_velocity(const dcell_geom *g, int dtype, const void *vel
 DCELL_API size_t dcell_volume_scratch_bytes(void);
 DCELL_API int dcell_volume(const dcell_geom *g, int dtype, const void *phi, double eps, double *volume, void *scratch,
                  size_t scratch_bytes, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Batched cells: many DCells' level sets of uneven sizes in one launch
+ * (the reference advances them one after another per rank,
+ * DWorld/DCellsArray.c:50-102).
+ * ---------------------------------------------------------------------- */
+
+/* One cell of a packed batch.  Its phi occupies elements
+ * [offset, offset + n0*n1*n2) of the packed phi arrays (x fastest) and its
+ * MAC velocity elements [3*offset, 3*(offset + n0*n1*n2)) of the packed
+ * velocity array.  The grid edge is the cell's domain boundary (samples
+ * outside are clamped).  dt is this cell's step. */
+typedef struct dcell_cell {
+  long long offset;
+  int n[3];
+  int pad;
+  double h[3];
+  double dt;
+} dcell_cell;
+
+/* A tile: the box [x0, x0+tx) x [y0, y0+ty) x [z0, z0+tz) of cell `cell`,
+ * clipped to the cell's grid. */
+typedef struct dcell_tile {
+  int cell;
+  int x0, y0, z0;
+} dcell_tile;
+
+/* Host-only: cover every point of every cell by tiles of tx*ty*tz points,
+ * cell by cell, z, y, x.  *ntiles receives the number needed even when it
+ * exceeds capacity (then DCELL_ERR_CAPACITY). */
+DCELL_API int dcell_batch_plan(const dcell_cell *cells, int ncells, int tx, int ty, int tz, dcell_tile *tiles,
+                               int capacity, int *ntiles);
+
+/* One SL step of every cell of the batch in ONE persistent launch over the
+ * tile queue (device arrays cells, tiles; FP32 phi0/vel/phi packed as
+ * above).  interp: DCELL_CUBIC_TC needs tx*ty*tz == 128; the CUDA-core
+ * modes need tx*ty*tz in [32, 1024].  ctas_per_sm (1..4 for TC, 1..8
+ * otherwise) sets the persistent grid; it and the tile shape are what the
+ * autotuner of dcell_b200.batch chooses. */
+DCELL_API int dcell_batch_sl_step(const dcell_cell *cells, int ncells, const dcell_tile *tiles, int ntiles, int tx,
+                                  int ty, int tz, int ctas_per_sm, const float *phi0, const float *vel, float *phi,
+                                  int interp, int backtrace, int *flags, void *stream);
 
 /* ------------------------------------------------------------------------
  * Host-buffer drop-in entry points (reference FP64 layout)

@@ -1,0 +1,95 @@
+"""Hand-written SL adjoint vs FP64 central differences and vs the FP64
+adjoint (the FP64 reference gradient), through torch.autograd."""
+import numpy as np
+import pytest
+import torch
+
+from dcell_b200 import fields
+from dcell_b200.autograd import FourierVelocity, c5_loss, sl_adjoint, transport
+from dcell_b200.levelset import sl_step
+
+pytestmark = pytest.mark.gpu
+
+
+def _dot(a, b):
+    return float((a.double() * b.double()).sum())
+
+
+@pytest.mark.parametrize("interp", ["linear", "cubic_separable"])
+@pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
+def test_single_step_adjoint_identity(cuda, interp, backtrace):
+    """<SL'(phi0) dphi + SL_vel dvel, gbar> == <dphi, gphi0> + <dvel, gvel> (FP64, tiny steps)."""
+    N = 24
+    h = 1.0 / N
+    torch.manual_seed(0)
+    phi0 = fields.sphere_sdf(N, center=(0.5, 0.5, 0.5), r=0.25, device=cuda)
+    k, a, ph = fields.fourier_modes(4, 11)
+    vel = fields.fourier_velocity((N, N, N), np.full(4, 0.05), (k, a, ph), device=cuda)
+    dt = 0.3 * h
+    gbar = torch.randn_like(phi0)
+    gphi0, gvel = torch.zeros_like(phi0), torch.zeros_like(vel)
+    sl_adjoint(phi0, vel, dt, h, gbar, gphi0, gvel, interp, backtrace)
+    dphi, dvel = torch.randn_like(phi0), torch.randn_like(vel) * 0.05
+    for eps in (1e-4,):
+        fp = sl_step(phi0 + eps * dphi, vel + eps * dvel, dt, h, interp=interp, backtrace=backtrace)
+        fm = sl_step(phi0 - eps * dphi, vel - eps * dvel, dt, h, interp=interp, backtrace=backtrace)
+        lhs = _dot((fp - fm) / (2 * eps), gbar)
+        rhs = _dot(dphi, gphi0) + _dot(dvel, gvel)
+        assert abs(lhs - rhs) <= 1e-6 * max(abs(lhs), 1.0), (lhs, rhs)
+
+
+def _c5(N, nsteps, dtype, cuda):
+    h = 1.0 / N
+    model = FourierVelocity((N, N, N), nmodes=16, seed=5, device=cuda, dtype=dtype)
+    phi0 = fields.sphere_sdf(N, center=(0.5, 0.5, 0.5), r=0.2, device=cuda).to(dtype)
+    with torch.no_grad():
+        c_tg = torch.as_tensor(np.random.default_rng(9).normal(size=16), dtype=dtype, device=cuda)
+        v_tg = model(c_tg)
+        vmax = max(float(model(torch.ones(16, dtype=dtype, device=cuda))[..., d].abs().max()) for d in range(3))
+        dt = 0.5 * h / max(vmax, float(v_tg.abs().max()))
+        dts = [dt] * nsteps
+        target = transport(phi0, v_tg, dts, h, "cubic_separable", "midpoint", 4)
+    return h, model, phi0, target, dts
+
+
+def test_gradient_matches_central_differences_fp64(cuda):
+    """dL/dc (16 Fourier coefficients) by the adjoint vs FP64 central differences (delta 1e-3)."""
+    N, K = 40, 12
+    h, model, phi0, target, dts = _c5(N, K, torch.float64, cuda)
+    loss = c5_loss(transport(phi0, model(), dts, h, "cubic_separable", "midpoint", 4), target, h)
+    loss.backward()
+    grad = model.coeffs.grad.detach().clone()
+    fd = torch.zeros_like(grad)
+    with torch.no_grad():
+        for m in range(16):
+            e = torch.zeros_like(grad)
+            e[m] = 1e-3
+            lp = c5_loss(transport(phi0, model(model.coeffs + e), dts, h, "cubic_separable", "midpoint", 4), target, h)
+            lm = c5_loss(transport(phi0, model(model.coeffs - e), dts, h, "cubic_separable", "midpoint", 4), target, h)
+            fd[m] = (lp - lm) / 2e-3
+    rel = float((grad - fd).norm() / fd.norm())
+    assert rel < 1e-4, (rel, grad.cpu().numpy(), fd.cpu().numpy())
+
+
+def test_fp32_gradient_matches_fp64_reference_gradient(cuda):
+    N, K = 40, 12
+    grads = {}
+    for dtype in (torch.float64, torch.float32):
+        h, model, phi0, target, dts = _c5(N, K, dtype, cuda)
+        loss = c5_loss(transport(phi0, model(), dts, h, "cubic_separable", "midpoint", 5), target, h)
+        loss.backward()
+        grads[dtype] = model.coeffs.grad.double()
+    rel = float((grads[torch.float32] - grads[torch.float64]).norm() / grads[torch.float64].norm())
+    assert rel < 1e-3, rel
+
+
+def test_checkpoint_interval_does_not_change_gradient(cuda):
+    N, K = 32, 10
+    out = []
+    for every in (1, 3, 10):
+        h, model, phi0, target, dts = _c5(N, K, torch.float64, cuda)
+        loss = c5_loss(transport(phi0, model(), dts, h, "cubic_separable", "midpoint", every), target, h)
+        loss.backward()
+        out.append(model.coeffs.grad.detach().clone())
+    assert torch.allclose(out[0], out[1], rtol=1e-9, atol=1e-12)
+    assert torch.allclose(out[0], out[2], rtol=1e-9, atol=1e-12)
