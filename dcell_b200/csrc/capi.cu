@@ -82,6 +82,29 @@ DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, co
   return launch_sl_cubic(G, dtype, phi0, vel, dt, band, npts, interp, backtrace, phi, flags, st);
 }
 
+DCELL_API int dcell_split_bf16(const dcell_geom *g, const float *phi, unsigned int *split, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (!phi || !split) FAIL(DCELL_ERR_ARG, "phi and split are required");
+  return launch_split_bf16(phi, split, grid_points(g), (cudaStream_t)stream);
+}
+
+DCELL_API int dcell_sl_step_tc_split(const dcell_geom *g, const unsigned int *phi0_split, const float *vel, double dt,
+                                     const int *band, int nband, int backtrace, float *phi, unsigned int *phi_split,
+                                     int *flags, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (g->n[2] < 2) FAIL(DCELL_ERR_UNSUPPORTED, "the tensor-core step is 3D only");
+  if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+  if (!phi0_split || !vel || !phi) FAIL(DCELL_ERR_ARG, "phi0_split, vel and phi must be device pointers");
+  if (band && nband < 0) FAIL(DCELL_ERR_ARG, "nband must be >= 0");
+  if (!(dt == dt)) FAIL(DCELL_ERR_NONFINITE, "dt is NaN");
+  const long long npts = band ? (long long)nband : grid_points(g);
+  if (npts == 0) return DCELL_OK;
+  return launch_sl_tc_split(dcell::to_geom(g), phi0_split, vel, dt, band, npts, backtrace, phi, phi_split, flags,
+                            (cudaStream_t)stream);
+}
+
 DCELL_API int dcell_sl_adjoint(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt,
                                int interp, int backtrace, const void *grad_phi, void *grad_phi0, void *grad_vel,
                                void *stream) {

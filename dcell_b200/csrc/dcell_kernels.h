@@ -13,6 +13,9 @@ int launch_sl_cubic(const dcell::Geom &g, int dtype, const void *phi0, const voi
 int launch_sl_tc(const dcell::Geom &g, const float *phi0, const float *vel, double dt, const int *band,
                  long long npts, int backtrace, float *phi, int *flags, cudaStream_t st);
 
+int launch_split_bf16(const float *phi, uint32_t *out, long long n, cudaStream_t st);
+int launch_sl_tc_split(const dcell::Geom &g, const uint32_t *phi0s, const float *vel, double dt, const int *band,
+                       long long npts, int backtrace, float *phi, uint32_t *phis, int *flags, cudaStream_t st);
 int launch_batch_tc(const dcell_cell *cells, const dcell_tile *tiles, int ntiles, int tx, int ty, int ctas_per_sm,
                     const float *phi0, const float *vel, int backtrace, float *phi, int *flags, cudaStream_t st);
 int launch_batch_cuda_core(const dcell_cell *cells, const dcell_tile *tiles, int ntiles, int tx, int ty, int tz,

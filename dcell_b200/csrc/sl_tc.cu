@@ -296,6 +296,94 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__
   if ((threadIdx.x >> 5) == 0) tmem_dealloc(c.tmem, kTmemCols);
 }
 
+// ---------------------------------------------------------------------------
+// Split-state variant.  The level set is carried as FP32 *and* as its packed
+// BF16 split (one 32-bit word per point: hi = RN_bf16(phi) in the low half,
+// lo = RN_bf16(phi - hi) in the high half), written by the step that produces
+// phi.  A step then gathers the 64 packed words of each stencil and forms the
+// A row's TMEM columns with one byte-permute per column -- no per-entry
+// subtraction or conversion.  M (hi + lo) = M phi to ~2^-17 relative.
+__device__ __forceinline__ uint32_t pack_split(float v) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+  return (uint32_t)__bfloat16_as_ushort(h) | ((uint32_t)__bfloat16_as_ushort(l) << 16);
+}
+
+__global__ void __launch_bounds__(256) split_kernel(const float *__restrict__ phi, uint32_t *__restrict__ out,
+                                                    long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    out[q] = pack_split(phi[q]);
+}
+
+__device__ __forceinline__ void tc_prepare_split(const Geom &g, const uint32_t *__restrict__ w,
+                                                 const float *__restrict__ vel, const float dth[3], int backtrace,
+                                                 bool valid, int x, int y, int z, float f[3], uint32_t *hi,
+                                                 uint32_t *lo, bool &clamped) {
+  if (valid) {
+    int cc[3];
+    uint32_t s[64];
+    clamped |= departure_cell<float, 3>(g, vel, dth, backtrace, x, y, z, cc, f);
+    gather_stencil<uint32_t, 3>(g, w, cc, s);
+#pragma unroll
+    for (int e = 0; e < 32; ++e) {
+      hi[e] = __byte_perm(s[2 * e], s[2 * e + 1], 0x5410);  // (hi_2e, hi_2e+1)
+      lo[e] = __byte_perm(s[2 * e], s[2 * e + 1], 0x7632);  // (lo_2e, lo_2e+1)
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < 32; ++e) hi[e] = lo[e] = 0u;
+  }
+}
+
+__global__ void __launch_bounds__(kTile, 4) sl_tc_split_kernel(Geom g, const uint32_t *__restrict__ phi0s,
+                                                               const float *__restrict__ vel, float dt,
+                                                               const int *__restrict__ band, long long npts,
+                                                               int backtrace, float *__restrict__ phi,
+                                                               uint32_t *__restrict__ phis, int *flags) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sB = smem;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kBBytes);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kBBytes + 8);
+  Ctx c;
+  setup(sB, bar, tmem_slot, c);
+
+  const float dth[3] = {dt / (float)g.hx, dt / (float)g.hy, dt / (float)g.hz};
+  const long long ntiles = (npts + kTile - 1) / kTile;
+  uint32_t parity = 0;
+  bool clamped = false, timeout = false, bad = false;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long q = tile * kTile + threadIdx.x;
+    int x = 0, y = 0, z = 0;
+    bool valid = q < npts;
+    if (valid && !arrival_local(g, band, q, x, y, z)) {
+      valid = false;
+      bad = true;
+    }
+    float f[3] = {0.f, 0.f, 0.f};
+    uint32_t hi[32], lo[32];
+    tc_prepare_split(g, phi0s, vel, dth, backtrace, valid, x, y, z, f, hi, lo, clamped);
+    float a[64];
+    if (!mma_tile(c, bar, parity, hi, lo, a)) {
+      timeout = true;
+      break;
+    }
+    parity ^= 1u;
+    if (valid) {
+      const int p = (z * g.ny + y) * g.nx + x;
+      const float v = horner3(a, f);
+      phi[p] = v;
+      if (phis) phis[p] = pack_split(v);
+    }
+  }
+  if (clamped && band) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);  // dense grids: the edge is the domain boundary
+  if (bad) raise_flag(flags, FLAG_BAD_BAND);
+  if (timeout && threadIdx.x == 0) raise_flag(flags, FLAG_WAIT_TIMEOUT);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if ((threadIdx.x >> 5) == 0) tmem_dealloc(c.tmem, kTmemCols);
+}
+
 // Batched cells: a persistent CTA walks a packed queue of 128-point tiles
 // (tx x ty x tz boxes of one cell's grid) over many uneven cell grids.
 __global__ void __launch_bounds__(kTile, 4) batch_tc_kernel(const dcell_cell *__restrict__ cells,
@@ -420,6 +508,27 @@ int launch_batch_tc(const dcell_cell *cells, const dcell_tile *tiles, int ntiles
   const int grid = per * sms < ntiles ? per * sms : ntiles;
   tc::batch_tc_kernel<<<grid, tc::kTile, tc::kDynSmem, st>>>(cells, tiles, ntiles, tx, ty, phi0, vel, backtrace, phi,
                                                             flags);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_split_bf16(const float *phi, uint32_t *out, long long n, cudaStream_t st) {
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148LL * 32) blocks = 148LL * 32;
+  if (n > 0) tc::split_kernel<<<(int)(blocks < 1 ? 1 : blocks), 256, 0, st>>>(phi, out, n);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_sl_tc_split(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, const int *band,
+                       long long npts, int backtrace, float *phi, uint32_t *phis, int *flags, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    DCELL_CUDA_CHECK(
+        cudaFuncSetAttribute(tc::sl_tc_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kDynSmem));
+    configured = true;
+  }
+  if (npts <= 0) return DCELL_OK;
+  tc::sl_tc_split_kernel<<<tc_grid(npts), tc::kTile, tc::kDynSmem, st>>>(g, phi0s, vel, (float)dt, band, npts,
+                                                                         backtrace, phi, phis, flags);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 

@@ -83,6 +83,34 @@ def sl_step(phi0: torch.Tensor, vel: torch.Tensor, dt: float, h, origin=(0, 0, 0
     return out
 
 
+def split_bf16(phi: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Packed BF16 hi/lo split of an FP32 grid (int32 words, see dcell_split_bf16)."""
+    _require_cuda(phi, out)
+    if phi.dtype != torch.float32:
+        raise DcellError(_lib.ERR_ARG, "split_bf16 takes an FP32 grid")
+    out = torch.empty(phi.shape, dtype=torch.int32, device=phi.device) if out is None else out
+    g = geom(phi.shape, 1.0)
+    check(lib().dcell_split_bf16(ctypes.byref(g), _ptr(phi), _ptr(out), _stream()))
+    return out
+
+
+def sl_step_tc_split(phi0_split: torch.Tensor, vel: torch.Tensor, dt: float, h, origin=(0, 0, 0), band=None,
+                     backtrace="midpoint", out: Optional[torch.Tensor] = None,
+                     out_split: Optional[torch.Tensor] = None, flags: Optional[torch.Tensor] = None):
+    """Tensor-core step on a split-state level set; returns (phi, phi_split)."""
+    _require_cuda(phi0_split, vel, band, out, out_split, flags)
+    if phi0_split.dtype != torch.int32 or vel.dtype != torch.float32 or phi0_split.dim() != 3:
+        raise DcellError(_lib.ERR_ARG, "phi0_split (int32 3D) and an FP32 velocity are required")
+    if out is None:
+        out = torch.empty(phi0_split.shape, dtype=torch.float32, device=phi0_split.device)
+    g = geom(phi0_split.shape, h, origin)
+    nb = int(band.shape[0]) if band is not None else 0
+    check(lib().dcell_sl_step_tc_split(ctypes.byref(g), _ptr(phi0_split), _ptr(vel), float(dt), _ptr(band), nb,
+                                       BACKTRACE[backtrace] if isinstance(backtrace, str) else int(backtrace),
+                                       _ptr(out), _ptr(out_split), _ptr(flags), _stream()))
+    return out, out_split
+
+
 def nodes_to_numpy(raw: torch.Tensor, count: int) -> np.ndarray:
     """Device node buffer (uint8, 120 B/node) -> numpy structured array."""
     n = int(count)

@@ -125,6 +125,20 @@ DCELL_API int dcell_version(void);
 DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
                   int nband, int interp, int backtrace, void *phi, int *flags, void *stream);
 
+/* Split-BF16 state of an FP32 grid: split[i] holds bf16 hi = RN(phi[i]) in
+ * its low 16 bits and bf16 lo = RN(phi[i] - hi) in its high 16 bits. */
+DCELL_API int dcell_split_bf16(const dcell_geom *g, const float *phi, unsigned int *split, void *stream);
+
+/* DCELL_CUBIC_TC step on a split-state level set: the stencil operands come
+ * from phi0_split (as made by dcell_split_bf16 or by a previous step), so the
+ * kernel forms the tensor-core A rows with byte permutes instead of per-entry
+ * conversions.  Writes phi (FP32) and, when phi_split != NULL, its split --
+ * the next step's input.  Same interpolant, backtrace, band and flag rules as
+ * dcell_sl_step; 3D only. */
+DCELL_API int dcell_sl_step_tc_split(const dcell_geom *g, const unsigned int *phi0_split, const float *vel, double dt,
+                                     const int *band, int nband, int backtrace, float *phi, unsigned int *phi_split,
+                                     int *flags, void *stream);
+
 /* Adjoint of one dense 3D SL step (dcell_sl_step with band == NULL): given
  * grad_phi = dL/dphi, ACCUMULATES dL/dphi0 into grad_phi0 and dL/dvel into
  * grad_vel (same layouts as phi0 / vel; zero them first for a fresh

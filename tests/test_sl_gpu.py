@@ -190,3 +190,50 @@ def test_integer_shift_is_exact_translation(cuda):
         out = L.sl_step(phi, vel, 1.0 / N, 1.0 / N, interp=interp)
         tol = 0 if interp != "cubic_tc" else 1e-7
         assert float((out[:, :, 1:] - phi[:, :, :-1]).abs().max()) <= tol, interp
+
+
+def test_split_bf16_words(cuda):
+    x = torch.randn(4, 8, 16, device=cuda) * torch.logspace(-6, 2, 16, device=cuda)
+    w = L.split_bf16(x.contiguous())
+    u = w.view(torch.int32).cpu().numpy().astype(np.uint32)
+    hi = (u & 0xFFFF).astype(np.uint32) << 16
+    lo = (u >> 16).astype(np.uint32) << 16
+    v = hi.view(np.float32).astype(np.float64) + lo.view(np.float32).astype(np.float64)
+    ref = x.double().cpu().numpy()
+    assert np.all(np.abs(v - ref) <= 2.0 ** -16 * np.abs(ref))
+
+
+@pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
+def test_tc_split_state_error_budget(cuda, backtrace):
+    """Split-state TC step: <= 1e-5 in the |phi| < 3h band vs the FP64 oracle."""
+    N = 64
+    h, phi, vel, dt = _sphere_case(N, cuda)
+    ref = L.sl_step(phi, vel, dt, h, interp="cubic_plain", backtrace=backtrace)
+    p32, v32 = phi.float().contiguous(), vel.float().contiguous()
+    out, spl = L.sl_step_tc_split(L.split_bf16(p32), v32, dt, h, backtrace=backtrace,
+                                  out_split=torch.empty((N, N, N), dtype=torch.int32, device=cuda))
+    band = ref.abs() < 3 * h
+    err = (out.double() - ref).abs()
+    assert float(err[band].max()) <= 1e-5, float(err[band].max())
+    assert float(err.max()) <= 1e-4, float(err.max())
+    assert torch.equal(spl, L.split_bf16(out))  # the written split is the next step's input
+
+
+def test_tc_split_band_mode_and_multistep(cuda):
+    N = 48
+    h, phi, vel, dt = _sphere_case(N, cuda)
+    p32, v32 = phi.float().contiguous(), vel.float().contiguous()
+    band = fields.band_of(phi, 6 * h).to(cuda)
+    dense, _ = L.sl_step_tc_split(L.split_bf16(p32), v32, dt, h)
+    banded, _ = L.sl_step_tc_split(L.split_bf16(p32), v32, dt, h, band=band, out=p32.clone())
+    sel = torch.zeros_like(phi, dtype=torch.bool)
+    sel[band[:, 2].long(), band[:, 1].long(), band[:, 0].long()] = True
+    assert torch.equal(banded[sel], dense[sel])
+    # 10 steps split-state vs 10 FP64 steps
+    a, s = p32, L.split_bf16(p32)
+    ref = phi.clone()
+    for k in range(10):
+        a, s = L.sl_step_tc_split(s, v32, dt, h, out_split=torch.empty_like(s))
+        ref = L.sl_step(ref, vel, dt, h, interp="cubic_plain", backtrace="midpoint")
+    err = (a.double() - ref).abs()[ref.abs() < 3 * h]
+    assert float(err.max()) <= 1e-5, float(err.max())
