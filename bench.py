@@ -51,7 +51,7 @@ def peaks():
 
 def profiled_traffic():
     """DRAM bytes per launch of the TC kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "sl_tc_kernel_256.md")
+    path = os.path.join(ROOT, "profiles", "sl_tc_kernel_256.md")  # ncu capture summary
     try:
         for ln in open(path):
             if ln.startswith("dram_bytes_per_launch_256:"):

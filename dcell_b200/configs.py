@@ -1,0 +1,247 @@
+"""The five benchmark configurations of the transport path, run end to end.
+
+    python -m dcell_b200.configs [c1|c2|c3|c4|c5|all] [--out results.json]
+
+Each runner returns a JSON-able dict with the errors (max and L2 of phi in
+the |phi| < 3h band, enclosed-volume error) and timings it measured.  Every
+field is synthetic (formulas and seeds; no dataset exists for this path):
+
+c1  2D Zalesak slotted disk, 256^2, rigid rotation, one revolution, CFL 0.5,
+    midpoint backtrace, bicubic: FP32 GPU vs the exact answer (the initial
+    disk) and vs an FP64 GPU run; plus the reference's own linear CPU
+    AdvectSL (oracle/_ref, when present) vs the FP32 GPU linear kernel on the
+    same inputs.
+c2  3D sphere in LeVeque's time-reversing deformation, 128^3, T=3, CFL 0.5,
+    tricubic, midpoint: FP32 vs FP64 oracle; volume loss and max phi error
+    after the return at t = T.
+c3  the same field at 256^3: split-BF16 tensor-core vs plain FP32 vs the FP64
+    oracle over a window of steps, per-step volume error.
+c4  512 cells, edges U{32..96} (seeded), ellipsoids in 8-mode divergence-free
+    Fourier velocities, 20 steps: one persistent CUDA-graph launch per step
+    with autotuned tiles vs one launch per cell.
+c5  128^3, 50 midpoint steps, velocity from 16 learnable Fourier
+    coefficients, loss sum (H_eps(phi_T) - H_eps(phi_target))^2: hand-written
+    adjoint (checkpoints every 10) vs FP64 central differences (delta 1e-3)
+    and vs the FP64 adjoint.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import fields
+from . import levelset as L
+
+
+def _band_err(out, ref, h):
+    band = ref.abs() < 3 * h
+    e = (out.double() - ref.double()).abs()[band]
+    return {"max": float(e.max()), "l2": float(e.pow(2).mean().sqrt()), "band_points": int(band.sum())}
+
+
+def _events():
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_c1(N=256, dev="cuda"):
+    h = 1.0 / N
+    phi0 = fields.slotted_disk_sdf(N, device=dev)
+    vel = fields.rotation_velocity_2d(N, device=dev)
+    steps = int(math.ceil(2 * math.pi / h))  # one revolution at CFL 0.5 (max |u| = pi)
+    dt = 1.0 / steps
+    out = {"grid": [N, N], "steps": steps, "dt": dt}
+    for name, dtype in (("fp32", torch.float32), ("fp64", torch.float64)):
+        a = phi0.to(dtype).contiguous()
+        v = vel.to(dtype).contiguous()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(steps):
+            a = L.sl_step(a, v, dt, h, interp="cubic_plain", backtrace="midpoint")
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"bicubic_{name}"] = {"vs_exact": _band_err(a, phi0, h), "ms": e0.elapsed_time(e1),
+                                  "area_rel_err": abs(float(L.volume(a, h, 1.5 * h)) -
+                                                      float(L.volume(phi0, h, 1.5 * h))) /
+                                  float(L.volume(phi0, h, 1.5 * h))}
+        out[f"_final_{name}"] = a
+    out["bicubic_fp32_vs_fp64"] = _band_err(out.pop("_final_fp32"), out.pop("_final_fp64"), h)
+    # the reference's own CPU AdvectSL (linear, Euler, FP64) vs the FP32 GPU linear kernel, 50 steps
+    try:
+        from oracle import reference as R
+        if R.available():
+            band = fields.band_of(phi0, 6 * h)
+            ls = R.RefLevelSet.create(h, (0, 0), (N, N))
+            p = phi0.cpu().numpy()
+            ls.set_phi(p)
+            ls.set_band(band.cpu().numpy())
+            ls.set_velocity(vel.cpu().numpy())
+            a = phi0.float().contiguous()
+            v = vel.float().contiguous()
+            b = band.to(dev)
+            t0 = time.perf_counter()
+            for _ in range(50):
+                ls.copy_phi_to_phi0()
+                ls.advect_sl(dt)
+            t_ref = time.perf_counter() - t0
+            for _ in range(50):
+                a = L.sl_step(a, v, dt, h, band=b, out=a.clone())
+            ref = torch.as_tensor(ls.get_phi(), device=dev)
+            ls.close()
+            out["reference_cpu_linear_vs_gpu_fp32_linear_50_steps"] = {
+                **_band_err(a, ref, h), "reference_cpu_s": t_ref, "band_points_per_step": int(band.shape[0])}
+    except Exception as exc:  # pragma: no cover - informational
+        out["reference_cpu_linear_vs_gpu_fp32_linear_50_steps"] = {"skipped": str(exc)}
+    return out
+
+
+def _deformation(N, dev):
+    h = 1.0 / N
+    return h, fields.sphere_sdf(N, device=dev), fields.deformation_velocity(N, device=dev)
+
+
+def run_c2(N=128, dev="cuda", T=3.0):
+    h, phi0, vel = _deformation(N, dev)
+    dt0 = fields.cfl_dt((2.0, 1.0, 1.0), h)
+    steps = int(math.ceil(T / dt0))
+    dt = T / steps
+    res = {"grid": [N] * 3, "steps": steps, "dt": dt}
+    finals = {}
+    for name, dtype, interp in (("fp32_plain", torch.float32, "cubic_plain"),
+                                ("fp32_tc", torch.float32, "cubic_tc"),
+                                ("fp64_oracle", torch.float64, "cubic_plain")):
+        a = phi0.to(dtype).contiguous()
+        v = vel.to(dtype).contiguous()
+        e0, e1 = _events()
+        e0.record()
+        for s in range(steps):
+            fac = math.cos(math.pi * (s + 0.5) * dt / T)
+            a = L.sl_step(a, v, dt * fac, h, interp=interp, backtrace="midpoint")
+        e1.record()
+        torch.cuda.synchronize()
+        v0 = float(L.volume(phi0, h, 1.5 * h))
+        res[name] = {"return_error_vs_initial": _band_err(a, phi0, h), "ms": e0.elapsed_time(e1),
+                     "volume_loss_rel": (v0 - float(L.volume(a, h, 1.5 * h))) / v0}
+        finals[name] = a
+    res["fp32_plain_vs_fp64_oracle"] = _band_err(finals["fp32_plain"], finals["fp64_oracle"], h)
+    res["fp32_tc_vs_fp64_oracle"] = _band_err(finals["fp32_tc"], finals["fp64_oracle"], h)
+    return res
+
+
+def run_c3(N=256, dev="cuda", window=20):
+    h, phi0, vel = _deformation(N, dev)
+    dt = fields.cfl_dt((2.0, 1.0, 1.0), h)
+    T = 3.0
+    a64, v64 = phi0.contiguous(), vel.contiguous()
+    v32 = vel.float().contiguous()
+    tc, s = phi0.float().contiguous(), L.split_bf16(phi0.float().contiguous())
+    pl = phi0.float().contiguous()
+    per_step = []
+    for k in range(window):
+        d = dt * math.cos(math.pi * (k + 0.5) * dt / T)
+        a64 = L.sl_step(a64, v64, d, h, interp="cubic_plain", backtrace="midpoint")
+        tc, s = L.sl_step_tc_split(s, v32, d, h, backtrace="midpoint", out_split=torch.empty_like(s))
+        pl = L.sl_step(pl, v32, d, h, interp="cubic_plain", backtrace="midpoint")
+        v_ref = float(L.volume(a64, h, 1.5 * h))
+        per_step.append({"step": k + 1, "tc": _band_err(tc, a64, h), "plain_fp32": _band_err(pl, a64, h),
+                         "volume_rel_err_tc": abs(float(L.volume(tc, h, 1.5 * h)) - v_ref) / v_ref})
+    worst = max(p["tc"]["max"] for p in per_step)
+    return {"grid": [N] * 3, "window_steps": window, "tc_max_band_err_worst_step": worst,
+            "tc_meets_1e-5": worst <= 1e-5, "per_step": per_step}
+
+
+def run_c4(dev="cuda", ncells=512, steps=20):
+    from .batch import CellBatch, c4_workload
+    phis, vels, hs, dt = c4_workload(ncells=ncells, device=dev)
+    b = CellBatch(phis, vels, hs, dt, device=dev)
+    res = {"cells": ncells, "points_per_step": b.npoints, "steps": steps, "dt": dt}
+    for interp in ("cubic_tc", "cubic_separable"):
+        (tile, ctas), table = b.autotune(interp, "midpoint", reps=2)
+        g, (a, _, outbuf) = b.capture(steps, interp, "midpoint")
+        g.replay()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ms_graph = e0.elapsed_time(e1)
+        x, y = b.phi.clone(), torch.empty_like(b.phi)
+        b.step_per_cell(x, y, interp, "midpoint")
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(steps):
+            b.step_per_cell(x, y, interp, "midpoint")
+            x, y = y, x
+        e1.record()
+        torch.cuda.synchronize()
+        ms_cells = e0.elapsed_time(e1)
+        res[interp] = {"tile": list(tile), "ctas_per_sm": ctas, "graph_ms": ms_graph, "per_cell_launch_ms": ms_cells,
+                       "speedup": ms_cells / ms_graph, "updates_per_s": b.npoints * steps / (ms_graph / 1e3),
+                       "autotune_top3": [[t[0], list(t[1]), t[2]] for t in table[:3]]}
+    return res
+
+
+def run_c5(N=128, steps=50, every=10, dev="cuda", fd_modes=16):
+    from .autograd import FourierVelocity, c5_loss, transport
+    h = 1.0 / N
+    res = {"grid": [N] * 3, "steps": steps, "checkpoint_every": every}
+    grads = {}
+    for dtype in (torch.float64, torch.float32):
+        model = FourierVelocity((N, N, N), nmodes=16, seed=5, device=dev, dtype=dtype)
+        phi0 = fields.sphere_sdf(N, center=(0.5, 0.5, 0.5), r=0.2, device=dev).to(dtype)
+        with torch.no_grad():
+            c_tg = torch.as_tensor(np.random.default_rng(9).normal(size=16), dtype=dtype, device=dev)
+            v_tg = model(c_tg)
+            vmax = max(float(model()[..., d].abs().max()) for d in range(3))
+            dt = 0.5 * h / max(vmax, float(v_tg.abs().max()))
+            dts = [dt] * steps
+            target = transport(phi0, v_tg, dts, h, "cubic_separable", "midpoint", every)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss = c5_loss(transport(phi0, model(), dts, h, "cubic_separable", "midpoint", every), target, h)
+        loss.backward()
+        torch.cuda.synchronize()
+        grads[dtype] = model.coeffs.grad.double().clone()
+        res[f"loss_{str(dtype)[6:]}"] = float(loss)
+        res[f"forward_backward_s_{str(dtype)[6:]}"] = time.perf_counter() - t0
+        if dtype == torch.float64:
+            fd = torch.zeros(16, dtype=torch.float64, device=dev)
+            with torch.no_grad():
+                for m in range(fd_modes):
+                    e = torch.zeros(16, dtype=dtype, device=dev)
+                    e[m] = 1e-3
+                    lp = c5_loss(transport(phi0, model(model.coeffs + e), dts, h, "cubic_separable", "midpoint",
+                                           every), target, h)
+                    lm = c5_loss(transport(phi0, model(model.coeffs - e), dts, h, "cubic_separable", "midpoint",
+                                           every), target, h)
+                    fd[m] = (lp - lm) / 2e-3
+            sel = slice(0, fd_modes)
+            res["fp64_adjoint_vs_fd_rel"] = float((grads[dtype][sel] - fd[sel]).norm() / fd[sel].norm())
+    res["fp32_adjoint_vs_fp64_adjoint_rel"] = float((grads[torch.float32] - grads[torch.float64]).norm() /
+                                                   grads[torch.float64].norm())
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("which", nargs="?", default="all")
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    todo = ["c1", "c2", "c3", "c4", "c5"] if a.which == "all" else a.which.split(",")
+    results = {}
+    for c in todo:
+        t0 = time.time()
+        results[c] = globals()[f"run_{c}"]()
+        results[c]["wall_s"] = time.time() - t0
+        print(json.dumps({c: results[c]}, default=float), flush=True)
+    if a.out:
+        json.dump(results, open(a.out, "w"), indent=1, default=float)
+
+
+if __name__ == "__main__":
+    main()
