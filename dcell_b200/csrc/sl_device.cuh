@@ -15,6 +15,36 @@ namespace dcell {
 // >= 2^31.  Gathers take LOCAL indices (origin subtracted) and clamp only on
 // the slow path, when a stencil touches the grid edge.
 
+// Explicitly rounded arithmetic for the velocity interpolation, so every code
+// path that interpolates the MAC field (global gathers, staged bricks,
+// adjoint recomputation) produces the same bits whatever the compiler's
+// contraction choices.
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+template <typename T>
+__device__ __forceinline__ T face_mean(T a, T b) {
+  return rfma(T(0.5), a, rmul(T(0.5), b));
+}
+
+// bilinear in (x, y) of v[yx] with fractions s0, s1
+template <typename T>
+__device__ __forceinline__ T bilerp(T v00, T v10, T v01, T v11, T s0, T s1) {
+  const T w0 = T(1) - s0;
+  const T a = rfma(w0, v00, rmul(s0, v10));
+  const T b = rfma(w0, v01, rmul(s0, v11));
+  return rfma(a, T(1) - s1, rmul(b, s1));
+}
+
+template <typename T>
+__device__ __forceinline__ T trilerp(T v000, T v100, T v010, T v110, T v001, T v101, T v011, T v111, const T s[3]) {
+  const T bot = bilerp(v000, v100, v010, v110, s[0], s[1]);
+  const T top = bilerp(v001, v101, v011, v111, s[0], s[1]);
+  return rfma(bot, T(1) - s[2], rmul(top, s[2]));
+}
+
 // MAC velocity at local node (x, y, z): each component is the mean of its two
 // faces around the node -- InterpolateVelocity3D/2D
 // (Common/InterpolateVelocity.c:35-67) at an integer point, where the
@@ -24,11 +54,11 @@ __device__ __forceinline__ void mac_vel_node(const Geom &g, const T *__restrict_
   const int q = (z * g.ny + y) * g.nx + x;
   const T *c = vel + DIM * q;
   const int dx = x + 1 < g.nx ? DIM : 0, dy = y + 1 < g.ny ? DIM * g.nx : 0;
-  V[0] = T(0.5) * __ldg(c) + T(0.5) * __ldg(c + dx);
-  V[1] = T(0.5) * __ldg(c + 1) + T(0.5) * __ldg(c + dy + 1);
+  V[0] = face_mean(__ldg(c), __ldg(c + dx));
+  V[1] = face_mean(__ldg(c + 1), __ldg(c + dy + 1));
   if (DIM == 3) {
     const int dz = z + 1 < g.nz ? 3 * g.nx * g.ny : 0;
-    V[2] = T(0.5) * __ldg(c + 2) + T(0.5) * __ldg(c + dz + 2);
+    V[2] = face_mean(__ldg(c + 2), __ldg(c + dz + 2));
   } else {
     V[2] = T(0);
   }
@@ -61,16 +91,13 @@ __device__ __forceinline__ void mac_vel_rel(const Geom &g, const T *__restrict__
       o[a] = up * (a == 0 ? DIM : a == 1 ? DIM * g.nx : DIM * g.nx * g.ny);
     }
     const T *c = vel + DIM * ((bc[2] * g.ny + bc[1]) * g.nx + bc[0]) + d;
-    const T wx0 = 1 - s[0], wy0 = 1 - s[1];
-    T sum = (wx0 * __ldg(c) + s[0] * __ldg(c + o[0])) * wy0 +
-            (wx0 * __ldg(c + o[1]) + s[0] * __ldg(c + o[1] + o[0])) * s[1];
     if (DIM == 3) {
       const T *c2 = c + o[2];
-      const T top = (wx0 * __ldg(c2) + s[0] * __ldg(c2 + o[0])) * wy0 +
-                    (wx0 * __ldg(c2 + o[1]) + s[0] * __ldg(c2 + o[1] + o[0])) * s[1];
-      sum = sum * (1 - s[2]) + top * s[2];
+      V[d] = trilerp(__ldg(c), __ldg(c + o[0]), __ldg(c + o[1]), __ldg(c + o[1] + o[0]), __ldg(c2), __ldg(c2 + o[0]),
+                     __ldg(c2 + o[1]), __ldg(c2 + o[1] + o[0]), s);
+    } else {
+      V[d] = bilerp(__ldg(c), __ldg(c + o[0]), __ldg(c + o[1]), __ldg(c + o[1] + o[0]), s[0], s[1]);
     }
-    V[d] = sum;
   }
   if (DIM == 2) V[2] = T(0);
 }
@@ -82,8 +109,9 @@ __device__ __forceinline__ bool departure_cell(const Geom &g, const T *__restric
                                                int x, int y, int z, int c[3], T f[3]) {
   T V[3];
   mac_vel_node<T, DIM>(g, vel, x, y, z, V);
-  if (backtrace == DCELL_MIDPOINT) {
-    const T dl[3] = {T(-0.5) * V[0] * dth[0], T(-0.5) * V[1] * dth[1], DIM == 3 ? T(-0.5) * V[2] * dth[2] : T(0)};
+  if (backtrace == DCELL_MIDPOINT) {  // products rounded explicitly: no path-dependent contraction
+    const T dl[3] = {rmul(rmul(T(-0.5), V[0]), dth[0]), rmul(rmul(T(-0.5), V[1]), dth[1]),
+                     DIM == 3 ? rmul(rmul(T(-0.5), V[2]), dth[2]) : T(0)};
     mac_vel_rel<T, DIM>(g, vel, x, y, z, dl, V);
   }
   const int X[3] = {x, y, z}, n[3] = {g.nx, g.ny, g.nz};
@@ -95,7 +123,7 @@ __device__ __forceinline__ bool departure_cell(const Geom &g, const T *__restric
       f[2] = T(0);
       continue;
     }
-    const T t = -V[a] * dth[a];
+    const T t = rmul(-V[a], dth[a]);
     const T fl = floor(t);
     c[a] = X[a] + (int)fl;
     f[a] = t - fl;

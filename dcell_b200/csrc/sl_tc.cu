@@ -29,6 +29,7 @@
 // Several CTAs per SM (128 TMEM columns each) overlap one CTA's gathers with
 // another's MMA.  Band structure and backtrace follow LevelSetAdvectSL_3D
 // (LevelSetMethod/AdvectSL.c:56-89).
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "dcell_common.cuh"
@@ -384,6 +385,246 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_split_kernel(Geom g, const uin
   if ((threadIdx.x >> 5) == 0) tmem_dealloc(c.tmem, kTmemCols);
 }
 
+// ---------------------------------------------------------------------------
+// TMA-staged brick variant of the split-state step (dense grids, nx % 4 == 0).
+//
+// A CTA walks bricks of 32 x 2 x 4 arrival points (two 128-point MMA tiles).
+// For each brick, thread 0 issues two tiled TMA loads into shared memory --
+// the phi-split words of the box [x0-4, x0+36) x [y0-2, y0+4) x [z0-2, z0+6)
+// and the interleaved velocity of [x0-4, x0+36) x [y0-1, y0+3) x [z0-1, z0+5)
+// -- one brick ahead, double-buffered, completion tracked by an mbarrier's
+// transaction count.  Gathers then read shared memory with 32-bit offsets.
+// Out-of-grid parts of a box are zero-filled by TMA but never read: indices
+// are clamped to the grid before they are made box-local.  Points whose
+// departure (or midpoint) leaves the box -- per-component CFL >= 1 -- take
+// the global-memory path.  TMA x coordinates are multiples of 4 elements
+// (16-byte rule); nothing starts a store at a negative coordinate.
+constexpr int kBX = 32, kBY = 2, kBZ = 4;               // brick = 256 points = 2 MMA tiles
+constexpr int kPX = kBX + 8, kPY = kBY + 4, kPZ = kBZ + 4;  // phi box (halo 4 | 2 | 2)
+constexpr int kVX = kBX + 8, kVY = kBY + 2, kVZ = kBZ + 2;  // velocity box (halo 4 | 1 | 1)
+constexpr int kPhiBoxBytes = kPX * kPY * kPZ * 4;
+constexpr int kVelBoxBytes = 3 * kVX * kVY * kVZ * 4;
+constexpr int kBufBytes = kPhiBoxBytes + kVelBoxBytes;
+constexpr int kBrickSmem = kBBytes + 2 * kBufBytes + 64;
+static_assert(kBrickSmem <= kDynSmem, "brick buffers exceed the CTA's shared memory budget");
+static_assert(kPhiBoxBytes % 128 == 0 && kBufBytes % 128 == 0, "TMA destinations must stay 128-byte aligned");
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, int c0, int c1, int c2,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+struct BrickGrid {
+  int nbx, nby, nbz;
+};
+
+__device__ __forceinline__ void brick_origin(const BrickGrid &bg, int b, int &x0, int &y0, int &z0) {
+  const int bx = b % bg.nbx, r = b / bg.nbx;
+  x0 = bx * kBX;
+  y0 = (r % bg.nby) * kBY;
+  z0 = (r / bg.nby) * kBZ;
+}
+
+// thread 0: both boxes of brick b into buffer `buf` (whose previous contents
+// every thread has finished reading: order those generic-proxy reads before
+// the async-proxy writes)
+__device__ __forceinline__ void issue_brick(const BrickGrid &bg, int b, uint8_t *buf, const CUtensorMap *tm_phi,
+                                            const CUtensorMap *tm_vel, uint64_t *bar) {
+  int x0, y0, z0;
+  brick_origin(bg, b, x0, y0, z0);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_expect_tx(bar, (uint32_t)kBufBytes);
+  tma_load_3d(buf, tm_phi, x0 - 4, y0 - 2, z0 - 2, bar);
+  tma_load_3d(buf + kPhiBoxBytes, tm_vel, 3 * (x0 - 4), y0 - 1, z0 - 1, bar);
+}
+
+// Front half of one point from the staged boxes; false -> use the global path.
+__device__ __forceinline__ bool brick_prepare(const Geom &g, const uint32_t *__restrict__ pbox,
+                                              const float *__restrict__ vbox, int x0, int y0, int z0,
+                                              const float dth[3], int backtrace, int x, int y, int z, float f[3],
+                                              uint32_t *hi, uint32_t *lo) {
+  const int ox = x0 - 4, oyv = y0 - 1, ozv = z0 - 1;  // velocity box origin
+  auto V = [&](int gx, int gy, int gz, int d) {
+    return vbox[((gz - ozv) * kVY + (gy - oyv)) * (3 * kVX) + 3 * (gx - ox) + d];
+  };
+  float U[3];
+  {
+    const int xp = min(x + 1, g.nx - 1), yp = min(y + 1, g.ny - 1), zp = min(z + 1, g.nz - 1);
+    U[0] = face_mean(V(x, y, z, 0), V(xp, y, z, 0));
+    U[1] = face_mean(V(x, y, z, 1), V(x, yp, z, 1));
+    U[2] = face_mean(V(x, y, z, 2), V(x, y, zp, 2));
+  }
+  if (backtrace == DCELL_MIDPOINT) {
+    const float dl[3] = {rmul(rmul(-0.5f, U[0]), dth[0]), rmul(rmul(-0.5f, U[1]), dth[1]),
+                         rmul(rmul(-0.5f, U[2]), dth[2])};
+    if (fabsf(dl[0]) >= 0.5f || fabsf(dl[1]) >= 0.5f || fabsf(dl[2]) >= 0.5f) return false;
+    const int X[3] = {x, y, z}, n[3] = {g.nx, g.ny, g.nz};
+    float Um[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      int b0[3], b1[3];
+      float s[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float t = dl[a] + (a == d ? 0.5f : 0.f);
+        const float fl = floorf(t);
+        const int b = X[a] + (int)fl;
+        s[a] = t - fl;
+        b0[a] = clampi(b, 0, n[a] - 1);
+        b1[a] = clampi(b + 1, 0, n[a] - 1);
+      }
+      Um[d] = trilerp(V(b0[0], b0[1], b0[2], d), V(b1[0], b0[1], b0[2], d), V(b0[0], b1[1], b0[2], d),
+                      V(b1[0], b1[1], b0[2], d), V(b0[0], b0[1], b1[2], d), V(b1[0], b0[1], b1[2], d),
+                      V(b0[0], b1[1], b1[2], d), V(b1[0], b1[1], b1[2], d), s);
+    }
+    U[0] = Um[0]; U[1] = Um[1]; U[2] = Um[2];
+  }
+  int c[3];
+  const int X[3] = {x, y, z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float t = rmul(-U[a], dth[a]);
+    const float fl = floorf(t);
+    c[a] = X[a] + (int)fl;
+    f[a] = t - fl;
+  }
+  // stencil window, clamped, then made box-local (phi box origin x0-4, y0-2, z0-2)
+  const int xs0 = clampi(c[0] - 1, 0, g.nx - 1) - ox, xs3 = clampi(c[0] + 2, 0, g.nx - 1) - ox;
+  const int ys0 = clampi(c[1] - 1, 0, g.ny - 1) - (y0 - 2), ys3 = clampi(c[1] + 2, 0, g.ny - 1) - (y0 - 2);
+  const int zs0 = clampi(c[2] - 1, 0, g.nz - 1) - (z0 - 2), zs3 = clampi(c[2] + 2, 0, g.nz - 1) - (z0 - 2);
+  if (xs0 < 0 || xs3 >= kPX || ys0 < 0 || ys3 >= kPY || zs0 < 0 || zs3 >= kPZ) return false;
+  uint32_t sv[64];
+  const bool unclamped = c[0] >= 1 && c[0] + 2 < g.nx && c[1] >= 1 && c[1] + 2 < g.ny && c[2] >= 1 && c[2] + 2 < g.nz;
+  if (unclamped) {
+    const uint32_t *p = pbox + (zs0 * kPY + ys0) * kPX + xs0;
+#pragma unroll
+    for (int zz = 0; zz < 4; ++zz)
+#pragma unroll
+      for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+        for (int xx = 0; xx < 4; ++xx) sv[xx + 4 * yy + 16 * zz] = p[(zz * kPY + yy) * kPX + xx];
+  } else {
+    int xi[4], yo[4], zo[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      xi[i] = clampi(c[0] - 1 + i, 0, g.nx - 1) - ox;
+      yo[i] = (clampi(c[1] - 1 + i, 0, g.ny - 1) - (y0 - 2)) * kPX;
+      zo[i] = (clampi(c[2] - 1 + i, 0, g.nz - 1) - (z0 - 2)) * (kPX * kPY);
+    }
+#pragma unroll
+    for (int zz = 0; zz < 4; ++zz)
+#pragma unroll
+      for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+        for (int xx = 0; xx < 4; ++xx) sv[xx + 4 * yy + 16 * zz] = pbox[zo[zz] + yo[yy] + xi[xx]];
+  }
+#pragma unroll
+  for (int e = 0; e < 32; ++e) {
+    hi[e] = __byte_perm(sv[2 * e], sv[2 * e + 1], 0x5410);
+    lo[e] = __byte_perm(sv[2 * e], sv[2 * e + 1], 0x7632);
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kTile, 4) sl_tc_brick_kernel(const __grid_constant__ CUtensorMap tm_phi,
+                                                               const __grid_constant__ CUtensorMap tm_vel, Geom g,
+                                                               BrickGrid bg, const uint32_t *__restrict__ phi0s,
+                                                               const float *__restrict__ vel, float dt,
+                                                               int backtrace, float *__restrict__ phi,
+                                                               uint32_t *__restrict__ phis, int *flags) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sB = smem;
+  uint8_t *const buf0 = smem + kBBytes, *const buf1 = smem + kBBytes + kBufBytes;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kBBytes + 2 * kBufBytes);
+  uint64_t *tbar = bar + 1;  // two TMA barriers
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 3);
+  if (threadIdx.x == 0) {
+    mbar_init(&tbar[0], 1);
+    mbar_init(&tbar[1], 1);
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_phi)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_vel)) : "memory");
+  }
+  Ctx c;
+  setup(sB, bar, tmem_slot, c);  // B operand, MMA barrier, TMEM; ends with a CTA barrier
+
+  const float dth[3] = {dt / (float)g.hx, dt / (float)g.hy, dt / (float)g.hz};
+  const int nbricks = bg.nbx * bg.nby * bg.nbz;
+  const int lx = threadIdx.x & (kBX - 1), ly = (threadIdx.x >> 5) & 1, lzt = threadIdx.x >> 6;  // tile: 32x2x2
+  uint32_t parity = 0;
+  uint32_t uses0 = 0u, uses1 = 0u;  // completed phases per TMA buffer
+  bool pending0 = false, pending1 = false;
+  bool timeout = false;
+  int it = 0;
+  if (threadIdx.x == 0 && (int)blockIdx.x < nbricks) issue_brick(bg, blockIdx.x, buf0, &tm_phi, &tm_vel, &tbar[0]);
+  pending0 = (int)blockIdx.x < nbricks;
+  for (int b = blockIdx.x; b < nbricks; b += gridDim.x, ++it) {
+    const bool odd = it & 1;
+    uint8_t *const cbuf = odd ? buf1 : buf0;
+    const int nb = b + gridDim.x;
+    if (threadIdx.x == 0 && nb < nbricks)
+      issue_brick(bg, nb, odd ? buf0 : buf1, &tm_phi, &tm_vel, odd ? &tbar[0] : &tbar[1]);
+    if (odd) pending0 = nb < nbricks; else pending1 = nb < nbricks;
+    const bool ok = mbar_wait(odd ? &tbar[1] : &tbar[0], (odd ? uses1 : uses0) & 1u);
+    if (!__syncthreads_and(ok ? 1 : 0)) {
+      timeout = true;
+      break;
+    }
+    if (odd) { pending1 = false; ++uses1; } else { pending0 = false; ++uses0; }
+    int x0, y0, z0;
+    brick_origin(bg, b, x0, y0, z0);
+    const uint32_t *pbox = reinterpret_cast<const uint32_t *>(cbuf);
+    const float *vbox = reinterpret_cast<const float *>(cbuf + kPhiBoxBytes);
+#pragma unroll 1
+    for (int t = 0; t < 2; ++t) {
+      const int x = x0 + lx, y = y0 + ly, z = z0 + 2 * t + lzt;
+      const bool valid = x < g.nx && y < g.ny && z < g.nz;
+      float f[3] = {0.f, 0.f, 0.f};
+      uint32_t hi[32], lo[32];
+      if (valid) {
+        if (!brick_prepare(g, pbox, vbox, x0, y0, z0, dth, backtrace, x, y, z, f, hi, lo)) {
+          bool clamped = false;
+          tc_prepare_split(g, phi0s, vel, dth, backtrace, true, x, y, z, f, hi, lo, clamped);
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < 32; ++e) hi[e] = lo[e] = 0u;
+      }
+      float a[64];
+      if (!mma_tile(c, bar, parity, hi, lo, a)) {
+        timeout = true;
+        break;
+      }
+      parity ^= 1u;
+      if (valid) {
+        const int p = (z * g.ny + y) * g.nx + x;
+        const float v = horner3(a, f);
+        phi[p] = v;
+        if (phis) phis[p] = pack_split(v);
+      }
+    }
+    if (timeout) break;
+    __syncthreads();  // everyone is done with buf[cur] before it is refilled
+  }
+  if (timeout && threadIdx.x == 0) {
+    raise_flag(flags, FLAG_WAIT_TIMEOUT);
+    // let every TMA still in flight land before the CTA's shared memory goes away (bounded waits)
+    if (pending0) mbar_wait(&tbar[0], uses0 & 1u);
+    if (pending1) mbar_wait(&tbar[1], uses1 & 1u);
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if ((threadIdx.x >> 5) == 0) tmem_dealloc(c.tmem, kTmemCols);
+}
+
 // Batched cells: a persistent CTA walks a packed queue of 128-point tiles
 // (tx x ty x tz boxes of one cell's grid) over many uneven cell grids.
 __global__ void __launch_bounds__(kTile, 4) batch_tc_kernel(const dcell_cell *__restrict__ cells,
@@ -518,8 +759,14 @@ int launch_split_bf16(const float *phi, uint32_t *out, long long n, cudaStream_t
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 
+bool tc_brick_applicable(const Geom &g, const void *phi0s, const void *vel);
+int launch_sl_tc_brick(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
+                       uint32_t *phis, int *flags, cudaStream_t st);
+
 int launch_sl_tc_split(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, const int *band,
                        long long npts, int backtrace, float *phi, uint32_t *phis, int *flags, cudaStream_t st) {
+  if (!band && tc_brick_applicable(g, phi0s, vel))
+    return launch_sl_tc_brick(g, phi0s, vel, dt, backtrace, phi, phis, flags, st);
   static bool configured = false;
   if (!configured) {
     DCELL_CUDA_CHECK(
@@ -529,6 +776,76 @@ int launch_sl_tc_split(const Geom &g, const uint32_t *phi0s, const float *vel, d
   if (npts <= 0) return DCELL_OK;
   tc::sl_tc_split_kernel<<<tc_grid(npts), tc::kTile, tc::kDynSmem, st>>>(g, phi0s, vel, (float)dt, band, npts,
                                                                          backtrace, phi, phis, flags);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+    cudaGetLastError();
+  }
+  return fn;
+}
+
+// 3-D tiled map over a row-major array (x fastest) of `elem` bytes per value.
+static bool make_map(CUtensorMap *m, CUtensorMapDataType type, const void *base, uint64_t dx, uint64_t dy,
+                     uint64_t dz, uint32_t bx, uint32_t by, uint32_t bz, uint32_t elem) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return false;
+  const cuuint64_t dims[3] = {dx, dy, dz};
+  const cuuint64_t strides[2] = {dx * elem, dx * dy * elem};
+  const cuuint32_t box[3] = {bx, by, bz};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, type, 3, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The TMA brick path applies to dense 3D grids with nx % 4 == 0 (16-byte row strides) and 16-byte aligned bases.
+bool tc_brick_applicable(const Geom &g, const void *phi0s, const void *vel) {
+  return g.nz >= tc::kPZ && g.ny >= tc::kPY && g.nx >= tc::kPX && g.nx % 4 == 0 && ((uintptr_t)phi0s % 16) == 0 &&
+         ((uintptr_t)vel % 16) == 0 && encode_tiled() != nullptr;
+}
+
+int launch_sl_tc_brick(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
+                       uint32_t *phis, int *flags, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    DCELL_CUDA_CHECK(
+        cudaFuncSetAttribute(tc::sl_tc_brick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kDynSmem));
+    configured = true;
+  }
+  CUtensorMap tm_phi, tm_vel;
+  if (!make_map(&tm_phi, CU_TENSOR_MAP_DATA_TYPE_UINT32, phi0s, (uint64_t)g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
+                tc::kPX, tc::kPY, tc::kPZ, 4) ||
+      !make_map(&tm_vel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel, 3ull * g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
+                3 * tc::kVX, tc::kVY, tc::kVZ, 4)) {
+    dcell_set_error(DCELL_ERR_CUDA, "cuTensorMapEncodeTiled failed for the TMA brick path");
+    return DCELL_ERR_CUDA;
+  }
+  tc::BrickGrid bg;
+  bg.nbx = (g.nx + tc::kBX - 1) / tc::kBX;
+  bg.nby = (g.ny + tc::kBY - 1) / tc::kBY;
+  bg.nbz = (g.nz + tc::kBZ - 1) / tc::kBZ;
+  const long long nbricks = (long long)bg.nbx * bg.nby * bg.nbz;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long grid = 4LL * sms;
+  if (grid > nbricks) grid = nbricks;
+  tc::sl_tc_brick_kernel<<<(int)grid, tc::kTile, tc::kDynSmem, st>>>(tm_phi, tm_vel, g, bg, phi0s, vel, (float)dt,
+                                                                       backtrace, phi, phis, flags);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 

@@ -107,7 +107,7 @@ def band_of(phi, width, origin=(0, 0, 0), margin=3):
     `margin` cells inside the grid, in x-fastest order."""
     dim = phi.dim()
     inner = torch.zeros_like(phi, dtype=torch.bool)
-    sl = tuple(slice(margin, -margin) for _ in range(dim))
+    sl = tuple(slice(margin, n - margin) for n in phi.shape)
     inner[sl] = True
     sel = inner & (phi.abs() < width)
     idx = torch.nonzero(sel)  # (nb, dim) in (z, y, x) order, lexicographic = x fastest

@@ -237,3 +237,25 @@ def test_tc_split_band_mode_and_multistep(cuda):
         ref = L.sl_step(ref, vel, dt, h, interp="cubic_plain", backtrace="midpoint")
     err = (a.double() - ref).abs()[ref.abs() < 3 * h]
     assert float(err.max()) <= 1e-5, float(err.max())
+
+
+@pytest.mark.parametrize("cfl_scale", [1.0, 3.0])
+def test_tc_brick_path_equals_gather_path(cuda, cfl_scale):
+    """Dense split-state steps on grids with nx % 4 == 0 run the TMA-staged
+    brick kernel; a band listing every point runs the global-gather kernel.
+    Both must give the same bits (3x the CFL exercises the brick fallbacks)."""
+    nz, ny, nx = 40, 48, 64
+    h = 1.0 / 64
+    phi = fields.sphere_sdf(64, device=cuda)[:nz, :ny, :nx].contiguous().float()
+    vel = fields.deformation_velocity(64, device=cuda)[:nz, :ny, :nx].contiguous().float()
+    dt = cfl_scale * fields.cfl_dt((2.0, 1.0, 1.0), h)
+    spl = L.split_bf16(phi)
+    for bt in ("midpoint", "euler"):
+        dense, dspl = L.sl_step_tc_split(spl, vel, dt, h, backtrace=bt, out_split=torch.empty_like(spl))
+        band = fields.band_of(torch.zeros_like(phi), 1.0, margin=0).to(cuda)  # every point, x fastest
+        assert band.shape[0] == nx * ny * nz
+        banded, bspl = L.sl_step_tc_split(spl, vel, dt, h, band=band, backtrace=bt, out=torch.zeros_like(phi),
+                                          out_split=torch.zeros_like(spl))
+        torch.cuda.synchronize()
+        assert torch.equal(dense, banded), float((dense - banded).abs().max())
+        assert torch.equal(dspl, bspl)
