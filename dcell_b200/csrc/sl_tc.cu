@@ -41,8 +41,9 @@ namespace tc {
 
 constexpr int kTile = 128;       // points per MMA (M)
 constexpr int kCoef = 64;        // coefficients (N)
-constexpr int kTmemCols = 128;   // A: 64 columns (hi 32 + lo 32), D: 64 columns
-constexpr int kBBytes = kCoef * 64 * 2;  // B: 64 rows x 64 K of bf16 (reused for hi and lo)
+constexpr int kK = 128;          // K: stencil entry j contributes hi_j at K = 2j and lo_j at K = 2j + 1
+constexpr int kTmemCols = 128;   // A: 64 columns (one packed hi|lo word per stencil entry), D: 64 columns
+constexpr int kBBytes = kCoef * kK * 2;  // B: 64 rows x 128 K of bf16, B[n][2j] = B[n][2j+1] = M[n][j]
 constexpr int kDynSmem = 56 * 1024;      // caps residency at 4 CTAs/SM = 512 TMEM columns
 constexpr unsigned kWaitLimit = 1u << 20;  // bounded mbarrier polls (a normal MMA completes in microseconds)
 
@@ -63,9 +64,9 @@ __host__ __device__ constexpr uint32_t instr_desc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// Byte offset of element (row n, k) of a K-major no-swizzle operand with K = 64.
+// Byte offset of element (row n, k) of a K-major no-swizzle operand with K = 128.
 __device__ __forceinline__ int b_offset(int n, int k) {
-  return (((n >> 3) * 8 + (k >> 3)) * 128) + (n & 7) * 16 + (k & 7) * 2;
+  return (((n >> 3) * (kK / 8) + (k >> 3)) * 128) + (n & 7) * 16 + (k & 7) * 2;
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
@@ -155,9 +156,9 @@ struct Ctx {
 
 __device__ __forceinline__ void setup(uint8_t *sB, uint64_t *bar, uint32_t *tmem_slot, Ctx &c) {
   const int tid = threadIdx.x, warp = tid >> 5;
-  for (int e = tid; e < kCoef * 64; e += blockDim.x) {
-    const int n = e >> 6, k = e & 63;  // B[n][k] = M[n][k]: coefficient n from stencil entry k
-    const float w = cr_coef(n >> 4, k >> 4) * cr_coef((n >> 2) & 3, (k >> 2) & 3) * cr_coef(n & 3, k & 3);
+  for (int e = tid; e < kCoef * kK; e += blockDim.x) {
+    const int n = e / kK, k = e % kK, j = k >> 1;  // B[n][k] = M[n][j]: coefficient n from stencil entry j
+    const float w = cr_coef(n >> 4, j >> 4) * cr_coef((n >> 2) & 3, (j >> 2) & 3) * cr_coef(n & 3, j & 3);
     *reinterpret_cast<__nv_bfloat16 *>(sB + b_offset(n, k)) = __float2bfloat16_rn(w);
   }
   if (tid == 0) mbar_init(bar, 1);
@@ -169,27 +170,24 @@ __device__ __forceinline__ void setup(uint8_t *sB, uint64_t *bar, uint32_t *tmem
   fence_after();
   c.tmem = *tmem_slot;
   c.lane_off = (uint32_t)(warp * 32) << 16;
-  c.bdesc = smem_desc(smem_u32(sB), 128, 1024);
+  c.bdesc = smem_desc(smem_u32(sB), 128, (kK / 8) * 128);
 }
 
-// Pack hi/lo BF16 halves of 64 values (already centred) into 2 x 32 columns.
-__device__ __forceinline__ void split_bf16(const float *s, uint32_t *hi, uint32_t *lo) {
-#pragma unroll
-  for (int e = 0; e < 32; ++e) {
-    const float v0 = s[2 * e], v1 = s[2 * e + 1];
-    const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);  // .x (low half) = element 2e
-    const __nv_bfloat162 l = __floats2bfloat162_rn(v0 - __low2float(h), v1 - __high2float(h));
-    hi[e] = *reinterpret_cast<const uint32_t *>(&h);
-    lo[e] = *reinterpret_cast<const uint32_t *>(&l);
-  }
+// Packed split word of v: bf16 hi = RN_bf16(v) in the low half, bf16
+// lo = RN_bf16(v - hi) in the high half (= TMEM column layout of one stencil
+// entry: K = 2j low half, K = 2j + 1 high half).
+__device__ __forceinline__ uint32_t pack_split(float v) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+  return (uint32_t)__bfloat16_as_ushort(h) | ((uint32_t)__bfloat16_as_ushort(l) << 16);
 }
 
-// A (this lane) -> TMEM, barrier, MMA by thread 0, bounded wait, D -> regs.
-// Returns false (CTA-uniformly) when the wait timed out.
-__device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t parity, const uint32_t *hi,
-                                         const uint32_t *lo, float *coef) {
-  tmem_st32(c.tmem + c.lane_off + 0, hi);
-  tmem_st32(c.tmem + c.lane_off + 32, lo);
+// A (this lane: 64 packed words) -> TMEM, barrier, MMA by thread 0, bounded
+// wait, D -> regs.  Returns false (CTA-uniformly) when the wait timed out.
+__device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t parity, const uint32_t *w,
+                                         float *coef) {
+  tmem_st32(c.tmem + c.lane_off + 0, w);
+  tmem_st32(c.tmem + c.lane_off + 32, w + 32);
   tmem_wait_st();
   fence_before();
   __syncthreads();
@@ -197,9 +195,9 @@ __device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t p
     fence_after();
     constexpr uint32_t idesc = instr_desc_bf16(kTile, kCoef);
 #pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-      const uint32_t a_tmem = c.tmem + (uint32_t)(kk * 8);               // 8 columns = 16 bf16 of K
-      const uint64_t bdesc = c.bdesc + (uint64_t)(((kk & 3) * 256) >> 4);  // K-step of B (2 core matrices)
+    for (int kk = 0; kk < kK / 16; ++kk) {
+      const uint32_t a_tmem = c.tmem + (uint32_t)(kk * 8);          // 8 columns = 16 bf16 of K
+      const uint64_t bdesc = c.bdesc + (uint64_t)((kk * 256) >> 4);  // K-step of B (2 core matrices)
       mma_bf16(c.tmem + 64, a_tmem, bdesc, idesc, kk > 0 ? 1u : 0u);
     }
     mma_commit(bar);
@@ -237,21 +235,20 @@ __device__ __forceinline__ float horner3(const float *a, const float f[3]) {
 // Invalid lanes contribute a zero A row.
 __device__ __forceinline__ void tc_prepare(const Geom &g, const float *__restrict__ phi0,
                                            const float *__restrict__ vel, const float dth[3], int backtrace,
-                                           bool valid, int x, int y, int z, float f[3], float &r, uint32_t *hi,
-                                           uint32_t *lo, bool &clamped) {
-  float s[64];
+                                           bool valid, int x, int y, int z, float f[3], float &r, uint32_t *w,
+                                           bool &clamped) {
   if (valid) {
     int cc[3];
+    float s[64];
     clamped |= departure_cell<float, 3>(g, vel, dth, backtrace, x, y, z, cc, f);
     gather_stencil<float, 3>(g, phi0, cc, s);
     r = s[21];
 #pragma unroll
-    for (int e = 0; e < 64; ++e) s[e] -= r;
+    for (int e = 0; e < 64; ++e) w[e] = pack_split(s[e] - r);
   } else {
 #pragma unroll
-    for (int e = 0; e < 64; ++e) s[e] = 0.f;
+    for (int e = 0; e < 64; ++e) w[e] = 0u;
   }
-  split_bf16(s, hi, lo);
 }
 
 __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__restrict__ phi0,
@@ -278,10 +275,10 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__
       bad = true;
     }
     float f[3] = {0.f, 0.f, 0.f}, r = 0.f;
-    uint32_t hi[32], lo[32];
-    tc_prepare(g, phi0, vel, dth, backtrace, valid, x, y, z, f, r, hi, lo, clamped);
+    uint32_t w[64];
+    tc_prepare(g, phi0, vel, dth, backtrace, valid, x, y, z, f, r, w, clamped);
     float a[64];
-    if (!mma_tile(c, bar, parity, hi, lo, a)) {
+    if (!mma_tile(c, bar, parity, w, a)) {
       timeout = true;
       break;
     }
@@ -303,36 +300,25 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_kernel(Geom g, const float *__
 // lo = RN_bf16(phi - hi) in the high half), written by the step that produces
 // phi.  A step then gathers the 64 packed words of each stencil and forms the
 // A row's TMEM columns with one byte-permute per column -- no per-entry
-// subtraction or conversion.  M (hi + lo) = M phi to ~2^-17 relative.
-__device__ __forceinline__ uint32_t pack_split(float v) {
-  const __nv_bfloat16 h = __float2bfloat16_rn(v);
-  const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
-  return (uint32_t)__bfloat16_as_ushort(h) | ((uint32_t)__bfloat16_as_ushort(l) << 16);
-}
-
+// subtraction or conversion: with the interleaved K order the gathered words
+// are the A row.  M (hi + lo) = M phi to ~2^-17 relative.
 __global__ void __launch_bounds__(256) split_kernel(const float *__restrict__ phi, uint32_t *__restrict__ out,
                                                     long long n) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
     out[q] = pack_split(phi[q]);
 }
 
-__device__ __forceinline__ void tc_prepare_split(const Geom &g, const uint32_t *__restrict__ w,
+__device__ __forceinline__ void tc_prepare_split(const Geom &g, const uint32_t *__restrict__ words,
                                                  const float *__restrict__ vel, const float dth[3], int backtrace,
-                                                 bool valid, int x, int y, int z, float f[3], uint32_t *hi,
-                                                 uint32_t *lo, bool &clamped) {
+                                                 bool valid, int x, int y, int z, float f[3], uint32_t *w,
+                                                 bool &clamped) {
   if (valid) {
     int cc[3];
-    uint32_t s[64];
     clamped |= departure_cell<float, 3>(g, vel, dth, backtrace, x, y, z, cc, f);
-    gather_stencil<uint32_t, 3>(g, w, cc, s);
-#pragma unroll
-    for (int e = 0; e < 32; ++e) {
-      hi[e] = __byte_perm(s[2 * e], s[2 * e + 1], 0x5410);  // (hi_2e, hi_2e+1)
-      lo[e] = __byte_perm(s[2 * e], s[2 * e + 1], 0x7632);  // (lo_2e, lo_2e+1)
-    }
+    gather_stencil<uint32_t, 3>(g, words, cc, w);  // the packed words are the A row as they stand
   } else {
 #pragma unroll
-    for (int e = 0; e < 32; ++e) hi[e] = lo[e] = 0u;
+    for (int e = 0; e < 64; ++e) w[e] = 0u;
   }
 }
 
@@ -361,10 +347,10 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_split_kernel(Geom g, const uin
       bad = true;
     }
     float f[3] = {0.f, 0.f, 0.f};
-    uint32_t hi[32], lo[32];
-    tc_prepare_split(g, phi0s, vel, dth, backtrace, valid, x, y, z, f, hi, lo, clamped);
+    uint32_t w[64];
+    tc_prepare_split(g, phi0s, vel, dth, backtrace, valid, x, y, z, f, w, clamped);
     float a[64];
-    if (!mma_tile(c, bar, parity, hi, lo, a)) {
+    if (!mma_tile(c, bar, parity, w, a)) {
       timeout = true;
       break;
     }
@@ -450,7 +436,7 @@ __device__ __forceinline__ void issue_brick(const BrickGrid &bg, int b, uint8_t 
 __device__ __forceinline__ bool brick_prepare(const Geom &g, const uint32_t *__restrict__ pbox,
                                               const float *__restrict__ vbox, int x0, int y0, int z0,
                                               const float dth[3], int backtrace, int x, int y, int z, float f[3],
-                                              uint32_t *hi, uint32_t *lo) {
+                                              uint32_t *sv) {
   const int ox = x0 - 4, oyv = y0 - 1, ozv = z0 - 1;  // velocity box origin
   auto V = [&](int gx, int gy, int gz, int d) {
     return vbox[((gz - ozv) * kVY + (gy - oyv)) * (3 * kVX) + 3 * (gx - ox) + d];
@@ -501,7 +487,6 @@ __device__ __forceinline__ bool brick_prepare(const Geom &g, const uint32_t *__r
   const int ys0 = clampi(c[1] - 1, 0, g.ny - 1) - (y0 - 2), ys3 = clampi(c[1] + 2, 0, g.ny - 1) - (y0 - 2);
   const int zs0 = clampi(c[2] - 1, 0, g.nz - 1) - (z0 - 2), zs3 = clampi(c[2] + 2, 0, g.nz - 1) - (z0 - 2);
   if (xs0 < 0 || xs3 >= kPX || ys0 < 0 || ys3 >= kPY || zs0 < 0 || zs3 >= kPZ) return false;
-  uint32_t sv[64];
   const bool unclamped = c[0] >= 1 && c[0] + 2 < g.nx && c[1] >= 1 && c[1] + 2 < g.ny && c[2] >= 1 && c[2] + 2 < g.nz;
   if (unclamped) {
     const uint32_t *p = pbox + (zs0 * kPY + ys0) * kPX + xs0;
@@ -525,11 +510,6 @@ __device__ __forceinline__ bool brick_prepare(const Geom &g, const uint32_t *__r
       for (int yy = 0; yy < 4; ++yy)
 #pragma unroll
         for (int xx = 0; xx < 4; ++xx) sv[xx + 4 * yy + 16 * zz] = pbox[zo[zz] + yo[yy] + xi[xx]];
-  }
-#pragma unroll
-  for (int e = 0; e < 32; ++e) {
-    hi[e] = __byte_perm(sv[2 * e], sv[2 * e + 1], 0x5410);
-    lo[e] = __byte_perm(sv[2 * e], sv[2 * e + 1], 0x7632);
   }
   return true;
 }
@@ -587,18 +567,18 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_brick_kernel(const __grid_cons
       const int x = x0 + lx, y = y0 + ly, z = z0 + 2 * t + lzt;
       const bool valid = x < g.nx && y < g.ny && z < g.nz;
       float f[3] = {0.f, 0.f, 0.f};
-      uint32_t hi[32], lo[32];
+      uint32_t w[64];
       if (valid) {
-        if (!brick_prepare(g, pbox, vbox, x0, y0, z0, dth, backtrace, x, y, z, f, hi, lo)) {
+        if (!brick_prepare(g, pbox, vbox, x0, y0, z0, dth, backtrace, x, y, z, f, w)) {
           bool clamped = false;
-          tc_prepare_split(g, phi0s, vel, dth, backtrace, true, x, y, z, f, hi, lo, clamped);
+          tc_prepare_split(g, phi0s, vel, dth, backtrace, true, x, y, z, f, w, clamped);
         }
       } else {
 #pragma unroll
-        for (int e = 0; e < 32; ++e) hi[e] = lo[e] = 0u;
+        for (int e = 0; e < 64; ++e) w[e] = 0u;
       }
       float a[64];
-      if (!mma_tile(c, bar, parity, hi, lo, a)) {
+      if (!mma_tile(c, bar, parity, w, a)) {
         timeout = true;
         break;
       }
@@ -653,10 +633,10 @@ __global__ void __launch_bounds__(kTile, 4) batch_tc_kernel(const dcell_cell *__
     const int x = T.x0 + lx, y = T.y0 + ly, z = T.z0 + lz;
     const bool valid = x < g.nx && y < g.ny && z < g.nz;
     float f[3] = {0.f, 0.f, 0.f}, r = 0.f;
-    uint32_t hi[32], lo[32];
-    tc_prepare(g, phi0 + C.offset, vel + 3 * C.offset, dth, backtrace, valid, x, y, z, f, r, hi, lo, clamped);
+    uint32_t w[64];
+    tc_prepare(g, phi0 + C.offset, vel + 3 * C.offset, dth, backtrace, valid, x, y, z, f, r, w, clamped);
     float a[64];
-    if (!mma_tile(c, bar, parity, hi, lo, a)) {
+    if (!mma_tile(c, bar, parity, w, a)) {
       timeout = true;
       break;
     }
@@ -681,13 +661,11 @@ __global__ void __launch_bounds__(kTile, 1) tc_gemm_check_kernel(const float *__
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + kBBytes + 8);
   Ctx c;
   setup(sB, bar, tmem_slot, c);
-  float s[64];
-  for (int e = 0; e < 64; ++e) s[e] = A[threadIdx.x * 64 + e];
-  uint32_t hi[32], lo[32];
-  split_bf16(s, hi, lo);
-  for (int e = 0; e < 32; ++e) lo[e] = 0u;  // hi only: D = bf16(A) M^T
+  uint32_t w[64];
+  for (int e = 0; e < 64; ++e)  // hi only (lo half zero): D = bf16(A) M^T
+    w[e] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(A[threadIdx.x * 64 + e]));
   float a[64];
-  if (mma_tile(c, bar, 0, hi, lo, a)) {
+  if (mma_tile(c, bar, 0, w, a)) {
     for (int e = 0; e < 64; ++e) D[threadIdx.x * 64 + e] = a[e];
   } else if (threadIdx.x == 0) {
     raise_flag(flags, FLAG_WAIT_TIMEOUT);
