@@ -412,11 +412,15 @@ struct BrickGrid {
   int nbx, nby, nbz;
 };
 
+// Bricks are numbered z fastest, x slowest: a persistent CTA striding by the
+// grid size then visits every x position (the x faces, where boxes need edge
+// replication, are shared out evenly), and the bricks in flight at one time
+// are z/y neighbours that share halo rows in L2.
 __device__ __forceinline__ void brick_origin(const BrickGrid &bg, int b, int &x0, int &y0, int &z0) {
-  const int bx = b % bg.nbx, r = b / bg.nbx;
-  x0 = bx * kBX;
+  const int bz = b % bg.nbz, r = b / bg.nbz;
+  z0 = bz * kBZ;
   y0 = (r % bg.nby) * kBY;
-  z0 = (r / bg.nby) * kBZ;
+  x0 = (r / bg.nby) * kBX;
 }
 
 // thread 0: both boxes of brick b into buffer `buf` (whose previous contents
@@ -432,86 +436,105 @@ __device__ __forceinline__ void issue_brick(const BrickGrid &bg, int b, uint8_t 
   tma_load_3d(buf + kPhiBoxBytes, tm_vel, 3 * (x0 - 4), y0 - 1, z0 - 1, bar);
 }
 
-// Front half of one point from the staged boxes; false -> use the global path.
-__device__ __forceinline__ bool brick_prepare(const Geom &g, const uint32_t *__restrict__ pbox,
-                                              const float *__restrict__ vbox, int x0, int y0, int z0,
-                                              const float dth[3], int backtrace, int x, int y, int z, float f[3],
-                                              uint32_t *sv) {
-  const int ox = x0 - 4, oyv = y0 - 1, ozv = z0 - 1;  // velocity box origin
-  auto V = [&](int gx, int gy, int gz, int d) {
-    return vbox[((gz - ozv) * kVY + (gy - oyv)) * (3 * kVX) + 3 * (gx - ox) + d];
-  };
-  float U[3];
-  {
-    const int xp = min(x + 1, g.nx - 1), yp = min(y + 1, g.ny - 1), zp = min(z + 1, g.nz - 1);
-    U[0] = face_mean(V(x, y, z, 0), V(xp, y, z, 0));
-    U[1] = face_mean(V(x, y, z, 1), V(x, yp, z, 1));
-    U[2] = face_mean(V(x, y, z, 2), V(x, y, zp, 2));
+// Edge replication of a staged box.  TMA zero-fills the parts of a box that
+// lie outside the grid; afterwards each of them holds the value of the
+// nearest in-grid cell along each axis -- exactly what the reference's
+// clamped interpolation indices read (Common/InterpolateVelocity.c and
+// Common/LevelSetMethod.c clamp i, j, k to the grid independently).  A
+// box-local read at an unclamped index then equals a global read at the
+// clamped index, so the per-point code needs no clamping.  Passes run x, y, z,
+// each reading what the one before wrote, which replicates edges and corners
+// like per-axis clamping.  The box is [DZ][DY][DX][C] 32-bit words whose cell
+// (0,0,0) sits at grid point (gx0, gy0, gz0); in-grid cells of each axis are a
+// non-empty range because the brick's own points are in the grid.  Only
+// CTA-uniform branches; every thread takes part.
+template <int DX, int DY, int DZ, int C>
+__device__ __forceinline__ void replicate_box_edges(uint32_t *box, int gx0, int gy0, int gz0, int nx, int ny,
+                                                    int nz) {
+  const int xl = min(max(-gx0, 0), DX), xh = min(max(nx - gx0, 0), DX);  // in-grid columns [xl, xh)
+  const int yl = min(max(-gy0, 0), DY), yh = min(max(ny - gy0, 0), DY);
+  const int zl = min(max(-gz0, 0), DZ), zh = min(max(nz - gz0, 0), DZ);
+  const int ox = xl + (DX - xh), oy = yl + (DY - yh), oz = zl + (DZ - zh);  // out-of-grid counts
+  if (ox) {
+    const int total = ox * DY * DZ * C;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int k = i % C, r = i / C, j = r % ox, row = r / ox;
+      const int col = j < xl ? j : xh + (j - xl), src = j < xl ? xl : xh - 1;
+      box[(row * DX + col) * C + k] = box[(row * DX + src) * C + k];
+    }
+    __syncthreads();
   }
+  if (oy) {
+    constexpr int W = DX * C;
+    const int total = oy * DZ * W;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int w = i % W, r = i / W, j = r % oy, plane = r / oy;
+      const int row = j < yl ? j : yh + (j - yl), src = j < yl ? yl : yh - 1;
+      box[(plane * DY + row) * W + w] = box[(plane * DY + src) * W + w];
+    }
+    __syncthreads();
+  }
+  if (oz) {
+    constexpr int P = DY * DX * C;
+    const int total = oz * P;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+      const int w = i % P, j = i / P;
+      const int plane = j < zl ? j : zh + (j - zl), src = j < zl ? zl : zh - 1;
+      box[plane * P + w] = box[src * P + w];
+    }
+  }
+  if (ox | oy | oz) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // before TMA refills the buffer
+}
+
+// Front half of one point from the staged, edge-replicated boxes: node
+// velocity, midpoint velocity, departure cell and fraction, and the box offset
+// of the stencil's first word.  (vx, vy, vz) is the point's cell in the
+// velocity box, (px, py, pz) in the phi box.  Returns false when the midpoint
+// or the stencil leaves the box (per-component CFL >= 1): the warp then takes
+// the global path.  The arithmetic is the clamped global path's, operation for
+// operation (explicit roundings), so both give the same bits.
+__device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int vx, int vy, int vz, int px, int py,
+                                             int pz, const float dth[3], int backtrace, float f[3], int &soff) {
+  constexpr int SX = 3, SY = 3 * kVX, SZ = 3 * kVX * kVY;
+  const float *vb = vbox + (vz * kVY + vy) * (3 * kVX) + 3 * vx;
+  float U[3] = {face_mean(vb[0], vb[SX]), face_mean(vb[1], vb[SY + 1]), face_mean(vb[2], vb[SZ + 2])};
   if (backtrace == DCELL_MIDPOINT) {
     const float dl[3] = {rmul(rmul(-0.5f, U[0]), dth[0]), rmul(rmul(-0.5f, U[1]), dth[1]),
                          rmul(rmul(-0.5f, U[2]), dth[2])};
     if (fabsf(dl[0]) >= 0.5f || fabsf(dl[1]) >= 0.5f || fabsf(dl[2]) >= 0.5f) return false;
-    const int X[3] = {x, y, z}, n[3] = {g.nx, g.ny, g.nz};
-    float Um[3];
+    // Along a component's own (staggered) axis the midpoint lies in [X, X+1):
+    // floor 0, fraction t.  Across the other two axes the node-centred
+    // fraction and floor are shared by both components.
+    float sn[3], sp[3];
+    int on[3];
+    constexpr int S[3] = {SX, SY, SZ};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float t = dl[a] + 0.f;
+      const float fl = floorf(t);
+      sn[a] = t - fl;
+      on[a] = (int)fl * S[a];
+      sp[a] = dl[a] + 0.5f;
+    }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      int b0[3], b1[3];
-      float s[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float t = dl[a] + (a == d ? 0.5f : 0.f);
-        const float fl = floorf(t);
-        const int b = X[a] + (int)fl;
-        s[a] = t - fl;
-        b0[a] = clampi(b, 0, n[a] - 1);
-        b1[a] = clampi(b + 1, 0, n[a] - 1);
-      }
-      Um[d] = trilerp(V(b0[0], b0[1], b0[2], d), V(b1[0], b0[1], b0[2], d), V(b0[0], b1[1], b0[2], d),
-                      V(b1[0], b1[1], b0[2], d), V(b0[0], b0[1], b1[2], d), V(b1[0], b0[1], b1[2], d),
-                      V(b0[0], b1[1], b1[2], d), V(b1[0], b1[1], b1[2], d), s);
+      const float s3[3] = {d == 0 ? sp[0] : sn[0], d == 1 ? sp[1] : sn[1], d == 2 ? sp[2] : sn[2]};
+      const float *q = vb + d + (d == 0 ? 0 : on[0]) + (d == 1 ? 0 : on[1]) + (d == 2 ? 0 : on[2]);
+      U[d] = trilerp(q[0], q[SX], q[SY], q[SY + SX], q[SZ], q[SZ + SX], q[SZ + SY], q[SZ + SY + SX], s3);
     }
-    U[0] = Um[0]; U[1] = Um[1]; U[2] = Um[2];
   }
-  int c[3];
-  const int X[3] = {x, y, z};
+  int cl[3];
+  const int P[3] = {px, py, pz};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const float t = rmul(-U[a], dth[a]);
     const float fl = floorf(t);
-    c[a] = X[a] + (int)fl;
+    cl[a] = P[a] + (int)fl - 1;  // first stencil cell, box-local
     f[a] = t - fl;
   }
-  // stencil window, clamped, then made box-local (phi box origin x0-4, y0-2, z0-2)
-  const int xs0 = clampi(c[0] - 1, 0, g.nx - 1) - ox, xs3 = clampi(c[0] + 2, 0, g.nx - 1) - ox;
-  const int ys0 = clampi(c[1] - 1, 0, g.ny - 1) - (y0 - 2), ys3 = clampi(c[1] + 2, 0, g.ny - 1) - (y0 - 2);
-  const int zs0 = clampi(c[2] - 1, 0, g.nz - 1) - (z0 - 2), zs3 = clampi(c[2] + 2, 0, g.nz - 1) - (z0 - 2);
-  if (xs0 < 0 || xs3 >= kPX || ys0 < 0 || ys3 >= kPY || zs0 < 0 || zs3 >= kPZ) return false;
-  const bool unclamped = c[0] >= 1 && c[0] + 2 < g.nx && c[1] >= 1 && c[1] + 2 < g.ny && c[2] >= 1 && c[2] + 2 < g.nz;
-  if (unclamped) {
-    const uint32_t *p = pbox + (zs0 * kPY + ys0) * kPX + xs0;
-#pragma unroll
-    for (int zz = 0; zz < 4; ++zz)
-#pragma unroll
-      for (int yy = 0; yy < 4; ++yy)
-#pragma unroll
-        for (int xx = 0; xx < 4; ++xx) sv[xx + 4 * yy + 16 * zz] = p[(zz * kPY + yy) * kPX + xx];
-  } else {
-    int xi[4], yo[4], zo[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      xi[i] = clampi(c[0] - 1 + i, 0, g.nx - 1) - ox;
-      yo[i] = (clampi(c[1] - 1 + i, 0, g.ny - 1) - (y0 - 2)) * kPX;
-      zo[i] = (clampi(c[2] - 1 + i, 0, g.nz - 1) - (z0 - 2)) * (kPX * kPY);
-    }
-#pragma unroll
-    for (int zz = 0; zz < 4; ++zz)
-#pragma unroll
-      for (int yy = 0; yy < 4; ++yy)
-#pragma unroll
-        for (int xx = 0; xx < 4; ++xx) sv[xx + 4 * yy + 16 * zz] = pbox[zo[zz] + yo[yy] + xi[xx]];
-  }
-  return true;
+  soff = (cl[2] * kPY + cl[1]) * kPX + cl[0];
+  return (unsigned)cl[0] <= (unsigned)(kPX - 4) && (unsigned)cl[1] <= (unsigned)(kPY - 4) &&
+         (unsigned)cl[2] <= (unsigned)(kPZ - 4);
 }
 
 __global__ void __launch_bounds__(kTile, 4) sl_tc_brick_kernel(const __grid_constant__ CUtensorMap tm_phi,
@@ -560,22 +583,37 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_brick_kernel(const __grid_cons
     if (odd) { pending1 = false; ++uses1; } else { pending0 = false; ++uses0; }
     int x0, y0, z0;
     brick_origin(bg, b, x0, y0, z0);
-    const uint32_t *pbox = reinterpret_cast<const uint32_t *>(cbuf);
+    uint32_t *pbox = reinterpret_cast<uint32_t *>(cbuf);
     const float *vbox = reinterpret_cast<const float *>(cbuf + kPhiBoxBytes);
+    if (x0 < 4 || x0 + kPX - 4 > g.nx || y0 < 2 || y0 + kPY - 2 > g.ny || z0 < 2 || z0 + kPZ - 2 > g.nz) {
+      replicate_box_edges<kPX, kPY, kPZ, 1>(pbox, x0 - 4, y0 - 2, z0 - 2, g.nx, g.ny, g.nz);
+      replicate_box_edges<kVX, kVY, kVZ, 3>(reinterpret_cast<uint32_t *>(cbuf + kPhiBoxBytes), x0 - 4, y0 - 1,
+                                            z0 - 1, g.nx, g.ny, g.nz);
+      __syncthreads();
+    }
 #pragma unroll 1
     for (int t = 0; t < 2; ++t) {
-      const int x = x0 + lx, y = y0 + ly, z = z0 + 2 * t + lzt;
-      const bool valid = x < g.nx && y < g.ny && z < g.nz;
-      float f[3] = {0.f, 0.f, 0.f};
+      // lanes past the grid's end (partial bricks) compute a copy of the last
+      // in-grid point and store nothing
+      const int xr = x0 + lx, yr = y0 + ly, zr = z0 + 2 * t + lzt;
+      const bool valid = xr < g.nx && yr < g.ny && zr < g.nz;
+      const int x = min(xr, g.nx - 1), y = min(yr, g.ny - 1), z = min(zr, g.nz - 1);
+      float f[3];
       uint32_t w[64];
-      if (valid) {
-        if (!brick_prepare(g, pbox, vbox, x0, y0, z0, dth, backtrace, x, y, z, f, w)) {
-          bool clamped = false;
-          tc_prepare_split(g, phi0s, vel, dth, backtrace, true, x, y, z, f, w, clamped);
-        }
-      } else {
+      int soff;
+      const bool inbox = brick_depart(vbox, x - x0 + 4, y - y0 + 1, z - z0 + 1, x - x0 + 4, y - y0 + 2, z - z0 + 2,
+                                      dth, backtrace, f, soff);
+      if (__all_sync(0xffffffffu, inbox)) {
+        const uint32_t *q = pbox + soff;
 #pragma unroll
-        for (int e = 0; e < 64; ++e) w[e] = 0u;
+        for (int zz = 0; zz < 4; ++zz)
+#pragma unroll
+          for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
+            for (int xx = 0; xx < 4; ++xx) w[xx + 4 * yy + 16 * zz] = q[(zz * kPY + yy) * kPX + xx];
+      } else {  // the whole warp recomputes from global memory with clamped indices
+        bool clamped = false;
+        tc_prepare_split(g, phi0s, vel, dth, backtrace, true, x, y, z, f, w, clamped);
       }
       float a[64];
       if (!mma_tile(c, bar, parity, w, a)) {
