@@ -154,7 +154,8 @@ struct Ctx {
   uint64_t bdesc;     // descriptor of B at K-step 0
 };
 
-__device__ __forceinline__ void setup(uint8_t *sB, uint64_t *bar, uint32_t *tmem_slot, Ctx &c) {
+__device__ __forceinline__ void setup(uint8_t *sB, uint64_t *bar, uint32_t *tmem_slot, Ctx &c,
+                                      int tmem_cols = kTmemCols) {
   const int tid = threadIdx.x, warp = tid >> 5;
   for (int e = tid; e < kCoef * kK; e += blockDim.x) {
     const int n = e / kK, k = e % kK, j = k >> 1;  // B[n][k] = M[n][j]: coefficient n from stencil entry j
@@ -162,7 +163,7 @@ __device__ __forceinline__ void setup(uint8_t *sB, uint64_t *bar, uint32_t *tmem
     *reinterpret_cast<__nv_bfloat16 *>(sB + b_offset(n, k)) = __float2bfloat16_rn(w);
   }
   if (tid == 0) mbar_init(bar, 1);
-  if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
+  if (warp == 0) tmem_alloc(tmem_slot, tmem_cols);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   fence_before();
@@ -182,10 +183,9 @@ __device__ __forceinline__ uint32_t pack_split(float v) {
   return (uint32_t)__bfloat16_as_ushort(h) | ((uint32_t)__bfloat16_as_ushort(l) << 16);
 }
 
-// A (this lane: 64 packed words) -> TMEM, barrier, MMA by thread 0, bounded
-// wait, D -> regs.  Returns false (CTA-uniformly) when the wait timed out.
-__device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t parity, const uint32_t *w,
-                                         float *coef) {
+// A (this lane: 64 packed words) -> TMEM, barrier, MMA by thread 0 with its
+// completion signalled on `bar`.  Every thread of the CTA takes part.
+__device__ __forceinline__ void mma_issue(const Ctx &c, uint64_t *bar, const uint32_t *w) {
   tmem_st32(c.tmem + c.lane_off + 0, w);
   tmem_st32(c.tmem + c.lane_off + 32, w + 32);
   tmem_wait_st();
@@ -202,7 +202,12 @@ __device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t p
     }
     mma_commit(bar);
   }
-  // only the issuing thread polls the mbarrier; the others sleep in the barrier
+}
+
+// Bounded wait for the MMA issued last, then D -> regs.  Only the issuing
+// thread polls the mbarrier; the others sleep in the barrier.  Returns false
+// (CTA-uniformly) when the wait timed out.
+__device__ __forceinline__ bool mma_finish(const Ctx &c, uint64_t *bar, uint32_t parity, float *coef) {
   const bool ok = threadIdx.x == 0 ? mbar_wait(bar, parity) : true;
   const int all_ok = __syncthreads_and(ok ? 1 : 0);
   if (!all_ok) return false;
@@ -213,6 +218,12 @@ __device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t p
   tmem_wait_ld();
   fence_before();
   return true;
+}
+
+__device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t parity, const uint32_t *w,
+                                         float *coef) {
+  mma_issue(c, bar, w);
+  return mma_finish(c, bar, parity, coef);
 }
 
 __device__ __forceinline__ float horner3(const float *a, const float f[3]) {
@@ -385,15 +396,20 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_split_kernel(Geom g, const uin
 // departure (or midpoint) leaves the box -- per-component CFL >= 1 -- take
 // the global-memory path.  TMA x coordinates are multiples of 4 elements
 // (16-byte rule); nothing starts a store at a negative coordinate.
-constexpr int kBX = 32, kBY = 2, kBZ = 4;               // brick = 256 points = 2 MMA tiles
+constexpr int kBX = 32, kBY = 4, kBZ = 8;               // brick = 1024 points = 4 steps of 2 MMA tiles
 constexpr int kPX = kBX + 8, kPY = kBY + 4, kPZ = kBZ + 4;  // phi box (halo 4 | 2 | 2)
 constexpr int kVX = kBX + 8, kVY = kBY + 2, kVZ = kBZ + 2;  // velocity box (halo 4 | 1 | 1)
 constexpr int kPhiBoxBytes = kPX * kPY * kPZ * 4;
 constexpr int kVelBoxBytes = 3 * kVX * kVY * kVZ * 4;
 constexpr int kBufBytes = kPhiBoxBytes + kVelBoxBytes;
-constexpr int kBrickSmem = kBBytes + 2 * kBufBytes + 64;
-static_assert(kBrickSmem <= kDynSmem, "brick buffers exceed the CTA's shared memory budget");
+constexpr int kBrickTmemCols = 256;                      // two tiles: A0 D0 | A1 D1
+constexpr int kBrickSmem = kBBytes + 2 * kBufBytes + 80;  // + 9 mbarriers and the TMEM slot
+// 2 CTAs per SM (2 x 256 TMEM columns); a third never fits, so no CTA waits in tcgen05.alloc
+constexpr int kBrickDynSmem = 105 * 1024;
+static_assert(kBrickSmem <= kBrickDynSmem && 3 * (kBrickDynSmem + 1024) > 228 * 1024,
+              "brick shared memory must admit exactly two CTAs per SM");
 static_assert(kPhiBoxBytes % 128 == 0 && kBufBytes % 128 == 0, "TMA destinations must stay 128-byte aligned");
+static_assert(3 * kVX <= 256 && kPX <= 256 && kPY <= 256 && kPZ <= 256, "TMA box dimensions are at most 256");
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
@@ -442,48 +458,39 @@ __device__ __forceinline__ void issue_brick(const BrickGrid &bg, int b, uint8_t 
 // clamped interpolation indices read (Common/InterpolateVelocity.c and
 // Common/LevelSetMethod.c clamp i, j, k to the grid independently).  A
 // box-local read at an unclamped index then equals a global read at the
-// clamped index, so the per-point code needs no clamping.  Passes run x, y, z,
-// each reading what the one before wrote, which replicates edges and corners
-// like per-axis clamping.  The box is [DZ][DY][DX][C] 32-bit words whose cell
-// (0,0,0) sits at grid point (gx0, gy0, gz0); in-grid cells of each axis are a
-// non-empty range because the brick's own points are in the grid.  Only
-// CTA-uniform branches; every thread takes part.
+// clamped index, so the per-point code needs no clamping.  One pass per axis
+// (x, y, z in that order, a CTA barrier between passes, each reading what the
+// one before wrote), which replicates edges and corners like per-axis
+// clamping.  The box is [DZ][DY][DX][C] 32-bit words whose cell (0,0,0) sits
+// at grid point o[0..2]; in-grid cells of each axis are a non-empty range
+// because the brick's own points are in the grid.  Run by threads 0 ..
+// nthreads-1, together.  Returns whether the pass had anything to do (uniform
+// over those threads).
 template <int DX, int DY, int DZ, int C>
-__device__ __forceinline__ void replicate_box_edges(uint32_t *box, int gx0, int gy0, int gz0, int nx, int ny,
-                                                    int nz) {
-  const int xl = min(max(-gx0, 0), DX), xh = min(max(nx - gx0, 0), DX);  // in-grid columns [xl, xh)
-  const int yl = min(max(-gy0, 0), DY), yh = min(max(ny - gy0, 0), DY);
-  const int zl = min(max(-gz0, 0), DZ), zh = min(max(nz - gz0, 0), DZ);
-  const int ox = xl + (DX - xh), oy = yl + (DY - yh), oz = zl + (DZ - zh);  // out-of-grid counts
-  if (ox) {
-    const int total = ox * DY * DZ * C;
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-      const int k = i % C, r = i / C, j = r % ox, row = r / ox;
-      const int col = j < xl ? j : xh + (j - xl), src = j < xl ? xl : xh - 1;
-      box[(row * DX + col) * C + k] = box[(row * DX + src) * C + k];
-    }
-    __syncthreads();
+__device__ __forceinline__ bool replicate_pass(uint32_t *box, int axis, const int o[3], const int n[3],
+                                               int nthreads) {
+  constexpr int D[3] = {DX, DY, DZ};
+  const int dim = D[axis];
+  const int lo = min(max(-o[axis], 0), dim), hi = min(max(n[axis] - o[axis], 0), dim);  // in-grid [lo, hi)
+  const int out = lo + (dim - hi);
+  if (!out) return false;
+  // a "line" is the stride-1 run of words inside one unit of this axis: C
+  // words for x, one row (DX*C) for y, one plane (DY*DX*C) for z; "lines"
+  // repeats over the slower axes
+  const int inner = axis == 0 ? C : axis == 1 ? DX * C : DY * DX * C;
+  const int lines = axis == 0 ? DY * DZ : axis == 1 ? DZ : 1;
+  const int total = out * inner * lines;
+  for (int i = threadIdx.x; i < total; i += nthreads) {
+    const int w = i % inner, r = i / inner, j = r % out, line = r / out;
+    const int dst = j < lo ? j : hi + (j - lo), src = j < lo ? lo : hi - 1;
+    const int base = line * dim * inner + w;
+    box[base + dst * inner] = box[base + src * inner];
   }
-  if (oy) {
-    constexpr int W = DX * C;
-    const int total = oy * DZ * W;
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-      const int w = i % W, r = i / W, j = r % oy, plane = r / oy;
-      const int row = j < yl ? j : yh + (j - yl), src = j < yl ? yl : yh - 1;
-      box[(plane * DY + row) * W + w] = box[(plane * DY + src) * W + w];
-    }
-    __syncthreads();
-  }
-  if (oz) {
-    constexpr int P = DY * DX * C;
-    const int total = oz * P;
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-      const int w = i % P, j = i / P;
-      const int plane = j < zl ? j : zh + (j - zl), src = j < zl ? zl : zh - 1;
-      box[plane * P + w] = box[src * P + w];
-    }
-  }
-  if (ox | oy | oz) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // before TMA refills the buffer
+  return true;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // Front half of one point from the staged, edge-replicated boxes: node
@@ -493,15 +500,19 @@ __device__ __forceinline__ void replicate_box_edges(uint32_t *box, int gx0, int 
 // or the stencil leaves the box (per-component CFL >= 1): the warp then takes
 // the global path.  The arithmetic is the clamped global path's, operation for
 // operation (explicit roundings), so both give the same bits.
+template <int BT>
 __device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int vx, int vy, int vz, int px, int py,
-                                             int pz, const float dth[3], int backtrace, float f[3], int &soff) {
+                                             int pz, const float dth[3], float f[3], int &soff) {
   constexpr int SX = 3, SY = 3 * kVX, SZ = 3 * kVX * kVY;
   const float *vb = vbox + (vz * kVY + vy) * (3 * kVX) + 3 * vx;
   float U[3] = {face_mean(vb[0], vb[SX]), face_mean(vb[1], vb[SY + 1]), face_mean(vb[2], vb[SZ + 2])};
-  if (backtrace == DCELL_MIDPOINT) {
+  bool near = true;
+  if (BT == DCELL_MIDPOINT) {
     const float dl[3] = {rmul(rmul(-0.5f, U[0]), dth[0]), rmul(rmul(-0.5f, U[1]), dth[1]),
                          rmul(rmul(-0.5f, U[2]), dth[2])};
-    if (fabsf(dl[0]) >= 0.5f || fabsf(dl[1]) >= 0.5f || fabsf(dl[2]) >= 0.5f) return false;
+    // a midpoint half a cell or more from the node may leave the box: the
+    // offsets below are clamped to stay in it and the point is reported out
+    near = fabsf(dl[0]) < 0.5f && fabsf(dl[1]) < 0.5f && fabsf(dl[2]) < 0.5f;
     // Along a component's own (staggered) axis the midpoint lies in [X, X+1):
     // floor 0, fraction t.  Across the other two axes the node-centred
     // fraction and floor are shared by both components.
@@ -513,7 +524,7 @@ __device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int
       const float t = dl[a] + 0.f;
       const float fl = floorf(t);
       sn[a] = t - fl;
-      on[a] = (int)fl * S[a];
+      on[a] = min(max((int)fl, -1), 0) * S[a];
       sp[a] = dl[a] + 0.5f;
     }
 #pragma unroll
@@ -533,114 +544,227 @@ __device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int
     f[a] = t - fl;
   }
   soff = (cl[2] * kPY + cl[1]) * kPX + cl[0];
-  return (unsigned)cl[0] <= (unsigned)(kPX - 4) && (unsigned)cl[1] <= (unsigned)(kPY - 4) &&
+  return near && (unsigned)cl[0] <= (unsigned)(kPX - 4) && (unsigned)cl[1] <= (unsigned)(kPY - 4) &&
          (unsigned)cl[2] <= (unsigned)(kPZ - 4);
 }
 
-__global__ void __launch_bounds__(kTile, 4) sl_tc_brick_kernel(const __grid_constant__ CUtensorMap tm_phi,
-                                                               const __grid_constant__ CUtensorMap tm_vel, Geom g,
-                                                               BrickGrid bg, const uint32_t *__restrict__ phi0s,
-                                                               const float *__restrict__ vel, float dt,
-                                                               int backtrace, float *__restrict__ phi,
-                                                               uint32_t *__restrict__ phis, int *flags) {
+// Dense-grid stepper over TMA-staged bricks.
+//
+// Each CTA owns bricks blockIdx.x, blockIdx.x + gridDim.x, ... (32 x 4 x 8
+// points, 4 steps each); their boxes are double-buffered with the next brick
+// in flight.  Four compute warps carry two points per thread and step -- the
+// same (x, y) in two consecutive z planes -- held in two TMEM stages (A | D
+// columns 0-127 and 128-255); a fifth warp only issues the MMAs and the TMA
+// loads.  Warps are decoupled by mbarriers, not CTA barriers:
+//
+//   compute warp, step j:
+//     a. A rows of point a -> stage 0, arrive on afull[0]
+//     b. A rows of point b -> stage 1, arrive on afull[1]
+//     c. departures of step j+1's two points (overlaps both MMAs)
+//     d. wait dfull[0]: coefficients -> value of point a; same for b
+//   issuer, step j: for each stage, wait afull[s] (all four warps), MMA,
+//     commit to dfull[s]; after stage 1 of a brick's last step, refill that
+//     brick's buffer with the brick two ahead.
+//
+// A stage's A columns are rewritten only after the writing warp saw that
+// stage's MMA complete (d of the step before); its D columns are overwritten
+// only after every warp arrived on afull for the next step, which each does
+// after reading D.  A buffer is refilled only after afull[1] of its brick's
+// last step: every warp has then gathered from it for the last time (its
+// departures were computed one step earlier).  Every wait is bounded; a warp
+// that gives up raises FLAG_WAIT_TIMEOUT and leaves, and the others then give
+// up at their next wait.  Before the CTA ends, the issuer waits for its last
+// TMA load per buffer and its last commit per stage.
+constexpr int kBrickThreads = kTile + 32;
+
+template <int BT>
+__global__ void __launch_bounds__(kBrickThreads, 2)
+    sl_tc_brick_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel, Geom g,
+                       BrickGrid bg, const uint32_t *__restrict__ phi0s, const float *__restrict__ vel, float dt,
+                       float *__restrict__ phi, uint32_t *__restrict__ phis, int *flags) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t *sB = smem;
   uint8_t *const buf0 = smem + kBBytes, *const buf1 = smem + kBBytes + kBufBytes;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kBBytes + 2 * kBufBytes);
-  uint64_t *tbar = bar + 1;  // two TMA barriers
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 3);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kBBytes + 2 * kBufBytes);
+  uint64_t *const unused = bars + 0;  // setup() initialises one MMA barrier; this kernel uses its own
+  uint64_t *const afull = bars + 1, *const dfull = bars + 3, *const tbar = bars + 5, *const fixbar = bars + 7;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 8);
   if (threadIdx.x == 0) {
+    mbar_init(&afull[0], 4);
+    mbar_init(&afull[1], 4);
+    mbar_init(&dfull[0], 1);
+    mbar_init(&dfull[1], 1);
     mbar_init(&tbar[0], 1);
     mbar_init(&tbar[1], 1);
-    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_phi)) : "memory");
-    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tm_vel)) : "memory");
+    mbar_init(fixbar, kTile);
   }
   Ctx c;
-  setup(sB, bar, tmem_slot, c);  // B operand, MMA barrier, TMEM; ends with a CTA barrier
+  setup(sB, unused, tmem_slot, c, kBrickTmemCols);  // B operand, TMEM; ends with a CTA barrier
 
-  const float dth[3] = {dt / (float)g.hx, dt / (float)g.hy, dt / (float)g.hz};
   const int nbricks = bg.nbx * bg.nby * bg.nbz;
-  const int lx = threadIdx.x & (kBX - 1), ly = (threadIdx.x >> 5) & 1, lzt = threadIdx.x >> 6;  // tile: 32x2x2
-  uint32_t parity = 0;
-  uint32_t uses0 = 0u, uses1 = 0u;  // completed phases per TMA buffer
-  bool pending0 = false, pending1 = false;
-  bool timeout = false;
-  int it = 0;
-  if (threadIdx.x == 0 && (int)blockIdx.x < nbricks) issue_brick(bg, blockIdx.x, buf0, &tm_phi, &tm_vel, &tbar[0]);
-  pending0 = (int)blockIdx.x < nbricks;
-  for (int b = blockIdx.x; b < nbricks; b += gridDim.x, ++it) {
-    const bool odd = it & 1;
-    uint8_t *const cbuf = odd ? buf1 : buf0;
-    const int nb = b + gridDim.x;
-    if (threadIdx.x == 0 && nb < nbricks)
-      issue_brick(bg, nb, odd ? buf0 : buf1, &tm_phi, &tm_vel, odd ? &tbar[0] : &tbar[1]);
-    if (odd) pending0 = nb < nbricks; else pending1 = nb < nbricks;
-    const bool ok = mbar_wait(odd ? &tbar[1] : &tbar[0], (odd ? uses1 : uses0) & 1u);
-    if (!__syncthreads_and(ok ? 1 : 0)) {
-      timeout = true;
-      break;
+  const int nmine = (int)blockIdx.x < nbricks ? (nbricks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int nsteps = 4 * nmine;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool err = false;
+
+  if (warp == 4) {  // ---------------- issuer ----------------
+    if (lane == 0) {
+      int tma_issued[2] = {0, 0}, mma_issued[2] = {0, 0};
+      if (nmine > 0) { issue_brick(bg, blockIdx.x, buf0, &tm_phi, &tm_vel, &tbar[0]); tma_issued[0] = 1; }
+      if (nmine > 1) { issue_brick(bg, blockIdx.x + gridDim.x, buf1, &tm_phi, &tm_vel, &tbar[1]); tma_issued[1] = 1; }
+      constexpr uint32_t idesc = instr_desc_bf16(kTile, kCoef);
+      for (int j = 0; j < nsteps && !err; ++j) {
+#pragma unroll
+        for (int st = 0; st < 2; ++st) {
+          if (!mbar_wait(&afull[st], (uint32_t)j & 1u)) { err = true; break; }
+          fence_after();
+#pragma unroll
+          for (int kk = 0; kk < kK / 16; ++kk)
+            mma_bf16(c.tmem + 128 * st + 64, c.tmem + 128 * st + (uint32_t)(kk * 8),
+                     c.bdesc + (uint64_t)((kk * 256) >> 4), idesc, kk > 0 ? 1u : 0u);
+          mma_commit(&dfull[st]);
+          ++mma_issued[st];
+        }
+        const int k = j >> 2;
+        if (!err && (j & 3) == 3 && k + 2 < nmine) {  // brick k read for the last time: refill with brick k+2
+          issue_brick(bg, (int)blockIdx.x + (k + 2) * (int)gridDim.x, k & 1 ? buf1 : buf0, &tm_phi, &tm_vel,
+                      k & 1 ? &tbar[1] : &tbar[0]);
+          ++tma_issued[k & 1];
+        }
+      }
+      // nothing of this CTA may still be in flight when its TMEM and shared memory go away
+      bool ok = true;
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        if (tma_issued[b]) ok &= mbar_wait(&tbar[b], (uint32_t)(tma_issued[b] - 1) & 1u);
+        if (mma_issued[b]) ok &= mbar_wait(&dfull[b], (uint32_t)(mma_issued[b] - 1) & 1u);
+      }
+      if (err || !ok) raise_flag(flags, FLAG_WAIT_TIMEOUT);
     }
-    if (odd) { pending1 = false; ++uses1; } else { pending0 = false; ++uses0; }
-    int x0, y0, z0;
-    brick_origin(bg, b, x0, y0, z0);
-    uint32_t *pbox = reinterpret_cast<uint32_t *>(cbuf);
-    const float *vbox = reinterpret_cast<const float *>(cbuf + kPhiBoxBytes);
-    if (x0 < 4 || x0 + kPX - 4 > g.nx || y0 < 2 || y0 + kPY - 2 > g.ny || z0 < 2 || z0 + kPZ - 2 > g.nz) {
-      replicate_box_edges<kPX, kPY, kPZ, 1>(pbox, x0 - 4, y0 - 2, z0 - 2, g.nx, g.ny, g.nz);
-      replicate_box_edges<kVX, kVY, kVZ, 3>(reinterpret_cast<uint32_t *>(cbuf + kPhiBoxBytes), x0 - 4, y0 - 1,
-                                            z0 - 1, g.nx, g.ny, g.nz);
-      __syncthreads();
-    }
-#pragma unroll 1
-    for (int t = 0; t < 2; ++t) {
-      // lanes past the grid's end (partial bricks) compute a copy of the last
-      // in-grid point and store nothing
-      const int xr = x0 + lx, yr = y0 + ly, zr = z0 + 2 * t + lzt;
-      const bool valid = xr < g.nx && yr < g.ny && zr < g.nz;
-      const int x = min(xr, g.nx - 1), y = min(yr, g.ny - 1), z = min(zr, g.nz - 1);
-      float f[3];
+  } else {  // ---------------- compute warps ----------------
+    const float dth[3] = {dt / (float)g.hx, dt / (float)g.hy, dt / (float)g.hz};
+    const int lx = lane, ly = warp;  // a tile: 32 x 4 points of one z plane
+    const int plane = g.nx * g.ny;
+    const int nn[3] = {g.nx, g.ny, g.nz};
+    uint32_t fixphase = 0;
+
+    // Boxes of brick k staged (and edge-replicated where they cross the grid).
+    auto open_brick = [&](int k, int &x0, int &y0, int &z0) -> bool {
+      const bool odd = k & 1;
+      if (!mbar_wait(odd ? &tbar[1] : &tbar[0], (uint32_t)(k >> 1) & 1u)) return false;
+      brick_origin(bg, (int)blockIdx.x + k * (int)gridDim.x, x0, y0, z0);
+      if (x0 < 4 || x0 + kPX - 4 > g.nx || y0 < 2 || y0 + kPY - 2 > g.ny || z0 < 2 || z0 + kPZ - 2 > g.nz) {
+        uint8_t *cbuf = odd ? buf1 : buf0;
+        const int op[3] = {x0 - 4, y0 - 2, z0 - 2}, ov[3] = {x0 - 4, y0 - 1, z0 - 1};
+        for (int axis = 0; axis < 3; ++axis) {
+          const bool a = replicate_pass<kPX, kPY, kPZ, 1>(reinterpret_cast<uint32_t *>(cbuf), axis, op, nn, kTile);
+          const bool b = replicate_pass<kVX, kVY, kVZ, 3>(reinterpret_cast<uint32_t *>(cbuf + kPhiBoxBytes), axis,
+                                                          ov, nn, kTile);
+          if (!(a || b)) continue;
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes before a later TMA refill
+          mbar_arrive(fixbar);
+          const bool ok = mbar_wait(fixbar, fixphase);
+          fixphase ^= 1u;
+          if (!ok) return false;
+        }
+      }
+      return true;
+    };
+    // Departures of step j's two points from brick (x0, y0, z0)'s boxes; lanes
+    // past the grid's end (partial bricks) compute a copy of the last in-grid
+    // point and store nothing.  Returns whether the whole warp stays in the boxes.
+    auto depart2 = [&](int j, int x0, int y0, int z0, float fa[3], float fb[3], int &sa, int &sb) -> bool {
+      const float *vbox = reinterpret_cast<const float *>(((j >> 2) & 1 ? buf1 : buf0) + kPhiBoxBytes);
+      const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
+      const int za = min(z0 + 2 * (j & 3), g.nz - 1), zb = min(z0 + 2 * (j & 3) + 1, g.nz - 1);
+      const bool ia = brick_depart<BT>(vbox, x - x0 + 4, y - y0 + 1, za - z0 + 1, x - x0 + 4, y - y0 + 2,
+                                       za - z0 + 2, dth, fa, sa);
+      const bool ib = brick_depart<BT>(vbox, x - x0 + 4, y - y0 + 1, zb - z0 + 1, x - x0 + 4, y - y0 + 2,
+                                       zb - z0 + 2, dth, fb, sb);
+      return __all_sync(0xffffffffu, ia && ib);
+    };
+    // A rows of one point -> TMEM stage `st`, then this warp's arrival.
+    auto stage_rows = [&](int j, int x0, int y0, int z0, int pt, bool boxed, int soff, float f[3], int st) {
       uint32_t w[64];
-      int soff;
-      const bool inbox = brick_depart(vbox, x - x0 + 4, y - y0 + 1, z - z0 + 1, x - x0 + 4, y - y0 + 2, z - z0 + 2,
-                                      dth, backtrace, f, soff);
-      if (__all_sync(0xffffffffu, inbox)) {
-        const uint32_t *q = pbox + soff;
+      if (boxed) {
+        const uint32_t *q = reinterpret_cast<const uint32_t *>((j >> 2) & 1 ? buf1 : buf0) + soff;
 #pragma unroll
-        for (int zz = 0; zz < 4; ++zz)
-#pragma unroll
-          for (int yy = 0; yy < 4; ++yy)
-#pragma unroll
-            for (int xx = 0; xx < 4; ++xx) w[xx + 4 * yy + 16 * zz] = q[(zz * kPY + yy) * kPX + xx];
+        for (int e = 0; e < 64; ++e) w[e] = q[((e >> 4) * kPY + ((e >> 2) & 3)) * kPX + (e & 3)];
       } else {  // the whole warp recomputes from global memory with clamped indices
+        const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
+        const int z = min(z0 + 2 * (j & 3) + pt, g.nz - 1);
         bool clamped = false;
-        tc_prepare_split(g, phi0s, vel, dth, backtrace, true, x, y, z, f, w, clamped);
+        tc_prepare_split(g, phi0s, vel, dth, BT, true, x, y, z, f, w, clamped);
       }
-      float a[64];
-      if (!mma_tile(c, bar, parity, w, a)) {
-        timeout = true;
-        break;
-      }
-      parity ^= 1u;
-      if (valid) {
-        const int p = (z * g.ny + y) * g.nx + x;
-        const float v = horner3(a, f);
-        phi[p] = v;
-        if (phis) phis[p] = pack_split(v);
-      }
+      __syncwarp();  // the TMEM store is warp-collective
+      tmem_st32(c.tmem + c.lane_off + 128 * st, w);
+      tmem_st32(c.tmem + c.lane_off + 128 * st + 32, w + 32);
+      tmem_wait_st();
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&afull[st]);
+    };
+
+    int x0 = 0, y0 = 0, z0 = 0;
+    float fa[3] = {0.f, 0.f, 0.f}, fb[3] = {0.f, 0.f, 0.f};
+    int sa = 0, sb = 0;
+    bool boxed = true;
+    if (nsteps > 0) {
+      err = !open_brick(0, x0, y0, z0);
+      if (__any_sync(0xffffffffu, err)) err = true;
+      else boxed = depart2(0, x0, y0, z0, fa, fb, sa, sb);
     }
-    if (timeout) break;
-    __syncthreads();  // everyone is done with buf[cur] before it is refilled
+    for (int j = 0; j < nsteps && !err; ++j) {
+      const int k = j >> 2;
+      // a, b: A rows of both points into their stages
+      stage_rows(j, x0, y0, z0, 0, boxed, sa, fa, 0);
+      stage_rows(j, x0, y0, z0, 1, boxed, sb, fb, 1);
+      // c: next step's departures while the tensor core works
+      int nx0 = x0, ny0 = y0, nz0 = z0;
+      float fan[3] = {0.f, 0.f, 0.f}, fbn[3] = {0.f, 0.f, 0.f};
+      int san = 0, sbn = 0;
+      bool boxedn = true;
+      if (j + 1 < nsteps) {
+        if (((j + 1) & 3) == 0) err = !open_brick(k + 1, nx0, ny0, nz0);
+        if (__any_sync(0xffffffffu, err)) err = true;
+        else boxedn = depart2(j + 1, nx0, ny0, nz0, fan, fbn, san, sbn);
+      }
+      // d: both stages' coefficients -> values
+      const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
+      const bool xy_valid = x0 + lx < g.nx && y0 + ly < g.ny;
+      const int zr = z0 + 2 * (j & 3);
+      const int p0 = (min(zr, g.nz - 1) * g.ny + y) * g.nx + x;
+#pragma unroll
+      for (int st = 0; st < 2; ++st) {
+        const bool ok = mbar_wait(&dfull[st], (uint32_t)j & 1u);
+        if (__any_sync(0xffffffffu, !ok)) { err = true; break; }
+        fence_after();
+        float a[64];
+        uint32_t *u = reinterpret_cast<uint32_t *>(a);
+        tmem_ld32(c.tmem + c.lane_off + 128 * st + 64, u);
+        tmem_ld32(c.tmem + c.lane_off + 128 * st + 96, u + 32);
+        tmem_wait_ld();
+        const float v = horner3(a, st == 0 ? fa : fb);
+        if (xy_valid && zr + st < g.nz) {
+          const int pt = p0 + st * plane;
+          phi[pt] = v;
+          if (phis) phis[pt] = pack_split(v);
+        }
+      }
+      fence_before();
+      x0 = nx0; y0 = ny0; z0 = nz0;
+      fa[0] = fan[0]; fa[1] = fan[1]; fa[2] = fan[2];
+      fb[0] = fbn[0]; fb[1] = fbn[1]; fb[2] = fbn[2];
+      sa = san; sb = sbn;
+      boxed = boxedn;
+    }
+    if (err) raise_flag(flags, FLAG_WAIT_TIMEOUT);
   }
-  if (timeout && threadIdx.x == 0) {
-    raise_flag(flags, FLAG_WAIT_TIMEOUT);
-    // let every TMA still in flight land before the CTA's shared memory goes away (bounded waits)
-    if (pending0) mbar_wait(&tbar[0], uses0 & 1u);
-    if (pending1) mbar_wait(&tbar[1], uses1 & 1u);
-  }
+  __syncwarp();  // the issuer warp's other lanes wait here for lane 0
   fence_before();
   __syncthreads();
   fence_after();
-  if ((threadIdx.x >> 5) == 0) tmem_dealloc(c.tmem, kTmemCols);
+  if (warp == 0) tmem_dealloc(c.tmem, kBrickTmemCols);
 }
 
 // Batched cells: a persistent CTA walks a packed queue of 128-point tiles
@@ -838,8 +962,10 @@ int launch_sl_tc_brick(const Geom &g, const uint32_t *phi0s, const float *vel, d
                        uint32_t *phis, int *flags, cudaStream_t st) {
   static bool configured = false;
   if (!configured) {
-    DCELL_CUDA_CHECK(
-        cudaFuncSetAttribute(tc::sl_tc_brick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kDynSmem));
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::sl_tc_brick_kernel<DCELL_EULER>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kBrickDynSmem));
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::sl_tc_brick_kernel<DCELL_MIDPOINT>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kBrickDynSmem));
     configured = true;
   }
   CUtensorMap tm_phi, tm_vel;
@@ -858,10 +984,14 @@ int launch_sl_tc_brick(const Geom &g, const uint32_t *phi0s, const float *vel, d
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  long long grid = 4LL * sms;
+  long long grid = 2LL * sms;
   if (grid > nbricks) grid = nbricks;
-  tc::sl_tc_brick_kernel<<<(int)grid, tc::kTile, tc::kDynSmem, st>>>(tm_phi, tm_vel, g, bg, phi0s, vel, (float)dt,
-                                                                       backtrace, phi, phis, flags);
+  if (backtrace == DCELL_MIDPOINT)
+    tc::sl_tc_brick_kernel<DCELL_MIDPOINT><<<(int)grid, tc::kBrickThreads, tc::kBrickDynSmem, st>>>(
+        tm_phi, tm_vel, g, bg, phi0s, vel, (float)dt, phi, phis, flags);
+  else
+    tc::sl_tc_brick_kernel<DCELL_EULER><<<(int)grid, tc::kBrickThreads, tc::kBrickDynSmem, st>>>(
+        tm_phi, tm_vel, g, bg, phi0s, vel, (float)dt, phi, phis, flags);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 

@@ -239,15 +239,18 @@ def test_tc_split_band_mode_and_multistep(cuda):
     assert float(err.max()) <= 1e-5, float(err.max())
 
 
+@pytest.mark.parametrize("shape", [(40, 48, 64), (37, 45, 68), (12, 8, 40)])
 @pytest.mark.parametrize("cfl_scale", [1.0, 3.0])
-def test_tc_brick_path_equals_gather_path(cuda, cfl_scale):
+def test_tc_brick_path_equals_gather_path(cuda, cfl_scale, shape):
     """Dense split-state steps on grids with nx % 4 == 0 run the TMA-staged
     brick kernel; a band listing every point runs the global-gather kernel.
-    Both must give the same bits (3x the CFL exercises the brick fallbacks)."""
-    nz, ny, nx = 40, 48, 64
+    Both must give the same bits (3x the CFL exercises the brick fallbacks;
+    the odd shapes end in partial bricks on every axis, the smallest is one
+    brick box)."""
+    nz, ny, nx = shape
     h = 1.0 / 64
-    phi = fields.sphere_sdf(64, device=cuda)[:nz, :ny, :nx].contiguous().float()
-    vel = fields.deformation_velocity(64, device=cuda)[:nz, :ny, :nx].contiguous().float()
+    phi = fields.sphere_sdf(72, device=cuda)[:nz, :ny, :nx].contiguous().float()
+    vel = fields.deformation_velocity(72, device=cuda)[:nz, :ny, :nx].contiguous().float()
     dt = cfl_scale * fields.cfl_dt((2.0, 1.0, 1.0), h)
     spl = L.split_bf16(phi)
     for bt in ("midpoint", "euler"):
