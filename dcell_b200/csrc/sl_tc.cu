@@ -90,6 +90,28 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   return false;
 }
 
+// Bounded wait that lets the hardware suspend the thread until the phase
+// completes (or `kSleepNs` pass) instead of spinning: pipeline waits inside
+// the brick kernel, where warps routinely wait a few hundred cycles.  At most
+// kSleepLimit rounds (well under a second in all).
+constexpr uint32_t kSleepNs = 20000;
+constexpr unsigned kSleepLimit = 1u << 15;
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (unsigned it = 0; it < kSleepLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity), "r"(kSleepNs)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -124,6 +146,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
       "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
       : DCELL_W8(0), DCELL_W8(8), DCELL_W8(16), DCELL_W8(24)
+      : "r"(taddr)
+      : "memory");
+}
+// v[0..15] <- 16 consecutive 32-bit columns of this thread's lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t *v) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : DCELL_W8(0), DCELL_W8(8)
       : "r"(taddr)
       : "memory");
 }
@@ -224,6 +255,18 @@ __device__ __forceinline__ bool mma_tile(const Ctx &c, uint64_t *bar, uint32_t p
                                          float *coef) {
   mma_issue(c, bar, w);
   return mma_finish(c, bar, parity, coef);
+}
+
+// One z-slice of horner3: the y/x polynomial of coefficients r[4j + i].
+__device__ __forceinline__ float horner_slice(const float *r, const float f[3]) {
+  float py = 0.f;
+#pragma unroll
+  for (int j = 3; j >= 0; --j) {
+    const float *q = r + 4 * j;
+    const float px = fmaf(fmaf(fmaf(q[3], f[0], q[2]), f[0], q[1]), f[0], q[0]);
+    py = fmaf(py, f[1], px);
+  }
+  return py;
 }
 
 __device__ __forceinline__ float horner3(const float *a, const float f[3]) {
@@ -403,7 +446,7 @@ constexpr int kPhiBoxBytes = kPX * kPY * kPZ * 4;
 constexpr int kVelBoxBytes = 3 * kVX * kVY * kVZ * 4;
 constexpr int kBufBytes = kPhiBoxBytes + kVelBoxBytes;
 constexpr int kBrickTmemCols = 256;                      // two tiles: A0 D0 | A1 D1
-constexpr int kBrickSmem = kBBytes + 2 * kBufBytes + 80;  // + 9 mbarriers and the TMEM slot
+constexpr int kBrickSmem = kBBytes + 2 * kBufBytes + 64;  // + 6 mbarriers and the TMEM slot
 // 2 CTAs per SM (2 x 256 TMEM columns); a third never fits, so no CTA waits in tcgen05.alloc
 constexpr int kBrickDynSmem = 105 * 1024;
 static_assert(kBrickSmem <= kBrickDynSmem && 3 * (kBrickDynSmem + 1024) > 228 * 1024,
@@ -558,23 +601,22 @@ __device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int
 // loads.  Warps are decoupled by mbarriers, not CTA barriers:
 //
 //   compute warp, step j:
-//     a. A rows of point a -> stage 0, arrive on afull[0]
-//     b. A rows of point b -> stage 1, arrive on afull[1]
-//     c. departures of step j+1's two points (overlaps both MMAs)
-//     d. wait dfull[0]: coefficients -> value of point a; same for b
-//   issuer, step j: for each stage, wait afull[s] (all four warps), MMA,
-//     commit to dfull[s]; after stage 1 of a brick's last step, refill that
-//     brick's buffer with the brick two ahead.
+//     a. A rows of both points -> their stages, arrive on afull
+//     b. departures of step j+1's two points (overlaps the MMAs)
+//     c. wait dfull: both points' coefficients -> values, evaluated together
+//   issuer, step j: wait afull (all four warps), both stages' MMAs, commit to
+//     dfull; after a brick's last step, refill that brick's buffer with the
+//     brick two ahead.
 //
-// A stage's A columns are rewritten only after the writing warp saw that
-// stage's MMA complete (d of the step before); its D columns are overwritten
-// only after every warp arrived on afull for the next step, which each does
-// after reading D.  A buffer is refilled only after afull[1] of its brick's
-// last step: every warp has then gathered from it for the last time (its
-// departures were computed one step earlier).  Every wait is bounded; a warp
-// that gives up raises FLAG_WAIT_TIMEOUT and leaves, and the others then give
-// up at their next wait.  Before the CTA ends, the issuer waits for its last
-// TMA load per buffer and its last commit per stage.
+// A stage's A columns are rewritten only after the writing warp saw the MMAs
+// complete (c of the step before); D columns are overwritten only after every
+// warp arrived on afull for the next step, which each does after reading D.
+// A buffer is refilled only after afull of its brick's last step: every warp
+// has then gathered from it for the last time (its departures were computed
+// one step earlier).  Every wait is bounded; a warp that gives up raises
+// FLAG_WAIT_TIMEOUT and leaves, and the others then give up at their next
+// wait.  Before the CTA ends, the issuer waits for its last TMA load per
+// buffer and its last commit.
 constexpr int kBrickThreads = kTile + 32;
 
 template <int BT>
@@ -587,13 +629,11 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
   uint8_t *const buf0 = smem + kBBytes, *const buf1 = smem + kBBytes + kBufBytes;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kBBytes + 2 * kBufBytes);
   uint64_t *const unused = bars + 0;  // setup() initialises one MMA barrier; this kernel uses its own
-  uint64_t *const afull = bars + 1, *const dfull = bars + 3, *const tbar = bars + 5, *const fixbar = bars + 7;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 8);
+  uint64_t *const afull = bars + 1, *const dfull = bars + 2, *const tbar = bars + 3, *const fixbar = bars + 5;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 6);
   if (threadIdx.x == 0) {
-    mbar_init(&afull[0], 4);
-    mbar_init(&afull[1], 4);
-    mbar_init(&dfull[0], 1);
-    mbar_init(&dfull[1], 1);
+    mbar_init(afull, 4);
+    mbar_init(dfull, 1);
     mbar_init(&tbar[0], 1);
     mbar_init(&tbar[1], 1);
     mbar_init(fixbar, kTile);
@@ -609,22 +649,21 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
 
   if (warp == 4) {  // ---------------- issuer ----------------
     if (lane == 0) {
-      int tma_issued[2] = {0, 0}, mma_issued[2] = {0, 0};
+      int tma_issued[2] = {0, 0}, mma_issued = 0;
       if (nmine > 0) { issue_brick(bg, blockIdx.x, buf0, &tm_phi, &tm_vel, &tbar[0]); tma_issued[0] = 1; }
       if (nmine > 1) { issue_brick(bg, blockIdx.x + gridDim.x, buf1, &tm_phi, &tm_vel, &tbar[1]); tma_issued[1] = 1; }
       constexpr uint32_t idesc = instr_desc_bf16(kTile, kCoef);
       for (int j = 0; j < nsteps && !err; ++j) {
+        if (!mbar_wait_sleep(afull, (uint32_t)j & 1u)) { err = true; break; }
+        fence_after();
 #pragma unroll
-        for (int st = 0; st < 2; ++st) {
-          if (!mbar_wait(&afull[st], (uint32_t)j & 1u)) { err = true; break; }
-          fence_after();
+        for (int st = 0; st < 2; ++st)
 #pragma unroll
           for (int kk = 0; kk < kK / 16; ++kk)
             mma_bf16(c.tmem + 128 * st + 64, c.tmem + 128 * st + (uint32_t)(kk * 8),
                      c.bdesc + (uint64_t)((kk * 256) >> 4), idesc, kk > 0 ? 1u : 0u);
-          mma_commit(&dfull[st]);
-          ++mma_issued[st];
-        }
+        mma_commit(dfull);
+        ++mma_issued;
         const int k = j >> 2;
         if (!err && (j & 3) == 3 && k + 2 < nmine) {  // brick k read for the last time: refill with brick k+2
           issue_brick(bg, (int)blockIdx.x + (k + 2) * (int)gridDim.x, k & 1 ? buf1 : buf0, &tm_phi, &tm_vel,
@@ -635,10 +674,9 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
       // nothing of this CTA may still be in flight when its TMEM and shared memory go away
       bool ok = true;
 #pragma unroll
-      for (int b = 0; b < 2; ++b) {
+      for (int b = 0; b < 2; ++b)
         if (tma_issued[b]) ok &= mbar_wait(&tbar[b], (uint32_t)(tma_issued[b] - 1) & 1u);
-        if (mma_issued[b]) ok &= mbar_wait(&dfull[b], (uint32_t)(mma_issued[b] - 1) & 1u);
-      }
+      if (mma_issued) ok &= mbar_wait(dfull, (uint32_t)(mma_issued - 1) & 1u);
       if (err || !ok) raise_flag(flags, FLAG_WAIT_TIMEOUT);
     }
   } else {  // ---------------- compute warps ----------------
@@ -651,7 +689,7 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     // Boxes of brick k staged (and edge-replicated where they cross the grid).
     auto open_brick = [&](int k, int &x0, int &y0, int &z0) -> bool {
       const bool odd = k & 1;
-      if (!mbar_wait(odd ? &tbar[1] : &tbar[0], (uint32_t)(k >> 1) & 1u)) return false;
+      if (!mbar_wait_sleep(odd ? &tbar[1] : &tbar[0], (uint32_t)(k >> 1) & 1u)) return false;
       brick_origin(bg, (int)blockIdx.x + k * (int)gridDim.x, x0, y0, z0);
       if (x0 < 4 || x0 + kPX - 4 > g.nx || y0 < 2 || y0 + kPY - 2 > g.ny || z0 < 2 || z0 + kPZ - 2 > g.nz) {
         uint8_t *cbuf = odd ? buf1 : buf0;
@@ -663,7 +701,7 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
           if (!(a || b)) continue;
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes before a later TMA refill
           mbar_arrive(fixbar);
-          const bool ok = mbar_wait(fixbar, fixphase);
+          const bool ok = mbar_wait_sleep(fixbar, fixphase);
           fixphase ^= 1u;
           if (!ok) return false;
         }
@@ -683,7 +721,7 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
                                        zb - z0 + 2, dth, fb, sb);
       return __all_sync(0xffffffffu, ia && ib);
     };
-    // A rows of one point -> TMEM stage `st`, then this warp's arrival.
+    // A rows of one point -> TMEM stage `st`.
     auto stage_rows = [&](int j, int x0, int y0, int z0, int pt, bool boxed, int soff, float f[3], int st) {
       uint32_t w[64];
       if (boxed) {
@@ -699,10 +737,6 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
       __syncwarp();  // the TMEM store is warp-collective
       tmem_st32(c.tmem + c.lane_off + 128 * st, w);
       tmem_st32(c.tmem + c.lane_off + 128 * st + 32, w + 32);
-      tmem_wait_st();
-      fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&afull[st]);
     };
 
     int x0 = 0, y0 = 0, z0 = 0;
@@ -716,10 +750,28 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     }
     for (int j = 0; j < nsteps && !err; ++j) {
       const int k = j >> 2;
-      // a, b: A rows of both points into their stages
-      stage_rows(j, x0, y0, z0, 0, boxed, sa, fa, 0);
-      stage_rows(j, x0, y0, z0, 1, boxed, sb, fb, 1);
-      // c: next step's departures while the tensor core works
+      // a: A rows of both points into their stages, then this warp's arrival.
+      // Where every lane's second stencil is its first one plane up (the
+      // usual case: both points depart from vertically adjacent cells), the
+      // warp gathers their 4 x 4 x 5 union once.
+      if (boxed && __all_sync(0xffffffffu, sb == sa + kPX * kPY)) {
+        const uint32_t *q = reinterpret_cast<const uint32_t *>(k & 1 ? buf1 : buf0) + sa;
+        uint32_t v[80];
+#pragma unroll
+        for (int e = 0; e < 80; ++e) v[e] = q[((e >> 4) * kPY + ((e >> 2) & 3)) * kPX + (e & 3)];
+        tmem_st32(c.tmem + c.lane_off + 0, v);
+        tmem_st32(c.tmem + c.lane_off + 32, v + 32);
+        tmem_st32(c.tmem + c.lane_off + 128, v + 16);
+        tmem_st32(c.tmem + c.lane_off + 160, v + 48);
+      } else {
+        stage_rows(j, x0, y0, z0, 0, boxed, sa, fa, 0);
+        stage_rows(j, x0, y0, z0, 1, boxed, sb, fb, 1);
+      }
+      tmem_wait_st();
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(afull);
+      // b: next step's departures while the tensor core works
       int nx0 = x0, ny0 = y0, nz0 = z0;
       float fan[3] = {0.f, 0.f, 0.f}, fbn[3] = {0.f, 0.f, 0.f};
       int san = 0, sbn = 0;
@@ -729,27 +781,35 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
         if (__any_sync(0xffffffffu, err)) err = true;
         else boxedn = depart2(j + 1, nx0, ny0, nz0, fan, fbn, san, sbn);
       }
-      // d: both stages' coefficients -> values
+      // c: both points' coefficients -> values, two z-slices per TMEM load round
       const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
       const bool xy_valid = x0 + lx < g.nx && y0 + ly < g.ny;
       const int zr = z0 + 2 * (j & 3);
       const int p0 = (min(zr, g.nz - 1) * g.ny + y) * g.nx + x;
+      const bool ok = mbar_wait_sleep(dfull, (uint32_t)j & 1u);
+      if (__any_sync(0xffffffffu, !ok)) { err = true; break; }
+      fence_after();
+      float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
 #pragma unroll
-      for (int st = 0; st < 2; ++st) {
-        const bool ok = mbar_wait(&dfull[st], (uint32_t)j & 1u);
-        if (__any_sync(0xffffffffu, !ok)) { err = true; break; }
-        fence_after();
-        float a[64];
-        uint32_t *u = reinterpret_cast<uint32_t *>(a);
-        tmem_ld32(c.tmem + c.lane_off + 128 * st + 64, u);
-        tmem_ld32(c.tmem + c.lane_off + 128 * st + 96, u + 32);
+      for (int kp = 1; kp >= 0; --kp) {
+        float ca[32], cb[32];
+        tmem_ld16(c.tmem + c.lane_off + 64 + 32 * kp + 16, reinterpret_cast<uint32_t *>(ca));
+        tmem_ld16(c.tmem + c.lane_off + 64 + 32 * kp, reinterpret_cast<uint32_t *>(ca + 16));
+        tmem_ld16(c.tmem + c.lane_off + 192 + 32 * kp + 16, reinterpret_cast<uint32_t *>(cb));
+        tmem_ld16(c.tmem + c.lane_off + 192 + 32 * kp, reinterpret_cast<uint32_t *>(cb + 16));
         tmem_wait_ld();
-        const float v = horner3(a, st == 0 ? fa : fb);
-        if (xy_valid && zr + st < g.nz) {
-          const int pt = p0 + st * plane;
-          phi[pt] = v;
-          if (phis) phis[pt] = pack_split(v);
-        }
+        va = fmaf(va, fa[2], horner_slice(ca, fa));
+        vb = fmaf(vb, fb[2], horner_slice(cb, fb));
+        va = fmaf(va, fa[2], horner_slice(ca + 16, fa));
+        vb = fmaf(vb, fb[2], horner_slice(cb + 16, fb));
+      }
+      if (xy_valid && zr < g.nz) {
+        phi[p0] = va;
+        if (phis) phis[p0] = pack_split(va);
+      }
+      if (xy_valid && zr + 1 < g.nz) {
+        phi[p0 + plane] = vb;
+        if (phis) phis[p0 + plane] = pack_split(vb);
       }
       fence_before();
       x0 = nx0; y0 = ny0; z0 = nz0;
