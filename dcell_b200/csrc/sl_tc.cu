@@ -136,6 +136,14 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t *v) {
       DCELL_R8(0), DCELL_R8(8), DCELL_R8(16), DCELL_R8(24)
       : "memory");
 }
+// 16 consecutive 32-bit columns of this thread's lane <- v[0..15]
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t *v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16};" ::"r"(taddr),
+      DCELL_R8(0), DCELL_R8(8)
+      : "memory");
+}
 #undef DCELL_R8
 
 #define DCELL_W8(b) "=r"(v[b + 0]), "=r"(v[b + 1]), "=r"(v[b + 2]), "=r"(v[b + 3]), "=r"(v[b + 4]), "=r"(v[b + 5]), \
@@ -591,6 +599,82 @@ __device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int
          (unsigned)cl[2] <= (unsigned)(kPZ - 4);
 }
 
+// brick_depart for a thread's two points: a at velocity-box cell (vx, vy, vz)
+// / phi-box cell (px, py, pz) and b one plane above it.  They share the w face
+// between them, and when their midpoint cells have the same floors (checked
+// over the warp) each velocity component's two trilinear stencils share a
+// layer: 12 corner loads instead of 16.  hdth = -dt/(2h) per axis, so
+// dl = U * hdth rounds exactly like (-U/2) * dt/h.  Same values and operations
+// as two brick_depart calls, so the same bits.
+template <int BT>
+__device__ __forceinline__ bool brick_depart2(const float *__restrict__ vbox, int vx, int vy, int vz, int px, int py,
+                                              int pz, const float dth[3], const float hdth[3], float fa[3],
+                                              float fb[3], int &sa, int &sb) {
+  constexpr int SX = 3, SY = 3 * kVX, SZ = 3 * kVX * kVY;
+  constexpr int S[3] = {SX, SY, SZ};
+  const float *va = vbox + (vz * kVY + vy) * (3 * kVX) + 3 * vx;  // b's node is va + SZ
+  const float wmid = va[SZ + 2];
+  float Ua[3] = {face_mean(va[0], va[SX]), face_mean(va[1], va[SY + 1]), face_mean(va[2], wmid)};
+  float Ub[3] = {face_mean(va[SZ], va[SZ + SX]), face_mean(va[SZ + 1], va[SZ + SY + 1]),
+                 face_mean(wmid, va[2 * SZ + 2])};
+  bool near = true;
+  if (BT == DCELL_MIDPOINT) {
+    float sna[3], spa[3], snb[3], spb[3];
+    int ona[3], onb[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float dla = rmul(Ua[a], hdth[a]), dlb = rmul(Ub[a], hdth[a]);
+      near = near && fabsf(dla) < 0.5f && fabsf(dlb) < 0.5f;
+      const float ta = dla + 0.f, tb = dlb + 0.f;
+      const float fla = floorf(ta), flb = floorf(tb);
+      sna[a] = ta - fla;
+      snb[a] = tb - flb;
+      ona[a] = min(max((int)fla, -1), 0) * S[a];
+      onb[a] = min(max((int)flb, -1), 0) * S[a];
+      spa[a] = dla + 0.5f;
+      spb[a] = dlb + 0.5f;
+    }
+    const bool same = ona[0] == onb[0] && ona[1] == onb[1] && ona[2] == onb[2];
+    if (__all_sync(0xffffffffu, same)) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float s3a[3] = {d == 0 ? spa[0] : sna[0], d == 1 ? spa[1] : sna[1], d == 2 ? spa[2] : sna[2]};
+        const float s3b[3] = {d == 0 ? spb[0] : snb[0], d == 1 ? spb[1] : snb[1], d == 2 ? spb[2] : snb[2]};
+        const float *q = va + d + (d == 0 ? 0 : ona[0]) + (d == 1 ? 0 : ona[1]) + (d == 2 ? 0 : ona[2]);
+        const float m00 = q[SZ], m10 = q[SZ + SX], m01 = q[SZ + SY], m11 = q[SZ + SY + SX];  // shared layer
+        Ua[d] = trilerp(q[0], q[SX], q[SY], q[SY + SX], m00, m10, m01, m11, s3a);
+        Ub[d] = trilerp(m00, m10, m01, m11, q[2 * SZ], q[2 * SZ + SX], q[2 * SZ + SY], q[2 * SZ + SY + SX], s3b);
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float s3a[3] = {d == 0 ? spa[0] : sna[0], d == 1 ? spa[1] : sna[1], d == 2 ? spa[2] : sna[2]};
+        const float s3b[3] = {d == 0 ? spb[0] : snb[0], d == 1 ? spb[1] : snb[1], d == 2 ? spb[2] : snb[2]};
+        const float *qa = va + d + (d == 0 ? 0 : ona[0]) + (d == 1 ? 0 : ona[1]) + (d == 2 ? 0 : ona[2]);
+        const float *qb = va + SZ + d + (d == 0 ? 0 : onb[0]) + (d == 1 ? 0 : onb[1]) + (d == 2 ? 0 : onb[2]);
+        Ua[d] = trilerp(qa[0], qa[SX], qa[SY], qa[SY + SX], qa[SZ], qa[SZ + SX], qa[SZ + SY], qa[SZ + SY + SX], s3a);
+        Ub[d] = trilerp(qb[0], qb[SX], qb[SY], qb[SY + SX], qb[SZ], qb[SZ + SX], qb[SZ + SY], qb[SZ + SY + SX], s3b);
+      }
+    }
+  }
+  int cla[3], clb[3];
+  const int P[3] = {px, py, pz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float ta = rmul(-Ua[a], dth[a]), tb = rmul(-Ub[a], dth[a]);
+    const float fla = floorf(ta), flb = floorf(tb);
+    cla[a] = P[a] + (int)fla - 1;  // first stencil cell, box-local
+    clb[a] = P[a] + (a == 2) + (int)flb - 1;
+    fa[a] = ta - fla;
+    fb[a] = tb - flb;
+  }
+  sa = (cla[2] * kPY + cla[1]) * kPX + cla[0];
+  sb = (clb[2] * kPY + clb[1]) * kPX + clb[0];
+  return near && (unsigned)cla[0] <= (unsigned)(kPX - 4) && (unsigned)cla[1] <= (unsigned)(kPY - 4) &&
+         (unsigned)cla[2] <= (unsigned)(kPZ - 4) && (unsigned)clb[0] <= (unsigned)(kPX - 4) &&
+         (unsigned)clb[1] <= (unsigned)(kPY - 4) && (unsigned)clb[2] <= (unsigned)(kPZ - 4);
+}
+
 // Dense-grid stepper over TMA-staged bricks.
 //
 // Each CTA owns bricks blockIdx.x, blockIdx.x + gridDim.x, ... (32 x 4 x 8
@@ -681,6 +765,7 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     }
   } else {  // ---------------- compute warps ----------------
     const float dth[3] = {dt / (float)g.hx, dt / (float)g.hy, dt / (float)g.hz};
+    const float hdth[3] = {-0.5f * dth[0], -0.5f * dth[1], -0.5f * dth[2]};
     const int lx = lane, ly = warp;  // a tile: 32 x 4 points of one z plane
     const int plane = g.nx * g.ny;
     const int nn[3] = {g.nx, g.ny, g.nz};
@@ -711,15 +796,16 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     // Departures of step j's two points from brick (x0, y0, z0)'s boxes; lanes
     // past the grid's end (partial bricks) compute a copy of the last in-grid
     // point and store nothing.  Returns whether the whole warp stays in the boxes.
+    // (A lane whose second point lies past the grid's last plane computes the
+    // out-of-grid point above its first one, from edge-replicated box cells,
+    // and stores nothing for it.)
     auto depart2 = [&](int j, int x0, int y0, int z0, float fa[3], float fb[3], int &sa, int &sb) -> bool {
       const float *vbox = reinterpret_cast<const float *>(((j >> 2) & 1 ? buf1 : buf0) + kPhiBoxBytes);
       const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
-      const int za = min(z0 + 2 * (j & 3), g.nz - 1), zb = min(z0 + 2 * (j & 3) + 1, g.nz - 1);
-      const bool ia = brick_depart<BT>(vbox, x - x0 + 4, y - y0 + 1, za - z0 + 1, x - x0 + 4, y - y0 + 2,
-                                       za - z0 + 2, dth, fa, sa);
-      const bool ib = brick_depart<BT>(vbox, x - x0 + 4, y - y0 + 1, zb - z0 + 1, x - x0 + 4, y - y0 + 2,
-                                       zb - z0 + 2, dth, fb, sb);
-      return __all_sync(0xffffffffu, ia && ib);
+      const int za = min(z0 + 2 * (j & 3), g.nz - 1);
+      const bool in = brick_depart2<BT>(vbox, x - x0 + 4, y - y0 + 1, za - z0 + 1, x - x0 + 4, y - y0 + 2,
+                                        za - z0 + 2, dth, hdth, fa, fb, sa, sb);
+      return __all_sync(0xffffffffu, in);
     };
     // A rows of one point -> TMEM stage `st`.
     auto stage_rows = [&](int j, int x0, int y0, int z0, int pt, bool boxed, int soff, float f[3], int st) {
@@ -759,10 +845,11 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
         uint32_t v[80];
 #pragma unroll
         for (int e = 0; e < 80; ++e) v[e] = q[((e >> 4) * kPY + ((e >> 2) & 3)) * kPX + (e & 3)];
-        tmem_st32(c.tmem + c.lane_off + 0, v);
-        tmem_st32(c.tmem + c.lane_off + 32, v + 32);
-        tmem_st32(c.tmem + c.lane_off + 128, v + 16);
-        tmem_st32(c.tmem + c.lane_off + 160, v + 48);
+#pragma unroll
+        for (int q16 = 0; q16 < 4; ++q16) {  // z-slices: point a's 0-3 are v's 0-3, point b's are v's 1-4
+          tmem_st16(c.tmem + c.lane_off + 16 * q16, v + 16 * q16);
+          tmem_st16(c.tmem + c.lane_off + 128 + 16 * q16, v + 16 * (q16 + 1));
+        }
       } else {
         stage_rows(j, x0, y0, z0, 0, boxed, sa, fa, 0);
         stage_rows(j, x0, y0, z0, 1, boxed, sb, fb, 1);
