@@ -544,68 +544,18 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Front half of one point from the staged, edge-replicated boxes: node
-// velocity, midpoint velocity, departure cell and fraction, and the box offset
-// of the stencil's first word.  (vx, vy, vz) is the point's cell in the
-// velocity box, (px, py, pz) in the phi box.  Returns false when the midpoint
-// or the stencil leaves the box (per-component CFL >= 1): the warp then takes
-// the global path.  The arithmetic is the clamped global path's, operation for
-// operation (explicit roundings), so both give the same bits.
-template <int BT>
-__device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int vx, int vy, int vz, int px, int py,
-                                             int pz, const float dth[3], float f[3], int &soff) {
-  constexpr int SX = 3, SY = 3 * kVX, SZ = 3 * kVX * kVY;
-  const float *vb = vbox + (vz * kVY + vy) * (3 * kVX) + 3 * vx;
-  float U[3] = {face_mean(vb[0], vb[SX]), face_mean(vb[1], vb[SY + 1]), face_mean(vb[2], vb[SZ + 2])};
-  bool near = true;
-  if (BT == DCELL_MIDPOINT) {
-    const float dl[3] = {rmul(rmul(-0.5f, U[0]), dth[0]), rmul(rmul(-0.5f, U[1]), dth[1]),
-                         rmul(rmul(-0.5f, U[2]), dth[2])};
-    // a midpoint half a cell or more from the node may leave the box: the
-    // offsets below are clamped to stay in it and the point is reported out
-    near = fabsf(dl[0]) < 0.5f && fabsf(dl[1]) < 0.5f && fabsf(dl[2]) < 0.5f;
-    // Along a component's own (staggered) axis the midpoint lies in [X, X+1):
-    // floor 0, fraction t.  Across the other two axes the node-centred
-    // fraction and floor are shared by both components.
-    float sn[3], sp[3];
-    int on[3];
-    constexpr int S[3] = {SX, SY, SZ};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float t = dl[a] + 0.f;
-      const float fl = floorf(t);
-      sn[a] = t - fl;
-      on[a] = min(max((int)fl, -1), 0) * S[a];
-      sp[a] = dl[a] + 0.5f;
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const float s3[3] = {d == 0 ? sp[0] : sn[0], d == 1 ? sp[1] : sn[1], d == 2 ? sp[2] : sn[2]};
-      const float *q = vb + d + (d == 0 ? 0 : on[0]) + (d == 1 ? 0 : on[1]) + (d == 2 ? 0 : on[2]);
-      U[d] = trilerp(q[0], q[SX], q[SY], q[SY + SX], q[SZ], q[SZ + SX], q[SZ + SY], q[SZ + SY + SX], s3);
-    }
-  }
-  int cl[3];
-  const int P[3] = {px, py, pz};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float t = rmul(-U[a], dth[a]);
-    const float fl = floorf(t);
-    cl[a] = P[a] + (int)fl - 1;  // first stencil cell, box-local
-    f[a] = t - fl;
-  }
-  soff = (cl[2] * kPY + cl[1]) * kPX + cl[0];
-  return near && (unsigned)cl[0] <= (unsigned)(kPX - 4) && (unsigned)cl[1] <= (unsigned)(kPY - 4) &&
-         (unsigned)cl[2] <= (unsigned)(kPZ - 4);
-}
-
-// brick_depart for a thread's two points: a at velocity-box cell (vx, vy, vz)
-// / phi-box cell (px, py, pz) and b one plane above it.  They share the w face
-// between them, and when their midpoint cells have the same floors (checked
-// over the warp) each velocity component's two trilinear stencils share a
-// layer: 12 corner loads instead of 16.  hdth = -dt/(2h) per axis, so
-// dl = U * hdth rounds exactly like (-U/2) * dt/h.  Same values and operations
-// as two brick_depart calls, so the same bits.
+// Front half of a thread's two points from the staged, edge-replicated boxes:
+// node velocity, midpoint velocity, departure cell and fraction, and the box
+// offset of each stencil's first word.  Point a sits at velocity-box cell
+// (vx, vy, vz) / phi-box cell (px, py, pz), point b one plane above it.  They
+// share the w face between them, and when their midpoint cells have the same
+// floors (checked over the warp) each velocity component's two trilinear
+// stencils share a layer: 12 corner loads instead of 16.  hdth = -dt/(2h) per
+// axis, so dl = U * hdth rounds exactly like (-U/2) * dt/h.  Returns false
+// when a midpoint or a stencil leaves the box (per-component CFL >= 1): the
+// warp then takes the global path.  The arithmetic is the clamped global
+// path's, operation for operation (explicit roundings), so both give the same
+// bits.
 template <int BT>
 __device__ __forceinline__ bool brick_depart2(const float *__restrict__ vbox, int vx, int vy, int vz, int px, int py,
                                               int pz, const float dth[3], const float hdth[3], float fa[3],
@@ -878,17 +828,15 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
       fence_after();
       float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
 #pragma unroll
-      for (int kp = 1; kp >= 0; --kp) {
+      for (int kp = 1; kp >= 0; --kp) {  // slices 2kp+1 then 2kp
         float ca[32], cb[32];
-        tmem_ld16(c.tmem + c.lane_off + 64 + 32 * kp + 16, reinterpret_cast<uint32_t *>(ca));
-        tmem_ld16(c.tmem + c.lane_off + 64 + 32 * kp, reinterpret_cast<uint32_t *>(ca + 16));
-        tmem_ld16(c.tmem + c.lane_off + 192 + 32 * kp + 16, reinterpret_cast<uint32_t *>(cb));
-        tmem_ld16(c.tmem + c.lane_off + 192 + 32 * kp, reinterpret_cast<uint32_t *>(cb + 16));
+        tmem_ld32(c.tmem + c.lane_off + 64 + 32 * kp, reinterpret_cast<uint32_t *>(ca));
+        tmem_ld32(c.tmem + c.lane_off + 192 + 32 * kp, reinterpret_cast<uint32_t *>(cb));
         tmem_wait_ld();
-        va = fmaf(va, fa[2], horner_slice(ca, fa));
-        vb = fmaf(vb, fb[2], horner_slice(cb, fb));
         va = fmaf(va, fa[2], horner_slice(ca + 16, fa));
         vb = fmaf(vb, fb[2], horner_slice(cb + 16, fb));
+        va = fmaf(va, fa[2], horner_slice(ca, fa));
+        vb = fmaf(vb, fb[2], horner_slice(cb, fb));
       }
       if (xy_valid && zr < g.nz) {
         phi[p0] = va;
