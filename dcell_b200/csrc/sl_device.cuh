@@ -21,6 +21,8 @@ namespace dcell {
 // contraction choices.
 __device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float rfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double rfma(double a, double b, double c) { return __fma_rn(a, b, c); }
 
@@ -29,20 +31,21 @@ __device__ __forceinline__ T face_mean(T a, T b) {
   return rfma(T(0.5), a, rmul(T(0.5), b));
 }
 
+// a + s (b - a): one subtraction and one fused multiply-add
+template <typename T>
+__device__ __forceinline__ T lerp(T a, T b, T s) {
+  return rfma(s, rsub(b, a), a);
+}
+
 // bilinear in (x, y) of v[yx] with fractions s0, s1
 template <typename T>
 __device__ __forceinline__ T bilerp(T v00, T v10, T v01, T v11, T s0, T s1) {
-  const T w0 = T(1) - s0;
-  const T a = rfma(w0, v00, rmul(s0, v10));
-  const T b = rfma(w0, v01, rmul(s0, v11));
-  return rfma(a, T(1) - s1, rmul(b, s1));
+  return lerp(lerp(v00, v10, s0), lerp(v01, v11, s0), s1);
 }
 
 template <typename T>
 __device__ __forceinline__ T trilerp(T v000, T v100, T v010, T v110, T v001, T v101, T v011, T v111, const T s[3]) {
-  const T bot = bilerp(v000, v100, v010, v110, s[0], s[1]);
-  const T top = bilerp(v001, v101, v011, v111, s[0], s[1]);
-  return rfma(bot, T(1) - s[2], rmul(top, s[2]));
+  return lerp(bilerp(v000, v100, v010, v110, s[0], s[1]), bilerp(v001, v101, v011, v111, s[0], s[1]), s[2]);
 }
 
 // MAC velocity at local node (x, y, z): each component is the mean of its two

@@ -544,6 +544,24 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// The global-memory path for one point of a brick warp that left its boxes:
+// departure and clamped gathers from global memory (tc_prepare_split), A row
+// straight to the TMEM columns at `taddr`; returns the fraction.  Out of line,
+// so the brick loop keeps its registers and code small; called by whole warps.
+__device__ __noinline__ float3 brick_rows_global(Geom g, const uint32_t *__restrict__ phi0s,
+                                                 const float *__restrict__ vel, float dth0, float dth1, float dth2,
+                                                 int backtrace, int x, int y, int z, uint32_t taddr) {
+  const float dth[3] = {dth0, dth1, dth2};
+  float f[3];
+  uint32_t w[64];
+  bool clamped = false;
+  tc_prepare_split(g, phi0s, vel, dth, backtrace, true, x, y, z, f, w, clamped);
+  __syncwarp();
+  tmem_st32(taddr, w);
+  tmem_st32(taddr + 32, w + 32);
+  return make_float3(f[0], f[1], f[2]);
+}
+
 // Front half of a thread's two points from the staged, edge-replicated boxes:
 // node velocity, midpoint velocity, departure cell and fraction, and the box
 // offset of each stencil's first word.  Point a sits at velocity-box cell
@@ -759,20 +777,23 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     };
     // A rows of one point -> TMEM stage `st`.
     auto stage_rows = [&](int j, int x0, int y0, int z0, int pt, bool boxed, int soff, float f[3], int st) {
-      uint32_t w[64];
       if (boxed) {
+        uint32_t w[64];
         const uint32_t *q = reinterpret_cast<const uint32_t *>((j >> 2) & 1 ? buf1 : buf0) + soff;
 #pragma unroll
         for (int e = 0; e < 64; ++e) w[e] = q[((e >> 4) * kPY + ((e >> 2) & 3)) * kPX + (e & 3)];
+        __syncwarp();  // the TMEM store is warp-collective
+        tmem_st32(c.tmem + c.lane_off + 128 * st, w);
+        tmem_st32(c.tmem + c.lane_off + 128 * st + 32, w + 32);
       } else {  // the whole warp recomputes from global memory with clamped indices
         const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
         const int z = min(z0 + 2 * (j & 3) + pt, g.nz - 1);
-        bool clamped = false;
-        tc_prepare_split(g, phi0s, vel, dth, BT, true, x, y, z, f, w, clamped);
+        const float3 r = brick_rows_global(g, phi0s, vel, dth[0], dth[1], dth[2], BT, x, y, z,
+                                           c.tmem + c.lane_off + 128 * st);
+        f[0] = r.x;
+        f[1] = r.y;
+        f[2] = r.z;
       }
-      __syncwarp();  // the TMEM store is warp-collective
-      tmem_st32(c.tmem + c.lane_off + 128 * st, w);
-      tmem_st32(c.tmem + c.lane_off + 128 * st + 32, w + 32);
     };
 
     int x0 = 0, y0 = 0, z0 = 0;
