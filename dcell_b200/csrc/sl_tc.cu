@@ -29,6 +29,7 @@
 // Several CTAs per SM (128 TMEM columns each) overlap one CTA's gathers with
 // another's MMA.  Band structure and backtrace follow LevelSetAdvectSL_3D
 // (LevelSetMethod/AdvectSL.c:56-89).
+#include <cstdlib>
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -436,36 +437,20 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_split_kernel(Geom g, const uin
 // ---------------------------------------------------------------------------
 // TMA-staged brick variant of the split-state step (dense grids, nx % 4 == 0).
 //
-// A CTA walks bricks of 32 x 2 x 4 arrival points (two 128-point MMA tiles).
-// For each brick, thread 0 issues two tiled TMA loads into shared memory --
-// the phi-split words of the box [x0-4, x0+36) x [y0-2, y0+4) x [z0-2, z0+6)
-// and the interleaved velocity of [x0-4, x0+36) x [y0-1, y0+3) x [z0-1, z0+5)
-// -- one brick ahead, double-buffered, completion tracked by an mbarrier's
-// transaction count.  Gathers then read shared memory with 32-bit offsets.
-// Out-of-grid parts of a box are zero-filled by TMA but never read: indices
-// are clamped to the grid before they are made box-local.  Points whose
-// departure (or midpoint) leaves the box -- per-component CFL >= 1 -- take
-// the global-memory path.  TMA x coordinates are multiples of 4 elements
-// (16-byte rule); nothing starts a store at a negative coordinate.
-constexpr int kBX = 32, kBY = 4, kBZ = 8;               // brick = 1024 points = 4 steps of 2 MMA tiles
-constexpr int kPX = kBX + 8, kPY = kBY + 4, kPZ = kBZ + 4;  // phi box (halo 4 | 2 | 2)
-constexpr int kVX = kBX + 8, kVY = kBY + 2, kVZ = kBZ + 2;  // velocity box (halo 4 | 1 | 1)
-constexpr int kPhiBoxBytes = kPX * kPY * kPZ * 4;
-constexpr int kVelBoxBytes = 3 * kVX * kVY * kVZ * 4;
-constexpr int kBufBytes = kPhiBoxBytes + kVelBoxBytes;
-constexpr int kBrickTmemCols = 256;                      // two tiles: A0 D0 | A1 D1
-constexpr int kBrickSmem = kBBytes + 2 * kBufBytes + 64;  // + 6 mbarriers and the TMEM slot
-// 2 CTAs per SM (2 x 256 TMEM columns); a third never fits, so no CTA waits in tcgen05.alloc
-constexpr int kBrickDynSmem = 105 * 1024;
-static_assert(kBrickSmem <= kBrickDynSmem && 3 * (kBrickDynSmem + 1024) > 228 * 1024,
-              "brick shared memory must admit exactly two CTAs per SM");
-static_assert(kPhiBoxBytes % 128 == 0 && kBufBytes % 128 == 0, "TMA destinations must stay 128-byte aligned");
-static_assert(3 * kVX <= 256 && kPX <= 256 && kPY <= 256 && kPZ <= 256, "TMA box dimensions are at most 256");
-
+// A CTA walks bricks of 32 x 4 x 4P arrival points, P = points each thread
+// carries per step along z (2 or 4).  For each brick two tiled TMA loads stage
+// the phi-split words of the box [x0-4, x0+36) x [y0-2, y0+6) x [z0-2, z0+4P+2)
+// and the interleaved velocity of [x0-4, x0+36) x [y0-1, y0+5) x
+// [z0-1, z0+4P+1) in shared memory, double-buffered, completion tracked by an
+// mbarrier's transaction count.  TMA x coordinates are multiples of 4
+// elements (16-byte rule); nothing starts a store at a negative coordinate.
+// Points whose departure (or midpoint) leaves the box -- per-component
+// CFL >= 1 -- take the global-memory path.
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+// 3-D tiled TMA load (no multicast) of the box at (c0, c1, c2) into shared memory
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, int c0, int c1, int c2,
                                             uint64_t *bar) {
   asm volatile(
@@ -479,28 +464,51 @@ struct BrickGrid {
   int nbx, nby, nbz;
 };
 
+template <int P>
+struct BrickShape {
+  static constexpr int BX = 32, BY = 4, BZ = 4 * P;          // 4 steps of P MMA tiles
+  static constexpr int PX = BX + 8, PY = BY + 4, PZ = BZ + 4;  // phi box (halo 4 | 2 | 2)
+  static constexpr int VX = BX + 8, VY = BY + 2, VZ = BZ + 2;  // velocity box (halo 4 | 1 | 1)
+  static constexpr int PhiBytes = PX * PY * PZ * 4;
+  static constexpr int VelBytes = 3 * VX * VY * VZ * 4;
+  static constexpr int BufBytes = PhiBytes + VelBytes;
+  static constexpr int TmemCols = 128 * P;                    // P stages of A | D
+  static constexpr int CtasPerSm = 512 / TmemCols;
+  static constexpr int Smem = kBBytes + 2 * BufBytes + 64;    // + 6 mbarriers and the TMEM slot
+  // shared memory sized so that exactly CtasPerSm CTAs fit on an SM: no CTA
+  // ever waits in tcgen05.alloc
+  static constexpr int DynSmem = CtasPerSm == 2 ? 105 * 1024 : ((Smem + 1023) / 1024) * 1024;
+  static_assert(Smem <= DynSmem && (CtasPerSm + 1) * (DynSmem + 1024) > 228 * 1024 &&
+                    CtasPerSm * (DynSmem + 1024) <= 228 * 1024,
+                "brick shared memory must admit exactly CtasPerSm CTAs per SM");
+  static_assert(PhiBytes % 128 == 0 && BufBytes % 128 == 0, "TMA destinations must stay 128-byte aligned");
+  static_assert(3 * VX <= 256 && PX <= 256 && PY <= 256 && PZ <= 256, "TMA box dimensions are at most 256");
+};
+
 // Bricks are numbered z fastest, x slowest: a persistent CTA striding by the
 // grid size then visits every x position (the x faces, where boxes need edge
 // replication, are shared out evenly), and the bricks in flight at one time
 // are z/y neighbours that share halo rows in L2.
+template <class S>
 __device__ __forceinline__ void brick_origin(const BrickGrid &bg, int b, int &x0, int &y0, int &z0) {
   const int bz = b % bg.nbz, r = b / bg.nbz;
-  z0 = bz * kBZ;
-  y0 = (r % bg.nby) * kBY;
-  x0 = (r / bg.nby) * kBX;
+  z0 = bz * S::BZ;
+  y0 = (r % bg.nby) * S::BY;
+  x0 = (r / bg.nby) * S::BX;
 }
 
-// thread 0: both boxes of brick b into buffer `buf` (whose previous contents
-// every thread has finished reading: order those generic-proxy reads before
-// the async-proxy writes)
+// one thread: both boxes of brick b into buffer `buf` (whose previous
+// contents every thread has finished reading: order those generic-proxy reads
+// before the async-proxy writes)
+template <class S>
 __device__ __forceinline__ void issue_brick(const BrickGrid &bg, int b, uint8_t *buf, const CUtensorMap *tm_phi,
                                             const CUtensorMap *tm_vel, uint64_t *bar) {
   int x0, y0, z0;
-  brick_origin(bg, b, x0, y0, z0);
+  brick_origin<S>(bg, b, x0, y0, z0);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_expect_tx(bar, (uint32_t)kBufBytes);
+  mbar_expect_tx(bar, (uint32_t)S::BufBytes);
   tma_load_3d(buf, tm_phi, x0 - 4, y0 - 2, z0 - 2, bar);
-  tma_load_3d(buf + kPhiBoxBytes, tm_vel, 3 * (x0 - 4), y0 - 1, z0 - 1, bar);
+  tma_load_3d(buf + S::PhiBytes, tm_vel, 3 * (x0 - 4), y0 - 1, z0 - 1, bar);
 }
 
 // Edge replication of a staged box.  TMA zero-fills the parts of a box that
@@ -562,124 +570,151 @@ __device__ __noinline__ float3 brick_rows_global(Geom g, const uint32_t *__restr
   return make_float3(f[0], f[1], f[2]);
 }
 
-// Front half of a thread's two points from the staged, edge-replicated boxes:
+// Front half of a thread's P points from the staged, edge-replicated boxes:
 // node velocity, midpoint velocity, departure cell and fraction, and the box
-// offset of each stencil's first word.  Point a sits at velocity-box cell
-// (vx, vy, vz) / phi-box cell (px, py, pz), point b one plane above it.  They
-// share the w face between them, and when their midpoint cells have the same
-// floors (checked over the warp) each velocity component's two trilinear
-// stencils share a layer: 12 corner loads instead of 16.  hdth = -dt/(2h) per
-// axis, so dl = U * hdth rounds exactly like (-U/2) * dt/h.  Returns false
-// when a midpoint or a stencil leaves the box (per-component CFL >= 1): the
-// warp then takes the global path.  The arithmetic is the clamped global
-// path's, operation for operation (explicit roundings), so both give the same
-// bits.
-template <int BT>
-__device__ __forceinline__ bool brick_depart2(const float *__restrict__ vbox, int vx, int vy, int vz, int px, int py,
-                                              int pz, const float dth[3], const float hdth[3], float fa[3],
-                                              float fb[3], int &sa, int &sb) {
-  constexpr int SX = 3, SY = 3 * kVX, SZ = 3 * kVX * kVY;
-  constexpr int S[3] = {SX, SY, SZ};
-  const float *va = vbox + (vz * kVY + vy) * (3 * kVX) + 3 * vx;  // b's node is va + SZ
-  const float wmid = va[SZ + 2];
-  float Ua[3] = {face_mean(va[0], va[SX]), face_mean(va[1], va[SY + 1]), face_mean(va[2], wmid)};
-  float Ub[3] = {face_mean(va[SZ], va[SZ + SX]), face_mean(va[SZ + 1], va[SZ + SY + 1]),
-                 face_mean(wmid, va[2 * SZ + 2])};
+// offset of each stencil's first word.  Point 0 sits at velocity-box cell
+// (vx, vy, vz) / phi-box cell (px, py, pz), point p p planes above it.
+// Consecutive points share the w face between them, and when all P midpoint
+// cells have the same floors (checked over the warp) the trilinear stencils of
+// one velocity component stack into P+1 layers: 4(P+1) corner loads instead
+// of 8P.  hdth = -dt/(2h) per axis, so dl = U * hdth rounds exactly like
+// (-U/2) * dt/h.  Returns false when a midpoint or a stencil leaves the box
+// (per-component CFL >= 1): the warp then takes the global path.  The
+// arithmetic is the clamped global path's, operation for operation (explicit
+// roundings), so both give the same bits.
+template <int BT, class S, int P>
+__device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int vx, int vy, int vz, int px, int py,
+                                             int pz, const float dth[3], const float hdth[3], float f[P][3],
+                                             int soff[P]) {
+  constexpr int SX = 3, SY = 3 * S::VX, SZ = 3 * S::VX * S::VY;
+  constexpr int ST[3] = {SX, SY, SZ};
+  const float *v0 = vbox + (vz * S::VY + vy) * (3 * S::VX) + 3 * vx;  // point p's node is v0 + p SZ
+  float wf[P + 1];
+#pragma unroll
+  for (int q = 0; q <= P; ++q) wf[q] = v0[q * SZ + 2];
+  float U[P][3];
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const float *v = v0 + p * SZ;
+    U[p][0] = face_mean(v[0], v[SX]);
+    U[p][1] = face_mean(v[1], v[SY + 1]);
+    U[p][2] = face_mean(wf[p], wf[p + 1]);
+  }
   bool near = true;
   if (BT == DCELL_MIDPOINT) {
-    float sna[3], spa[3], snb[3], spb[3];
-    int ona[3], onb[3];
+    float sn[P][3], sp[P][3];
+    int on[P][3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float dla = rmul(Ua[a], hdth[a]), dlb = rmul(Ub[a], hdth[a]);
-      near = near && fabsf(dla) < 0.5f && fabsf(dlb) < 0.5f;
-      const float ta = dla + 0.f, tb = dlb + 0.f;
-      const float fla = floorf(ta), flb = floorf(tb);
-      sna[a] = ta - fla;
-      snb[a] = tb - flb;
-      ona[a] = min(max((int)fla, -1), 0) * S[a];
-      onb[a] = min(max((int)flb, -1), 0) * S[a];
-      spa[a] = dla + 0.5f;
-      spb[a] = dlb + 0.5f;
-    }
-    const bool same = ona[0] == onb[0] && ona[1] == onb[1] && ona[2] == onb[2];
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float dl = rmul(U[p][a], hdth[a]);
+        near = near && fabsf(dl) < 0.5f;
+        // Along a component's own (staggered) axis the midpoint lies in
+        // [X, X+1): floor 0, fraction t.  Across the other two axes the
+        // node-centred fraction and floor serve both other components.
+        const float t = dl + 0.f;
+        const float fl = floorf(t);
+        sn[p][a] = t - fl;
+        on[p][a] = min(max((int)fl, -1), 0) * ST[a];
+        sp[p][a] = dl + 0.5f;
+      }
+    bool same = true;
+#pragma unroll
+    for (int p = 1; p < P; ++p) same = same && on[p][0] == on[0][0] && on[p][1] == on[0][1] && on[p][2] == on[0][2];
     if (__all_sync(0xffffffffu, same)) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        const float s3a[3] = {d == 0 ? spa[0] : sna[0], d == 1 ? spa[1] : sna[1], d == 2 ? spa[2] : sna[2]};
-        const float s3b[3] = {d == 0 ? spb[0] : snb[0], d == 1 ? spb[1] : snb[1], d == 2 ? spb[2] : snb[2]};
-        const float *q = va + d + (d == 0 ? 0 : ona[0]) + (d == 1 ? 0 : ona[1]) + (d == 2 ? 0 : ona[2]);
-        const float m00 = q[SZ], m10 = q[SZ + SX], m01 = q[SZ + SY], m11 = q[SZ + SY + SX];  // shared layer
-        Ua[d] = trilerp(q[0], q[SX], q[SY], q[SY + SX], m00, m10, m01, m11, s3a);
-        Ub[d] = trilerp(m00, m10, m01, m11, q[2 * SZ], q[2 * SZ + SX], q[2 * SZ + SY], q[2 * SZ + SY + SX], s3b);
+        const float *q = v0 + d + (d == 0 ? 0 : on[0][0]) + (d == 1 ? 0 : on[0][1]) + (d == 2 ? 0 : on[0][2]);
+        float L[P + 1][4];  // layer l: the 4 corners one z plane up per l
+#pragma unroll
+        for (int l = 0; l <= P; ++l) {
+          L[l][0] = q[l * SZ];
+          L[l][1] = q[l * SZ + SX];
+          L[l][2] = q[l * SZ + SY];
+          L[l][3] = q[l * SZ + SY + SX];
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const float s3[3] = {d == 0 ? sp[p][0] : sn[p][0], d == 1 ? sp[p][1] : sn[p][1],
+                               d == 2 ? sp[p][2] : sn[p][2]};
+          U[p][d] = trilerp(L[p][0], L[p][1], L[p][2], L[p][3], L[p + 1][0], L[p + 1][1], L[p + 1][2], L[p + 1][3],
+                            s3);
+        }
       }
     } else {
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const float s3a[3] = {d == 0 ? spa[0] : sna[0], d == 1 ? spa[1] : sna[1], d == 2 ? spa[2] : sna[2]};
-        const float s3b[3] = {d == 0 ? spb[0] : snb[0], d == 1 ? spb[1] : snb[1], d == 2 ? spb[2] : snb[2]};
-        const float *qa = va + d + (d == 0 ? 0 : ona[0]) + (d == 1 ? 0 : ona[1]) + (d == 2 ? 0 : ona[2]);
-        const float *qb = va + SZ + d + (d == 0 ? 0 : onb[0]) + (d == 1 ? 0 : onb[1]) + (d == 2 ? 0 : onb[2]);
-        Ua[d] = trilerp(qa[0], qa[SX], qa[SY], qa[SY + SX], qa[SZ], qa[SZ + SX], qa[SZ + SY], qa[SZ + SY + SX], s3a);
-        Ub[d] = trilerp(qb[0], qb[SX], qb[SY], qb[SY + SX], qb[SZ], qb[SZ + SX], qb[SZ + SY], qb[SZ + SY + SX], s3b);
-      }
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const float s3[3] = {d == 0 ? sp[p][0] : sn[p][0], d == 1 ? sp[p][1] : sn[p][1],
+                               d == 2 ? sp[p][2] : sn[p][2]};
+          const float *q = v0 + p * SZ + d + (d == 0 ? 0 : on[p][0]) + (d == 1 ? 0 : on[p][1]) +
+                           (d == 2 ? 0 : on[p][2]);
+          U[p][d] = trilerp(q[0], q[SX], q[SY], q[SY + SX], q[SZ], q[SZ + SX], q[SZ + SY], q[SZ + SY + SX], s3);
+        }
     }
   }
-  int cla[3], clb[3];
-  const int P[3] = {px, py, pz};
+  bool in = near;
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float ta = rmul(-Ua[a], dth[a]), tb = rmul(-Ub[a], dth[a]);
-    const float fla = floorf(ta), flb = floorf(tb);
-    cla[a] = P[a] + (int)fla - 1;  // first stencil cell, box-local
-    clb[a] = P[a] + (a == 2) + (int)flb - 1;
-    fa[a] = ta - fla;
-    fb[a] = tb - flb;
+  for (int p = 0; p < P; ++p) {
+    int cl[3];
+    const int Pc[3] = {px, py, pz + p};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float t = rmul(-U[p][a], dth[a]);
+      const float fl = floorf(t);
+      cl[a] = Pc[a] + (int)fl - 1;  // first stencil cell, box-local
+      f[p][a] = t - fl;
+    }
+    soff[p] = (cl[2] * S::PY + cl[1]) * S::PX + cl[0];
+    in = in && (unsigned)cl[0] <= (unsigned)(S::PX - 4) && (unsigned)cl[1] <= (unsigned)(S::PY - 4) &&
+         (unsigned)cl[2] <= (unsigned)(S::PZ - 4);
   }
-  sa = (cla[2] * kPY + cla[1]) * kPX + cla[0];
-  sb = (clb[2] * kPY + clb[1]) * kPX + clb[0];
-  return near && (unsigned)cla[0] <= (unsigned)(kPX - 4) && (unsigned)cla[1] <= (unsigned)(kPY - 4) &&
-         (unsigned)cla[2] <= (unsigned)(kPZ - 4) && (unsigned)clb[0] <= (unsigned)(kPX - 4) &&
-         (unsigned)clb[1] <= (unsigned)(kPY - 4) && (unsigned)clb[2] <= (unsigned)(kPZ - 4);
+  return in;
 }
 
 // Dense-grid stepper over TMA-staged bricks.
 //
-// Each CTA owns bricks blockIdx.x, blockIdx.x + gridDim.x, ... (32 x 4 x 8
+// Each CTA owns bricks blockIdx.x, blockIdx.x + gridDim.x, ... (32 x 4 x 4P
 // points, 4 steps each); their boxes are double-buffered with the next brick
-// in flight.  Four compute warps carry two points per thread and step -- the
-// same (x, y) in two consecutive z planes -- held in two TMEM stages (A | D
-// columns 0-127 and 128-255); a fifth warp only issues the MMAs and the TMA
-// loads.  Warps are decoupled by mbarriers, not CTA barriers:
+// in flight.  Four compute warps carry P points per thread and step -- the
+// same (x, y) in P consecutive z planes -- held in P TMEM stages (A | D, 128
+// columns each); a fifth warp only issues the MMAs and the TMA loads.  Warps
+// are decoupled by mbarriers, not CTA barriers:
 //
 //   compute warp, step j:
-//     a. A rows of both points -> their stages, arrive on afull
-//     b. departures of step j+1's two points (overlaps the MMAs)
-//     c. wait dfull: both points' coefficients -> values, evaluated together
-//   issuer, step j: wait afull (all four warps), both stages' MMAs, commit to
+//     a. A rows of the P points -> their stages, arrive on afull
+//     b. departures of step j+1's points (overlaps the MMAs)
+//     c. wait dfull: coefficients -> values, two points evaluated together
+//   issuer, step j: wait afull (all four warps), every stage's MMAs, commit to
 //     dfull; after a brick's last step, refill that brick's buffer with the
 //     brick two ahead.
 //
-// A stage's A columns are rewritten only after the writing warp saw the MMAs
-// complete (c of the step before); D columns are overwritten only after every
-// warp arrived on afull for the next step, which each does after reading D.
-// A buffer is refilled only after afull of its brick's last step: every warp
-// has then gathered from it for the last time (its departures were computed
-// one step earlier).  Every wait is bounded; a warp that gives up raises
-// FLAG_WAIT_TIMEOUT and leaves, and the others then give up at their next
-// wait.  Before the CTA ends, the issuer waits for its last TMA load per
-// buffer and its last commit.
+// When every lane's P stencils are stacked one plane apart (the usual case:
+// the points depart from vertically adjacent cells) the warp gathers their
+// 4 x 4 x (P+3) union once.  A stage's A columns are rewritten only after the
+// writing warp saw the MMAs complete (c of the step before); D columns are
+// overwritten only after every warp arrived on afull for the next step, which
+// each does after reading D.  A buffer is refilled only after afull of its
+// brick's last step: every warp has then gathered from it for the last time
+// (its departures were computed one step earlier).  Every wait is bounded; a
+// warp that gives up raises FLAG_WAIT_TIMEOUT and leaves, and the others then
+// give up at their next wait.  Before the CTA ends, the issuer waits for its
+// last TMA load per buffer and its last commit.  SPLIT: also write the
+// stepped values as packed split words (the next step's input).
 constexpr int kBrickThreads = kTile + 32;
 
-template <int BT>
-__global__ void __launch_bounds__(kBrickThreads, 2)
+template <int BT, int P, bool SPLIT>
+__global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
     sl_tc_brick_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel, Geom g,
                        BrickGrid bg, const uint32_t *__restrict__ phi0s, const float *__restrict__ vel, float dt,
                        float *__restrict__ phi, uint32_t *__restrict__ phis, int *flags) {
+  using S = BrickShape<P>;
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t *sB = smem;
-  uint8_t *const buf0 = smem + kBBytes, *const buf1 = smem + kBBytes + kBufBytes;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kBBytes + 2 * kBufBytes);
+  uint8_t *const buf0 = smem + kBBytes, *const buf1 = smem + kBBytes + S::BufBytes;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kBBytes + 2 * S::BufBytes);
   uint64_t *const unused = bars + 0;  // setup() initialises one MMA barrier; this kernel uses its own
   uint64_t *const afull = bars + 1, *const dfull = bars + 2, *const tbar = bars + 3, *const fixbar = bars + 5;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 6);
@@ -691,7 +726,7 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     mbar_init(fixbar, kTile);
   }
   Ctx c;
-  setup(sB, unused, tmem_slot, c, kBrickTmemCols);  // B operand, TMEM; ends with a CTA barrier
+  setup(sB, unused, tmem_slot, c, S::TmemCols);  // B operand, TMEM; ends with a CTA barrier
 
   const int nbricks = bg.nbx * bg.nby * bg.nbz;
   const int nmine = (int)blockIdx.x < nbricks ? (nbricks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -702,14 +737,20 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
   if (warp == 4) {  // ---------------- issuer ----------------
     if (lane == 0) {
       int tma_issued[2] = {0, 0}, mma_issued = 0;
-      if (nmine > 0) { issue_brick(bg, blockIdx.x, buf0, &tm_phi, &tm_vel, &tbar[0]); tma_issued[0] = 1; }
-      if (nmine > 1) { issue_brick(bg, blockIdx.x + gridDim.x, buf1, &tm_phi, &tm_vel, &tbar[1]); tma_issued[1] = 1; }
+      if (nmine > 0) {
+        issue_brick<S>(bg, blockIdx.x, buf0, &tm_phi, &tm_vel, &tbar[0]);
+        tma_issued[0] = 1;
+      }
+      if (nmine > 1) {
+        issue_brick<S>(bg, blockIdx.x + gridDim.x, buf1, &tm_phi, &tm_vel, &tbar[1]);
+        tma_issued[1] = 1;
+      }
       constexpr uint32_t idesc = instr_desc_bf16(kTile, kCoef);
       for (int j = 0; j < nsteps && !err; ++j) {
         if (!mbar_wait_sleep(afull, (uint32_t)j & 1u)) { err = true; break; }
         fence_after();
 #pragma unroll
-        for (int st = 0; st < 2; ++st)
+        for (int st = 0; st < P; ++st)
 #pragma unroll
           for (int kk = 0; kk < kK / 16; ++kk)
             mma_bf16(c.tmem + 128 * st + 64, c.tmem + 128 * st + (uint32_t)(kk * 8),
@@ -717,9 +758,9 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
         mma_commit(dfull);
         ++mma_issued;
         const int k = j >> 2;
-        if (!err && (j & 3) == 3 && k + 2 < nmine) {  // brick k read for the last time: refill with brick k+2
-          issue_brick(bg, (int)blockIdx.x + (k + 2) * (int)gridDim.x, k & 1 ? buf1 : buf0, &tm_phi, &tm_vel,
-                      k & 1 ? &tbar[1] : &tbar[0]);
+        if ((j & 3) == 3 && k + 2 < nmine) {  // brick k read for the last time: refill with brick k+2
+          issue_brick<S>(bg, (int)blockIdx.x + (k + 2) * (int)gridDim.x, k & 1 ? buf1 : buf0, &tm_phi, &tm_vel,
+                         k & 1 ? &tbar[1] : &tbar[0]);
           ++tma_issued[k & 1];
         }
       }
@@ -743,14 +784,15 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     auto open_brick = [&](int k, int &x0, int &y0, int &z0) -> bool {
       const bool odd = k & 1;
       if (!mbar_wait_sleep(odd ? &tbar[1] : &tbar[0], (uint32_t)(k >> 1) & 1u)) return false;
-      brick_origin(bg, (int)blockIdx.x + k * (int)gridDim.x, x0, y0, z0);
-      if (x0 < 4 || x0 + kPX - 4 > g.nx || y0 < 2 || y0 + kPY - 2 > g.ny || z0 < 2 || z0 + kPZ - 2 > g.nz) {
+      brick_origin<S>(bg, (int)blockIdx.x + k * (int)gridDim.x, x0, y0, z0);
+      if (x0 < 4 || x0 + S::PX - 4 > g.nx || y0 < 2 || y0 + S::PY - 2 > g.ny || z0 < 2 || z0 + S::PZ - 2 > g.nz) {
         uint8_t *cbuf = odd ? buf1 : buf0;
         const int op[3] = {x0 - 4, y0 - 2, z0 - 2}, ov[3] = {x0 - 4, y0 - 1, z0 - 1};
         for (int axis = 0; axis < 3; ++axis) {
-          const bool a = replicate_pass<kPX, kPY, kPZ, 1>(reinterpret_cast<uint32_t *>(cbuf), axis, op, nn, kTile);
-          const bool b = replicate_pass<kVX, kVY, kVZ, 3>(reinterpret_cast<uint32_t *>(cbuf + kPhiBoxBytes), axis,
-                                                          ov, nn, kTile);
+          const bool a =
+              replicate_pass<S::PX, S::PY, S::PZ, 1>(reinterpret_cast<uint32_t *>(cbuf), axis, op, nn, kTile);
+          const bool b = replicate_pass<S::VX, S::VY, S::VZ, 3>(reinterpret_cast<uint32_t *>(cbuf + S::PhiBytes),
+                                                                axis, ov, nn, kTile);
           if (!(a || b)) continue;
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes before a later TMA refill
           mbar_arrive(fixbar);
@@ -761,33 +803,33 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
       }
       return true;
     };
-    // Departures of step j's two points from brick (x0, y0, z0)'s boxes; lanes
+    // Departures of step j's P points from brick (x0, y0, z0)'s boxes; lanes
     // past the grid's end (partial bricks) compute a copy of the last in-grid
-    // point and store nothing.  Returns whether the whole warp stays in the boxes.
-    // (A lane whose second point lies past the grid's last plane computes the
-    // out-of-grid point above its first one, from edge-replicated box cells,
-    // and stores nothing for it.)
-    auto depart2 = [&](int j, int x0, int y0, int z0, float fa[3], float fb[3], int &sa, int &sb) -> bool {
-      const float *vbox = reinterpret_cast<const float *>(((j >> 2) & 1 ? buf1 : buf0) + kPhiBoxBytes);
+    // column and store nothing; points past the grid's last plane are
+    // computed from edge-replicated box cells and not stored.  Returns
+    // whether the whole warp stays in the boxes.
+    auto depart = [&](int j, int x0, int y0, int z0, float f[P][3], int soff[P]) -> bool {
+      const float *vbox = reinterpret_cast<const float *>(((j >> 2) & 1 ? buf1 : buf0) + S::PhiBytes);
       const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
-      const int za = min(z0 + 2 * (j & 3), g.nz - 1);
-      const bool in = brick_depart2<BT>(vbox, x - x0 + 4, y - y0 + 1, za - z0 + 1, x - x0 + 4, y - y0 + 2,
-                                        za - z0 + 2, dth, hdth, fa, fb, sa, sb);
+      const int zl = P * (j & 3);  // brick-local plane of point 0
+      const bool in = brick_depart<BT, S, P>(vbox, x - x0 + 4, y - y0 + 1, zl + 1, x - x0 + 4, y - y0 + 2, zl + 2,
+                                             dth, hdth, f, soff);
       return __all_sync(0xffffffffu, in);
     };
-    // A rows of one point -> TMEM stage `st`.
-    auto stage_rows = [&](int j, int x0, int y0, int z0, int pt, bool boxed, int soff, float f[3], int st) {
+    // A rows of one point -> TMEM stage `st` (gathered from the box, or the
+    // whole warp's global path).
+    auto stage_rows = [&](int j, int x0, int y0, int z0, bool boxed, int soff, float f[3], int st) {
       if (boxed) {
         uint32_t w[64];
         const uint32_t *q = reinterpret_cast<const uint32_t *>((j >> 2) & 1 ? buf1 : buf0) + soff;
 #pragma unroll
-        for (int e = 0; e < 64; ++e) w[e] = q[((e >> 4) * kPY + ((e >> 2) & 3)) * kPX + (e & 3)];
+        for (int e = 0; e < 64; ++e) w[e] = q[((e >> 4) * S::PY + ((e >> 2) & 3)) * S::PX + (e & 3)];
         __syncwarp();  // the TMEM store is warp-collective
         tmem_st32(c.tmem + c.lane_off + 128 * st, w);
         tmem_st32(c.tmem + c.lane_off + 128 * st + 32, w + 32);
-      } else {  // the whole warp recomputes from global memory with clamped indices
+      } else {
         const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
-        const int z = min(z0 + 2 * (j & 3) + pt, g.nz - 1);
+        const int z = min(z0 + P * (j & 3) + st, g.nz - 1);
         const float3 r = brick_rows_global(g, phi0s, vel, dth[0], dth[1], dth[2], BT, x, y, z,
                                            c.tmem + c.lane_off + 128 * st);
         f[0] = r.x;
@@ -797,33 +839,33 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
     };
 
     int x0 = 0, y0 = 0, z0 = 0;
-    float fa[3] = {0.f, 0.f, 0.f}, fb[3] = {0.f, 0.f, 0.f};
-    int sa = 0, sb = 0;
+    float f[P][3];
+    int soff[P];
     bool boxed = true;
     if (nsteps > 0) {
       err = !open_brick(0, x0, y0, z0);
       if (__any_sync(0xffffffffu, err)) err = true;
-      else boxed = depart2(0, x0, y0, z0, fa, fb, sa, sb);
+      else boxed = depart(0, x0, y0, z0, f, soff);
     }
     for (int j = 0; j < nsteps && !err; ++j) {
       const int k = j >> 2;
-      // a: A rows of both points into their stages, then this warp's arrival.
-      // Where every lane's second stencil is its first one plane up (the
-      // usual case: both points depart from vertically adjacent cells), the
-      // warp gathers their 4 x 4 x 5 union once.
-      if (boxed && __all_sync(0xffffffffu, sb == sa + kPX * kPY)) {
-        const uint32_t *q = reinterpret_cast<const uint32_t *>(k & 1 ? buf1 : buf0) + sa;
-        uint32_t v[80];
+      // a: A rows of the P points into their stages, then this warp's arrival
+      bool stacked = boxed;
 #pragma unroll
-        for (int e = 0; e < 80; ++e) v[e] = q[((e >> 4) * kPY + ((e >> 2) & 3)) * kPX + (e & 3)];
+      for (int p = 1; p < P; ++p) stacked = stacked && soff[p] == soff[0] + p * S::PX * S::PY;
+      if (__all_sync(0xffffffffu, stacked)) {
+        const uint32_t *q = reinterpret_cast<const uint32_t *>(k & 1 ? buf1 : buf0) + soff[0];
+        uint32_t v[16 * (P + 3)];
 #pragma unroll
-        for (int q16 = 0; q16 < 4; ++q16) {  // z-slices: point a's 0-3 are v's 0-3, point b's are v's 1-4
-          tmem_st16(c.tmem + c.lane_off + 16 * q16, v + 16 * q16);
-          tmem_st16(c.tmem + c.lane_off + 128 + 16 * q16, v + 16 * (q16 + 1));
-        }
+        for (int e = 0; e < 16 * (P + 3); ++e) v[e] = q[((e >> 4) * S::PY + ((e >> 2) & 3)) * S::PX + (e & 3)];
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+          for (int q16 = 0; q16 < 4; ++q16)  // point p's z-slice q16 is plane p + q16 of the union
+            tmem_st16(c.tmem + c.lane_off + 128 * p + 16 * q16, v + 16 * (p + q16));
       } else {
-        stage_rows(j, x0, y0, z0, 0, boxed, sa, fa, 0);
-        stage_rows(j, x0, y0, z0, 1, boxed, sb, fb, 1);
+#pragma unroll
+        for (int p = 0; p < P; ++p) stage_rows(j, x0, y0, z0, boxed, soff[p], f[p], p);
       }
       tmem_wait_st();
       fence_before();
@@ -831,47 +873,53 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
       if (lane == 0) mbar_arrive(afull);
       // b: next step's departures while the tensor core works
       int nx0 = x0, ny0 = y0, nz0 = z0;
-      float fan[3] = {0.f, 0.f, 0.f}, fbn[3] = {0.f, 0.f, 0.f};
-      int san = 0, sbn = 0;
+      float fn[P][3];
+      int soffn[P];
       bool boxedn = true;
       if (j + 1 < nsteps) {
         if (((j + 1) & 3) == 0) err = !open_brick(k + 1, nx0, ny0, nz0);
         if (__any_sync(0xffffffffu, err)) err = true;
-        else boxedn = depart2(j + 1, nx0, ny0, nz0, fan, fbn, san, sbn);
+        else boxedn = depart(j + 1, nx0, ny0, nz0, fn, soffn);
       }
-      // c: both points' coefficients -> values, two z-slices per TMEM load round
+      // c: coefficients -> values, two points at a time, two z-slices per TMEM load round
       const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
       const bool xy_valid = x0 + lx < g.nx && y0 + ly < g.ny;
-      const int zr = z0 + 2 * (j & 3);
+      const int zr = z0 + P * (j & 3);
       const int p0 = (min(zr, g.nz - 1) * g.ny + y) * g.nx + x;
       const bool ok = mbar_wait_sleep(dfull, (uint32_t)j & 1u);
       if (__any_sync(0xffffffffu, !ok)) { err = true; break; }
       fence_after();
-      float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
 #pragma unroll
-      for (int kp = 1; kp >= 0; --kp) {  // slices 2kp+1 then 2kp
-        float ca[32], cb[32];
-        tmem_ld32(c.tmem + c.lane_off + 64 + 32 * kp, reinterpret_cast<uint32_t *>(ca));
-        tmem_ld32(c.tmem + c.lane_off + 192 + 32 * kp, reinterpret_cast<uint32_t *>(cb));
+      for (int pp = 0; pp < P; pp += 2) {
+        // both points' 64 coefficients in one TMEM load round
+        float ca[64], cb[64];
+        tmem_ld32(c.tmem + c.lane_off + 128 * pp + 64, reinterpret_cast<uint32_t *>(ca));
+        tmem_ld32(c.tmem + c.lane_off + 128 * (pp + 1) + 64, reinterpret_cast<uint32_t *>(cb));
+        tmem_ld32(c.tmem + c.lane_off + 128 * pp + 96, reinterpret_cast<uint32_t *>(ca + 32));
+        tmem_ld32(c.tmem + c.lane_off + 128 * (pp + 1) + 96, reinterpret_cast<uint32_t *>(cb + 32));
         tmem_wait_ld();
-        va = fmaf(va, fa[2], horner_slice(ca + 16, fa));
-        vb = fmaf(vb, fb[2], horner_slice(cb + 16, fb));
-        va = fmaf(va, fa[2], horner_slice(ca, fa));
-        vb = fmaf(vb, fb[2], horner_slice(cb, fb));
-      }
-      if (xy_valid && zr < g.nz) {
-        phi[p0] = va;
-        if (phis) phis[p0] = pack_split(va);
-      }
-      if (xy_valid && zr + 1 < g.nz) {
-        phi[p0 + plane] = vb;
-        if (phis) phis[p0 + plane] = pack_split(vb);
+        float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
+#pragma unroll
+        for (int kz = 3; kz >= 0; --kz) {
+          va = fmaf(va, f[pp][2], horner_slice(ca + 16 * kz, f[pp]));
+          vb = fmaf(vb, f[pp + 1][2], horner_slice(cb + 16 * kz, f[pp + 1]));
+        }
+        if (xy_valid && zr + pp < g.nz) {
+          phi[p0 + pp * plane] = va;
+          if (SPLIT) phis[p0 + pp * plane] = pack_split(va);
+        }
+        if (xy_valid && zr + pp + 1 < g.nz) {
+          phi[p0 + (pp + 1) * plane] = vb;
+          if (SPLIT) phis[p0 + (pp + 1) * plane] = pack_split(vb);
+        }
       }
       fence_before();
       x0 = nx0; y0 = ny0; z0 = nz0;
-      fa[0] = fan[0]; fa[1] = fan[1]; fa[2] = fan[2];
-      fb[0] = fbn[0]; fb[1] = fbn[1]; fb[2] = fbn[2];
-      sa = san; sb = sbn;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        f[p][0] = fn[p][0]; f[p][1] = fn[p][1]; f[p][2] = fn[p][2];
+        soff[p] = soffn[p];
+      }
       boxed = boxedn;
     }
     if (err) raise_flag(flags, FLAG_WAIT_TIMEOUT);
@@ -880,7 +928,7 @@ __global__ void __launch_bounds__(kBrickThreads, 2)
   fence_before();
   __syncthreads();
   fence_after();
-  if (warp == 0) tmem_dealloc(c.tmem, kBrickTmemCols);
+  if (warp == 0) tmem_dealloc(c.tmem, S::TmemCols);
 }
 
 // Batched cells: a persistent CTA walks a packed queue of 128-point tiles
@@ -1068,47 +1116,70 @@ static bool make_map(CUtensorMap *m, CUtensorMapDataType type, const void *base,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// The TMA brick path applies to dense 3D grids with nx % 4 == 0 (16-byte row strides) and 16-byte aligned bases.
+// The TMA brick path applies to dense 3D grids with nx % 4 == 0 (16-byte row
+// strides), 16-byte aligned bases and at least one box per axis.
 bool tc_brick_applicable(const Geom &g, const void *phi0s, const void *vel) {
-  return g.nz >= tc::kPZ && g.ny >= tc::kPY && g.nx >= tc::kPX && g.nx % 4 == 0 && ((uintptr_t)phi0s % 16) == 0 &&
+  using S = tc::BrickShape<2>;
+  return g.nz >= S::PZ && g.ny >= S::PY && g.nx >= S::PX && g.nx % 4 == 0 && ((uintptr_t)phi0s % 16) == 0 &&
          ((uintptr_t)vel % 16) == 0 && encode_tiled() != nullptr;
 }
 
-int launch_sl_tc_brick(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
-                       uint32_t *phis, int *flags, cudaStream_t st) {
+template <int P>
+static int launch_brick(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
+                        uint32_t *phis, int *flags, cudaStream_t st) {
+  using S = tc::BrickShape<P>;
   static bool configured = false;
   if (!configured) {
-    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::sl_tc_brick_kernel<DCELL_EULER>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kBrickDynSmem));
-    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::sl_tc_brick_kernel<DCELL_MIDPOINT>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kBrickDynSmem));
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::sl_tc_brick_kernel<DCELL_EULER, P, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, S::DynSmem));
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::sl_tc_brick_kernel<DCELL_MIDPOINT, P, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, S::DynSmem));
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::sl_tc_brick_kernel<DCELL_EULER, P, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, S::DynSmem));
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::sl_tc_brick_kernel<DCELL_MIDPOINT, P, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, S::DynSmem));
     configured = true;
   }
   CUtensorMap tm_phi, tm_vel;
   if (!make_map(&tm_phi, CU_TENSOR_MAP_DATA_TYPE_UINT32, phi0s, (uint64_t)g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
-                tc::kPX, tc::kPY, tc::kPZ, 4) ||
+                S::PX, S::PY, S::PZ, 4) ||
       !make_map(&tm_vel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel, 3ull * g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
-                3 * tc::kVX, tc::kVY, tc::kVZ, 4)) {
+                3 * S::VX, S::VY, S::VZ, 4)) {
     dcell_set_error(DCELL_ERR_CUDA, "cuTensorMapEncodeTiled failed for the TMA brick path");
     return DCELL_ERR_CUDA;
   }
   tc::BrickGrid bg;
-  bg.nbx = (g.nx + tc::kBX - 1) / tc::kBX;
-  bg.nby = (g.ny + tc::kBY - 1) / tc::kBY;
-  bg.nbz = (g.nz + tc::kBZ - 1) / tc::kBZ;
+  bg.nbx = (g.nx + S::BX - 1) / S::BX;
+  bg.nby = (g.ny + S::BY - 1) / S::BY;
+  bg.nbz = (g.nz + S::BZ - 1) / S::BZ;
   const long long nbricks = (long long)bg.nbx * bg.nby * bg.nbz;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  long long grid = 2LL * sms;
+  long long grid = (long long)S::CtasPerSm * sms;
   if (grid > nbricks) grid = nbricks;
-  if (backtrace == DCELL_MIDPOINT)
-    tc::sl_tc_brick_kernel<DCELL_MIDPOINT><<<(int)grid, tc::kBrickThreads, tc::kBrickDynSmem, st>>>(
-        tm_phi, tm_vel, g, bg, phi0s, vel, (float)dt, phi, phis, flags);
-  else
-    tc::sl_tc_brick_kernel<DCELL_EULER><<<(int)grid, tc::kBrickThreads, tc::kBrickDynSmem, st>>>(
-        tm_phi, tm_vel, g, bg, phi0s, vel, (float)dt, phi, phis, flags);
+  const bool mid = backtrace == DCELL_MIDPOINT, split = phis != nullptr;
+  auto kern = mid ? (split ? tc::sl_tc_brick_kernel<DCELL_MIDPOINT, P, true> : tc::sl_tc_brick_kernel<DCELL_MIDPOINT, P, false>)
+                  : (split ? tc::sl_tc_brick_kernel<DCELL_EULER, P, true> : tc::sl_tc_brick_kernel<DCELL_EULER, P, false>);
+  kern<<<(int)grid, tc::kBrickThreads, S::DynSmem, st>>>(tm_phi, tm_vel, g, bg, phi0s, vel, (float)dt, phi, phis,
+                                                          flags);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+// Points per thread of the brick kernel: 2 (two CTAs per SM) or 4 (one CTA
+// per SM, deeper z columns).  DCELL_TC_BRICK_POINTS overrides the default;
+// grids too shallow for the 4-point box use 2.
+static int brick_points(const Geom &g) {
+  int p = 2;
+  if (const char *e = getenv("DCELL_TC_BRICK_POINTS")) p = atoi(e) == 4 ? 4 : 2;
+  if (p == 4 && g.nz < tc::BrickShape<4>::PZ) p = 2;
+  return p;
+}
+
+int launch_sl_tc_brick(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
+                       uint32_t *phis, int *flags, cudaStream_t st) {
+  if (brick_points(g) == 4) return launch_brick<4>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st);
+  return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st);
 }
 
 int launch_tc_gemm_check(const float *A, float *D, int *flags, cudaStream_t st) {
