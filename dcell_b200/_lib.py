@@ -17,6 +17,7 @@ F32, F64 = 0, 1
 LINEAR, CUBIC_PLAIN, CUBIC_SEPARABLE, CUBIC_TC = 0, 1, 2, 3
 EULER, MIDPOINT = 0, 1
 FLAG_DEPARTURE_CLAMPED, FLAG_NONFINITE, FLAG_CAPACITY, FLAG_WAIT_TIMEOUT, FLAG_BAD_BAND = 1, 2, 4, 8, 16
+FLAG_UNSETTLED = 32
 
 INTERP = {"linear": LINEAR, "cubic": CUBIC_PLAIN, "cubic_plain": CUBIC_PLAIN, "cubic_separable": CUBIC_SEPARABLE,
           "cubic_tc": CUBIC_TC}
@@ -86,6 +87,9 @@ def lib():
     L.dcell_max_velocity.argtypes = [G, i, vp, vp, vp, i, vp, vp]
     L.dcell_volume_scratch_bytes.restype = sz
     L.dcell_volume.argtypes = [G, i, vp, d, vp, vp, sz, vp]
+    L.dcell_reinit_scratch_bytes.argtypes = [G, i]
+    L.dcell_reinit_scratch_bytes.restype = sz
+    L.dcell_reinitialize.argtypes = [G, i, vp, vp, i, d, d, vp, i, vp, vp, sz, vp, vp]
     L.dcell_session_create.argtypes = [i, ctypes.POINTER(vp)]
     L.dcell_session_destroy.argtypes = [vp]
     L.dcell_ls_advect_sl.argtypes = [vp, G, vp, vp, vp, i, d, i, i, i, vp]
@@ -98,7 +102,7 @@ def lib():
     L.dcell_batch_plan.argtypes = [vp, i, i, i, i, vp, i, vp]
     L.dcell_batch_sl_step.argtypes = [vp, i, vp, i, i, i, i, i, vp, vp, vp, i, i, vp, vp]
     for name in ("dcell_sl_step", "dcell_irregular_nodes", "dcell_irregular_nodes_noalloc", "dcell_max_velocity",
-                 "dcell_volume",
+                 "dcell_volume", "dcell_reinitialize",
                  "dcell_session_create", "dcell_session_destroy", "dcell_ls_advect_sl",
                  "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_tc_gemm_check",
                  "dcell_sl_adjoint", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",

@@ -136,6 +136,30 @@ DCELL_API int dcell_irregular_nodes(const dcell_geom *g, int dtype, const void *
                           flags, (cudaStream_t)stream);
 }
 
+DCELL_API size_t dcell_reinit_scratch_bytes(const dcell_geom *g, int dtype) {
+  if (!g) return 0;
+  const long long n = (long long)g->n[0] * g->n[1] * (g->n[2] > 1 ? g->n[2] : 1);
+  return reinit_scratch_bytes(n, dtype);
+}
+
+DCELL_API int dcell_reinitialize(const dcell_geom *g, int dtype, void *phi, const dcell_irregular_node *nodes,
+                                 int nnodes, double band_width, double bucket, int *band, int capacity, int *count,
+                                 void *scratch, size_t scratch_bytes, int *flags, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (!phi || !count || nnodes < 0 || (nnodes > 0 && !nodes)) FAIL(DCELL_ERR_ARG, "phi, nodes and count are required");
+  if (capacity < 0 || (capacity > 0 && !band)) FAIL(DCELL_ERR_ARG, "invalid band buffer");
+  if (!(band_width > 0)) FAIL(DCELL_ERR_ARG, "band_width must be positive");
+  if (bucket == 0) bucket = 1.0 / 64;
+  if (!(bucket > 0) || band_width / bucket > 1e6) FAIL(DCELL_ERR_ARG, "bucket must be positive and not tiny");
+  const size_t need = dcell_reinit_scratch_bytes(g, dtype);
+  if (!scratch || scratch_bytes < need) FAIL(DCELL_ERR_ARG, "scratch must hold %zu bytes", need);
+  if ((uintptr_t)scratch % 256) FAIL(DCELL_ERR_ARG, "scratch must be 256-byte aligned");
+  return launch_reinit(dcell::to_geom(g), dtype, phi, nodes, nnodes, band_width, bucket, band, capacity, count,
+                       scratch, flags, (cudaStream_t)stream);
+}
+
 DCELL_API int dcell_irregular_nodes_noalloc(const dcell_geom *g, int dtype, const void *phi, const int *band,
                                             int nband, int with_surface, dcell_irregular_node *nodes, int capacity,
                                             int *count, int *flags, void *stream) {

@@ -109,6 +109,7 @@ enum : int {
   FLAG_CAPACITY = 4,           // output list capacity exceeded
   FLAG_WAIT_TIMEOUT = 8,       // a bounded device wait gave up
   FLAG_BAD_BAND = 16,          // a band entry lies outside the grid (skipped)
+  FLAG_UNSETTLED = 32,         // reinitialisation: points still tentative after the last bucket
 };
 
 __device__ __forceinline__ void raise_flag(int *flags, int bit) {

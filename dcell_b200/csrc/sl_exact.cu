@@ -827,6 +827,267 @@ __global__ void __launch_bounds__(32) volume_final_kernel(const double *__restri
   if (threadIdx.x == 0) *out = acc * cell;
 }
 
+
+// ---------------------------------------------------------------------------
+// Narrow-band reinitialisation by bucketed fast marching (replaces
+// LevelSetReinitialize, LevelSetMethod/FastMarching.c:11-146, after its
+// LevelSetResize).  The heap of FMM_SolveEikonal is replaced by buckets of
+// width `bucket` cells: every tentative value below (b+1)*bucket (and <=
+// bandWidth) is fixed together, then the neighbours of the newly fixed points
+// are re-evaluated with the reference's second-order update (AccumulateCoef
+// FastMarching2D.c:33-99, FMM_PushNeighbors2D/3D FastMarching2D.c:103-185,
+// FastMarching3D.c:13-101) and keep the smallest value (atomicMin on an
+// order-preserving integer image).  Each evaluation sees what the heap had
+// fixed when it popped the pushing point: the seeds and the marched points
+// whose value is not larger than the pusher's.  Evaluations read only fixed
+// points, so the result is independent of thread order and identical to the
+// oracle's restatement of the same procedure.  Compiled, like the rest of
+// this file, without FMA contraction.
+constexpr int REINIT_TAIL = 16;   // buckets past bandWidth in which the last pushes settle
+constexpr int REINIT_THREADS = 256;
+
+enum ReinitMark : int { RM_FAR = 0, RM_TENT = 1, RM_MARCHED = 2, RM_SEED = 3 };
+
+// order-preserving integer images of floating-point values (smaller value <=> smaller image)
+__device__ __forceinline__ unsigned long long ord_bits(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double ord_value(unsigned long long o) {
+  const unsigned long long b = (o >> 63) ? (o & 0x7fffffffffffffffull) : ~o;
+  return __longlong_as_double((long long)b);
+}
+__device__ __forceinline__ unsigned int ord_bits(float v) {
+  const unsigned int b = __float_as_uint(v);
+  return (b >> 31) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ord_value(unsigned int o) {
+  const unsigned int b = (o >> 31) ? (o & 0x7fffffffu) : ~o;
+  return __uint_as_float(b);
+}
+template <typename T> struct OrdOf;
+template <> struct OrdOf<double> { typedef unsigned long long type; };
+template <> struct OrdOf<float> { typedef unsigned int type; };
+
+struct ReinitState {
+  int *mark;          // ReinitMark per point
+  void *tent;         // OrdOf<T>::type per point
+  int *list[2];       // tentative lists (ping-pong)
+  int *acc;           // points fixed in the current bucket
+  int *cnt;           // [0],[1] list lengths, [2] accepted, [3] error
+};
+
+template <typename T>
+__device__ void fmm_accumulate_dev(T bw, const T *p, T &a, T &b, T &c) {
+  const T D2p = (3 * p[0] - 4 * p[1] + p[2]) / T(2);
+  const T D2m = (3 * p[0] - 4 * p[-1] + p[-2]) / T(2);
+  const T D1p = p[0] - p[1];
+  const T D1m = p[0] - p[-1];
+  T Dm, am, bm, cm, Dp, ap, bp, cp, t;
+  if (0 <= p[1] && p[1] < bw && 0 <= p[2] && p[2] < bw && D2p > 0) {
+    t = (4 * p[1] - p[2]) / T(3);
+    ap = T(9) / T(4);
+    bp = -T(9) / T(2) * t;
+    cp = T(9) / T(4) * t * t;
+    Dp = D2p;
+  } else if (0 <= p[1] && p[1] < bw && D1p > 0) {
+    ap = 1;
+    bp = -2 * p[1];
+    cp = p[1] * p[1];
+    Dp = D1p;
+  } else {
+    ap = bp = cp = Dp = 0;
+  }
+  if (0 <= p[-1] && p[-1] < bw && 0 <= p[-2] && p[-2] < bw && D2m > 0) {
+    t = (4 * p[-1] - p[-2]) / T(3);
+    am = T(9) / T(4);
+    bm = -T(9) / T(2) * t;
+    cm = T(9) / T(4) * t * t;
+    Dm = D2m;
+  } else if (0 <= p[-1] && p[-1] < bw && D1m > 0) {
+    am = 1;
+    bm = -2 * p[-1];
+    cm = p[-1] * p[-1];
+    Dm = D1m;
+  } else {
+    am = bm = cm = Dm = 0;
+  }
+  if (Dm > Dp) {
+    a += am;
+    b += bm;
+    c += cm;
+  } else {
+    a += ap;
+    b += bp;
+    c += cp;
+  }
+}
+
+// update of local point (x,y,z) on side `sign`, seeing seeds and marched points <= lim
+template <typename T, int DIM>
+__device__ T fmm_update_dev(const Geom &g, const T *__restrict__ phi, const int *__restrict__ mark, int x, int y,
+                            int z, int sign, T inf, T lim) {
+  T a = 0, b = 0, c = -1, line[7];
+  const int X[3] = {x, y, z}, n[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+  for (int ax = 0; ax < DIM; ++ax) {
+#pragma unroll
+    for (int m = 0; m < 7; ++m) {
+      int q[3] = {X[0], X[1], X[2]};
+      q[ax] += m - 3;
+      if (q[ax] < 0 || q[ax] >= n[ax]) {
+        line[m] = inf;
+      } else {
+        const int r = (q[2] * g.ny + q[1]) * g.nx + q[0];
+        const T v = sign * phi[r];
+        line[m] = (mark[r] == RM_MARCHED && v > lim) ? inf : v;
+      }
+    }
+    fmm_accumulate_dev<T>(inf, line + 3, a, b, c);
+  }
+  const T disc = sqrt(b * b - 4 * a * c);
+  T d1 = (-b + disc) / (2 * a);
+  if (d1 != d1) d1 = -b / (2 * a);
+  return d1;
+}
+
+template <typename T, int DIM>
+__device__ void fmm_relax_dev(const Geom &g, const T *__restrict__ phi, ReinitState st, int out, int x, int y, int z,
+                              int sign, T bw, T inf, T lim) {
+  typedef typename OrdOf<T>::type O;
+  O *tent = (O *)st.tent;
+  constexpr int kStarDev[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+#pragma unroll
+  for (int s = 0; s < 2 * DIM; ++s) {
+    const int i = x + kStarDev[s][0], j = y + kStarDev[s][1], k = z + kStarDev[s][2];
+    if (i < 0 || i >= g.nx || j < 0 || j >= g.ny || k < 0 || k >= g.nz) continue;
+    const int q = (k * g.ny + j) * g.nx + i;
+    if (sign * phi[q] < bw) continue;  // fixed, or the other side
+    const T v = fmm_update_dev<T, DIM>(g, phi, st.mark, i, j, k, sign, inf, lim);
+    if (v != v) {
+      atomicExch(&st.cnt[3], 1);
+      continue;
+    }
+    atomicMin(&tent[q], ord_bits(v));
+    if (atomicCAS(&st.mark[q], RM_FAR, RM_TENT) == RM_FAR) st.list[out][atomicAdd(&st.cnt[out], 1)] = q;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(REINIT_THREADS) reinit_init_kernel(T *phi, long long n, T inf, int *mark) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    phi[q] = phi[q] > 0 ? inf : -inf;  // FastMarching.c:28-30
+    mark[q] = RM_FAR;
+  }
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(REINIT_THREADS) reinit_seed_kernel(Geom g, T *phi, const dcell_irregular_node *nodes,
+                                                                   int nnodes, int *mark) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nnodes) return;
+  const dcell_irregular_node nd = nodes[r];
+  if (nd.axis != -1) return;  // FastMarching.c:57-70
+  const int x = nd.pos[0] - g.px, y = nd.pos[1] - g.py, z = DIM == 3 ? nd.pos[2] - g.pz : 0;
+  if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) return;
+  const int q = (z * g.ny + y) * g.nx + x;
+  const double len = DIM == 2 ? sqrt(nd.op[0] * nd.op[0] + nd.op[1] * nd.op[1])
+                              : sqrt(nd.op[0] * nd.op[0] + nd.op[1] * nd.op[1] + nd.op[2] * nd.op[2]);
+  phi[q] = (T)(nd.signCenter * len);
+  mark[q] = RM_SEED;
+}
+
+// per side: tentative values back to +inf, tentative marks back to far
+template <typename T>
+__global__ void __launch_bounds__(REINIT_THREADS) reinit_side_kernel(long long n, ReinitState st) {
+  typedef typename OrdOf<T>::type O;
+  O *tent = (O *)st.tent;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    tent[q] = ord_bits((T)INFINITY);
+    if (st.mark[q] == RM_TENT) st.mark[q] = RM_FAR;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) st.cnt[0] = st.cnt[1] = st.cnt[2] = 0;
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(REINIT_THREADS) reinit_push_seeds_kernel(Geom g, const T *phi,
+                                                                         const dcell_irregular_node *nodes, int nnodes,
+                                                                         ReinitState st, int sign, T bw, T inf) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nnodes) return;
+  const dcell_irregular_node nd = nodes[r];
+  if (nd.axis != -1) return;
+  const int x = nd.pos[0] - g.px, y = nd.pos[1] - g.py, z = DIM == 3 ? nd.pos[2] - g.pz : 0;
+  if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) return;
+  if (sign * phi[(z * g.ny + y) * g.nx + x] >= 0)  // FastMarching.c:72-84
+    fmm_relax_dev<T, DIM>(g, phi, st, 0, x, y, z, sign, bw, inf, -(T)INFINITY);
+}
+
+// bucket b: fix list[in] entries below thr (and <= bw), keep the rest <= bw in list[out]
+template <typename T>
+__global__ void __launch_bounds__(REINIT_THREADS) reinit_accept_kernel(T *phi, ReinitState st, int in, int sign, T thr,
+                                                                     T bw) {
+  typedef typename OrdOf<T>::type O;
+  const O *tent = (const O *)st.tent;
+  const int n = st.cnt[in];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int q = st.list[in][t];
+    const T v = ord_value(tent[q]);
+    if (v < thr && v <= bw) {
+      phi[q] = sign * v;
+      st.mark[q] = RM_MARCHED;
+      st.acc[atomicAdd(&st.cnt[2], 1)] = q;
+    } else if (v <= bw) {
+      st.list[in ^ 1][atomicAdd(&st.cnt[in ^ 1], 1)] = q;
+    } else {
+      st.mark[q] = RM_FAR;  // past the band unless a later push lowers it
+    }
+  }
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(REINIT_THREADS) reinit_relax_kernel(Geom g, const T *phi, ReinitState st, int out,
+                                                                    int sign, T bw, T inf) {
+  const int n = st.cnt[2];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int q = st.acc[t];
+    const int x = q % g.nx, y = (q / g.nx) % g.ny, z = q / (g.nx * g.ny);
+    fmm_relax_dev<T, DIM>(g, phi, st, out, x, y, z, sign, bw, inf, sign * phi[q]);
+  }
+}
+
+// between buckets: the consumed list and the accepted list start empty
+__global__ void reinit_next_kernel(ReinitState st, int consumed) {
+  st.cnt[consumed] = 0;
+  st.cnt[2] = 0;
+}
+
+__global__ void reinit_finish_side_kernel(ReinitState st, int last, int *flags) {
+  if (st.cnt[last] > 0) st.cnt[3] = 2;  // still tentative after the last bucket
+}
+
+__global__ void __launch_bounds__(REINIT_THREADS) reinit_band_flags_kernel(const int *mark, long long n, int *flag) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    flag[q] = mark[q] >= RM_MARCHED ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(REINIT_THREADS) reinit_band_write_kernel(Geom g, const int *mark, const int *offs,
+                                                                         long long n, int *band, int cap) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    if (mark[q] >= RM_MARCHED) {
+      const int o = offs[q];
+      if (o < cap) {
+        band[3 * o + 0] = g.px + (int)(q % g.nx);
+        band[3 * o + 1] = g.py + (int)((q / g.nx) % g.ny);
+        band[3 * o + 2] = g.pz + (int)(q / ((long long)g.nx * g.ny));
+      }
+    }
+}
+
+__global__ void reinit_status_kernel(const ReinitState st, int *flags) {
+  if (st.cnt[3] == 1) raise_flag(flags, FLAG_NONFINITE);
+  if (st.cnt[3] == 2) raise_flag(flags, FLAG_UNSETTLED);
+}
 }  // namespace dcell
 
 // ===========================================================================
@@ -914,6 +1175,80 @@ int launch_max_velocity(const Geom &g, int dtype, const void *vel, const dcell_i
   } else {
     if (is2d) maxvel_kernel<float, 2><<<blocks, 256, 0, st>>>(g, (const float *)vel, nodes, count, cap, o);
     else maxvel_kernel<float, 3><<<blocks, 256, 0, st>>>(g, (const float *)vel, nodes, count, cap, o);
+  }
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+
+// ---------------------------------------------------------------------------
+// Reinitialisation.  Scratch layout (bytes, each part 256-aligned): mark
+// int[n], tentative values [n] (8 or 4 bytes), two tentative lists int[n],
+// accepted list int[n], counters int[8]; the band scan reuses the two lists.
+static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+size_t reinit_scratch_bytes(long long n, int dtype) {
+  const size_t w = dtype == DCELL_F64 ? 8 : 4;
+  const size_t nblk = ((size_t)n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  return align256(sizeof(int) * n) + align256(w * n) + 3 * align256(sizeof(int) * n) + align256(sizeof(int) * 8) +
+         align256(sizeof(int) * (nblk + 1));
+}
+
+template <typename T, int DIM>
+static void reinit_run(const Geom &g, T *phi, const dcell_irregular_node *nodes, int nnodes, T bw, T bucket,
+                       int *band, int cap, int *count, uint8_t *sc, int *flags, cudaStream_t st) {
+  const long long n = (long long)g.nx * g.ny * g.nz;
+  const size_t w = sizeof(T);
+  ReinitState rs;
+  size_t off = 0;
+  rs.mark = (int *)(sc + off); off += align256(sizeof(int) * n);
+  rs.tent = sc + off; off += align256(w * n);
+  rs.list[0] = (int *)(sc + off); off += align256(sizeof(int) * n);
+  rs.list[1] = (int *)(sc + off); off += align256(sizeof(int) * n);
+  rs.acc = (int *)(sc + off); off += align256(sizeof(int) * n);
+  rs.cnt = (int *)(sc + off); off += align256(sizeof(int) * 8);
+  int *partial = (int *)(sc + off);
+  const T inf = bw + T(1.5);  // PHI_INF, LevelSet.c:64
+  const int dense = grid_for(n, REINIT_THREADS), sparse = 148 * 8;
+  const int nodeb = nnodes > 0 ? (nnodes + REINIT_THREADS - 1) / REINIT_THREADS : 1;
+  cudaMemsetAsync(rs.cnt, 0, sizeof(int) * 8, st);
+  reinit_init_kernel<T><<<dense, REINIT_THREADS, 0, st>>>(phi, n, inf, rs.mark);
+  if (nnodes > 0) reinit_seed_kernel<T, DIM><<<nodeb, REINIT_THREADS, 0, st>>>(g, phi, nodes, nnodes, rs.mark);
+  const int nb = (int)ceil((double)bw / (double)bucket) + REINIT_TAIL;
+  for (int sign = -1; sign <= 1; sign += 2) {
+    reinit_side_kernel<T><<<dense, REINIT_THREADS, 0, st>>>(n, rs);
+    if (nnodes > 0)
+      reinit_push_seeds_kernel<T, DIM><<<nodeb, REINIT_THREADS, 0, st>>>(g, phi, nodes, nnodes, rs, sign, bw, inf);
+    int in = 0;
+    for (int b = 0; b < nb; ++b) {
+      const T thr = bucket * (T)(b + 1);
+      reinit_accept_kernel<T><<<sparse, REINIT_THREADS, 0, st>>>(phi, rs, in, sign, thr, bw);
+      reinit_relax_kernel<T, DIM><<<sparse, REINIT_THREADS, 0, st>>>(g, phi, rs, in ^ 1, sign, bw, inf);
+      reinit_next_kernel<<<1, 1, 0, st>>>(rs, in);
+      in ^= 1;
+    }
+    reinit_finish_side_kernel<<<1, 1, 0, st>>>(rs, in, flags);
+  }
+  reinit_status_kernel<<<1, 1, 0, st>>>(rs, flags);
+  // band: the fixed points in grid order
+  int *flag = rs.list[0], *offs = rs.list[0];
+  const int nblk = (int)((n + SCAN_BLOCK - 1) / SCAN_BLOCK);
+  reinit_band_flags_kernel<<<dense, REINIT_THREADS, 0, st>>>(rs.mark, n, flag);
+  scan_blocks_kernel<<<nblk, SCAN_BLOCK, 0, st>>>(flag, (int)n, offs, partial);
+  scan_partials_kernel<<<1, SCAN_BLOCK, 0, st>>>(partial, nblk);
+  scan_add_kernel<<<nblk, SCAN_BLOCK, 0, st>>>(offs, (int)n, partial, nblk, count, cap, flags);
+  reinit_band_write_kernel<<<dense, REINIT_THREADS, 0, st>>>(g, rs.mark, offs, n, band, cap);
+}
+
+int launch_reinit(const Geom &g, int dtype, void *phi, const dcell_irregular_node *nodes, int nnodes, double bw,
+                  double bucket, int *band, int cap, int *count, void *scratch, int *flags, cudaStream_t st) {
+  const bool is2d = g.nz == 1;
+  uint8_t *sc = (uint8_t *)scratch;
+  if (dtype == DCELL_F64) {
+    if (is2d) reinit_run<double, 2>(g, (double *)phi, nodes, nnodes, bw, bucket, band, cap, count, sc, flags, st);
+    else reinit_run<double, 3>(g, (double *)phi, nodes, nnodes, bw, bucket, band, cap, count, sc, flags, st);
+  } else {
+    if (is2d) reinit_run<float, 2>(g, (float *)phi, nodes, nnodes, (float)bw, (float)bucket, band, cap, count, sc, flags, st);
+    else reinit_run<float, 3>(g, (float *)phi, nodes, nnodes, (float)bw, (float)bucket, band, cap, count, sc, flags, st);
   }
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }

@@ -163,6 +163,29 @@ def max_velocity(vel: torch.Tensor, h, raw_nodes: torch.Tensor, count: torch.Ten
     return out
 
 
+def reinitialize(phi: torch.Tensor, raw_nodes: torch.Tensor, count, band_width: float = 6.0, bucket: float = 1.0 / 64,
+                 origin=(0, 0, 0), flags: Optional[torch.Tensor] = None):
+    """Narrow-band reinitialisation of phi in place (cell units; the
+    reference's LevelSetReinitialize, LevelSetMethod/FastMarching.c:11-146,
+    after its LevelSetResize) from the irregular nodes of phi (raw buffer and
+    count as irregular_nodes returns them).  Returns the band, (nb, 3) int32
+    global indices in grid order."""
+    _require_cuda(phi, raw_nodes, flags)
+    nn = int(count.item()) if isinstance(count, torch.Tensor) else int(count)
+    cap = phi.numel()
+    band = torch.empty((max(cap, 1), 3), dtype=torch.int32, device=phi.device)
+    nb = torch.zeros(1, dtype=torch.int32, device=phi.device)
+    g = geom(phi.shape, 1.0, origin)
+    sb = int(lib().dcell_reinit_scratch_bytes(ctypes.byref(g), _dtype_code(phi)))
+    scratch = torch.empty(sb + 256, dtype=torch.uint8, device=phi.device)
+    base = scratch.data_ptr()
+    off = (-base) % 256
+    check(lib().dcell_reinitialize(ctypes.byref(g), _dtype_code(phi), _ptr(phi), _ptr(raw_nodes), nn,
+                                   float(band_width), float(bucket), _ptr(band), cap, _ptr(nb),
+                                   ctypes.c_void_p(base + off), sb, _ptr(flags), _stream()))
+    return band[: int(nb.item())]
+
+
 def volume(phi: torch.Tensor, h, eps: float):
     """Enclosed volume through the smoothed Heaviside (FP64, deterministic)."""
     _require_cuda(phi)

@@ -71,6 +71,8 @@ def lib():
         L.orc_max_velocity.restype = d
         L.orc_volume.argtypes = [vp, vp, d]
         L.orc_volume.restype = d
+        L.orc_reinit.argtypes = [vp, vp, vp, l, d, d, vp, l]
+        L.orc_reinit.restype = l
         _LIB = L
     return _LIB
 
@@ -197,3 +199,22 @@ def volume(phi, h, eps):
     phi = np.ascontiguousarray(phi, dtype=np.float64)
     g = geom(phi.shape, h)
     return lib().orc_volume(ctypes.byref(g), _ptr(phi), float(eps))
+
+
+def reinit(phi, nodes, band_width=6.0, bucket=1.0 / 64, origin=(0, 0, 0)):
+    """Bucketed fast-marching reinitialisation (orc_reinit; the reference's
+    LevelSetReinitialize, FastMarching.c:11-146, with buckets of width
+    `bucket` cells in place of its heap).  phi in cell units; nodes: (n, 18)
+    irregular-node rows of phi.  Returns (phi, band (nb, 3) int32, grid order)."""
+    phi = np.array(phi, dtype=np.float64, copy=True, order="C")
+    g = geom(phi.shape, 1.0, origin)
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64).reshape(-1, NODE_W)
+    cap = phi.size
+    band = np.zeros((cap, 3), dtype=np.int32)
+    n = lib().orc_reinit(ctypes.byref(g), _ptr(phi), _ptr(nodes), nodes.shape[0], float(band_width), float(bucket),
+                         _ptr(band), cap)
+    if n == -1:
+        raise FloatingPointError("fast-marching update is not a number")
+    if n < 0:
+        raise RuntimeError("fast marching did not settle within the buckets")
+    return phi, band[:n].copy()

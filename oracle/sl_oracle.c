@@ -739,3 +739,216 @@ ORC_EXPORT double orc_volume(const orc_geom *g, const double *phi, double eps) {
   }
   return acc * cell;
 }
+
+/* ---------------------------------------------------------------------------
+ * Narrow-band reinitialisation by bucketed fast marching.
+ *
+ * The reference (LevelSetReinitialize, LevelSetMethod/FastMarching.c:11-41)
+ * resets phi to +/-PHI_INF (PHI_INF = bandWidth + 1.5, LevelSet.c:64), seeds
+ * the orthogonal-projection irregular nodes (axis == -1) with
+ * signCenter * |op| (FMM_InitializeEikonal, :43-89), and marches each side
+ * (sign -1, then +1) outwards with a binary heap (FMM_SolveEikonal, :94-146):
+ * pop the smallest tentative value, stop past bandWidth, fix it, and push its
+ * 4/6 neighbours with the second-order Rickett-Fomel update
+ * (FMM_PushNeighbors2D FastMarching2D.c:103-185, FMM_PushNeighbors3D
+ * FastMarching3D.c:13-101, AccumulateCoef FastMarching2D.c:33-99).
+ *
+ * Here the heap is replaced by buckets of width `bucket` (cells): every
+ * tentative value below (b+1)*bucket (and <= bandWidth) is fixed together,
+ * then the neighbours of the newly fixed points are re-evaluated with the
+ * reference's update and keep the smallest value any evaluation gave them.
+ * Each evaluation sees what the heap had fixed when it popped the pushing
+ * point: the seeds and the marched points whose value is not larger than the
+ * pusher's.  A point's update only reads fixed points, so the result does
+ * not depend on the order the points of a bucket are handled in: the GPU
+ * kernels follow exactly this procedure.  It equals the heap's result except
+ * where a point depends on another point of its own bucket or the heap pops
+ * out of value order.  Neighbours outside the grid are skipped (the reference reads them
+ * out of bounds; its bands stay inside, Resize.c).  The band comes out in
+ * grid order (x fastest) instead of the reference's march order.
+ * Returns the band length; -1 if an update is not a number (where the
+ * reference exits), -2 if points were still tentative after the last bucket.
+ */
+#define FMM_REINIT_TAIL 16
+
+/* AccumulateCoef, FastMarching2D.c:33-99: the one-sided (1st or 2nd order)
+ * difference of the upwind side along one axis, p[-3..3] centred on the point. */
+static void fmm_accumulate(double bw, const double *p, double *a, double *b, double *c) {
+  const double D2p = (3 * p[0] - 4 * p[1] + p[2]) / 2.;
+  const double D2m = (3 * p[0] - 4 * p[-1] + p[-2]) / 2.;
+  const double D1p = p[0] - p[1];
+  const double D1m = p[0] - p[-1];
+  double Dm, am, bm, cm, Dp, ap, bp, cp, t;
+  if (0 <= p[1] && p[1] < bw && 0 <= p[2] && p[2] < bw && D2p > 0) {
+    t = (4 * p[1] - p[2]) / 3;
+    ap = 9. / 4.;
+    bp = -9. / 2. * t;
+    cp = 9. / 4. * t * t;
+    Dp = D2p;
+  } else if (0 <= p[1] && p[1] < bw && D1p > 0) {
+    ap = 1.;
+    bp = -2. * p[1];
+    cp = p[1] * p[1];
+    Dp = D1p;
+  } else {
+    ap = bp = cp = Dp = 0;
+  }
+  if (0 <= p[-1] && p[-1] < bw && 0 <= p[-2] && p[-2] < bw && D2m > 0) {
+    t = (4 * p[-1] - p[-2]) / 3;
+    am = 9. / 4.;
+    bm = -9. / 2. * t;
+    cm = 9. / 4. * t * t;
+    Dm = D2m;
+  } else if (0 <= p[-1] && p[-1] < bw && D1m > 0) {
+    am = 1;
+    bm = -2. * p[-1];
+    cm = p[-1] * p[-1];
+    Dm = D1m;
+  } else {
+    am = bm = cm = Dm = 0;
+  }
+  if (Dm > Dp) {
+    *a += am;
+    *b += bm;
+    *c += cm;
+  } else {
+    *a += ap;
+    *b += bp;
+    *c += cp;
+  }
+}
+
+/* The update of point (i,j,k) from its fixed neighbours on side `sign`
+ * (FMM_PushNeighbors3D :40-81 / 2D :126-157): 7-point lines per axis,
+ * PHI_INF outside the grid, quadratic a d^2 + b d + c = 0, larger root. */
+static double fmm_update(const orc_geom *g, const double *phi, const unsigned char *mark, int i, int j, int k,
+                         int sign, double inf, double lim) {
+  const int dim = g->nz == 1 ? 2 : 3;
+  double a = 0, b = 0, c = -1, line[7];
+  for (int ax = 0; ax < dim; ++ax) {
+    for (int m = 0; m < 7; ++m) {
+      int q[3] = {i, j, k};
+      q[ax] += m - 3;
+      const int lo = ax == 0 ? g->px : ax == 1 ? g->py : g->pz;
+      const int n = ax == 0 ? g->nx : ax == 1 ? g->ny : g->nz;
+      if (q[ax] < lo || q[ax] > lo + n - 1) {
+        line[m] = inf;
+      } else {
+        const size_t r = gidx(g, q[0], q[1], q[2]);
+        const double v = sign * phi[r];
+        line[m] = (mark[r] == 2 && v > lim) ? inf : v;  /* marched later than the pushing point: not yet known */
+      }
+    }
+    fmm_accumulate(inf, line + 3, &a, &b, &c);
+  }
+  const double disc = sqrt(b * b - 4 * a * c);
+  double d1 = (-b + disc) / (2 * a);
+  if (d1 != d1) d1 = -b / (2 * a);
+  return d1;
+}
+
+static const int kStar[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+
+/* mark: 0 far, 1 tentative (in the list), 2 fixed by the march, 3 seed.
+ * The pushes of point (i,j,k) -- value lim on this side -- see what the heap
+ * had fixed when it popped that point: the seeds and the marched points of
+ * value <= lim. */
+static int fmm_relax(const orc_geom *g, double *phi, double *tent, unsigned char *mark, size_t *list, size_t *nlist,
+                     int i, int j, int k, int sign, double bw, double inf, double lim) {
+  const int nn = g->nz == 1 ? 4 : 6;
+  for (int s = 0; s < nn; ++s) {
+    const int x = i + kStar[s][0], y = j + kStar[s][1], z = k + kStar[s][2];
+    if (x < g->px || x >= g->px + g->nx || y < g->py || y >= g->py + g->ny || z < g->pz || z >= g->pz + g->nz)
+      continue;
+    const size_t q = gidx(g, x, y, z);
+    if (sign * phi[q] < bw) continue;  /* fixed, or the other side */
+    const double v = fmm_update(g, phi, mark, x, y, z, sign, inf, lim);
+    if (v != v) return -1;
+    if (v < tent[q]) tent[q] = v;
+    if (mark[q] == 0) {
+      mark[q] = 1;
+      list[(*nlist)++] = q;
+    }
+  }
+  return 0;
+}
+
+ORC_EXPORT long orc_reinit(const orc_geom *g, double *phi, const double *nodes, long nnodes, double bw,
+                           double bucket, int *band, long cap) {
+  const double inf = bw + 1.5;
+  const size_t n = (size_t)g->nx * g->ny * g->nz;
+  const int is2d = g->nz == 1;
+  unsigned char *mark = calloc(n, 1);
+  double *tent = malloc(sizeof(double) * n);
+  size_t *list = malloc(sizeof(size_t) * n), *acc = malloc(sizeof(size_t) * n);
+  long status = 0;
+  for (size_t q = 0; q < n; ++q) phi[q] = phi[q] > 0 ? inf : -inf;  /* FastMarching.c:28-30 */
+  for (long r = 0; r < nnodes; ++r) {                                  /* FastMarching.c:57-70 */
+    const double *nd = nodes + 18 * r;
+    if ((int)nd[3] != -1) continue;
+    const size_t q = gidx(g, (int)nd[0], (int)nd[1], (int)nd[2]);
+    const double ox = nd[11], oy = nd[12], oz = nd[13];
+    phi[q] = nd[5] * (is2d ? sqrt(ox * ox + oy * oy) : sqrt(ox * ox + oy * oy + oz * oz));
+    mark[q] = 3;
+  }
+  for (int sign = -1; sign <= 1 && status == 0; sign += 2) {
+    size_t nl = 0;
+    for (size_t q = 0; q < n; ++q) {
+      tent[q] = HUGE_VAL;
+      if (mark[q] == 1) mark[q] = 0;
+    }
+    for (long r = 0; r < nnodes && status == 0; ++r) {  /* FastMarching.c:72-84 */
+      const double *nd = nodes + 18 * r;
+      if ((int)nd[3] != -1) continue;
+      const int x = (int)nd[0], y = (int)nd[1], z = (int)nd[2];
+      if (sign * phi[gidx(g, x, y, z)] >= 0.)
+        status = fmm_relax(g, phi, tent, mark, list, &nl, x, y, z, sign, bw, inf, -HUGE_VAL);
+    }
+    /* a fixed number of buckets: past bandWidth every bucket fixes all that
+       is left <= bandWidth, and FMM_REINIT_TAIL more of them let the last
+       pushes settle; a list still not empty after that is an error */
+    const long nb = (long)ceil(bw / bucket) + FMM_REINIT_TAIL;
+    for (long b = 0; b < nb && status == 0; ++b) {
+      const double thr = bucket * (double)(b + 1);
+      size_t na = 0, keep = 0;
+      for (size_t t = 0; t < nl; ++t) {
+        const size_t q = list[t];
+        const double v = tent[q];
+        if (v < thr && v <= bw) {
+          phi[q] = sign * v;
+          mark[q] = 2;
+          acc[na++] = q;
+        } else if (v <= bw) {
+          list[keep++] = q;
+        } else {
+          mark[q] = 0;  /* past the band: never fixed unless a later update lowers it */
+        }
+      }
+      nl = keep;
+      for (size_t t = 0; t < na && status == 0; ++t) {
+        const size_t q = acc[t];
+        const int x = g->px + (int)(q % g->nx), y = g->py + (int)((q / g->nx) % g->ny),
+                  z = g->pz + (int)(q / ((size_t)g->nx * g->ny));
+        status = fmm_relax(g, phi, tent, mark, list, &nl, x, y, z, sign, bw, inf, sign * phi[q]);
+      }
+    }
+    if (nl > 0 && status == 0) status = -2;
+  }
+  long count = 0;
+  if (status == 0) {
+    for (size_t q = 0; q < n; ++q)
+      if (mark[q] >= 2) {
+        if (count < cap) {
+          band[3 * count + 0] = g->px + (int)(q % g->nx);
+          band[3 * count + 1] = g->py + (int)((q / g->nx) % g->ny);
+          band[3 * count + 2] = g->pz + (int)(q / ((size_t)g->nx * g->ny));
+        }
+        ++count;
+      }
+  }
+  free(mark);
+  free(tent);
+  free(list);
+  free(acc);
+  return status ? status : count;
+}

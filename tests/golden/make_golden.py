@@ -93,8 +93,26 @@ def run_rk2(phi, vel_n, vel_half, band, h, origin, dt):
     return half, full, nodes_half, nodes_full
 
 
+def run_reinit(ls):
+    """LevelSetReinitialize (FastMarching.c:11-41) of a reference level set
+    after an irregular-node pass: its input phi and nodes, output phi and band."""
+    nodes = ls.irregular_nodes(surface=False)
+    phi_in, origin, shape = ls.get_phi().copy(), ls.origin, ls.shape
+    ls.reinitialize()
+    assert ls.shape == shape and ls.origin == origin, "fixture case must not trigger LevelSetResize"
+    return dict(phi_in=phi_in, nodes=nodes, origin=np.array(origin), phi=ls.get_phi().copy(), band=ls.band().copy(),
+                band_width=ls.param("bandWidth"))
+
+
 def main():
     assert R.available(), "build oracle/_ref first: make -C oracle ref"
+    # fast-marching reinitialisation: a sphere and a circle as the reference's
+    # own initialisers build them (off-grid centres, no symmetric ties)
+    r3 = run_reinit(R.RefLevelSet.sphere(1.0 / 20, (0.4512, 0.3371, 0.5618), 0.2))
+    r2 = run_reinit(R.RefLevelSet.circle(1.0 / 64, (0.4512, 0.5371), 0.2))
+    np.savez_compressed(os.path.join(OUT, "reinit.npz"), **{k + "3": v for k, v in r3.items()},
+                        **{k + "2": v for k, v in r2.items()})
+
     h3 = 1.0 / 40
     # 3D: non-cubic grid, non-zero (partly negative) global origin
     shape3, origin3 = (20, 22, 24), (5, -3, 7)
