@@ -220,6 +220,60 @@ def reference_linear_rate(phi, vel, h, dt, nplanes=24):
     return xs.size / t
 
 
+def reinit_case(torch, N, dev):
+    """The 256^3 sphere of the workload in cell units, its band (|phi| < 6
+    cells, 3 cells inside the grid) and the GPU irregular nodes of it."""
+    from dcell_b200 import fields
+    from dcell_b200 import levelset as L
+    phi = (fields.sphere_sdf(N, device=dev) * N).contiguous()
+    band = fields.band_of(phi, 6.0, margin=3).to(dev)
+    raw, count = L.irregular_nodes(phi, 1.0, band, with_surface=False)
+    return phi, band, raw, count
+
+
+def timed_reinit(torch, phi, raw, count, dtype, K=5):
+    """GPU reinitialisation (bucketed fast marching, dcell_reinitialize) of the
+    case, CUDA events around each call on a fresh copy; median ms and the
+    result of the last call."""
+    from dcell_b200 import levelset as L
+    x = phi.to(dtype)
+    nn = int(count.item())
+    ms = []
+    for k in range(K + 1):
+        y = x.clone()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        band = L.reinitialize(y, raw, nn, 6.0, 1.0 / 64)
+        e1.record()
+        torch.cuda.synchronize()
+        if k:
+            ms.append(e0.elapsed_time(e1))
+    ms.sort()
+    return ms[len(ms) // 2], y, band
+
+
+def reference_reinit(phi, band):
+    """The reference's own LevelSetReinitialize (FastMarching.c:11-146, heap
+    FMM, FP64, one core) on the same phi after its own irregular-node pass."""
+    import numpy as np
+
+    from oracle import reference as R
+    if not R.available():
+        return None
+    N = phi.shape[0]
+    ls = R.RefLevelSet.create(1.0 / N, (0, 0, 0), (N, N, N))
+    ls.set_phi(phi.double().cpu().numpy())
+    ls.set_band(band.cpu().numpy())
+    ls.update_irregular()
+    t0 = time.perf_counter()
+    ls.reinitialize()
+    t = time.perf_counter() - t0
+    out = ls.get_phi().copy()
+    nb = int(ls.L.dref_ls_band_length(ls.h))
+    ls.close()
+    return t, out, nb
+
+
 def e2e_rate(phi, vel, h, dt, K, torch):
     """Through the reference-facing C ABI with pinned FP64 host buffers
     (reference Grid layout): H2D of phi0 + velocity, TC step, D2H of phi,
@@ -376,6 +430,26 @@ def main():
                 ref_lin = reference_linear_rate(phi, vel, h, dt, nplanes=24)
                 if ref_lin:
                     line["cpu_baseline"]["reference_linear_advectsl_updates_per_s"] = ref_lin
+            # narrow-band reinitialisation of the same sphere (cell units), GPU vs the reference's heap FMM
+            rphi, rband, raw, count = reinit_case(torch, args.size, dev)
+            ms64, y64, b64 = timed_reinit(torch, rphi, raw, count, torch.float64)
+            ms32, _, _ = timed_reinit(torch, rphi, raw, count, torch.float32)
+            line["reinit"] = {"grid": [args.size] * 3, "band_points": int(b64.shape[0]),
+                              "seed_nodes": int(count.item()), "gpu_fp64_ms": ms64, "gpu_fp32_ms": ms32,
+                              "how": "dcell_reinitialize: bucketed fast marching (buckets of 1/64 cell), band "
+                                     "width 6, CUDA events, median of 5"}
+            if world == 1:
+                ref = reference_reinit(rphi, rband)
+                if ref:
+                    t, out, nb = ref
+                    import numpy as np
+                    got = y64.cpu().numpy()
+                    inb = np.abs(out) < 6.0
+                    d = np.abs(got - out)[inb]
+                    line["cpu_baseline"]["reference_fmm_reinit"] = {
+                        "ms": t * 1e3, "cores": 1, "band_points": nb, "kind": "reference",
+                        "gpu_fp64_vs_reference": {"max": float(d.max()), "mean": float(d.mean())},
+                        "gpu_fp64_speedup": t * 1e3 / ms64}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

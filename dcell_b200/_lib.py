@@ -95,6 +95,7 @@ def lib():
     L.dcell_ls_advect_sl.argtypes = [vp, G, vp, vp, vp, i, d, i, i, i, vp]
     L.dcell_ls_update_irregular_nodes.argtypes = [vp, G, vp, vp, i, i, i, vp, i, vp]
     L.dcell_ls_max_velocity.argtypes = [vp, G, vp, vp, i, vp]
+    L.dcell_ls_reinitialize.argtypes = [vp, G, vp, vp, i, d, i, vp, i, vp]
     L.dcell_tc_gemm_check.argtypes = [vp, vp, vp, vp]
     L.dcell_sl_adjoint.argtypes = [G, i, vp, vp, d, i, i, vp, vp, vp, vp]
     L.dcell_split_bf16.argtypes = [G, vp, vp, vp]
@@ -104,7 +105,8 @@ def lib():
     for name in ("dcell_sl_step", "dcell_irregular_nodes", "dcell_irregular_nodes_noalloc", "dcell_max_velocity",
                  "dcell_volume", "dcell_reinitialize",
                  "dcell_session_create", "dcell_session_destroy", "dcell_ls_advect_sl",
-                 "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_tc_gemm_check",
+                 "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_ls_reinitialize",
+                 "dcell_tc_gemm_check",
                  "dcell_sl_adjoint", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",
                  "dcell_sl_step_tc_split"):
         getattr(L, name).restype = i

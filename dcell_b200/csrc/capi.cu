@@ -288,6 +288,9 @@ static int session_flags_status(dcell_session *s, int flags) {
   if (flags & DCELL_FLAG_WAIT_TIMEOUT) FAIL(DCELL_ERR_TIMEOUT, "a device-side wait timed out");
   if (flags & DCELL_FLAG_CAPACITY) FAIL(DCELL_ERR_CAPACITY, "node capacity exceeded");
   if (flags & DCELL_FLAG_BAD_BAND) FAIL(DCELL_ERR_ARG, "a band entry lies outside the grid");
+  if (flags & DCELL_FLAG_NONFINITE) FAIL(DCELL_ERR_NONFINITE, "a fast-marching update is not a number");
+  if (flags & DCELL_FLAG_UNSETTLED)
+    FAIL(DCELL_ERR_UNSUPPORTED, "fast marching left points tentative after its last bucket");
   if (flags & DCELL_FLAG_DEPARTURE_CLAMPED)
     FAIL(DCELL_ERR_DEPARTURE, "a departure point left the grid; its sample was clamped to the grid");
   (void)s;
@@ -470,6 +473,52 @@ DCELL_API int dcell_ls_update_irregular_nodes(dcell_session *s, const dcell_geom
   const int ncopy = hv[1] < capacity ? hv[1] : capacity;
   if (ncopy > 0)
     DCELL_CUDA_CHECK(cudaMemcpy(nodes, s->nodes.p, (size_t)ncopy * sizeof(dcell_irregular_node), cudaMemcpyDeviceToHost));
+  return session_flags_status(s, hv[0]);
+}
+
+DCELL_API int dcell_ls_reinitialize(dcell_session *s, const dcell_geom *g, double *phi,
+                                    const dcell_irregular_node *nodes, int nnodes, double band_width, int precision,
+                                    int *band, int capacity, int *count) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (!phi || !count || nnodes < 0 || (nnodes > 0 && !nodes)) FAIL(DCELL_ERR_ARG, "phi, nodes and count are required");
+  if (capacity < 0 || (capacity > 0 && !band)) FAIL(DCELL_ERR_ARG, "invalid band buffer");
+  if (precision != DCELL_F32 && precision != DCELL_F64) FAIL(DCELL_ERR_ARG, "precision must be F32 or F64");
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long n = grid_points(g);
+  ENSURE(s->phi_64, n * sizeof(double));
+  int *dflags = (int *)s->small.p;
+  int *dcount = dflags + 1;
+  DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, 2 * sizeof(int), st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi_64.p, phi, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  void *dphi = s->phi_64.p;
+  if (precision == DCELL_F32) {
+    ENSURE(s->phi_32, n * sizeof(float));
+    if ((rc = launch_convert(s->phi_64.p, DCELL_F64, s->phi_32.p, DCELL_F32, n, st))) return rc;
+    dphi = s->phi_32.p;
+  }
+  ENSURE(s->nodes, (size_t)(nnodes > 0 ? nnodes : 1) * sizeof(dcell_irregular_node));
+  if (nnodes > 0)
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->nodes.p, nodes, (size_t)nnodes * sizeof(dcell_irregular_node),
+                                     cudaMemcpyHostToDevice, st));
+  const size_t sb = dcell_reinit_scratch_bytes(g, precision);
+  ENSURE(s->scratch, sb);
+  ENSURE(s->band, (size_t)(capacity > 0 ? capacity : 1) * 3 * sizeof(int));
+  rc = dcell_reinitialize(g, precision, dphi, (const dcell_irregular_node *)s->nodes.p, nnodes, band_width, 0.0,
+                          (int *)s->band.p, capacity, dcount, s->scratch.p, sb, dflags, st);
+  if (rc) return rc;
+  if (precision == DCELL_F32 && (rc = launch_convert(s->phi_32.p, DCELL_F32, s->phi_64.p, DCELL_F64, n, st)))
+    return rc;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(phi, s->phi_64.p, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  int hv[2] = {0, 0};
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(hv, dflags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  *count = hv[1];
+  const int ncopy = hv[1] < capacity ? hv[1] : capacity;
+  if (ncopy > 0)
+    DCELL_CUDA_CHECK(cudaMemcpy(band, s->band.p, (size_t)ncopy * 3 * sizeof(int), cudaMemcpyDeviceToHost));
   return session_flags_status(s, hv[0]);
 }
 

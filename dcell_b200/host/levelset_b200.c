@@ -9,10 +9,17 @@
  *                                        the reference's definition is renamed
  *                                        away when IrregularNodes.c is built)
  *   LevelSet_MaxVelocity                (LevelSetMethod/Advect.c:70-111; likewise)
+ *   LevelSetReinitialize                (LevelSetMethod/FastMarching.c:11-41; the
+ *                                        reference's definition is renamed to
+ *                                        LevelSetReinitialize_cpu when
+ *                                        FastMarching.c is built, and stays the
+ *                                        default)
  * Everything that calls them -- LevelSetAdvectAndReinit, the RK2 half/full
  * steps (AdvectRK2.c), the particle and implicit variants, DCell's ls->Advect
  * slot -- is unchanged and now runs the GPU path.  Fast-marching
- * reinitialisation stays the reference's CPU code.
+ * reinitialisation runs the reference's CPU code unless
+ * DCELL_LS_REINIT=gpu selects the GPU's bucketed march (dcell_reinitialize;
+ * within 1e-2 cells of the heap, band in grid order).
  *
  * The calls go through the C ABI of libdcell_ls.so (include/dcell_ls.h) with
  * the LevelSet's own FP64 arrays (Grid.v1, band Array data); a process-wide
@@ -23,6 +30,7 @@
  *   DCELL_LS_PRECISION=f32|f64
  *   DCELL_LS_INTERP=linear|cubic|cubic_separable|cubic_tc
  *   DCELL_LS_BACKTRACE=euler|midpoint
+ *   DCELL_LS_REINIT=cpu|gpu                (read at every call)
  * Errors come back as PetscErrorCode through SETERRQ with the library's
  * message; nothing exits.
  */
@@ -208,5 +216,67 @@ PetscErrorCode LevelSet_MaxVelocity(LevelSet ls, Grid velgrid) {
   rc = dcell_ls_max_velocity(s, &g, velgrid->v1, buf, len, &ls->maxVel);
   free(buf);
   if (rc) SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_max_velocity: %s", dcell_last_error());
+  PetscFunctionReturn(0);
+}
+
+/* The reference's own LevelSetReinitialize, renamed at link time. */
+PetscErrorCode LevelSetReinitialize_cpu(LevelSet ls);
+
+#undef __FUNCT__
+#define __FUNCT__ "LevelSetReinitialize"
+PetscErrorCode LevelSetReinitialize(LevelSet ls) {
+  dcell_session *s;
+  dcell_geom g;
+  dcell_irregular_node *buf;
+  int *bandbuf, rc, count = 0, i, cap;
+  const char *mode = getenv("DCELL_LS_REINIT");
+  const int len = ArrayLength(ls->irregularNodes);
+  const IrregularNode *nodes;
+  iCoor *band;
+  PetscErrorCode ierr;
+
+  PetscFunctionBegin;
+  if (!mode || strcmp(mode, "gpu")) {
+    ierr = LevelSetReinitialize_cpu(ls); CHKERRQ(ierr);
+    PetscFunctionReturn(0);
+  }
+  ierr = PetscLogEventBegin(EVENT_LevelSetReinitialize, 0, 0, 0, 0); CHKERRQ(ierr);
+  ierr = LevelSetB200Session(&s); CHKERRQ(ierr);
+  ierr = LevelSetResize(ls); CHKERRQ(ierr);  /* as the reference does first (FastMarching.c:25) */
+  b200_geom(ls->phi, &g);
+  nodes = (const IrregularNode *)ArrayGetData(ls->irregularNodes);
+  buf = (dcell_irregular_node *)calloc((size_t)(len > 0 ? len : 1), sizeof(dcell_irregular_node));
+  cap = ls->phi->SIZE;
+  bandbuf = (int *)malloc(sizeof(int) * 3 * (size_t)(cap > 0 ? cap : 1));
+  if (!buf || !bandbuf) {
+    free(buf);
+    free(bandbuf);
+    SETERRQ(PETSC_COMM_SELF, PETSC_ERR_MEM, "out of host memory");
+  }
+  for (i = 0; i < len; ++i) {
+    buf[i].pos[0] = nodes[i].pos.x;
+    buf[i].pos[1] = nodes[i].pos.y;
+    buf[i].pos[2] = nodes[i].pos.z;
+    buf[i].axis = nodes[i].axis;
+    buf[i].signCenter = nodes[i].signCenter;
+    buf[i].op[0] = nodes[i].op.x;
+    buf[i].op[1] = nodes[i].op.y;
+    buf[i].op[2] = nodes[i].op.z;
+  }
+  rc = dcell_ls_reinitialize(s, &g, ls->phi->v1, buf, len, ls->bandWidth, b200_precision, bandbuf, cap, &count);
+  free(buf);
+  if (rc) {
+    free(bandbuf);
+    SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_reinitialize: %s", dcell_last_error());
+  }
+  ierr = ArraySetSize(ls->band, count); CHKERRQ(ierr);
+  band = (iCoor *)ArrayGetData(ls->band);
+  for (i = 0; i < count; ++i) {
+    band[i].x = bandbuf[3 * i];
+    band[i].y = bandbuf[3 * i + 1];
+    band[i].z = bandbuf[3 * i + 2];
+  }
+  free(bandbuf);
+  ierr = PetscLogEventEnd(EVENT_LevelSetReinitialize, 0, 0, 0, 0); CHKERRQ(ierr);
   PetscFunctionReturn(0);
 }

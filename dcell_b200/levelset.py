@@ -119,7 +119,7 @@ def nodes_to_numpy(raw: torch.Tensor, count: int) -> np.ndarray:
 
 def nodes_to_rows(nodes: np.ndarray) -> np.ndarray:
     """Structured nodes -> (n, 18) float64 rows: pos, axis, shift, signCenter,
-    signFace, d, X, op, n, k (the oracle's record layout)."""
+    signFace, d, X, op, n, k (the row layout the test checkers use)."""
     r = np.zeros((len(nodes), 18))
     r[:, 0:3] = nodes["pos"]
     r[:, 3] = nodes["axis"]

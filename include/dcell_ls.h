@@ -291,6 +291,15 @@ DCELL_API int dcell_ls_update_irregular_nodes(dcell_session *s, const dcell_geom
                                     int nband, int with_surface, int precision, dcell_irregular_node *nodes,
                                     int capacity, int *count);
 
+/* LevelSetReinitialize(ls) after its LevelSetResize, on host arrays (see
+ * dcell_reinitialize): phi (FP64 host grid, overwritten), the irregular nodes
+ * of phi (as dcell_ls_update_irregular_nodes returns them; only axis, pos,
+ * signCenter and op are read), band_width = ls->bandWidth.  band (host int
+ * [capacity][3]) receives the new band in grid order, *count its length.
+ * precision: the arithmetic, DCELL_F64 or DCELL_F32. */
+DCELL_API int dcell_ls_reinitialize(dcell_session *s, const dcell_geom *g, double *phi, const dcell_irregular_node *nodes,
+                                    int nnodes, double band_width, int precision, int *band, int capacity, int *count);
+
 /* LevelSet_MaxVelocity(ls, velgrid) on host arrays. */
 DCELL_API int dcell_ls_max_velocity(dcell_session *s, const dcell_geom *g, const double *vel,
                           const dcell_irregular_node *nodes, int count, double *maxvel);
