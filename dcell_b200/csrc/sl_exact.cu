@@ -872,9 +872,15 @@ template <> struct OrdOf<float> { typedef unsigned int type; };
 struct ReinitState {
   int *mark;          // ReinitMark per point
   void *tent;         // OrdOf<T>::type per point
-  int *list[2];       // tentative lists (ping-pong)
+  int *near[2];       // tentative points below the window end (ping-pong)
+  int *far[2];        // tentative points at or past it (ping-pong)
   int *acc;           // points fixed in the current bucket
-  int *cnt;           // [0],[1] list lengths, [2] accepted, [3] error
+  int *err;           // bit 1: an update was not a number, bit 2: unsettled (global)
+};
+
+// list lengths of one side's march, in shared memory
+struct ReinitCounts {
+  int near[2], far[2], acc;
 };
 
 template <typename T>
@@ -951,34 +957,51 @@ __device__ T fmm_update_dev(const Geom &g, const T *__restrict__ phi, const int 
   return d1;
 }
 
+// Push neighbour s (STAR order) of (x,y,z): re-evaluate it if unfixed and
+// keep the smaller value.  A point whose value dropped below the window end `win` goes
+// on the near list (again, if it was there with a larger value: the first
+// copy to be fixed wins); a point seen for the first time at or past it goes
+// on the far list.  Values only fall and the window only grows, so a far
+// point is either improved into the near list or moved there when the window
+// passes it.
 template <typename T, int DIM>
-__device__ void fmm_relax_dev(const Geom &g, const T *__restrict__ phi, ReinitState st, int out, int x, int y, int z,
-                              int sign, T bw, T inf, T lim) {
+__device__ void fmm_relax_dev(const Geom &g, const T *__restrict__ phi, const ReinitState &st, ReinitCounts *c,
+                              int nout, int fcur, int x, int y, int z, int s, int sign, T bw, T inf, T lim, T win) {
   typedef typename OrdOf<T>::type O;
   O *tent = (O *)st.tent;
   constexpr int kStarDev[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-#pragma unroll
-  for (int s = 0; s < 2 * DIM; ++s) {
-    const int i = x + kStarDev[s][0], j = y + kStarDev[s][1], k = z + kStarDev[s][2];
-    if (i < 0 || i >= g.nx || j < 0 || j >= g.ny || k < 0 || k >= g.nz) continue;
-    const int q = (k * g.ny + j) * g.nx + i;
-    if (sign * phi[q] < bw) continue;  // fixed, or the other side
-    const T v = fmm_update_dev<T, DIM>(g, phi, st.mark, i, j, k, sign, inf, lim);
-    if (v != v) {
-      atomicExch(&st.cnt[3], 1);
-      continue;
+  const int i = x + kStarDev[s][0], j = y + kStarDev[s][1], k = z + kStarDev[s][2];
+  if (i < 0 || i >= g.nx || j < 0 || j >= g.ny || k < 0 || k >= g.nz) return;
+  const int q = (k * g.ny + j) * g.nx + i;
+  if (sign * phi[q] < bw) return;  // fixed, or the other side
+  const T v = fmm_update_dev<T, DIM>(g, phi, st.mark, i, j, k, sign, inf, lim);
+  if (v != v) {
+    atomicOr(st.err, 1);
+    return;
+  }
+  const O ov = ord_bits(v);
+  const O old = atomicMin(&tent[q], ov);
+  if (v < win) {
+    if (ov < old) {
+      atomicExch(&st.mark[q], RM_TENT);
+      st.near[nout][atomicAdd(&c->near[nout], 1)] = q;
     }
-    atomicMin(&tent[q], ord_bits(v));
-    if (atomicCAS(&st.mark[q], RM_FAR, RM_TENT) == RM_FAR) st.list[out][atomicAdd(&st.cnt[out], 1)] = q;
+  } else if (atomicCAS(&st.mark[q], RM_FAR, RM_TENT) == RM_FAR) {
+    st.far[fcur][atomicAdd(&c->far[fcur], 1)] = q;
   }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(REINIT_THREADS) reinit_init_kernel(T *phi, long long n, T inf, int *mark) {
+__global__ void __launch_bounds__(REINIT_THREADS) reinit_init_kernel(T *phi, long long n, T inf, int *mark,
+                                                                   void *tent_v, int *err) {
+  typedef typename OrdOf<T>::type O;
+  O *tent = (O *)tent_v;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     phi[q] = phi[q] > 0 ? inf : -inf;  // FastMarching.c:28-30
     mark[q] = RM_FAR;
+    tent[q] = ord_bits((T)INFINITY);
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *err = 0;
 }
 
 template <typename T, int DIM>
@@ -997,73 +1020,106 @@ __global__ void __launch_bounds__(REINIT_THREADS) reinit_seed_kernel(Geom g, T *
   mark[q] = RM_SEED;
 }
 
-// per side: tentative values back to +inf, tentative marks back to far
-template <typename T>
-__global__ void __launch_bounds__(REINIT_THREADS) reinit_side_kernel(long long n, ReinitState st) {
-  typedef typename OrdOf<T>::type O;
-  O *tent = (O *)st.tent;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    tent[q] = ord_bits((T)INFINITY);
-    if (st.mark[q] == RM_TENT) st.mark[q] = RM_FAR;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) st.cnt[0] = st.cnt[1] = st.cnt[2] = 0;
-}
+// The whole march of one side in one CTA (blockIdx.x 0: sign -1, 1: sign +1):
+// the sides touch disjoint points (each only ever reads the other's values,
+// which are negative on its scale and so never "known"), so they march
+// concurrently from one launch.  Tentative points below the window end
+// (REINIT_WINDOW buckets ahead) sit on the near list, which each bucket
+// scans; the far list is redistributed when the window moves on.  Per
+// bucket: accept, block barrier, relax, block barrier -- no kernel launches;
+// list lengths in shared memory.  Acceptance and values are those of the
+// single-list procedure (the oracle's): a point is fixed in the bucket its
+// value falls in, by the first of its near-list copies to get there.
+constexpr int REINIT_MARCH_THREADS = 1024;
+constexpr int REINIT_WINDOW = 16;
 
 template <typename T, int DIM>
-__global__ void __launch_bounds__(REINIT_THREADS) reinit_push_seeds_kernel(Geom g, const T *phi,
-                                                                         const dcell_irregular_node *nodes, int nnodes,
-                                                                         ReinitState st, int sign, T bw, T inf) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nnodes) return;
-  const dcell_irregular_node nd = nodes[r];
-  if (nd.axis != -1) return;
-  const int x = nd.pos[0] - g.px, y = nd.pos[1] - g.py, z = DIM == 3 ? nd.pos[2] - g.pz : 0;
-  if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) return;
-  if (sign * phi[(z * g.ny + y) * g.nx + x] >= 0)  // FastMarching.c:72-84
-    fmm_relax_dev<T, DIM>(g, phi, st, 0, x, y, z, sign, bw, inf, -(T)INFINITY);
-}
-
-// bucket b: fix list[in] entries below thr (and <= bw), keep the rest <= bw in list[out]
-template <typename T>
-__global__ void __launch_bounds__(REINIT_THREADS) reinit_accept_kernel(T *phi, ReinitState st, int in, int sign, T thr,
-                                                                     T bw) {
+__global__ void __launch_bounds__(REINIT_MARCH_THREADS) reinit_march_kernel(Geom g, T *phi,
+                                                                          const dcell_irregular_node *nodes,
+                                                                          int nnodes, ReinitState s0, ReinitState s1,
+                                                                          T bw, T inf, T bucket, int nb) {
   typedef typename OrdOf<T>::type O;
-  const O *tent = (const O *)st.tent;
-  const int n = st.cnt[in];
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int q = st.list[in][t];
-    const T v = ord_value(tent[q]);
-    if (v < thr && v <= bw) {
-      phi[q] = sign * v;
-      st.mark[q] = RM_MARCHED;
-      st.acc[atomicAdd(&st.cnt[2], 1)] = q;
-    } else if (v <= bw) {
-      st.list[in ^ 1][atomicAdd(&st.cnt[in ^ 1], 1)] = q;
-    } else {
-      st.mark[q] = RM_FAR;  // past the band unless a later push lowers it
+  const int sign = blockIdx.x == 0 ? -1 : 1;
+  const ReinitState st = blockIdx.x == 0 ? s0 : s1;
+  O *tent = (O *)st.tent;
+  __shared__ ReinitCounts c;
+  if (threadIdx.x == 0) c.near[0] = c.near[1] = c.far[0] = c.far[1] = c.acc = 0;
+  __syncthreads();
+  int in = 0, fcur = 0;
+  T win = bucket * (T)REINIT_WINDOW;
+  for (int r = threadIdx.x; r < nnodes * 2 * DIM; r += blockDim.x) {  // FastMarching.c:72-84, one neighbour each
+    const dcell_irregular_node nd = nodes[r / (2 * DIM)];
+    if (nd.axis != -1) continue;
+    const int x = nd.pos[0] - g.px, y = nd.pos[1] - g.py, z = DIM == 3 ? nd.pos[2] - g.pz : 0;
+    if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
+    if (sign * phi[(z * g.ny + y) * g.nx + x] >= 0)
+      fmm_relax_dev<T, DIM>(g, phi, st, &c, in, fcur, x, y, z, r % (2 * DIM), sign, bw, inf, -(T)INFINITY, win);
+  }
+  __syncthreads();
+  for (int b = 0; b < nb; ++b) {
+    const T thr = bucket * (T)(b + 1);
+    // accept what falls below this bucket's threshold; keep the rest of the window
+    const int n_in = c.near[in];
+    for (int t = threadIdx.x; t < n_in; t += blockDim.x) {
+      const int q = st.near[in][t];
+      if (st.mark[q] == RM_MARCHED) continue;
+      const T v = ord_value(tent[q]);
+      if (v < thr && v <= bw) {
+        if (atomicCAS(&st.mark[q], RM_TENT, RM_MARCHED) == RM_TENT) {
+          phi[q] = sign * v;
+          st.acc[atomicAdd(&c.acc, 1)] = q;
+        }
+      } else if (v <= bw) {
+        st.near[in ^ 1][atomicAdd(&c.near[in ^ 1], 1)] = q;
+      } else {
+        st.mark[q] = RM_FAR;  // past the band unless a later push lowers it
+      }
+    }
+    __syncthreads();
+    const int n_acc = c.acc;
+    for (int t = threadIdx.x; t < n_acc * 2 * DIM; t += blockDim.x) {  // one (point, neighbour) pair each
+      const int q = st.acc[t / (2 * DIM)];
+      const int x = q % g.nx, y = (q / g.nx) % g.ny, z = q / (g.nx * g.ny);
+      fmm_relax_dev<T, DIM>(g, phi, st, &c, in ^ 1, fcur, x, y, z, t % (2 * DIM), sign, bw, inf, sign * phi[q], win);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      c.near[in] = 0;
+      c.acc = 0;
+    }
+    __syncthreads();
+    in ^= 1;
+    if ((b + 1) % REINIT_WINDOW == 0) {  // the window moves on: far points now inside it join the near list
+      win = bucket * (T)(b + 1 + REINIT_WINDOW);
+      const int n_far = c.far[fcur];
+      for (int t = threadIdx.x; t < n_far; t += blockDim.x) {
+        const int q = st.far[fcur][t];
+        if (st.mark[q] == RM_MARCHED) continue;
+        const T v = ord_value(tent[q]);
+        if (v < win) {
+          if (v <= bw) {
+            st.mark[q] = RM_TENT;
+            st.near[in][atomicAdd(&c.near[in], 1)] = q;
+          } else {
+            st.mark[q] = RM_FAR;
+          }
+        } else {
+          st.far[fcur ^ 1][atomicAdd(&c.far[fcur ^ 1], 1)] = q;
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) c.far[fcur] = 0;
+      __syncthreads();
+      fcur ^= 1;
     }
   }
-}
-
-template <typename T, int DIM>
-__global__ void __launch_bounds__(REINIT_THREADS) reinit_relax_kernel(Geom g, const T *phi, ReinitState st, int out,
-                                                                    int sign, T bw, T inf) {
-  const int n = st.cnt[2];
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int q = st.acc[t];
-    const int x = q % g.nx, y = (q / g.nx) % g.ny, z = q / (g.nx * g.ny);
-    fmm_relax_dev<T, DIM>(g, phi, st, out, x, y, z, sign, bw, inf, sign * phi[q]);
-  }
-}
-
-// between buckets: the consumed list and the accepted list start empty
-__global__ void reinit_next_kernel(ReinitState st, int consumed) {
-  st.cnt[consumed] = 0;
-  st.cnt[2] = 0;
-}
-
-__global__ void reinit_finish_side_kernel(ReinitState st, int last, int *flags) {
-  if (st.cnt[last] > 0) st.cnt[3] = 2;  // still tentative after the last bucket
+  // still tentative (within the band) after the last bucket
+  bool left = false;
+  for (int t = threadIdx.x; t < c.near[in]; t += blockDim.x)
+    if (st.mark[st.near[in][t]] == RM_TENT && ord_value(tent[st.near[in][t]]) <= bw) left = true;
+  for (int t = threadIdx.x; t < c.far[fcur]; t += blockDim.x)
+    if (st.mark[st.far[fcur][t]] == RM_TENT && ord_value(tent[st.far[fcur][t]]) <= bw) left = true;
+  if (left) atomicOr(st.err, 2);
 }
 
 __global__ void __launch_bounds__(REINIT_THREADS) reinit_band_flags_kernel(const int *mark, long long n, int *flag) {
@@ -1084,9 +1140,9 @@ __global__ void __launch_bounds__(REINIT_THREADS) reinit_band_write_kernel(Geom 
     }
 }
 
-__global__ void reinit_status_kernel(const ReinitState st, int *flags) {
-  if (st.cnt[3] == 1) raise_flag(flags, FLAG_NONFINITE);
-  if (st.cnt[3] == 2) raise_flag(flags, FLAG_UNSETTLED);
+__global__ void reinit_status_kernel(const int *err, int *flags) {
+  if (*err & 1) raise_flag(flags, FLAG_NONFINITE);
+  if (*err & 2) raise_flag(flags, FLAG_UNSETTLED);
 }
 }  // namespace dcell
 
@@ -1182,14 +1238,16 @@ int launch_max_velocity(const Geom &g, int dtype, const void *vel, const dcell_i
 
 // ---------------------------------------------------------------------------
 // Reinitialisation.  Scratch layout (bytes, each part 256-aligned): mark
-// int[n], tentative values [n] (8 or 4 bytes), two tentative lists int[n],
-// accepted list int[n], counters int[8]; the band scan reuses the two lists.
+// int[n]; tentative values [n] (8 or 4 bytes; the sides touch disjoint
+// points, so they share it); per side two near lists, two far lists and an
+// accepted list, int[n] each; the error word; the band scan's block totals.
+// The band scan reuses the first list.
 static size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
 size_t reinit_scratch_bytes(long long n, int dtype) {
   const size_t w = dtype == DCELL_F64 ? 8 : 4;
   const size_t nblk = ((size_t)n + SCAN_BLOCK - 1) / SCAN_BLOCK;
-  return align256(sizeof(int) * n) + align256(w * n) + 3 * align256(sizeof(int) * n) + align256(sizeof(int) * 8) +
+  return align256(sizeof(int) * n) + align256(w * n) + 10 * align256(sizeof(int) * n) + align256(sizeof(int) * 8) +
          align256(sizeof(int) * (nblk + 1));
 }
 
@@ -1197,46 +1255,40 @@ template <typename T, int DIM>
 static void reinit_run(const Geom &g, T *phi, const dcell_irregular_node *nodes, int nnodes, T bw, T bucket,
                        int *band, int cap, int *count, uint8_t *sc, int *flags, cudaStream_t st) {
   const long long n = (long long)g.nx * g.ny * g.nz;
-  const size_t w = sizeof(T);
-  ReinitState rs;
   size_t off = 0;
-  rs.mark = (int *)(sc + off); off += align256(sizeof(int) * n);
-  rs.tent = sc + off; off += align256(w * n);
-  rs.list[0] = (int *)(sc + off); off += align256(sizeof(int) * n);
-  rs.list[1] = (int *)(sc + off); off += align256(sizeof(int) * n);
-  rs.acc = (int *)(sc + off); off += align256(sizeof(int) * n);
-  rs.cnt = (int *)(sc + off); off += align256(sizeof(int) * 8);
+  int *mark = (int *)(sc + off); off += align256(sizeof(int) * n);
+  void *tent = sc + off; off += align256(sizeof(T) * n);
+  ReinitState side[2];
+  for (int k = 0; k < 2; ++k) {
+    side[k].mark = mark;
+    side[k].tent = tent;
+    for (int l = 0; l < 2; ++l) {
+      side[k].near[l] = (int *)(sc + off); off += align256(sizeof(int) * n);
+      side[k].far[l] = (int *)(sc + off); off += align256(sizeof(int) * n);
+    }
+    side[k].acc = (int *)(sc + off); off += align256(sizeof(int) * n);
+  }
+  int *err = (int *)(sc + off); off += align256(sizeof(int) * 8);
+  side[0].err = side[1].err = err;
   int *partial = (int *)(sc + off);
   const T inf = bw + T(1.5);  // PHI_INF, LevelSet.c:64
-  const int dense = grid_for(n, REINIT_THREADS), sparse = 148 * 8;
-  const int nodeb = nnodes > 0 ? (nnodes + REINIT_THREADS - 1) / REINIT_THREADS : 1;
-  cudaMemsetAsync(rs.cnt, 0, sizeof(int) * 8, st);
-  reinit_init_kernel<T><<<dense, REINIT_THREADS, 0, st>>>(phi, n, inf, rs.mark);
-  if (nnodes > 0) reinit_seed_kernel<T, DIM><<<nodeb, REINIT_THREADS, 0, st>>>(g, phi, nodes, nnodes, rs.mark);
+  const int dense = grid_for(n, REINIT_THREADS);
+  reinit_init_kernel<T><<<dense, REINIT_THREADS, 0, st>>>(phi, n, inf, mark, tent, err);
+  if (nnodes > 0)
+    reinit_seed_kernel<T, DIM><<<(nnodes + REINIT_THREADS - 1) / REINIT_THREADS, REINIT_THREADS, 0, st>>>(
+        g, phi, nodes, nnodes, mark);
   const int nb = (int)ceil((double)bw / (double)bucket) + REINIT_TAIL;
-  for (int sign = -1; sign <= 1; sign += 2) {
-    reinit_side_kernel<T><<<dense, REINIT_THREADS, 0, st>>>(n, rs);
-    if (nnodes > 0)
-      reinit_push_seeds_kernel<T, DIM><<<nodeb, REINIT_THREADS, 0, st>>>(g, phi, nodes, nnodes, rs, sign, bw, inf);
-    int in = 0;
-    for (int b = 0; b < nb; ++b) {
-      const T thr = bucket * (T)(b + 1);
-      reinit_accept_kernel<T><<<sparse, REINIT_THREADS, 0, st>>>(phi, rs, in, sign, thr, bw);
-      reinit_relax_kernel<T, DIM><<<sparse, REINIT_THREADS, 0, st>>>(g, phi, rs, in ^ 1, sign, bw, inf);
-      reinit_next_kernel<<<1, 1, 0, st>>>(rs, in);
-      in ^= 1;
-    }
-    reinit_finish_side_kernel<<<1, 1, 0, st>>>(rs, in, flags);
-  }
-  reinit_status_kernel<<<1, 1, 0, st>>>(rs, flags);
+  reinit_march_kernel<T, DIM><<<2, REINIT_MARCH_THREADS, 0, st>>>(g, phi, nodes, nnodes, side[0], side[1], bw, inf,
+                                                                  bucket, nb);
+  reinit_status_kernel<<<1, 1, 0, st>>>(err, flags);
   // band: the fixed points in grid order
-  int *flag = rs.list[0], *offs = rs.list[0];
+  int *flag = side[0].near[0], *offs = side[0].near[0];
   const int nblk = (int)((n + SCAN_BLOCK - 1) / SCAN_BLOCK);
-  reinit_band_flags_kernel<<<dense, REINIT_THREADS, 0, st>>>(rs.mark, n, flag);
+  reinit_band_flags_kernel<<<dense, REINIT_THREADS, 0, st>>>(mark, n, flag);
   scan_blocks_kernel<<<nblk, SCAN_BLOCK, 0, st>>>(flag, (int)n, offs, partial);
   scan_partials_kernel<<<1, SCAN_BLOCK, 0, st>>>(partial, nblk);
   scan_add_kernel<<<nblk, SCAN_BLOCK, 0, st>>>(offs, (int)n, partial, nblk, count, cap, flags);
-  reinit_band_write_kernel<<<dense, REINIT_THREADS, 0, st>>>(g, rs.mark, offs, n, band, cap);
+  reinit_band_write_kernel<<<dense, REINIT_THREADS, 0, st>>>(g, mark, offs, n, band, cap);
 }
 
 int launch_reinit(const Geom &g, int dtype, void *phi, const dcell_irregular_node *nodes, int nnodes, double bw,

@@ -767,7 +767,8 @@ ORC_EXPORT double orc_volume(const orc_geom *g, const double *phi, double eps) {
  * out of bounds; its bands stay inside, Resize.c).  The band comes out in
  * grid order (x fastest) instead of the reference's march order.
  * Returns the band length; -1 if an update is not a number (where the
- * reference exits), -2 if points were still tentative after the last bucket.
+ * reference exits), -2 if a point within the band width was still tentative
+ * after the last bucket.
  */
 #define FMM_REINIT_TAIL 16
 
@@ -906,7 +907,8 @@ ORC_EXPORT long orc_reinit(const orc_geom *g, double *phi, const double *nodes, 
     }
     /* a fixed number of buckets: past bandWidth every bucket fixes all that
        is left <= bandWidth, and FMM_REINIT_TAIL more of them let the last
-       pushes settle; a list still not empty after that is an error */
+       pushes settle; a point <= bandWidth still tentative after that is an
+       error */
     const long nb = (long)ceil(bw / bucket) + FMM_REINIT_TAIL;
     for (long b = 0; b < nb && status == 0; ++b) {
       const double thr = bucket * (double)(b + 1);
@@ -932,7 +934,8 @@ ORC_EXPORT long orc_reinit(const orc_geom *g, double *phi, const double *nodes, 
         status = fmm_relax(g, phi, tent, mark, list, &nl, x, y, z, sign, bw, inf, sign * phi[q]);
       }
     }
-    if (nl > 0 && status == 0) status = -2;
+    for (size_t t = 0; t < nl && status == 0; ++t)
+      if (tent[list[t]] <= bw) status = -2;  /* a point that could still be fixed */
   }
   long count = 0;
   if (status == 0) {
