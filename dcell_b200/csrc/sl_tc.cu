@@ -747,7 +747,9 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
       }
       constexpr uint32_t idesc = instr_desc_bf16(kTile, kCoef);
       for (int j = 0; j < nsteps && !err; ++j) {
-        if (!mbar_wait_sleep(afull, (uint32_t)j & 1u)) { err = true; break; }
+        // the issuer polls without a suspend hint: it reacts a little sooner
+        // to the fourth arrival (measured ~1% on the 256^3 step)
+        if (!mbar_wait(afull, (uint32_t)j & 1u)) { err = true; break; }
         fence_after();
 #pragma unroll
         for (int st = 0; st < P; ++st)
