@@ -45,6 +45,8 @@ NODE_DTYPE = np.dtype([("pos", "<i4", 3), ("axis", "<i4"), ("shift", "<i4"), ("s
                        ("signFace", "<i4"), ("pad", "<i4"), ("d", "<f8"), ("X", "<f8", 3), ("op", "<f8", 3),
                        ("n", "<f8", 3), ("k", "<f8")])
 assert NODE_DTYPE.itemsize == ctypes.sizeof(IrregularNode) == 120
+BOX_DTYPE = np.dtype([("offset", "<i8"), ("p", "<i4", 3), ("n", "<i4", 3)])  # struct dcell_box
+assert BOX_DTYPE.itemsize == 32
 
 
 def geom(shape, h, origin=(0, 0, 0)) -> Geom:
@@ -87,6 +89,8 @@ def lib():
     L.dcell_max_velocity.argtypes = [G, i, vp, vp, vp, i, vp, vp]
     L.dcell_volume_scratch_bytes.restype = sz
     L.dcell_volume.argtypes = [G, i, vp, d, vp, vp, sz, vp]
+    L.dcell_velocity_box.argtypes = [G, i, vp, vp, i, i, vp, vp]
+    L.dcell_velocity_boxes.argtypes = [vp, i, i, i, vp, vp, i, i, ctypes.c_longlong, vp, vp]
     L.dcell_reinit_scratch_bytes.argtypes = [G, i]
     L.dcell_reinit_scratch_bytes.restype = sz
     L.dcell_reinitialize.argtypes = [G, i, vp, vp, i, d, d, vp, i, vp, vp, sz, vp, vp]
@@ -103,7 +107,7 @@ def lib():
     L.dcell_batch_plan.argtypes = [vp, i, i, i, i, vp, i, vp]
     L.dcell_batch_sl_step.argtypes = [vp, i, vp, i, i, i, i, i, vp, vp, vp, i, i, vp, vp]
     for name in ("dcell_sl_step", "dcell_irregular_nodes", "dcell_irregular_nodes_noalloc", "dcell_max_velocity",
-                 "dcell_volume", "dcell_reinitialize",
+                 "dcell_volume", "dcell_reinitialize", "dcell_velocity_box", "dcell_velocity_boxes",
                  "dcell_session_create", "dcell_session_destroy", "dcell_ls_advect_sl",
                  "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_ls_reinitialize",
                  "dcell_tc_gemm_check",

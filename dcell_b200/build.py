@@ -31,6 +31,7 @@ UNITS = {
     "sl_cubic.cu": [],
     "sl_tc.cu": [],
     "sl_adjoint.cu": [],
+    "velocity.cu": [],
     "capi.cu": [],
 }
 

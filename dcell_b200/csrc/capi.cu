@@ -136,6 +136,40 @@ DCELL_API int dcell_irregular_nodes(const dcell_geom *g, int dtype, const void *
                           flags, (cudaStream_t)stream);
 }
 
+static int check_field(const int gdims[3], int gdof, int first, int dim) {
+  if (!gdims || gdims[0] < 1 || gdims[1] < 1 || gdims[2] < 1) FAIL(DCELL_ERR_ARG, "field extents must be positive");
+  if (first < 0 || first + dim > gdof)
+    FAIL(DCELL_ERR_ARG, "components %d..%d outside the field's %d", first, first + dim - 1, gdof);
+  if ((long long)gdims[0] * gdims[1] * gdims[2] * gdof >= (1LL << 40)) FAIL(DCELL_ERR_ARG, "field too large");
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_velocity_box(const dcell_geom *g, int dtype, const void *global, const int gdims[3], int gdof,
+                                 int first, void *vel, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (!global || !vel) FAIL(DCELL_ERR_ARG, "global and vel are required");
+  const int dim = g->n[2] > 1 ? 3 : 2;
+  if (dim == 2 && gdims && gdims[2] > 1) FAIL(DCELL_ERR_ARG, "a 2D box needs a 2D field (gdims[2] == 1)");
+  if ((rc = check_field(gdims, gdof, first, dim))) return rc;
+  return launch_velocity_box(dcell::to_geom(g), dtype, global, gdims, gdof, first, vel, (cudaStream_t)stream);
+}
+
+DCELL_API int dcell_velocity_boxes(const dcell_box *boxes, int nboxes, int dim, int dtype, const void *global,
+                                   const int gdims[3], int gdof, int first, long long max_points, void *vel,
+                                   void *stream) {
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (dim != 2 && dim != 3) FAIL(DCELL_ERR_ARG, "dim must be 2 or 3");
+  if (nboxes < 0 || nboxes > 65535 || (nboxes > 0 && (!boxes || !global || !vel)))
+    FAIL(DCELL_ERR_ARG, "boxes (at most 65535), global and vel are required");
+  if (max_points < 0) FAIL(DCELL_ERR_ARG, "max_points must be >= 0");
+  int rc = check_field(gdims, gdof, first, dim);
+  if (rc) return rc;
+  return launch_velocity_boxes(boxes, nboxes, dim, dtype, global, gdims, gdof, first, max_points, vel,
+                               (cudaStream_t)stream);
+}
+
 DCELL_API size_t dcell_reinit_scratch_bytes(const dcell_geom *g, int dtype) {
   if (!g) return 0;
   const long long n = (long long)g->n[0] * g->n[1] * (g->n[2] > 1 ? g->n[2] : 1);

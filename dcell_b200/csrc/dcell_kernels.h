@@ -37,6 +37,10 @@ constexpr int kNoAllocMaxDevices = 64;
 int launch_irregular_noalloc(const dcell::Geom &g, int dtype, const void *phi, const int *band, int nband,
                              int with_surface, dcell_irregular_node *nodes, int cap, int *count, int *flags,
                              cudaStream_t st);
+int launch_velocity_box(const dcell::Geom &g, int dtype, const void *global, const int gdims[3], int gdof, int first,
+                        void *vel, cudaStream_t st);
+int launch_velocity_boxes(const dcell_box *boxes, int nboxes, int dim, int dtype, const void *global,
+                          const int gdims[3], int gdof, int first, long long max_points, void *vel, cudaStream_t st);
 size_t reinit_scratch_bytes(long long n, int dtype);
 int launch_reinit(const dcell::Geom &g, int dtype, void *phi, const dcell_irregular_node *nodes, int nnodes, double bw,
                   double bucket, int *band, int cap, int *count, void *scratch, int *flags, cudaStream_t st);

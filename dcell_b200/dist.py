@@ -14,6 +14,13 @@ Two decompositions of the level-set transport step:
   the velocity halos once.  `halo` must cover the departure reach:
   ceil(max |w| dt / h_z) + 2 planes for the cubic stencil.
 
+* **velocity acquisition** -- the fluid's velocity field is z-slab
+  distributed over the ranks (like the reference's Global Array); every rank
+  sends the parts of the cells' velocity boxes that lie in its slab to the
+  cells' owners in one all_to_all (LevelSetGetVelocity's NGA_Get,
+  LevelSetMethod/Advect.c:145-192), and each owner assembles its boxes with
+  zeros outside the field.
+
 The per-slab / per-cell step is a callable (default: the CUDA kernels via
 dcell_b200.levelset.sl_step), so the same host logic runs on GPUs with NCCL
 and in CPU tests with gloo.
@@ -131,3 +138,85 @@ def gather_interiors(slab: Slab, local: torch.Tensor, nz: int):
     dist.all_gather(out, pad)
     counts = [nz // slab.world + (1 if r < nz % slab.world else 0) for r in range(slab.world)]
     return torch.cat([o[:c] for o, c in zip(out, counts)], dim=0)
+
+
+def slab_ranges(nz: int, world: int):
+    """Planes [z0, z1) of each rank in a block distribution of nz planes (the
+    first nz % world ranks hold one plane more)."""
+    base, extra = divmod(nz, world)
+    out, z = [], 0
+    for r in range(world):
+        n = base + (1 if r < extra else 0)
+        out.append((z, z + n))
+        z += n
+    return out
+
+
+def _box_part(box, gdims, z0: int, z1: int):
+    """Global index range (lo, hi per axis x, y, z) of the part of a box
+    ((x, y, z) origin, (nz, ny, nx) shape) inside the field and planes [z0, z1); None if empty."""
+    o, sh = box
+    lo = [max(0, int(o[0])), max(0, int(o[1])), max(z0, int(o[2]))]
+    hi = [min(int(gdims[0]), int(o[0]) + int(sh[2])), min(int(gdims[1]), int(o[1]) + int(sh[1])),
+          min(z1, int(gdims[2]), int(o[2]) + int(sh[0]))]
+    if any(h <= l for l, h in zip(lo, hi)):
+        return None
+    return lo, hi
+
+
+def gather_velocity_boxes(local_field: torch.Tensor, gdims, boxes, owner, first: int = 1):
+    """Velocity grids of the boxes this rank owns, from a z-slab distributed
+    global field.
+
+    local_field: this rank's planes slab_ranges(gdims[2], world)[rank] of the
+    global [z][y][x][c] field; gdims = (gx, gy, gz); boxes: list of ((x, y, z)
+    origin, (nz, ny, nx) shape), the same list on every rank; owner[b]: the
+    rank that owns box b.  Components first .. first+2.  Returns {b: tensor
+    shape + (3,)} for the boxes owned here, zero outside the field (GridResize
+    zeroes the velocity grid before NGA_Get, Common/Grid.c:146).  One
+    all_to_all_single carries every part; the receive sizes follow from the
+    box list and the slab ranges, so no size exchange is needed."""
+    rank, world = dist.get_rank(), dist.get_world_size()
+    ranges = slab_ranges(int(gdims[2]), world)
+    z0, z1 = ranges[rank]
+    dim = 3
+    send_chunks = [[] for _ in range(world)]
+    for b, box in enumerate(boxes):
+        part = _box_part(box, gdims, z0, z1)
+        if part is None:
+            continue
+        lo, hi = part
+        blk = local_field[lo[2] - z0:hi[2] - z0, lo[1]:hi[1], lo[0]:hi[0], first:first + dim]
+        send_chunks[owner[b]].append(blk.reshape(-1))
+    send_sizes = [sum(c.numel() for c in ch) for ch in send_chunks]
+    flat = [c for ch in send_chunks for c in ch]
+    send = torch.cat(flat) if flat else local_field.new_empty(0)
+    recv_sizes = [0] * world
+    for src, (s0, s1) in enumerate(ranges):
+        for b, box in enumerate(boxes):
+            if owner[b] != rank:
+                continue
+            part = _box_part(box, gdims, s0, s1)
+            if part is not None:
+                lo, hi = part
+                recv_sizes[src] += (hi[0] - lo[0]) * (hi[1] - lo[1]) * (hi[2] - lo[2]) * dim
+    recv = local_field.new_empty(sum(recv_sizes))
+    dist.all_to_all_single(recv, send.contiguous(), recv_sizes, send_sizes)
+    out = {b: local_field.new_zeros(tuple(int(v) for v in box[1]) + (dim,))
+           for b, box in enumerate(boxes) if owner[b] == rank}
+    pos = 0
+    for src, (s0, s1) in enumerate(ranges):
+        for b, box in enumerate(boxes):
+            if owner[b] != rank:
+                continue
+            part = _box_part(box, gdims, s0, s1)
+            if part is None:
+                continue
+            lo, hi = part
+            o = box[0]
+            ext = (hi[2] - lo[2], hi[1] - lo[1], hi[0] - lo[0], dim)
+            n = ext[0] * ext[1] * ext[2] * dim
+            out[b][lo[2] - o[2]:hi[2] - o[2], lo[1] - o[1]:hi[1] - o[1], lo[0] - o[0]:hi[0] - o[0]] = \
+                recv[pos:pos + n].view(ext)
+            pos += n
+    return out

@@ -186,6 +186,59 @@ def reinitialize(phi: torch.Tensor, raw_nodes: torch.Tensor, count, band_width: 
     return band[: int(nb.item())]
 
 
+def _field_dims(global_field: torch.Tensor):
+    if global_field.dim() == 4:
+        gz, gy, gx, gdof = global_field.shape
+    elif global_field.dim() == 3:
+        gy, gx, gdof = global_field.shape
+        gz = 1
+    else:
+        raise DcellError(_lib.ERR_ARG, "global field must be [z][y][x][c] or [y][x][c]")
+    return (ctypes.c_int * 3)(int(gx), int(gy), int(gz)), int(gdof)
+
+
+def velocity_box(global_field: torch.Tensor, origin, shape, first: int = 1):
+    """The velocity grid of a level set's phi box (global index `origin`
+    (x, y(, z)), extents `shape` (nz, ny, nx) or (ny, nx)) from the fluid's
+    global field: the reference's LevelSetGetVelocity (Advect.c:145-192) with
+    the Global Array on the device.  Components first .. first+dim-1; zero
+    outside the field.  Returns shape + (dim,)."""
+    _require_cuda(global_field)
+    gd, gdof = _field_dims(global_field)
+    dim = len(shape)
+    out = torch.empty(tuple(shape) + (dim,), dtype=global_field.dtype, device=global_field.device)
+    g = geom(shape, 1.0, origin)
+    check(lib().dcell_velocity_box(ctypes.byref(g), _dtype_code(global_field), _ptr(global_field), gd, gdof, int(first),
+                                   _ptr(out), _stream()))
+    return out
+
+
+def velocity_boxes(global_field: torch.Tensor, boxes, first: int = 1):
+    """velocity_box for a list of (origin, shape) boxes in one launch; returns
+    one tensor per box (views of one packed buffer)."""
+    _require_cuda(global_field)
+    gd, gdof = _field_dims(global_field)
+    dim = global_field.dim() - 1
+    rec = np.zeros(len(boxes), dtype=_lib.BOX_DTYPE)
+    off, sizes = 0, []
+    for b, (o, sh) in enumerate(boxes):
+        n = int(np.prod(sh))
+        rec[b]["offset"] = off
+        rec[b]["p"] = tuple(int(v) for v in o) + (0,) * (3 - len(o))
+        rec[b]["n"] = tuple(int(v) for v in reversed(sh)) + (1,) * (3 - len(sh))
+        sizes.append(n)
+        off += n
+    out = torch.empty(max(off, 1) * dim, dtype=global_field.dtype, device=global_field.device)
+    d_rec = torch.from_numpy(np.frombuffer(rec.tobytes(), dtype=np.uint8).copy()).to(global_field.device)
+    check(lib().dcell_velocity_boxes(_ptr(d_rec), len(boxes), dim, _dtype_code(global_field), _ptr(global_field), gd,
+                                     gdof, int(first), max(sizes, default=0), _ptr(out), _stream()))
+    res, start = [], 0
+    for (o, sh), n in zip(boxes, sizes):
+        res.append(out[start * dim:(start + n) * dim].view(tuple(sh) + (dim,)))
+        start += n
+    return res
+
+
 def volume(phi: torch.Tensor, h, eps: float):
     """Enclosed volume through the smoothed Heaviside (FP64, deterministic)."""
     _require_cuda(phi)

@@ -94,6 +94,14 @@ typedef struct dcell_irregular_node {
   double k;        /* curvature at X (with_surface) */
 } dcell_irregular_node;
 
+/* A box of a level set on the global index grid, packed at `offset` points
+ * into a batch buffer (velocity acquisition of many cells). */
+typedef struct dcell_box {
+  long long offset; /* first point of the box in the packed output */
+  int p[3];         /* global index of the box's first point */
+  int n[3];         /* extents (n[2] == 1 in 2D) */
+} dcell_box;
+
 /* Text of the last error on this thread ("" if none). */
 DCELL_API const char *dcell_last_error(void);
 DCELL_API int dcell_version(void);
@@ -189,6 +197,25 @@ DCELL_API size_t dcell_reinit_scratch_bytes(const dcell_geom *g, int dtype);
 DCELL_API int dcell_reinitialize(const dcell_geom *g, int dtype, void *phi, const dcell_irregular_node *nodes,
                                  int nnodes, double band_width, double bucket, int *band, int capacity, int *count,
                                  void *scratch, size_t scratch_bytes, int *flags, void *stream);
+
+/* Velocity acquisition: replaces LevelSetGetVelocity
+ * (LevelSetMethod/Advect.c:145-192), i.e. GridResize of the velocity grid to
+ * the phi box (which zeroes it, Common/Grid.c:146) and NGA_Get of the part of
+ * the box inside the fluid's Global Array.  global: device array of the
+ * fluid's field, [gdims[2]][gdims[1]][gdims[0]][gdof] (3D) or
+ * [gdims[1]][gdims[0]][gdof] (2D, gdims[2] = 1), components in VelFace order
+ * (CELL_CENTER, U_FACE, V_FACE, W_FACE); components first .. first+dim-1
+ * (first = 1: U_FACE..) are copied.  vel: device array of the box (the
+ * extents and global origin of g; h unused), dim components innermost; box
+ * points outside the field get 0. */
+DCELL_API int dcell_velocity_box(const dcell_geom *g, int dtype, const void *global, const int gdims[3], int gdof,
+                                 int first, void *vel, void *stream);
+/* The same for nboxes boxes (device array) in one launch, box b written at
+ * boxes[b].offset * dim of vel; max_points bounds the largest box (sizes the
+ * launch).  dim 2 or 3; nboxes <= 65535. */
+DCELL_API int dcell_velocity_boxes(const dcell_box *boxes, int nboxes, int dim, int dtype, const void *global,
+                                   const int gdims[3], int gdof, int first, long long max_points, void *vel,
+                                   void *stream);
 
 /* Allocation-free variant of dcell_irregular_nodes.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory -- a

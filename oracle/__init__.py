@@ -218,3 +218,23 @@ def reinit(phi, nodes, band_width=6.0, bucket=1.0 / 64, origin=(0, 0, 0)):
     if n < 0:
         raise RuntimeError("fast marching did not settle within the buckets")
     return phi, band[:n].copy()
+
+
+def velocity_box(global_field, origin, shape, first=1):
+    """The velocity grid of a level set whose phi box starts at global index
+    `origin` (x, y(, z)) with extents `shape` ((nz, ny, nx) or (ny, nx)):
+    components first .. first+dim-1 of the fluid's global field ([z][y][x][c]
+    or [y][x][c]) where the box overlaps the global domain, zero elsewhere
+    (LevelSetGetVelocity, Advect.c:145-192: GridResize zeroes the grid, then
+    NGA_Get fills the part of the box inside the global array)."""
+    gf = np.asarray(global_field, dtype=np.float64)
+    dim = len(shape)
+    out = np.zeros(tuple(shape) + (dim,))
+    lo = [max(0, int(origin[a])) for a in range(dim)]                            # x, y(, z)
+    hi = [min(int(origin[a]) + int(shape[dim - 1 - a]), gf.shape[dim - 1 - a]) for a in range(dim)]
+    if any(h <= l for l, h in zip(lo, hi)):
+        return out
+    src = tuple(slice(lo[a], hi[a]) for a in reversed(range(dim)))
+    dst = tuple(slice(lo[a] - int(origin[a]), hi[a] - int(origin[a])) for a in reversed(range(dim)))
+    out[dst] = gf[src + (slice(first, first + dim),)]
+    return out

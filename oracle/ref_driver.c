@@ -11,6 +11,7 @@
  *   LevelSet_MaxVelocity        LevelSetMethod/Advect.c:70
  *   LevelSetCFLIncrement        LevelSetMethod/Advect.c:54
  *   LevelSetReinitialize        LevelSetMethod/FastMarching.c:11
+ *   LevelSetGetVelocity         LevelSetMethod/Advect.c:145 (one-process GA in the shim)
  *   LevelSetInitializeToSphere/Circle  LevelSetMethod/Initializations.c:10,61
  *   Bilinear2D/3D + GridFunction*_Curv/Deriv*  Common/Grid.c:190, Common/Grid3D.c:4
  *   LevelSetDiracDelta2D/3D     LevelSetMethod/NormalDirection.c:36,47
@@ -137,6 +138,23 @@ DREF_EXPORT int dref_update_irregular(void *h) {
 }
 
 DREF_EXPORT int dref_reinitialize(void *h) { return LevelSetReinitialize((LevelSet)h); }
+
+/* LevelSetGetVelocity (Advect.c:145-192) against the shim's one-process
+ * Global Array `global` (dims[ndim], last index the component); writes the
+ * level set's velocity grid (its phi box, dof 2/3) to out. */
+void dref_ga_set(const double *data, int ndim, const int *dims);
+DREF_EXPORT int dref_get_velocity(void *h, const double *global, int ndim, const int *dims, double *out) {
+  LevelSet ls = (LevelSet)h;
+  Grid velgrid = NULL;
+  int e = GridCreate(ls->phi->d, ls->phi->p, ls->phi->n, ls->phi->is2D ? 2 : 3, &velgrid);
+  if (e) return e;
+  dref_ga_set(global, ndim, dims);
+  e = LevelSetGetVelocity(ls, 0, velgrid);
+  if (!e) memcpy(out, velgrid->v1, sizeof(double) * (size_t)velgrid->SIZE);
+  GridDestroy(velgrid);
+  dref_ga_set(NULL, 0, dims);
+  return e;
+}
 
 /* Irregular node export: 18 doubles per node
  *  0-2 pos.xyz, 3 axis, 4 shift, 5 signCenter, 6 signFace, 7 d,

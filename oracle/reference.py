@@ -62,6 +62,7 @@ def lib(path=PATH):
         L.dref_ortho3d.argtypes = [vp, vp, vp]
         L.dref_ortho2d.argtypes = [vp, vp, vp]
         L.dref_tricubic_coefs.argtypes = [vp, vp]
+        L.dref_get_velocity.argtypes = [vp, vp, ctypes.c_int, vp, vp]
         _LIBS[path] = L
     return _LIBS[path]
 
@@ -191,6 +192,18 @@ class RefLevelSet:
 
     def reinitialize(self):
         assert self.L.dref_reinitialize(self.h) == 0
+
+    def get_velocity(self, global_field):
+        """LevelSetGetVelocity (Advect.c:145-192) from a one-process Global
+        Array holding `global_field` ([z][y][x][c] in 3D, [y][x][c] in 2D,
+        c = CELL_CENTER, U_FACE, V_FACE(, W_FACE)); returns the velocity grid
+        of the level set's phi box, (nz, ny, nx, 3) or (ny, nx, 2)."""
+        gf = np.ascontiguousarray(global_field, dtype=np.float64)
+        dims = np.array(gf.shape, dtype=np.int32)
+        shape = self.shape
+        out = np.zeros(shape + (len(shape),))
+        assert self.L.dref_get_velocity(self.h, _p(gf), gf.ndim, _p(dims), _p(out)) == 0
+        return out
 
     def sample(self, fn, X):
         return np.array([self.L.dref_sample(self.h, int(fn), *map(float, x)) for x in np.reshape(X, (-1, 3))])

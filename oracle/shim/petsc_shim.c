@@ -160,13 +160,54 @@ PetscErrorCode PetscBinaryClose(int fd) { (void)fd; return 0; }
 PetscErrorCode MatView(Mat m, PetscViewer v) { (void)m; (void)v; return 0; }
 int MPI_Comm_rank(MPI_Comm c, int *rank) { (void)c; *rank = 0; return 0; }
 
-/* GA link stubs: velocity is never fetched through GA by the oracle. */
+/* A one-process Global Array: one double array with dims[ndim] (row major,
+ * last index fastest), registered by the driver (dref_ga_set).  NGA_Get
+ * copies the patch [lo, hi] (inclusive) into buf, whose trailing extents are
+ * ld[0..ndim-2] (Global Arrays' NGA_Get contract; an empty patch copies
+ * nothing); NGA_Inquire reports the dims.  Enough for LevelSetGetVelocity
+ * (Advect.c:145-192) to run as written. */
+static const double *shim_ga_data = NULL;
+static int shim_ga_ndim = 0, shim_ga_dims[4] = {0, 0, 0, 0};
+
+void dref_ga_set(const double *data, int ndim, const int *dims) {
+  shim_ga_data = data;
+  shim_ga_ndim = ndim;
+  for (int i = 0; i < 4; ++i) shim_ga_dims[i] = i < ndim ? dims[i] : 0;
+}
+
 void NGA_Get(int g_a, int lo[], int hi[], void *buf, int ld[]) {
-  (void)g_a; (void)lo; (void)hi; (void)buf; (void)ld;
-  fprintf(stderr, "[oracle shim] NGA_Get called: velocity must be supplied directly\n");
+  (void)g_a;
+  double *out = (double *)buf;
+  const int nd = shim_ga_ndim;
+  if (!shim_ga_data || nd < 2) {
+    fprintf(stderr, "[oracle shim] NGA_Get without a registered array\n");
+    return;
+  }
+  int idx[4] = {0, 0, 0, 0};
+  for (int d = 0; d < nd; ++d) {
+    if (hi[d] < lo[d]) return; /* empty patch */
+    idx[d] = lo[d];
+  }
+  for (;;) {
+    size_t src = 0, dst = 0;
+    for (int d = 0; d < nd; ++d) {
+      src = src * (size_t)shim_ga_dims[d] + (size_t)idx[d];
+      dst = d == 0 ? (size_t)(idx[0] - lo[0]) : dst * (size_t)ld[d - 1] + (size_t)(idx[d] - lo[d]);
+    }
+    out[dst] = shim_ga_data[src];
+    int d = nd - 1;
+    while (d >= 0 && ++idx[d] > hi[d]) {
+      idx[d] = lo[d];
+      --d;
+    }
+    if (d < 0) break;
+  }
 }
 void NGA_Inquire(int g_a, int *type, int *ndim, int dims[]) {
-  (void)g_a; *type = 0; *ndim = 0; dims[0] = dims[1] = dims[2] = dims[3] = 0;
+  (void)g_a;
+  *type = 0;
+  *ndim = shim_ga_ndim;
+  for (int i = 0; i < 4; ++i) dims[i] = shim_ga_dims[i];
 }
 
 /* Symbols referenced by the compiled files but defined in subsystems the

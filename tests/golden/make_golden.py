@@ -113,6 +113,25 @@ def main():
     np.savez_compressed(os.path.join(OUT, "reinit.npz"), **{k + "3": v for k, v in r3.items()},
                         **{k + "2": v for k, v in r2.items()})
 
+    # velocity acquisition: LevelSetGetVelocity (Advect.c:145-192) through the
+    # shim's one-process Global Array, for boxes inside, across and beyond the
+    # fluid domain (components CELL_CENTER, U, V(, W) per cell)
+    rng = np.random.default_rng(21)
+    g3 = f32(rng.uniform(-2.0, 2.0, size=(20, 24, 28, 4)))
+    boxes3 = [((-3, 5, 12), (14, 16, 22)), ((4, 3, 2), (6, 7, 8)), ((20, -6, -2), (12, 9, 10)), ((30, 30, 30), (4, 4, 4))]
+    out3 = [R.RefLevelSet.create(0.05, o, s).get_velocity(g3) for o, s in boxes3]
+    g2 = f32(rng.uniform(-2.0, 2.0, size=(30, 26, 3)))
+    boxes2 = [((20, -4), (15, 12)), ((3, 7), (10, 9))]
+    out2 = [R.RefLevelSet.create(0.05, o, s).get_velocity(g2) for o, s in boxes2]
+    np.savez_compressed(os.path.join(OUT, "velocity.npz"), global3=g3.astype(np.float32),
+                        global2=g2.astype(np.float32),
+                        **{f"origin3_{i}": np.array(o) for i, (o, s) in enumerate(boxes3)},
+                        **{f"shape3_{i}": np.array(s) for i, (o, s) in enumerate(boxes3)},
+                        **{f"vel3_{i}": v.astype(np.float32) for i, v in enumerate(out3)},
+                        **{f"origin2_{i}": np.array(o) for i, (o, s) in enumerate(boxes2)},
+                        **{f"shape2_{i}": np.array(s) for i, (o, s) in enumerate(boxes2)},
+                        **{f"vel2_{i}": v.astype(np.float32) for i, v in enumerate(out2)})
+
     h3 = 1.0 / 40
     # 3D: non-cubic grid, non-zero (partly negative) global origin
     shape3, origin3 = (20, 22, 24), (5, -3, 7)
