@@ -450,6 +450,12 @@ def main():
                         "ms": t * 1e3, "cores": 1, "band_points": nb, "kind": "reference",
                         "gpu_fp64_vs_reference": {"max": float(d.max()), "mean": float(d.mean())},
                         "gpu_fp64_speedup": t * 1e3 / ms64}
+        if rank == 0:
+            # velocity acquisition of 512 cells' boxes from a 512^3 fluid field (HBM-bound copy)
+            from dcell_b200.configs import run_vel
+            v = run_vel(dev=dev)
+            v.update({"peak_gbs": hbm, "frac": v["achieved_gbs"] / hbm})
+            line["velocity_acquisition"] = v
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -141,3 +141,22 @@ def test_gpu_velocity_boxes_many_cells(cuda):
     outs = L.velocity_boxes(g, boxes)
     for t, (o, sh) in zip(outs, boxes):
         assert np.array_equal(t.cpu().numpy(), oracle.velocity_box(gf, o, sh, first=1))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("gdof,first", [(4, 0), (4, 1), (5, 2), (3, 0)])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_gpu_velocity_box_record_layouts(cuda, gdof, first, dtype):
+    """Vector-load records (four components: 16 B FP32, 32 B FP64) and
+    per-component loads (other widths), any first component, against the oracle."""
+    from dcell_b200 import levelset as L
+    rng = np.random.default_rng(gdof * 10 + first)
+    gf = rng.standard_normal((21, 19, 37, gdof))
+    want_dtype = np.float64 if dtype == torch.float64 else np.float32
+    g = torch.from_numpy(gf).to(cuda, dtype)
+    boxes = [((-5, 3, 2), (9, 11, 50)), ((30, -2, 18), (6, 25, 13)), ((0, 0, 0), (21, 19, 37)), ((40, 0, 0), (2, 3, 4))]
+    outs = L.velocity_boxes(g, boxes, first=first)
+    for (o, sh), t in zip(boxes, outs):
+        want = oracle.velocity_box(gf.astype(want_dtype), o, sh, first=first).astype(want_dtype)
+        assert np.array_equal(L.velocity_box(g, o, sh, first=first).cpu().numpy(), want)
+        assert np.array_equal(t.cpu().numpy(), want)
