@@ -44,6 +44,29 @@ def test_oracle_velocity_box_vs_reference_golden(golden, d):
     assert outside > 0  # the fixture has box points outside the field
 
 
+def _getvel_case():
+    """The reference's own GetVelocity test (LevelSetMethod/tests/getVel.c):
+    a 10x10 2D field with 3 values per point, g[j][i][0] = i, g[j][i][1] = j,
+    and a 19x19 box at (-5, -5).  GetVelocity takes components U_FACE..V_FACE
+    (1..2), so inside the field the box holds (j, 0), zero elsewhere."""
+    g = np.zeros((10, 10, 3))
+    j, i = np.meshgrid(np.arange(10), np.arange(10), indexing="ij")
+    g[..., 0], g[..., 1] = i, j
+    want = np.zeros((19, 19, 2))
+    want[5:15, 5:15, 0] = j
+    return g, want
+
+
+def test_getvel_known_answer():
+    from oracle import reference as R
+    g, want = _getvel_case()
+    assert np.array_equal(oracle.velocity_box(g, (-5, -5), (19, 19), first=1), want)
+    if R.available():
+        ls = R.RefLevelSet.create(1.0, (-5, -5), (19, 19))
+        assert np.array_equal(ls.get_velocity(g), want)
+        ls.close()
+
+
 def test_slab_ranges_and_box_part():
     assert D.slab_ranges(10, 3) == [(0, 4), (4, 7), (7, 10)]
     assert D.slab_ranges(2, 4) == [(0, 1), (1, 2), (2, 2), (2, 2)]
@@ -122,6 +145,14 @@ def test_gpu_velocity_box_vs_reference_golden(golden, cuda, d, dtype):
     outs = L.velocity_boxes(g, [(o, s) for o, s, _ in cases], first=1)
     for t, (_, _, want) in zip(outs, cases):
         assert np.array_equal(t.cpu().numpy(), want.astype(t.cpu().numpy().dtype))
+
+
+@pytest.mark.gpu
+def test_gpu_getvel_known_answer(cuda):
+    from dcell_b200 import levelset as L
+    g, want = _getvel_case()
+    got = L.velocity_box(torch.from_numpy(g).to(cuda), (-5, -5), (19, 19), first=1)
+    assert np.array_equal(got.cpu().numpy(), want)
 
 
 @pytest.mark.gpu
