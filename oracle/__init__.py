@@ -73,6 +73,14 @@ def lib():
         L.orc_volume.restype = d
         L.orc_reinit.argtypes = [vp, vp, vp, l, d, d, vp, l]
         L.orc_reinit.restype = l
+        L.orc_pls_advect.argtypes = [vp, vp, vp, l, d]
+        L.orc_pls_correct.argtypes = [vp, vp, vp, l, vp, l]
+        L.orc_pls_correct.restype = l
+        L.orc_pls_adjust.argtypes = [vp, vp, vp, l, vp]
+        L.orc_pls_init.argtypes = [vp, vp, vp, l, vp, vp, vp, l]
+        L.orc_pls_init.restype = l
+        L.orc_pls_reseed.argtypes = [vp, vp, vp, l, vp, vp, vp, l, l, vp]
+        L.orc_pls_reseed.restype = l
         _LIB = L
     return _LIB
 
@@ -238,3 +246,93 @@ def velocity_box(global_field, origin, shape, first=1):
     dst = tuple(slice(lo[a] - int(origin[a]), hi[a] - int(origin[a])) for a in reversed(range(dim)))
     out[dst] = gf[src + (slice(first, first + dim),)]
     return out
+
+
+# ---------------------------------------------------------------------------
+# particle level set (LevelSetMethod/ParticleLS*.c); particles are (n, 4)
+# float64 rows X.x, X.y, X.z, radius in global index space
+
+class PlsParams(ctypes.Structure):
+    """LevelSetInitializeParticles' parameters (ParticleLS.c:21-27)."""
+    _fields_ = [("r_min", ctypes.c_double), ("r_max", ctypes.c_double), ("d_init", ctypes.c_double),
+                ("g_tol", ctypes.c_double), ("e_dist", ctypes.c_double), ("s_init", ctypes.c_int),
+                ("l_max", ctypes.c_int)]
+
+
+def pls_params(dim=2, **kw):
+    p = PlsParams(0.1, 0.5, 3.0, 1e-3, 0.5, 16 if dim == 2 else 32, 30)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _parts(parts):
+    return np.array(parts, dtype=np.float64, copy=True, order="C").reshape(-1, 4)
+
+
+def pls_advect(vel, parts, dt, h, origin=(0, 0, 0)):
+    """RK2-midpoint particle advection (ParticleLS2D.c:6-36 / ParticleLS3D.c:6-36)."""
+    vel = np.ascontiguousarray(vel, dtype=np.float64)
+    out = _parts(parts)
+    g = geom(vel.shape[:-1], h, origin)
+    lib().orc_pls_advect(ctypes.byref(g), _ptr(vel), _ptr(out), out.shape[0], float(dt))
+    return out
+
+
+def pls_correct(phi, band, parts, h=1.0, origin=(0, 0, 0)):
+    """Escaped-particle error correction of phi at the band points
+    (ParticleLS2D.c:40-115 / ParticleLS3D.c:40-116).  Returns (phi, number
+    of corners skipped outside the grid)."""
+    phi = np.array(phi, dtype=np.float64, copy=True, order="C")
+    g = geom(phi.shape, h, origin)
+    b, _ = _band(band)
+    P = _parts(parts)
+    skipped = lib().orc_pls_correct(ctypes.byref(g), _ptr(phi), _ptr(b), b.shape[0], _ptr(P), P.shape[0])
+    return phi, skipped
+
+
+def pls_adjust(phi, parts, h=1.0, origin=(0, 0, 0), params=None):
+    """ParticleLS_AdjustRadii (ParticleLS.c:158-185)."""
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    g = geom(phi.shape, h, origin)
+    P = _parts(parts)
+    prm = params or pls_params(phi.ndim)
+    lib().orc_pls_adjust(ctypes.byref(g), _ptr(phi), _ptr(P), P.shape[0], ctypes.byref(prm))
+    return P
+
+
+def pls_init(phi, band, rng, h=1.0, origin=(0, 0, 0), params=None):
+    """LevelSetInitializeParticles (ParticleLS.c:6-88), 2D.  rng: the drand48
+    state.  Returns (particles, rng after)."""
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    g = geom(phi.shape, h, origin)
+    b, _ = _band(band)
+    prm = params or pls_params(2)
+    st = ctypes.c_uint64(int(rng))
+    cap = b.shape[0] * prm.s_init
+    out = np.zeros((max(cap, 1), 4))
+    n = lib().orc_pls_init(ctypes.byref(g), _ptr(phi), _ptr(b), b.shape[0], ctypes.byref(prm), ctypes.byref(st),
+                           _ptr(out), cap)
+    if n < 0:
+        raise ValueError("particle seeding is 2D")
+    return out[:n].copy(), st.value
+
+
+def pls_reseed(phi, band, parts, rng, h=1.0, origin=(0, 0, 0), params=None):
+    """ParticleLS_ReseedParticles (ParticleLS.c:202-295), 2D.  Returns
+    (particles, rng after, particles not counted because outside the box)."""
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    g = geom(phi.shape, h, origin)
+    b, _ = _band(band)
+    prm = params or pls_params(2)
+    P0 = _parts(parts)
+    cap = P0.shape[0] + b.shape[0] * prm.s_init
+    P = np.zeros((max(cap, 1), 4))
+    P[:P0.shape[0]] = P0
+    st = ctypes.c_uint64(int(rng))
+    miss = ctypes.c_long(0)
+    n = lib().orc_pls_reseed(ctypes.byref(g), _ptr(phi), _ptr(b), b.shape[0], ctypes.byref(prm), ctypes.byref(st),
+                             _ptr(P), P0.shape[0], cap, ctypes.byref(miss))
+    if n < 0:
+        raise ValueError("particle reseeding is 2D")
+    return P[:n].copy(), st.value, miss.value

@@ -17,7 +17,9 @@
  *   LevelSetDiracDelta2D/3D     LevelSetMethod/NormalDirection.c:36,47
  *   OrthogonalProjection2D/3D   LevelSetMethod/OrthogonalProjection*.c
  *   TricubicInverse.h           (64 Catmull-Rom coefficients of a 4^3 stencil)
+ *   particle level set          LevelSetMethod/ParticleLS.c, ParticleLS2D.c, ParticleLS3D.c
  */
+#include <stdlib.h>
 #include "LevelSetMethod.h"
 #include "LSM_private.h"
 
@@ -295,4 +297,105 @@ DREF_EXPORT void dref_tricubic_coefs(const double *stencil64, double *a) {
       for (int x = 0; x < 4; ++x) phi[z][y][x] = stencil64[(z * 4 + y) * 4 + x];
 #include "TricubicInverse.h"
   (void)i; (void)j; (void)k;
+}
+
+/* ---------------------------------------------------------------------------
+ * Particle level set (LevelSetMethod/ParticleLS*.c).  Particles are exchanged
+ * as 4 doubles each (struct _Particle: X.x, X.y, X.z, radius). */
+
+/* LevelSetInitializeParticles (ParticleLS.c:6-88): seeds from the band. */
+DREF_EXPORT int dref_pls_init(void *h) { return LevelSetInitializeParticles((LevelSet)h); }
+
+/* A particle set with LevelSetInitializeParticles' parameters and function
+ * slots but no seeding (its seeding is 2D-only code; 3D particles come from
+ * dref_pls_set). */
+DREF_EXPORT int dref_pls_create_empty(void *h) {
+  LevelSet ls = (LevelSet)h;
+  ParticleLS pls;
+  int e = PetscNew(struct _ParticleLS, &ls->pls);
+  if (e) return e;
+  pls = ls->pls;
+  pls->R_MIN = 0.1;
+  pls->R_MAX = 0.5;
+  pls->D_INIT = 3.0;
+  pls->S_INIT = ls->phi->is2D ? 16 : 32;
+  pls->L_MAX = 30;
+  pls->G_TOL = 1e-3;
+  pls->E_DIST = 0.5;
+  if ((e = ArrayCreate("particles", sizeof(struct _Particle), &pls->particles))) return e;
+  if ((e = PetscRandomCreate(PETSC_COMM_WORLD, &pls->rnd))) return e;
+  if ((e = PetscRandomSetType(pls->rnd, PETSCRAND48))) return e;
+  pls->AdvectParticles = ls->phi->is2D ? ParticleLS_AdvectParticles2D : ParticleLS_AdvectParticles3D;
+  pls->ErrorCorrection = ls->phi->is2D ? ParticleLS_ErrorCorrection2D : ParticleLS_ErrorCorrection3D;
+  ls->Advect = LevelSetAdvectPLS;
+  return 0;
+}
+
+/* R_MIN, R_MAX, D_INIT, S_INIT, L_MAX, G_TOL, E_DIST */
+DREF_EXPORT int dref_pls_params(void *h, double *out) {
+  ParticleLS pls = ((LevelSet)h)->pls;
+  if (!pls) return -1;
+  out[0] = pls->R_MIN; out[1] = pls->R_MAX; out[2] = pls->D_INIT; out[3] = pls->S_INIT;
+  out[4] = pls->L_MAX; out[5] = pls->G_TOL; out[6] = pls->E_DIST;
+  return 0;
+}
+
+DREF_EXPORT int dref_pls_count(void *h) {
+  ParticleLS pls = ((LevelSet)h)->pls;
+  return pls ? ArrayLength(pls->particles) : -1;
+}
+
+DREF_EXPORT int dref_pls_get(void *h, double *out) {
+  ParticleLS pls = ((LevelSet)h)->pls;
+  int n = ArrayLength(pls->particles);
+  memcpy(out, ArrayGetData(pls->particles), sizeof(struct _Particle) * (size_t)n);
+  return n;
+}
+
+DREF_EXPORT int dref_pls_set(void *h, const double *src, int n) {
+  ParticleLS pls = ((LevelSet)h)->pls;
+  int e = ArraySetSize(pls->particles, n);
+  if (e) return e;
+  memcpy(ArrayGetData(pls->particles), src, sizeof(struct _Particle) * (size_t)n);
+  return 0;
+}
+
+DREF_EXPORT int dref_pls_advect(void *h, void *vel, double dt) {
+  LevelSet ls = (LevelSet)h;
+  return ls->pls->AdvectParticles(ls->pls, ls->phi->d, (Grid)vel, dt);
+}
+
+DREF_EXPORT int dref_pls_correct(void *h) {
+  LevelSet ls = (LevelSet)h;
+  return ls->pls->ErrorCorrection(ls->pls, ls);
+}
+
+DREF_EXPORT int dref_pls_adjust(void *h) {
+  LevelSet ls = (LevelSet)h;
+  return ParticleLS_AdjustRadii(ls->pls, ls);
+}
+
+DREF_EXPORT int dref_pls_reseed(void *h) {
+  LevelSet ls = (LevelSet)h;
+  return ParticleLS_ReseedParticles(ls->pls, ls);
+}
+
+DREF_EXPORT int dref_pls_step(void *h, void *vel, double dt) { return LevelSetAdvectPLS((LevelSet)h, (Grid)vel, dt); }
+DREF_EXPORT int dref_pls_rk2_half(void *h, void *vel, double dt) {
+  return LevelSetAdvectPLSRK2HalfStep((LevelSet)h, (Grid)vel, dt);
+}
+DREF_EXPORT int dref_pls_rk2_full(void *h, void *vel, double dt) {
+  return LevelSetAdvectPLSRK2FullStep((LevelSet)h, (Grid)vel, dt);
+}
+
+/* the drand48 state (three 16-bit words, least significant first) */
+DREF_EXPORT void dref_rand48_get(unsigned short *s) {
+  unsigned short tmp[3] = {0, 0, 0};
+  unsigned short *old = seed48(tmp);
+  s[0] = old[0]; s[1] = old[1]; s[2] = old[2];
+  seed48(s);
+}
+DREF_EXPORT void dref_rand48_set(const unsigned short *s) {
+  unsigned short t[3] = {s[0], s[1], s[2]};
+  seed48(t);
 }

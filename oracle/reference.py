@@ -63,12 +63,36 @@ def lib(path=PATH):
         L.dref_ortho2d.argtypes = [vp, vp, vp]
         L.dref_tricubic_coefs.argtypes = [vp, vp]
         L.dref_get_velocity.argtypes = [vp, vp, ctypes.c_int, vp, vp]
+        for f in ("dref_pls_init", "dref_pls_create_empty", "dref_pls_count", "dref_pls_correct",
+                  "dref_pls_adjust", "dref_pls_reseed"):
+            getattr(L, f).argtypes = [vp]
+        L.dref_pls_params.argtypes = [vp, vp]
+        L.dref_pls_get.argtypes = [vp, vp]
+        L.dref_pls_set.argtypes = [vp, vp, i]
+        for f in ("dref_pls_advect", "dref_pls_step", "dref_pls_rk2_half", "dref_pls_rk2_full"):
+            getattr(L, f).argtypes = [vp, vp, d]
+        L.dref_rand48_get.argtypes = [vp]
+        L.dref_rand48_get.restype = None
+        L.dref_rand48_set.argtypes = [vp]
+        L.dref_rand48_set.restype = None
         _LIBS[path] = L
     return _LIBS[path]
 
 
 def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def rand48_state(path=PATH) -> int:
+    """The C library's drand48 state (48 bits) that PETSCRAND48 draws from."""
+    s = np.zeros(3, dtype=np.uint16)
+    lib(path).dref_rand48_get(_p(s))
+    return int(s[0]) | (int(s[1]) << 16) | (int(s[2]) << 32)
+
+
+def set_rand48_state(x: int, path=PATH):
+    s = np.array([x & 0xFFFF, (x >> 16) & 0xFFFF, (x >> 32) & 0xFFFF], dtype=np.uint16)
+    lib(path).dref_rand48_set(_p(s))
 
 
 class RefLevelSet:
@@ -204,6 +228,58 @@ class RefLevelSet:
         out = np.zeros(shape + (len(shape),))
         assert self.L.dref_get_velocity(self.h, _p(gf), gf.ndim, _p(dims), _p(out)) == 0
         return out
+
+    # particle level set (LevelSetMethod/ParticleLS*.c); particles are
+    # (n, 4) float64 rows X.x, X.y, X.z, radius (struct _Particle)
+    def pls_init(self):
+        """LevelSetInitializeParticles (ParticleLS.c:6-88)."""
+        assert self.L.dref_pls_init(self.h) == 0
+
+    def pls_create_empty(self):
+        assert self.L.dref_pls_create_empty(self.h) == 0
+
+    def pls_params(self):
+        out = np.zeros(7)
+        assert self.L.dref_pls_params(self.h, _p(out)) == 0
+        keys = ("R_MIN", "R_MAX", "D_INIT", "S_INIT", "L_MAX", "G_TOL", "E_DIST")
+        return dict(zip(keys, out.tolist()))
+
+    def particles(self):
+        n = self.L.dref_pls_count(self.h)
+        out = np.zeros((max(n, 0), 4))
+        if n > 0:
+            self.L.dref_pls_get(self.h, _p(out))
+        return out
+
+    def set_particles(self, parts):
+        a = np.ascontiguousarray(parts, dtype=np.float64).reshape(-1, 4)
+        assert self.L.dref_pls_set(self.h, _p(a), len(a)) == 0
+
+    def pls_advect(self, dt):
+        """pls->AdvectParticles (ParticleLS2D.c:6-36 / ParticleLS3D.c:6-36) on the set velocity."""
+        assert self.L.dref_pls_advect(self.h, self._vel, float(dt)) == 0
+
+    def pls_correct(self):
+        """pls->ErrorCorrection (ParticleLS2D.c:40-115 / ParticleLS3D.c:40-116)."""
+        assert self.L.dref_pls_correct(self.h) == 0
+
+    def pls_adjust(self):
+        """ParticleLS_AdjustRadii (ParticleLS.c:158-185)."""
+        assert self.L.dref_pls_adjust(self.h) == 0
+
+    def pls_reseed(self):
+        """ParticleLS_ReseedParticles (ParticleLS.c:202-295)."""
+        assert self.L.dref_pls_reseed(self.h) == 0
+
+    def pls_step(self, dt):
+        """LevelSetAdvectPLS (ParticleLS.c:299-329)."""
+        assert self.L.dref_pls_step(self.h, self._vel, float(dt)) == 0
+
+    def pls_rk2_half(self, dt):
+        assert self.L.dref_pls_rk2_half(self.h, self._vel, float(dt)) == 0
+
+    def pls_rk2_full(self, dt):
+        assert self.L.dref_pls_rk2_full(self.h, self._vel, float(dt)) == 0
 
     def sample(self, fn, X):
         return np.array([self.L.dref_sample(self.h, int(fn), *map(float, x)) for x in np.reshape(X, (-1, 3))])

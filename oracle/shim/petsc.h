@@ -44,7 +44,9 @@ typedef struct dcell_shim_vec {
 typedef void *Mat;
 typedef void *DM;
 typedef void *PetscViewer;
-typedef void *PetscRandom;
+typedef struct dcell_shim_random *PetscRandom;
+typedef const char *PetscRandomType;
+#define PETSCRAND48 "rand48"
 
 #define PETSC_COMM_SELF 0
 #define PETSC_COMM_WORLD 1
@@ -81,6 +83,7 @@ int dcell_shim_calloc(size_t bytes, void **out);
 #define PetscAbs(x) (((x) < 0) ? -(x) : (x))
 #define PetscMax(a, b) (((a) < (b)) ? (b) : (a))
 #define PetscMin(a, b) (((a) < (b)) ? (a) : (b))
+#define PetscSign(a) (((a) >= 0) ? ((a) == 0 ? 0 : 1) : -1)
 
 /* logging, info and options: accepted and ignored */
 #define PetscInfo(o, ...) 0
@@ -113,6 +116,14 @@ PetscErrorCode VecGetArray4d(Vec x, PetscInt m, PetscInt n, PetscInt p, PetscInt
                              PetscInt ps, PetscInt qs, PetscScalar *****a);
 PetscErrorCode VecRestoreArray4d(Vec x, PetscInt m, PetscInt n, PetscInt p, PetscInt q, PetscInt ms,
                                  PetscInt ns, PetscInt ps, PetscInt qs, PetscScalar *****a);
+
+/* random numbers: PETSCRAND48 draws from the C library's drand48 stream
+ * (one global state, seeded by srand48(seed) when the type is set; the
+ * default seed is 0x12345678 + 76543 * rank), values in [0, 1). */
+PetscErrorCode PetscRandomCreate(MPI_Comm c, PetscRandom *r);
+PetscErrorCode PetscRandomSetType(PetscRandom r, PetscRandomType t);
+PetscErrorCode PetscRandomGetValue(PetscRandom r, PetscScalar *v);
+PetscErrorCode PetscRandomDestroy(PetscRandom *r);
 
 /* viewers and files: the oracle never writes files */
 PetscErrorCode PetscViewerDestroy(PetscViewer *v);

@@ -210,12 +210,41 @@ void NGA_Inquire(int g_a, int *type, int *ndim, int dims[]) {
   for (int i = 0; i < 4; ++i) dims[i] = shim_ga_dims[i];
 }
 
+/* PETSCRAND48: the C library's drand48 (POSIX: X <- (0x5DEECE66D X + 0xB)
+ * mod 2^48, value X / 2^48), seeded with srand48 when the type is set. */
+struct dcell_shim_random {
+  long seed;
+};
+
+PetscErrorCode PetscRandomCreate(MPI_Comm c, PetscRandom *r) {
+  int rank = 0;
+  (void)c;
+  MPI_Comm_rank(c, &rank);
+  *r = (PetscRandom)calloc(1, sizeof(struct dcell_shim_random));
+  if (!*r) return PETSC_ERR_MEM;
+  (*r)->seed = 0x12345678 + 76543 * rank;
+  return 0;
+}
+PetscErrorCode PetscRandomSetType(PetscRandom r, PetscRandomType t) {
+  if (strcmp(t, PETSCRAND48)) return dcell_shim_error(PETSC_ERR_ARG_OUTOFRANGE, "random type %s", t);
+  srand48(r->seed);
+  return 0;
+}
+PetscErrorCode PetscRandomGetValue(PetscRandom r, PetscScalar *v) {
+  (void)r;
+  *v = drand48();
+  return 0;
+}
+PetscErrorCode PetscRandomDestroy(PetscRandom *r) {
+  free(*r);
+  *r = NULL;
+  return 0;
+}
+
 /* Symbols referenced by the compiled files but defined in subsystems the
- * oracle does not build (GA gather glue, particle level set, file output). */
+ * oracle does not build (GA gather glue, file output). */
 typedef struct _Array *Array;
-typedef struct _ParticleLS *ParticleLS;
 PetscErrorCode GAGather(int ga, Array c, Array v) { (void)ga; (void)c; (void)v; return 1; }
-PetscErrorCode ParticleLSDestroy(ParticleLS pls) { (void)pls; return 0; }
 PetscErrorCode DCellGetWorkingDirectory(char *wd) { strcpy(wd, "."); return 0; }
 typedef struct _Grid *Grid;
 PetscErrorCode GridWrite(Grid g, int t) { (void)g; (void)t; return 0; }

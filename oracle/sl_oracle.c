@@ -955,3 +955,296 @@ ORC_EXPORT long orc_reinit(const orc_geom *g, double *phi, const double *nodes, 
   free(acc);
   return status ? status : count;
 }
+
+/* ===========================================================================
+ * Particle level set (LevelSetMethod/ParticleLS.c, ParticleLS2D.c,
+ * ParticleLS3D.c).  Particles are rows of 4 doubles: X.x, X.y, X.z, radius
+ * (struct _Particle, LSM_private.h:45-48), positions in global index space.
+ * ======================================================================== */
+
+typedef struct {
+  double r_min, r_max, d_init, g_tol, e_dist; /* ParticleLS.c:21-27 */
+  int s_init, l_max;
+} orc_pls_params;
+
+/* PetscSign: 1, 0 or -1 */
+static inline double psign(double a) { return a >= 0 ? (a == 0 ? 0 : 1) : -1; }
+static inline double pabs(double a) { return a < 0 ? -a : a; }
+
+/* drand48 (POSIX): X <- (0x5DEECE66D X + 0xB) mod 2^48, value X / 2^48 --
+ * the stream PETSc's PETSCRAND48 PetscRandomGetValue draws from. */
+static double r48(uint64_t *x) {
+  *x = (0x5DEECE66DULL * *x + 0xBULL) & 0xFFFFFFFFFFFFULL;
+  return (double)*x * (1.0 / 281474976710656.0);
+}
+
+/* GridInterpolate2D/3D, Common/Grid.c:351-410 (weights (1-s)(1-i) + i s). */
+static double grid_interp(const orc_geom *g, const double *f, const double X[3]) {
+  int xs = (int)floor(X[0]), ys = (int)floor(X[1]);
+  double sx = X[0] - xs, sy = X[1] - ys, val = 0;
+  if (g->nz == 1) {
+    for (int j = 0; j < 2; ++j)
+      for (int i = 0; i < 2; ++i)
+        val += ((1 - sx) * (1 - i) + i * sx) * ((1 - sy) * (1 - j) + j * sy) * f[gidx(g, xs + i, ys + j, 0)];
+    return val;
+  }
+  int zs = (int)floor(X[2]);
+  double sz = X[2] - zs;
+  for (int k = 0; k < 2; ++k)
+    for (int j = 0; j < 2; ++j)
+      for (int i = 0; i < 2; ++i)
+        val += ((1 - sx) * (1 - i) + i * sx) * ((1 - sy) * (1 - j) + j * sy) * ((1 - sz) * (1 - k) + k * sz) *
+               f[gidx(g, xs + i, ys + j, zs + k)];
+  return val;
+}
+
+/* Bilinear2D (Common/Grid.c:190-212) of GridFunction2D_Identity / DerivX /
+ * DerivY (:214-227): fn 0, 1, 2 as in gf2. */
+static double bilinear_gf(const orc_geom *g, const double *p, int fn, double x, double y) {
+  int xi = (int)floor(x), yi = (int)floor(y);
+  double xf = (2. * (x - xi) - 1.), yf = (2. * (y - yi) - 1.), sum = 0.;
+  for (int k = 0; k < 2; ++k)
+    for (int l = 0; l < 2; ++l) {
+      double xb = 1. + (2. * k - 1.) * xf;
+      double yb = 1. + (2. * l - 1.) * yf;
+      sum += gf2(g, p, fn, xi + k, yi + l) * xb * yb;
+    }
+  sum /= 4.;
+  return sum;
+}
+
+/* ParticleLS_AdvectParticles2D/3D (ParticleLS2D.c:6-36, ParticleLS3D.c:6-36):
+ * RK2 midpoint, V1 = U(Xp), X = Xp + dt/2 V1/h, V2 = U(X), Xp += dt V2/h. */
+ORC_EXPORT void orc_pls_advect(const orc_geom *g, const double *vel, double *parts, long n, double dt) {
+  const int dim = g->nz == 1 ? 2 : 3;
+  for (long m = 0; m < n; ++m) {
+    double *p = parts + 4 * m, V1[3] = {0, 0, 0}, V2[3] = {0, 0, 0}, X[3];
+    if (dim == 2) {
+      interp_vel2d(g, vel, p, V1);
+      X[0] = p[0] + dt / 2 * V1[0] / g->hx;
+      X[1] = p[1] + dt / 2 * V1[1] / g->hy;
+      interp_vel2d(g, vel, X, V2);
+      p[0] += dt * V2[0] / g->hx;
+      p[1] += dt * V2[1] / g->hy;
+    } else {
+      interp_vel3d(g, vel, p, V1);
+      X[0] = p[0] + dt / 2 * V1[0] / g->hx;
+      X[1] = p[1] + dt / 2 * V1[1] / g->hy;
+      X[2] = p[2] + dt / 2 * V1[2] / g->hz;
+      interp_vel3d(g, vel, X, V2);
+      p[0] += dt * V2[0] / g->hx;
+      p[1] += dt * V2[1] / g->hy;
+      p[2] += dt * V2[2] / g->hz;
+    }
+  }
+}
+
+/* ParticleLS_ErrorCorrection2D/3D (ParticleLS2D.c:40-115,
+ * ParticleLS3D.c:40-116): phi+ = phi- = phi; every escaped particle (on the
+ * wrong side by more than its radius) raises phi+ / lowers phi- at the
+ * corners of its cell to sign (sign r - |X - a|); band points take the one
+ * of phi+, phi- with the smaller magnitude.  The 3D corner z is floor(X.y),
+ * as the reference writes it (ParticleLS3D.c:76).  Corners outside the grid
+ * are skipped (the reference writes out of bounds there); returns their
+ * number. */
+ORC_EXPORT long orc_pls_correct(const orc_geom *g, double *phi, const int *band, long nband, const double *parts,
+                                long n) {
+  const int dim = g->nz == 1 ? 2 : 3;
+  const size_t N = (size_t)g->nx * g->ny * g->nz;
+  double *pos = (double *)malloc(N * sizeof(double)), *neg = (double *)malloc(N * sizeof(double));
+  long skipped = 0;
+  memcpy(pos, phi, N * sizeof(double));
+  memcpy(neg, phi, N * sizeof(double));
+  for (long m = 0; m < n; ++m) {
+    const double *p = parts + 4 * m;
+    double dist = grid_interp(g, phi, p);
+    double sign = psign(p[3]);
+    if (!(sign * dist < 0 && pabs(dist) > pabs(p[3]))) continue;
+    int A[3] = {(int)floor(p[0]), (int)floor(p[1]), dim == 3 ? (int)floor(p[1]) : 0};
+    for (int k = 0; k < (dim == 3 ? 2 : 1); ++k)
+      for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) {
+          int a[3] = {A[0] + i, A[1] + j, A[2] + k};
+          if (a[0] < g->px || a[0] >= g->px + g->nx || a[1] < g->py || a[1] >= g->py + g->ny ||
+              (dim == 3 && (a[2] < g->pz || a[2] >= g->pz + g->nz))) {
+            ++skipped;
+            continue;
+          }
+          double d2 = (p[0] - a[0]) * (p[0] - a[0]) + (p[1] - a[1]) * (p[1] - a[1]);
+          if (dim == 3) d2 = d2 + (p[2] - a[2]) * (p[2] - a[2]);
+          double phi_p = sign * (sign * p[3] - sqrt(d2));
+          size_t q = gidx(g, a[0], a[1], a[2]);
+          if (sign > 0)
+            pos[q] = phi_p < pos[q] ? pos[q] : phi_p;
+          else
+            neg[q] = phi_p < neg[q] ? phi_p : neg[q];
+        }
+  }
+  for (long b = 0; b < nband; ++b) {
+    size_t q = gidx(g, band[3 * b], band[3 * b + 1], dim == 3 ? band[3 * b + 2] : 0);
+    phi[q] = pabs(pos[q]) <= pabs(neg[q]) ? pos[q] : neg[q];
+  }
+  free(pos);
+  free(neg);
+  return skipped;
+}
+
+/* ParticleLS_AdjustRadii (ParticleLS.c:158-185). */
+ORC_EXPORT void orc_pls_adjust(const orc_geom *g, const double *phi, double *parts, long n, const orc_pls_params *prm) {
+  for (long m = 0; m < n; ++m) {
+    double *p = parts + 4 * m;
+    double dist = grid_interp(g, phi, p);
+    double sign = psign(p[3]);
+    double sphi = sign * dist;
+    if (prm->r_min < sphi && sphi < prm->r_max)
+      p[3] = sign * sphi;
+    else if (sphi > prm->r_max)
+      p[3] = sign * prm->r_max;
+    else if (sphi < prm->r_min)
+      p[3] = sign * prm->r_min;
+  }
+}
+
+/* ParticleLS_AttractParticleToPhiGoal (ParticleLS.c:108-154), 2D: steps of
+ * lambda along the normal towards phi_goal, halving lambda after a step that
+ * does not improve; the accepted position is the local Coor X whose z stays
+ * 0.  Without convergence in L_MAX steps the radius becomes sign(phi). */
+static void pls_attract2(const orc_geom *g, const double *phi, double *p, double goal, const orc_pls_params *prm) {
+  double X[3] = {0, 0, 0}, lambda = 1, phi_X = 0;
+  double phi_Xp = bilinear_gf(g, phi, 0, p[0], p[1]);
+  int l;
+  for (l = 0; l < prm->l_max; ++l) {
+    double Nx = bilinear_gf(g, phi, 1, p[0], p[1]);
+    double Ny = bilinear_gf(g, phi, 2, p[0], p[1]);
+    double mag = sqrt(Nx * Nx + Ny * Ny);
+    Nx = Nx / mag;
+    Ny = Ny / mag;
+    double sign = psign(goal - phi_Xp);
+    X[0] = p[0] + sign * lambda * Nx;
+    X[1] = p[1] + sign * lambda * Ny;
+    phi_X = bilinear_gf(g, phi, 0, X[0], X[1]);
+    if (pabs(phi_X - goal) > pabs(phi_Xp - goal)) {
+      lambda = lambda / 2.;
+    } else {
+      p[0] = X[0];
+      p[1] = X[1];
+      p[2] = X[2];
+      phi_Xp = phi_X;
+    }
+    if (pabs(phi_X - goal) < prm->g_tol) break;
+  }
+  if (l == prm->l_max) {
+    phi_X = bilinear_gf(g, phi, 0, p[0], p[1]);
+    p[3] = psign(phi_X);
+  }
+}
+
+/* LevelSetInitializeParticles (ParticleLS.c:6-88), 2D: S_INIT particles in
+ * every band cell with |phi| < D_INIT, each from five draws (position x, y,
+ * z in the cell, side, |phi_goal| in [R_MIN, D_INIT)), attracted to its
+ * phi_goal; then AdjustRadii.  *rng is the drand48 state (in/out).  Returns
+ * the number of particles (at most cap are written), -1 for 3D. */
+ORC_EXPORT long orc_pls_init(const orc_geom *g, const double *phi, const int *band, long nband,
+                             const orc_pls_params *prm, uint64_t *rng, double *out, long cap) {
+  if (g->nz != 1) return -1;
+  long cnt = 0;
+  for (long b = 0; b < nband; ++b) {
+    const int bx = band[3 * b], by = band[3 * b + 1], bz = band[3 * b + 2];
+    double dist = pabs(phi[gidx(g, bx, by, 0)]);
+    if (!(-prm->d_init < dist && dist < prm->d_init)) continue;
+    for (int m = 0; m < prm->s_init; ++m, ++cnt) {
+      double p[4], sign, goal;
+      p[0] = r48(rng);
+      p[1] = r48(rng);
+      p[2] = r48(rng);
+      p[0] += bx - 0.5;
+      p[1] += by - 0.5;
+      p[2] += bz - 0.5;
+      sign = r48(rng);
+      sign = sign > 0.5 ? 1 : -1;
+      goal = r48(rng);
+      goal = (prm->d_init - prm->r_min) * goal + prm->r_min;
+      goal *= sign;
+      p[3] = sign;
+      pls_attract2(g, phi, p, goal, prm);
+      if (cnt < cap) memcpy(out + 4 * cnt, p, sizeof p);
+    }
+  }
+  orc_pls_adjust(g, phi, out, cnt < cap ? cnt : cap, prm);
+  return cnt;
+}
+
+/* ParticleLS_ReseedParticles (ParticleLS.c:202-295), 2D:
+ *  1. delete particles farther than D_INIT (E_DIST for escaped ones), each by
+ *     moving the last particle into its slot (ArrayDelete1, Common/Array.c:
+ *     272-285) and re-examining the slot;
+ *  2. count the non-escaped particles per cell floor(X + 1/2) over phi's box
+ *     (ArrayGetCoor's linear index; particles whose index falls outside are
+ *     not counted -- the reference then increments the previous lookup);
+ *  3. append particles, in band order, to every band cell with |phi| <=
+ *     D_INIT until it holds S_INIT: three draws for the position, then draws
+ *     of phi_goal in [max(-D, phi-0.71), min(D, phi+0.71)) until |phi_goal|
+ *     > R_MIN; radius phi_goal; attracted.
+ * parts holds n particles and room for cap; *rng is the drand48 state.
+ * Returns the new count (> cap: nothing past cap written), -1 for 3D; *uncounted
+ * receives the number of particles of step 2 outside the box. */
+ORC_EXPORT long orc_pls_reseed(const orc_geom *g, const double *phi, const int *band, long nband,
+                               const orc_pls_params *prm, uint64_t *rng, double *parts, long n, long cap,
+                               long *uncounted) {
+  if (g->nz != 1) return -1;
+  for (long i = 0; i < n; ++i) {
+    double *p = parts + 4 * i;
+    double dist = grid_interp(g, phi, p);
+    double sign = psign(p[3]);
+    double thres = sign * dist < 0 ? prm->e_dist : prm->d_init;
+    if (pabs(dist) > thres) {
+      memcpy(p, parts + 4 * (n - 1), 4 * sizeof(double));
+      --n;
+      --i;
+    }
+  }
+  const long ncell = (long)g->nx * g->ny;
+  int *count = (int *)calloc((size_t)ncell, sizeof(int));
+  long miss = 0;
+  for (long i = 0; i < n; ++i) {
+    const double *p = parts + 4 * i;
+    double v = grid_interp(g, phi, p);
+    if (p[3] * v < 0) continue;
+    long cx = (long)floor(p[0] + 0.5), cy = (long)floor(p[1] + 0.5), cz = (long)floor(p[2] + 0.5);
+    long idx = (cx - g->px) + (long)g->nx * (cy - g->py) + (long)g->nx * g->ny * (cz - g->pz);
+    if (idx < 0 || idx >= ncell) {
+      ++miss;
+      continue;
+    }
+    count[idx]++;
+  }
+  if (uncounted) *uncounted = miss;
+  long cnt = n;
+  for (long b = 0; b < nband; ++b) {
+    const int bx = band[3 * b], by = band[3 * b + 1], bz = band[3 * b + 2];
+    double dist = phi[gidx(g, bx, by, 0)];
+    if (pabs(dist) > prm->d_init) continue;
+    long idx = (bx - g->px) + (long)g->nx * (by - g->py);
+    for (int c = count[idx]; c < prm->s_init; ++c, ++cnt) {
+      double p[4], goal, phimax, phimin;
+      p[0] = r48(rng);
+      p[1] = r48(rng);
+      p[2] = r48(rng);
+      p[0] += bx - 0.5;
+      p[1] += by - 0.5;
+      p[2] += bz - 0.5;
+      for (;;) {
+        goal = r48(rng);
+        phimax = prm->d_init < dist + 0.71 ? prm->d_init : dist + 0.71;
+        phimin = -prm->d_init < dist - 0.71 ? dist - 0.71 : -prm->d_init;
+        goal = (phimax - phimin) * goal + phimin;
+        if (goal < -prm->r_min || prm->r_min < goal) break;
+      }
+      p[3] = goal;
+      pls_attract2(g, phi, p, goal, prm);
+      if (cnt < cap) memcpy(parts + 4 * cnt, p, sizeof p);
+    }
+  }
+  free(count);
+  return cnt;
+}

@@ -104,6 +104,86 @@ def run_reinit(ls):
                 band_width=ls.param("bandWidth"))
 
 
+def _swirl(shape, origin, seed, noise):
+    rng = np.random.default_rng(seed)
+    idx = np.meshgrid(*[np.arange(n) + o for n, o in zip(shape, reversed(origin[:len(shape)]))], indexing="ij")
+    if len(shape) == 2:
+        y, x = idx
+        v = np.stack([np.sin(0.3 * x) * np.cos(0.2 * y), -np.cos(0.3 * x) * np.sin(0.2 * y)], -1)
+    else:
+        z, y, x = idx
+        v = np.stack([np.sin(0.3 * y), np.cos(0.2 * z), np.sin(0.25 * x)], -1)
+    return f32(v + noise * rng.standard_normal(v.shape))
+
+
+def run_pls2d():
+    h = 1.0 / 24
+    ls = R.RefLevelSet.circle(h, (0.4512, 0.5371), 0.1)
+    p, _ = ls.geometry()
+    phi, band = ls.get_phi().copy(), ls.band().copy()
+    ls.pls_init()  # PetscRandomSetType seeds drand48 with 0x12345678 (state 0x12345678330E)
+    init, rng_init = ls.particles(), R.rand48_state()
+    vel = _swirl(ls.shape, p, 31, 0.3)
+    dt = 2 * h
+    ls.set_velocity(vel)
+    ls.pls_advect(dt)
+    adv = ls.particles()
+    ls.L.dref_copy_phi_to_phi0(ls.h)
+    ls.L.dref_advect_sl(ls.h, ls._vel, dt)
+    phi_sl = ls.get_phi().copy()
+    ls.pls_correct()
+    corr = np.flatnonzero(ls.get_phi() != phi_sl)
+    phi_corr = ls.get_phi().ravel()[corr]
+    ls.pls_adjust()
+    adj = ls.particles()
+    assert np.array_equal(adj[:, :3], adv[:, :3])
+    ls.pls_reseed()
+    reseed, rng_reseed = ls.particles(), R.rand48_state()
+    ls.close()
+    return dict(origin2=np.array(p[:2]), h2=h, phi2=phi, band2=band, init2=init,
+                rng_init2=np.uint64(rng_init), vel2=vel.astype(np.float32), dt2=dt, adv2=adv, phi_sl2=phi_sl,
+                corr_idx2=corr, corr_val2=phi_corr, adj_radius2=adj[:, 3], reseed2=reseed,
+                rng_reseed2=np.uint64(rng_reseed))
+
+
+def run_pls3d():
+    """A 20x18x16 (z, y, x) box at global origin (3, 1, 0) around a sphere of
+    radius 3.4 cells, band |phi| < 4 cells, 1000 particles in the band.  The
+    reference takes the corner z of an escaped particle from floor(X.y)
+    (ParticleLS3D.c:76), so the z range covers the particles' y range (the
+    reference writes out of bounds otherwise)."""
+    h = 1.0 / 16
+    shape, origin = (20, 18, 16), (3, 1, 0)
+    z, y, x = np.meshgrid(*[np.arange(n) + o for n, o in zip(shape, reversed(origin))], indexing="ij")
+    phi = f32(np.sqrt((x - 10.6) ** 2 + (y - 9.7) ** 2 + (z - 10.2) ** 2) - 3.4)
+    inner = np.zeros(shape, bool)
+    inner[2:-2, 2:-2, 2:-2] = True
+    sel = inner & (np.abs(phi) < 4)
+    band = np.stack([x[sel], y[sel], z[sel]], 1).astype(np.int32)
+    ls = R.RefLevelSet.create(h, origin, shape)
+    ls.set_phi(phi)
+    ls.set_band(band)
+    ls.pls_create_empty()
+    rng = np.random.default_rng(33)
+    pick = band[rng.choice(len(band), 1000)]
+    parts = np.concatenate([pick + rng.uniform(-0.5, 0.5, pick.shape), rng.uniform(-0.6, 0.6, (len(pick), 1))], 1)
+    ls.set_particles(parts)
+    vel = _swirl(shape, origin, 35, 0.2)
+    dt = 0.05
+    ls.set_velocity(vel)
+    ls.pls_advect(dt)
+    adv = ls.particles()
+    ls.pls_correct()
+    corr = np.flatnonzero(ls.get_phi() != phi)
+    phi_corr = ls.get_phi().ravel()[corr]
+    ls.pls_adjust()
+    adj = ls.particles()
+    assert np.array_equal(adj[:, :3], adv[:, :3])
+    ls.close()
+    return dict(origin3=np.array(origin), h3=h, phi3=phi, band3=band, parts3=parts, vel3=vel.astype(np.float32),
+                dt3=dt, adv3=adv, corr_idx3=corr, corr_val3=phi_corr, adj_radius3=adj[:, 3])
+
+
 def main():
     assert R.available(), "build oracle/_ref first: make -C oracle ref"
     # fast-marching reinitialisation: a sphere and a circle as the reference's
@@ -131,6 +211,13 @@ def main():
                         **{f"origin2_{i}": np.array(o) for i, (o, s) in enumerate(boxes2)},
                         **{f"shape2_{i}": np.array(s) for i, (o, s) in enumerate(boxes2)},
                         **{f"vel2_{i}": v.astype(np.float32) for i, v in enumerate(out2)})
+
+    # particle level set (ParticleLS*.c): 2D seeding from the reference's own
+    # rand48 stream, RK2 particle advection in a noisy swirl, SL advection of
+    # phi, escaped-particle correction, radius adjustment and reseeding; 3D
+    # advection / correction / adjustment of particles seeded here (the
+    # reference's seeding is 2D code)
+    np.savez_compressed(os.path.join(OUT, "pls.npz"), **run_pls2d(), **run_pls3d())
 
     h3 = 1.0 / 40
     # 3D: non-cubic grid, non-zero (partly negative) global origin
