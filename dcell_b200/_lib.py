@@ -18,6 +18,7 @@ LINEAR, CUBIC_PLAIN, CUBIC_SEPARABLE, CUBIC_TC = 0, 1, 2, 3
 EULER, MIDPOINT = 0, 1
 FLAG_DEPARTURE_CLAMPED, FLAG_NONFINITE, FLAG_CAPACITY, FLAG_WAIT_TIMEOUT, FLAG_BAD_BAND = 1, 2, 4, 8, 16
 FLAG_UNSETTLED = 32
+FLAG_PARTICLE_OUTSIDE = 64
 
 INTERP = {"linear": LINEAR, "cubic": CUBIC_PLAIN, "cubic_plain": CUBIC_PLAIN, "cubic_separable": CUBIC_SEPARABLE,
           "cubic_tc": CUBIC_TC}
@@ -39,6 +40,13 @@ class IrregularNode(ctypes.Structure):
                 ("signCenter", ctypes.c_int), ("signFace", ctypes.c_int), ("pad", ctypes.c_int),
                 ("d", ctypes.c_double), ("X", ctypes.c_double * 3), ("op", ctypes.c_double * 3),
                 ("n", ctypes.c_double * 3), ("k", ctypes.c_double)]
+
+
+class PlsParams(ctypes.Structure):
+    """struct dcell_pls_params: LevelSetInitializeParticles' parameters (ParticleLS.c:21-27)."""
+    _fields_ = [("r_min", ctypes.c_double), ("r_max", ctypes.c_double), ("d_init", ctypes.c_double),
+                ("g_tol", ctypes.c_double), ("e_dist", ctypes.c_double), ("s_init", ctypes.c_int),
+                ("l_max", ctypes.c_int)]
 
 
 NODE_DTYPE = np.dtype([("pos", "<i4", 3), ("axis", "<i4"), ("shift", "<i4"), ("signCenter", "<i4"),
@@ -106,13 +114,32 @@ def lib():
     L.dcell_sl_step_tc_split.argtypes = [G, vp, vp, d, vp, i, i, vp, vp, vp, vp]
     L.dcell_batch_plan.argtypes = [vp, i, i, i, i, vp, i, vp]
     L.dcell_batch_sl_step.argtypes = [vp, i, vp, i, i, i, i, i, vp, vp, vp, i, i, vp, vp]
+    ll, P = ctypes.c_longlong, ctypes.POINTER(PlsParams)
+    L.dcell_pls_default_params.argtypes = [i, P]
+    L.dcell_pls_default_params.restype = None
+    L.dcell_pls_advect.argtypes = [G, i, vp, vp, ll, d, vp, vp]
+    L.dcell_pls_correct_scratch_bytes.argtypes = [G, i]
+    L.dcell_pls_correct_scratch_bytes.restype = sz
+    L.dcell_pls_correct.argtypes = [G, i, vp, vp, ll, vp, ll, vp, sz, vp, vp]
+    L.dcell_pls_adjust_radii.argtypes = [G, i, vp, vp, ll, P, vp, vp]
+    L.dcell_pls_scratch_bytes.argtypes = [G, ll, ll]
+    L.dcell_pls_scratch_bytes.restype = sz
+    L.dcell_pls_seed.argtypes = [G, i, vp, vp, ll, P, vp, vp, ll, vp, vp, sz, vp, vp]
+    L.dcell_pls_reseed.argtypes = [G, i, vp, vp, ll, P, vp, vp, ll, ll, vp, vp, sz, vp, vp]
+    L.dcell_ls_pls_advect.argtypes = [vp, G, vp, vp, ll, d]
+    L.dcell_ls_pls_correct.argtypes = [vp, G, vp, vp, i, vp, ll]
+    L.dcell_ls_pls_adjust_radii.argtypes = [vp, G, vp, vp, ll, P]
+    L.dcell_ls_pls_seed.argtypes = [vp, G, vp, vp, i, P, vp, vp, ll, vp]
+    L.dcell_ls_pls_reseed.argtypes = [vp, G, vp, vp, i, P, vp, vp, ll, ll, vp]
     for name in ("dcell_sl_step", "dcell_irregular_nodes", "dcell_irregular_nodes_noalloc", "dcell_max_velocity",
                  "dcell_volume", "dcell_reinitialize", "dcell_velocity_box", "dcell_velocity_boxes",
                  "dcell_session_create", "dcell_session_destroy", "dcell_ls_advect_sl",
                  "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_ls_reinitialize",
                  "dcell_tc_gemm_check",
                  "dcell_sl_adjoint", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",
-                 "dcell_sl_step_tc_split"):
+                 "dcell_sl_step_tc_split", "dcell_pls_advect", "dcell_pls_correct", "dcell_pls_adjust_radii",
+                 "dcell_pls_seed", "dcell_pls_reseed", "dcell_ls_pls_advect", "dcell_ls_pls_correct",
+                 "dcell_ls_pls_adjust_radii", "dcell_ls_pls_seed", "dcell_ls_pls_reseed"):
         getattr(L, name).restype = i
     _LIB = L
     return L

@@ -3,9 +3,9 @@
 Every CUDA translation unit under ``dcell_b200/csrc`` is compiled with
 ``nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo`` and linked into one
 C-ABI shared library (static CUDA runtime, so it loads on machines without a
-GPU; kernels need a B200 to run).  ``sl_exact.cu`` is compiled with
-``-fmad=false`` so its FP64 kernels keep the reference's one-rounding-per-
-operation arithmetic.
+GPU; kernels need a B200 to run).  ``sl_exact.cu`` and ``pls.cu`` are
+compiled with ``-fmad=false`` so their FP64 kernels keep the reference's
+one-rounding-per-operation arithmetic.
 
     python -m dcell_b200.build [--force] [--verbose]
 """
@@ -32,6 +32,7 @@ UNITS = {
     "sl_tc.cu": [],
     "sl_adjoint.cu": [],
     "velocity.cu": [],
+    "pls.cu": ["-fmad=false"],
     "capi.cu": [],
 }
 

@@ -194,6 +194,117 @@ DCELL_API int dcell_reinitialize(const dcell_geom *g, int dtype, void *phi, cons
                        scratch, flags, (cudaStream_t)stream);
 }
 
+// ---------------------------------------------------------------------------
+// Particle level set
+
+DCELL_API void dcell_pls_default_params(int dim, dcell_pls_params *out) {
+  if (!out) return;
+  out->r_min = 0.1;
+  out->r_max = 0.5;
+  out->d_init = 3.0;
+  out->g_tol = 1e-3;
+  out->e_dist = 0.5;
+  out->s_init = dim == 3 ? 32 : 16;
+  out->l_max = 30;
+}
+
+static int check_pls_common(const dcell_geom *g, int dtype, long long n, const void *parts) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (n < 0 || n >= (1LL << 31)) FAIL(DCELL_ERR_ARG, "particle count must be in [0, 2^31)");
+  if (n > 0 && !parts) FAIL(DCELL_ERR_ARG, "particles are required");
+  return DCELL_OK;
+}
+
+static int check_pls_params(const dcell_pls_params *prm) {
+  if (!prm) FAIL(DCELL_ERR_ARG, "parameters are required");
+  if (prm->s_init < 0 || prm->s_init > 4096 || prm->l_max < 0 || prm->l_max > 100000)
+    FAIL(DCELL_ERR_ARG, "s_init must be in [0, 4096] and l_max in [0, 100000]");
+  if (!(prm->r_min >= 0) || !(prm->d_init > prm->r_min)) FAIL(DCELL_ERR_ARG, "need 0 <= r_min < d_init");
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_pls_advect(const dcell_geom *g, int dtype, const void *vel, void *particles, long long n,
+                               double dt, int *flags, void *stream) {
+  int rc = check_pls_common(g, dtype, n, particles);
+  if (rc) return rc;
+  if (!vel) FAIL(DCELL_ERR_ARG, "vel is required");
+  return launch_pls_advect(dcell::to_geom(g), dtype, vel, particles, n, dt, flags, (cudaStream_t)stream);
+}
+
+DCELL_API size_t dcell_pls_correct_scratch_bytes(const dcell_geom *g, int dtype) {
+  if (check_geom(g)) return 0;
+  return pls_correct_scratch_bytes(grid_points(g), dtype);
+}
+
+DCELL_API int dcell_pls_correct(const dcell_geom *g, int dtype, void *phi, const int *band, long long nband,
+                                const void *particles, long long n, void *scratch, size_t scratch_bytes, int *flags,
+                                void *stream) {
+  int rc = check_pls_common(g, dtype, n, particles);
+  if (rc) return rc;
+  if (!phi || nband < 0 || nband >= (1LL << 31) || (nband > 0 && !band)) FAIL(DCELL_ERR_ARG, "phi and band are required");
+  const size_t need = pls_correct_scratch_bytes(grid_points(g), dtype);
+  if (!scratch || scratch_bytes < need) FAIL(DCELL_ERR_ARG, "scratch must hold %zu bytes", need);
+  if ((uintptr_t)scratch % 256) FAIL(DCELL_ERR_ARG, "scratch must be 256-byte aligned");
+  return launch_pls_correct(dcell::to_geom(g), dtype, phi, band, nband, particles, n, scratch, flags,
+                            (cudaStream_t)stream);
+}
+
+DCELL_API int dcell_pls_adjust_radii(const dcell_geom *g, int dtype, const void *phi, void *particles, long long n,
+                                     const dcell_pls_params *prm, int *flags, void *stream) {
+  int rc = check_pls_common(g, dtype, n, particles);
+  if (rc) return rc;
+  if ((rc = check_pls_params(prm))) return rc;
+  if (!phi) FAIL(DCELL_ERR_ARG, "phi is required");
+  return launch_pls_adjust(dcell::to_geom(g), dtype, phi, particles, n, *prm, flags, (cudaStream_t)stream);
+}
+
+DCELL_API size_t dcell_pls_scratch_bytes(const dcell_geom *g, long long nband, long long n) {
+  if (check_geom(g) || nband < 0 || n < 0) return 0;
+  return pls_scratch_bytes(grid_points(g), nband, n);
+}
+
+static int check_pls_seed_args(const dcell_geom *g, int dtype, const void *phi, const int *band, long long nband,
+                               const dcell_pls_params *prm, const unsigned long long *rng, const void *parts,
+                               long long n, long long capacity, const long long *count, const void *scratch,
+                               size_t scratch_bytes) {
+  int rc = check_pls_common(g, dtype, n, parts);
+  if (rc) return rc;
+  if ((rc = check_pls_params(prm))) return rc;
+  if (g->n[2] > 1) FAIL(DCELL_ERR_UNSUPPORTED, "particle seeding is 2D (the reference's attraction is 2D code)");
+  if (!phi || !rng || !count) FAIL(DCELL_ERR_ARG, "phi, rng and count are required");
+  if (nband < 0 || nband * (long long)(prm->s_init > 0 ? prm->s_init : 1) >= (1LL << 31) || (nband > 0 && !band))
+    FAIL(DCELL_ERR_ARG, "invalid band");
+  if (capacity < 0 || capacity >= (1LL << 31) || (capacity > 0 && !parts)) FAIL(DCELL_ERR_ARG, "invalid particle buffer");
+  const size_t need = pls_scratch_bytes(grid_points(g), nband, n);
+  if (!scratch || scratch_bytes < need) FAIL(DCELL_ERR_ARG, "scratch must hold %zu bytes", need);
+  if ((uintptr_t)scratch % 256) FAIL(DCELL_ERR_ARG, "scratch must be 256-byte aligned");
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_pls_seed(const dcell_geom *g, int dtype, const void *phi, const int *band, long long nband,
+                             const dcell_pls_params *prm, unsigned long long *rng, void *particles, long long capacity,
+                             long long *count, void *scratch, size_t scratch_bytes, int *flags, void *stream) {
+  int rc = check_pls_seed_args(g, dtype, phi, band, nband, prm, rng, particles, 0, capacity, count, scratch,
+                               scratch_bytes);
+  if (rc) return rc;
+  return launch_pls_seed(dcell::to_geom(g), dtype, phi, band, nband, *prm, rng, particles, capacity, count, scratch,
+                         flags, (cudaStream_t)stream);
+}
+
+DCELL_API int dcell_pls_reseed(const dcell_geom *g, int dtype, const void *phi, const int *band, long long nband,
+                               const dcell_pls_params *prm, unsigned long long *rng, void *particles, long long n,
+                               long long capacity, long long *count, void *scratch, size_t scratch_bytes, int *flags,
+                               void *stream) {
+  int rc = check_pls_seed_args(g, dtype, phi, band, nband, prm, rng, particles, n, capacity, count, scratch,
+                               scratch_bytes);
+  if (rc) return rc;
+  if (n > capacity) FAIL(DCELL_ERR_ARG, "n exceeds the capacity");
+  return launch_pls_reseed(dcell::to_geom(g), dtype, phi, band, nband, *prm, rng, particles, n, capacity, count,
+                           scratch, flags, (cudaStream_t)stream);
+}
+
 DCELL_API int dcell_irregular_nodes_noalloc(const dcell_geom *g, int dtype, const void *phi, const int *band,
                                             int nband, int with_surface, dcell_irregular_node *nodes, int capacity,
                                             int *count, int *flags, void *stream) {
@@ -308,7 +419,7 @@ struct DevBuf {
 struct dcell_session {
   int device = 0;
   cudaStream_t stream = nullptr;
-  DevBuf phi0_64, vel_64, phi_64, phi0_32, vel_32, phi_32, stage32, band, vals, nodes, scratch, small;
+  DevBuf phi0_64, vel_64, phi_64, phi0_32, vel_32, phi_32, stage32, band, vals, nodes, scratch, small, parts;
   std::vector<double> host_vals;
 };
 
@@ -327,6 +438,8 @@ static int session_flags_status(dcell_session *s, int flags) {
     FAIL(DCELL_ERR_UNSUPPORTED, "fast marching left points tentative after its last bucket");
   if (flags & DCELL_FLAG_DEPARTURE_CLAMPED)
     FAIL(DCELL_ERR_DEPARTURE, "a departure point left the grid; its sample was clamped to the grid");
+  if (flags & DCELL_FLAG_PARTICLE_OUTSIDE)
+    FAIL(DCELL_ERR_DEPARTURE, "a particle's stencil or cell left the grid (clamped or skipped)");
   (void)s;
   return DCELL_OK;
 }
@@ -375,7 +488,7 @@ DCELL_API int dcell_session_destroy(dcell_session *s) {
   cudaSetDevice(s->device);
   cudaStreamSynchronize(s->stream);
   for (DevBuf *b : {&s->phi0_64, &s->vel_64, &s->phi_64, &s->phi0_32, &s->vel_32, &s->phi_32, &s->stage32, &s->band, &s->vals,
-                    &s->nodes, &s->scratch, &s->small})
+                    &s->nodes, &s->scratch, &s->small, &s->parts})
     b->release();
   cudaStreamDestroy(s->stream);
   delete s;
@@ -580,6 +693,148 @@ DCELL_API int dcell_ls_max_velocity(dcell_session *s, const dcell_geom *g, const
   DCELL_CUDA_CHECK(cudaMemcpyAsync(maxvel, dmax, sizeof(double), cudaMemcpyDeviceToHost, st));
   DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
   return DCELL_OK;
+}
+
+// Particle level set on host arrays: particles and phi are copied in and
+// out around the device entry points on the session's stream.
+DCELL_API int dcell_ls_pls_advect(dcell_session *s, const dcell_geom *g, const double *vel, double *particles,
+                                  long long n, double dt) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_pls_common(g, DCELL_F64, n, particles);
+  if (rc) return rc;
+  if (!vel) FAIL(DCELL_ERR_ARG, "vel is required");
+  if (n == 0) return DCELL_OK;
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long np = grid_points(g);
+  const int dof = g->n[2] > 1 ? 3 : 2;
+  ENSURE(s->vel_64, np * dof * sizeof(double));
+  ENSURE(s->parts, (size_t)n * 4 * sizeof(double));
+  int *dflags = (int *)s->small.p;
+  DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->vel_64.p, vel, np * dof * sizeof(double), cudaMemcpyHostToDevice, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->parts.p, particles, n * 4 * sizeof(double), cudaMemcpyHostToDevice, st));
+  if ((rc = dcell_pls_advect(g, DCELL_F64, s->vel_64.p, s->parts.p, n, dt, dflags, st))) return rc;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(particles, s->parts.p, n * 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  int hf = 0;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(&hf, dflags, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  return session_flags_status(s, hf);
+}
+
+DCELL_API int dcell_ls_pls_correct(dcell_session *s, const dcell_geom *g, double *phi, const int *band, int nband,
+                                   const double *particles, long long n) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_pls_common(g, DCELL_F64, n, particles);
+  if (rc) return rc;
+  if (!phi || nband < 0 || (nband > 0 && !band)) FAIL(DCELL_ERR_ARG, "phi and band are required");
+  if ((rc = check_band_host(g, band, nband))) return rc;
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long np = grid_points(g);
+  ENSURE(s->phi_64, np * sizeof(double));
+  ENSURE(s->parts, (size_t)(n > 0 ? n : 1) * 4 * sizeof(double));
+  ENSURE(s->band, (size_t)(nband > 0 ? nband : 1) * 3 * sizeof(int));
+  const size_t sb = pls_correct_scratch_bytes(np, DCELL_F64);
+  ENSURE(s->scratch, sb);
+  int *dflags = (int *)s->small.p;
+  DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi_64.p, phi, np * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (n > 0)
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->parts.p, particles, n * 4 * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (nband > 0)
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->band.p, band, (size_t)nband * 3 * sizeof(int), cudaMemcpyHostToDevice, st));
+  if ((rc = dcell_pls_correct(g, DCELL_F64, s->phi_64.p, (const int *)s->band.p, nband, s->parts.p, n, s->scratch.p,
+                              sb, dflags, st)))
+    return rc;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(phi, s->phi_64.p, np * sizeof(double), cudaMemcpyDeviceToHost, st));
+  int hf = 0;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(&hf, dflags, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  return session_flags_status(s, hf);
+}
+
+DCELL_API int dcell_ls_pls_adjust_radii(dcell_session *s, const dcell_geom *g, const double *phi, double *particles,
+                                        long long n, const dcell_pls_params *prm) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_pls_common(g, DCELL_F64, n, particles);
+  if (rc) return rc;
+  if ((rc = check_pls_params(prm))) return rc;
+  if (!phi) FAIL(DCELL_ERR_ARG, "phi is required");
+  if (n == 0) return DCELL_OK;
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long np = grid_points(g);
+  ENSURE(s->phi_64, np * sizeof(double));
+  ENSURE(s->parts, (size_t)n * 4 * sizeof(double));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi_64.p, phi, np * sizeof(double), cudaMemcpyHostToDevice, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->parts.p, particles, n * 4 * sizeof(double), cudaMemcpyHostToDevice, st));
+  if ((rc = dcell_pls_adjust_radii(g, DCELL_F64, s->phi_64.p, s->parts.p, n, prm, nullptr, st))) return rc;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(particles, s->parts.p, n * 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  return DCELL_OK;
+}
+
+// Seed (n < 0) or reseed n particles on host arrays.
+static int ls_pls_seed_common(dcell_session *s, const dcell_geom *g, const double *phi, const int *band, int nband,
+                              const dcell_pls_params *prm, unsigned long long *rng, double *particles, long long n,
+                              long long capacity, long long *count) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  if (!rng || !count) FAIL(DCELL_ERR_ARG, "rng and count are required");
+  int rc = check_pls_common(g, DCELL_F64, n > 0 ? n : 0, particles);
+  if (rc) return rc;
+  if ((rc = check_pls_params(prm))) return rc;
+  if (!phi || nband < 0 || (nband > 0 && !band)) FAIL(DCELL_ERR_ARG, "phi and band are required");
+  if (capacity < (n > 0 ? n : 0) || (capacity > 0 && !particles)) FAIL(DCELL_ERR_ARG, "invalid particle buffer");
+  if ((rc = check_band_host(g, band, nband))) return rc;
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long np = grid_points(g);
+  const long long nn = n > 0 ? n : 0;
+  ENSURE(s->phi_64, np * sizeof(double));
+  ENSURE(s->parts, (size_t)(capacity > 0 ? capacity : 1) * 4 * sizeof(double));
+  ENSURE(s->band, (size_t)(nband > 0 ? nband : 1) * 3 * sizeof(int));
+  const size_t sb = pls_scratch_bytes(np, nband, nn);
+  ENSURE(s->scratch, sb);
+  int *dflags = (int *)s->small.p;
+  unsigned long long *drng = (unsigned long long *)((char *)s->small.p + 128);
+  long long *dcount = (long long *)((char *)s->small.p + 136);
+  DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(drng, rng, sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi_64.p, phi, np * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (nn > 0)
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->parts.p, particles, nn * 4 * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (nband > 0)
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->band.p, band, (size_t)nband * 3 * sizeof(int), cudaMemcpyHostToDevice, st));
+  rc = n < 0 ? dcell_pls_seed(g, DCELL_F64, s->phi_64.p, (const int *)s->band.p, nband, prm, drng, s->parts.p,
+                              capacity, dcount, s->scratch.p, sb, dflags, st)
+             : dcell_pls_reseed(g, DCELL_F64, s->phi_64.p, (const int *)s->band.p, nband, prm, drng, s->parts.p, nn,
+                                capacity, dcount, s->scratch.p, sb, dflags, st);
+  if (rc) return rc;
+  long long hc = 0;
+  int hf = 0;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(&hc, dcount, sizeof(long long), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(rng, drng, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(&hf, dflags, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  *count = hc;
+  const long long ncopy = hc < capacity ? hc : capacity;
+  if (ncopy > 0)
+    DCELL_CUDA_CHECK(cudaMemcpy(particles, s->parts.p, ncopy * 4 * sizeof(double), cudaMemcpyDeviceToHost));
+  return session_flags_status(s, hf);
+}
+
+DCELL_API int dcell_ls_pls_seed(dcell_session *s, const dcell_geom *g, const double *phi, const int *band, int nband,
+                                const dcell_pls_params *prm, unsigned long long *rng, double *particles,
+                                long long capacity, long long *count) {
+  return ls_pls_seed_common(s, g, phi, band, nband, prm, rng, particles, -1, capacity, count);
+}
+
+DCELL_API int dcell_ls_pls_reseed(dcell_session *s, const dcell_geom *g, const double *phi, const int *band,
+                                  int nband, const dcell_pls_params *prm, unsigned long long *rng, double *particles,
+                                  long long n, long long capacity, long long *count) {
+  if (n < 0) FAIL(DCELL_ERR_ARG, "n must be >= 0");
+  return ls_pls_seed_common(s, g, phi, band, nband, prm, rng, particles, n, capacity, count);
 }
 
 }  // extern "C"

@@ -110,6 +110,7 @@ enum : int {
   FLAG_WAIT_TIMEOUT = 8,       // a bounded device wait gave up
   FLAG_BAD_BAND = 16,          // a band entry lies outside the grid (skipped)
   FLAG_UNSETTLED = 32,         // reinitialisation: points still tentative after the last bucket
+  FLAG_PARTICLE_OUTSIDE = 64,  // a particle's stencil or cell left the grid (clamped / skipped)
 };
 
 __device__ __forceinline__ void raise_flag(int *flags, int bit) {

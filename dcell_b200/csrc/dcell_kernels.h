@@ -25,6 +25,12 @@ int launch_batch_cuda_core(const dcell_cell *cells, const dcell_tile *tiles, int
 int launch_sl_adjoint(const dcell::Geom &g, int dtype, const void *phi0, const void *vel, double dt, int interp,
                       int backtrace, const void *gphi, void *gphi0, void *gvel, cudaStream_t st);
 
+// Exclusive scan of n ints (in may alias out); *total = the sum, FLAG_CAPACITY
+// raised in flags when it exceeds cap.  partial: scan_partial_ints(n) ints.
+size_t scan_partial_ints(long long n);
+int launch_scan_exclusive(const int *in, int n, int *out, int *partial, int *total, int cap, int *flags,
+                          cudaStream_t st);
+
 size_t irregular_scratch_bytes(int nband);
 int launch_irregular(const dcell::Geom &g, int dtype, const void *phi, const int *band, int nband, int with_surface,
                      dcell_irregular_node *nodes, int cap, int *count, void *scratch, int *flags, cudaStream_t st);
@@ -51,3 +57,19 @@ int launch_volume(const dcell::Geom &g, int dtype, const void *phi, double eps, 
 int launch_convert(const void *src, int src_dtype, void *dst, int dst_dtype, long long n, cudaStream_t st);
 int launch_gather_band(const dcell::Geom &g, int dtype, const void *phi, const int *band, int nband, void *out,
                        cudaStream_t st);
+
+// particle level set (pls.cu)
+int launch_pls_advect(const dcell::Geom &g, int dtype, const void *vel, void *parts, long long n, double dt,
+                      int *flags, cudaStream_t st);
+size_t pls_correct_scratch_bytes(long long npts, int dtype);
+int launch_pls_correct(const dcell::Geom &g, int dtype, void *phi, const int *band, long long nband,
+                       const void *parts, long long n, void *scratch, int *flags, cudaStream_t st);
+int launch_pls_adjust(const dcell::Geom &g, int dtype, const void *phi, void *parts, long long n,
+                      const dcell_pls_params &prm, int *flags, cudaStream_t st);
+size_t pls_scratch_bytes(long long npts, long long nband, long long n);
+int launch_pls_seed(const dcell::Geom &g, int dtype, const void *phi, const int *band, long long nband,
+                    const dcell_pls_params &prm, unsigned long long *rng, void *parts, long long cap, long long *count,
+                    void *scratch, int *flags, cudaStream_t st);
+int launch_pls_reseed(const dcell::Geom &g, int dtype, const void *phi, const int *band, long long nband,
+                      const dcell_pls_params &prm, unsigned long long *rng, void *parts, long long n, long long cap,
+                      long long *count, void *scratch, int *flags, cudaStream_t st);

@@ -275,6 +275,7 @@ class LevelSet:
     Advect: Optional[Callable] = None
     Reinitialize: Optional[Callable] = None
     flags: Optional[torch.Tensor] = field(default=None)
+    pls: Optional[object] = None  # dcell_b200.pls.ParticleLS once particles are seeded
 
     @property
     def is2D(self) -> bool:
@@ -353,6 +354,14 @@ def LevelSetAdvectAndReinit(ls: LevelSet, velgrid: torch.Tensor, dt: float):
             raise DcellError(_lib.ERR_UNSUPPORTED, "reinitialisation threshold reached but no Reinitialize hook is "
                              "set (fast marching stays the reference's CPU LevelSetReinitialize)")
         ls.Reinitialize(ls)
+
+
+def LevelSetReinitializeGPU(ls: LevelSet, bucket: float = 1.0 / 64):
+    """A Reinitialize hook on the GPU: the reference's LevelSetReinitialize
+    (FastMarching.c:11-146) without its LevelSetResize -- bucketed fast
+    marching from the irregular nodes of phi, new band in grid order."""
+    raw, count = irregular_nodes(ls.phi, ls.h, ls.band, ls.origin, with_surface=False, flags=ls.flags)
+    ls.band = reinitialize(ls.phi, raw, count, ls.bandWidth, bucket, ls.origin, flags=ls.flags)
 
 
 def status(ls: LevelSet) -> int:

@@ -131,6 +131,7 @@ DCELL_API int dcell_version(void);
 #define DCELL_FLAG_WAIT_TIMEOUT 8
 #define DCELL_FLAG_BAD_BAND 16
 #define DCELL_FLAG_UNSETTLED 32 /* reinitialisation: points still tentative after its last bucket */
+#define DCELL_FLAG_PARTICLE_OUTSIDE 64 /* a particle's stencil or cell left the grid (clamped / skipped) */
 DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
                   int nband, int interp, int backtrace, void *phi, int *flags, void *stream);
 
@@ -254,6 +255,74 @@ DCELL_API int dcell_volume(const dcell_geom *g, int dtype, const void *phi, doub
                  size_t scratch_bytes, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Particle level set (LevelSetMethod/ParticleLS.c, ParticleLS2D.c,
+ * ParticleLS3D.c).  Particles are device records of four values of the
+ * dtype: X.x, X.y, X.z in global index space and the signed radius, i.e.
+ * struct _Particle (LevelSetMethod/LSM_private.h:45-48).  Random draws follow
+ * the reference's PETSCRAND48 stream, the C library's drand48: rng holds the
+ * 48-bit state X (X <- 0x5DEECE66D X + 0xB mod 2^48, value X / 2^48); srand48
+ * (0x12345678), PETSc's default seed, gives 0x12345678330E.
+ * ---------------------------------------------------------------------- */
+
+/* LevelSetInitializeParticles' parameters (ParticleLS.c:21-27). */
+typedef struct dcell_pls_params {
+  double r_min, r_max; /* particle radius bounds: 0.1, 0.5 */
+  double d_init;       /* seeding band |phi| < d_init: 3 */
+  double g_tol;        /* attraction tolerance: 1e-3 */
+  double e_dist;       /* escaped particles farther than this are deleted: 0.5 */
+  int s_init;          /* particles per cell: 16 (2D), 32 (3D) */
+  int l_max;           /* attraction steps: 30 */
+} dcell_pls_params;
+DCELL_API void dcell_pls_default_params(int dim, dcell_pls_params *out);
+
+/* ParticleLS_AdvectParticles2D/3D (ParticleLS2D.c:6-36, ParticleLS3D.c:6-36):
+ * RK2 midpoint with the MAC velocity interpolation of InterpolateVelocity*.
+ * vel: the velocity grid of g (dof 2/3 innermost).  Stencils outside the
+ * grid are clamped and raise DCELL_FLAG_PARTICLE_OUTSIDE. */
+DCELL_API int dcell_pls_advect(const dcell_geom *g, int dtype, const void *vel, void *particles, long long n,
+                               double dt, int *flags, void *stream);
+
+/* ParticleLS_ErrorCorrection2D/3D (ParticleLS2D.c:40-115,
+ * ParticleLS3D.c:40-116): escaped particles correct phi at the band points.
+ * The 3D cell corner z is floor(X.y), as the reference computes it
+ * (ParticleLS3D.c:76).  Corners outside the grid are skipped (the reference
+ * writes out of bounds) and raise DCELL_FLAG_PARTICLE_OUTSIDE.  Several
+ * escaped particles giving a corner exactly +0 and -0 may leave the other
+ * zero than the reference's particle order would.  scratch: at least
+ * dcell_pls_correct_scratch_bytes(g, dtype) bytes. */
+DCELL_API size_t dcell_pls_correct_scratch_bytes(const dcell_geom *g, int dtype);
+DCELL_API int dcell_pls_correct(const dcell_geom *g, int dtype, void *phi, const int *band, long long nband,
+                                const void *particles, long long n, void *scratch, size_t scratch_bytes, int *flags,
+                                void *stream);
+
+/* ParticleLS_AdjustRadii (ParticleLS.c:158-185). */
+DCELL_API int dcell_pls_adjust_radii(const dcell_geom *g, int dtype, const void *phi, void *particles, long long n,
+                                     const dcell_pls_params *prm, int *flags, void *stream);
+
+/* LevelSetInitializeParticles' seeding (ParticleLS.c:36-75, 2D): s_init
+ * particles in every band cell with |phi| < d_init, five draws each from
+ * *rng (device, advanced), attracted to their phi goal, then AdjustRadii.
+ * *count (device) = the number seeded; records past capacity are not written
+ * (DCELL_FLAG_CAPACITY).  scratch: dcell_pls_scratch_bytes(g, nband, 0). */
+DCELL_API size_t dcell_pls_scratch_bytes(const dcell_geom *g, long long nband, long long n);
+DCELL_API int dcell_pls_seed(const dcell_geom *g, int dtype, const void *phi, const int *band, long long nband,
+                             const dcell_pls_params *prm, unsigned long long *rng, void *particles, long long capacity,
+                             long long *count, void *scratch, size_t scratch_bytes, int *flags, void *stream);
+
+/* ParticleLS_ReseedParticles (ParticleLS.c:202-295, 2D) on n particles:
+ * deletion in the reference's order (the last particle moves into a deleted
+ * slot), per-cell counts of the non-escaped particles, and new particles in
+ * band order for cells below s_init (draws from *rng, attracted).  *count
+ * (device) = the new number; records past capacity are not written
+ * (DCELL_FLAG_CAPACITY).  Particles whose cell lies outside phi's box are not
+ * counted (DCELL_FLAG_PARTICLE_OUTSIDE; the reference counts them against the
+ * previous lookup).  scratch: dcell_pls_scratch_bytes(g, nband, n). */
+DCELL_API int dcell_pls_reseed(const dcell_geom *g, int dtype, const void *phi, const int *band, long long nband,
+                               const dcell_pls_params *prm, unsigned long long *rng, void *particles, long long n,
+                               long long capacity, long long *count, void *scratch, size_t scratch_bytes, int *flags,
+                               void *stream);
+
+/* ------------------------------------------------------------------------
  * Batched cells: many DCells' level sets of uneven sizes in one launch
  * (the reference advances them one after another per rank,
  * DWorld/DCellsArray.c:50-102).
@@ -330,6 +399,23 @@ DCELL_API int dcell_ls_reinitialize(dcell_session *s, const dcell_geom *g, doubl
 /* LevelSet_MaxVelocity(ls, velgrid) on host arrays. */
 DCELL_API int dcell_ls_max_velocity(dcell_session *s, const dcell_geom *g, const double *vel,
                           const dcell_irregular_node *nodes, int count, double *maxvel);
+
+/* The particle level set on host arrays (FP64, the reference's layout):
+ * particles are ls->pls->particles' struct _Particle records.  rng is the
+ * drand48 state (in/out).  Seed and reseed write at most capacity records
+ * and return DCELL_ERR_CAPACITY when *count exceeds it. */
+DCELL_API int dcell_ls_pls_advect(dcell_session *s, const dcell_geom *g, const double *vel, double *particles,
+                                  long long n, double dt);
+DCELL_API int dcell_ls_pls_correct(dcell_session *s, const dcell_geom *g, double *phi, const int *band, int nband,
+                                   const double *particles, long long n);
+DCELL_API int dcell_ls_pls_adjust_radii(dcell_session *s, const dcell_geom *g, const double *phi, double *particles,
+                                        long long n, const dcell_pls_params *prm);
+DCELL_API int dcell_ls_pls_seed(dcell_session *s, const dcell_geom *g, const double *phi, const int *band, int nband,
+                                const dcell_pls_params *prm, unsigned long long *rng, double *particles,
+                                long long capacity, long long *count);
+DCELL_API int dcell_ls_pls_reseed(dcell_session *s, const dcell_geom *g, const double *phi, const int *band,
+                                  int nband, const dcell_pls_params *prm, unsigned long long *rng, double *particles,
+                                  long long n, long long capacity, long long *count);
 
 /* ------------------------------------------------------------------------
  * Diagnostics

@@ -118,3 +118,195 @@ def test_oracle_pls_vs_reference_live():
     parts, rng, _ = oracle.pls_reseed(phi, band, parts, rng, h, origin=p)
     assert np.array_equal(parts, ls.particles()) and rng == R.rand48_state()
     ls.close()
+
+
+# ---------------------------------------------------------------------------
+# GPU: the CUDA kernels against the reference's golden records and the oracle
+
+def _dev(a, cuda, dtype=None):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+    return t.to(dtype) if dtype is not None else t
+
+
+@pytest.mark.gpu
+def test_gpu_pls2d_fp64_equals_reference(golden, cuda):
+    import torch
+
+    from dcell_b200 import pls
+    g = _g(golden)
+    o, h = tuple(int(v) for v in g["origin2"]), float(g["h2"])
+    phi = _dev(g["phi2"], cuda)
+    band = _dev(g["band2"].astype(np.int32), cuda)
+    rng = pls.new_rng(SEED_STATE, cuda)
+    flags = torch.zeros(1, dtype=torch.int32, device=cuda)
+    parts, n = pls.seed(phi, band, rng, h, o, flags=flags)
+    assert n == len(g["init2"]) and int(rng.item()) == int(g["rng_init2"])
+    assert np.array_equal(parts[:n].cpu().numpy(), g["init2"])
+    vel = _dev(g["vel2"].astype(np.float64), cuda)
+    pls.advect(parts, n, vel, float(g["dt2"]), h, o, flags=flags)
+    assert np.array_equal(parts[:n].cpu().numpy(), g["adv2"])
+    phi_sl = _dev(g["phi_sl2"], cuda)
+    pls.correct(phi_sl, band, parts, n, h, o, flags=flags)
+    want = _corrected(g["phi_sl2"], g["corr_idx2"], g["corr_val2"])
+    assert np.array_equal(phi_sl.cpu().numpy(), want)
+    pls.adjust_radii(phi_sl, parts, n, h, o, flags=flags)
+    assert np.array_equal(parts[:n, 3].cpu().numpy(), g["adj_radius2"])
+    parts, n2 = pls.reseed(phi_sl, band, parts, n, rng, h, o, flags=flags)
+    assert n2 == len(g["reseed2"]) and int(rng.item()) == int(g["rng_reseed2"])
+    assert np.array_equal(parts[:n2].cpu().numpy(), g["reseed2"])
+    assert int(flags.item()) == 0
+
+
+@pytest.mark.gpu
+def test_gpu_pls3d_fp64_equals_reference(golden, cuda):
+    import torch
+
+    from dcell_b200 import pls
+    g = _g(golden)
+    o, h = tuple(int(v) for v in g["origin3"]), float(g["h3"])
+    parts = _dev(g["parts3"], cuda)
+    n = parts.shape[0]
+    flags = torch.zeros(1, dtype=torch.int32, device=cuda)
+    pls.advect(parts, n, _dev(g["vel3"].astype(np.float64), cuda), float(g["dt3"]), h, o, flags=flags)
+    assert np.array_equal(parts.cpu().numpy(), g["adv3"])
+    phi = _dev(g["phi3"], cuda)
+    pls.correct(phi, _dev(g["band3"].astype(np.int32), cuda), parts, n, h, o, flags=flags)
+    assert np.array_equal(phi.cpu().numpy(), _corrected(g["phi3"], g["corr_idx3"], g["corr_val3"]))
+    pls.adjust_radii(phi, parts, n, h, o, pls.params(3), flags=flags)
+    assert np.array_equal(parts[:, 3].cpu().numpy(), g["adj_radius3"])
+    assert int(flags.item()) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("d", ["2", "3"])
+def test_gpu_pls_fp32_within_rounding(golden, cuda, d):
+    """FP32 particles: advection within 1e-4 cells of the reference's FP64,
+    corrected phi within 1e-5 cells, radii within 1e-5."""
+    import torch
+
+    from dcell_b200 import pls
+    g = _g(golden)
+    o, h = tuple(int(v) for v in g["origin" + d]), float(g["h" + d])
+    f32 = torch.float32
+    start = g["init2"] if d == "2" else g["parts3"]
+    base = g["phi_sl2"] if d == "2" else g["phi3"]
+    parts = _dev(start, cuda, f32)
+    n = parts.shape[0]
+    pls.advect(parts, n, _dev(g["vel" + d], cuda, f32), float(g["dt" + d]), h, o)
+    adv = g["adv" + d]
+    assert np.abs(parts.double().cpu().numpy() - adv).max() <= 1e-4
+    phi = _dev(base, cuda, f32)
+    pls.correct(phi, _dev(g["band" + d].astype(np.int32), cuda), _dev(adv, cuda, f32), n, h, o)
+    want = _corrected(base, g["corr_idx" + d], g["corr_val" + d])
+    assert np.abs(phi.double().cpu().numpy() - want).max() <= 1e-5
+    adj = _dev(adv, cuda, f32)
+    pls.adjust_radii(_dev(want, cuda, f32), adj, n, h, o, pls.params(int(d)))
+    assert np.abs(adj[:, 3].double().cpu().numpy() - g["adj_radius" + d]).max() <= 1e-5
+
+
+@pytest.mark.gpu
+def test_gpu_pls_larger_case_equals_oracle(cuda):
+    """A 160^2 circle: GPU seeding, three advect / correct / adjust rounds in
+    a random velocity, and a reseed that deletes and adds many particles --
+    FP64 bit for bit against the oracle."""
+    import torch
+
+    from dcell_b200 import pls
+    N, h = 160, 1 / 160.
+    y, x = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
+    phi_np = np.sqrt((x - 77.3) ** 2 + (y - 81.6) ** 2) - 40.2
+    band_np = np.stack([x[np.abs(phi_np) < 6], y[np.abs(phi_np) < 6], 0 * x[np.abs(phi_np) < 6]], 1).astype(np.int32)
+    rng_np = np.random.default_rng(7)
+    vel_np = rng_np.uniform(-1, 1, (N, N, 2))
+    phi, band, vel = _dev(phi_np, cuda), _dev(band_np, cuda), _dev(vel_np, cuda)
+    rng = pls.new_rng(SEED_STATE, cuda)
+    parts, n = pls.seed(phi, band, rng, h)
+    want, want_rng = oracle.pls_init(phi_np, band_np, SEED_STATE, h)
+    assert n == len(want) and int(rng.item()) == want_rng
+    assert np.array_equal(parts[:n].cpu().numpy(), want)
+    for _ in range(3):
+        pls.advect(parts, n, vel, 2 * h, h)
+        want = oracle.pls_advect(vel_np, want, 2 * h, h)
+        pls.correct(phi, band, parts, n, h)
+        phi_np, _ = oracle.pls_correct(phi_np, band_np, want, h)
+        pls.adjust_radii(phi, parts, n, h)
+        want = oracle.pls_adjust(phi_np, want, h)
+    assert np.array_equal(parts[:n].cpu().numpy(), want)
+    assert np.array_equal(phi.cpu().numpy(), phi_np)
+    parts, n2 = pls.reseed(phi, band, parts, n, rng, h)
+    want, want_rng, _ = oracle.pls_reseed(phi_np, band_np, want, want_rng, h)
+    assert n2 == len(want) and int(rng.item()) == want_rng
+    assert np.array_equal(parts[:n2].cpu().numpy(), want)
+
+
+@pytest.mark.gpu
+def test_gpu_pls_host_buffer_abi(golden, cuda):
+    """dcell_ls_pls_* on host arrays (the drop-in's calls) reproduce the
+    reference's golden records."""
+    import ctypes
+
+    from dcell_b200 import _lib, pls
+    L = _lib.lib()
+    g = _g(golden)
+    o, h = tuple(int(v) for v in g["origin2"]), float(g["h2"])
+    sess = ctypes.c_void_p()
+    _lib.check(L.dcell_session_create(0, ctypes.byref(sess)))
+    try:
+        geo = _lib.geom(g["phi2"].shape, h, o)
+        prm = pls.params(2)
+        band = np.ascontiguousarray(g["band2"], dtype=np.int32)
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        cap = len(band) * prm.s_init
+        parts = np.zeros((cap, 4))
+        rng, count = ctypes.c_ulonglong(SEED_STATE), ctypes.c_longlong(0)
+        _lib.check(L.dcell_ls_pls_seed(sess, ctypes.byref(geo), p(g["phi2"]), p(band), len(band), ctypes.byref(prm),
+                                       ctypes.byref(rng), p(parts), cap, ctypes.byref(count)))
+        n = count.value
+        assert np.array_equal(parts[:n], g["init2"]) and rng.value == int(g["rng_init2"])
+        vel = np.ascontiguousarray(g["vel2"], dtype=np.float64)
+        _lib.check(L.dcell_ls_pls_advect(sess, ctypes.byref(geo), p(vel), p(parts), n, float(g["dt2"])))
+        assert np.array_equal(parts[:n], g["adv2"])
+        phi = g["phi_sl2"].copy()
+        _lib.check(L.dcell_ls_pls_correct(sess, ctypes.byref(geo), p(phi), p(band), len(band), p(parts), n))
+        assert np.array_equal(phi, _corrected(g["phi_sl2"], g["corr_idx2"], g["corr_val2"]))
+        _lib.check(L.dcell_ls_pls_adjust_radii(sess, ctypes.byref(geo), p(phi), p(parts), n, ctypes.byref(prm)))
+        cap2 = n + cap
+        big = np.zeros((cap2, 4))
+        big[:n] = parts[:n]
+        _lib.check(L.dcell_ls_pls_reseed(sess, ctypes.byref(geo), p(phi), p(band), len(band), ctypes.byref(prm),
+                                         ctypes.byref(rng), p(big), n, cap2, ctypes.byref(count)))
+        assert np.array_equal(big[:count.value], g["reseed2"]) and rng.value == int(g["rng_reseed2"])
+        # too small a buffer: the count is reported, nothing past the capacity is written
+        small = np.zeros((3, 4))
+        rc = L.dcell_ls_pls_seed(sess, ctypes.byref(geo), p(g["phi2"]), p(band), len(band), ctypes.byref(prm),
+                                 ctypes.byref(ctypes.c_ulonglong(SEED_STATE)), p(small), 3, ctypes.byref(count))
+        assert rc == _lib.ERR_CAPACITY and count.value == n
+    finally:
+        L.dcell_session_destroy(sess)
+
+
+@pytest.mark.gpu
+def test_gpu_pls_edge_cases(cuda):
+    import torch
+
+    from dcell_b200 import pls
+    from dcell_b200._lib import DcellError
+    phi = _dev(np.linspace(-2, 2, 100).reshape(10, 10), cuda)
+    band = _dev(np.array([[i, j, 0] for j in range(3, 7) for i in range(3, 7)], dtype=np.int32), cuda)
+    empty = torch.zeros((0, 4), dtype=torch.float64, device=cuda)
+    before = phi.clone()
+    pls.correct(phi, band, empty, 0, 1.0)
+    assert torch.equal(phi, before)
+    rng = pls.new_rng(SEED_STATE, cuda)
+    parts, n = pls.reseed(phi, band, torch.zeros((1, 4), dtype=torch.float64, device=cuda), 0, rng)
+    want, want_rng, _ = oracle.pls_reseed(phi.cpu().numpy(), band.cpu().numpy(), np.zeros((0, 4)), SEED_STATE)
+    assert n == len(want) and int(rng.item()) == want_rng and np.array_equal(parts[:n].cpu().numpy(), want)
+    # a particle whose stencil leaves the grid is flagged, not read out of bounds
+    out = _dev(np.array([[0.2, 8.9, 0.0, 0.3]]), cuda)
+    flags = torch.zeros(1, dtype=torch.int32, device=cuda)
+    pls.advect(out, 1, _dev(np.ones((10, 10, 2)), cuda), 0.5, 1.0, flags=flags)
+    assert int(flags.item()) & 64
+    # seeding is 2D
+    with pytest.raises(DcellError):
+        pls.seed(_dev(np.zeros((4, 4, 4)), cuda), band, rng)
