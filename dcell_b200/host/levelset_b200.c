@@ -14,6 +14,13 @@
  *                                        LevelSetReinitialize_cpu when
  *                                        FastMarching.c is built, and stays the
  *                                        default)
+ *   LevelSetInitializeParticles, ParticleLS_AdjustRadii,
+ *   ParticleLS_ReseedParticles          (LevelSetMethod/ParticleLS.c:6-88,
+ *                                        158-185, 202-295)
+ *   ParticleLS_AdvectParticles2D/3D,
+ *   ParticleLS_ErrorCorrection2D/3D     (ParticleLS2D.c, ParticleLS3D.c; the
+ *                                        reference's definitions are renamed
+ *                                        away as above)
  * Everything that calls them -- LevelSetAdvectAndReinit, the RK2 half/full
  * steps (AdvectRK2.c), the particle and implicit variants, DCell's ls->Advect
  * slot -- is unchanged and now runs the GPU path.  Fast-marching
@@ -278,5 +285,220 @@ PetscErrorCode LevelSetReinitialize(LevelSet ls) {
   }
   free(bandbuf);
   ierr = PetscLogEventEnd(EVENT_LevelSetReinitialize, 0, 0, 0, 0); CHKERRQ(ierr);
+  PetscFunctionReturn(0);
+}
+
+/* ---------------------------------------------------------------------------
+ * Particle level set (LevelSetMethod/ParticleLS.c, ParticleLS2D.c,
+ * ParticleLS3D.c).  The particle Array's struct _Particle records (X, radius:
+ * four doubles) go to the GPU as they are.  Random draws continue the C
+ * library's drand48 stream that PETSCRAND48 draws from: its state is read
+ * before and written back after each GPU seeding.  Seeding and reseeding are
+ * 2D, as the reference's attraction step is; in 3D they return an error.
+ */
+
+static void b200_rand48_get(unsigned long long *x) {
+  unsigned short t[3] = {0, 0, 0};
+  unsigned short *o = seed48(t);
+  unsigned short s[3];
+  s[0] = o[0];
+  s[1] = o[1];
+  s[2] = o[2];
+  seed48(s);
+  *x = (unsigned long long)s[0] | ((unsigned long long)s[1] << 16) | ((unsigned long long)s[2] << 32);
+}
+
+static void b200_rand48_set(unsigned long long x) {
+  unsigned short s[3];
+  s[0] = (unsigned short)(x & 0xFFFF);
+  s[1] = (unsigned short)((x >> 16) & 0xFFFF);
+  s[2] = (unsigned short)((x >> 32) & 0xFFFF);
+  seed48(s);
+}
+
+static void b200_pls_params(ParticleLS pls, dcell_pls_params *p) {
+  p->r_min = pls->R_MIN;
+  p->r_max = pls->R_MAX;
+  p->d_init = pls->D_INIT;
+  p->g_tol = pls->G_TOL;
+  p->e_dist = pls->E_DIST;
+  p->s_init = (int)pls->S_INIT;
+  p->l_max = pls->L_MAX;
+}
+
+#undef __FUNCT__
+#define __FUNCT__ "ParticleLS_AdvectParticles"
+static PetscErrorCode b200_pls_advect(ParticleLS pls, Coor dh, Grid velgrid, PetscReal dt) {
+  dcell_session *s;
+  dcell_geom g;
+  int rc;
+  PetscErrorCode ierr;
+
+  PetscFunctionBegin;
+  ierr = PetscLogEventBegin(EVENT_ParticleLS_AdvectParticles, 0, 0, 0, 0); CHKERRQ(ierr);
+  ierr = LevelSetB200Session(&s); CHKERRQ(ierr);
+  b200_geom(velgrid, &g);
+  g.h[0] = dh.x;
+  g.h[1] = dh.y;
+  g.h[2] = dh.z;
+  rc = dcell_ls_pls_advect(s, &g, velgrid->v1, (double *)ArrayGetData(pls->particles), ArrayLength(pls->particles),
+                           dt);
+  if (rc == DCELL_ERR_DEPARTURE) {
+    ierr = PetscInfo1(0, "dcell_ls_pls_advect: %s\n", dcell_last_error()); CHKERRQ(ierr);
+  } else if (rc) {
+    SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_pls_advect: %s", dcell_last_error());
+  }
+  ierr = PetscLogEventEnd(EVENT_ParticleLS_AdvectParticles, 0, 0, 0, 0); CHKERRQ(ierr);
+  PetscFunctionReturn(0);
+}
+
+/* ParticleLS_AdvectParticles2D/3D (ParticleLS2D.c:6-36, ParticleLS3D.c:6-36):
+ * the velocity grid's own dimension decides (the reference's RK2 steps call
+ * the 2D routine in any dimension). */
+PetscErrorCode ParticleLS_AdvectParticles2D(ParticleLS pls, Coor dh, Grid velgrid, PetscReal dt) {
+  return b200_pls_advect(pls, dh, velgrid, dt);
+}
+PetscErrorCode ParticleLS_AdvectParticles3D(ParticleLS pls, Coor dh, Grid velgrid, PetscReal dt) {
+  return b200_pls_advect(pls, dh, velgrid, dt);
+}
+
+#undef __FUNCT__
+#define __FUNCT__ "ParticleLS_ErrorCorrection"
+static PetscErrorCode b200_pls_correct(ParticleLS pls, LevelSet ls) {
+  dcell_session *s;
+  dcell_geom g;
+  int *bscratch, rc;
+  const int *band;
+  PetscErrorCode ierr;
+
+  PetscFunctionBegin;
+  ierr = PetscLogEventBegin(EVENT_ParticleLS_ErrorCorrection, 0, 0, 0, 0); CHKERRQ(ierr);
+  ierr = LevelSetB200Session(&s); CHKERRQ(ierr);
+  b200_geom(ls->phi, &g);
+  band = b200_band(ls->band, &bscratch);
+  rc = dcell_ls_pls_correct(s, &g, ls->phi->v1, band, ArrayLength(ls->band),
+                            (const double *)ArrayGetData(pls->particles), ArrayLength(pls->particles));
+  free(bscratch);
+  if (rc == DCELL_ERR_DEPARTURE) {
+    ierr = PetscInfo1(0, "dcell_ls_pls_correct: %s\n", dcell_last_error()); CHKERRQ(ierr);
+  } else if (rc) {
+    SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_pls_correct: %s", dcell_last_error());
+  }
+  ierr = PetscLogEventEnd(EVENT_ParticleLS_ErrorCorrection, 0, 0, 0, 0); CHKERRQ(ierr);
+  PetscFunctionReturn(0);
+}
+
+/* ParticleLS_ErrorCorrection2D/3D (ParticleLS2D.c:40-115, ParticleLS3D.c:40-116). */
+PetscErrorCode ParticleLS_ErrorCorrection2D(ParticleLS pls, LevelSet ls) { return b200_pls_correct(pls, ls); }
+PetscErrorCode ParticleLS_ErrorCorrection3D(ParticleLS pls, LevelSet ls) { return b200_pls_correct(pls, ls); }
+
+/* ParticleLS_AdjustRadii (ParticleLS.c:158-185). */
+#undef __FUNCT__
+#define __FUNCT__ "ParticleLS_AdjustRadii"
+PetscErrorCode ParticleLS_AdjustRadii(ParticleLS pls, LevelSet ls) {
+  dcell_session *s;
+  dcell_geom g;
+  dcell_pls_params prm;
+  int rc;
+  PetscErrorCode ierr;
+
+  PetscFunctionBegin;
+  ierr = PetscLogEventBegin(EVENT_ParticleLS_AdjustRadii, 0, 0, 0, 0); CHKERRQ(ierr);
+  ierr = LevelSetB200Session(&s); CHKERRQ(ierr);
+  b200_geom(ls->phi, &g);
+  b200_pls_params(pls, &prm);
+  rc = dcell_ls_pls_adjust_radii(s, &g, ls->phi->v1, (double *)ArrayGetData(pls->particles),
+                                 ArrayLength(pls->particles), &prm);
+  if (rc) SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_pls_adjust_radii: %s", dcell_last_error());
+  ierr = PetscLogEventEnd(EVENT_ParticleLS_AdjustRadii, 0, 0, 0, 0); CHKERRQ(ierr);
+  PetscFunctionReturn(0);
+}
+
+/* Seed (n < 0: LevelSetInitializeParticles' loop) or reseed the particle
+ * Array on the GPU, continuing the drand48 stream. */
+static PetscErrorCode b200_pls_seed(ParticleLS pls, LevelSet ls, int reseed) {
+  dcell_session *s;
+  dcell_geom g;
+  dcell_pls_params prm;
+  int *bscratch, rc;
+  const int *band;
+  const int nband = ArrayLength(ls->band);
+  const int n = reseed ? ArrayLength(pls->particles) : 0;
+  long long cap, count = 0;
+  unsigned long long rng;
+  PetscErrorCode ierr;
+
+  PetscFunctionBegin;
+  if (!ls->phi->is2D) SETERRQ(PETSC_COMM_SELF, PETSC_ERR_LIB, "particle seeding is 2D (as the reference's)");
+  ierr = LevelSetB200Session(&s); CHKERRQ(ierr);
+  b200_geom(ls->phi, &g);
+  b200_pls_params(pls, &prm);
+  cap = (long long)n + (long long)nband * prm.s_init;
+  if (cap >= (1LL << 31)) SETERRQ(PETSC_COMM_SELF, PETSC_ERR_LIB, "too many particles");
+  ierr = ArraySetSize(pls->particles, (int)(cap > 0 ? cap : 1)); CHKERRQ(ierr);
+  ierr = ArraySetSize(pls->particles, n); CHKERRQ(ierr);  /* room for cap; n live records kept */
+  band = b200_band(ls->band, &bscratch);
+  b200_rand48_get(&rng);
+  rc = reseed ? dcell_ls_pls_reseed(s, &g, ls->phi->v1, band, nband, &prm, &rng,
+                                    (double *)ArrayGetData(pls->particles), n, cap, &count)
+              : dcell_ls_pls_seed(s, &g, ls->phi->v1, band, nband, &prm, &rng,
+                                  (double *)ArrayGetData(pls->particles), cap, &count);
+  free(bscratch);
+  if (rc && rc != DCELL_ERR_DEPARTURE)
+    SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_pls_(re)seed: %s", dcell_last_error());
+  b200_rand48_set(rng);
+  ierr = ArraySetSize(pls->particles, (int)count); CHKERRQ(ierr);
+  PetscFunctionReturn(0);
+}
+
+/* ParticleLS_ReseedParticles (ParticleLS.c:202-295). */
+#undef __FUNCT__
+#define __FUNCT__ "ParticleLS_ReseedParticles"
+PetscErrorCode ParticleLS_ReseedParticles(ParticleLS pls, LevelSet ls) {
+  PetscErrorCode ierr;
+  PetscFunctionBegin;
+  ierr = PetscLogEventBegin(EVENT_ParticleLS_ReseedParticles, 0, 0, 0, 0); CHKERRQ(ierr);
+  ierr = b200_pls_seed(pls, ls, 1); CHKERRQ(ierr);
+  ierr = PetscLogEventEnd(EVENT_ParticleLS_ReseedParticles, 0, 0, 0, 0); CHKERRQ(ierr);
+  PetscFunctionReturn(0);
+}
+
+/* LevelSetInitializeParticles (ParticleLS.c:6-88): the reference's
+ * parameters, options and PETSCRAND48 generator, the seeding on the GPU
+ * (its AdjustRadii included), the 2D/3D function slots and ls->Advect. */
+#undef __FUNCT__
+#define __FUNCT__ "LevelSetInitializeParticles"
+PetscErrorCode LevelSetInitializeParticles(LevelSet ls) {
+  ParticleLS pls;
+  PetscErrorCode ierr;
+
+  PetscFunctionBegin;
+  ierr = PetscNew(struct _ParticleLS, &ls->pls); CHKERRQ(ierr);
+  pls = ls->pls;
+  pls->R_MIN = 0.1;
+  pls->R_MAX = 0.5;
+  pls->D_INIT = 3.0;
+  pls->S_INIT = ls->phi->is2D ? 16 : 32;
+  pls->L_MAX = 30;
+  pls->G_TOL = 1e-3;
+  pls->E_DIST = 0.5;
+  ierr = PetscOptionsGetReal(0, "-pls_rmin", &pls->R_MIN, 0); CHKERRQ(ierr);
+  ierr = PetscOptionsGetReal(0, "-pls_rmax", &pls->R_MAX, 0); CHKERRQ(ierr);
+  ierr = PetscOptionsGetReal(0, "-pls_dinit", &pls->D_INIT, 0); CHKERRQ(ierr);
+  ierr = PetscOptionsGetInt(0, "-pls_sinit", &pls->S_INIT, 0); CHKERRQ(ierr);
+  ierr = PetscOptionsGetReal(0, "-pls_edist", &pls->E_DIST, 0); CHKERRQ(ierr);
+  ierr = ArrayCreate("particles", sizeof(struct _Particle), &pls->particles); CHKERRQ(ierr);
+  ierr = PetscRandomCreate(PETSC_COMM_WORLD, &pls->rnd); CHKERRQ(ierr);
+  ierr = PetscRandomSetType(pls->rnd, PETSCRAND48); CHKERRQ(ierr);
+  ierr = b200_pls_seed(pls, ls, 0); CHKERRQ(ierr);
+  if (ls->phi->is2D) {
+    pls->AdvectParticles = ParticleLS_AdvectParticles2D;
+    pls->ErrorCorrection = ParticleLS_ErrorCorrection2D;
+  } else {
+    pls->AdvectParticles = ParticleLS_AdvectParticles3D;
+    pls->ErrorCorrection = ParticleLS_ErrorCorrection3D;
+  }
+  ls->Advect = LevelSetAdvectPLS;
+  ierr = PetscInfo(0, "Particles initialized\n"); CHKERRQ(ierr);
   PetscFunctionReturn(0);
 }

@@ -152,3 +152,46 @@ def test_dropin_gpu_reinitialize(cuda, monkeypatch):
     assert set(map(tuple, ref.band().tolist())) == set(map(tuple, b200.band().tolist()))
     ref.close()
     b200.close()
+
+
+def test_dropin_particle_level_set(golden, cuda):
+    """LevelSetInitializeParticles + LevelSetAdvectPLS (ParticleLS.c) with the
+    GPU's seeding, particle advection, error correction, radius adjustment
+    and reseeding linked in: bit-identical to the unmodified reference until
+    the CFL threshold triggers the fast marching (fed the GPU's irregular
+    nodes, projections within ~1e-11), then within 1e-6 cells with the same
+    particle count and random-number state."""
+    g = golden("pls")
+    h, o = float(g["h2"]), tuple(int(v) for v in g["origin2"])
+    ny, nx = g["phi2"].shape
+    y, x = np.meshgrid(np.arange(ny) + o[1], np.arange(nx) + o[0], indexing="ij")
+    c = (o[0] + nx / 2.0, o[1] + ny / 2.0)
+    vel = np.zeros((ny, nx, 2))  # a rotation; about 1.2 CFL per step, so the third step reinitialises
+    vel[..., 0] = -2 * np.pi * h * (y - c[1])
+    vel[..., 1] = 2 * np.pi * h * (x - c[0])
+    dt = 5.3 * h / np.abs(vel).max()
+    runs = []
+    for path in (R.PATH, R.DROPIN_PATH):  # one after the other: both draw from the C library's drand48 state
+        ls = R.RefLevelSet.create(h, o, g["phi2"].shape, path=path)
+        ls.set_phi(g["phi2"])
+        ls.set_band(g["band2"])
+        ls.pls_init()
+        rec = [(ls.particles(), ls.get_phi(), R.rand48_state(path))]
+        ls.set_velocity(vel)
+        for _ in range(5):
+            ls.pls_step(dt)
+            rec.append((ls.particles(), ls.get_phi(), R.rand48_state(path), ls.param("CFLcount")))
+        runs.append(rec)
+        ls.close()
+    ref, b200 = runs
+    assert np.array_equal(ref[0][0], b200[0][0]) and ref[0][2] == b200[0][2]
+    assert np.array_equal(ref[0][0], g["init2"])
+    triggered = False
+    for a, b in zip(ref[1:], b200[1:]):
+        assert a[0].shape == b[0].shape and a[2] == b[2]
+        if not triggered:
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        else:
+            assert np.abs(a[0] - b[0]).max() <= 1e-6 and np.abs(a[1] - b[1]).max() <= 1e-9
+        triggered = triggered or a[3] == 0.0
+    assert triggered  # the reinitialisation and reseeding ran
