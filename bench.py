@@ -274,6 +274,33 @@ def reference_reinit(phi, band):
     return t, out, nb
 
 
+def reference_pls_step(phi, band, vel, parts, h, dt):
+    """One particle step of the reference's own FP64 code (ParticleLS3D.c
+    AdvectParticles3D + ErrorCorrection3D, ParticleLS.c AdjustRadii) on the
+    same particles, one core; seconds per routine."""
+    from oracle import reference as R
+    if not R.available():
+        return None
+    N = phi.shape[0]
+    ls = R.RefLevelSet.create(h, (0, 0, 0), (N, N, N))
+    ls.set_phi(phi.double().cpu().numpy())
+    ls.set_band(band.cpu().numpy())
+    ls.set_velocity(vel.double().cpu().numpy())
+    ls.pls_create_empty()
+    ls.set_particles(parts.double().cpu().numpy())
+    ls.pls_adjust()
+    t0 = time.perf_counter()
+    ls.pls_advect(dt)
+    t1 = time.perf_counter()
+    ls.pls_correct()
+    t2 = time.perf_counter()
+    ls.pls_adjust()
+    t3 = time.perf_counter()
+    adv = ls.particles()
+    ls.close()
+    return {"advect_s": t1 - t0, "correct_s": t2 - t1, "adjust_s": t3 - t2, "step_s": t3 - t0}, adv
+
+
 def e2e_rate(phi, vel, h, dt, K, torch):
     """Through the reference-facing C ABI with pinned FP64 host buffers
     (reference Grid layout): H2D of phi0 + velocity, TC step, D2H of phi,
@@ -456,6 +483,20 @@ def main():
             v = run_vel(dev=dev)
             v.update({"peak_gbs": hbm, "frac": v["achieved_gbs"] / hbm})
             line["velocity_acquisition"] = v
+            # particle level set: ~3.5 M particles around the workload sphere, GPU FP32 vs the reference's FP64
+            from dcell_b200.configs import pls_workload, run_pls
+            wl = pls_workload(args.size, dev=dev)
+            pr = run_pls(args.size, workload=wl, dev=dev)
+            pr.update({"peak_gbs": hbm, "advect_frac": pr["advect_gbs"] / hbm})
+            if world == 1:
+                ref = reference_pls_step(*wl, 1.0 / args.size, 0.5 / args.size)
+                if ref:
+                    times, _ = ref
+                    pr["reference_cpu"] = {**times, "cores": 1, "kind": "reference",
+                                           "particle_updates_per_s": pr["particles"] / times["step_s"],
+                                           "gpu_speedup": times["step_s"] * 1e3 / pr["ms_per_step"]}
+            line["pls"] = pr
+            del wl
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

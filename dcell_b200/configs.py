@@ -22,6 +22,10 @@ vel velocity acquisition of 512 cells' boxes (edges U{32..96}, some
     straddling the domain edge) from a 512^3 fluid field [z][y][x][c] (FP32,
     c = CELL_CENTER, U, V, W) in one dcell_velocity_boxes launch: time,
     achieved bytes/s, and 8 boxes checked against slicing.
+pls the particle level set at 256^3: ~3.5 M FP32 particles (32 per cell
+    within 3 cells of a sphere of radius 0.15) in LeVeque's deformation field;
+    per step RK2 particle advection, escaped-particle error correction and
+    radius adjustment, timed on the device.
 c5  128^3, 50 midpoint steps, velocity from 16 learnable Fourier
     coefficients, loss sum (H_eps(phi_T) - H_eps(phi_target))^2: hand-written
     adjoint (checkpoints every 10) vs FP64 central differences (delta 1e-3)
@@ -225,6 +229,67 @@ def run_vel(G=512, ncells=512, dev="cuda", K=10, W=3):
             "how": "dcell_velocity_boxes, one launch for all boxes, CUDA events, mean of 10 (field + boxes > L2)"}
 
 
+def pls_workload(N=256, per_cell=32, seed=5, dev="cuda", dtype=torch.float32):
+    """phi (cell units) of the workload sphere, its band |phi| < 6 cells, the
+    deformation velocity, and per_cell particles uniform in every cell with
+    |phi| < 3 whose side is phi's sign there (the radius is set by the first
+    adjustment)."""
+    phi = (fields.sphere_sdf(N, device=dev) * N).to(dtype).contiguous()
+    band = fields.band_of(phi, 6.0, margin=3).to(dev)
+    vel = fields.deformation_velocity(N, device=dev).to(dtype).contiguous()
+    near = band[phi[band[:, 2].long(), band[:, 1].long(), band[:, 0].long()].abs() < 3]
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    cells = near.repeat_interleave(per_cell, dim=0).to(dtype)
+    parts = torch.empty((cells.shape[0], 4), dtype=dtype, device=dev)
+    parts[:, :3] = cells + torch.rand(cells.shape, generator=gen, device=dev, dtype=dtype) - 0.5
+    side = phi[near[:, 2].long(), near[:, 1].long(), near[:, 0].long()].sign().repeat_interleave(per_cell)
+    parts[:, 3] = torch.where(side == 0, torch.ones_like(side), side) * 0.3
+    return phi, band, vel, parts.contiguous()
+
+
+def run_pls(N=256, steps=10, warmup=3, dev="cuda", workload=None):
+    import ctypes
+
+    from . import _lib, pls
+    phi, band, vel, parts = workload if workload is not None else pls_workload(N, dev=dev)
+    parts = parts.clone()
+    n = parts.shape[0]
+    h = 1.0 / N
+    dt = 0.5 * h / 1.0  # CFL 0.5 of the field's unit maximum speed
+    prm = pls.params(3)
+    g = _lib.geom(tuple(phi.shape), h)
+    scr = pls._scratch(_lib.lib().dcell_pls_correct_scratch_bytes(ctypes.byref(g), _lib.F32), dev)
+    pls.adjust_radii(phi, parts, n, h, prm=prm)
+    work = phi.clone()
+
+    def step():
+        pls.advect(parts, n, vel, dt, h)
+        pls.correct(work, band, parts, n, h, scratch=scr)
+        pls.adjust_radii(work, parts, n, h, prm=prm)
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    # the three kernels timed alone (advection dominates)
+    parts_f = parts.clone()
+    e0.record()
+    for _ in range(steps):
+        pls.advect(parts_f, n, vel, dt, h)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_adv = e0.elapsed_time(e1) / steps
+    return {"grid": [N] * 3, "particles": n, "band_points": int(band.shape[0]), "dtype": "f32", "steps": steps,
+            "ms_per_step": ms, "particle_updates_per_s": n / (ms / 1e3), "advect_ms": ms_adv,
+            "advect_bytes_per_particle": 32, "advect_gbs": n * 32 / (ms_adv / 1e3) / 1e9,
+            "how": "advect (RK2 midpoint) + error correction + adjust radii per step, CUDA events, phi held fixed"}
+
+
 def run_c5(N=128, steps=50, every=10, dev="cuda", fd_modes=16):
     from .autograd import FourierVelocity, c5_loss, transport
     h = 1.0 / N
@@ -270,14 +335,15 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("which", nargs="?", default="all")
     ap.add_argument("--out", default=None)
-    ap.add_argument("--grid", type=int, default=512, help="vel: edge of the fluid field")
+    ap.add_argument("--grid", type=int, default=None, help="vel: edge of the fluid field (512); pls: grid edge (256)")
     ap.add_argument("--cells", type=int, default=512, help="vel: number of cell boxes")
     a = ap.parse_args()
     todo = ["c1", "c2", "c3", "c4", "c5"] if a.which == "all" else a.which.split(",")
     results = {}
     for c in todo:
         t0 = time.time()
-        results[c] = run_vel(a.grid, a.cells) if c == "vel" else globals()[f"run_{c}"]()
+        results[c] = (run_vel(a.grid or 512, a.cells) if c == "vel" else
+                      run_pls(a.grid or 256) if c == "pls" else globals()[f"run_{c}"]())
         results[c]["wall_s"] = time.time() - t0
         print(json.dumps({c: results[c]}, default=float), flush=True)
     if a.out:

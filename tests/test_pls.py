@@ -310,3 +310,41 @@ def test_gpu_pls_edge_cases(cuda):
     # seeding is 2D
     with pytest.raises(DcellError):
         pls.seed(_dev(np.zeros((4, 4, 4)), cuda), band, rng)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")
+def test_gpu_levelset_advect_pls_equals_reference(golden, cuda):
+    """dcell_b200.pls.LevelSetAdvectPLS (GPU SL, correction, irregular nodes,
+    CFL count, radius adjustment) against the reference's LevelSetAdvectPLS
+    for steps below the reinitialisation threshold: FP64 bit for bit."""
+    import torch
+
+    from dcell_b200 import levelset as L
+    from dcell_b200 import pls
+    g = _g(golden)
+    h, o = float(g["h2"]), tuple(int(v) for v in g["origin2"])
+    ny, nx = g["phi2"].shape
+    y, x = np.meshgrid(np.arange(ny) + o[1], np.arange(nx) + o[0], indexing="ij")
+    vel = np.zeros((ny, nx, 2))
+    vel[..., 0] = -2 * np.pi * h * (y - (o[1] + ny / 2.0))
+    vel[..., 1] = 2 * np.pi * h * (x - (o[0] + nx / 2.0))
+    dt = 1.5 * h / np.abs(vel).max()
+    ref = R.RefLevelSet.create(h, o, (ny, nx))
+    ref.set_phi(g["phi2"])
+    ref.set_band(g["band2"])
+    ref.pls_init()
+    ref.set_velocity(vel)
+    ls = L.LevelSetCreate((h, h, h), o + (0,), (nx, ny, 0), dtype=torch.float64, device=cuda)
+    ls.phi.copy_(_dev(g["phi2"], cuda))
+    ls.band = _dev(g["band2"].astype(np.int32), cuda)
+    pls.LevelSetInitializeParticles(ls)
+    assert ls.Advect is pls.LevelSetAdvectPLS
+    v = _dev(vel, cuda)
+    for _ in range(2):
+        ref.pls_step(dt)
+        ls.Advect(ls, v, dt)
+        assert np.array_equal(ls.pls.live.cpu().numpy(), ref.particles())
+        assert np.array_equal(ls.phi.cpu().numpy(), ref.get_phi())
+        assert abs(ls.CFLcount - ref.param("CFLcount")) <= 1e-12
+    ref.close()
