@@ -189,9 +189,9 @@ def test_dropin_particle_level_set(golden, cuda):
     triggered = False
     for a, b in zip(ref[1:], b200[1:]):
         assert a[0].shape == b[0].shape and a[2] == b[2]
+        triggered = triggered or a[3] == 0.0  # this step reinitialised and reseeded
         if not triggered:
             assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
         else:
             assert np.abs(a[0] - b[0]).max() <= 1e-6 and np.abs(a[1] - b[1]).max() <= 1e-9
-        triggered = triggered or a[3] == 0.0
     assert triggered  # the reinitialisation and reseeding ran
