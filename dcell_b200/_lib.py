@@ -131,6 +131,20 @@ def lib():
     L.dcell_ls_pls_adjust_radii.argtypes = [vp, G, vp, vp, ll, P]
     L.dcell_ls_pls_seed.argtypes = [vp, G, vp, vp, i, P, vp, vp, ll, vp]
     L.dcell_ls_pls_reseed.argtypes = [vp, G, vp, vp, i, P, vp, vp, ll, ll, vp]
+    cp = ctypes.c_char_p
+    L.dcell_writer_create.argtypes = [cp, cp, i, ctypes.POINTER(vp)]
+    L.dcell_writer_flush.argtypes = [vp]
+    L.dcell_writer_destroy.argtypes = [vp]
+    L.dcell_writer_grid.argtypes = [vp, cp, i, G, i, i, vp, vp]
+    L.dcell_writer_grid_host.argtypes = [vp, cp, i, G, i, vp]
+    L.dcell_writer_irregular_nodes.argtypes = [vp, cp, i, i, vp, vp, i, vp]
+    L.dcell_writer_irregular_nodes_host.argtypes = [vp, cp, i, i, vp, i]
+    L.dcell_writer_particles.argtypes = [vp, cp, i, vp, ll, i, vp]
+    L.dcell_writer_particles_host.argtypes = [vp, cp, i, vp, ll]
+    for name in ("dcell_writer_create", "dcell_writer_flush", "dcell_writer_destroy", "dcell_writer_grid",
+                 "dcell_writer_grid_host", "dcell_writer_irregular_nodes", "dcell_writer_irregular_nodes_host",
+                 "dcell_writer_particles", "dcell_writer_particles_host"):
+        getattr(L, name).restype = i
     for name in ("dcell_sl_step", "dcell_irregular_nodes", "dcell_irregular_nodes_noalloc", "dcell_max_velocity",
                  "dcell_volume", "dcell_reinitialize", "dcell_velocity_box", "dcell_velocity_boxes",
                  "dcell_session_create", "dcell_session_destroy", "dcell_ls_advect_sl",

@@ -33,6 +33,7 @@ UNITS = {
     "sl_adjoint.cu": [],
     "velocity.cu": [],
     "pls.cu": ["-fmad=false"],
+    "writer.cu": [],
     "capi.cu": [],
 }
 

@@ -26,6 +26,9 @@ pls the particle level set at 256^3: ~3.5 M FP32 particles (32 per cell
     within 3 cells of a sphere of radius 0.15) in LeVeque's deformation field;
     per step RK2 particle advection, escaped-particle error correction and
     radius adjustment, timed on the device.
+io  output: phi of the 256^3 workload (FP32) written 10 times in the
+    reference's .Real64 format by the asynchronous writer -- the time the
+    compute stream spends on each snapshot, and the drain rate to disk.
 c5  128^3, 50 midpoint steps, velocity from 16 learnable Fourier
     coefficients, loss sum (H_eps(phi_T) - H_eps(phi_target))^2: hand-written
     adjoint (checkpoints every 10) vs FP64 central differences (delta 1e-3)
@@ -290,6 +293,40 @@ def run_pls(N=256, steps=10, warmup=3, dev="cuda", workload=None):
             "how": "advect (RK2 midpoint) + error correction + adjust radii per step, CUDA events, phi held fixed"}
 
 
+def run_io(N=256, writes=10, directory=None, dev="cuda"):
+    import shutil
+    import tempfile
+
+    from .writer import Writer
+    phi = (fields.sphere_sdf(N, device=dev) * N).float().contiguous()
+    h = 1.0 / N
+    d = directory or tempfile.mkdtemp(prefix="dcell_io_")
+    try:
+        with Writer(d, tmpdir=d) as w:
+            w.grid("warm", 0, phi, h)
+            w.flush()
+            e0, e1 = _events()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e0.record()
+            for t in range(writes):
+                w.grid("phi", t, phi, h)
+            e1.record()
+            torch.cuda.synchronize()
+            stream_ms = e0.elapsed_time(e1) / writes
+            w.flush()
+            wall = time.perf_counter() - t0
+        nbytes = phi.numel() * 8 + 8
+    finally:
+        if directory is None:
+            shutil.rmtree(d, ignore_errors=True)
+    return {"grid": [N] * 3, "writes": writes, "file_bytes": nbytes, "stream_ms_per_write": stream_ms,
+            "snapshot_gbs": 2 * phi.numel() * 4 / (stream_ms / 1e3) / 1e9, "drain_s": wall,
+            "drain_gbs": writes * nbytes / wall / 1e9,
+            "how": "dcell_writer_grid: device snapshot on the stream (CUDA events), file writing by the writer thread "
+                   "(wall clock to the flush)"}
+
+
 def run_c5(N=128, steps=50, every=10, dev="cuda", fd_modes=16):
     from .autograd import FourierVelocity, c5_loss, transport
     h = 1.0 / N
@@ -343,7 +380,8 @@ def main():
     for c in todo:
         t0 = time.time()
         results[c] = (run_vel(a.grid or 512, a.cells) if c == "vel" else
-                      run_pls(a.grid or 256) if c == "pls" else globals()[f"run_{c}"]())
+                      run_pls(a.grid or 256) if c == "pls" else run_io(a.grid or 256) if c == "io" else
+                      globals()[f"run_{c}"]())
         results[c]["wall_s"] = time.time() - t0
         print(json.dumps({c: results[c]}, default=float), flush=True)
     if a.out:

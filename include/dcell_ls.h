@@ -418,6 +418,52 @@ DCELL_API int dcell_ls_pls_reseed(dcell_session *s, const dcell_geom *g, const d
                                   long long n, long long capacity, long long *count);
 
 /* ------------------------------------------------------------------------
+ * Output in the reference's file formats, written asynchronously
+ * ---------------------------------------------------------------------- */
+typedef struct dcell_writer dcell_writer;
+
+/* A writer with a background thread; dir receives grids and node lists,
+ * tmpdir (NULL: $PETSC_TMP, else /tmp) the particle arrays, as PetscGetTmp
+ * directs the reference's ArrayWrite.  Device writes use `device`. */
+DCELL_API int dcell_writer_create(const char *dir, const char *tmpdir, int device, dcell_writer **out);
+/* Waits for every pending write; returns the first error since the last flush. */
+DCELL_API int dcell_writer_flush(dcell_writer *w);
+DCELL_API int dcell_writer_destroy(dcell_writer *w);
+
+/* GridWrite (Common/Serialize.c:23-55): <dir>/<name>.<t+10000>.Real64 in
+ * PETSc's binary Vec format (big-endian int32 class id 1211214, int32
+ * length, FP64 values; FP32 data is widened), its .info companion
+ * ("-vecload_block_size <dof>" for dof > 1), and one line "px py [pz]" /
+ * "nx ny [nz]" appended to <dir>/<name>.pos / .size (truncated by this
+ * writer's first write).  data: the grid's dof values per point on the device
+ * (dcell_writer_grid; snapshotted on `stream`, the caller may overwrite it
+ * once the stream passes this call) or FP64 on the host. */
+DCELL_API int dcell_writer_grid(dcell_writer *w, const char *name, int t, const dcell_geom *g, int dof, int dtype,
+                                const void *data, void *stream);
+DCELL_API int dcell_writer_grid_host(dcell_writer *w, const char *name, int t, const dcell_geom *g, int dof,
+                                     const double *data);
+
+/* LevelSetWriteIrregularNodeList (LevelSetMethod/IrregularNodes.c:145-246):
+ * <dir>/<name>.irregNode.<idx+10000>.array, big-endian FP64 rows -- 2D: X,
+ * pos, n, f1, fa1, k, f1_n, f1_nn (11) for nodes with axis != -1; 3D: X, pos,
+ * n, k and the 13 IIM quantities (23) for every node.  IIM quantities this
+ * path does not compute are 0.  count is a device int (dcell_irregular_nodes'
+ * output) for the device form. */
+DCELL_API int dcell_writer_irregular_nodes(dcell_writer *w, const char *name, int idx, int dim,
+                                           const dcell_irregular_node *nodes, const int *count, int capacity,
+                                           void *stream);
+DCELL_API int dcell_writer_irregular_nodes_host(dcell_writer *w, const char *name, int idx, int dim,
+                                                const dcell_irregular_node *nodes, int count);
+
+/* ArrayWrite of the particle Array (Common/Array.c:133-150, via
+ * ParticleLSWriteParticles, ParticleLS.c:190-198): <tmpdir>/<name>.<t+10000>.array,
+ * the n records as native FP64 (FP32 data is widened). */
+DCELL_API int dcell_writer_particles(dcell_writer *w, const char *name, int t, const void *particles, long long n,
+                                     int dtype, void *stream);
+DCELL_API int dcell_writer_particles_host(dcell_writer *w, const char *name, int t, const double *particles,
+                                          long long n);
+
+/* ------------------------------------------------------------------------
  * Diagnostics
  * ---------------------------------------------------------------------- */
 
