@@ -16,12 +16,15 @@
 //              133-150): the raw records (X.x, X.y, X.z, radius as native
 //              FP64).
 //
-// A device write snapshots the data into a device staging buffer on the
-// caller's stream (HBM to HBM), then a copy stream of the writer moves it to
-// pinned host memory while the caller's stream runs on; a writer thread waits
-// for each copy, converts and writes the file.  Host writes copy into pinned
-// memory and go through the same thread.  dcell_writer_flush waits for every
-// pending write and returns the first error.
+// A device write snapshots the data on the caller's stream into memory from
+// the writer's stream-ordered pool (HBM to HBM: the only cost the caller's
+// stream sees); the writer thread moves each snapshot through two pinned
+// 60 MiB chunks on its own copy stream (the copy of one chunk overlaps the
+// formatting and writing of the other) and frees it.  The staged total is
+// bounded (DCELL_WRITER_MAX_STAGED_MB, default 16 GiB): a write waits while
+// it would exceed it.  Host writes keep a copy of the data and go through the
+// same thread.  dcell_writer_flush waits for every pending write and returns
+// the first error.
 #include <errno.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -43,6 +46,9 @@ namespace {
 
 constexpr int FILE_COUNT_START = 10000;  // Common/Common.h:59
 constexpr int32_t VEC_FILE_CLASSID = 1211214;
+// pinned chunk: a multiple of every record size (4, 8, 16, 32, 120 bytes)
+constexpr size_t CHUNK = 480u << 17;  // 60 MiB
+constexpr size_t DEFAULT_MAX_STAGED = 16ull << 30;
 
 enum JobKind { JOB_GRID, JOB_NODES, JOB_PARTICLES };
 
@@ -53,69 +59,23 @@ struct Job {
   int dof = 1;            // grid block size
   int dim = 3;            // nodes: 2 or 3
   int dtype = DCELL_F64;  // grid / particles element type
-  long long count = 0;    // values (grid), records (particles); nodes: capacity
+  long long count = 0;    // values (grid), records (particles / nodes; nodes: capacity)
   std::string pos_path, size_path, pos_line, size_line;  // grid: appended lines
-  std::vector<unsigned char> host;  // host data (host writes)
-  void *pinned = nullptr;           // pinned data (device writes), from the pool
-  size_t pinned_cap = 0;
-  size_t bytes = 0;
-  void *staging = nullptr;          // device staging buffer, from the pool
-  size_t staging_cap = 0;
-  cudaEvent_t done = nullptr;       // copy completion (device writes)
+  std::vector<unsigned char> host;  // host writes: the data (nodes: records + int32 count)
+  void *staging = nullptr;          // device writes: stream-ordered snapshot
+  size_t bytes = 0;                 // staged bytes (nodes: records + int32 count)
+  cudaEvent_t snap = nullptr;       // snapshot complete on the caller's stream
 };
 
-// Reusable buffers (device staging, pinned host): a buffer is taken when it
-// holds the request and at most twice it, else a new one is allocated.
-struct BufPool {
-  std::multimap<size_t, void *> free_;
-  bool device;
-  explicit BufPool(bool dev) : device(dev) {}
-  void *take(size_t bytes, size_t &cap) {
-    auto it = free_.lower_bound(bytes);
-    if (it != free_.end() && it->first <= 2 * bytes + 4096) {
-      void *p = it->second;
-      cap = it->first;
-      free_.erase(it);
-      return p;
-    }
-    void *p = nullptr;
-    const cudaError_t e = device ? cudaMalloc(&p, bytes) : cudaMallocHost(&p, bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return nullptr;
-    }
-    cap = bytes;
-    return p;
-  }
-  void give(void *p, size_t cap) {
-    if (p) free_.emplace(cap, p);
-  }
-  void clear() {
-    for (auto &kv : free_) device ? cudaFree(kv.second) : cudaFreeHost(kv.second);
-    free_.clear();
-  }
-};
-
-void put_be32(FILE *f, int32_t v) {
-  unsigned char b[4] = {(unsigned char)(v >> 24), (unsigned char)(v >> 16), (unsigned char)(v >> 8), (unsigned char)v};
-  fwrite(b, 1, 4, f);
+void be32(unsigned char *o, int32_t v) {
+  o[0] = (unsigned char)(v >> 24), o[1] = (unsigned char)(v >> 16), o[2] = (unsigned char)(v >> 8),
+  o[3] = (unsigned char)v;
 }
 
-// FP64 values, big-endian, in chunks
-bool put_be64(FILE *f, const double *v, long long n) {
-  unsigned char buf[8 * 1024];
-  long long i = 0;
-  while (i < n) {
-    const long long m = (n - i) < 1024 ? (n - i) : 1024;
-    for (long long k = 0; k < m; ++k) {
-      uint64_t u;
-      memcpy(&u, v + i + k, 8);
-      for (int b = 0; b < 8; ++b) buf[8 * k + b] = (unsigned char)(u >> (56 - 8 * b));
-    }
-    if (fwrite(buf, 8, (size_t)m, f) != (size_t)m) return false;
-    i += m;
-  }
-  return true;
+void be64(unsigned char *o, double d) {
+  uint64_t u;
+  memcpy(&u, &d, 8);
+  for (int b = 0; b < 8; ++b) o[b] = (unsigned char)(u >> (56 - 8 * b));
 }
 
 }  // namespace
@@ -125,16 +85,19 @@ struct dcell_writer {
   int device = 0;
   bool cuda_ready = false;
   cudaStream_t copy = nullptr;
+  cudaMemPool_t pool = nullptr;
+  void *pin[2] = {nullptr, nullptr};
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   std::mutex mu;
   std::condition_variable cv, idle;
   std::deque<std::unique_ptr<Job>> queue;
   int inflight = 0;
+  size_t staged = 0, max_staged = DEFAULT_MAX_STAGED;
   bool stop = false;
   int error = DCELL_OK;
   std::string error_text;
   std::map<std::string, bool> opened;  // .pos/.size files truncated on first write
-  std::mutex pool_mu;
-  BufPool dev_pool{true}, host_pool{false};
+  std::vector<unsigned char> out;      // formatted bytes of one chunk
   std::thread thread;
 
   void fail(int code, const std::string &text) {
@@ -160,92 +123,159 @@ struct dcell_writer {
       {
         std::lock_guard<std::mutex> g(mu);
         --inflight;
+        staged -= job->staging ? job->bytes : 0;
       }
       idle.notify_all();
     }
   }
 
   void release(Job &j) {
-    if (j.done) {
-      cudaSetDevice(device);
-      cudaEventDestroy(j.done);
-      j.done = nullptr;
-    }
-    std::lock_guard<std::mutex> g(pool_mu);
-    dev_pool.give(j.staging, j.staging_cap);
-    host_pool.give(j.pinned, j.pinned_cap);
-    j.staging = j.pinned = nullptr;
+    if (!j.snap) return;
+    cudaSetDevice(device);
+    cudaFreeAsync(j.staging, copy);
+    cudaEventDestroy(j.snap);
+    j.snap = nullptr;
   }
 
-  const unsigned char *data(Job &j) {
-    if (j.done) {
-      cudaSetDevice(device);
-      if (cudaEventSynchronize(j.done) != cudaSuccess) {
-        fail(DCELL_ERR_CUDA, "device-to-host copy of " + j.path + " failed");
-        return nullptr;
+  // Feed the job's first `bytes` bytes to sink in pieces of whole records:
+  // host data at once, device data through the two pinned chunks (the copy of
+  // one overlaps the formatting of the other).
+  template <typename Sink>
+  bool drain(Job &j, size_t bytes, Sink sink) {
+    if (!j.snap) return bytes == 0 || sink(j.host.data(), bytes);
+    cudaSetDevice(device);
+    if (!ensure_pins() || cudaStreamWaitEvent(copy, j.snap, 0) != cudaSuccess) return false;
+    const size_t nchunk = (bytes + CHUNK - 1) / CHUNK;
+    size_t prev_len = 0;
+    for (size_t c = 0; c <= nchunk; ++c) {
+      if (c < nchunk) {
+        const size_t off = c * CHUNK, len = bytes - off < CHUNK ? bytes - off : CHUNK;
+        if (cudaMemcpyAsync(pin[c & 1], (const char *)j.staging + off, len, cudaMemcpyDeviceToHost, copy) !=
+                cudaSuccess ||
+            cudaEventRecord(pin_ev[c & 1], copy) != cudaSuccess)
+          return false;
+        if (c == 0) {
+          prev_len = len;
+          continue;
+        }
+        if (cudaEventSynchronize(pin_ev[(c - 1) & 1]) != cudaSuccess) return false;
+        if (!sink((const unsigned char *)pin[(c - 1) & 1], prev_len)) return false;
+        prev_len = len;
+      } else if (nchunk) {
+        if (cudaEventSynchronize(pin_ev[(c - 1) & 1]) != cudaSuccess) return false;
+        if (!sink((const unsigned char *)pin[(c - 1) & 1], prev_len)) return false;
       }
-      return (const unsigned char *)j.pinned;
     }
-    static const unsigned char empty = 0;
-    return j.host.empty() ? &empty : j.host.data();
+    return true;
+  }
+
+  // The node count stored after the records.
+  bool node_count(Job &j, int32_t &cnt) {
+    if (!j.snap) {
+      memcpy(&cnt, j.host.data() + j.bytes - sizeof(int32_t), sizeof cnt);
+      return true;
+    }
+    cudaSetDevice(device);
+    if (!ensure_pins() || cudaStreamWaitEvent(copy, j.snap, 0) != cudaSuccess ||
+        cudaMemcpyAsync(pin[0], (const char *)j.staging + j.bytes - sizeof(int32_t), sizeof(int32_t),
+                        cudaMemcpyDeviceToHost, copy) != cudaSuccess ||
+        cudaStreamSynchronize(copy) != cudaSuccess)
+      return false;
+    memcpy(&cnt, pin[0], sizeof cnt);
+    return true;
+  }
+
+  bool ensure_pins() {
+    if (pin[0]) return true;
+    for (int k = 0; k < 2; ++k) {
+      if (cudaMallocHost(&pin[k], CHUNK) != cudaSuccess ||
+          cudaEventCreateWithFlags(&pin_ev[k], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        fail(DCELL_ERR_NOMEM, "pinned staging of the writer");
+        return false;
+      }
+    }
+    return true;
   }
 
   void process(Job &j) {
-    const unsigned char *p = data(j);
-    if (!p) return;
     FILE *f = fopen(j.path.c_str(), "wb");
     if (!f) {
       fail(DCELL_ERR_ARG, "cannot open " + j.path + ": " + strerror(errno));
       return;
     }
     bool ok = true;
-    std::vector<double> tmp;
+    const size_t el = j.dtype == DCELL_F64 ? 8 : 4;
     if (j.kind == JOB_GRID) {
-      const double *v = (const double *)p;
-      if (j.dtype == DCELL_F32) {
-        tmp.resize((size_t)j.count);
-        for (long long i = 0; i < j.count; ++i) tmp[i] = ((const float *)p)[i];
-        v = tmp.data();
-      }
-      put_be32(f, VEC_FILE_CLASSID);
-      put_be32(f, (int32_t)j.count);
-      ok = put_be64(f, v, j.count);
+      unsigned char head[8];
+      be32(head, VEC_FILE_CLASSID);
+      be32(head + 4, (int32_t)j.count);
+      ok = fwrite(head, 1, 8, f) == 8;
+      ok = ok && drain(j, (size_t)j.count * el, [&](const unsigned char *p, size_t n) {
+             const size_t m = n / el;
+             out.resize(m * 8);
+             for (size_t i = 0; i < m; ++i) {
+               double v;
+               if (el == 8)
+                 memcpy(&v, p + 8 * i, 8);
+               else {
+                 float x;
+                 memcpy(&x, p + 4 * i, 4);
+                 v = x;
+               }
+               be64(out.data() + 8 * i, v);
+             }
+             return fwrite(out.data(), 1, out.size(), f) == out.size();
+           });
     } else if (j.kind == JOB_NODES) {
-      const dcell_irregular_node *nodes = (const dcell_irregular_node *)p;
-      int32_t cnt;
-      memcpy(&cnt, p + j.bytes - sizeof(int32_t), sizeof(int32_t));
-      const long long n = cnt < j.count ? cnt : j.count;
-      for (long long i = 0; i < n && ok; ++i) {
-        const dcell_irregular_node &q = nodes[i];
-        double row[23] = {0};
-        if (j.dim == 2) {
-          if (q.axis == -1) continue;
-          // X, pos, n, f1, fa1, k, f1_n, f1_nn (IrregularNodes.c:159-169)
-          row[0] = q.X[0], row[1] = q.X[1], row[2] = q.pos[0], row[3] = q.pos[1], row[4] = q.n[0], row[5] = q.n[1];
-          row[8] = q.k;
-          ok = put_be64(f, row, 11);
-        } else {
-          // X, pos, n, k, then the IIM quantities (IrregularNodes.c:190-212)
-          row[0] = q.X[0], row[1] = q.X[1], row[2] = q.X[2], row[3] = q.pos[0], row[4] = q.pos[1],
-          row[5] = q.pos[2], row[6] = q.n[0], row[7] = q.n[1], row[8] = q.n[2], row[9] = q.k;
-          ok = put_be64(f, row, 23);
-        }
-      }
+      int32_t cnt = 0;
+      ok = node_count(j, cnt);
+      const long long n = cnt < 0 ? 0 : (cnt < j.count ? cnt : j.count);
+      ok = ok && drain(j, (size_t)n * sizeof(dcell_irregular_node), [&](const unsigned char *p, size_t nb) {
+             const size_t m = nb / sizeof(dcell_irregular_node);
+             out.resize(m * 23 * 8);
+             size_t o = 0;
+             for (size_t i = 0; i < m; ++i) {
+               dcell_irregular_node q;
+               memcpy(&q, p + i * sizeof q, sizeof q);
+               double row[23] = {0};
+               int w = 23;
+               if (j.dim == 2) {
+                 if (q.axis == -1) continue;
+                 // X, pos, n, f1, fa1, k, f1_n, f1_nn (IrregularNodes.c:159-169)
+                 row[0] = q.X[0], row[1] = q.X[1], row[2] = q.pos[0], row[3] = q.pos[1], row[4] = q.n[0],
+                 row[5] = q.n[1], row[8] = q.k;
+                 w = 11;
+               } else {
+                 // X, pos, n, k, then the IIM quantities (IrregularNodes.c:190-212)
+                 row[0] = q.X[0], row[1] = q.X[1], row[2] = q.X[2], row[3] = q.pos[0], row[4] = q.pos[1],
+                 row[5] = q.pos[2], row[6] = q.n[0], row[7] = q.n[1], row[8] = q.n[2], row[9] = q.k;
+               }
+               for (int k = 0; k < w; ++k) be64(out.data() + o + 8 * k, row[k]);
+               o += 8 * w;
+             }
+             return fwrite(out.data(), 1, o, f) == o;
+           });
     } else {
-      const double *v = (const double *)p;
-      if (j.dtype == DCELL_F32) {
-        tmp.resize((size_t)j.count * 4);
-        for (long long i = 0; i < 4 * j.count; ++i) tmp[i] = ((const float *)p)[i];
-        v = tmp.data();
-      }
-      ok = fwrite(v, sizeof(double) * 4, (size_t)j.count, f) == (size_t)j.count;
+      ok = drain(j, (size_t)j.count * 4 * el, [&](const unsigned char *p, size_t n) {
+        if (el == 8) return fwrite(p, 1, n, f) == n;
+        const size_t m = n / 4;
+        out.resize(m * 8);
+        for (size_t i = 0; i < m; ++i) {
+          float x;
+          memcpy(&x, p + 4 * i, 4);
+          const double v = x;
+          memcpy(out.data() + 8 * i, &v, 8);
+        }
+        return fwrite(out.data(), 1, out.size(), f) == out.size();
+      });
     }
     ok = (fclose(f) == 0) && ok;
     if (!ok) {
       fail(DCELL_ERR_ARG, "writing " + j.path + " failed");
       return;
     }
-    if (!j.info.empty() || j.kind != JOB_PARTICLES) {
+    if (j.kind != JOB_PARTICLES) {  // PetscViewerBinaryOpen's .info companion
       FILE *fi = fopen((j.path + ".info").c_str(), "wb");
       if (!fi) {
         fail(DCELL_ERR_ARG, "cannot open " + j.path + ".info");
@@ -284,37 +314,55 @@ struct dcell_writer {
     if (cuda_ready) return DCELL_OK;
     DCELL_CUDA_CHECK(cudaSetDevice(device));
     DCELL_CUDA_CHECK(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    DCELL_CUDA_CHECK(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = UINT64_MAX;  // keep freed snapshots for reuse
+    DCELL_CUDA_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    const char *m = getenv("DCELL_WRITER_MAX_STAGED_MB");
+    if (m && atoll(m) > 0) max_staged = (size_t)atoll(m) << 20;
     cuda_ready = true;
     return DCELL_OK;
   }
 
-  // Snapshot `bytes` of device data (plus an optional trailing device int)
-  // and queue its copy to pinned memory.
+  // Snapshot `bytes` of device data (and an optional trailing device int32)
+  // on the caller's stream; waits first while the staged total would exceed
+  // the limit (the writer thread drains to disk).
   int stage_device(Job &j, const void *src, size_t bytes, const int *tail, cudaStream_t st) {
     int rc = ensure_cuda();
     if (rc) return rc;
     const size_t total = bytes + (tail ? sizeof(int32_t) : 0);
     j.bytes = total;
     {
-      std::lock_guard<std::mutex> g(pool_mu);
-      j.staging = dev_pool.take(total > 0 ? total : 1, j.staging_cap);
-      j.pinned = j.staging ? host_pool.take(total > 0 ? total : 1, j.pinned_cap) : nullptr;
+      std::unique_lock<std::mutex> g(mu);
+      idle.wait(g, [&] { return staged == 0 || staged + total <= max_staged; });
+      staged += total;
     }
-    if (!j.staging || !j.pinned) {
-      dcell_set_error(DCELL_ERR_NOMEM, "staging or pinned buffer of %zu bytes", total);
+    if (cudaMallocFromPoolAsync(&j.staging, total > 0 ? total : 1, pool, st) != cudaSuccess) {
+      cudaGetLastError();
+      std::lock_guard<std::mutex> g(mu);
+      staged -= total;
+      j.staging = nullptr;
+      dcell_set_error(DCELL_ERR_NOMEM, "snapshot of %zu bytes", total);
       return DCELL_ERR_NOMEM;
     }
-    cudaEvent_t snap;
-    DCELL_CUDA_CHECK(cudaEventCreateWithFlags(&snap, cudaEventDisableTiming));
-    DCELL_CUDA_CHECK(cudaEventCreateWithFlags(&j.done, cudaEventDisableTiming));
-    if (bytes) DCELL_CUDA_CHECK(cudaMemcpyAsync(j.staging, src, bytes, cudaMemcpyDeviceToDevice, st));
-    if (tail)
-      DCELL_CUDA_CHECK(cudaMemcpyAsync((char *)j.staging + bytes, tail, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-    DCELL_CUDA_CHECK(cudaEventRecord(snap, st));
-    DCELL_CUDA_CHECK(cudaStreamWaitEvent(copy, snap, 0));
-    DCELL_CUDA_CHECK(cudaMemcpyAsync(j.pinned, j.staging, total, cudaMemcpyDeviceToHost, copy));
-    DCELL_CUDA_CHECK(cudaEventRecord(j.done, copy));
-    cudaEventDestroy(snap);
+    cudaError_t e = cudaEventCreateWithFlags(&j.snap, cudaEventDisableTiming);
+    if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(j.staging, src, bytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && tail)
+      e = cudaMemcpyAsync((char *)j.staging + bytes, tail, sizeof(int32_t), cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(j.snap, st);
+    if (e != cudaSuccess) {
+      cudaFreeAsync(j.staging, st);
+      if (j.snap) cudaEventDestroy(j.snap);
+      j.snap = nullptr;
+      j.staging = nullptr;
+      std::lock_guard<std::mutex> g(mu);
+      staged -= total;
+      dcell_set_error(DCELL_ERR_CUDA, "snapshot for %s: %s", j.path.c_str(), cudaGetErrorString(e));
+      return DCELL_ERR_CUDA;
+    }
     return DCELL_OK;
   }
 };
@@ -426,9 +474,12 @@ DCELL_API int dcell_writer_destroy(dcell_writer *w) {
   if (w->cuda_ready) {
     cudaSetDevice(w->device);
     cudaStreamSynchronize(w->copy);
+    for (int k = 0; k < 2; ++k) {
+      if (w->pin[k]) cudaFreeHost(w->pin[k]);
+      if (w->pin_ev[k]) cudaEventDestroy(w->pin_ev[k]);
+    }
     cudaStreamDestroy(w->copy);
-    w->dev_pool.clear();
-    w->host_pool.clear();
+    cudaMemPoolDestroy(w->pool);
   }
   delete w;
   return rc;
@@ -440,10 +491,7 @@ DCELL_API int dcell_writer_grid(dcell_writer *w, const char *name, int t, const 
   if (rc) return rc;
   std::unique_ptr<Job> j = grid_job(w, name, t, g, dof, dtype);
   const size_t bytes = (size_t)j->count * (dtype == DCELL_F64 ? 8 : 4);
-  if ((rc = w->stage_device(*j, data, bytes, nullptr, (cudaStream_t)stream))) {
-    w->release(*j);
-    return rc;
-  }
+  if ((rc = w->stage_device(*j, data, bytes, nullptr, (cudaStream_t)stream))) return rc;
   return w->enqueue(std::move(j));
 }
 
@@ -470,10 +518,9 @@ DCELL_API int dcell_writer_irregular_nodes(dcell_writer *w, const char *name, in
   j->dim = dim;
   j->count = capacity;
   j->path = w->dir + "/" + name + ".irregNode." + std::to_string(idx + FILE_COUNT_START) + ".array";
-  if ((rc = w->stage_device(*j, nodes, (size_t)capacity * sizeof(dcell_irregular_node), count, (cudaStream_t)stream))) {
-    w->release(*j);
+  if ((rc = w->stage_device(*j, nodes, (size_t)capacity * sizeof(dcell_irregular_node), count,
+                            (cudaStream_t)stream)))
     return rc;
-  }
   return w->enqueue(std::move(j));
 }
 
@@ -513,10 +560,8 @@ DCELL_API int dcell_writer_particles(dcell_writer *w, const char *name, int t, c
   j->count = n;
   j->path = w->tmpdir + "/" + name + "." + std::to_string(t + FILE_COUNT_START) + ".array";
   if ((rc = w->stage_device(*j, particles, (size_t)n * 4 * (dtype == DCELL_F64 ? 8 : 4), nullptr,
-                            (cudaStream_t)stream))) {
-    w->release(*j);
+                            (cudaStream_t)stream)))
     return rc;
-  }
   return w->enqueue(std::move(j));
 }
 
