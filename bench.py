@@ -497,6 +497,9 @@ def main():
                                            "gpu_speedup": times["step_s"] * 1e3 / pr["ms_per_step"]}
             line["pls"] = pr
             del wl
+            # output in the reference's formats: the stream's cost of a 256^3 snapshot and the drain to disk
+            from dcell_b200.configs import run_io
+            line["io"] = run_io(args.size)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
