@@ -26,6 +26,8 @@ pls the particle level set at 256^3: ~3.5 M FP32 particles (32 per cell
     within 3 cells of a sphere of radius 0.15) in LeVeque's deformation field;
     per step RK2 particle advection, escaped-particle error correction and
     radius adjustment, timed on the device.
+reinit  narrow-band reinitialisation (bucketed fast marching) of the
+    workload sphere at 256^3 (cell units, band width 6), FP64 and FP32.
 io  output: phi of the 256^3 workload (FP32) written 10 times in the
     reference's .Real64 format by the asynchronous writer -- the time the
     compute stream spends on each snapshot, and the drain rate to disk.
@@ -293,6 +295,31 @@ def run_pls(N=256, steps=10, warmup=3, dev="cuda", workload=None):
             "how": "advect (RK2 midpoint) + error correction + adjust radii per step, CUDA events, phi held fixed"}
 
 
+def run_reinit(N=256, reps=5, dev="cuda"):
+    phi = (fields.sphere_sdf(N, device=dev) * N).contiguous()
+    band = fields.band_of(phi, 6.0, margin=3).to(dev)
+    raw, count = L.irregular_nodes(phi, 1.0, band, with_surface=False)
+    nn = int(count.item())
+    out = {"grid": [N] * 3, "seed_nodes": nn}
+    for name, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        x = phi.to(dt)
+        ms = []
+        for k in range(reps + 1):
+            y = x.clone()
+            e0, e1 = _events()
+            e0.record()
+            b = L.reinitialize(y, raw, nn, 6.0, 1.0 / 64)
+            e1.record()
+            torch.cuda.synchronize()
+            if k:
+                ms.append(e0.elapsed_time(e1))
+        ms.sort()
+        out[name + "_ms"] = ms[len(ms) // 2]
+        out["band_points"] = int(b.shape[0])
+    out["how"] = "dcell_reinitialize, CUDA events, median of %d" % reps
+    return out
+
+
 def run_io(N=256, writes=10, directory=None, dev="cuda"):
     import shutil
     import tempfile
@@ -382,6 +409,7 @@ def main():
         t0 = time.time()
         results[c] = (run_vel(a.grid or 512, a.cells) if c == "vel" else
                       run_pls(a.grid or 256) if c == "pls" else run_io(a.grid or 256) if c == "io" else
+                      run_reinit(a.grid or 256) if c == "reinit" else
                       globals()[f"run_{c}"]())
         results[c]["wall_s"] = time.time() - t0
         print(json.dumps({c: results[c]}, default=float), flush=True)
