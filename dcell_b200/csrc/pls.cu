@@ -104,6 +104,50 @@ __device__ __forceinline__ void vel_at(const Geom &g, const T *__restrict__ vel,
   }
 }
 
+// FP32 MAC velocity at X and whether every stencil lies in the grid: per
+// axis the cell and the half-staggered cell are floored once and shared by
+// the three components and the test (the values equal mac_vel_rel's).
+template <int DIM>
+__device__ __forceinline__ void vel_at_f32(const Geom &g, const float *__restrict__ vel, const float X[3], float V[3],
+                                           bool &inside) {
+  const int p[3] = {g.px, g.py, g.pz}, n[3] = {g.nx, g.ny, g.nz};
+  int i0[3] = {0, 0, 0}, i1[3] = {0, 0, 0};
+  float s0[3] = {0.f, 0.f, 0.f}, s1[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    const float xl = X[a] - (float)p[a], t1 = xl + 0.5f;
+    const float f0 = floorf(xl), f1 = floorf(t1);
+    i0[a] = (int)f0;
+    i1[a] = (int)f1;
+    s0[a] = xl - f0;
+    s1[a] = t1 - f1;
+    inside = inside && i0[a] >= 0 && i1[a] + 1 <= n[a] - 1;
+  }
+  const int pitch[3] = {DIM, DIM * g.nx, DIM * g.nx * g.ny};
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    int off = d, o[3] = {0, 0, 0};
+    float s[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      const int b = a == d ? i1[a] : i0[a];
+      const int bc = clampi(b, 0, n[a] - 1);
+      o[a] = (clampi(b + 1, 0, n[a] - 1) - bc) * pitch[a];
+      off += bc * pitch[a];
+      s[a] = a == d ? s1[a] : s0[a];
+    }
+    const float *c = vel + off;
+    if (DIM == 3) {
+      const float *c2 = c + o[2];
+      V[d] = trilerp(__ldg(c), __ldg(c + o[0]), __ldg(c + o[1]), __ldg(c + o[1] + o[0]), __ldg(c2), __ldg(c2 + o[0]),
+                     __ldg(c2 + o[1]), __ldg(c2 + o[1] + o[0]), s);
+    } else {
+      V[d] = bilerp(__ldg(c), __ldg(c + o[0]), __ldg(c + o[1]), __ldg(c + o[1] + o[0]), s[0], s[1]);
+    }
+  }
+  if (DIM == 2) V[2] = 0.f;
+}
+
 template <typename T, int DIM>
 __device__ __forceinline__ T phi_at(const Geom &g, const T *__restrict__ f, const T X[3]) {
   if constexpr (sizeof(T) == 4) {
@@ -166,13 +210,22 @@ __global__ void __launch_bounds__(256) pls_advect_kernel(Geom g, const T *__rest
   load4(parts, i, p);
   const T hx = (T)g.hx, hy = (T)g.hy, hz = (T)g.hz;
   T V1[3], V2[3], X[3];
-  bool inside = stencil_inside<T, DIM>(g, p);
-  vel_at<T, DIM>(g, vel, p, V1);
+  bool inside = true;
+  if constexpr (sizeof(T) == 4) {
+    vel_at_f32<DIM>(g, vel, p, V1, inside);
+  } else {
+    inside = stencil_inside<T, DIM>(g, p);
+    vel_at<T, DIM>(g, vel, p, V1);
+  }
   X[0] = p[0] + dt / T(2) * V1[0] / hx;
   X[1] = p[1] + dt / T(2) * V1[1] / hy;
   X[2] = DIM == 3 ? p[2] + dt / T(2) * V1[2] / hz : p[2];
-  inside = inside && stencil_inside<T, DIM>(g, X);
-  vel_at<T, DIM>(g, vel, X, V2);
+  if constexpr (sizeof(T) == 4) {
+    vel_at_f32<DIM>(g, vel, X, V2, inside);
+  } else {
+    inside = inside && stencil_inside<T, DIM>(g, X);
+    vel_at<T, DIM>(g, vel, X, V2);
+  }
   p[0] += dt * V2[0] / hx;
   p[1] += dt * V2[1] / hy;
   if (DIM == 3) p[2] += dt * V2[2] / hz;
