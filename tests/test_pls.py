@@ -348,3 +348,41 @@ def test_gpu_levelset_advect_pls_equals_reference(golden, cuda):
         assert np.array_equal(ls.phi.cpu().numpy(), ref.get_phi())
         assert abs(ls.CFLcount - ref.param("CFLcount")) <= 1e-12
     ref.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not R.available(), reason="oracle/_ref not built")
+def test_gpu_pls_rk2_half_full_equals_reference(golden, cuda):
+    """LevelSetAdvectPLSRK2HalfStep / FullStep (ParticleLS.c:333-375): the
+    particles restart from particles0 for the full step, SL from the same
+    phi0 -- FP64 bit for bit against the reference below the threshold."""
+    import torch
+
+    from dcell_b200 import levelset as L
+    from dcell_b200 import pls
+    g = _g(golden)
+    h, o = float(g["h2"]), tuple(int(v) for v in g["origin2"])
+    ny, nx = g["phi2"].shape
+    rng = np.random.default_rng(12)
+    vel_n = rng.uniform(-0.5, 0.5, (ny, nx, 2)) * h
+    vel_half = vel_n + rng.uniform(-0.05, 0.05, (ny, nx, 2)) * h
+    dt = 1.0
+    ref = R.RefLevelSet.create(h, o, (ny, nx))
+    ref.set_phi(g["phi2"])
+    ref.set_band(g["band2"])
+    ref.pls_init()
+    ls = L.LevelSetCreate((h, h, h), o + (0,), (nx, ny, 0), dtype=torch.float64, device=cuda)
+    ls.phi.copy_(_dev(g["phi2"], cuda))
+    ls.band = _dev(g["band2"].astype(np.int32), cuda)
+    pls.LevelSetInitializeParticles(ls)
+    ref.set_velocity(vel_n)
+    ref.pls_rk2_half(dt / 2)
+    pls.LevelSetAdvectPLSRK2HalfStep(ls, _dev(vel_n, cuda), dt / 2)
+    assert np.array_equal(ls.pls.live.cpu().numpy(), ref.particles())
+    assert np.array_equal(ls.phi.cpu().numpy(), ref.get_phi())
+    ref.set_velocity(vel_half)
+    ref.pls_rk2_full(dt)
+    pls.LevelSetAdvectPLSRK2FullStep(ls, _dev(vel_half, cuda), dt)
+    assert np.array_equal(ls.pls.live.cpu().numpy(), ref.particles())
+    assert np.array_equal(ls.phi.cpu().numpy(), ref.get_phi())
+    ref.close()
