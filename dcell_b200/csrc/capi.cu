@@ -419,7 +419,10 @@ struct DevBuf {
 struct dcell_session {
   int device = 0;
   cudaStream_t stream = nullptr;
-  DevBuf phi0_64, vel_64, phi_64, phi0_32, vel_32, phi_32, stage32, band, vals, nodes, scratch, small, parts;
+  cudaStream_t h2d = nullptr, d2h = nullptr;  // copy streams of the pipelined dense step
+  std::vector<cudaEvent_t> ev_in, ev_out;
+  DevBuf gates;
+  DevBuf phi0_64, vel_64, phi_64, phi0_32, vel_32, phi_32, stage32, band, vals, nodes, scratch, small, parts, split;
   std::vector<double> host_vals;
 };
 
@@ -488,11 +491,112 @@ DCELL_API int dcell_session_destroy(dcell_session *s) {
   cudaSetDevice(s->device);
   cudaStreamSynchronize(s->stream);
   for (DevBuf *b : {&s->phi0_64, &s->vel_64, &s->phi_64, &s->phi0_32, &s->vel_32, &s->phi_32, &s->stage32, &s->band, &s->vals,
-                    &s->nodes, &s->scratch, &s->small, &s->parts})
+                    &s->nodes, &s->scratch, &s->small, &s->parts, &s->split, &s->gates})
     b->release();
+  for (cudaEvent_t e : s->ev_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : s->ev_out) cudaEventDestroy(e);
+  if (s->h2d) cudaStreamDestroy(s->h2d);
+  if (s->d2h) cudaStreamDestroy(s->d2h);
   cudaStreamDestroy(s->stream);
   delete s;
   return DCELL_OK;
+}
+
+// The dense FP32 tensor-core step on host arrays, pipelined over z-slabs:
+// the inputs go up in plane chunks on one copy stream (converted to FP32 and
+// split on arrival), slab k is stepped once the planes up to its top + kHalo
+// are on the device, and its result comes down on a second copy stream while
+// later chunks still go up.  A slab launch runs only if max |w| dt / h_z over
+// the planes present is at most kHalo - 3 (every departure stencil then lies
+// in them); otherwise it leaves its slab, and once all inputs are present
+// the whole grid is stepped again and copied down (identical results either
+// way: the same kernel on the same inputs).
+static int ls_advect_tc_pipelined(dcell_session *s, const dcell_geom *g, const double *phi0, const double *vel,
+                                  double dt, int backtrace, double *phi) {
+  constexpr int kHalo = 6, kSlabs = 8;
+  const dcell::Geom G = dcell::to_geom(g);
+  const long long plane = (long long)G.nx * G.ny, n = plane * G.nz;
+  cudaStream_t st = s->stream;
+  if (!s->h2d) {
+    DCELL_CUDA_CHECK(cudaStreamCreateWithFlags(&s->h2d, cudaStreamNonBlocking));
+    DCELL_CUDA_CHECK(cudaStreamCreateWithFlags(&s->d2h, cudaStreamNonBlocking));
+  }
+  while ((int)s->ev_in.size() < kSlabs) {
+    cudaEvent_t a, b;
+    DCELL_CUDA_CHECK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    DCELL_CUDA_CHECK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    s->ev_in.push_back(a);
+    s->ev_out.push_back(b);
+  }
+  ENSURE(s->phi0_64, n * sizeof(double));
+  ENSURE(s->vel_64, n * 3 * sizeof(double));
+  ENSURE(s->phi_64, n * sizeof(double));
+  ENSURE(s->vel_32, n * 3 * sizeof(float));
+  ENSURE(s->phi0_32, n * sizeof(float));
+  ENSURE(s->phi_32, n * sizeof(float));
+  ENSURE(s->split, n * sizeof(uint32_t));
+  ENSURE(s->gates, kSlabs * sizeof(int));
+  int *dflags = (int *)s->small.p, *gates = (int *)s->gates.p;
+  double *p64 = (double *)s->phi0_64.p, *v64 = (double *)s->vel_64.p, *o64 = (double *)s->phi_64.p;
+  float *p32 = (float *)s->phi0_32.p, *v32 = (float *)s->vel_32.p, *o32 = (float *)s->phi_32.p;
+  uint32_t *w = (uint32_t *)s->split.p;
+  int rc;
+  // every stream starts after the work this session queued before
+  cudaEvent_t start = s->ev_out[kSlabs - 1];
+  DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
+  DCELL_CUDA_CHECK(cudaMemsetAsync(gates, 0, kSlabs * sizeof(int), st));
+  DCELL_CUDA_CHECK(cudaEventRecord(start, st));
+  DCELL_CUDA_CHECK(cudaStreamWaitEvent(s->h2d, start, 0));
+  const int BZ = tc_slab_planes();
+  const int nbz = (G.nz + BZ - 1) / BZ, per = (nbz + kSlabs - 1) / kSlabs;
+  int have = 0, nslab = 0;  // planes present on the device
+  for (int k = 0; k < kSlabs; ++k) {
+    const int b0 = k * per, b1 = b0 + per < nbz ? b0 + per : nbz;
+    if (b0 >= b1) break;
+    const int z0 = b0 * BZ, z1 = b1 * BZ < G.nz ? b1 * BZ : G.nz;
+    const int need = z1 + kHalo < G.nz ? z1 + kHalo : G.nz;
+    if (need > have) {  // the next chunk of planes: up, to FP32, split
+      const long long o = have * plane, m = (need - have) * plane;
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(p64 + o, phi0 + o, m * sizeof(double), cudaMemcpyHostToDevice, s->h2d));
+      DCELL_CUDA_CHECK(
+          cudaMemcpyAsync(v64 + 3 * o, vel + 3 * o, 3 * m * sizeof(double), cudaMemcpyHostToDevice, s->h2d));
+      if ((rc = launch_convert(p64 + o, DCELL_F64, p32 + o, DCELL_F32, m, s->h2d))) return rc;
+      if ((rc = launch_convert(v64 + 3 * o, DCELL_F64, v32 + 3 * o, DCELL_F32, 3 * m, s->h2d))) return rc;
+      if ((rc = launch_split_bf16(p32 + o, w + o, m, s->h2d))) return rc;
+      have = need;
+    }
+    DCELL_CUDA_CHECK(cudaEventRecord(s->ev_in[k], s->h2d));
+    DCELL_CUDA_CHECK(cudaStreamWaitEvent(st, s->ev_in[k], 0));
+    // the gate: max |w| over every plane present bounds the departures of this slab
+    if ((rc = launch_max_abs_component(v32, have * plane, 3, 2, gates + k, st))) return rc;
+    TcSlab slab;
+    slab.bz0 = b0;
+    slab.nbz = b1 - b0;
+    slab.gate_maxw = gates + k;
+    slab.gate_limit = (float)(kHalo - 3);
+    if ((rc = launch_sl_tc_slab(G, w, v32, dt, backtrace, o32, dflags, st, slab))) return rc;
+    const long long oz = z0 * plane, mz = (z1 - z0) * plane;
+    if ((rc = launch_convert(o32 + oz, DCELL_F32, o64 + oz, DCELL_F64, mz, st))) return rc;
+    DCELL_CUDA_CHECK(cudaEventRecord(s->ev_out[k], st));
+    DCELL_CUDA_CHECK(cudaStreamWaitEvent(s->d2h, s->ev_out[k], 0));
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(phi + oz, o64 + oz, mz * sizeof(double), cudaMemcpyDeviceToHost, s->d2h));
+    ++nslab;
+  }
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(s->h2d));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(s->d2h));
+  int hf = 0;
+  DCELL_CUDA_CHECK(cudaMemcpy(&hf, dflags, sizeof(int), cudaMemcpyDeviceToHost));
+  if (hf & dcell::FLAG_PIPELINE_REDO) {  // a slab was left: step the whole grid with every plane present
+    DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
+    if ((rc = launch_sl_tc_split(G, w, v32, dt, nullptr, n, backtrace, o32, nullptr, dflags, st))) return rc;
+    if ((rc = launch_convert(o32, DCELL_F32, o64, DCELL_F64, n, st))) return rc;
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(phi, o64, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(&hf, dflags, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+  (void)nslab;
+  return session_flags_status(s, hf & ~dcell::FLAG_PIPELINE_REDO);
 }
 
 DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const double *phi0, const double *vel,
@@ -509,6 +613,13 @@ DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const do
     if (rc) return rc;
   }
   DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  if (precision == DCELL_F32 && interp == DCELL_CUBIC_TC && !band && g->n[2] > 1) {
+    if (!(dt == dt)) FAIL(DCELL_ERR_NONFINITE, "dt is NaN");
+    if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+    const dcell::Geom G = dcell::to_geom(g);
+    if (G.nz >= 4 * tc_slab_planes() && tc_brick_applicable(G, (const void *)256, (const void *)256))
+      return ls_advect_tc_pipelined(s, g, phi0, vel, dt, backtrace, phi);
+  }
   const long long n = grid_points(g);
   const int dof = g->n[2] > 1 ? 3 : 2;
   const long long npts = band ? nband : n;
@@ -542,7 +653,18 @@ DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const do
     dphi = s->phi_64.p;
   }
   if (npts > 0) {
-    rc = dcell_sl_step(g, dtype, dphi0, dvel, dt, dband, band ? nband : 0, interp, backtrace, dphi, dflags, st);
+    const dcell::Geom G = dcell::to_geom(g);
+    if (precision == DCELL_F32 && interp == DCELL_CUBIC_TC && !band && G.nz > 1) {
+      // dense tensor-core step: split phi0 into packed BF16 words and run the
+      // split-state stepper (TMA bricks where the grid allows)
+      if (!(dt == dt)) FAIL(DCELL_ERR_NONFINITE, "dt is NaN");
+      ENSURE(s->split, n * sizeof(uint32_t));
+      if ((rc = launch_split_bf16((const float *)dphi0, (uint32_t *)s->split.p, n, st))) return rc;
+      rc = launch_sl_tc_split(G, (const uint32_t *)s->split.p, (const float *)dvel, dt, nullptr, n, backtrace,
+                              (float *)dphi, nullptr, dflags, st);
+    } else {
+      rc = dcell_sl_step(g, dtype, dphi0, dvel, dt, dband, band ? nband : 0, interp, backtrace, dphi, dflags, st);
+    }
     if (rc) return rc;
   }
   // results back: band values (gathered) or the whole grid

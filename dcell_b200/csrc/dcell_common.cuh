@@ -111,6 +111,7 @@ enum : int {
   FLAG_BAD_BAND = 16,          // a band entry lies outside the grid (skipped)
   FLAG_UNSETTLED = 32,         // reinitialisation: points still tentative after the last bucket
   FLAG_PARTICLE_OUTSIDE = 64,  // a particle's stencil or cell left the grid (clamped / skipped)
+  FLAG_PIPELINE_REDO = 128,    // internal: a gated z-slab launch left its slab to a full-grid step
 };
 
 __device__ __forceinline__ void raise_flag(int *flags, int bit) {

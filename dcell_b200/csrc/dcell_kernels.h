@@ -14,6 +14,18 @@ int launch_sl_tc(const dcell::Geom &g, const float *phi0, const float *vel, doub
                  long long npts, int backtrace, float *phi, int *flags, cudaStream_t st);
 
 int launch_split_bf16(const float *phi, uint32_t *out, long long n, cudaStream_t st);
+// One z-slab of the dense split-state tensor-core step: z bricks [bz0, bz0 +
+// nbz) of tc_slab_planes() planes each, gated on max |w| (FP32 bits at
+// gate_maxw) * dt / h_z <= gate_limit.
+struct TcSlab {
+  int bz0, nbz;
+  const int *gate_maxw;
+  float gate_limit;
+};
+int tc_slab_planes();
+bool tc_brick_applicable(const dcell::Geom &g, const void *phi0s, const void *vel);
+int launch_sl_tc_slab(const dcell::Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace,
+                      float *phi, int *flags, cudaStream_t st, const TcSlab &slab);
 int launch_sl_tc_split(const dcell::Geom &g, const uint32_t *phi0s, const float *vel, double dt, const int *band,
                        long long npts, int backtrace, float *phi, uint32_t *phis, int *flags, cudaStream_t st);
 int launch_batch_tc(const dcell_cell *cells, const dcell_tile *tiles, int ntiles, int tx, int ty, int ctas_per_sm,
@@ -47,6 +59,9 @@ int launch_velocity_box(const dcell::Geom &g, int dtype, const void *global, con
                         void *vel, cudaStream_t st);
 int launch_velocity_boxes(const dcell_box *boxes, int nboxes, int dim, int dtype, const void *global,
                           const int gdims[3], int gdof, int first, long long max_points, void *vel, cudaStream_t st);
+// max |v[comp]| over n points of a dof-component FP32 field, atomicMax'ed
+// into *out as FP32 bits (initialise *out to 0)
+int launch_max_abs_component(const float *v, long long n, int dof, int comp, int *out, cudaStream_t st);
 size_t reinit_scratch_bytes(long long n, int dtype);
 int launch_reinit(const dcell::Geom &g, int dtype, void *phi, const dcell_irregular_node *nodes, int nnodes, double bw,
                   double bucket, int *band, int cap, int *count, void *scratch, int *flags, cudaStream_t st);

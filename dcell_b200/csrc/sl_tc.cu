@@ -461,7 +461,8 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, in
 }
 
 struct BrickGrid {
-  int nbx, nby, nbz;
+  int nbx, nby, nbz;  // bricks of this launch per axis
+  int bz0;            // z brick index of the launch's first brick (z-slab launches)
 };
 
 template <int P>
@@ -491,7 +492,7 @@ struct BrickShape {
 // are z/y neighbours that share halo rows in L2.
 template <class S>
 __device__ __forceinline__ void brick_origin(const BrickGrid &bg, int b, int &x0, int &y0, int &z0) {
-  const int bz = b % bg.nbz, r = b / bg.nbz;
+  const int bz = bg.bz0 + b % bg.nbz, r = b / bg.nbz;
   z0 = bz * S::BZ;
   y0 = (r % bg.nby) * S::BY;
   x0 = (r / bg.nby) * S::BX;
@@ -709,8 +710,16 @@ template <int BT, int P, bool SPLIT>
 __global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
     sl_tc_brick_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel, Geom g,
                        BrickGrid bg, const uint32_t *__restrict__ phi0s, const float *__restrict__ vel, float dt,
-                       float *__restrict__ phi, uint32_t *__restrict__ phis, int *flags) {
+                       float *__restrict__ phi, uint32_t *__restrict__ phis, int *flags, const int *gate_maxw,
+                       float gate_limit) {
   using S = BrickShape<P>;
+  // z-slab launches: run only if the staged planes bound every departure
+  // (max |w| dt / h_z over them within gate_limit); otherwise leave the slab
+  // to a full-grid step once all planes are present
+  if (gate_maxw && __int_as_float(*gate_maxw) * (dt / (float)g.hz) > gate_limit) {
+    if (threadIdx.x == 0) raise_flag(flags, FLAG_PIPELINE_REDO);
+    return;
+  }
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t *sB = smem;
   uint8_t *const buf0 = smem + kBBytes, *const buf1 = smem + kBBytes + S::BufBytes;
@@ -1128,7 +1137,7 @@ bool tc_brick_applicable(const Geom &g, const void *phi0s, const void *vel) {
 
 template <int P>
 static int launch_brick(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
-                        uint32_t *phis, int *flags, cudaStream_t st) {
+                        uint32_t *phis, int *flags, cudaStream_t st, const TcSlab *slab) {
   using S = tc::BrickShape<P>;
   static bool configured = false;
   if (!configured) {
@@ -1154,6 +1163,11 @@ static int launch_brick(const Geom &g, const uint32_t *phi0s, const float *vel, 
   bg.nbx = (g.nx + S::BX - 1) / S::BX;
   bg.nby = (g.ny + S::BY - 1) / S::BY;
   bg.nbz = (g.nz + S::BZ - 1) / S::BZ;
+  bg.bz0 = 0;
+  if (slab) {  // z bricks [bz0, bz0 + nbz) only
+    bg.bz0 = slab->bz0;
+    bg.nbz = slab->nbz;
+  }
   const long long nbricks = (long long)bg.nbx * bg.nby * bg.nbz;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -1164,7 +1178,8 @@ static int launch_brick(const Geom &g, const uint32_t *phi0s, const float *vel, 
   auto kern = mid ? (split ? tc::sl_tc_brick_kernel<DCELL_MIDPOINT, P, true> : tc::sl_tc_brick_kernel<DCELL_MIDPOINT, P, false>)
                   : (split ? tc::sl_tc_brick_kernel<DCELL_EULER, P, true> : tc::sl_tc_brick_kernel<DCELL_EULER, P, false>);
   kern<<<(int)grid, tc::kBrickThreads, S::DynSmem, st>>>(tm_phi, tm_vel, g, bg, phi0s, vel, (float)dt, phi, phis,
-                                                          flags);
+                                                          flags, slab ? slab->gate_maxw : nullptr,
+                                                          slab ? slab->gate_limit : 0.f);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 
@@ -1180,8 +1195,15 @@ static int brick_points(const Geom &g) {
 
 int launch_sl_tc_brick(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
                        uint32_t *phis, int *flags, cudaStream_t st) {
-  if (brick_points(g) == 4) return launch_brick<4>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st);
-  return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st);
+  if (brick_points(g) == 4) return launch_brick<4>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st, nullptr);
+  return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st, nullptr);
+}
+
+int tc_slab_planes() { return tc::BrickShape<2>::BZ; }
+
+int launch_sl_tc_slab(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
+                      int *flags, cudaStream_t st, const TcSlab &slab) {
+  return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, nullptr, flags, st, &slab);
 }
 
 int launch_tc_gemm_check(const float *A, float *D, int *flags, cudaStream_t st) {

@@ -262,3 +262,23 @@ int launch_velocity_boxes(const dcell_box *boxes, int nboxes, int dim, int dtype
   }
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
+
+// max |v[c]| over n points of a dof-component field, as the bits of a
+// non-negative FP32 (monotone as integers) combined with atomicMax into *out
+__global__ void __launch_bounds__(256) max_abs_component_kernel(const float *__restrict__ v, long long n, int dof,
+                                                                int comp, int *out) {
+  float m = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = fmaxf(m, fabsf(__ldg(v + i * dof + comp)));
+#pragma unroll
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_int(m));
+}
+
+int launch_max_abs_component(const float *v, long long n, int dof, int comp, int *out, cudaStream_t st) {
+  if (n <= 0) return DCELL_OK;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148LL * 8) blocks = 148LL * 8;
+  max_abs_component_kernel<<<(int)blocks, 256, 0, st>>>(v, n, dof, comp, out);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}

@@ -265,3 +265,38 @@ def test_tc_brick_path_equals_gather_path(cuda, cfl_scale, shape, points, monkey
         torch.cuda.synchronize()
         assert torch.equal(dense, banded), float((dense - banded).abs().max())
         assert torch.equal(dspl, bspl)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("speed", [1.0, 40.0])
+def test_host_buffer_tc_step_pipelined_equals_device_step(cuda, speed):
+    """dcell_ls_advect_sl (FP32 tensor-core, dense) on host FP64 arrays is
+    stepped slab by slab while the inputs are still going up; its result
+    equals the device-resident split-state step bit for bit -- also when the
+    velocity is too fast for the staged halo (speed 40: every slab defers to
+    the full-grid step)."""
+    import ctypes
+
+    N, nz = 64, 96
+    h = 1.0 / N
+    ramp = torch.linspace(-0.3, 0.3, nz, device=cuda, dtype=torch.float64)[:, None, None].expand(nz, N, N)
+    phi = (ramp + torch.rand((nz, N, N), device=cuda, dtype=torch.float64) * 0.01).contiguous()
+    vel = (torch.rand((nz, N, N, 3), device=cuda, dtype=torch.float64) - 0.5) * speed
+    dt = 0.4 * h
+    want = L.sl_step_tc_split(L.split_bf16(phi.float().contiguous()), vel.float().contiguous(), dt, h,
+                              backtrace="midpoint")[0]
+    Lb = _lib.lib()
+    sess = ctypes.c_void_p()
+    _lib.check(Lb.dcell_session_create(0, ctypes.byref(sess)))
+    try:
+        p0 = phi.cpu().pin_memory()
+        v0 = vel.cpu().pin_memory()
+        out = torch.empty_like(p0).pin_memory()
+        g = _lib.geom(tuple(phi.shape), h)
+        for _ in range(2):  # twice: buffers and streams reused
+            _lib.check(Lb.dcell_ls_advect_sl(sess, ctypes.byref(g), ctypes.c_void_p(p0.data_ptr()),
+                                             ctypes.c_void_p(v0.data_ptr()), None, 0, dt, _lib.CUBIC_TC,
+                                             _lib.MIDPOINT, _lib.F32, ctypes.c_void_p(out.data_ptr())))
+            assert torch.equal(out.to(cuda), want.double())
+    finally:
+        Lb.dcell_session_destroy(sess)
