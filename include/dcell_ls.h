@@ -377,8 +377,12 @@ DCELL_API int dcell_session_destroy(dcell_session *s);
  * vel, ls->band = band and ls->phi->v1 = phi (updated in place at the band
  * points, or everywhere when band == NULL).  precision: DCELL_F64 computes in
  * FP64 (the reference's arithmetic, bit-identical for DCELL_LINEAR +
- * DCELL_EULER), DCELL_F32 in FP32.  Returns DCELL_ERR_DEPARTURE (after
- * writing the clamped result) if a departure point left the grid. */
+ * DCELL_EULER), DCELL_F32 in FP32.  DCELL_F32 + DCELL_CUBIC_TC on a dense 3D
+ * grid runs the split-state step (phi0 carried as BF16 hi + lo, 2^-17
+ * relative; dcell_sl_step_tc_split) pipelined with the copies: z-slabs are
+ * stepped while later planes are still going up and finished slabs come
+ * down.  Returns DCELL_ERR_DEPARTURE (after writing the clamped result) if a
+ * departure point left the grid. */
 DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const double *phi0, const double *vel, const int *band,
                        int nband, double dt, int interp, int backtrace, int precision, double *phi);
 
