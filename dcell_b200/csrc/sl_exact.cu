@@ -13,7 +13,9 @@
 //   surface_kernel       IIMUpdateSurfaceQuantities normal + curvature
 //   maxvel_kernel        LevelSet_MaxVelocity (Advect.c:70-111)
 //   volume kernels       smoothed-Heaviside volume, deterministic FP64 sum
+#include <cooperative_groups.h>
 #include <math.h>
+#include <stdlib.h>
 
 #include <mutex>
 
@@ -694,7 +696,7 @@ struct ReinitState {
 
 // list lengths of one side's march, in shared memory
 struct ReinitCounts {
-  int near[2], far[2], acc;
+  int near[2], far[2], acc[2];  // acc: ping-pong by bucket parity
 };
 
 template <typename T>
@@ -853,15 +855,22 @@ __global__ void __launch_bounds__(REINIT_MARCH_THREADS) reinit_march_kernel(Geom
                                                                           int nnodes, ReinitState s0, ReinitState s1,
                                                                           T bw, T inf, T bucket, int nb) {
   typedef typename OrdOf<T>::type O;
-  const int sign = blockIdx.x == 0 ? -1 : 1;
-  const ReinitState st = blockIdx.x == 0 ? s0 : s1;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();  // the CTAs of one side (a single CTA without clusters)
+  const int rank = (int)cl.block_rank(), nrank = (int)cl.num_blocks();
+  const int side = (int)blockIdx.x / nrank;
+  const int sign = side == 0 ? -1 : 1;
+  const ReinitState st = side == 0 ? s0 : s1;
   O *tent = (O *)st.tent;
-  __shared__ ReinitCounts c;
-  if (threadIdx.x == 0) c.near[0] = c.near[1] = c.far[0] = c.far[1] = c.acc = 0;
-  __syncthreads();
+  __shared__ ReinitCounts c_rank;
+  ReinitCounts &c = *cl.map_shared_rank(&c_rank, 0);  // the side's list lengths, in rank 0's shared memory
+  const int tid = rank * (int)blockDim.x + (int)threadIdx.x, nthr = nrank * (int)blockDim.x;
+  const bool lead = rank == 0 && threadIdx.x == 0;
+  if (lead) c.near[0] = c.near[1] = c.far[0] = c.far[1] = c.acc[0] = c.acc[1] = 0;
+  cl.sync();
   int in = 0, fcur = 0;
   T win = bucket * (T)REINIT_WINDOW;
-  for (int r = threadIdx.x; r < nnodes * 2 * DIM; r += blockDim.x) {  // FastMarching.c:72-84, one neighbour each
+  for (int r = tid; r < nnodes * 2 * DIM; r += nthr) {  // FastMarching.c:72-84, one neighbour each
     const dcell_irregular_node nd = nodes[r / (2 * DIM)];
     if (nd.axis != -1) continue;
     const int x = nd.pos[0] - g.px, y = nd.pos[1] - g.py, z = DIM == 3 ? nd.pos[2] - g.pz : 0;
@@ -869,19 +878,19 @@ __global__ void __launch_bounds__(REINIT_MARCH_THREADS) reinit_march_kernel(Geom
     if (sign * phi[(z * g.ny + y) * g.nx + x] >= 0)
       fmm_relax_dev<T, DIM>(g, phi, st, &c, in, fcur, x, y, z, r % (2 * DIM), sign, bw, inf, -(T)INFINITY, win);
   }
-  __syncthreads();
+  cl.sync();
   for (int b = 0; b < nb; ++b) {
     const T thr = bucket * (T)(b + 1);
     // accept what falls below this bucket's threshold; keep the rest of the window
     const int n_in = c.near[in];
-    for (int t = threadIdx.x; t < n_in; t += blockDim.x) {
+    for (int t = tid; t < n_in; t += nthr) {
       const int q = st.near[in][t];
       if (st.mark[q] == RM_MARCHED) continue;
       const T v = ord_value(tent[q]);
       if (v < thr && v <= bw) {
         if (atomicCAS(&st.mark[q], RM_TENT, RM_MARCHED) == RM_TENT) {
           phi[q] = sign * v;
-          st.acc[atomicAdd(&c.acc, 1)] = q;
+          st.acc[atomicAdd(&c.acc[b & 1], 1)] = q;
         }
       } else if (v <= bw) {
         st.near[in ^ 1][atomicAdd(&c.near[in ^ 1], 1)] = q;
@@ -889,24 +898,25 @@ __global__ void __launch_bounds__(REINIT_MARCH_THREADS) reinit_march_kernel(Geom
         st.mark[q] = RM_FAR;  // past the band unless a later push lowers it
       }
     }
-    __syncthreads();
-    const int n_acc = c.acc;
-    for (int t = threadIdx.x; t < n_acc * 2 * DIM; t += blockDim.x) {  // one (point, neighbour) pair each
+    cl.sync();
+    const int n_acc = c.acc[b & 1];
+    // nobody reads the consumed near list or the other parity's accept count
+    // again before the barrier after the relax pass: reset them meanwhile
+    if (lead) {
+      c.near[in] = 0;
+      c.acc[(b + 1) & 1] = 0;
+    }
+    for (int t = tid; t < n_acc * 2 * DIM; t += nthr) {  // one (point, neighbour) pair each
       const int q = st.acc[t / (2 * DIM)];
       const int x = q % g.nx, y = (q / g.nx) % g.ny, z = q / (g.nx * g.ny);
       fmm_relax_dev<T, DIM>(g, phi, st, &c, in ^ 1, fcur, x, y, z, t % (2 * DIM), sign, bw, inf, sign * phi[q], win);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      c.near[in] = 0;
-      c.acc = 0;
-    }
-    __syncthreads();
+    cl.sync();
     in ^= 1;
     if ((b + 1) % REINIT_WINDOW == 0) {  // the window moves on: far points now inside it join the near list
       win = bucket * (T)(b + 1 + REINIT_WINDOW);
       const int n_far = c.far[fcur];
-      for (int t = threadIdx.x; t < n_far; t += blockDim.x) {
+      for (int t = tid; t < n_far; t += nthr) {
         const int q = st.far[fcur][t];
         if (st.mark[q] == RM_MARCHED) continue;
         const T v = ord_value(tent[q]);
@@ -921,19 +931,21 @@ __global__ void __launch_bounds__(REINIT_MARCH_THREADS) reinit_march_kernel(Geom
           st.far[fcur ^ 1][atomicAdd(&c.far[fcur ^ 1], 1)] = q;
         }
       }
-      __syncthreads();
-      if (threadIdx.x == 0) c.far[fcur] = 0;
-      __syncthreads();
+      cl.sync();
+      // the consumed far list's length is read again only at the next
+      // redistribution, many barriers later
+      if (lead) c.far[fcur] = 0;
       fcur ^= 1;
     }
   }
   // still tentative (within the band) after the last bucket
   bool left = false;
-  for (int t = threadIdx.x; t < c.near[in]; t += blockDim.x)
+  for (int t = tid; t < c.near[in]; t += nthr)
     if (st.mark[st.near[in][t]] == RM_TENT && ord_value(tent[st.near[in][t]]) <= bw) left = true;
-  for (int t = threadIdx.x; t < c.far[fcur]; t += blockDim.x)
+  for (int t = tid; t < c.far[fcur]; t += nthr)
     if (st.mark[st.far[fcur][t]] == RM_TENT && ord_value(tent[st.far[fcur][t]]) <= bw) left = true;
   if (left) atomicOr(st.err, 2);
+  cl.sync();  // rank 0's shared counters stay alive until every CTA of the side is done with them
 }
 
 __global__ void __launch_bounds__(REINIT_THREADS) reinit_band_flags_kernel(const int *mark, long long n, int *flag) {
@@ -1078,6 +1090,18 @@ size_t reinit_scratch_bytes(long long n, int dtype) {
          align256(sizeof(int) * (nblk + 1));
 }
 
+// CTAs per side of the march (a thread-block cluster): 8, or
+// DCELL_REINIT_CLUSTER (1, 2, 4 or 8)
+static int reinit_cluster() {
+  static int cl = 0;
+  if (!cl) {
+    const char *e = getenv("DCELL_REINIT_CLUSTER");
+    const int v = e ? atoi(e) : 8;
+    cl = (v == 1 || v == 2 || v == 4 || v == 8) ? v : 8;
+  }
+  return cl;
+}
+
 template <typename T, int DIM>
 static void reinit_run(const Geom &g, T *phi, const dcell_irregular_node *nodes, int nnodes, T bw, T bucket,
                        int *band, int cap, int *count, uint8_t *sc, int *flags, cudaStream_t st) {
@@ -1105,8 +1129,28 @@ static void reinit_run(const Geom &g, T *phi, const dcell_irregular_node *nodes,
     reinit_seed_kernel<T, DIM><<<(nnodes + REINIT_THREADS - 1) / REINIT_THREADS, REINIT_THREADS, 0, st>>>(
         g, phi, nodes, nnodes, mark);
   const int nb = (int)ceil((double)bw / (double)bucket) + REINIT_TAIL;
-  reinit_march_kernel<T, DIM><<<2, REINIT_MARCH_THREADS, 0, st>>>(g, phi, nodes, nnodes, side[0], side[1], bw, inf,
-                                                                  bucket, nb);
+  // each side a cluster of reinit_cluster() CTAs; one CTA per side where
+  // clusters of that size cannot be scheduled
+  bool launched = false;
+  for (int cl = reinit_cluster(); cl > 1 && !launched; cl >>= 1) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * cl);
+    cfg.blockDim = dim3(REINIT_MARCH_THREADS);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    launched = cudaLaunchKernelEx(&cfg, reinit_march_kernel<T, DIM>, g, phi, nodes, nnodes, side[0], side[1], bw, inf,
+                                  bucket, nb) == cudaSuccess;
+    if (!launched) cudaGetLastError();
+  }
+  if (!launched)
+    reinit_march_kernel<T, DIM><<<2, REINIT_MARCH_THREADS, 0, st>>>(g, phi, nodes, nnodes, side[0], side[1], bw, inf,
+                                                                    bucket, nb);
   reinit_status_kernel<<<1, 1, 0, st>>>(err, flags);
   // band: the fixed points in grid order
   int *flag = side[0].near[0], *offs = side[0].near[0];
