@@ -500,6 +500,12 @@ def main():
             # output in the reference's formats: the stream's cost of a 256^3 snapshot and the drain to disk
             from dcell_b200.configs import run_io
             line["io"] = run_io(args.size)
+            # first-order upwind step on MAC faces (LevelSetAdvectMAC_3D), HBM-bound stencil
+            from dcell_b200.configs import run_mac
+            m = run_mac(args.size, dev=dev)
+            for k in ("fp32", "fp64"):
+                m[k]["frac"] = m[k]["achieved_gbs"] / hbm
+            line["advect_mac"] = m
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -108,6 +108,8 @@ def lib():
     L.dcell_ls_update_irregular_nodes.argtypes = [vp, G, vp, vp, i, i, i, vp, i, vp]
     L.dcell_ls_max_velocity.argtypes = [vp, G, vp, vp, i, vp]
     L.dcell_ls_reinitialize.argtypes = [vp, G, vp, vp, i, d, i, vp, i, vp]
+    L.dcell_advect_mac.argtypes = [G, i, vp, vp, vp, vp, d, vp, vp]
+    L.dcell_ls_advect_mac.argtypes = [vp, G, vp, vp, vp, vp, d, i, vp]
     L.dcell_tc_gemm_check.argtypes = [vp, vp, vp, vp]
     L.dcell_sl_adjoint.argtypes = [G, i, vp, vp, d, i, i, vp, vp, vp, vp]
     L.dcell_split_bf16.argtypes = [G, vp, vp, vp]
@@ -153,7 +155,8 @@ def lib():
                  "dcell_sl_adjoint", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",
                  "dcell_sl_step_tc_split", "dcell_pls_advect", "dcell_pls_correct", "dcell_pls_adjust_radii",
                  "dcell_pls_seed", "dcell_pls_reseed", "dcell_ls_pls_advect", "dcell_ls_pls_correct",
-                 "dcell_ls_pls_adjust_radii", "dcell_ls_pls_seed", "dcell_ls_pls_reseed"):
+                 "dcell_ls_pls_adjust_radii", "dcell_ls_pls_seed", "dcell_ls_pls_reseed", "dcell_advect_mac",
+                 "dcell_ls_advect_mac"):
         getattr(L, name).restype = i
     _LIB = L
     return L

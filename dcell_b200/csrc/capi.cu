@@ -328,6 +328,42 @@ DCELL_API int dcell_max_velocity(const dcell_geom *g, int dtype, const void *vel
   return launch_max_velocity(dcell::to_geom(g), dtype, vel, nodes, count, capacity, maxvel, (cudaStream_t)stream);
 }
 
+// Updated global range [s, e) of one axis of LevelSetAdvectMAC
+// (AdvectMAC.c:30-35, :68-74); false where the reference would read outside
+// its grid on that axis (a non-empty range with p > 0 or n < 3).
+static bool mac_axis(int p, int n, int *s, int *e) {
+  *s = p < 0 ? 0 : p;
+  *e = p + n - 1;
+  return !(*e > *s && (p > 0 || n < 3));
+}
+
+static int mac_ranges(const dcell_geom *g, int range[6]) {
+  bool ok = mac_axis(g->p[0], g->n[0], &range[0], &range[1]);
+  ok = mac_axis(g->p[1], g->n[1], &range[2], &range[3]) && ok;
+  range[4] = 0;
+  range[5] = 1;
+  if (g->n[2] > 1) ok = mac_axis(g->p[2], g->n[2], &range[4], &range[5]) && ok;
+  if (!ok)
+    FAIL(DCELL_ERR_UNSUPPORTED,
+         "LevelSetAdvectMAC reads outside its grid when an updated axis has origin > 0 or fewer than 3 points");
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_advect_mac(const dcell_geom *g, int dtype, const void *phi, const void *u, const void *v,
+                               const void *w, double dt, void *out, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  if (!phi || !u || !v || !out || (g->n[2] > 1 && !w)) FAIL(DCELL_ERR_ARG, "phi, u, v, (3D: w) and out are required");
+  if (out == phi) FAIL(DCELL_ERR_ARG, "out must not alias phi (the step reads phi's neighbours)");
+  if (!(dt == dt)) FAIL(DCELL_ERR_NONFINITE, "dt is NaN");
+  int range[6];
+  rc = mac_ranges(g, range);
+  if (rc) return rc;
+  return launch_advect_mac(dcell::to_geom(g), dtype, phi, u, v, g->n[2] > 1 ? w : nullptr, dt, range, out,
+                           (cudaStream_t)stream);
+}
+
 DCELL_API size_t dcell_volume_scratch_bytes(void) { return volume_scratch_bytes(); }
 
 DCELL_API int dcell_volume(const dcell_geom *g, int dtype, const void *phi, double eps, double *volume, void *scratch,
@@ -813,6 +849,53 @@ DCELL_API int dcell_ls_max_velocity(dcell_session *s, const dcell_geom *g, const
   rc = dcell_max_velocity(g, DCELL_F64, s->vel_64.p, (const dcell_irregular_node *)s->nodes.p, dcount, count, dmax, st);
   if (rc) return rc;
   DCELL_CUDA_CHECK(cudaMemcpyAsync(maxvel, dmax, sizeof(double), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_ls_advect_mac(dcell_session *s, const dcell_geom *g, const double *phi, const double *u,
+                                  const double *v, const double *w, double dt, int precision, double *out) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_geom(g);
+  if (rc) return rc;
+  const bool is3 = g->n[2] > 1;
+  if (!phi || !u || !v || !out || (is3 && !w)) FAIL(DCELL_ERR_ARG, "phi, u, v, (3D: w) and out are required");
+  if (precision != DCELL_F32 && precision != DCELL_F64) FAIL(DCELL_ERR_ARG, "precision must be DCELL_F32 or DCELL_F64");
+  int range[6];
+  rc = mac_ranges(g, range);
+  if (rc) return rc;
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long n = grid_points(g);
+  const size_t b64 = (size_t)n * sizeof(double);
+  const int ncomp = is3 ? 3 : 2;
+  ENSURE(s->phi_64, b64);
+  ENSURE(s->phi0_64, b64);
+  ENSURE(s->vel_64, b64 * ncomp);
+  double *dphi = (double *)s->phi_64.p, *dout = (double *)s->phi0_64.p, *dvel = (double *)s->vel_64.p;
+  const double *comp[3] = {u, v, w};
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(dphi, phi, b64, cudaMemcpyHostToDevice, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(dout, out, b64, cudaMemcpyHostToDevice, st));
+  for (int c = 0; c < ncomp; ++c)
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(dvel + c * n, comp[c], b64, cudaMemcpyHostToDevice, st));
+  if (precision == DCELL_F64) {
+    rc = dcell_advect_mac(g, DCELL_F64, dphi, dvel, dvel + n, is3 ? dvel + 2 * n : nullptr, dt, dout, st);
+    if (rc) return rc;
+  } else {  // FP32 arithmetic on converted copies
+    const size_t b32 = (size_t)n * sizeof(float);
+    ENSURE(s->phi_32, b32);
+    ENSURE(s->phi0_32, b32);
+    ENSURE(s->vel_32, b32 * ncomp);
+    float *fphi = (float *)s->phi_32.p, *fout = (float *)s->phi0_32.p, *fvel = (float *)s->vel_32.p;
+    if ((rc = launch_convert(dphi, DCELL_F64, fphi, DCELL_F32, n, st)) ||
+        (rc = launch_convert(dout, DCELL_F64, fout, DCELL_F32, n, st)) ||
+        (rc = launch_convert(dvel, DCELL_F64, fvel, DCELL_F32, n * ncomp, st)))
+      return rc;
+    rc = dcell_advect_mac(g, DCELL_F32, fphi, fvel, fvel + n, is3 ? fvel + 2 * n : nullptr, dt, fout, st);
+    if (rc) return rc;
+    if ((rc = launch_convert(fout, DCELL_F32, dout, DCELL_F64, n, st))) return rc;
+  }
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(out, dout, b64, cudaMemcpyDeviceToHost, st));
   DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
   return DCELL_OK;
 }

@@ -61,6 +61,9 @@ int launch_velocity_boxes(const dcell_box *boxes, int nboxes, int dim, int dtype
                           const int gdims[3], int gdof, int first, long long max_points, void *vel, cudaStream_t st);
 // max |v[comp]| over n points of a dof-component FP32 field, atomicMax'ed
 // into *out as FP32 bits (initialise *out to 0)
+// range: updated global index range [xs, xe, ys, ye, zs, ze) (2D: zs = 0, ze = 1)
+int launch_advect_mac(const dcell::Geom &g, int dtype, const void *phi, const void *u, const void *v, const void *w,
+                      double dt, const int range[6], void *out, cudaStream_t st);
 int launch_max_abs_component(const float *v, long long n, int dof, int comp, int *out, cudaStream_t st);
 size_t reinit_scratch_bytes(long long n, int dtype);
 int launch_reinit(const dcell::Geom &g, int dtype, void *phi, const dcell_irregular_node *nodes, int nnodes, double bw,

@@ -970,6 +970,73 @@ __global__ void reinit_status_kernel(const int *err, int *flags) {
   if (*err & 1) raise_flag(flags, FLAG_NONFINITE);
   if (*err & 2) raise_flag(flags, FLAG_UNSETTLED);
 }
+
+// ---------------------------------------------------------------------------
+// First-order conservative upwind step on MAC faces: LevelSetAdvectMAC and
+// LevelSetAdvectMAC_3D (LevelSetMethod/AdvectMAC.c:18-111), the reference's
+// expressions in its operation order (this unit is compiled without FMA
+// contraction, so FP64 gives its bits).  u / v / w hold at (i, j, k) the face
+// between cells i-1 and i along x / y / z.  At global index 0 and at the
+// range's last point the missing neighbour is extrapolated as
+// 2 phi - (the other neighbour) (AdvectMAC.c:83-88).  Every read stays in the
+// grid: the caller admits only updated ranges [s, e) with p <= 0 and n >= 3.
+//
+// A thread owns one (i, j) column and marches kMacChunk planes of the updated
+// z range upwards, carrying phi at k-1 and k and w at k in registers: per
+// point it loads phi's four x/y neighbours and plane k+1, u at i and i+1, v at
+// j and j+1 and w at k+1 (10 loads instead of 13), and the loads of the next
+// planes do not wait for this plane's arithmetic.  Bound: HBM (4 arrays read
+// and one written per point; the neighbour re-reads hit L1/L2).
+constexpr int kMacChunk = 8;
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 6)
+    advect_mac_kernel(Geom g, const T *__restrict__ phi, const T *__restrict__ u, const T *__restrict__ v,
+                      const T *__restrict__ w, T dt, int xs, int xe, int ys, int ye, int zs, int ze,
+                      T *__restrict__ out) {
+  const int i = xs + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= xe) return;
+  const T hx = (T)g.hx, hy = (T)g.hy, hz = (T)g.hz;
+  const int sy = g.nx, sz = g.nx * g.ny;
+  for (int j = ys + (int)(blockIdx.y * blockDim.y + threadIdx.y); j < ye; j += (int)(gridDim.y * blockDim.y))
+    for (int k0 = zs + (int)blockIdx.z * kMacChunk; k0 < ze; k0 += (int)gridDim.z * kMacChunk) {
+      const int k1 = min(k0 + kMacChunk, ze);
+      int c = (k0 - g.pz) * sz + (j - g.py) * sy + (i - g.px);
+      T p = __ldg(phi + c), below = T(0), w0 = T(0);
+      if (DIM == 3) {
+        below = k0 > g.pz ? __ldg(phi + c - sz) : T(0);  // read where k > 0 or k == ze-1: both imply k0 > p_z
+        w0 = __ldg(w + c);
+      }
+#pragma unroll(sizeof(T) == 4 ? 2 : 4)
+      for (int k = k0; k < k1; ++k, c += sz) {
+        const T am = i == 0 ? T(2) * p - __ldg(phi + c + 1) : __ldg(phi + c - 1);
+        const T an = i == xe - 1 ? T(2) * p - __ldg(phi + c - 1) : __ldg(phi + c + 1);
+        const T bm = j == 0 ? T(2) * p - __ldg(phi + c + sy) : __ldg(phi + c - sy);
+        const T bn = j == ye - 1 ? T(2) * p - __ldg(phi + c - sy) : __ldg(phi + c + sy);
+        const T u0 = __ldg(u + c), u1 = __ldg(u + c + 1);
+        const T v0 = __ldg(v + c), v1 = __ldg(v + c + sy);
+        T du = u0 > T(0) ? am * u0 : p * u0;
+        T dv = v0 > T(0) ? bm * v0 : p * v0;
+        du -= u1 > T(0) ? p * u1 : an * u1;
+        dv -= v1 > T(0) ? p * v1 : bn * v1;
+        if (DIM == 3) {
+          const T above = __ldg(phi + c + sz);  // plane k+1 <= e is in the grid
+          const T w1 = __ldg(w + c + sz);
+          const T cm = k == 0 ? T(2) * p - above : below;
+          const T cn = k == ze - 1 ? T(2) * p - below : above;
+          T dw = w0 > T(0) ? cm * w0 : p * w0;
+          dw -= w1 > T(0) ? p * w1 : cn * w1;
+          out[c] = p + dt * (du / hx + dv / hy + dw / hz);
+          below = p;
+          p = above;
+          w0 = w1;
+        } else {
+          out[c] = p + dt * (du / hx + dv / hy);
+        }
+      }
+    }
+}
+
 }  // namespace dcell
 
 // ===========================================================================
@@ -1074,6 +1141,29 @@ int launch_max_velocity(const Geom &g, int dtype, const void *vel, const dcell_i
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 
+
+int launch_advect_mac(const Geom &g, int dtype, const void *phi, const void *u, const void *v, const void *w, double dt,
+                      const int range[6], void *out, cudaStream_t st) {
+  const int X = range[1] - range[0], Y = range[3] - range[2], Z = range[5] - range[4];
+  if (X <= 0 || Y <= 0 || Z <= 0) return DCELL_OK;
+  const dim3 block(32, 8);
+  const dim3 grid((unsigned)((X + 31) / 32), (unsigned)min((Y + 7) / 8, 65535),
+                  (unsigned)min((Z + kMacChunk - 1) / kMacChunk, 65535));
+  const bool is2d = g.nz == 1;
+#define DCELL_MAC_LAUNCH(T, D)                                                                                    \
+  advect_mac_kernel<T, D><<<grid, block, 0, st>>>(g, (const T *)phi, (const T *)u, (const T *)v, (const T *)w,   \
+                                                  (T)dt, range[0], range[1], range[2], range[3], range[4], range[5], \
+                                                  (T *)out)
+  if (dtype == DCELL_F64) {
+    if (is2d) DCELL_MAC_LAUNCH(double, 2);
+    else DCELL_MAC_LAUNCH(double, 3);
+  } else {
+    if (is2d) DCELL_MAC_LAUNCH(float, 2);
+    else DCELL_MAC_LAUNCH(float, 3);
+  }
+#undef DCELL_MAC_LAUNCH
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
 
 // ---------------------------------------------------------------------------
 // Reinitialisation.  Scratch layout (bytes, each part 256-aligned): mark

@@ -21,6 +21,10 @@
  *   ParticleLS_ErrorCorrection2D/3D     (ParticleLS2D.c, ParticleLS3D.c; the
  *                                        reference's definitions are renamed
  *                                        away as above)
+ *   LevelSetAdvectMAC, _3D              (LevelSetMethod/AdvectMAC.c:18-111; that
+ *                                        file is not in the reference's build:
+ *                                        it reads ls->g, which the current
+ *                                        struct _LevelSet no longer has)
  * Everything that calls them -- LevelSetAdvectAndReinit, the RK2 half/full
  * steps (AdvectRK2.c), the particle and implicit variants, DCell's ls->Advect
  * slot -- is unchanged and now runs the GPU path.  Fast-marching
@@ -224,6 +228,79 @@ PetscErrorCode LevelSet_MaxVelocity(LevelSet ls, Grid velgrid) {
   free(buf);
   if (rc) SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_max_velocity: %s", dcell_last_error());
   PetscFunctionReturn(0);
+}
+
+/* LevelSetAdvectMAC / LevelSetAdvectMAC_3D (LevelSetMethod/AdvectMAC.c:
+ * 18-111): one first-order conservative upwind step on MAC faces.  The
+ * reference routines read the level set's grid as ls->g; with the current
+ * struct _LevelSet that grid is ls->phi, and out->phi (same geometry)
+ * receives the updated points.  u, v (, w) are the caller's global-index
+ * pointer tables (DAVecGetArray of the fluid's face velocities,
+ * FluidField/tests/testSource.c:72-84); exactly the face values the step
+ * reads are copied out of them. */
+PetscErrorCode LevelSetAdvectMAC(LevelSet ls, Coor d, PetscReal dt, PetscReal **u, PetscReal **v, LevelSet out);
+PetscErrorCode LevelSetAdvectMAC_3D(LevelSet ls, Coor d, PetscReal dt, PetscReal ***u, PetscReal ***v,
+                                    PetscReal ***w, LevelSet out);
+
+/* per axis: the global range [lo, hi] of a component's reads (the updated
+ * range [max(p,0), p+n-1), extended by one along the component's own axis) */
+static void b200_mac_reads(const dcell_geom *g, int comp, int lo[3], int hi[3]) {
+  int a;
+  for (a = 0; a < 3; ++a) {
+    const int p = g->p[a], n = a < 2 || g->n[2] > 1 ? g->n[a] : 1;
+    lo[a] = p < 0 ? 0 : p;
+    hi[a] = (a < 2 || g->n[2] > 1) ? p + n - 2 + (a == comp) : 0;
+  }
+}
+
+#undef __FUNCT__
+#define __FUNCT__ "LevelSetAdvectMAC"
+static PetscErrorCode b200_advect_mac(LevelSet ls, Coor d, PetscReal dt, PetscReal **u2, PetscReal **v2,
+                                      PetscReal ***u3, PetscReal ***v3, PetscReal ***w3, LevelSet out) {
+  dcell_session *s;
+  dcell_geom g;
+  double *buf;
+  size_t n;
+  int c, i, j, k, rc, lo[3], hi[3];
+  const int is3 = u3 != NULL;
+  PetscErrorCode ierr;
+
+  PetscFunctionBegin;
+  ierr = LevelSetB200Session(&s); CHKERRQ(ierr);
+  if (out->phi->SIZE != ls->phi->SIZE || out->phi->p.x != ls->phi->p.x || out->phi->p.y != ls->phi->p.y ||
+      out->phi->p.z != ls->phi->p.z)
+    SETERRQ(PETSC_COMM_SELF, PETSC_ERR_ARG_OUTOFRANGE, "the output level set's grid differs from the input's");
+  b200_geom(ls->phi, &g);
+  g.h[0] = d.x;
+  g.h[1] = d.y;
+  g.h[2] = d.z;
+  n = (size_t)ls->phi->SIZE;
+  buf = (double *)calloc(n * (is3 ? 3 : 2), sizeof(double));
+  if (!buf) SETERRQ(PETSC_COMM_SELF, PETSC_ERR_MEM, "out of host memory");
+  for (c = 0; c < (is3 ? 3 : 2); ++c) {
+    double *dst = buf + (size_t)c * n;
+    b200_mac_reads(&g, c, lo, hi);
+    for (k = lo[2]; k <= hi[2]; ++k)
+      for (j = lo[1]; j <= hi[1]; ++j)
+        for (i = lo[0]; i <= hi[0]; ++i) {
+          const size_t at = ((size_t)(k - g.p[2]) * g.n[1] + (size_t)(j - g.p[1])) * g.n[0] + (size_t)(i - g.p[0]);
+          dst[at] = is3 ? (c == 0 ? u3 : c == 1 ? v3 : w3)[k][j][i] : (c == 0 ? u2 : v2)[j][i];
+        }
+  }
+  rc = dcell_ls_advect_mac(s, &g, ls->phi->v1, buf, buf + n, is3 ? buf + 2 * n : NULL, dt, b200_precision,
+                           out->phi->v1);
+  free(buf);
+  if (rc) SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_advect_mac: %s", dcell_last_error());
+  PetscFunctionReturn(0);
+}
+
+PetscErrorCode LevelSetAdvectMAC(LevelSet ls, Coor d, PetscReal dt, PetscReal **u, PetscReal **v, LevelSet out) {
+  return b200_advect_mac(ls, d, dt, u, v, NULL, NULL, NULL, out);
+}
+
+PetscErrorCode LevelSetAdvectMAC_3D(LevelSet ls, Coor d, PetscReal dt, PetscReal ***u, PetscReal ***v,
+                                    PetscReal ***w, LevelSet out) {
+  return b200_advect_mac(ls, d, dt, NULL, NULL, u, v, w, out);
 }
 
 /* The reference's own LevelSetReinitialize, renamed at link time. */

@@ -251,6 +251,32 @@ def volume(phi: torch.Tensor, h, eps: float):
     return out
 
 
+def advect_mac(phi: torch.Tensor, u: torch.Tensor, v: torch.Tensor, w: Optional[torch.Tensor], dt: float, h,
+               origin=(0, 0, 0), out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """One first-order conservative upwind step on MAC faces
+    (LevelSetAdvectMAC / LevelSetAdvectMAC_3D, LevelSetMethod/AdvectMAC.c:
+    18-111): phi, u, v (, w in 3D) share the grid at global `origin`; u[k, j,
+    i] is the face between cells i-1 and i.  Writes the updated range
+    [max(p, 0), p + n - 1) of each axis into `out` (default: a copy of phi,
+    so the other points keep phi's values) and returns it."""
+    is3 = phi.dim() == 3
+    ts = (phi, u, v, w) if is3 else (phi, u, v)
+    _require_cuda(*ts)
+    for t in ts[1:]:
+        if t.shape != phi.shape or t.dtype != phi.dtype or not t.is_contiguous():
+            raise ValueError("u, v (, w) must be contiguous, with phi's shape and dtype")
+    if not phi.is_contiguous():
+        raise ValueError("phi must be contiguous")
+    if out is None:
+        out = phi.clone()
+    elif out.shape != phi.shape or out.dtype != phi.dtype or not out.is_contiguous():
+        raise ValueError("out must be contiguous, with phi's shape and dtype")
+    g = geom(phi.shape, h, origin)
+    check(lib().dcell_advect_mac(ctypes.byref(g), _dtype_code(phi), _ptr(phi), _ptr(u), _ptr(v),
+                                 _ptr(w) if is3 else None, float(dt), _ptr(out), _stream()))
+    return out
+
+
 # ---------------------------------------------------------------------------
 # LevelSet object and the reference-named entry points
 @dataclass
@@ -354,6 +380,18 @@ def LevelSetAdvectAndReinit(ls: LevelSet, velgrid: torch.Tensor, dt: float):
             raise DcellError(_lib.ERR_UNSUPPORTED, "reinitialisation threshold reached but no Reinitialize hook is "
                              "set (fast marching stays the reference's CPU LevelSetReinitialize)")
         ls.Reinitialize(ls)
+
+
+def LevelSetAdvectMAC(ls: LevelSet, d, dt: float, u: torch.Tensor, v: torch.Tensor, new: LevelSet):
+    """LevelSetAdvectMAC (AdvectMAC.c:18-60): one upwind step of ls.phi into
+    new.phi on the MAC faces u, v of ls's grid (d: the spacing)."""
+    advect_mac(ls.phi, u, v, None, dt, d, ls.origin, out=new.phi)
+
+
+def LevelSetAdvectMAC_3D(ls: LevelSet, d, dt: float, u: torch.Tensor, v: torch.Tensor, w: torch.Tensor,
+                         new: LevelSet):
+    """LevelSetAdvectMAC_3D (AdvectMAC.c:62-111)."""
+    advect_mac(ls.phi, u, v, w, dt, d, ls.origin, out=new.phi)
 
 
 def LevelSetReinitializeGPU(ls: LevelSet, bucket: float = 1.0 / 64):

@@ -364,6 +364,24 @@ DCELL_API int dcell_batch_sl_step(const dcell_cell *cells, int ncells, const dce
                                   int ty, int tz, int ctas_per_sm, const float *phi0, const float *vel, float *phi,
                                   int interp, int backtrace, int *flags, void *stream);
 
+/* One explicit first-order conservative upwind step of phi on MAC faces:
+ * LevelSetAdvectMAC (2D) / LevelSetAdvectMAC_3D, LevelSetMethod/AdvectMAC.c:
+ * 18-111 (replaces them; the reference routines read the level set's grid
+ * through members the current struct _LevelSet no longer has).  phi, u, v,
+ * w (3D only; NULL in 2D) and out are device arrays on the grid g, x
+ * fastest; u at (i, j, k) is the face between cells i-1 and i (v, w likewise
+ * along y, z).  Per axis the updated global range is [max(p, 0), p + n - 1);
+ * at global index 0 and at the range's last point the missing neighbour is
+ * extrapolated as 2 phi - (the other neighbour), and
+ *   out = phi + dt (du / h.x + dv / h.y (+ dw / h.z))
+ * with each face's upwind product.  Points outside the ranges are not
+ * written (the reference leaves its output level set's other values); out
+ * must not alias phi.  The reference reads outside its grid when an updated
+ * axis has p > 0 or n < 3: such grids return DCELL_ERR_UNSUPPORTED and
+ * nothing is written.  DCELL_F64 gives the reference's bits. */
+DCELL_API int dcell_advect_mac(const dcell_geom *g, int dtype, const void *phi, const void *u, const void *v,
+                               const void *w, double dt, void *out, void *stream);
+
 /* ------------------------------------------------------------------------
  * Host-buffer drop-in entry points (reference FP64 layout)
  * ---------------------------------------------------------------------- */
@@ -399,6 +417,13 @@ DCELL_API int dcell_ls_update_irregular_nodes(dcell_session *s, const dcell_geom
  * precision: the arithmetic, DCELL_F64 or DCELL_F32. */
 DCELL_API int dcell_ls_reinitialize(dcell_session *s, const dcell_geom *g, double *phi, const dcell_irregular_node *nodes,
                                     int nnodes, double band_width, int precision, int *band, int capacity, int *count);
+
+/* LevelSetAdvectMAC / LevelSetAdvectMAC_3D on host FP64 arrays (see
+ * dcell_advect_mac; w is NULL in 2D): out is read and updated in place at the
+ * updated points.  precision: the arithmetic, DCELL_F64 (the reference's
+ * bits) or DCELL_F32. */
+DCELL_API int dcell_ls_advect_mac(dcell_session *s, const dcell_geom *g, const double *phi, const double *u,
+                                  const double *v, const double *w, double dt, int precision, double *out);
 
 /* LevelSet_MaxVelocity(ls, velgrid) on host arrays. */
 DCELL_API int dcell_ls_max_velocity(dcell_session *s, const dcell_geom *g, const double *vel,

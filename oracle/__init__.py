@@ -80,6 +80,7 @@ def lib():
         L.orc_pls_init.argtypes = [vp, vp, vp, l, vp, vp, vp, l]
         L.orc_pls_init.restype = l
         L.orc_pls_reseed.argtypes = [vp, vp, vp, l, vp, vp, vp, l, l, vp]
+        L.orc_advect_mac.argtypes = [vp, vp, vp, vp, vp, d, vp]
         L.orc_pls_reseed.restype = l
         _LIB = L
     return _LIB
@@ -336,3 +337,22 @@ def pls_reseed(phi, band, parts, rng, h=1.0, origin=(0, 0, 0), params=None):
     if n < 0:
         raise ValueError("particle reseeding is 2D")
     return P[:n].copy(), st.value, miss.value
+
+
+# ---------------------------------------------------------------------------
+# first-order conservative upwind step on MAC faces (LevelSetMethod/AdvectMAC.c)
+
+def advect_mac(phi, u, v, w, dt, h, origin=(0, 0, 0), out=None):
+    """LevelSetAdvectMAC (2D, phi (ny, nx)) / LevelSetAdvectMAC_3D (phi
+    (nz, ny, nx)), AdvectMAC.c:18-111: phi, u, v (, w) share one grid at
+    global `origin`; returns a copy of `out` (default phi) with the updated
+    points replaced, or None where the reference would read outside its grid
+    (an axis with a non-empty range and origin > 0 or extent < 3)."""
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64) if phi.ndim == 3 else None
+    res = (phi if out is None else np.asarray(out, dtype=np.float64)).copy()
+    g = geom(phi.shape, h, origin)
+    rc = lib().orc_advect_mac(ctypes.byref(g), _ptr(phi), _ptr(u), _ptr(v), _ptr(w), float(dt), _ptr(res))
+    return None if rc else res

@@ -75,6 +75,8 @@ def lib(path=PATH):
         L.dref_rand48_get.restype = None
         L.dref_rand48_set.argtypes = [vp]
         L.dref_rand48_set.restype = None
+        if hasattr(L, "dref_advect_mac"):  # the reference-only library (shim/mac)
+            L.dref_advect_mac.argtypes = [vp, vp, vp, vp, vp, vp, vp, d, vp]
         _LIBS[path] = L
     return _LIBS[path]
 
@@ -314,3 +316,25 @@ def ortho2d(phi3, phi5):
     op = np.zeros(3)
     lib().dref_ortho2d(_p(a3), _p(a5), _p(op))
     return op
+
+
+def advect_mac(phi, u, v, w, dt, h, origin=(0, 0, 0), out=None):
+    """The reference's LevelSetAdvectMAC (2D, phi (ny, nx)) or
+    LevelSetAdvectMAC_3D (phi (nz, ny, nx)), LevelSetMethod/AdvectMAC.c:18-111,
+    compiled from its own source: phi, u, v (, w) share the grid at global
+    `origin` (x, y(, z)); returns a copy of `out` (default phi) with the
+    updated points replaced.  Call only on grids where the routine stays in
+    bounds (oracle.advect_mac returns None for the others)."""
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (u, v)]
+    arrs.append(np.ascontiguousarray(w, dtype=np.float64) if phi.ndim == 3 else np.zeros(1))
+    res = (phi if out is None else np.asarray(out, dtype=np.float64)).copy()
+    shape = phi.shape if phi.ndim == 3 else (1,) + phi.shape
+    n = np.array([shape[2], shape[1], shape[0]], dtype=np.int32)
+    o = tuple(int(x) for x in origin) + (0,) * (3 - len(origin))
+    pp = np.array([o[0], o[1], o[2] if phi.ndim == 3 else 0], dtype=np.int32)
+    hh = np.broadcast_to(np.asarray(h, dtype=np.float64), (3,)).copy()
+    rc = lib().dref_advect_mac(_p(n), _p(pp), _p(hh), _p(phi), _p(arrs[0]), _p(arrs[1]), _p(arrs[2]), float(dt),
+                               _p(res))
+    assert rc == 0
+    return res

@@ -1248,3 +1248,65 @@ ORC_EXPORT long orc_pls_reseed(const orc_geom *g, const double *phi, const int *
   free(count);
   return cnt;
 }
+
+/* ------------------------------------------------------------------------
+ * First-order conservative upwind step on MAC faces: LevelSetAdvectMAC
+ * (2D) and LevelSetAdvectMAC_3D, LevelSetMethod/AdvectMAC.c:18-111.
+ *
+ * phi, u, v (, w) and out share the grid g; u[i] is the face between cells
+ * i-1 and i (v, w likewise along y, z).  Per axis the updated global range is
+ * [max(p, 0), p + n - 1) (AdvectMAC.c:30-35, :68-74); at global index 0 and
+ * at the range's last point the missing neighbour is extrapolated as
+ * 2 phi - (the other neighbour) (:45-48, :83-88).  Each face contributes the
+ * upwind product (:50-53, :90-95) and
+ *   out = phi + dt * (du / h.x + dv / h.y (+ dw / h.z))    (:55, :97).
+ * Points outside the ranges keep their value in out.  The reference reads
+ * outside its grid when an axis with a non-empty range has p > 0 or n < 3;
+ * those grids return 7 (nothing written).  Returns 0 otherwise.
+ * ---------------------------------------------------------------------- */
+static inline double mac_at(const orc_geom *g, const double *a, int i, int j, int k) {
+  return a[((size_t)(k - g->pz) * g->ny + (size_t)(j - g->py)) * g->nx + (size_t)(i - g->px)];
+}
+
+static int mac_range(int p, int n, int *s, int *e) {
+  *s = p < 0 ? 0 : p;
+  *e = p + n - 1;
+  return *e > *s && (p > 0 || n < 3);
+}
+
+ORC_EXPORT int orc_advect_mac(const orc_geom *g, const double *phi, const double *u, const double *v,
+                              const double *w, double dt, double *out) {
+  const int is3 = g->nz > 1;
+  int xs, xe, ys, ye, zs = 0, ze = 1;
+  int bad = mac_range(g->px, g->nx, &xs, &xe) | mac_range(g->py, g->ny, &ys, &ye);
+  if (is3) bad |= mac_range(g->pz, g->nz, &zs, &ze);
+  if (bad) return 7;
+  for (int k = zs; k < ze; ++k)
+    for (int j = ys; j < ye; ++j)
+      for (int i = xs; i < xe; ++i) {
+        const double p = mac_at(g, phi, i, j, k);
+        const double am = i == 0 ? 2 * p - mac_at(g, phi, i + 1, j, k) : mac_at(g, phi, i - 1, j, k);
+        const double an = i == xe - 1 ? 2 * p - mac_at(g, phi, i - 1, j, k) : mac_at(g, phi, i + 1, j, k);
+        const double bm = j == 0 ? 2 * p - mac_at(g, phi, i, j + 1, k) : mac_at(g, phi, i, j - 1, k);
+        const double bn = j == ye - 1 ? 2 * p - mac_at(g, phi, i, j - 1, k) : mac_at(g, phi, i, j + 1, k);
+        const double u0 = mac_at(g, u, i, j, k), u1 = mac_at(g, u, i + 1, j, k);
+        const double v0 = mac_at(g, v, i, j, k), v1 = mac_at(g, v, i, j + 1, k);
+        double du = u0 > 0. ? am * u0 : p * u0;
+        double dv = v0 > 0. ? bm * v0 : p * v0;
+        du -= u1 > 0. ? p * u1 : an * u1;
+        dv -= v1 > 0. ? p * v1 : bn * v1;
+        double r;
+        if (is3) {
+          const double cm = k == 0 ? 2 * p - mac_at(g, phi, i, j, k + 1) : mac_at(g, phi, i, j, k - 1);
+          const double cn = k == ze - 1 ? 2 * p - mac_at(g, phi, i, j, k - 1) : mac_at(g, phi, i, j, k + 1);
+          const double w0 = mac_at(g, w, i, j, k), w1 = mac_at(g, w, i, j, k + 1);
+          double dw = w0 > 0. ? cm * w0 : p * w0;
+          dw -= w1 > 0. ? p * w1 : cn * w1;
+          r = p + dt * (du / g->hx + dv / g->hy + dw / g->hz);
+        } else {
+          r = p + dt * (du / g->hx + dv / g->hy);
+        }
+        out[((size_t)(k - g->pz) * g->ny + (size_t)(j - g->py)) * g->nx + (size_t)(i - g->px)] = r;
+      }
+  return 0;
+}

@@ -10,6 +10,7 @@ exactly), so FP32 and FP64 kernels see the very same data the FP64
 reference saw.
 
     python tests/golden/make_golden.py        # needs oracle/_ref/libdcell_ref.so
+    python tests/golden/make_golden.py mac    # only mac.npz
 """
 from __future__ import annotations
 
@@ -184,8 +185,43 @@ def run_pls3d():
                 dt3=dt, adv3=adv, corr_idx3=corr, corr_val3=phi_corr, adj_radius3=adj[:, 3])
 
 
-def main():
+MAC_CASES = [  # (shape (z, y, x) or (y, x), global origin x, y(, z), spacing)
+    ((11, 13, 17), (0, 0, 0), (0.05, 0.04, 0.03)),
+    ((9, 12, 10), (-3, -1, -4), (0.05, 0.05, 0.05)),
+    ((3, 3, 3), (0, 0, 0), (0.1, 0.2, 0.3)),
+    ((23, 19), (0, 0), (0.02, 0.03, 1.0)),
+    ((15, 21), (-5, -2), (0.04, 0.04, 1.0)),
+]
+
+
+def run_mac():
+    """LevelSetAdvectMAC / _3D (LevelSetMethod/AdvectMAC.c:18-111), compiled
+    from its own source against oracle/shim/mac: random phi, random face
+    velocities of both signs (with exact zeros), out pre-filled with other
+    values so untouched points are visible; dt chosen per case."""
+    rng = np.random.default_rng(31)
+    res = {}
+    for c, (shape, origin, h) in enumerate(MAC_CASES):
+        phi = f32(rng.uniform(-1.0, 1.0, size=shape))
+        comps = [f32(rng.uniform(-2.0, 2.0, size=shape) * (rng.random(shape) > 0.1)) for _ in range(len(shape))]
+        out0 = f32(rng.uniform(5.0, 6.0, size=shape))
+        dt = f32(0.3 * min(h[:len(shape)]))
+        w = comps[2] if len(shape) == 3 else None
+        out = R.advect_mac(phi, comps[0], comps[1], w, dt, h, origin, out=out0)
+        res.update({f"phi_{c}": phi.astype(np.float32), f"out0_{c}": out0.astype(np.float32), f"out_{c}": out,
+                    f"origin_{c}": np.array(origin), f"h_{c}": np.array(h), f"dt_{c}": dt,
+                    **{f"vel{a}_{c}": comps[a].astype(np.float32) for a in range(len(shape))}})
+    res["ncases"] = len(MAC_CASES)
+    return res
+
+
+def main(only=None):
     assert R.available(), "build oracle/_ref first: make -C oracle ref"
+    if only == "mac":
+        np.savez_compressed(os.path.join(OUT, "mac.npz"), **run_mac())
+        print("mac.npz written to", OUT)
+        return
+    np.savez_compressed(os.path.join(OUT, "mac.npz"), **run_mac())
     # fast-marching reinitialisation: a sphere and a circle as the reference's
     # own initialisers build them (off-grid centres, no symmetric ties)
     r3 = run_reinit(R.RefLevelSet.sphere(1.0 / 20, (0.4512, 0.3371, 0.5618), 0.2))
@@ -277,4 +313,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else None)  # "mac": that fixture only
