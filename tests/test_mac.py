@@ -85,6 +85,32 @@ def test_oracle_known_answer_uniform_flow():
     assert (out[nz - 1] == 9.0).all() and (out[:, ny - 1] == 9.0).all() and (out[:, :, nx - 1] == 9.0).all()
 
 
+def test_c_abi_argument_errors():
+    """dcell_advect_mac / dcell_ls_advect_mac reject bad arguments with status
+    codes before any device work (runs without a GPU)."""
+    from dcell_b200 import _lib
+    L = _lib.lib()
+    d = ctypes.c_void_p(64)  # never dereferenced: every call below fails or has nothing to do first
+    e = ctypes.c_void_p(128)
+    g3 = _lib.geom((6, 6, 6), 0.1)
+    g2 = _lib.geom((6, 6), 0.1)
+
+    def rc(g, dtype=_lib.F64, phi=d, u=d, v=d, w=d, dt=0.1, out=e):
+        return L.dcell_advect_mac(ctypes.byref(g) if g is not None else None, dtype, phi, u, v, w, dt, out, None)
+    assert rc(None) == _lib.ERR_ARG
+    assert rc(g3, dtype=7) == _lib.ERR_ARG
+    assert rc(g3, phi=None) == _lib.ERR_ARG
+    assert rc(g3, w=None) == _lib.ERR_ARG           # 3D needs w
+    assert rc(g3, out=d) == _lib.ERR_ARG            # out aliases phi
+    assert rc(g3, dt=float("nan")) == _lib.ERR_NONFINITE
+    assert rc(_lib.geom((6, 6, 6), 0.1, (0, 2, 0))) == _lib.ERR_UNSUPPORTED
+    assert b"outside its grid" in L.dcell_last_error()
+    assert rc(_lib.geom((6, 2), 0.1)) == _lib.ERR_UNSUPPORTED
+    assert rc(_lib.geom((6, 6, 6), 0.1, (0, -9, 0))) == _lib.OK  # empty y range: nothing to do, no launch
+    assert rc(g2, u=None, w=None) == _lib.ERR_ARG
+    assert L.dcell_ls_advect_mac(None, ctypes.byref(g3), d, d, d, d, 0.1, _lib.F64, e) == _lib.ERR_ARG
+
+
 # --------------------------------------------------------------------------- GPU
 def _mac_gpu(case, dtype, torch):
     from dcell_b200 import levelset as L
