@@ -189,54 +189,79 @@ __device__ __forceinline__ bool stencil_inside(const Geom &g, const T X[3]) {
   return true;
 }
 
-template <typename T>
+// One particle record; VEC (FP32 records on a 16-byte aligned array, chosen
+// at launch): one 16-byte access instead of four.
+template <typename T, bool VEC = false>
 __device__ __forceinline__ void load4(const T *__restrict__ parts, long long i, T p[4]) {
+  if constexpr (VEC && sizeof(T) == 4) {
+    const float4 v = reinterpret_cast<const float4 *>(parts)[i];
+    p[0] = v.x;
+    p[1] = v.y;
+    p[2] = v.z;
+    p[3] = v.w;
+  } else {
 #pragma unroll
-  for (int c = 0; c < 4; ++c) p[c] = parts[4 * i + c];
+    for (int c = 0; c < 4; ++c) p[c] = parts[4 * i + c];
+  }
 }
-template <typename T>
+template <typename T, bool VEC = false>
 __device__ __forceinline__ void store4(T *__restrict__ parts, long long i, const T p[4]) {
+  if constexpr (VEC && sizeof(T) == 4) {
+    reinterpret_cast<float4 *>(parts)[i] = make_float4(p[0], p[1], p[2], p[3]);
+  } else {
 #pragma unroll
-  for (int c = 0; c < 4; ++c) parts[4 * i + c] = p[c];
+    for (int c = 0; c < 4; ++c) parts[4 * i + c] = p[c];
+  }
 }
 
 // ParticleLS_AdvectParticles2D/3D (ParticleLS2D.c:6-36, ParticleLS3D.c:6-36).
-template <typename T, int DIM>
+// FP64 keeps the reference's expressions (its bits); FP32 scales the
+// velocities by kh = dt/(2h) and kf = dt/h, formed on the host in FP64 and
+// rounded once (within FP32 rounding of the reference's divisions).
+template <typename T, int DIM, bool VEC>
 __global__ void __launch_bounds__(256) pls_advect_kernel(Geom g, const T *__restrict__ vel, T *__restrict__ parts,
-                                                         long long n, T dt, int *flags) {
+                                                         long long n, T dt, float3 kh, float3 kf, int *flags) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   T p[4];
-  load4(parts, i, p);
+  load4<T, VEC>(parts, i, p);
   const T hx = (T)g.hx, hy = (T)g.hy, hz = (T)g.hz;
   T V1[3], V2[3], X[3];
   bool inside = true;
   if constexpr (sizeof(T) == 4) {
     vel_at_f32<DIM>(g, vel, p, V1, inside);
+    X[0] = p[0] + V1[0] * kh.x;
+    X[1] = p[1] + V1[1] * kh.y;
+    X[2] = DIM == 3 ? p[2] + V1[2] * kh.z : p[2];
+    vel_at_f32<DIM>(g, vel, X, V2, inside);
+    p[0] += V2[0] * kf.x;
+    p[1] += V2[1] * kf.y;
+    if (DIM == 3) p[2] += V2[2] * kf.z;
   } else {
     inside = stencil_inside<T, DIM>(g, p);
     vel_at<T, DIM>(g, vel, p, V1);
-  }
-  X[0] = p[0] + dt / T(2) * V1[0] / hx;
-  X[1] = p[1] + dt / T(2) * V1[1] / hy;
-  X[2] = DIM == 3 ? p[2] + dt / T(2) * V1[2] / hz : p[2];
-  if constexpr (sizeof(T) == 4) {
-    vel_at_f32<DIM>(g, vel, X, V2, inside);
-  } else {
+    X[0] = p[0] + dt / T(2) * V1[0] / hx;
+    X[1] = p[1] + dt / T(2) * V1[1] / hy;
+    X[2] = DIM == 3 ? p[2] + dt / T(2) * V1[2] / hz : p[2];
     inside = inside && stencil_inside<T, DIM>(g, X);
     vel_at<T, DIM>(g, vel, X, V2);
+    p[0] += dt * V2[0] / hx;
+    p[1] += dt * V2[1] / hy;
+    if (DIM == 3) p[2] += dt * V2[2] / hz;
   }
-  p[0] += dt * V2[0] / hx;
-  p[1] += dt * V2[1] / hy;
-  if (DIM == 3) p[2] += dt * V2[2] / hz;
-  store4(parts, i, p);
+  store4<T, VEC>(parts, i, p);
   if (!inside) raise_flag(flags, FLAG_PARTICLE_OUTSIDE);
 }
 
 // ErrorCorrection, identification and phi+/phi- (ParticleLS2D.c:65-97,
 // ParticleLS3D.c:65-98).  pos / neg hold order-preserving images of phi+ and
 // phi- over phi's grid, 0 / all ones meaning "phi itself".
-template <typename T, int DIM>
+//
+// FP32: the particles of a warp usually share a cell and so the same corners;
+// their scatters are aggregated per (grid point, side) with warp reductions,
+// one atomic per group (max and min do not depend on the order, so the result
+// is the same).
+template <typename T, int DIM, bool VEC>
 __global__ void __launch_bounds__(256) pls_escape_kernel(Geom g, const T *__restrict__ phi,
                                                          const T *__restrict__ parts, long long n,
                                                          typename OrdOf<T>::type *pos, typename OrdOf<T>::type *neg,
@@ -244,10 +269,45 @@ __global__ void __launch_bounds__(256) pls_escape_kernel(Geom g, const T *__rest
   const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (m >= n) return;
   T p[4];
-  load4(parts, m, p);
+  load4<T, VEC>(parts, m, p);
   const T dist = phi_at<T, DIM>(g, phi, p);
   const T sign = psign(p[3]);
-  if (!(sign * dist < T(0) && fabs(dist) > fabs(p[3]))) return;
+  const bool esc = sign * dist < T(0) && fabs(dist) > fabs(p[3]);
+  if constexpr (sizeof(T) == 4) {
+    const unsigned act = __activemask();  // the lanes with a particle
+    if (!__any_sync(act, esc)) return;
+    const int lane = threadIdx.x & 31;
+    const int A[3] = {(int)floor(p[0]), (int)floor(p[1]), DIM == 3 ? (int)floor(p[1]) : 0};
+    bool outside = false;
+#pragma unroll
+    for (int c = 0; c < (DIM == 3 ? 8 : 4); ++c) {
+      const int a[3] = {A[0] + (c & 1), A[1] + ((c >> 1) & 1), A[2] + (c >> 2)};
+      const int lx = a[0] - g.px, ly = a[1] - g.py, lz = DIM == 3 ? a[2] - g.pz : 0;
+      const bool in = (unsigned)lx < (unsigned)g.nx && (unsigned)ly < (unsigned)g.ny && (unsigned)lz < (unsigned)g.nz;
+      outside = outside || (esc && !in);
+      T d2 = (p[0] - (T)a[0]) * (p[0] - (T)a[0]) + (p[1] - (T)a[1]) * (p[1] - (T)a[1]);
+      if (DIM == 3) d2 = d2 + (p[2] - (T)a[2]) * (p[2] - (T)a[2]);
+      const T phi_p = sign * (sign * p[3] - sqrt(d2));
+      const unsigned bits = ord_bits(phi_p);
+      const long long key = esc && in ? 2LL * ((lz * g.ny + ly) * g.nx + lx) + (sign > T(0) ? 1 : 0) : -1LL;
+      unsigned pending = __ballot_sync(act, key >= 0);
+      while (pending) {  // one round per distinct (grid point, side) in the warp
+        const int leader = __ffs(pending) - 1;
+        const long long lk = __shfl_sync(act, key, leader);
+        const bool mine = key == lk;
+        const unsigned vmax = __reduce_max_sync(act, mine ? bits : 0u);
+        const unsigned vmin = __reduce_min_sync(act, mine ? bits : ~0u);
+        if (lane == leader) {
+          if (lk & 1) atomicMax(pos + (lk >> 1), vmax);
+          else atomicMin(neg + (lk >> 1), vmin);
+        }
+        pending &= ~__ballot_sync(act, mine);
+      }
+    }
+    if (outside) raise_flag(flags, FLAG_PARTICLE_OUTSIDE);
+    return;
+  }
+  if (!esc) return;
   const int A[3] = {(int)floor(p[0]), (int)floor(p[1]), DIM == 3 ? (int)floor(p[1]) : 0};
   bool outside = false;
 #pragma unroll
@@ -303,13 +363,13 @@ __global__ void __launch_bounds__(256) pls_merge_kernel(Geom g, T *__restrict__ 
 }
 
 // ParticleLS_AdjustRadii (ParticleLS.c:158-185).
-template <typename T, int DIM>
+template <typename T, int DIM, bool VEC>
 __global__ void __launch_bounds__(256) pls_adjust_kernel(Geom g, const T *__restrict__ phi, T *__restrict__ parts,
                                                          long long n, const long long *dcount, T r_min, T r_max) {
   const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (m >= n || (dcount && m >= *dcount)) return;
   T p[4];
-  load4(parts, m, p);
+  load4<T, VEC>(parts, m, p);
   const T dist = phi_at<T, DIM>(g, phi, p);
   const T sign = psign(p[3]);
   const T sphi = sign * dist;
@@ -559,10 +619,24 @@ static inline unsigned blocks_for(long long n, int threads) {
   return (unsigned)(b < 1 ? 1 : b);
 }
 
+// 16-byte records: FP32 particles on a 16-byte aligned array
+template <typename T>
+static bool vec_records(const void *parts) {
+  return sizeof(T) == 4 && ((uintptr_t)parts % 16) == 0;
+}
+
 template <typename T, int DIM>
 static void advect_launch(const Geom &g, const void *vel, void *parts, long long n, double dt, int *flags,
                           cudaStream_t st) {
-  pls_advect_kernel<T, DIM><<<blocks_for(n, 256), 256, 0, st>>>(g, (const T *)vel, (T *)parts, n, (T)dt, flags);
+  const double d = (double)(T)dt;  // the kernels' dt
+  const float3 kh = make_float3((float)(0.5 * d / g.hx), (float)(0.5 * d / g.hy), (float)(0.5 * d / g.hz));
+  const float3 kf = make_float3((float)(d / g.hx), (float)(d / g.hy), (float)(d / g.hz));
+  if (vec_records<T>(parts))
+    pls_advect_kernel<T, DIM, true><<<blocks_for(n, 256), 256, 0, st>>>(g, (const T *)vel, (T *)parts, n, (T)dt, kh,
+                                                                        kf, flags);
+  else
+    pls_advect_kernel<T, DIM, false><<<blocks_for(n, 256), 256, 0, st>>>(g, (const T *)vel, (T *)parts, n, (T)dt, kh,
+                                                                         kf, flags);
 }
 
 template <typename T, int DIM>
@@ -573,17 +647,24 @@ static void correct_launch(const Geom &g, void *phi, const int *band, long long 
   O *pos = (O *)scratch, *neg = pos + npts;
   cudaMemsetAsync(pos, 0x00, npts * sizeof(O), st);
   cudaMemsetAsync(neg, 0xFF, npts * sizeof(O), st);
-  if (n > 0)
-    pls_escape_kernel<T, DIM><<<blocks_for(n, 256), 256, 0, st>>>(g, (const T *)phi, (const T *)parts, n, pos, neg,
-                                                                  flags);
+  if (n > 0 && vec_records<T>(parts))
+    pls_escape_kernel<T, DIM, true><<<blocks_for(n, 256), 256, 0, st>>>(g, (const T *)phi, (const T *)parts, n, pos,
+                                                                        neg, flags);
+  else if (n > 0)
+    pls_escape_kernel<T, DIM, false><<<blocks_for(n, 256), 256, 0, st>>>(g, (const T *)phi, (const T *)parts, n, pos,
+                                                                         neg, flags);
   if (nband > 0) pls_merge_kernel<T><<<blocks_for(nband, 256), 256, 0, st>>>(g, (T *)phi, band, nband, pos, neg, flags);
 }
 
 template <typename T, int DIM>
 static void adjust_launch(const Geom &g, const void *phi, void *parts, long long n, const long long *dcount,
                           const dcell_pls_params &prm, cudaStream_t st) {
-  pls_adjust_kernel<T, DIM><<<blocks_for(n, 256), 256, 0, st>>>(g, (const T *)phi, (T *)parts, n, dcount,
-                                                                (T)prm.r_min, (T)prm.r_max);
+  if (vec_records<T>(parts))
+    pls_adjust_kernel<T, DIM, true><<<blocks_for(n, 256), 256, 0, st>>>(g, (const T *)phi, (T *)parts, n, dcount,
+                                                                        (T)prm.r_min, (T)prm.r_max);
+  else
+    pls_adjust_kernel<T, DIM, false><<<blocks_for(n, 256), 256, 0, st>>>(g, (const T *)phi, (T *)parts, n, dcount,
+                                                                         (T)prm.r_min, (T)prm.r_max);
 }
 
 // scratch of seeding / reseeding, ints: keep, excl, holes (n each), counts
