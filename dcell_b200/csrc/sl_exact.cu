@@ -779,32 +779,52 @@ __device__ T fmm_update_dev(const Geom &g, const T *__restrict__ phi, const int 
 // copy to be fixed wins); a point seen for the first time at or past it goes
 // on the far list.  Values only fall and the window only grows, so a far
 // point is either improved into the near list or moved there when the window
-// passes it.
+// passes it.  One relaxation returns which list the neighbour must join
+// (RELAX_NEAR / RELAX_FAR, its index in *qn) or RELAX_NONE; the caller
+// appends, warp-wide.
+enum { RELAX_NONE = 0, RELAX_NEAR = 1, RELAX_FAR = 2 };
+
 template <typename T, int DIM>
-__device__ void fmm_relax_dev(const Geom &g, const T *__restrict__ phi, const ReinitState &st, ReinitCounts *c,
-                              int nout, int fcur, int x, int y, int z, int s, int sign, T bw, T inf, T lim, T win) {
+__device__ int fmm_relax_dev(const Geom &g, const T *__restrict__ phi, const ReinitState &st, int x, int y, int z,
+                             int s, int sign, T bw, T inf, T lim, T win, int *qn) {
   typedef typename OrdOf<T>::type O;
   O *tent = (O *)st.tent;
   constexpr int kStarDev[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
   const int i = x + kStarDev[s][0], j = y + kStarDev[s][1], k = z + kStarDev[s][2];
-  if (i < 0 || i >= g.nx || j < 0 || j >= g.ny || k < 0 || k >= g.nz) return;
+  if (i < 0 || i >= g.nx || j < 0 || j >= g.ny || k < 0 || k >= g.nz) return RELAX_NONE;
   const int q = (k * g.ny + j) * g.nx + i;
-  if (sign * phi[q] < bw) return;  // fixed, or the other side
+  if (sign * phi[q] < bw) return RELAX_NONE;  // fixed, or the other side
   const T v = fmm_update_dev<T, DIM>(g, phi, st.mark, i, j, k, sign, inf, lim);
   if (v != v) {
     atomicOr(st.err, 1);
-    return;
+    return RELAX_NONE;
   }
   const O ov = ord_bits(v);
   const O old = atomicMin(&tent[q], ov);
+  *qn = q;
   if (v < win) {
     if (ov < old) {
       atomicExch(&st.mark[q], RM_TENT);
-      st.near[nout][atomicAdd(&c->near[nout], 1)] = q;
+      return RELAX_NEAR;
     }
   } else if (atomicCAS(&st.mark[q], RM_FAR, RM_TENT) == RM_FAR) {
-    st.far[fcur][atomicAdd(&c->far[fcur], 1)] = q;
+    return RELAX_FAR;
   }
+  return RELAX_NONE;
+}
+
+// Appends `value` of every lane that wants to, with one atomic per warp on
+// the list's length (a counter in the cluster's distributed shared memory,
+// which all eight CTAs of a side update); called by all 32 lanes.  The lists
+// are sets -- which thread handles which entry does not change the march.
+__device__ __forceinline__ void warp_append(int *list, int *count, bool want, int value) {
+  const unsigned m = __ballot_sync(0xffffffffu, want);
+  if (!m) return;
+  const int lane = (int)(threadIdx.x & 31), leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (want) list[base + __popc(m & ((1u << lane) - 1u))] = value;
 }
 
 template <typename T>
@@ -870,33 +890,46 @@ __global__ void __launch_bounds__(REINIT_MARCH_THREADS) reinit_march_kernel(Geom
   cl.sync();
   int in = 0, fcur = 0;
   T win = bucket * (T)REINIT_WINDOW;
-  for (int r = tid; r < nnodes * 2 * DIM; r += nthr) {  // FastMarching.c:72-84, one neighbour each
-    const dcell_irregular_node nd = nodes[r / (2 * DIM)];
-    if (nd.axis != -1) continue;
-    const int x = nd.pos[0] - g.px, y = nd.pos[1] - g.py, z = DIM == 3 ? nd.pos[2] - g.pz : 0;
-    if (x < 0 || x >= g.nx || y < 0 || y >= g.ny || z < 0 || z >= g.nz) continue;
-    if (sign * phi[(z * g.ny + y) * g.nx + x] >= 0)
-      fmm_relax_dev<T, DIM>(g, phi, st, &c, in, fcur, x, y, z, r % (2 * DIM), sign, bw, inf, -(T)INFINITY, win);
+  // every loop below runs a warp-uniform number of rounds (t0 = the warp's
+  // first index), so that the appends can be aggregated warp-wide
+  const int wtid = tid - (int)(threadIdx.x & 31);
+  for (int r0 = wtid; r0 < nnodes * 2 * DIM; r0 += nthr) {  // FastMarching.c:72-84, one neighbour each
+    const int r = r0 + (int)(threadIdx.x & 31);
+    int req = RELAX_NONE, qn = 0;
+    if (r < nnodes * 2 * DIM) {
+      const dcell_irregular_node nd = nodes[r / (2 * DIM)];
+      const int x = nd.pos[0] - g.px, y = nd.pos[1] - g.py, z = DIM == 3 ? nd.pos[2] - g.pz : 0;
+      if (nd.axis == -1 && x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz &&
+          sign * phi[(z * g.ny + y) * g.nx + x] >= 0)
+        req = fmm_relax_dev<T, DIM>(g, phi, st, x, y, z, r % (2 * DIM), sign, bw, inf, -(T)INFINITY, win, &qn);
+    }
+    warp_append(st.near[in], &c.near[in], req == RELAX_NEAR, qn);
+    warp_append(st.far[fcur], &c.far[fcur], req == RELAX_FAR, qn);
   }
   cl.sync();
   for (int b = 0; b < nb; ++b) {
     const T thr = bucket * (T)(b + 1);
     // accept what falls below this bucket's threshold; keep the rest of the window
     const int n_in = c.near[in];
-    for (int t = tid; t < n_in; t += nthr) {
-      const int q = st.near[in][t];
-      if (st.mark[q] == RM_MARCHED) continue;
-      const T v = ord_value(tent[q]);
-      if (v < thr && v <= bw) {
-        if (atomicCAS(&st.mark[q], RM_TENT, RM_MARCHED) == RM_TENT) {
-          phi[q] = sign * v;
-          st.acc[atomicAdd(&c.acc[b & 1], 1)] = q;
+    for (int t0 = wtid; t0 < n_in; t0 += nthr) {
+      const int t = t0 + (int)(threadIdx.x & 31);
+      const int q = t < n_in ? st.near[in][t] : 0;
+      bool acc = false, keep = false;
+      if (t < n_in && st.mark[q] != RM_MARCHED) {
+        const T v = ord_value(tent[q]);
+        if (v < thr && v <= bw) {
+          if (atomicCAS(&st.mark[q], RM_TENT, RM_MARCHED) == RM_TENT) {
+            phi[q] = sign * v;
+            acc = true;
+          }
+        } else if (v <= bw) {
+          keep = true;
+        } else {
+          st.mark[q] = RM_FAR;  // past the band unless a later push lowers it
         }
-      } else if (v <= bw) {
-        st.near[in ^ 1][atomicAdd(&c.near[in ^ 1], 1)] = q;
-      } else {
-        st.mark[q] = RM_FAR;  // past the band unless a later push lowers it
       }
+      warp_append(st.acc, &c.acc[b & 1], acc, q);
+      warp_append(st.near[in ^ 1], &c.near[in ^ 1], keep, q);
     }
     cl.sync();
     const int n_acc = c.acc[b & 1];
@@ -906,30 +939,41 @@ __global__ void __launch_bounds__(REINIT_MARCH_THREADS) reinit_march_kernel(Geom
       c.near[in] = 0;
       c.acc[(b + 1) & 1] = 0;
     }
-    for (int t = tid; t < n_acc * 2 * DIM; t += nthr) {  // one (point, neighbour) pair each
-      const int q = st.acc[t / (2 * DIM)];
-      const int x = q % g.nx, y = (q / g.nx) % g.ny, z = q / (g.nx * g.ny);
-      fmm_relax_dev<T, DIM>(g, phi, st, &c, in ^ 1, fcur, x, y, z, t % (2 * DIM), sign, bw, inf, sign * phi[q], win);
+    for (int t0 = wtid; t0 < n_acc * 2 * DIM; t0 += nthr) {  // one (point, neighbour) pair each
+      const int t = t0 + (int)(threadIdx.x & 31);
+      int req = RELAX_NONE, qn = 0;
+      if (t < n_acc * 2 * DIM) {
+        const int q = st.acc[t / (2 * DIM)];
+        const int x = q % g.nx, y = (q / g.nx) % g.ny, z = q / (g.nx * g.ny);
+        req = fmm_relax_dev<T, DIM>(g, phi, st, x, y, z, t % (2 * DIM), sign, bw, inf, sign * phi[q], win, &qn);
+      }
+      warp_append(st.near[in ^ 1], &c.near[in ^ 1], req == RELAX_NEAR, qn);
+      warp_append(st.far[fcur], &c.far[fcur], req == RELAX_FAR, qn);
     }
     cl.sync();
     in ^= 1;
     if ((b + 1) % REINIT_WINDOW == 0) {  // the window moves on: far points now inside it join the near list
       win = bucket * (T)(b + 1 + REINIT_WINDOW);
       const int n_far = c.far[fcur];
-      for (int t = tid; t < n_far; t += nthr) {
-        const int q = st.far[fcur][t];
-        if (st.mark[q] == RM_MARCHED) continue;
-        const T v = ord_value(tent[q]);
-        if (v < win) {
-          if (v <= bw) {
-            st.mark[q] = RM_TENT;
-            st.near[in][atomicAdd(&c.near[in], 1)] = q;
+      for (int t0 = wtid; t0 < n_far; t0 += nthr) {
+        const int t = t0 + (int)(threadIdx.x & 31);
+        const int q = t < n_far ? st.far[fcur][t] : 0;
+        bool to_near = false, stay = false;
+        if (t < n_far && st.mark[q] != RM_MARCHED) {
+          const T v = ord_value(tent[q]);
+          if (v < win) {
+            if (v <= bw) {
+              st.mark[q] = RM_TENT;
+              to_near = true;
+            } else {
+              st.mark[q] = RM_FAR;
+            }
           } else {
-            st.mark[q] = RM_FAR;
+            stay = true;
           }
-        } else {
-          st.far[fcur ^ 1][atomicAdd(&c.far[fcur ^ 1], 1)] = q;
         }
+        warp_append(st.near[in], &c.near[in], to_near, q);
+        warp_append(st.far[fcur ^ 1], &c.far[fcur ^ 1], stay, q);
       }
       cl.sync();
       // the consumed far list's length is read again only at the next
