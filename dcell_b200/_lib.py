@@ -111,6 +111,7 @@ def lib():
     L.dcell_advect_mac.argtypes = [G, i, vp, vp, vp, vp, d, vp, vp]
     L.dcell_ls_advect_mac.argtypes = [vp, G, vp, vp, vp, vp, d, i, vp]
     L.dcell_tc_gemm_check.argtypes = [vp, vp, vp, vp]
+    L.dcell_wait_timeout_check.argtypes = [vp, vp]
     L.dcell_sl_adjoint.argtypes = [G, i, vp, vp, d, i, i, vp, vp, vp, vp]
     L.dcell_split_bf16.argtypes = [G, vp, vp, vp]
     L.dcell_sl_step_tc_split.argtypes = [G, vp, vp, d, vp, i, i, vp, vp, vp, vp]
@@ -151,7 +152,7 @@ def lib():
                  "dcell_volume", "dcell_reinitialize", "dcell_velocity_box", "dcell_velocity_boxes",
                  "dcell_session_create", "dcell_session_destroy", "dcell_ls_advect_sl",
                  "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_ls_reinitialize",
-                 "dcell_tc_gemm_check",
+                 "dcell_tc_gemm_check", "dcell_wait_timeout_check",
                  "dcell_sl_adjoint", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",
                  "dcell_sl_step_tc_split", "dcell_pls_advect", "dcell_pls_correct", "dcell_pls_adjust_radii",
                  "dcell_pls_seed", "dcell_pls_reseed", "dcell_ls_pls_advect", "dcell_ls_pls_correct",

@@ -15,6 +15,7 @@
 #include "dcell_kernels.h"
 
 int launch_tc_gemm_check(const float *A, float *D, int *flags, cudaStream_t st);
+int launch_wait_timeout_check(int *result, cudaStream_t st);
 static_assert(DCELL_NOALLOC_MAX_BAND == kNoAllocMaxBand, "header and kernel limits differ");
 
 namespace {
@@ -419,6 +420,11 @@ DCELL_API int dcell_batch_sl_step(const dcell_cell *cells, int ncells, const dce
   if (threads < 32 || threads > 1024) FAIL(DCELL_ERR_ARG, "tiles must hold 32..1024 points (got %d)", threads);
   return launch_batch_cuda_core(cells, tiles, ntiles, tx, ty, tz, ctas_per_sm, phi0, vel, interp, backtrace, phi,
                                 flags, st);
+}
+
+DCELL_API int dcell_wait_timeout_check(int *result, void *stream) {
+  if (!result) FAIL(DCELL_ERR_ARG, "result is required");
+  return launch_wait_timeout_check(result, (cudaStream_t)stream);
 }
 
 DCELL_API int dcell_tc_gemm_check(const float *a, float *d, int *flags, void *stream) {

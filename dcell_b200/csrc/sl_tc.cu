@@ -988,6 +988,21 @@ __global__ void __launch_bounds__(kTile, 4) batch_tc_kernel(const dcell_cell *__
   if ((threadIdx.x >> 5) == 0) tmem_dealloc(c.tmem, kTmemCols);
 }
 
+// The give-up path of the kernels' bounded waits: one thread waits on phase 0
+// of an mbarrier that expects one arrival nobody makes, first with the
+// polling wait (the MMA issuer's), then with the suspending wait (the compute
+// warps'); result = 1 if the first gave up, + 2 if the second did.
+__global__ void wait_timeout_check_kernel(int *result) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const bool a = mbar_wait(&bar, 0u);
+    const bool b = mbar_wait_sleep(&bar, 0u);
+    *result = (a ? 0 : 1) | (b ? 0 : 2);
+  }
+}
+
 // D = bf16(A) * M^T on the same tensor-core path (hi half only): a check of
 // the operand layouts against a host GEMM.  A: 128 x 64 row-major, D: 128 x 64.
 __global__ void __launch_bounds__(kTile, 1) tc_gemm_check_kernel(const float *__restrict__ A, float *__restrict__ D,
@@ -1204,6 +1219,11 @@ int tc_slab_planes() { return tc::BrickShape<2>::BZ; }
 int launch_sl_tc_slab(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
                       int *flags, cudaStream_t st, const TcSlab &slab) {
   return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, nullptr, flags, st, &slab);
+}
+
+int launch_wait_timeout_check(int *result, cudaStream_t st) {
+  tc::wait_timeout_check_kernel<<<1, 32, 0, st>>>(result);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 
 int launch_tc_gemm_check(const float *A, float *D, int *flags, cudaStream_t st) {

@@ -502,6 +502,13 @@ DCELL_API int dcell_writer_particles_host(dcell_writer *w, const char *name, int
  * layouts on the running GPU against a host product. */
 DCELL_API int dcell_tc_gemm_check(const float *a, float *d, int *flags, void *stream);
 
+/* The give-up path of the device-side waits: one thread waits, with both
+ * bounded mbarrier waits the tensor-core kernels use (polling, then
+ * suspending), on a phase that nothing completes.  *result (a device int)
+ * receives 1 if the polling wait gave up, + 2 if the suspending one did
+ * (3 expected, within about a second); the context stays usable. */
+DCELL_API int dcell_wait_timeout_check(int *result, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

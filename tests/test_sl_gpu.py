@@ -149,6 +149,29 @@ def test_tc_gemm_layout(cuda):
     assert np.abs(d.cpu().numpy() - expect).max() < 1e-4 * np.abs(expect).max()
 
 
+def test_bounded_waits_give_up_and_the_context_survives(cuda):
+    """Failure detection without a fault: both bounded mbarrier waits of the
+    tensor-core kernels, waiting on a phase that nothing completes, give up
+    within their limits and say so; the context then still runs a
+    tensor-core step."""
+    import ctypes
+    import time
+    res = torch.full((1,), -1, dtype=torch.int32, device=cuda)
+    t0 = time.perf_counter()
+    _lib.check(_lib.lib().dcell_wait_timeout_check(ctypes.c_void_p(res.data_ptr()),
+                                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    took = time.perf_counter() - t0
+    assert int(res.item()) == 3
+    assert took < 30.0
+    N = 24
+    phi = fields.sphere_sdf(N, device=cuda).float().contiguous()
+    vel = fields.deformation_velocity(N, device=cuda).float().contiguous()
+    out, _ = L.sl_step_tc_split(L.split_bf16(phi), vel, 0.25 / N, 1.0 / N)
+    torch.cuda.synchronize()
+    assert bool(torch.isfinite(out).all())
+
+
 def test_departure_outside_grid_is_flagged(cuda):
     """Band points whose departure leaves the grid raise the flag; a dense
     step treats the grid edge as the domain boundary and does not."""
