@@ -1,0 +1,171 @@
+"""Parity at the benchmark's full size, 256^3: properties that do not depend on
+the size (exact invariants, bit-identity of the two tensor-core paths, the
+error budget against the FP64 path), and the oracle wherever it finishes in
+seconds at that size (FP64 paths, bit for bit).
+
+Workload: the benchmark's sphere (r = 0.15 at (0.35, 0.35, 0.35)) in
+LeVeque's deformation field, dt at CFL 0.5."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from dcell_b200 import fields
+from dcell_b200 import levelset as L
+
+pytestmark = pytest.mark.gpu
+N = 256
+H = 1.0 / N
+DT = fields.cfl_dt((2.0, 1.0, 1.0), H)
+
+
+@pytest.fixture(scope="module")
+def wl32(cuda):
+    phi = fields.sphere_sdf(N, device=cuda).float().contiguous()
+    vel = fields.deformation_velocity(N, device=cuda).float().contiguous()
+    return phi, vel
+
+
+def _recon(split):
+    """hi + lo of packed split words (bf16 hi in the low half, lo in the high half)."""
+    s = split.view(torch.int32)
+    hi = (s << 16).view(torch.float32)
+    lo = (s & -65536).view(torch.float32)
+    return hi + lo
+
+
+def test_tc_bricks_equal_gather_path(wl32, cuda):
+    """The dense brick kernel and the global-gather kernel (a band listing
+    every point) give the same bits for the whole 256^3 step."""
+    phi, vel = wl32
+    spl = L.split_bf16(phi)
+    dense, dspl = L.sl_step_tc_split(spl, vel, DT, H, backtrace="midpoint", out_split=torch.empty_like(spl))
+    band = fields.band_of(torch.zeros_like(phi), 1.0, margin=0).to(cuda)
+    assert band.shape[0] == N ** 3
+    banded, bspl = L.sl_step_tc_split(spl, vel, DT, H, band=band, backtrace="midpoint", out=torch.zeros_like(phi),
+                                      out_split=torch.zeros_like(spl))
+    torch.cuda.synchronize()
+    assert torch.equal(dense, banded)
+    assert torch.equal(dspl, bspl)
+
+
+def test_tc_error_budget_against_fp64(wl32, cuda):
+    """Split-BF16 tensor-core step vs the FP64 tricubic step on the same
+    (FP32-exact) inputs: max |error| <= 1e-5 where |phi| < 3h (the scope's
+    bar), and the two agree on the sign of phi at every band point."""
+    phi, vel = wl32
+    ref = L.sl_step(phi.double(), vel.double(), DT, H, interp="cubic_plain", backtrace="midpoint")
+    out, _ = L.sl_step_tc_split(L.split_bf16(phi), vel, DT, H, backtrace="midpoint")
+    band = ref.abs() < 3 * H
+    err = (out.double() - ref).abs()[band]
+    assert int(band.sum()) > 100000
+    assert float(err.max()) <= 1e-5, float(err.max())
+    assert bool(((out.double() > 0) == (ref > 0))[ref.abs() > 1e-6].all())
+
+
+def test_tc_invariants(wl32, cuda):
+    """A constant field stays exactly constant in any velocity (the operator
+    maps the constant stencil to the constant coefficient, every product and
+    sum exact); with dt = 0 every point returns exactly hi + lo of its own
+    split value."""
+    phi, vel = wl32
+    c = torch.full_like(phi, 0.375)  # 0.375 = hi exactly, lo = 0
+    out, _ = L.sl_step_tc_split(L.split_bf16(c), vel, DT, H, backtrace="midpoint")
+    assert bool((out == 0.375).all())
+    spl = L.split_bf16(phi)
+    out0, _ = L.sl_step_tc_split(spl, vel, 0.0, H, backtrace="midpoint")
+    torch.cuda.synchronize()
+    assert torch.equal(out0, _recon(spl))
+
+
+@pytest.fixture(scope="module")
+def wl64():
+    phi = fields.sphere_sdf(N).double().contiguous()
+    vel = fields.deformation_velocity(N).double().contiguous()
+    return phi, vel
+
+
+def test_linear_fp64_band_equals_oracle(wl64, cuda):
+    """The reference's linear SL (Euler) in FP64 on the |phi| < 6h band."""
+    phi, vel = wl64
+    band = fields.band_of(phi, 6 * H, margin=3)
+    out = L.sl_step(phi.to(cuda), vel.to(cuda), DT, H, band=band.to(cuda), interp="linear", backtrace="euler")
+    want = oracle.sl_step(phi.numpy(), vel.numpy(), DT, H, band=band.numpy(), interp="linear", backtrace="euler")
+    assert np.array_equal(out.cpu().numpy(), want)
+
+
+def test_irregular_nodes_fp64_equal_oracle(wl64, cuda):
+    """The irregular-node pass at 256^3: node set, axes, shifts, signs and d
+    exact; projections, normals and curvature within evaluation order."""
+    phi, _ = wl64
+    band = fields.band_of(phi, 6 * H, margin=3)
+    raw, count = L.irregular_nodes(phi.to(cuda), H, band.to(cuda), with_surface=True)
+    rows = L.nodes_to_rows(L.nodes_to_numpy(raw, int(count.item())))
+    ref = oracle.irregular_nodes(phi.numpy(), H, band.numpy())
+    assert rows.shape == ref.shape and rows.shape[0] > 100000
+    assert np.array_equal(rows[:, :8], ref[:, :8])
+    assert np.abs(rows[:, 8:17] - ref[:, 8:17]).max() < 1e-11
+    assert np.allclose(rows[:, 17], ref[:, 17], rtol=1e-9, atol=1e-9)
+
+
+def test_reinit_fp64_equals_oracle(cuda):
+    """Irregular nodes then the bucketed march at 256^3 (cell units), against
+    the oracle fed the node list the GPU produced: phi and band exact."""
+    phi = (fields.sphere_sdf(N, device=cuda) * N).contiguous()
+    band = fields.band_of(phi, 6.0, margin=3).to(cuda)
+    raw, count = L.irregular_nodes(phi, 1.0, band, with_surface=False)
+    rows = L.nodes_to_rows(L.nodes_to_numpy(raw, int(count.item())))
+    phi_in = phi.cpu().numpy().copy()
+    flags = torch.zeros(1, dtype=torch.int32, device=cuda)
+    got_band = L.reinitialize(phi, raw, count, 6.0, 1.0 / 64, flags=flags)
+    want, want_band = oracle.reinit(phi_in, rows, 6.0, 1.0 / 64)
+    assert int(flags.item()) == 0
+    assert np.array_equal(phi.cpu().numpy(), want)
+    assert np.array_equal(got_band.cpu().numpy(), want_band)
+
+
+def test_particle_step_fp64_equals_oracle(cuda):
+    """3.57 M particles around the sphere: RK2 advection and the escaped-
+    particle correction in FP64, bit for bit."""
+    from dcell_b200 import configs, pls
+    phi32, band, vel32, parts32 = configs.pls_workload(N, dev=cuda)
+    phi, vel, parts = phi32.double(), vel32.double().contiguous(), parts32.double().contiguous()
+    n = parts.shape[0]
+    dt = 0.5 * H
+    want = oracle.pls_advect(vel.cpu().numpy(), parts.cpu().numpy(), dt, H)
+    pls.advect(parts, n, vel, dt, H)
+    got = parts.cpu().numpy()
+    assert np.array_equal(got, want)
+    want_phi, _ = oracle.pls_correct(phi.cpu().numpy(), band.cpu().numpy(), got, H)
+    pls.correct(phi, band, parts, n, H)
+    assert np.array_equal(phi.cpu().numpy(), want_phi)
+
+
+def test_upwind_mac_fp64_equals_oracle(wl64, cuda):
+    phi, vel = wl64
+    comps = [vel[..., a].contiguous() for a in range(3)]
+    want = oracle.advect_mac(phi.numpy(), *(c.numpy() for c in comps), DT, H)
+    got = L.advect_mac(phi.to(cuda), *(c.to(cuda) for c in comps), DT, H)
+    assert np.array_equal(got.cpu().numpy(), want)
+
+
+def test_velocity_boxes_copy_exactly(cuda):
+    """64 cell boxes (edges 32..96, some straddling the domain) from a 256^3
+    x 4 FP32 fluid field: every box equals the slice of the field (zero
+    outside), one launch."""
+    rng = np.random.default_rng(7)
+    field = torch.rand((N, N, N, 4), device=cuda)
+    boxes = []
+    for _ in range(64):
+        shape = tuple(int(v) for v in rng.integers(32, 97, size=3))  # (nz, ny, nx)
+        origin = tuple(int(v) for v in rng.integers(-20, N - 10, size=3))  # (x, y, z)
+        boxes.append((origin, shape))
+    outs = L.velocity_boxes(field, boxes)
+    for (o, s), got in zip(boxes, outs):
+        want = torch.zeros(s + (3,), device=cuda)
+        lo = [max(0, o[a]) for a in range(3)]
+        hi = [min(N, o[a] + s[2 - a]) for a in range(3)]
+        if all(h > l for l, h in zip(lo, hi)):
+            want[lo[2] - o[2]:hi[2] - o[2], lo[1] - o[1]:hi[1] - o[1], lo[0] - o[0]:hi[0] - o[0]] = \
+                field[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0], 1:4]
+        assert torch.equal(got.reshape(want.shape), want)
