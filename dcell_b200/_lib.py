@@ -106,6 +106,8 @@ def lib():
     L.dcell_session_destroy.argtypes = [vp]
     L.dcell_ls_advect_sl.argtypes = [vp, G, vp, vp, vp, i, d, i, i, i, vp]
     L.dcell_ls_update_irregular_nodes.argtypes = [vp, G, vp, vp, i, i, i, vp, i, vp]
+    L.dcell_ls_advect_sl_rk2_half.argtypes = [vp, G, vp, vp, vp, i, d, i, i, i, vp, i, vp, i, vp]
+    L.dcell_ls_advect_sl_rk2_full.argtypes = [vp, G, vp, vp, vp, i, d, i, i, i, vp, i, vp, i, vp]
     L.dcell_ls_max_velocity.argtypes = [vp, G, vp, vp, i, vp]
     L.dcell_ls_reinitialize.argtypes = [vp, G, vp, vp, i, d, i, vp, i, vp]
     L.dcell_advect_mac.argtypes = [G, i, vp, vp, vp, vp, d, vp, vp]
@@ -152,6 +154,7 @@ def lib():
                  "dcell_volume", "dcell_reinitialize", "dcell_velocity_box", "dcell_velocity_boxes",
                  "dcell_session_create", "dcell_session_destroy", "dcell_ls_advect_sl",
                  "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_ls_reinitialize",
+                 "dcell_ls_advect_sl_rk2_half", "dcell_ls_advect_sl_rk2_full",
                  "dcell_tc_gemm_check", "dcell_wait_timeout_check",
                  "dcell_sl_adjoint", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",
                  "dcell_sl_step_tc_split", "dcell_pls_advect", "dcell_pls_correct", "dcell_pls_adjust_radii",

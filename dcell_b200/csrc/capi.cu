@@ -743,6 +743,134 @@ DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const do
   return session_flags_status(s, hflags);
 }
 
+// One substep of LevelSetAdvectSLRK2HalfStep / FullStep (AdvectRK2.c:5-26):
+// (half: phi0 <- phi, GridCopy), phi <- SL(phi0) at the band points (or
+// everywhere), then the irregular-node list of the new phi -- the same device
+// paths as dcell_ls_advect_sl followed by dcell_ls_update_irregular_nodes, with
+// phi staying on the device between them.
+static int ls_rk2(dcell_session *s, const dcell_geom *g, int half, double *phi0, const double *vel,
+                  const int *band, int nband, double dt, int interp, int backtrace, int precision, double *phi,
+                  int with_surface, dcell_irregular_node *nodes, int capacity, int *count) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (!phi0 || !vel || !phi || !count) FAIL(DCELL_ERR_ARG, "phi0, vel, phi and count are required");
+  if (precision != DCELL_F32 && precision != DCELL_F64) FAIL(DCELL_ERR_ARG, "precision must be F32 or F64");
+  if (nband < 0 || (nband > 0 && !band)) FAIL(DCELL_ERR_ARG, "invalid band");
+  if (capacity < 0 || (capacity > 0 && !nodes)) FAIL(DCELL_ERR_ARG, "invalid node buffer");
+  if (interp < DCELL_LINEAR || interp > DCELL_CUBIC_TC) FAIL(DCELL_ERR_ARG, "unknown interpolation %d", interp);
+  if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+  if (!(dt == dt)) FAIL(DCELL_ERR_NONFINITE, "dt is NaN");
+  if ((rc = check_band_host(g, band, nband))) return rc;
+  const long long n = grid_points(g);
+  const int dof = g->n[2] > 1 ? 3 : 2;
+  const bool dense = band == nullptr;
+  if (half) memcpy(phi0, phi, (size_t)n * sizeof(double));  // GridCopy(ls->phi, ls->phi0)
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  ENSURE(s->phi0_64, n * sizeof(double));
+  ENSURE(s->vel_64, n * dof * sizeof(double));
+  ENSURE(s->phi_64, n * sizeof(double));
+  int *dflags = (int *)s->small.p, *dcount = dflags + 1;
+  DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, 2 * sizeof(int), st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi0_64.p, phi0, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(s->vel_64.p, vel, n * dof * sizeof(double), cudaMemcpyHostToDevice, st));
+  // phi before the step: the points off the band keep it
+  if (!dense) {
+    if (half)
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi_64.p, s->phi0_64.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    else
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi_64.p, phi, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  const int *dband = nullptr;
+  if (nband > 0) {
+    ENSURE(s->band, (size_t)nband * 3 * sizeof(int));
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->band.p, band, (size_t)nband * 3 * sizeof(int), cudaMemcpyHostToDevice, st));
+    dband = (const int *)s->band.p;
+  }
+  const void *dphi0 = s->phi0_64.p, *dvel = s->vel_64.p;
+  void *dphi = s->phi_64.p;
+  if (precision == DCELL_F32) {
+    ENSURE(s->phi0_32, n * sizeof(float));
+    ENSURE(s->vel_32, n * dof * sizeof(float));
+    ENSURE(s->phi_32, n * sizeof(float));
+    if ((rc = launch_convert(s->phi0_64.p, DCELL_F64, s->phi0_32.p, DCELL_F32, n, st))) return rc;
+    if ((rc = launch_convert(s->vel_64.p, DCELL_F64, s->vel_32.p, DCELL_F32, n * dof, st))) return rc;
+    if (!dense && (rc = launch_convert(s->phi_64.p, DCELL_F64, s->phi_32.p, DCELL_F32, n, st))) return rc;
+    dphi0 = s->phi0_32.p;
+    dvel = s->vel_32.p;
+    dphi = s->phi_32.p;
+  }
+  const dcell::Geom G = dcell::to_geom(g);
+  if (!dense && nband == 0) {
+    // nothing to advect
+  } else if (precision == DCELL_F32 && interp == DCELL_CUBIC_TC && dense && G.nz > 1) {
+    ENSURE(s->split, n * sizeof(uint32_t));  // split-state step, as dcell_ls_advect_sl
+    if ((rc = launch_split_bf16((const float *)dphi0, (uint32_t *)s->split.p, n, st))) return rc;
+    if ((rc = launch_sl_tc_split(G, (const uint32_t *)s->split.p, (const float *)dvel, dt, nullptr, n, backtrace,
+                                 (float *)dphi, nullptr, dflags, st)))
+      return rc;
+  } else if ((rc = dcell_sl_step(g, precision, dphi0, dvel, dt, dband, nband, interp, backtrace, dphi, dflags, st))) {
+    return rc;
+  }
+  // the node list of the new phi, on the device copy
+  const size_t sb = irregular_scratch_bytes(nband);
+  ENSURE(s->scratch, sb);
+  ENSURE(s->nodes, (size_t)(capacity > 0 ? capacity : 1) * sizeof(dcell_irregular_node));
+  rc = dcell_irregular_nodes(g, precision, dphi, dband, nband, with_surface, (dcell_irregular_node *)s->nodes.p,
+                             capacity, dcount, s->scratch.p, sb, dflags, st);
+  if (rc) return rc;
+  // phi back: the band values (gathered, widened) or the whole grid
+  if (!dense) {
+    if (nband > 0) {
+      ENSURE(s->vals, (size_t)nband * sizeof(double));
+      if (precision == DCELL_F32) {
+        ENSURE(s->stage32, (size_t)nband * sizeof(float));
+        if ((rc = launch_gather_band(G, DCELL_F32, dphi, dband, nband, s->stage32.p, st))) return rc;
+        if ((rc = launch_convert(s->stage32.p, DCELL_F32, s->vals.p, DCELL_F64, nband, st))) return rc;
+      } else if ((rc = launch_gather_band(G, DCELL_F64, dphi, dband, nband, s->vals.p, st))) {
+        return rc;
+      }
+      s->host_vals.resize((size_t)nband);
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(s->host_vals.data(), s->vals.p, (size_t)nband * sizeof(double),
+                                       cudaMemcpyDeviceToHost, st));
+    }
+  } else {
+    if (precision == DCELL_F32) {
+      if ((rc = launch_convert(dphi, DCELL_F32, s->phi0_64.p, DCELL_F64, n, st))) return rc;
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(phi, s->phi0_64.p, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    } else {
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(phi, dphi, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+  }
+  int hv[2] = {0, 0};
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(hv, dflags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  if (!dense)
+    for (int b = 0; b < nband; ++b) phi[band_index(g, band + 3 * b)] = s->host_vals[(size_t)b];
+  *count = hv[1];
+  const int ncopy = hv[1] < capacity ? hv[1] : capacity;
+  if (ncopy > 0)
+    DCELL_CUDA_CHECK(cudaMemcpy(nodes, s->nodes.p, (size_t)ncopy * sizeof(dcell_irregular_node), cudaMemcpyDeviceToHost));
+  return session_flags_status(s, hv[0]);
+}
+
+DCELL_API int dcell_ls_advect_sl_rk2_half(dcell_session *s, const dcell_geom *g, double *phi0, const double *vel,
+                                          const int *band, int nband, double dt, int interp, int backtrace,
+                                          int precision, double *phi, int with_surface, dcell_irregular_node *nodes,
+                                          int capacity, int *count) {
+  return ls_rk2(s, g, 1, phi0, vel, band, nband, dt, interp, backtrace, precision, phi, with_surface, nodes,
+                capacity, count);
+}
+
+DCELL_API int dcell_ls_advect_sl_rk2_full(dcell_session *s, const dcell_geom *g, const double *phi0,
+                                          const double *vel, const int *band, int nband, double dt, int interp,
+                                          int backtrace, int precision, double *phi, int with_surface,
+                                          dcell_irregular_node *nodes, int capacity, int *count) {
+  return ls_rk2(s, g, 0, const_cast<double *>(phi0), vel, band, nband, dt, interp, backtrace, precision, phi,
+                with_surface, nodes, capacity, count);
+}
+
 DCELL_API int dcell_ls_update_irregular_nodes(dcell_session *s, const dcell_geom *g, const double *phi,
                                               const int *band, int nband, int with_surface, int precision,
                                               dcell_irregular_node *nodes, int capacity, int *count) {

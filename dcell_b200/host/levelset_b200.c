@@ -5,6 +5,10 @@
  * Compiled INSIDE adrielb/DCell's build in place of the CPU definitions:
  *   LevelSetAdvectSL, _2D, _3D          (LevelSetMethod/AdvectSL.c:6-89; the
  *                                        whole file is replaced)
+ *   LevelSetAdvectSLRK2HalfStep,
+ *   LevelSetAdvectSLRK2FullStep         (LevelSetMethod/AdvectRK2.c:5-26; the
+ *                                        reference's definitions are renamed
+ *                                        away when AdvectRK2.c is built)
  *   LevelSetUpdateIrregularNodeList     (LevelSetMethod/IrregularNodes.c:9-28;
  *                                        the reference's definition is renamed
  *                                        away when IrregularNodes.c is built)
@@ -149,34 +153,14 @@ PetscErrorCode LevelSetAdvectSL(LevelSet ls, Grid velgrid, PetscReal dt) {
 PetscErrorCode LevelSetAdvectSL_2D(LevelSet ls, Grid velgrid, PetscReal dt) { return LevelSetAdvectSL(ls, velgrid, dt); }
 PetscErrorCode LevelSetAdvectSL_3D(LevelSet ls, Grid velgrid, PetscReal dt) { return LevelSetAdvectSL(ls, velgrid, dt); }
 
-#undef __FUNCT__
-#define __FUNCT__ "LevelSetUpdateIrregularNodeList"
-PetscErrorCode LevelSetUpdateIrregularNodeList(LevelSet ls) {
-  dcell_session *s;
-  dcell_geom g;
-  dcell_irregular_node *buf;
+/* The node list of the GPU into ls->irregularNodes (the fields the transport
+ * path writes; the rest stay zero). */
+static PetscErrorCode b200_store_nodes(LevelSet ls, const dcell_irregular_node *buf, int count) {
   IrregularNode *nodes;
-  int *tmp, rc, count = 0, cap, i;
-  const int nb = ArrayLength(ls->band);
-  const int *band;
+  int i;
   PetscErrorCode ierr;
 
   PetscFunctionBegin;
-  ierr = PetscLogEventBegin(EVENT_LevelSetUpdateIrregularNodeList, 0, 0, 0, 0); CHKERRQ(ierr);
-  ierr = LevelSetB200Session(&s); CHKERRQ(ierr);
-  ierr = ArraySetSize(ls->irregularNodes, 0); CHKERRQ(ierr);
-  ierr = ArrayZero(ls->irregularNodes); CHKERRQ(ierr);
-  b200_geom(ls->phi, &g);
-  cap = (ls->phi->is2D ? 5 : 10) * (nb > 0 ? nb : 1); /* per point at most 5 (2D) / 10 (3D) nodes */
-  buf = (dcell_irregular_node *)malloc(sizeof(dcell_irregular_node) * (size_t)cap);
-  if (!buf) SETERRQ(PETSC_COMM_SELF, PETSC_ERR_MEM, "out of host memory");
-  band = b200_band(ls->band, &tmp);
-  rc = dcell_ls_update_irregular_nodes(s, &g, ls->phi->v1, band, nb, 0, b200_precision, buf, cap, &count);
-  free(tmp);
-  if (rc) {
-    free(buf);
-    SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_update_irregular_nodes: %s", dcell_last_error());
-  }
   ierr = ArraySetSize(ls->irregularNodes, count); CHKERRQ(ierr);
   ierr = ArrayZero(ls->irregularNodes); CHKERRQ(ierr);
   nodes = (IrregularNode *)ArrayGetData(ls->irregularNodes);
@@ -198,9 +182,92 @@ PetscErrorCode LevelSetUpdateIrregularNodeList(LevelSet ls) {
     n->op.y = q->op[1];
     n->op.z = q->op[2];
   }
+  PetscFunctionReturn(0);
+}
+
+#undef __FUNCT__
+#define __FUNCT__ "LevelSetUpdateIrregularNodeList"
+PetscErrorCode LevelSetUpdateIrregularNodeList(LevelSet ls) {
+  dcell_session *s;
+  dcell_geom g;
+  dcell_irregular_node *buf;
+  int *tmp, rc, count = 0, cap;
+  const int nb = ArrayLength(ls->band);
+  const int *band;
+  PetscErrorCode ierr;
+
+  PetscFunctionBegin;
+  ierr = PetscLogEventBegin(EVENT_LevelSetUpdateIrregularNodeList, 0, 0, 0, 0); CHKERRQ(ierr);
+  ierr = LevelSetB200Session(&s); CHKERRQ(ierr);
+  ierr = ArraySetSize(ls->irregularNodes, 0); CHKERRQ(ierr);
+  ierr = ArrayZero(ls->irregularNodes); CHKERRQ(ierr);
+  b200_geom(ls->phi, &g);
+  cap = (ls->phi->is2D ? 5 : 10) * (nb > 0 ? nb : 1); /* per point at most 5 (2D) / 10 (3D) nodes */
+  buf = (dcell_irregular_node *)malloc(sizeof(dcell_irregular_node) * (size_t)cap);
+  if (!buf) SETERRQ(PETSC_COMM_SELF, PETSC_ERR_MEM, "out of host memory");
+  band = b200_band(ls->band, &tmp);
+  rc = dcell_ls_update_irregular_nodes(s, &g, ls->phi->v1, band, nb, 0, b200_precision, buf, cap, &count);
+  free(tmp);
+  if (rc) {
+    free(buf);
+    SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_update_irregular_nodes: %s", dcell_last_error());
+  }
+  ierr = b200_store_nodes(ls, buf, count);
   free(buf);
+  CHKERRQ(ierr);
   ierr = PetscLogEventEnd(EVENT_LevelSetUpdateIrregularNodeList, 0, 0, 0, 0); CHKERRQ(ierr);
   PetscFunctionReturn(0);
+}
+
+/* LevelSetAdvectSLRK2HalfStep / FullStep (AdvectRK2.c:5-26): the GridCopy
+ * (half step), LevelSetAdvectSL and LevelSetUpdateIrregularNodeList in one
+ * library call, phi staying on the device between the advection and the
+ * node pass. */
+#undef __FUNCT__
+#define __FUNCT__ "LevelSetAdvectSLRK2"
+static PetscErrorCode b200_rk2(LevelSet ls, Grid velgrid, PetscReal dt, int half) {
+  dcell_session *s;
+  dcell_geom g;
+  dcell_irregular_node *buf;
+  int *tmp, rc, count = 0, cap;
+  const int nb = ArrayLength(ls->band);
+  const int *band;
+  PetscErrorCode ierr;
+
+  PetscFunctionBegin;
+  ierr = LevelSetB200Session(&s); CHKERRQ(ierr);
+  if (ls->phi0->SIZE != ls->phi->SIZE || velgrid->SIZE != ls->phi->SIZE * velgrid->dof)
+    SETERRQ(PETSC_COMM_SELF, PETSC_ERR_ARG_OUTOFRANGE, "phi0/velgrid do not match phi");
+  b200_geom(ls->phi, &g);
+  cap = (ls->phi->is2D ? 5 : 10) * (nb > 0 ? nb : 1); /* per point at most 5 (2D) / 10 (3D) nodes */
+  buf = (dcell_irregular_node *)malloc(sizeof(dcell_irregular_node) * (size_t)cap);
+  if (!buf) SETERRQ(PETSC_COMM_SELF, PETSC_ERR_MEM, "out of host memory");
+  band = b200_band(ls->band, &tmp);
+  if (half)
+    rc = dcell_ls_advect_sl_rk2_half(s, &g, ls->phi0->v1, velgrid->v1, band, nb, dt, b200_interp, b200_backtrace,
+                                     b200_precision, ls->phi->v1, 0, buf, cap, &count);
+  else
+    rc = dcell_ls_advect_sl_rk2_full(s, &g, ls->phi0->v1, velgrid->v1, band, nb, dt, b200_interp, b200_backtrace,
+                                     b200_precision, ls->phi->v1, 0, buf, cap, &count);
+  free(tmp);
+  if (rc == DCELL_ERR_DEPARTURE) {
+    /* the reference would read outside its arrays here; the GPU path clamped the sample */
+    ierr = PetscInfo1(0, "LevelSetAdvectSLRK2: %s\n", dcell_last_error()); CHKERRQ(ierr);
+  } else if (rc) {
+    free(buf);
+    SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "dcell_ls_advect_sl_rk2: %s", dcell_last_error());
+  }
+  ierr = b200_store_nodes(ls, buf, count);
+  free(buf);
+  CHKERRQ(ierr);
+  PetscFunctionReturn(0);
+}
+
+PetscErrorCode LevelSetAdvectSLRK2HalfStep(LevelSet ls, Grid velgrid, PetscReal dt) {
+  return b200_rk2(ls, velgrid, dt, 1);
+}
+PetscErrorCode LevelSetAdvectSLRK2FullStep(LevelSet ls, Grid velgrid, PetscReal dt) {
+  return b200_rk2(ls, velgrid, dt, 0);
 }
 
 #undef __FUNCT__

@@ -404,6 +404,23 @@ DCELL_API int dcell_session_destroy(dcell_session *s);
 DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const double *phi0, const double *vel, const int *band,
                        int nband, double dt, int interp, int backtrace, int precision, double *phi);
 
+/* LevelSetAdvectSLRK2HalfStep / LevelSetAdvectSLRK2FullStep (AdvectRK2.c:
+ * 5-26) on host arrays in one call each: the half step first copies phi into
+ * phi0 (GridCopy), then both advect phi from phi0 as dcell_ls_advect_sl does
+ * (same arguments, same device paths, same results) and rebuild the
+ * irregular-node list of the new phi as dcell_ls_update_irregular_nodes does,
+ * with phi kept on the device between the two.  The status is that of the
+ * pair (DCELL_ERR_DEPARTURE after writing phi and the nodes, as
+ * dcell_ls_advect_sl). */
+DCELL_API int dcell_ls_advect_sl_rk2_half(dcell_session *s, const dcell_geom *g, double *phi0, const double *vel,
+                                          const int *band, int nband, double dt, int interp, int backtrace,
+                                          int precision, double *phi, int with_surface, dcell_irregular_node *nodes,
+                                          int capacity, int *count);
+DCELL_API int dcell_ls_advect_sl_rk2_full(dcell_session *s, const dcell_geom *g, const double *phi0,
+                                          const double *vel, const int *band, int nband, double dt, int interp,
+                                          int backtrace, int precision, double *phi, int with_surface,
+                                          dcell_irregular_node *nodes, int capacity, int *count);
+
 /* LevelSetUpdateIrregularNodeList(ls) on host phi; *count = node count. */
 DCELL_API int dcell_ls_update_irregular_nodes(dcell_session *s, const dcell_geom *g, const double *phi, const int *band,
                                     int nband, int with_surface, int precision, dcell_irregular_node *nodes,

@@ -291,6 +291,43 @@ def test_tc_brick_path_equals_gather_path(cuda, cfl_scale, shape, points, monkey
 
 
 @pytest.mark.gpu
+def test_host_buffer_rk2_half_full_equal_reference(golden, cuda):
+    """dcell_ls_advect_sl_rk2_half / _full (AdvectRK2.c:5-26) on host FP64
+    arrays: the half step copies phi into phi0, and phi and the irregular-node
+    list of each substep equal the reference's (golden)."""
+    import ctypes
+    g = golden("sl3d_rk2")
+    Lb = _lib.lib()
+    sess = ctypes.c_void_p()
+    _lib.check(Lb.dcell_session_create(0, ctypes.byref(sess)))
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    try:
+        geo = _lib.geom(g["phi0"].shape, float(g["h"]), tuple(int(v) for v in g["origin"]))
+        phi = np.ascontiguousarray(g["phi0"], dtype=np.float64).copy()
+        phi0 = np.zeros_like(phi)
+        band = np.ascontiguousarray(g["band"], dtype=np.int32)
+        cap = 10 * len(band)
+        nodes = np.zeros(cap, dtype=_lib.NODE_DTYPE)
+        count = ctypes.c_int()
+        dt = float(g["dt"])
+        for step, (vel, tau, want_phi, want_nodes) in enumerate(
+                [(g["vel"], dt / 2, g["phi_half"], g["nodes_half"]), (g["vel_half"], dt, g["phi_full"], g["nodes_full"])]):
+            v = np.ascontiguousarray(vel, dtype=np.float64)
+            fn = Lb.dcell_ls_advect_sl_rk2_half if step == 0 else Lb.dcell_ls_advect_sl_rk2_full
+            _lib.check(fn(sess, ctypes.byref(geo), p(phi0), p(v), p(band), len(band), tau, _lib.LINEAR, _lib.EULER,
+                          _lib.F64, p(phi), 0, p(nodes), cap, ctypes.byref(count)))
+            if step == 0:
+                assert np.array_equal(phi0, g["phi0"])  # GridCopy(phi, phi0) before the half step
+            assert np.array_equal(phi, want_phi)
+            rows = L.nodes_to_rows(nodes[:count.value])
+            assert rows.shape == want_nodes.shape
+            assert np.array_equal(rows[:, :8], want_nodes[:, :8])
+            assert np.abs(rows[:, 8:14] - want_nodes[:, 8:14]).max() < 1e-11
+    finally:
+        Lb.dcell_session_destroy(sess)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("speed", [1.0, 40.0])
 def test_host_buffer_tc_step_pipelined_equals_device_step(cuda, speed):
     """dcell_ls_advect_sl (FP32 tensor-core, dense) on host FP64 arrays is
