@@ -520,6 +520,9 @@ def main():
             # output in the reference's formats: the stream's cost of a 256^3 snapshot and the drain to disk
             from dcell_b200.configs import run_io
             line["io"] = run_io(args.size)
+            # the irregular-node pass that follows the step (projections, normals, curvature)
+            from dcell_b200.configs import run_nodes
+            line["irregular_nodes"] = run_nodes(args.size, dev=dev)
             # first-order upwind step on MAC faces (LevelSetAdvectMAC_3D), HBM-bound stencil
             from dcell_b200.configs import run_mac
             m = run_mac(args.size, dev=dev)

@@ -296,6 +296,59 @@ def run_mac(N=256, dev="cuda", K=10, W=3):
     return res
 
 
+def run_nodes(N=256, dev="cuda", reps=5):
+    """The irregular-node pass (LevelSetUpdateIrregularNodeList,
+    IrregularNodes3D.c:6-117: sign tests, orthogonal projections; plus the
+    normals and curvature of IIM/SurfaceQuantities.c) on the |phi| < 6h band
+    of the N^3 workload sphere, FP64 and FP32, CUDA events, median of `reps`
+    calls; beside it the reference's own routine on the same phi (one core,
+    oracle/_ref) with its node list compared (FP64)."""
+    import statistics
+    h = 1.0 / N
+    phi64 = fields.sphere_sdf(N, device=dev).double().contiguous()
+    band = fields.band_of(phi64, 6 * h, margin=3).to(dev)
+    res = {"workload": f"{N}^3 sphere r=0.15, band |phi| < 6h", "band_points": int(band.shape[0])}
+    rows64 = None
+    for name, dtype in (("fp64", torch.float64), ("fp32", torch.float32)):
+        ph = phi64.to(dtype)
+        L.irregular_nodes(ph, h, band, with_surface=True)  # warm-up (allocations)
+        times = []
+        for _ in range(reps):
+            e0, e1 = _events()
+            torch.cuda.synchronize()
+            e0.record()
+            raw, count = L.irregular_nodes(ph, h, band, with_surface=True)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        res[name] = {"ms": statistics.median(times), "nodes": int(count.item())}
+        if dtype == torch.float64:
+            rows64 = L.nodes_to_rows(L.nodes_to_numpy(raw, int(count.item())))
+    try:
+        from oracle import reference as R
+        ok = R.available()
+    except ImportError:
+        ok = False
+    if ok:
+        ls = R.RefLevelSet.create(h, (0, 0, 0), (N, N, N))
+        ls.set_phi(phi64.cpu().numpy())
+        ls.set_band(band.cpu().numpy())
+        t0 = time.perf_counter()
+        n = ls.update_irregular()
+        t1 = time.perf_counter()
+        ref = ls.nodes_no_update(n, surface=True)
+        t2 = time.perf_counter()
+        ls.close()
+        same = rows64.shape == ref.shape and bool(np.array_equal(rows64[:, :8], ref[:, :8]))
+        res["reference_cpu"] = {"node_list_s": t1 - t0, "surface_s": t2 - t1, "cores": 1, "kind": "reference",
+                                "nodes": int(n), "fp64_exact_fields_equal": same,
+                                "fp64_max_projection_diff": float(np.abs(rows64[:, 8:14] - ref[:, 8:14]).max())
+                                if same else None,
+                                "gpu_fp64_speedup": (t2 - t0) * 1e3 / res["fp64"]["ms"]}
+    res["how"] = "levelset.irregular_nodes(with_surface=True): count, scan, write, projections, normals/curvature"
+    return res
+
+
 def pls_workload(N=256, per_cell=32, seed=5, dev="cuda", dtype=torch.float32):
     """phi (cell units) of the workload sphere, its band |phi| < 6 cells, the
     deformation velocity, and per_cell particles uniform in every cell with
@@ -472,6 +525,7 @@ def main():
         results[c] = (run_vel(a.grid or 512, a.cells) if c == "vel" else
                       run_pls(a.grid or 256) if c == "pls" else run_io(a.grid or 256) if c == "io" else
                       run_reinit(a.grid or 256) if c == "reinit" else run_mac(a.grid or 256) if c == "mac" else
+                      run_nodes(a.grid or 256) if c == "nodes" else
                       globals()[f"run_{c}"]())
         results[c]["wall_s"] = time.time() - t0
         print(json.dumps({c: results[c]}, default=float), flush=True)

@@ -67,82 +67,93 @@ __global__ void __launch_bounds__(256) sl_linear_kernel(Geom g, const T *__restr
 }
 
 // ---------------------------------------------------------------------------
-// Catmull-Rom operator (TricubicInverse.h == C (x) C (x) C; OrthogonalProjection.c:48-63 == C (x) C).
-__device__ __constant__ double kCR[4][4] = {
-    {0, 1, 0, 0}, {-0.5, 0, 0.5, 0}, {1, -2.5, 2, -0.5}, {-0.5, 1.5, -1.5, 0.5}};
+// Catmull-Rom polynomial of a stencil for the orthogonal projection
+// (OrthogonalProjection3D.c builds it with TricubicInverse.h == C (x) C (x) C,
+// OrthogonalProjection.c:48-63 with C (x) C).  Here the operator is applied
+// one axis at a time (x, then y, then z: 3 x 16 x 11 products instead of
+// the 1331 of the full matrix) and the value and gradient are evaluated by
+// nested Horner; both are fully unrolled so the 64 values stay in
+// registers.  The coefficients and values equal the reference's up to
+// rounding (the projection's tolerance is 1e-3 cells; the results agree with
+// the reference's to ~1e-13).
 
-template <typename T>
-__device__ void cubic_coefs3(const T *s, T *a) {
-  for (int pz = 0; pz < 4; ++pz)
-    for (int py = 0; py < 4; ++py)
-      for (int px = 0; px < 4; ++px) {
-        T acc = 0;
-        for (int sz = 0; sz < 4; ++sz) {
-          const double cz = kCR[pz][sz];
-          if (cz == 0.0) continue;
-          for (int sy = 0; sy < 4; ++sy) {
-            const double cy = kCR[py][sy];
-            if (cy == 0.0) continue;
-            for (int sx = 0; sx < 4; ++sx) {
-              const double cx = kCR[px][sx];
-              if (cx == 0.0) continue;
-              acc += (T)(cz * cy * cx) * s[sx + 4 * sy + 16 * sz];
-            }
-          }
-        }
-        a[px + 4 * py + 16 * pz] = acc;
-      }
+// C[p][q]: row p = the monomial t^p, column q = stencil entry q - 1
+__host__ __device__ constexpr double cr_c(int p, int q) {
+  return p == 0 ? (q == 1 ? 1.0 : 0.0)
+       : p == 1 ? (q == 0 ? -0.5 : q == 2 ? 0.5 : 0.0)
+       : p == 2 ? (q == 0 ? 1.0 : q == 1 ? -2.5 : q == 2 ? 2.0 : -0.5)
+                : (q == 0 ? -0.5 : q == 1 ? 1.5 : q == 2 ? -1.5 : 0.5);
 }
 
+// one axis of C on 4 values with stride `st` (compile-time after unrolling)
 template <typename T>
-__device__ void cubic_coefs2(const T *s, T *a) {
-  for (int py = 0; py < 4; ++py)
-    for (int px = 0; px < 4; ++px) {
-      T acc = 0;
-      for (int sy = 0; sy < 4; ++sy) {
-        const double cy = kCR[py][sy];
-        if (cy == 0.0) continue;
-        for (int sx = 0; sx < 4; ++sx) {
-          const double cx = kCR[px][sx];
-          if (cx == 0.0) continue;
-          acc += (T)(cy * cx) * s[sx + 4 * sy];
-        }
-      }
-      a[px + 4 * py] = acc;
-    }
-}
-
-template <typename T>
-__device__ void cubic_eval3(const T *a, T x, T y, T z, T &p, T &gx, T &gy, T &gz) {
-  const T X[4] = {1, x, x * x, x * x * x}, Y[4] = {1, y, y * y, y * y * y}, Z[4] = {1, z, z * z, z * z * z};
-  const T dX[4] = {0, 1, 2 * x, 3 * x * x}, dY[4] = {0, 1, 2 * y, 3 * y * y}, dZ[4] = {0, 1, 2 * z, 3 * z * z};
-  T v = 0, vx = 0, vy = 0, vz = 0;
-  for (int k = 0; k < 4; ++k)
-    for (int j = 0; j < 4; ++j)
+__device__ __forceinline__ void cr_apply(const T *in, T *out, int st) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const T c = a[i + 4 * j + 16 * k];
-        v += c * X[i] * Y[j] * Z[k];
-        vx += c * dX[i] * Y[j] * Z[k];
-        vy += c * X[i] * dY[j] * Z[k];
-        vz += c * X[i] * Y[j] * dZ[k];
-      }
+  for (int p = 0; p < 4; ++p) {
+    T acc = T(0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (cr_c(p, q) != 0.0) acc += (T)cr_c(p, q) * in[q * st];
+    out[p * st] = acc;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void cubic_coefs3(const T *s, T *a) {
+  T t[64], u[64];
+#pragma unroll
+  for (int l = 0; l < 16; ++l) cr_apply(s + 4 * l, t + 4 * l, 1);  // x
+#pragma unroll
+  for (int l = 0; l < 16; ++l) cr_apply(t + (l & 3) + 16 * (l >> 2), u + (l & 3) + 16 * (l >> 2), 4);  // y
+#pragma unroll
+  for (int l = 0; l < 16; ++l) cr_apply(u + l, a + l, 16);  // z
+}
+
+template <typename T>
+__device__ __forceinline__ void cubic_coefs2(const T *s, T *a) {
+  T t[16];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) cr_apply(s + 4 * l, t + 4 * l, 1);  // x
+#pragma unroll
+  for (int l = 0; l < 4; ++l) cr_apply(t + l, a + l, 4);  // y
+}
+
+// value and gradient of sum a[i + 4j + 16k] x^i y^j z^k
+template <typename T>
+__device__ __forceinline__ void cubic_eval3(const T *a, T x, T y, T z, T &p, T &gx, T &gy, T &gz) {
+  T v = 0, vx = 0, vy = 0, vz = 0;
+#pragma unroll
+  for (int k = 3; k >= 0; --k) {
+    T w = 0, wx = 0, wy = 0;  // the (x, y) polynomial of slice k, its x and y derivatives
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+      const T *c = a + 4 * j + 16 * k;
+      const T px = ((c[3] * x + c[2]) * x + c[1]) * x + c[0];
+      const T dpx = (T(3) * c[3] * x + T(2) * c[2]) * x + c[1];
+      wy = wy * y + w;
+      w = w * y + px;
+      wx = wx * y + dpx;
+    }
+    vz = vz * z + v;
+    v = v * z + w;
+    vx = vx * z + wx;
+    vy = vy * z + wy;
+  }
   p = v; gx = vx; gy = vy; gz = vz;
 }
 
 template <typename T>
-__device__ void cubic_eval2(const T *a, T x, T y, T &p, T &gx, T &gy) {
-  const T X[4] = {1, x, x * x, x * x * x}, Y[4] = {1, y, y * y, y * y * y};
-  const T dX[4] = {0, 1, 2 * x, 3 * x * x}, dY[4] = {0, 1, 2 * y, 3 * y * y};
+__device__ __forceinline__ void cubic_eval2(const T *a, T x, T y, T &p, T &gx, T &gy) {
   T v = 0, vx = 0, vy = 0;
-  for (int j = 0; j < 4; ++j)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const T c = a[i + 4 * j];
-      v += c * X[i] * Y[j];
-      vx += c * dX[i] * Y[j];
-      vy += c * X[i] * dY[j];
-    }
+  for (int j = 3; j >= 0; --j) {
+    const T *c = a + 4 * j;
+    const T px = ((c[3] * x + c[2]) * x + c[1]) * x + c[0];
+    const T dpx = (T(3) * c[3] * x + T(2) * c[2]) * x + c[1];
+    vy = vy * y + v;
+    v = v * y + px;
+    vx = vx * y + dpx;
+  }
   p = v; gx = vx; gy = vy;
 }
 
@@ -491,8 +502,11 @@ __global__ void __launch_bounds__(256) ortho_kernel(Geom g, const T *__restrict_
     int m;
     if (DIM == 3) {
       T s[64], a[64];
+#pragma unroll
       for (int zz = 0; zz < 4; ++zz)
+#pragma unroll
         for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
           for (int xx = 0; xx < 4; ++xx)
             s[xx + 4 * yy + 16 * zz] = phi[gidx(g, ci - 2 + i + xx, cj - 2 + j + yy, ck - 2 + k + zz)];
       cubic_coefs3<T>(s, a);
@@ -514,7 +528,9 @@ __global__ void __launch_bounds__(256) ortho_kernel(Geom g, const T *__restrict_
       res[0] = x + (T)i - 1; res[1] = y + (T)j - 1; res[2] = z + (T)k - 1;
     } else {
       T s[16], a[16];
+#pragma unroll
       for (int yy = 0; yy < 4; ++yy)
+#pragma unroll
         for (int xx = 0; xx < 4; ++xx) s[xx + 4 * yy] = phi[gidx(g, ci - 2 + i + xx, cj - 2 + j + yy, 0)];
       cubic_coefs2<T>(s, a);
       for (m = 0; m < 20; ++m) {
