@@ -482,7 +482,7 @@ __device__ void ortho_linear2(const T s[3][3], T op[3], T &mindist) {
 }
 
 template <typename T, int DIM>
-__global__ void __launch_bounds__(256) ortho_kernel(Geom g, const T *__restrict__ phi,
+__global__ void __launch_bounds__(256, 3) ortho_kernel(Geom g, const T *__restrict__ phi,
                                                     dcell_irregular_node *__restrict__ nodes,
                                                     const int *__restrict__ count, int cap) {
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
