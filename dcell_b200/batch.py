@@ -21,6 +21,7 @@ import torch
 
 from . import _lib, fields
 from ._lib import BACKTRACE, INTERP, DcellError, check, lib
+from .levelset import split_bf16
 
 CELL_DTYPE = np.dtype([("offset", "<i8"), ("n", "<i4", 3), ("pad", "<i4"), ("h", "<f8", 3), ("dt", "<f8")])
 TILE_DTYPE = np.dtype([("cell", "<i4"), ("x0", "<i4"), ("y0", "<i4"), ("z0", "<i4")])
@@ -119,6 +120,40 @@ class CellBatch:
                                   ctypes.c_void_p(self.vel.data_ptr() + 12 * o), float(c["dt"]), None, 0, mode, bt,
                                   ctypes.c_void_p(phi.data_ptr() + 4 * o), None, st))
         return phi
+
+    # ------------------------------------------------------------------
+    BRICK = (32, 4, 8)  # the brick kernel's points per brick (x, y, z)
+
+    def split(self, phi=None):
+        """Packed BF16 hi/lo words of the packed FP32 phi (the split state)."""
+        phi = self.phi if phi is None else phi
+        return split_bf16(phi.view(1, 1, -1)).view(-1)
+
+    def step_tc_split(self, phi0_split, phi, phi_split, backtrace="midpoint", flags=None):
+        """One split-state tensor-core step of every cell in ONE launch over
+        bricks of 32 x 4 x 8 points (dcell_batch_sl_step_tc_split): phi and
+        phi_split (the next step's input) receive the new state."""
+        bricks, n = self.plan(self.BRICK)
+        check(lib().dcell_batch_sl_step_tc_split(_vp(self.cells), self.ncells, _vp(bricks), n, _vp(phi0_split),
+                                                 _vp(self.vel), BACKTRACE[backtrace] if isinstance(backtrace, str)
+                                                 else int(backtrace), _vp(phi), _vp(phi_split),
+                                                 _vp(flags) if flags is not None else None, _stream()))
+        return phi, phi_split
+
+    def step_tc_split_per_cell(self, phi0_split, phi, phi_split, backtrace="midpoint"):
+        """The comparator: dcell_sl_step_tc_split launched once per cell."""
+        bt = BACKTRACE[backtrace] if isinstance(backtrace, str) else int(backtrace)
+        L = lib()
+        st = _stream()
+        for i, s in enumerate(self.shapes):
+            c = self.cells_host[i]
+            g = _lib.geom(s, tuple(c["h"]))
+            o = int(self.offsets[i])
+            check(L.dcell_sl_step_tc_split(ctypes.byref(g), ctypes.c_void_p(phi0_split.data_ptr() + 4 * o),
+                                           ctypes.c_void_p(self.vel.data_ptr() + 12 * o), float(c["dt"]), None, 0,
+                                           bt, ctypes.c_void_p(phi.data_ptr() + 4 * o),
+                                           ctypes.c_void_p(phi_split.data_ptr() + 4 * o), None, st))
+        return phi, phi_split
 
     def cell_view(self, flat, i):
         o, s = int(self.offsets[i]), self.shapes[i]

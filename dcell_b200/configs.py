@@ -169,6 +169,35 @@ def run_c4(dev="cuda", ncells=512, steps=20):
         res[interp] = {"tile": list(tile), "ctas_per_sm": ctas, "graph_ms": ms_graph, "per_cell_launch_ms": ms_cells,
                        "speedup": ms_cells / ms_graph, "updates_per_s": b.npoints * steps / (ms_graph / 1e3),
                        "autotune_top3": [[t[0], list(t[1]), t[2]] for t in table[:3]]}
+    # split-state tensor-core steps over bricks of all cells (one launch per
+    # step), against dcell_sl_step_tc_split per cell, and the error of both TC
+    # forms against the FP64 tricubic step per cell after `steps` steps
+    s0 = b.split()
+    xa, ya = s0.clone(), torch.empty_like(s0)
+    pa = torch.empty_like(b.phi)
+    b.step_tc_split(xa, pa, ya)
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(steps):
+        b.step_tc_split(xa, pa, ya)
+        xa, ya = ya, xa
+    e1.record()
+    torch.cuda.synchronize()
+    ms_bricks = e0.elapsed_time(e1)
+    xc, yc, pc = s0.clone(), torch.empty_like(s0), torch.empty_like(b.phi)
+    e0.record()
+    for _ in range(steps):
+        b.step_tc_split_per_cell(xc, pc, yc)
+        xc, yc = yc, xc
+    e1.record()
+    torch.cuda.synchronize()
+    ms_split_cells = e0.elapsed_time(e1)
+    res["cubic_tc_split_bricks"] = {"ms": ms_bricks, "per_cell_launch_ms": ms_split_cells,
+                                    "updates_per_s": b.npoints * steps / (ms_bricks / 1e3),
+                                    "equal_to_per_cell": bool(torch.equal(pa, pc)),
+                                    "how": "dcell_batch_sl_step_tc_split, one launch per step over bricks of all "
+                                           "cells, split state, CUDA events"}
     return res
 
 
@@ -516,7 +545,8 @@ def main():
     ap.add_argument("which", nargs="?", default="all")
     ap.add_argument("--out", default=None)
     ap.add_argument("--grid", type=int, default=None, help="vel: edge of the fluid field (512); pls: grid edge (256)")
-    ap.add_argument("--cells", type=int, default=512, help="vel: number of cell boxes")
+    ap.add_argument("--cells", type=int, default=512, help="vel: number of cell boxes; c4: number of cells")
+    ap.add_argument("--steps", type=int, default=20, help="c4: steps per timed run")
     a = ap.parse_args()
     todo = ["c1", "c2", "c3", "c4", "c5"] if a.which == "all" else a.which.split(",")
     results = {}
@@ -525,7 +555,7 @@ def main():
         results[c] = (run_vel(a.grid or 512, a.cells) if c == "vel" else
                       run_pls(a.grid or 256) if c == "pls" else run_io(a.grid or 256) if c == "io" else
                       run_reinit(a.grid or 256) if c == "reinit" else run_mac(a.grid or 256) if c == "mac" else
-                      run_nodes(a.grid or 256) if c == "nodes" else
+                      run_nodes(a.grid or 256) if c == "nodes" else run_c4(ncells=a.cells, steps=a.steps) if c == "c4" else
                       globals()[f"run_{c}"]())
         results[c]["wall_s"] = time.time() - t0
         print(json.dumps({c: results[c]}, default=float), flush=True)

@@ -427,6 +427,18 @@ DCELL_API int dcell_wait_timeout_check(int *result, void *stream) {
   return launch_wait_timeout_check(result, (cudaStream_t)stream);
 }
 
+DCELL_API int dcell_batch_sl_step_tc_split(const dcell_cell *cells, int ncells, const dcell_tile *bricks,
+                                           int nbricks, const unsigned int *phi0_split, const float *vel,
+                                           int backtrace, float *phi, unsigned int *phi_split, int *flags,
+                                           void *stream) {
+  if (ncells < 0 || nbricks < 0) FAIL(DCELL_ERR_ARG, "ncells and nbricks must be >= 0");
+  if (nbricks > 0 && (!cells || !bricks || !phi0_split || !vel || !phi || !phi_split))
+    FAIL(DCELL_ERR_ARG, "cells, bricks, phi0_split, vel, phi and phi_split are required");
+  if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+  return launch_batch_brick(cells, bricks, nbricks, phi0_split, vel, backtrace, phi, phi_split, flags,
+                            (cudaStream_t)stream);
+}
+
 DCELL_API int dcell_tc_gemm_check(const float *a, float *d, int *flags, void *stream) {
   if (!a || !d) FAIL(DCELL_ERR_ARG, "a and d are required");
   return launch_tc_gemm_check(a, d, flags, (cudaStream_t)stream);

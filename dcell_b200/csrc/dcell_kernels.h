@@ -14,6 +14,8 @@ int launch_sl_tc(const dcell::Geom &g, const float *phi0, const float *vel, doub
                  long long npts, int backtrace, float *phi, int *flags, cudaStream_t st);
 
 int launch_split_bf16(const float *phi, uint32_t *out, long long n, cudaStream_t st);
+int launch_batch_brick(const dcell_cell *cells, const dcell_tile *bricks, int nbricks, const uint32_t *phi0s,
+                       const float *vel, int backtrace, float *phi, uint32_t *phis, int *flags, cudaStream_t st);
 // One z-slab of the dense split-state tensor-core step: z bricks [bz0, bz0 +
 // nbz) of tc_slab_planes() planes each, gated on max |w| (FP32 bits at
 // gate_maxw) * dt / h_z <= gate_limit.

@@ -942,6 +942,277 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
   if (warp == 0) tmem_dealloc(c.tmem, S::TmemCols);
 }
 
+// Batched split-state stepper over the bricks of many cells (cells of uneven
+// sizes in one persistent launch).  Same bricks, step loop and arithmetic as
+// sl_tc_brick_kernel, hence per cell the bits of dcell_sl_step_tc_split.
+// The cells' rows have arbitrary lengths and offsets in the packed arrays,
+// which TMA's 16-byte strides do not admit, so the compute warps stage the
+// boxes themselves with 4-byte cp.async copies from source indices clamped to
+// the cell: the edge replication that zero fill + replicate_pass gives the
+// dense kernel.  Double-buffered as there: brick m lands in buffer m & 1;
+// its copies are issued when brick m-2 has been read for the last time and
+// complete on staged[m & 1] (each thread's copies arrive with
+// cp.async.mbarrier.arrive.noinc), which the first departure of brick m waits
+// for; freed[m & 1] collects the compute threads after brick m's last step.
+// The issuer warp only issues MMAs.  Every wait is bounded.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// one brick of a cell and the cell's grid
+struct CellBrick {
+  Geom g;         // the cell's grid, origin 0
+  long long off;  // the cell's first point in the packed arrays
+  float dth[3], hdth[3];
+  int x0, y0, z0;
+};
+
+__device__ __forceinline__ CellBrick cell_brick(const dcell_cell *__restrict__ cells,
+                                                const dcell_tile *__restrict__ bricks, int b) {
+  const dcell_tile T = bricks[b];
+  const dcell_cell C = cells[T.cell];
+  CellBrick r;
+  r.g.nx = C.n[0];
+  r.g.ny = C.n[1];
+  r.g.nz = C.n[2];
+  r.g.px = r.g.py = r.g.pz = 0;
+  r.g.hx = C.h[0];
+  r.g.hy = C.h[1];
+  r.g.hz = C.h[2];
+  r.off = C.offset;
+  const float dt = (float)C.dt;  // the rounding of the single-grid launch
+  r.dth[0] = dt / (float)C.h[0];
+  r.dth[1] = dt / (float)C.h[1];
+  r.dth[2] = dt / (float)C.h[2];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) r.hdth[a] = -0.5f * r.dth[a];
+  r.x0 = T.x0;
+  r.y0 = T.y0;
+  r.z0 = T.z0;
+  return r;
+}
+
+// A compute thread's share of brick B's two boxes into buf (rows spread over
+// the four compute warps, lanes along a row), then its arrival on `bar` once
+// its copies have landed.
+template <class S>
+__device__ __forceinline__ void stage_brick(uint8_t *buf, const CellBrick &B, const uint32_t *__restrict__ phi0s,
+                                            const float *__restrict__ vel, int warp, int lane, uint64_t *bar) {
+  const int nx = B.g.nx, ny = B.g.ny, nz = B.g.nz;
+  const uint32_t *ps = phi0s + B.off;
+  const float *vs = vel + 3 * B.off;
+  uint32_t *pb = reinterpret_cast<uint32_t *>(buf);
+  float *vb = reinterpret_cast<float *>(buf + S::PhiBytes);
+  for (int r = warp; r < S::PY * S::PZ; r += 4) {
+    const int gy = min(max(B.y0 - 2 + r % S::PY, 0), ny - 1), gz = min(max(B.z0 - 2 + r / S::PY, 0), nz - 1);
+    const uint32_t *src = ps + ((long long)gz * ny + gy) * nx;
+    for (int x = lane; x < S::PX; x += 32) cp_async4(pb + r * S::PX + x, src + min(max(B.x0 - 4 + x, 0), nx - 1));
+  }
+  for (int r = warp; r < S::VY * S::VZ; r += 4) {
+    const int gy = min(max(B.y0 - 1 + r % S::VY, 0), ny - 1), gz = min(max(B.z0 - 1 + r / S::VY, 0), nz - 1);
+    const float *src = vs + ((long long)gz * ny + gy) * nx * 3;
+    for (int c = lane; c < 3 * S::VX; c += 32) {
+      const int x = c / 3;
+      cp_async4(vb + r * 3 * S::VX + c, src + 3 * min(max(B.x0 - 4 + x, 0), nx - 1) + (c - 3 * x));
+    }
+  }
+  cp_async_arrive(bar);
+}
+
+template <int BT>
+__global__ void __launch_bounds__(kBrickThreads, BrickShape<2>::CtasPerSm)
+    batch_brick_kernel(const dcell_cell *__restrict__ cells, const dcell_tile *__restrict__ bricks, int nbricks,
+                       const uint32_t *__restrict__ phi0s, const float *__restrict__ vel, float *__restrict__ phi,
+                       uint32_t *__restrict__ phis, int *flags) {
+  constexpr int P = 2;
+  using S = BrickShape<P>;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sB = smem;
+  uint8_t *const buf0 = smem + kBBytes, *const buf1 = smem + kBBytes + S::BufBytes;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kBBytes + 2 * S::BufBytes);
+  uint64_t *const unused = bars + 0;  // setup() initialises one MMA barrier; this kernel uses its own
+  uint64_t *const afull = bars + 1, *const dfull = bars + 2, *const staged = bars + 3, *const freed = bars + 5;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 7);
+  if (threadIdx.x == 0) {
+    mbar_init(afull, 4);
+    mbar_init(dfull, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&staged[b], kTile);
+      mbar_init(&freed[b], kTile);
+    }
+  }
+  Ctx c;
+  setup(sB, unused, tmem_slot, c, S::TmemCols);  // B operand, TMEM; ends with a CTA barrier
+
+  const int nmine = (int)blockIdx.x < nbricks ? (nbricks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int nsteps = 4 * nmine;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool err = false;
+
+  if (warp == 4) {  // ---------------- issuer ----------------
+    if (lane == 0) {
+      int mma_issued = 0;
+      constexpr uint32_t idesc = instr_desc_bf16(kTile, kCoef);
+      for (int j = 0; j < nsteps && !err; ++j) {
+        if (!mbar_wait(afull, (uint32_t)j & 1u)) { err = true; break; }
+        fence_after();
+#pragma unroll
+        for (int st = 0; st < P; ++st)
+#pragma unroll
+          for (int kk = 0; kk < kK / 16; ++kk)
+            mma_bf16(c.tmem + 128 * st + 64, c.tmem + 128 * st + (uint32_t)(kk * 8),
+                     c.bdesc + (uint64_t)((kk * 256) >> 4), idesc, kk > 0 ? 1u : 0u);
+        mma_commit(dfull);
+        ++mma_issued;
+      }
+      bool ok = true;
+      if (mma_issued) ok &= mbar_wait(dfull, (uint32_t)(mma_issued - 1) & 1u);
+      if (err || !ok) raise_flag(flags, FLAG_WAIT_TIMEOUT);
+    }
+  } else {  // ---------------- compute warps ----------------
+    const int lx = lane, ly = warp;
+    auto brick = [&](int k) { return cell_brick(cells, bricks, (int)blockIdx.x + k * (int)gridDim.x); };
+    auto buffer = [&](int k) { return k & 1 ? buf1 : buf0; };
+    // brick k staged (bounded wait)
+    auto landed = [&](int k) -> bool { return mbar_wait_sleep(&staged[k & 1], (uint32_t)(k >> 1) & 1u); };
+    auto depart = [&](int j, const CellBrick &B, float f[P][3], int soff[P]) -> bool {
+      const float *vbox = reinterpret_cast<const float *>(buffer(j >> 2) + S::PhiBytes);
+      const int x = min(B.x0 + lx, B.g.nx - 1), y = min(B.y0 + ly, B.g.ny - 1);
+      const int zl = P * (j & 3);
+      const bool in = brick_depart<BT, S, P>(vbox, x - B.x0 + 4, y - B.y0 + 1, zl + 1, x - B.x0 + 4, y - B.y0 + 2,
+                                             zl + 2, B.dth, B.hdth, f, soff);
+      return __all_sync(0xffffffffu, in);
+    };
+    if (nmine > 0) stage_brick<S>(buf0, brick(0), phi0s, vel, warp, lane, &staged[0]);
+    if (nmine > 1) stage_brick<S>(buf1, brick(1), phi0s, vel, warp, lane, &staged[1]);
+    CellBrick B;
+    float f[P][3];
+    int soff[P];
+    bool boxed = true;
+    if (nsteps > 0) {
+      B = brick(0);
+      if (!landed(0)) err = true;
+      if (__any_sync(0xffffffffu, err)) err = true;
+      else boxed = depart(0, B, f, soff);
+    }
+    for (int j = 0; j < nsteps && !err; ++j) {
+      const int k = j >> 2;
+      const uint32_t *ps = phi0s + B.off;
+      const float *vs = vel + 3 * B.off;
+      // a: A rows of the P points into their stages, then this warp's arrival
+      bool stacked = boxed;
+#pragma unroll
+      for (int p = 1; p < P; ++p) stacked = stacked && soff[p] == soff[0] + p * S::PX * S::PY;
+      if (__all_sync(0xffffffffu, stacked)) {
+        const uint32_t *q = reinterpret_cast<const uint32_t *>(buffer(k)) + soff[0];
+        uint32_t v[16 * (P + 3)];
+#pragma unroll
+        for (int e = 0; e < 16 * (P + 3); ++e) v[e] = q[((e >> 4) * S::PY + ((e >> 2) & 3)) * S::PX + (e & 3)];
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+          for (int q16 = 0; q16 < 4; ++q16) tmem_st16(c.tmem + c.lane_off + 128 * p + 16 * q16, v + 16 * (p + q16));
+      } else {
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          if (boxed) {
+            uint32_t w[64];
+            const uint32_t *q = reinterpret_cast<const uint32_t *>(buffer(k)) + soff[p];
+#pragma unroll
+            for (int e = 0; e < 64; ++e) w[e] = q[((e >> 4) * S::PY + ((e >> 2) & 3)) * S::PX + (e & 3)];
+            __syncwarp();
+            tmem_st32(c.tmem + c.lane_off + 128 * p, w);
+            tmem_st32(c.tmem + c.lane_off + 128 * p + 32, w + 32);
+          } else {  // the warp left its boxes: departure and gathers from global memory
+            const int x = min(B.x0 + lx, B.g.nx - 1), y = min(B.y0 + ly, B.g.ny - 1);
+            const int z = min(B.z0 + P * (j & 3) + p, B.g.nz - 1);
+            const float3 r = brick_rows_global(B.g, ps, vs, B.dth[0], B.dth[1], B.dth[2], BT, x, y, z,
+                                               c.tmem + c.lane_off + 128 * p);
+            f[p][0] = r.x;
+            f[p][1] = r.y;
+            f[p][2] = r.z;
+          }
+        }
+      }
+      tmem_wait_st();
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(afull);
+      // b: next step's departures while the tensor core works
+      CellBrick Bn = B;
+      float fn[P][3];
+      int soffn[P];
+      bool boxedn = true;
+      if (j + 1 < nsteps) {
+        if (((j + 1) & 3) == 0) {  // brick k+1: staged?
+          Bn = brick(k + 1);
+          if (!landed(k + 1)) err = true;
+        }
+        if (__any_sync(0xffffffffu, err)) err = true;
+        else boxedn = depart(j + 1, Bn, fn, soffn);
+      }
+      // c: coefficients -> values, two points at a time
+      const int x = min(B.x0 + lx, B.g.nx - 1), y = min(B.y0 + ly, B.g.ny - 1);
+      const bool xy_valid = B.x0 + lx < B.g.nx && B.y0 + ly < B.g.ny;
+      const int zr = B.z0 + P * (j & 3);
+      const int plane = B.g.nx * B.g.ny;
+      const long long p0 = B.off + ((long long)min(zr, B.g.nz - 1) * B.g.ny + y) * B.g.nx + x;
+      const bool ok = mbar_wait_sleep(dfull, (uint32_t)j & 1u);
+      if (__any_sync(0xffffffffu, !ok)) { err = true; break; }
+      fence_after();
+      {
+        float ca[64], cb[64];
+        tmem_ld32(c.tmem + c.lane_off + 64, reinterpret_cast<uint32_t *>(ca));
+        tmem_ld32(c.tmem + c.lane_off + 128 + 64, reinterpret_cast<uint32_t *>(cb));
+        tmem_ld32(c.tmem + c.lane_off + 96, reinterpret_cast<uint32_t *>(ca + 32));
+        tmem_ld32(c.tmem + c.lane_off + 128 + 96, reinterpret_cast<uint32_t *>(cb + 32));
+        tmem_wait_ld();
+        float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
+#pragma unroll
+        for (int kz = 3; kz >= 0; --kz) {
+          va = fmaf(va, f[0][2], horner_slice(ca + 16 * kz, f[0]));
+          vb = fmaf(vb, f[1][2], horner_slice(cb + 16 * kz, f[1]));
+        }
+        if (xy_valid && zr < B.g.nz) {
+          phi[p0] = va;
+          phis[p0] = pack_split(va);
+        }
+        if (xy_valid && zr + 1 < B.g.nz) {
+          phi[p0 + plane] = vb;
+          phis[p0 + plane] = pack_split(vb);
+        }
+      }
+      fence_before();
+      if ((j & 3) == 3) {  // brick k read for the last time: its buffer takes brick k+2
+        mbar_arrive(&freed[k & 1]);
+        if (k + 2 < nmine) {
+          if (!mbar_wait_sleep(&freed[k & 1], (uint32_t)(k >> 1) & 1u)) err = true;
+          if (__any_sync(0xffffffffu, err)) { err = true; break; }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the reads above before the copies
+          stage_brick<S>(buffer(k), brick(k + 2), phi0s, vel, warp, lane, &staged[k & 1]);
+        }
+      }
+      B = Bn;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        f[p][0] = fn[p][0]; f[p][1] = fn[p][1]; f[p][2] = fn[p][2];
+        soff[p] = soffn[p];
+      }
+      boxed = boxedn;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy may land after the CTA is gone
+    if (err) raise_flag(flags, FLAG_WAIT_TIMEOUT);
+  }
+  __syncwarp();  // the issuer warp's other lanes wait here for lane 0
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0) tmem_dealloc(c.tmem, S::TmemCols);
+}
+
 // Batched cells: a persistent CTA walks a packed queue of 128-point tiles
 // (tx x ty x tz boxes of one cell's grid) over many uneven cell grids.
 __global__ void __launch_bounds__(kTile, 4) batch_tc_kernel(const dcell_cell *__restrict__ cells,
@@ -1079,6 +1350,27 @@ int launch_batch_tc(const dcell_cell *cells, const dcell_tile *tiles, int ntiles
   const int grid = per * sms < ntiles ? per * sms : ntiles;
   tc::batch_tc_kernel<<<grid, tc::kTile, tc::kDynSmem, st>>>(cells, tiles, ntiles, tx, ty, phi0, vel, backtrace, phi,
                                                             flags);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_batch_brick(const dcell_cell *cells, const dcell_tile *bricks, int nbricks, const uint32_t *phi0s,
+                       const float *vel, int backtrace, float *phi, uint32_t *phis, int *flags, cudaStream_t st) {
+  using S = tc::BrickShape<2>;
+  static bool configured = false;
+  if (!configured) {
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::batch_brick_kernel<DCELL_EULER>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, S::DynSmem));
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::batch_brick_kernel<DCELL_MIDPOINT>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, S::DynSmem));
+    configured = true;
+  }
+  if (nbricks <= 0) return DCELL_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = S::CtasPerSm * sms < nbricks ? S::CtasPerSm * sms : nbricks;
+  auto kern = backtrace == DCELL_MIDPOINT ? tc::batch_brick_kernel<DCELL_MIDPOINT> : tc::batch_brick_kernel<DCELL_EULER>;
+  kern<<<grid, tc::kBrickThreads, S::DynSmem, st>>>(cells, bricks, nbricks, phi0s, vel, phi, phis, flags);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 

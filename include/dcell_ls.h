@@ -364,6 +364,19 @@ DCELL_API int dcell_batch_sl_step(const dcell_cell *cells, int ncells, const dce
                                   int ty, int tz, int ctas_per_sm, const float *phi0, const float *vel, float *phi,
                                   int interp, int backtrace, int *flags, void *stream);
 
+/* The split-state tensor-core step (dcell_sl_step_tc_split) of every cell
+ * of a batch in ONE persistent launch over bricks of 32 x 4 x 8 points:
+ * bricks = dcell_batch_plan(cells, ncells, 32, 4, 8, ...) as a device array;
+ * phi0_split (packed split words), vel, phi and phi_split (the next step's
+ * input) packed as for dcell_batch_sl_step.  Every cell gets the bits
+ * dcell_sl_step_tc_split gives it alone (cells of any shape: the brick boxes
+ * are staged with copies clamped to the cell, the edge replication of the
+ * single-grid kernel).  3D cells, FP32. */
+DCELL_API int dcell_batch_sl_step_tc_split(const dcell_cell *cells, int ncells, const dcell_tile *bricks,
+                                           int nbricks, const unsigned int *phi0_split, const float *vel,
+                                           int backtrace, float *phi, unsigned int *phi_split, int *flags,
+                                           void *stream);
+
 /* One explicit first-order conservative upwind step of phi on MAC faces:
  * LevelSetAdvectMAC (2D) / LevelSetAdvectMAC_3D, LevelSetMethod/AdvectMAC.c:
  * 18-111 (replaces them; the reference routines read the level set's grid

@@ -97,3 +97,31 @@ def test_autotune_and_graph_replay(cuda):
         x, y = y, x
     torch.cuda.synchronize()
     assert torch.equal(out, x)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("backtrace", ["midpoint", "euler"])
+def test_batched_split_bricks_equal_per_cell_split_steps(cuda, backtrace):
+    """The batched split-state brick kernel (cp.async-staged boxes clamped to
+    each cell) gives every cell the bits of dcell_sl_step_tc_split on that
+    cell alone -- cells narrower, shorter and shallower than a brick box,
+    widths not a multiple of 4, and cells the brick kernel of the single-grid
+    path would take -- over three consecutive steps, also at 3x the CFL (the
+    global fallback)."""
+    from dcell_b200.batch import CellBatch, c4_workload
+    phis, vels, hs, dt = c4_workload(ncells=10, emin=5, emax=70, seed=11, device=cuda)
+    shapes = [tuple(p.shape) for p in phis]
+    assert any(s[2] % 4 for s in shapes) and any(min(s) < 12 for s in shapes)
+    for scale in (1.0, 3.0):
+        b = CellBatch(phis, vels, hs, [d * scale for d in dt] if np.ndim(dt) else dt * scale, device=cuda)
+        s0 = b.split()
+        a_phi, a_s = torch.empty_like(b.phi), torch.empty_like(s0)
+        c_phi, c_s = torch.empty_like(b.phi), torch.empty_like(s0)
+        xa, xc = s0.clone(), s0.clone()
+        for _ in range(3):
+            b.step_tc_split(xa, a_phi, a_s, backtrace)
+            b.step_tc_split_per_cell(xc, c_phi, c_s, backtrace)
+            torch.cuda.synchronize()
+            assert torch.equal(a_phi, c_phi)
+            assert torch.equal(a_s, c_s)
+            xa, xc = a_s.clone(), c_s.clone()
