@@ -17,6 +17,7 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "dcell_common.cuh"
@@ -485,10 +486,13 @@ template <typename T, int DIM>
 __global__ void __launch_bounds__(256, 3) ortho_kernel(Geom g, const T *__restrict__ phi,
                                                     dcell_irregular_node *__restrict__ nodes,
                                                     const int *__restrict__ count, int cap) {
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int n = min(*count, cap);
+  // a block-uniform loop over the nodes written (the launch is sized for the capacity)
+  for (long long base = blockIdx.x * (long long)blockDim.x; base < 8LL * n;
+       base += (long long)gridDim.x * blockDim.x) {
+  const long long tid = base + threadIdx.x;
   const long long node = tid >> 3;
   const int sub = (int)(tid & 7);
-  const int n = min(*count, cap);
   const bool active = node < n && nodes[node].axis == -1 && (DIM == 3 || sub < 4);
   const T TOL = T(1e-3), TOL2 = TOL * TOL;
   const double BIG = 1.7976931348623157e308;
@@ -562,7 +566,7 @@ __global__ void __launch_bounds__(256, 3) ortho_kernel(Geom g, const T *__restri
   T w0 = __shfl_sync(0xffffffffu, res[0], best, 8);
   T w1 = __shfl_sync(0xffffffffu, res[1], best, 8);
   T w2 = __shfl_sync(0xffffffffu, res[2], best, 8);
-  if (!active || sub != 0) return;
+  if (!active || sub != 0) continue;
   T op[3] = {w0, w1, w2};
   if (DIM == 3) {
     if (bd == BIG) {  // no sub-cell converged: quadratic, then linear fallback
@@ -585,29 +589,72 @@ __global__ void __launch_bounds__(256, 3) ortho_kernel(Geom g, const T *__restri
   r.X[0] = (double)((T)ci + op[0]);
   r.X[1] = (double)((T)cj + op[1]);
   r.X[2] = DIM == 3 ? (double)((T)ck + op[2]) : 0.0;
+  }
 }
 
-// Normal and curvature at node X (IIM/SurfaceQuantities.c 2D:48-56, 3D:83-89,111).
+// Normal and curvature at node X (IIM/SurfaceQuantities.c 2D:48-56, 3D:83-89,111):
+// Bilinear3D / Bilinear2D samples of the gradient components and of the
+// curvature grid function.  8 lanes per node, lane c = trilinear corner c in
+// the reference's loop order (i, j, k nested; 2D: 4 lanes, x then y); each
+// lane forms its corner's terms exactly as Bilinear3D does, and the node's
+// first lane sums them in corner order -- the reference's bits, with the
+// corners' divisions and square roots spread over the lanes.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(128) surface_kernel(Geom g, const T *__restrict__ phi,
                                                       dcell_irregular_node *__restrict__ nodes,
                                                       const int *__restrict__ count, int cap) {
-  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  constexpr int NC = DIM == 3 ? 8 : 4;  // corners
   const int n = min(*count, cap);
-  if (q >= n) return;
-  dcell_irregular_node &r = nodes[q];
-  const T X[3] = {(T)r.X[0], (T)r.X[1], (T)r.X[2]};
-  if (DIM == 2) {
-    const T nx = sample_gf<T, 2>(g, phi, 1, X), ny = sample_gf<T, 2>(g, phi, 2, X);
-    const T h = sqrt(nx * nx + ny * ny);
-    r.n[0] = (double)(nx / h); r.n[1] = (double)(ny / h); r.n[2] = 0.0;
-    r.k = (double)sample_gf<T, 2>(g, phi, 4, X);
-  } else {
-    T nx = sample_gf<T, 3>(g, phi, 1, X), ny = sample_gf<T, 3>(g, phi, 2, X), nz = sample_gf<T, 3>(g, phi, 3, X);
-    const T h = sqrt(nx * nx + ny * ny + nz * nz);
-    nx /= h; ny /= h; nz /= h;
-    r.n[0] = (double)nx; r.n[1] = (double)ny; r.n[2] = (double)nz;
-    r.k = (double)sample_gf<T, 3>(g, phi, 4, X);
+  const T dx = (T)g.hx, dy = (T)g.hy, dz = (T)g.hz;
+  for (long long base = blockIdx.x * (long long)blockDim.x; base < 8LL * n;
+       base += (long long)gridDim.x * blockDim.x) {
+    const long long tid = base + threadIdx.x;
+    const long long q = tid >> 3;
+    const int c = (int)(tid & 7);
+    const bool active = q < n;
+    T t[4] = {0, 0, 0, 0};  // this corner's terms of d/dx, d/dy, d/dz, curvature
+    if (active && c < NC) {
+      const dcell_irregular_node &r = nodes[q];
+      const T X[3] = {(T)r.X[0], (T)r.X[1], (T)r.X[2]};
+      if (DIM == 3) {
+        const int xs = (int)floor(X[0]), ys = (int)floor(X[1]), zs = (int)floor(X[2]);
+        const T sx = X[0] - (T)xs, sy = X[1] - (T)ys, sz = X[2] - (T)zs;
+        const int i = c >> 2, j = (c >> 1) & 1, k = c & 1;
+        const T xb = (T)i * sx + (T)(1 - i) * (1 - sx);
+        const T yb = (T)j * sy + (T)(1 - j) * (1 - sy);
+        const T zb = (T)k * sz + (T)(1 - k) * (1 - sz);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) t[f] = gf3<T>(g, phi, f + 1, xs + i, ys + j, zs + k, dx, dy, dz) * xb * yb * zb;
+      } else {
+        const int xi = (int)floor(X[0]), yi = (int)floor(X[1]);
+        const T xf = (T(2.) * (X[0] - (T)xi) - T(1.)), yf = (T(2.) * (X[1] - (T)yi) - T(1.));
+        const int k = c >> 1, l = c & 1;
+        const T xb = T(1.) + (T(2.) * (T)k - T(1.)) * xf;
+        const T yb = T(1.) + (T(2.) * (T)l - T(1.)) * yf;
+        t[0] = gf2<T>(g, phi, 1, xi + k, yi + l, dx, dy) * xb * yb;
+        t[1] = gf2<T>(g, phi, 2, xi + k, yi + l, dx, dy) * xb * yb;
+        t[3] = gf2<T>(g, phi, 4, xi + k, yi + l, dx, dy) * xb * yb;
+      }
+    }
+    T sum[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+#pragma unroll
+      for (int e = 0; e < NC; ++e) sum[f] += __shfl_sync(0xffffffffu, t[f], e, 8);
+    if (!active || c != 0) continue;
+    dcell_irregular_node &r = nodes[q];
+    if (DIM == 2) {
+      const T nx = sum[0] / T(4.), ny = sum[1] / T(4.);
+      const T h = sqrt(nx * nx + ny * ny);
+      r.n[0] = (double)(nx / h); r.n[1] = (double)(ny / h); r.n[2] = 0.0;
+      r.k = (double)(sum[3] / T(4.));
+    } else {
+      T nx = sum[0], ny = sum[1], nz = sum[2];
+      const T h = sqrt(nx * nx + ny * ny + nz * nz);
+      nx /= h; ny /= h; nz /= h;
+      r.n[0] = (double)nx; r.n[1] = (double)ny; r.n[2] = (double)nz;
+      r.k = (double)sum[3];
+    }
   }
 }
 
@@ -1160,9 +1207,13 @@ static void irr_launch(const Geom &g, const T *phi, const int *band, int nband, 
   scan_add_kernel<<<nblk, SCAN_BLOCK, 0, st>>>(offsets, nband, partial, nblk, count, cap, flags);
   irr_write_kernel<T, DIM><<<(nband + 255) / 256, 256, 0, st>>>(g, phi, band, nband, offsets, nodes, cap);
   // projection nodes: 8 threads each; bounded by the capacity
+  // the node count is on the device: grids sized for the capacity, capped,
+  // and the kernels loop over the nodes actually written
   const long long nthreads = 8LL * cap;
-  ortho_kernel<T, DIM><<<(int)((nthreads + 255) / 256), 256, 0, st>>>(g, phi, nodes, count, cap);
-  if (with_surface) surface_kernel<T, DIM><<<(cap + 127) / 128, 128, 0, st>>>(g, phi, nodes, count, cap);
+  const int ob = (int)std::min<long long>((nthreads + 255) / 256, 148LL * 24);
+  const int sb = (int)std::min<long long>((nthreads + 127) / 128, 148LL * 48);
+  ortho_kernel<T, DIM><<<ob < 1 ? 1 : ob, 256, 0, st>>>(g, phi, nodes, count, cap);
+  if (with_surface) surface_kernel<T, DIM><<<sb < 1 ? 1 : sb, 128, 0, st>>>(g, phi, nodes, count, cap);
 }
 
 int launch_irregular(const Geom &g, int dtype, const void *phi, const int *band, int nband, int with_surface,
