@@ -10,7 +10,7 @@ Two libraries sit behind this module:
   tree was available at build time.  ``oracle.reference`` wraps it.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
-leg may use this package, and only as the checker / the timed CPU baseline.
+leg may use this package, and only to check results / as the timed CPU baseline.
 The product path (``dcell_b200``) never imports it.
 
 Array conventions: phi is (nz, ny, nx) or (ny, nx) float64, x fastest;

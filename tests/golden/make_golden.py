@@ -2,7 +2,7 @@
 
 Runs the reference's level-set C (compiled by ``make -C oracle ref`` from the
 reference tree against oracle/shim) on small seeded inputs and stores inputs
-and outputs as .npz.  The fixtures let the GPU box, where the reference tree
+and outputs as .npz.  The fixtures let a GPU machine, where the reference tree
 is absent, pin both the oracle and the CUDA path to the reference.
 
 All inputs are FP32-representable (stored as float32; widen to float64

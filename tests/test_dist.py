@@ -1,7 +1,7 @@
 """Multi-process host logic of the multi-GPU path on CPU (gloo, world size 2):
 z-slab decomposition with halo exchange, cells over ranks with all-reduced
 diagnostics, and a peer that dies between steps.  The per-slab step is the
-CPU oracle here (the checker); on GPUs it is the CUDA kernel over NCCL."""
+CPU oracle here; on GPUs it is the CUDA kernel over NCCL."""
 import datetime
 import os
 import socket
