@@ -113,6 +113,26 @@ def run_c2(N=128, dev="cuda", T=3.0):
         res[name] = {"return_error_vs_initial": _band_err(a, phi0, h), "ms": e0.elapsed_time(e1),
                      "volume_loss_rel": (v0 - float(L.volume(a, h, 1.5 * h))) / v0}
         finals[name] = a
+    # the split-state stepper of the dense benchmark: phi carried between
+    # steps as packed BF16 hi/lo words (fp32_tc splits the FP32 field inside
+    # every step instead)
+    v = vel.float().contiguous()
+    spl = [L.split_bf16(phi0.float().contiguous()), None]
+    spl[1] = torch.empty_like(spl[0])
+    outs = [torch.empty(phi0.shape, dtype=torch.float32, device=phi0.device) for _ in range(2)]
+    a = None
+    e0, e1 = _events()
+    e0.record()
+    for s in range(steps):
+        fac = math.cos(math.pi * (s + 0.5) * dt / T)
+        a, _ = L.sl_step_tc_split(spl[s & 1], v, dt * fac, h, backtrace="midpoint", out=outs[s & 1],
+                                  out_split=spl[(s + 1) & 1])
+    e1.record()
+    torch.cuda.synchronize()
+    v0 = float(L.volume(phi0, h, 1.5 * h))
+    res["fp32_tc_split_state"] = {"return_error_vs_initial": _band_err(a, phi0, h), "ms": e0.elapsed_time(e1),
+                                  "volume_loss_rel": (v0 - float(L.volume(a, h, 1.5 * h))) / v0,
+                                  "vs_fp64_gpu": _band_err(a, finals["fp64_gpu"], h)}
     res["fp32_plain_vs_fp64_gpu"] = _band_err(finals["fp32_plain"], finals["fp64_gpu"], h)
     res["fp32_tc_vs_fp64_gpu"] = _band_err(finals["fp32_tc"], finals["fp64_gpu"], h)
     return res
