@@ -219,8 +219,10 @@ __device__ __forceinline__ void setup(uint8_t *sB, uint64_t *bar, uint32_t *tmem
 // entry: K = 2j low half, K = 2j + 1 high half).
 __device__ __forceinline__ uint32_t pack_split(float v) {
   const __nv_bfloat16 h = __float2bfloat16_rn(v);
-  const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
-  return (uint32_t)__bfloat16_as_ushort(h) | ((uint32_t)__bfloat16_as_ushort(l) << 16);
+  const float r = v - __bfloat162float(h);
+  uint32_t w;  // one paired conversion: RN_bf16(r) to the high half, RN_bf16(v) = h to the low half
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(w) : "f"(r), "f"(v));
+  return w;
 }
 
 // A (this lane: 64 packed words) -> TMEM, barrier, MMA by thread 0 with its
@@ -614,10 +616,12 @@ __device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int
         // Along a component's own (staggered) axis the midpoint lies in
         // [X, X+1): floor 0, fraction t.  Across the other two axes the
         // node-centred fraction and floor serve both other components.
+        // Where the result is used (|dl| < 0.5: `near`) floor(t) is -1 or 0,
+        // so a sign test gives the floor and t - floor(t) is t + 1 or t.
         const float t = dl + 0.f;
-        const float fl = floorf(t);
-        sn[p][a] = t - fl;
-        on[p][a] = min(max((int)fl, -1), 0) * ST[a];
+        const bool ng = t < 0.f;
+        sn[p][a] = ng ? t + 1.f : t;
+        on[p][a] = ng ? -ST[a] : 0;
         sp[p][a] = dl + 0.5f;
       }
     bool same = true;
