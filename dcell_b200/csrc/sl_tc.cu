@@ -679,6 +679,23 @@ __device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int
   return in;
 }
 
+// wait::ld that also ties the 64 registers it completes (a[0..32), b[0..32))
+// to the wait, so that no use of them is scheduled before it
+__device__ __forceinline__ void tmem_wait_ld_tied(float *a, float *b) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               :
+                 "+f"(a[0]), "+f"(a[1]), "+f"(a[2]), "+f"(a[3]), "+f"(a[4]), "+f"(a[5]), "+f"(a[6]), "+f"(a[7]),
+                 "+f"(a[8]), "+f"(a[9]), "+f"(a[10]), "+f"(a[11]), "+f"(a[12]), "+f"(a[13]), "+f"(a[14]), "+f"(a[15]),
+                 "+f"(a[16]), "+f"(a[17]), "+f"(a[18]), "+f"(a[19]), "+f"(a[20]), "+f"(a[21]), "+f"(a[22]), "+f"(a[23]),
+                 "+f"(a[24]), "+f"(a[25]), "+f"(a[26]), "+f"(a[27]), "+f"(a[28]), "+f"(a[29]), "+f"(a[30]), "+f"(a[31]),
+                 "+f"(b[0]), "+f"(b[1]), "+f"(b[2]), "+f"(b[3]), "+f"(b[4]), "+f"(b[5]), "+f"(b[6]), "+f"(b[7]),
+                 "+f"(b[8]), "+f"(b[9]), "+f"(b[10]), "+f"(b[11]), "+f"(b[12]), "+f"(b[13]), "+f"(b[14]), "+f"(b[15]),
+                 "+f"(b[16]), "+f"(b[17]), "+f"(b[18]), "+f"(b[19]), "+f"(b[20]), "+f"(b[21]), "+f"(b[22]), "+f"(b[23]),
+                 "+f"(b[24]), "+f"(b[25]), "+f"(b[26]), "+f"(b[27]), "+f"(b[28]), "+f"(b[29]), "+f"(b[30]), "+f"(b[31])
+               :
+               : "memory");
+}
+
 // Dense-grid stepper over TMA-staged bricks.
 //
 // Each CTA owns bricks blockIdx.x, blockIdx.x + gridDim.x, ... (32 x 4 x 4P
@@ -908,14 +925,20 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
       for (int pp = 0; pp < P; pp += 2) {
         // both points' 64 coefficients in one TMEM load round
         float ca[64], cb[64];
-        tmem_ld32(c.tmem + c.lane_off + 128 * pp + 64, reinterpret_cast<uint32_t *>(ca));
-        tmem_ld32(c.tmem + c.lane_off + 128 * (pp + 1) + 64, reinterpret_cast<uint32_t *>(cb));
         tmem_ld32(c.tmem + c.lane_off + 128 * pp + 96, reinterpret_cast<uint32_t *>(ca + 32));
         tmem_ld32(c.tmem + c.lane_off + 128 * (pp + 1) + 96, reinterpret_cast<uint32_t *>(cb + 32));
-        tmem_wait_ld();
+        tmem_wait_ld_tied(ca + 32, cb + 32);
+        tmem_ld32(c.tmem + c.lane_off + 128 * pp + 64, reinterpret_cast<uint32_t *>(ca));
+        tmem_ld32(c.tmem + c.lane_off + 128 * (pp + 1) + 64, reinterpret_cast<uint32_t *>(cb));
         float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
 #pragma unroll
-        for (int kz = 3; kz >= 0; --kz) {
+        for (int kz = 3; kz >= 2; --kz) {
+          va = fmaf(va, f[pp][2], horner_slice(ca + 16 * kz, f[pp]));
+          vb = fmaf(vb, f[pp + 1][2], horner_slice(cb + 16 * kz, f[pp + 1]));
+        }
+        tmem_wait_ld_tied(ca, cb);
+#pragma unroll
+        for (int kz = 1; kz >= 0; --kz) {
           va = fmaf(va, f[pp][2], horner_slice(ca + 16 * kz, f[pp]));
           vb = fmaf(vb, f[pp + 1][2], horner_slice(cb + 16 * kz, f[pp + 1]));
         }
