@@ -301,6 +301,52 @@ def reference_pls_step(phi, band, vel, parts, h, dt):
     return {"advect_s": t1 - t0, "correct_s": t2 - t1, "adjust_s": t3 - t2, "step_s": t3 - t0}, adv
 
 
+def reference_nodes(res, phi, band, rows64, h):
+    """The reference's own LevelSetUpdateIrregularNodeList_3D and surface
+    quantities (oracle/_ref, FP64, one core) on the same phi and band, timed,
+    with its node list compared to the GPU's FP64 rows."""
+    import numpy as np
+
+    from oracle import reference as R
+    if not R.available():
+        return
+    N = phi.shape[0]
+    ls = R.RefLevelSet.create(h, (0, 0, 0), (N, N, N))
+    ls.set_phi(phi)
+    ls.set_band(band)
+    t0 = time.perf_counter()
+    n = ls.update_irregular()
+    t1 = time.perf_counter()
+    ref = ls.nodes_no_update(n, surface=True)
+    t2 = time.perf_counter()
+    ls.close()
+    same = rows64.shape == ref.shape and bool(np.array_equal(rows64[:, :8], ref[:, :8]))
+    res["reference_cpu"] = {"node_list_s": t1 - t0, "surface_s": t2 - t1, "cores": 1, "kind": "reference",
+                            "nodes": int(n), "fp64_exact_fields_equal": same,
+                            "fp64_max_projection_diff": float(np.abs(rows64[:, 8:14] - ref[:, 8:14]).max())
+                            if same else None,
+                            "gpu_fp64_speedup": (t2 - t0) * 1e3 / res["fp64"]["ms"]}
+
+
+def reference_mac(res, phi, u, v, w, dt, h, got):
+    """The reference's own LevelSetAdvectMAC_3D (oracle/_ref, one core, timed)
+    on the FP64 inputs of the GPU leg, compared bit for bit with the GPU's
+    FP64 result; the oracle restatement is the checker where the reference
+    was not compiled."""
+    from oracle import reference as R
+    ref_ok = R.available()
+    t0 = time.perf_counter()
+    if ref_ok:
+        want = R.advect_mac(phi, u, v, w, dt, h)
+        t = time.perf_counter() - t0
+        res["reference_cpu"] = {"s": t, "cores": 1, "kind": "reference", "updates_per_s": res["points_updated"] / t}
+    else:
+        import oracle
+        want = oracle.advect_mac(phi, u, v, w, dt, h)
+    res["fp64_mismatches"] = int((got != want).sum())
+    res["fp64_checked_against"] = "reference" if ref_ok else "oracle"
+
+
 def e2e_rate(phi, vel, h, dt, K, torch):
     """Through the reference-facing C ABI with pinned FP64 host buffers
     (reference Grid layout): H2D of phi0 + velocity, TC step, D2H of phi,
@@ -367,18 +413,22 @@ def run_reference(args, rank, world):
     h, phi, vel, dt, _ = workload(args.size, "cpu")
     threads = os.cpu_count() or 1
     nplanes = 16
-    rates = []
+    times, npts = [], 0
     for s in range(args.warmup + args.steps):
         r, npts, t = cpu_oracle_rate(phi, vel, h, dt_at(s, dt), nplanes=nplanes, threads=threads)
         if s >= args.warmup:
-            rates.append(r)
-    value = statistics.median(rates)
-    n = args.size ** 3
+            times.append(t)
+    # a step is one bounded sample of the 256^3 step (nplanes z-planes):
+    # ms_per_step is the measured time of such a sample, value the rate over
+    # all timed samples
+    value = npts * len(times) / sum(times)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / value * 1e3, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(times) / len(times) * 1e3,
+            "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"sphere r=0.15 in LeVeque deformation, {args.size}^3, tricubic, midpoint SL",
-                       "sample": f"{nplanes} z-planes ({nplanes * args.size ** 2} points) per step"},
+                       "sample": f"{nplanes} z-planes ({nplanes * args.size ** 2} points) per step; "
+                                 "ms_per_step is the time of one such sample"},
             "cpu_baseline": {"value": value, "unit": "updates/s", "cores": threads, "kind": "port",
                              "sample": f"{nplanes} of {args.size} z-planes per step; the reference has no tricubic "
                                        "SL, so its FP64 restatement (oracle/sl_oracle.c) is timed"},
@@ -464,6 +514,13 @@ def main():
             "tc_over_plain_fp32": ms_pl / ms_tc,
             "tc_over_separable_fp32": ms_sep / ms_tc}
         line["accuracy"] = error_check(L, torch, phi, vel, h, dt)
+        if world == 1:
+            # the whole period of the field (t = 0 .. T): one-step error of the
+            # TC step at every step and the accumulated error at t = T, vs FP64
+            from dcell_b200.configs import run_c3
+            c3 = run_c3(args.size, dev=dev)
+            line["accuracy"]["period"] = {k: c3[k] for k in ("steps", "one_step_tc_vs_fp64",
+                                                             "tc_meets_1e-5_every_step", "accumulated", "wall_s")}
         # end to end on every rank at once (the ranks share the host's memory
         # and PCIe); the slowest rank's rate sets the job's
         if dist:
@@ -531,12 +588,16 @@ def main():
             line["io"] = run_io(args.size)
             # the irregular-node pass that follows the step (projections, normals, curvature)
             from dcell_b200.configs import run_nodes
-            line["irregular_nodes"] = run_nodes(args.size, dev=dev)
+            nres, ncase = run_nodes(args.size, dev=dev, return_fp64=True)
+            if world == 1:
+                reference_nodes(nres, *ncase, 1.0 / args.size)
+            line["irregular_nodes"] = nres
             # first-order upwind step on MAC faces (LevelSetAdvectMAC_3D), HBM-bound stencil
             from dcell_b200.configs import run_mac
-            m = run_mac(args.size, dev=dev)
+            m, mcase = run_mac(args.size, dev=dev, return_fp64=True)
             for k in ("fp32", "fp64"):
                 m[k]["frac"] = m[k]["achieved_gbs"] / hbm
+            reference_mac(m, *mcase)
             line["advect_mac"] = m
     if rank == 0:
         print(json.dumps(line), flush=True)

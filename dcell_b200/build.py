@@ -26,6 +26,12 @@ INCLUDE = os.path.join(os.path.dirname(PKG), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "-I", INCLUDE,
           "-I", CSRC, "--expt-relaxed-constexpr"]
+# Kernels that keep tcgen05.ld results in flight across other code (the
+# loaded registers are only valid after the tied tcgen05.wait::ld): the build
+# fails if ptxas spills any of their registers, since a spill store placed
+# between a load and its wait would save a register that is not yet written.
+NO_SPILL = {"sl_tc.cu": ["sl_tc_brick_kernel"]}
+
 UNITS = {
     "sl_exact.cu": ["-fmad=false"],
     "sl_cubic.cu": [],
@@ -52,6 +58,22 @@ def _stale(target, sources):
     return any(os.path.getmtime(s) > t for s in sources)
 
 
+def _spilling(ptxas_log, names):
+    """Kernels of `names` whose ptxas report shows spill stores or loads."""
+    bad, cur = [], None
+    for ln in ptxas_log.splitlines():
+        if "Compiling entry function" in ln:
+            cur = next((n for n in names if n in ln), None)
+        elif cur and "spill stores" in ln:
+            parts = ln.replace(",", "").split()
+            stores = int(parts[parts.index("spill") - 2])
+            loads = int(parts[parts.index("loads") - 3])
+            if stores or loads:
+                bad.append(cur)
+            cur = None
+    return sorted(set(bad))
+
+
 def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
     """Compile all translation units and link the shared library; returns its path."""
     os.makedirs(LIBDIR, exist_ok=True)
@@ -66,10 +88,21 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
         obj = os.path.join(objdir, unit.replace(".cu", ".o"))
         objs.append(obj)
         if force or _stale(obj, [src] + headers + [__file__]):
-            cmd = [cc] + ARCH + COMMON + extra + (["-Xptxas", "-v"] if ptxas_verbose else []) + ["-c", src, "-o", obj]
+            guard = NO_SPILL.get(unit)
+            cmd = [cc] + ARCH + COMMON + extra + (["-Xptxas", "-v"] if ptxas_verbose or guard else []) + \
+                ["-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            r = subprocess.run(cmd, stderr=subprocess.PIPE, text=True)
+            if ptxas_verbose or r.returncode:
+                sys.stderr.write(r.stderr)
+            if r.returncode:
+                raise subprocess.CalledProcessError(r.returncode, cmd)
+            if guard:
+                bad = _spilling(r.stderr, guard)
+                if bad:
+                    os.remove(obj)
+                    raise RuntimeError(f"{unit}: ptxas spilled registers of {', '.join(bad)}")
     if force or _stale(LIB, objs):
         cmd = [cc] + ARCH + ["-shared", "-cudart", "static", "-Xcompiler", "-fPIC", "-o", LIB] + objs
         if verbose:

@@ -147,30 +147,40 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t *v) {
 }
 #undef DCELL_R8
 
-#define DCELL_W8(b) "=r"(v[b + 0]), "=r"(v[b + 1]), "=r"(v[b + 2]), "=r"(v[b + 3]), "=r"(v[b + 4]), "=r"(v[b + 5]), \
-                    "=r"(v[b + 6]), "=r"(v[b + 7])
-// v[0..31] <- 32 consecutive 32-bit columns of this thread's lane
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *v) {
+#define DCELL_F8(b) "=f"(v[b + 0]), "=f"(v[b + 1]), "=f"(v[b + 2]), "=f"(v[b + 3]), "=f"(v[b + 4]), "=f"(v[b + 5]), \
+                    "=f"(v[b + 6]), "=f"(v[b + 7])
+// FP32 coefficients v[0..31] <- 32 consecutive columns of this thread's lane,
+// written straight into the float registers that a tied tcgen05.wait::ld
+// (tmem_wait_ld_tied) then completes: no copy of them sits between the load
+// and its wait
+__device__ __forceinline__ void tmem_ld32f(uint32_t taddr, float *v) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
       "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-      : DCELL_W8(0), DCELL_W8(8), DCELL_W8(16), DCELL_W8(24)
+      : DCELL_F8(0), DCELL_F8(8), DCELL_F8(16), DCELL_F8(24)
       : "r"(taddr)
       : "memory");
 }
-// v[0..15] <- 16 consecutive 32-bit columns of this thread's lane
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t *v) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : DCELL_W8(0), DCELL_W8(8)
-      : "r"(taddr)
-      : "memory");
+#undef DCELL_F8
+
+// wait::ld that also ties the 64 registers it completes (a[0..32), b[0..32))
+// to the wait, so that no use of them is scheduled before it
+__device__ __forceinline__ void tmem_wait_ld_tied(float *a, float *b) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               :
+                 "+f"(a[0]), "+f"(a[1]), "+f"(a[2]), "+f"(a[3]), "+f"(a[4]), "+f"(a[5]), "+f"(a[6]), "+f"(a[7]),
+                 "+f"(a[8]), "+f"(a[9]), "+f"(a[10]), "+f"(a[11]), "+f"(a[12]), "+f"(a[13]), "+f"(a[14]), "+f"(a[15]),
+                 "+f"(a[16]), "+f"(a[17]), "+f"(a[18]), "+f"(a[19]), "+f"(a[20]), "+f"(a[21]), "+f"(a[22]), "+f"(a[23]),
+                 "+f"(a[24]), "+f"(a[25]), "+f"(a[26]), "+f"(a[27]), "+f"(a[28]), "+f"(a[29]), "+f"(a[30]), "+f"(a[31]),
+                 "+f"(b[0]), "+f"(b[1]), "+f"(b[2]), "+f"(b[3]), "+f"(b[4]), "+f"(b[5]), "+f"(b[6]), "+f"(b[7]),
+                 "+f"(b[8]), "+f"(b[9]), "+f"(b[10]), "+f"(b[11]), "+f"(b[12]), "+f"(b[13]), "+f"(b[14]), "+f"(b[15]),
+                 "+f"(b[16]), "+f"(b[17]), "+f"(b[18]), "+f"(b[19]), "+f"(b[20]), "+f"(b[21]), "+f"(b[22]), "+f"(b[23]),
+                 "+f"(b[24]), "+f"(b[25]), "+f"(b[26]), "+f"(b[27]), "+f"(b[28]), "+f"(b[29]), "+f"(b[30]), "+f"(b[31])
+               :
+               : "memory");
 }
-#undef DCELL_W8
 
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
                                          uint32_t accumulate) {
@@ -254,10 +264,9 @@ __device__ __forceinline__ bool mma_finish(const Ctx &c, uint64_t *bar, uint32_t
   const int all_ok = __syncthreads_and(ok ? 1 : 0);
   if (!all_ok) return false;
   fence_after();
-  uint32_t *u = reinterpret_cast<uint32_t *>(coef);
-  tmem_ld32(c.tmem + c.lane_off + 64, u);
-  tmem_ld32(c.tmem + c.lane_off + 96, u + 32);
-  tmem_wait_ld();
+  tmem_ld32f(c.tmem + c.lane_off + 64, coef);
+  tmem_ld32f(c.tmem + c.lane_off + 96, coef + 32);
+  tmem_wait_ld_tied(coef, coef + 32);
   fence_before();
   return true;
 }
@@ -679,22 +688,6 @@ __device__ __forceinline__ bool brick_depart(const float *__restrict__ vbox, int
   return in;
 }
 
-// wait::ld that also ties the 64 registers it completes (a[0..32), b[0..32))
-// to the wait, so that no use of them is scheduled before it
-__device__ __forceinline__ void tmem_wait_ld_tied(float *a, float *b) {
-  asm volatile("tcgen05.wait::ld.sync.aligned;"
-               :
-                 "+f"(a[0]), "+f"(a[1]), "+f"(a[2]), "+f"(a[3]), "+f"(a[4]), "+f"(a[5]), "+f"(a[6]), "+f"(a[7]),
-                 "+f"(a[8]), "+f"(a[9]), "+f"(a[10]), "+f"(a[11]), "+f"(a[12]), "+f"(a[13]), "+f"(a[14]), "+f"(a[15]),
-                 "+f"(a[16]), "+f"(a[17]), "+f"(a[18]), "+f"(a[19]), "+f"(a[20]), "+f"(a[21]), "+f"(a[22]), "+f"(a[23]),
-                 "+f"(a[24]), "+f"(a[25]), "+f"(a[26]), "+f"(a[27]), "+f"(a[28]), "+f"(a[29]), "+f"(a[30]), "+f"(a[31]),
-                 "+f"(b[0]), "+f"(b[1]), "+f"(b[2]), "+f"(b[3]), "+f"(b[4]), "+f"(b[5]), "+f"(b[6]), "+f"(b[7]),
-                 "+f"(b[8]), "+f"(b[9]), "+f"(b[10]), "+f"(b[11]), "+f"(b[12]), "+f"(b[13]), "+f"(b[14]), "+f"(b[15]),
-                 "+f"(b[16]), "+f"(b[17]), "+f"(b[18]), "+f"(b[19]), "+f"(b[20]), "+f"(b[21]), "+f"(b[22]), "+f"(b[23]),
-                 "+f"(b[24]), "+f"(b[25]), "+f"(b[26]), "+f"(b[27]), "+f"(b[28]), "+f"(b[29]), "+f"(b[30]), "+f"(b[31])
-               :
-               : "memory");
-}
 
 // Dense-grid stepper over TMA-staged bricks.
 //
@@ -925,11 +918,11 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
       for (int pp = 0; pp < P; pp += 2) {
         // both points' 64 coefficients in one TMEM load round
         float ca[64], cb[64];
-        tmem_ld32(c.tmem + c.lane_off + 128 * pp + 96, reinterpret_cast<uint32_t *>(ca + 32));
-        tmem_ld32(c.tmem + c.lane_off + 128 * (pp + 1) + 96, reinterpret_cast<uint32_t *>(cb + 32));
+        tmem_ld32f(c.tmem + c.lane_off + 128 * pp + 96, ca + 32);
+        tmem_ld32f(c.tmem + c.lane_off + 128 * (pp + 1) + 96, cb + 32);
         tmem_wait_ld_tied(ca + 32, cb + 32);
-        tmem_ld32(c.tmem + c.lane_off + 128 * pp + 64, reinterpret_cast<uint32_t *>(ca));
-        tmem_ld32(c.tmem + c.lane_off + 128 * (pp + 1) + 64, reinterpret_cast<uint32_t *>(cb));
+        tmem_ld32f(c.tmem + c.lane_off + 128 * pp + 64, ca);
+        tmem_ld32f(c.tmem + c.lane_off + 128 * (pp + 1) + 64, cb);
         float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
 #pragma unroll
         for (int kz = 3; kz >= 2; --kz) {
@@ -1192,11 +1185,12 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<2>::CtasPerSm)
       fence_after();
       {
         float ca[64], cb[64];
-        tmem_ld32(c.tmem + c.lane_off + 64, reinterpret_cast<uint32_t *>(ca));
-        tmem_ld32(c.tmem + c.lane_off + 128 + 64, reinterpret_cast<uint32_t *>(cb));
-        tmem_ld32(c.tmem + c.lane_off + 96, reinterpret_cast<uint32_t *>(ca + 32));
-        tmem_ld32(c.tmem + c.lane_off + 128 + 96, reinterpret_cast<uint32_t *>(cb + 32));
-        tmem_wait_ld();
+        tmem_ld32f(c.tmem + c.lane_off + 64, ca);
+        tmem_ld32f(c.tmem + c.lane_off + 128 + 64, cb);
+        tmem_ld32f(c.tmem + c.lane_off + 96, ca + 32);
+        tmem_ld32f(c.tmem + c.lane_off + 128 + 96, cb + 32);
+        tmem_wait_ld_tied(ca, cb);
+        tmem_wait_ld_tied(ca + 32, cb + 32);  // completes nothing more: ties the other halves
         float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
 #pragma unroll
         for (int kz = 3; kz >= 0; --kz) {

@@ -132,6 +132,9 @@ struct dcell_writer {
   void release(Job &j) {
     if (!j.snap) return;
     cudaSetDevice(device);
+    // order the free after the snapshot copy on the caller's stream, also
+    // when process() gave up before drain() made the copy stream wait for it
+    cudaStreamWaitEvent(copy, j.snap, 0);
     cudaFreeAsync(j.staging, copy);
     cudaEventDestroy(j.snap);
     j.snap = nullptr;

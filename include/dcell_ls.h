@@ -229,6 +229,10 @@ DCELL_API int dcell_velocity_boxes(const dcell_box *boxes, int nboxes, int dim, 
  *   - nband <= DCELL_NOALLOC_MAX_BAND, else DCELL_ERR_ARG and no work;
  *   - the first call on a device (made with that device current) looks up the
  *     array's device address; make that first call before any stream capture;
+ *   - that address is kept per device number for the life of the process:
+ *     make every call from the device's primary context (the CUDA runtime's
+ *     own), and do not call cudaDeviceReset between calls -- a reset or
+ *     another context would leave the kept address pointing elsewhere;
  *   - all calls on a device share the array, so calls that overlap on the GPU
  *     (different streams, or a second call before the first one finished)
  *     race; serialise them;

@@ -2,7 +2,7 @@
 TEST INFRASTRUCTURE ONLY.
 
 ``_ref/libdcell_ref.so`` is the reference's unmodified hot-path sources plus
-``oracle/ref_driver.c``, compiled by ``make -C oracle ref`` where the
+``oracle/ref_driver.c``, compiled by ``make -C oracle ref REF=<reference tree>`` where the
 reference tree is present.  ``available()`` says whether it was built.
 """
 from __future__ import annotations
@@ -16,7 +16,7 @@ from . import NODE_W
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PATH = os.path.join(HERE, "_ref", "libdcell_ref.so")
-# the same reference sources linked with the B200 drop-in (make -C oracle dropin)
+# the same reference sources linked with the B200 drop-in (make -C oracle dropin REF=<reference tree>)
 DROPIN_PATH = os.path.join(HERE, "_ref", "libdcell_ref_b200.so")
 _LIBS = {}
 

@@ -1,6 +1,6 @@
 """Generate the golden fixtures in tests/golden/ from the reference's OWN code.
 
-Runs the reference's level-set C (compiled by ``make -C oracle ref`` from the
+Runs the reference's level-set C (compiled by ``make -C oracle ref REF=<reference tree>`` from the
 reference tree against oracle/shim) on small seeded inputs and stores inputs
 and outputs as .npz.  The fixtures let a GPU machine, where the reference tree
 is absent, pin both the oracle and the CUDA path to the reference.
@@ -216,7 +216,7 @@ def run_mac():
 
 
 def main(only=None):
-    assert R.available(), "build oracle/_ref first: make -C oracle ref"
+    assert R.available(), "build oracle/_ref first: make -C oracle ref REF=<reference tree>"
     if only == "mac":
         np.savez_compressed(os.path.join(OUT, "mac.npz"), **run_mac())
         print("mac.npz written to", OUT)

@@ -93,3 +93,19 @@ def test_checkpoint_interval_does_not_change_gradient(cuda):
         out.append(model.coeffs.grad.detach().clone())
     assert torch.allclose(out[0], out[1], rtol=1e-9, atol=1e-12)
     assert torch.allclose(out[0], out[2], rtol=1e-9, atol=1e-12)
+
+
+def test_c5_configuration_as_stated(cuda):
+    """The differentiation configuration itself: 128^3, 50 midpoint steps,
+    velocity from 16 learnable Fourier coefficients, loss sum (H_eps(phi_T) -
+    H_eps(phi_target))^2 with eps = 1.5h, checkpoints every 10.  The FP64
+    adjoint gradient matches FP64 central differences (delta 1e-3, all 16
+    coefficients) to 1e-4 relative, and the FP32 adjoint matches the FP64
+    adjoint (the FP64 reference gradient) to 1e-4 relative."""
+    from dcell_b200.configs import run_c5
+    r = run_c5(N=128, steps=50, every=10, dev=cuda, fd_modes=16)
+    print(f"\nC5 128^3 x 50: FP64 adjoint vs FD {r['fp64_adjoint_vs_fd_rel']:.2e}, FP32 vs FP64 adjoint "
+          f"{r['fp32_adjoint_vs_fp64_adjoint_rel']:.2e}, forward+backward {r['forward_backward_s_float32'] * 1e3:.1f} ms "
+          f"(FP32), {r['forward_backward_s_float64'] * 1e3:.1f} ms (FP64)")
+    assert r["fp64_adjoint_vs_fd_rel"] <= 1e-4, r
+    assert r["fp32_adjoint_vs_fp64_adjoint_rel"] <= 1e-4, r

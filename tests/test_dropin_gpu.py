@@ -1,7 +1,7 @@
 """The drop-in: the reference's own C host with dcell_b200/host/levelset_b200.c
 linked in place of its CPU LevelSetAdvectSL / LevelSetUpdateIrregularNodeList /
 LevelSet_MaxVelocity (oracle/_ref/libdcell_ref_b200.so, built by
-`make -C oracle dropin`), driven through the very same reference call
+`make -C oracle dropin REF=<reference tree>`), driven through the very same reference call
 sequence as the unmodified reference library.  FP64 linear is bit-identical.
 """
 import numpy as np

@@ -63,6 +63,32 @@ def test_tc_error_budget_against_fp64(wl32, cuda):
     assert bool(((out.double() > 0) == (ref > 0))[ref.abs() > 1e-6].all())
 
 
+def test_tc_over_the_full_period_against_fp64(cuda):
+    """C3 over the whole period of the time-reversing field (3072 steps at
+    256^3, t = 0 .. T = 3).  At every step the split-BF16 tensor-core step
+    taken from the FP32 rounding of the FP64 state stays within 1e-5 of the
+    FP64 tricubic step in the |phi| < 3h band (the scope's bar, one step),
+    and its volume within 1e-7 relative.  Accumulated over the period (phi
+    carried as packed BF16 hi/lo words between steps, 16 significant bits),
+    the split-state trajectory stays within 1e-4 of the FP64 trajectory;
+    the measured figures are printed beside the bounds."""
+    from dcell_b200.configs import run_c3
+    r = run_c3(N, dev=cuda)
+    one, acc = r["one_step_tc_vs_fp64"], r["accumulated"]
+    print(f"\nC3 full period: {r['steps']} steps; one-step TC vs FP64 worst max {one['worst_max']:.3e} "
+          f"(step {one['worst_step']}), worst L2 {one['worst_l2']:.3e}, worst volume {one['worst_volume_rel']:.3e}; "
+          f"accumulated at t = T: TC split-state {acc['tc_split_state']['vs_fp64']['max']:.3e}, plain FP32 "
+          f"{acc['plain_fp32']['vs_fp64']['max']:.3e}; worst over the run TC {acc['tc_worst_max_vs_fp64_over_run']:.3e}")
+    assert r["steps"] == r["period_steps"] == 3072
+    assert one["worst_max"] <= 1e-5, one
+    assert one["worst_volume_rel"] <= 1e-7, one
+    assert acc["tc_worst_max_vs_fp64_over_run"] <= 1e-4, acc
+    assert acc["tc_split_state"]["vs_fp64"]["max"] <= 1e-4, acc
+    # the return to the initial sphere is limited by the scheme, not the precision
+    ret = acc["fp64"]["return_error_vs_initial"]["max"]
+    assert abs(acc["tc_split_state"]["return_error_vs_initial"]["max"] - ret) <= 1e-4
+
+
 def test_tc_invariants(wl32, cuda):
     """A constant field stays exactly constant in any velocity (the operator
     maps the constant stencil to the constant coefficient, every product and

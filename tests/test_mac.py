@@ -45,7 +45,7 @@ def test_oracle_matches_reference_golden():
             assert not changed.take(keep, axis=a).any()
 
 
-@pytest.mark.skipif(not R.available(), reason="reference not compiled here (make -C oracle ref)")
+@pytest.mark.skipif(not R.available(), reason="reference not compiled here (make -C oracle ref REF=<reference tree>)")
 @pytest.mark.parametrize("shape,origin", [((7, 8, 9), (-2, -1, -4)), ((6, 5, 4), (-1, 0, -2)), ((4, 3, 5), (0, -2, 0)),
                                           ((9, 11), (-3, -2)), ((4, 3), (-2, 0)), ((3, 7), (0, -6))])
 def test_oracle_matches_reference_live(shape, origin):
@@ -212,7 +212,7 @@ def test_host_buffer_entry(precision):
 
 
 @pytest.mark.gpu
-@pytest.mark.skipif(not os.path.exists(R.DROPIN_PATH), reason="drop-in library not built (make -C oracle dropin)")
+@pytest.mark.skipif(not os.path.exists(R.DROPIN_PATH), reason="drop-in library not built (make -C oracle dropin REF=<reference tree>)")
 def test_dropin_levelset_advect_mac():
     """The B200 LevelSetAdvectMAC / _3D in the reference's own C host, called
     as FluidField/tests/testSource.c calls the originals, gives the
