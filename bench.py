@@ -129,10 +129,10 @@ def dt_at(step, dt):
     return dt * math.cos(math.pi * (step + 0.5) * dt / T_PERIOD)
 
 
-def timed_steps(L, torch, phi, vel, h, dt, interp, K, W, dist=None):
+def timed_steps(L, torch, phi, vel, h, dt, interp, K, W, dist=None, backtrace="midpoint"):
     a, b = phi.clone(), phi.clone()
     for s in range(W):
-        L.sl_step(a, vel, dt_at(s, dt), h, interp=interp, backtrace="midpoint", out=b)
+        L.sl_step(a, vel, dt_at(s, dt), h, interp=interp, backtrace=backtrace, out=b)
         a, b = b, a
     if dist:
         dist.barrier()
@@ -141,7 +141,7 @@ def timed_steps(L, torch, phi, vel, h, dt, interp, K, W, dist=None):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
     for s in range(K):
-        L.sl_step(a, vel, dt_at(W + s, dt), h, interp=interp, backtrace="midpoint", out=b)
+        L.sl_step(a, vel, dt_at(W + s, dt), h, interp=interp, backtrace=backtrace, out=b)
         a, b = b, a
     e1.record(st)
     torch.cuda.synchronize()
@@ -506,13 +506,23 @@ def main():
         ms_sep = timed_steps(L, torch, phi, vel, h, dt, "cubic_separable", K, W)
         ms_tc_unsplit = timed_steps(L, torch, phi, vel, h, dt, "cubic_tc", K, W)
         ms_lin = timed_steps(L, torch, phi, vel, h, dt, "linear", K, W)
+        ms_lin_e = timed_steps(L, torch, phi, vel, h, dt, "linear", K, W, backtrace="euler")
+
+        def hbm_leg(ms):  # one dense FP32 step: 20 algorithmic bytes per update
+            t = ms / K / 1e3
+            return {"updates_per_s": n / t, "ms_per_step": t * 1e3, "achieved_gbs": BYTES_PER_UPDATE * n / t / 1e9,
+                    "hbm_frac": BYTES_PER_UPDATE * n / t / 1e9 / hbm}
         line["comparators"] = {
             "plain_fp32_updates_per_s": n * K / (ms_pl / 1e3),
             "separable_fp32_updates_per_s": n * K / (ms_sep / 1e3),
             "linear_fp32_updates_per_s": n * K / (ms_lin / 1e3),
             "tc_unsplit_state_updates_per_s": n * K / (ms_tc_unsplit / 1e3),
             "tc_over_plain_fp32": ms_pl / ms_tc,
-            "tc_over_separable_fp32": ms_sep / ms_tc}
+            "tc_over_separable_fp32": ms_sep / ms_tc,
+            # the reference's own mode (trilinear, Euler backtrace) and its
+            # midpoint form: TMA z-march, HBM-bound
+            "linear_fp32": {"euler": hbm_leg(ms_lin_e), "midpoint": hbm_leg(ms_lin),
+                            "kernel": "sl_lin_march_kernel"}}
         line["accuracy"] = error_check(L, torch, phi, vel, h, dt)
         if world == 1:
             # the whole period of the field (t = 0 .. T): one-step error of the

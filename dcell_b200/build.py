@@ -34,6 +34,7 @@ NO_SPILL = {"sl_tc.cu": ["sl_tc_brick_kernel"]}
 
 UNITS = {
     "sl_exact.cu": ["-fmad=false"],
+    "sl_lin.cu": [],
     "sl_cubic.cu": [],
     "sl_tc.cu": [],
     "sl_adjoint.cu": [],

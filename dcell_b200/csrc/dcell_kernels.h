@@ -2,12 +2,22 @@
 // C ABI (capi.cu).  Not part of the public header.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "dcell_common.cuh"
 
+// 3-D tiled TMA map (zero fill out of bounds, no swizzle) over a row-major
+// array (x fastest) of dx x dy x dz values of `elem` bytes; box bx x by x bz.
+// False when the driver's encoder is unavailable or rejects the map.
+bool make_tensor_map_3d(CUtensorMap *m, CUtensorMapDataType type, const void *base, uint64_t dx, uint64_t dy,
+                        uint64_t dz, uint32_t bx, uint32_t by, uint32_t bz, uint32_t elem);
+
 int launch_sl_linear(const dcell::Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
                      long long npts, int backtrace, void *phi, int *flags, cudaStream_t st);
+// FP32 trilinear step (sl_lin.cu): TMA z-march on dense 3-D grids, gathers otherwise
+int launch_sl_lin_f32(const dcell::Geom &g, const float *phi0, const float *vel, double dt, const int *band,
+                      long long npts, int backtrace, float *phi, int *flags, cudaStream_t st);
 int launch_sl_cubic(const dcell::Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
                     long long npts, int interp, int backtrace, void *phi, int *flags, cudaStream_t st);
 int launch_sl_tc(const dcell::Geom &g, const float *phi0, const float *vel, double dt, const int *band,

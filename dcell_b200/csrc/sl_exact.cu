@@ -4,7 +4,8 @@
 // the reference's operation order with one rounding per operation, so in
 // FP64 the results are bit-identical to the reference's x86 double
 // arithmetic (Common/Grid.c, Grid3D.c, InterpolateVelocity.c, AdvectSL.c,
-// IrregularNodes*.c).  The FP32 instantiations follow the same order.
+// IrregularNodes*.c).  The FP32 instantiations follow the same order (the
+// FP32 linear step itself runs the fast unit sl_lin.cu).
 //
 // Kernels:
 //   sl_linear_kernel     LevelSetAdvectSL_2D/_3D (AdvectSL.c:23-89)
@@ -1173,21 +1174,17 @@ int launch_sl_linear(const Geom &g, int dtype, const void *phi0, const void *vel
                      long long npts, int backtrace, void *phi, int *flags, cudaStream_t st) {
   const int threads = 256, blocks = grid_for(npts, threads);
   const bool is2d = g.nz == 1;
-  if (dtype == DCELL_F64) {
-    if (is2d)
-      sl_linear_kernel<double, 2><<<blocks, threads, 0, st>>>(g, (const double *)phi0, (const double *)vel, dt, band,
-                                                              npts, backtrace, (double *)phi, flags);
-    else
-      sl_linear_kernel<double, 3><<<blocks, threads, 0, st>>>(g, (const double *)phi0, (const double *)vel, dt, band,
-                                                              npts, backtrace, (double *)phi, flags);
-  } else {
-    if (is2d)
-      sl_linear_kernel<float, 2><<<blocks, threads, 0, st>>>(g, (const float *)phi0, (const float *)vel, (float)dt,
-                                                             band, npts, backtrace, (float *)phi, flags);
-    else
-      sl_linear_kernel<float, 3><<<blocks, threads, 0, st>>>(g, (const float *)phi0, (const float *)vel, (float)dt,
-                                                             band, npts, backtrace, (float *)phi, flags);
-  }
+  // FP32 runs the fast unit (sl_lin.cu); this one keeps the reference's
+  // FP64 operation order
+  if (dtype == DCELL_F32)
+    return launch_sl_lin_f32(g, (const float *)phi0, (const float *)vel, dt, band, npts, backtrace, (float *)phi,
+                             flags, st);
+  if (is2d)
+    sl_linear_kernel<double, 2><<<blocks, threads, 0, st>>>(g, (const double *)phi0, (const double *)vel, dt, band,
+                                                            npts, backtrace, (double *)phi, flags);
+  else
+    sl_linear_kernel<double, 3><<<blocks, threads, 0, st>>>(g, (const double *)phi0, (const double *)vel, dt, band,
+                                                            npts, backtrace, (double *)phi, flags);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 

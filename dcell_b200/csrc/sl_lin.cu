@@ -1,0 +1,346 @@
+// Production FP32 trilinear semi-Lagrangian step: the reference's own
+// LevelSetAdvectSL_2D / _3D mode (LevelSetMethod/AdvectSL.c:23-89) -- MAC
+// velocity at the arrival node (Common/InterpolateVelocity.c:7-67), departure
+// S = X - V dt / h, bi/trilinear phi0 at S (Common/Grid.c:190-212,
+// Grid3D.c:4-31) -- plus the midpoint backtrace.
+//
+// This unit is compiled with FMA contraction.  The bit-exact FP64 path stays
+// the reference-order kernel of sl_exact.cu; this one is the fast FP32 form:
+// dt / h is formed once on the host, the departure is carried as an integer
+// cell plus an FP32 fraction (S = X + t, cell = X + floor(t), frac = t -
+// floor(t): exact to the precision of the displacement, not of the absolute
+// coordinate), interpolation is nested lerps (one subtraction and one FMA
+// each), and index math is 32-bit.  Every rounding is explicit
+// (__fmul_rn / __fmaf_rn / __fsub_rn / __fadd_rn), so the staged and the
+// global-memory paths below give the same bits.
+//
+// Dense 3-D grids (nx % 4 == 0) march z-columns through a plane ring staged
+// by TMA: a CTA of 256 threads owns a 32 x 8 tile of every plane of a z-run,
+// and keeps planes z-2 .. z+5 of phi0 (40 x 12 floats, halo 4 | 2) and of the
+// interleaved velocity (120 x 12 floats) in an 8-slot ring; each plane is
+// loaded once as it enters the window, three planes ahead of its first use.
+// Per point: 6 (Euler) or 6 + 24 (midpoint) velocity and 8 phi0 values from
+// shared memory, one coalesced store.  Bands, 2-D grids and other shapes run
+// the global-gather kernel with the same arithmetic.
+#include <math.h>
+
+#include <algorithm>
+
+#include "dcell_common.cuh"
+#include "dcell_kernels.h"
+#include "dcell_tma.cuh"
+#include "sl_device.cuh"
+
+namespace dcell {
+namespace lin {
+
+constexpr int TX = 32, TY = 8;             // points of one plane per CTA (one warp per row)
+constexpr int kThreads = TX * TY;
+constexpr int HX = 4, HY = 2;              // box halo (x: 4 keeps TMA x coordinates 16-byte aligned)
+constexpr int PW = TX + 2 * HX;            // 40 phi values per box row
+constexpr int PH = TY + 2 * HY;            // 12 box rows
+constexpr int VW = 3 * PW;                 // 120 velocity values per box row (u, v, w interleaved)
+constexpr int kPlanePhi = PW * PH;         // floats of one staged phi plane (1920 B)
+constexpr int kPlaneVel = VW * PH;         // floats of one staged velocity plane (5760 B)
+constexpr int kRing = 8;                   // ring slots: planes z-2 .. z+2 in use, three ahead
+constexpr int kPlaneBytes = 4 * (kPlanePhi + kPlaneVel);
+constexpr int kSmem = kRing * kPlaneBytes + kRing * 8;  // + one mbarrier per slot
+static_assert((4 * kPlanePhi) % 128 == 0 && (4 * kPlaneVel) % 128 == 0, "staged planes stay 128-byte aligned");
+static_assert((kRing & (kRing - 1)) == 0 && kRing >= 8, "ring slot of plane p is (p + kRing) & (kRing - 1)");
+
+// phi0 / velocity through global memory, indices clamped into the grid (the
+// reference's per-axis clamping).
+template <int DIM>
+struct GlobalAcc {
+  const float *__restrict__ phi0;
+  const float *__restrict__ vel;
+  int nx, ny, nz;
+  __device__ __forceinline__ int at(int i, int j, int k) const {
+    i = clampi(i, 0, nx - 1);
+    j = clampi(j, 0, ny - 1);
+    k = DIM == 3 ? clampi(k, 0, nz - 1) : 0;
+    return (k * ny + j) * nx + i;
+  }
+  __device__ __forceinline__ float phi(int i, int j, int k) const { return __ldg(phi0 + at(i, j, k)); }
+  __device__ __forceinline__ float v(int i, int j, int k, int d) const { return __ldg(vel + DIM * at(i, j, k) + d); }
+};
+
+// The staged ring: box origin (bx, by) = (x0 - 4, y0 - 2) of the tile; plane
+// p of the grid sits in slot (p + kRing) & (kRing - 1) and holds plane
+// clamp(p, 0, nz - 1) (the z clamping is done by the load).  Columns and rows
+// are clamped into the grid and into the box in one step: for an index whose
+// grid-clamped position lies in the box the read equals the global clamped
+// read; any other index still reads inside the ring (a value that the caller
+// discards, since lin_point then reports the point as outside the box).
+struct BoxAcc {
+  const float *phis;  // ring of phi planes
+  const float *vels;  // ring of velocity planes
+  int bx, by;         // box origin (grid coordinates)
+  int clo, chi;       // box columns that hold grid columns: [max(-bx, 0), min(nx - 1 - bx, PW - 1)]
+  int rlo, rhi;       // box rows that hold grid rows
+  __device__ __forceinline__ BoxAcc(const float *p, const float *v, int x0, int y0, int nx, int ny)
+      : phis(p), vels(v), bx(x0 - HX), by(y0 - HY), clo(max(HX - x0, 0)), chi(min(nx - 1 - (x0 - HX), PW - 1)),
+        rlo(max(HY - y0, 0)), rhi(min(ny - 1 - (y0 - HY), PH - 1)) {}
+  __device__ __forceinline__ int col(int i) const { return clampi(i - bx, clo, chi); }
+  __device__ __forceinline__ int row(int j) const { return clampi(j - by, rlo, rhi); }
+  __device__ __forceinline__ static int slot(int k) { return (k + kRing) & (kRing - 1); }
+  __device__ __forceinline__ float phi(int i, int j, int k) const {
+    return phis[slot(k) * kPlanePhi + row(j) * PW + col(i)];
+  }
+  __device__ __forceinline__ float v(int i, int j, int k, int d) const {
+    return vels[slot(k) * kPlaneVel + row(j) * VW + 3 * col(i) + d];
+  }
+};
+
+// One arrival point (local indices x, y, z): node velocity, optional
+// midpoint velocity, departure, bi/trilinear phi0.  dth = dt / h per axis,
+// hdth = -dt / (2 h).  `in` reports whether every value read lies within
+// the staged box of the point's tile (|midpoint offset| < 1 and departure
+// offset in [-2, 2) per axis); c, f: the departure cell (local) and fraction.
+template <int BT, int DIM, class A>
+__device__ __forceinline__ float lin_point(const A &acc, int x, int y, int z, const float dth[3], const float hdth[3],
+                                           bool &in, int c[3], float f[3]) {
+  const int X[3] = {x, y, z};
+  float U[3];
+  U[0] = face_mean(acc.v(x, y, z, 0), acc.v(x + 1, y, z, 0));
+  U[1] = face_mean(acc.v(x, y, z, 1), acc.v(x, y + 1, z, 1));
+  U[2] = DIM == 3 ? face_mean(acc.v(x, y, z, 2), acc.v(x, y, z + 1, 2)) : 0.f;
+  in = true;
+  if (BT == DCELL_MIDPOINT) {
+    float dl[3];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      dl[a] = rmul(U[a], hdth[a]);
+      in = in && fabsf(dl[a]) < 1.f;
+    }
+    float V[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      int b[3] = {0, 0, z};
+      float s[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {  // the component's own axis carries the half-cell stagger
+        const float t = a == d ? __fadd_rn(dl[a], 0.5f) : dl[a];
+        const float fl = floorf(t);
+        b[a] = X[a] + (int)fl;
+        s[a] = __fsub_rn(t, fl);
+      }
+      if (DIM == 3)
+        V[d] = trilerp(acc.v(b[0], b[1], b[2], d), acc.v(b[0] + 1, b[1], b[2], d), acc.v(b[0], b[1] + 1, b[2], d),
+                       acc.v(b[0] + 1, b[1] + 1, b[2], d), acc.v(b[0], b[1], b[2] + 1, d),
+                       acc.v(b[0] + 1, b[1], b[2] + 1, d), acc.v(b[0], b[1] + 1, b[2] + 1, d),
+                       acc.v(b[0] + 1, b[1] + 1, b[2] + 1, d), s);
+      else
+        V[d] = bilerp(acc.v(b[0], b[1], 0, d), acc.v(b[0] + 1, b[1], 0, d), acc.v(b[0], b[1] + 1, 0, d),
+                      acc.v(b[0] + 1, b[1] + 1, 0, d), s[0], s[1]);
+    }
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) U[a] = V[a];
+  }
+  c[2] = z;
+  f[2] = 0.f;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    const float t = rmul(-U[a], dth[a]);
+    in = in && t >= -2.f && t < 2.f;
+    const float fl = floorf(t);
+    c[a] = X[a] + (int)fl;
+    f[a] = __fsub_rn(t, fl);
+  }
+  if (DIM == 3)
+    return trilerp(acc.phi(c[0], c[1], c[2]), acc.phi(c[0] + 1, c[1], c[2]), acc.phi(c[0], c[1] + 1, c[2]),
+                   acc.phi(c[0] + 1, c[1] + 1, c[2]), acc.phi(c[0], c[1], c[2] + 1), acc.phi(c[0] + 1, c[1], c[2] + 1),
+                   acc.phi(c[0], c[1] + 1, c[2] + 1), acc.phi(c[0] + 1, c[1] + 1, c[2] + 1), f);
+  return bilerp(acc.phi(c[0], c[1], 0), acc.phi(c[0] + 1, c[1], 0), acc.phi(c[0], c[1] + 1, 0),
+                acc.phi(c[0] + 1, c[1] + 1, 0), f[0], f[1]);
+}
+
+// Global-gather form: one thread per arrival point of the band (or of the
+// dense grid when band is null).  Band entries outside the grid are skipped
+// and flagged; on bands, a departure outside the grid (clamped) is flagged.
+template <int BT, int DIM>
+__global__ void __launch_bounds__(256) sl_lin_gather_kernel(Geom g, const float *__restrict__ phi0,
+                                                            const float *__restrict__ vel, float dth0, float dth1,
+                                                            float dth2, const int *__restrict__ band, int npts,
+                                                            float *__restrict__ phi, int *flags) {
+  const float dth[3] = {dth0, dth1, dth2};
+  const float hdth[3] = {-0.5f * dth0, -0.5f * dth1, -0.5f * dth2};
+  const GlobalAcc<DIM> acc{phi0, vel, g.nx, g.ny, g.nz};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  bool bad = false, clamped = false;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npts; q += gridDim.x * blockDim.x) {
+    int x, y, z;
+    if (!arrival_local(g, band, q, x, y, z)) {
+      bad = true;
+      continue;
+    }
+    bool in;
+    int c[3];
+    float f[3];
+    phi[(z * g.ny + y) * g.nx + x] = lin_point<BT, DIM>(acc, x, y, z, dth, hdth, in, c, f);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) clamped |= c[a] < 0 || c[a] + (f[a] > 0.f ? 1 : 0) > n[a] - 1;
+  }
+  if (bad) raise_flag(flags, FLAG_BAD_BAND);
+  if (clamped && band) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);  // dense grids: the edge is the domain boundary
+}
+
+struct MarchGrid {
+  int ncx;    // tiles per row of tiles (x)
+  int units;  // tiles x planes: unit u = tile * nz + z
+};
+
+// Dense 3-D march (see the head of the file).  CTA b owns units
+// [b U / G, (b+1) U / G) in order: z-runs of one tile, a new run (ring
+// restart) where the range crosses into the next tile.  Thread 0 issues the
+// loads; all threads wait on the slot's mbarrier before a plane's first use;
+// one CTA barrier per plane releases the slot of plane z-2, which thread 0
+// then refills with plane z+6.  Warps whose points read outside the staged
+// box (per-axis displacement >= 2, or a midpoint offset >= 1) take the
+// global path for that plane.  Every wait is bounded; on a timeout the CTA
+// raises FLAG_WAIT_TIMEOUT, waits (bounded) for its loads in flight and
+// leaves.
+template <int BT>
+__global__ void __launch_bounds__(kThreads, 3)
+    sl_lin_march_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel,
+                        Geom g, MarchGrid mg, const float *__restrict__ phi0, const float *__restrict__ vel, float dth0,
+                        float dth1, float dth2, float *__restrict__ phi, int *flags) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  float *const phis = reinterpret_cast<float *>(smem);
+  float *const vels = phis + kRing * kPlanePhi;
+  uint64_t *const full = reinterpret_cast<uint64_t *>(smem + kRing * kPlaneBytes);
+  const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5;
+  if (tid == 0)
+    for (int s = 0; s < kRing; ++s) mbar_init(&full[s], 1);
+  __syncthreads();
+
+  const float dth[3] = {dth0, dth1, dth2};
+  const float hdth[3] = {-0.5f * dth0, -0.5f * dth1, -0.5f * dth2};
+  const GlobalAcc<3> gacc{phi0, vel, g.nx, g.ny, g.nz};
+  const int U = mg.units, G = (int)gridDim.x, b = (int)blockIdx.x;
+  const int ubeg = (int)((long long)U * b / G), uend = (int)((long long)U * (b + 1) / G);
+  uint32_t parity = 0;         // bit s: phase of slot s's next completion (same in every thread)
+  int issued = 0, waited = 0;  // planes of the current run loaded / waited for, up to (exclusive)
+  bool err = false;
+
+  auto issue = [&](int x0, int y0, int p) {  // thread 0: plane p of the tile at (x0, y0) into its slot
+    const int s = BoxAcc::slot(p), pz = clampi(p, 0, g.nz - 1);
+    mbar_expect_tx(&full[s], (uint32_t)kPlaneBytes);
+    tma_load_3d(phis + s * kPlanePhi, &tm_phi, x0 - HX, y0 - HY, pz, &full[s]);
+    tma_load_3d(vels + s * kPlaneVel, &tm_vel, 3 * (x0 - HX), y0 - HY, pz, &full[s]);
+  };
+
+  for (int u = ubeg; u < uend && !err;) {
+    const int tile = u / g.nz, zs = u - tile * g.nz;
+    const int ze = min(g.nz, zs + (uend - u));
+    u += ze - zs;
+    const int x0 = (tile % mg.ncx) * TX, y0 = (tile / mg.ncx) * TY;
+    const int last = ze + 1;                      // the last plane this run reads (ze - 1 + 2)
+    const int head = min(zs + kRing - 3, last);   // the prologue loads planes zs - 2 .. head
+    if (tid == 0) {
+      fence_proxy_async();  // earlier reads of the ring before these writes
+      for (int p = zs - 2; p <= head; ++p) issue(x0, y0, p);
+    }
+    issued = head + 1;
+    waited = zs - 2;
+    const BoxAcc bacc(phis, vels, x0, y0, g.nx, g.ny);
+    const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
+    const bool store = x0 + lx < g.nx && y0 + ly < g.ny;
+    for (int z = zs; z < ze; ++z) {
+      for (; !err && waited <= z + 2; ++waited) {  // planes up to z + 2 present
+        const int s = BoxAcc::slot(waited);
+        if (!mbar_wait_sleep(&full[s], (parity >> s) & 1u)) {
+          err = true;
+          break;
+        }
+        parity ^= 1u << s;
+      }
+      // (after a timeout the ring holds stale values: reads stay in bounds,
+      // the results are discarded with the flag raised)
+      bool in;
+      int c[3];
+      float f[3];
+      float v = lin_point<BT, 3>(bacc, x, y, z, dth, hdth, in, c, f);
+      if (!__all_sync(0xffffffffu, in)) v = lin_point<BT, 3>(gacc, x, y, z, dth, hdth, in, c, f);
+      if (store) phi[(z * g.ny + y) * g.nx + x] = v;
+      if (__syncthreads_or(err)) {  // also: slot of plane z - 2 read for the last time
+        err = true;
+        break;
+      }
+      if (issued <= last) {  // refill that slot with plane z + 6
+        if (tid == 0) {
+          fence_proxy_async();
+          issue(x0, y0, issued);
+        }
+        ++issued;
+      }
+    }
+  }
+  if (err && tid == 0) {
+    // loads still in flight: planes [waited, issued) of the run that stopped
+    for (int p = waited; p < issued; ++p) {
+      const int s = BoxAcc::slot(p);
+      if (!mbar_wait(&full[s], (parity >> s) & 1u)) break;
+      parity ^= 1u << s;
+    }
+    raise_flag(flags, FLAG_WAIT_TIMEOUT);
+  }
+}
+
+}  // namespace lin
+}  // namespace dcell
+
+using namespace dcell;
+
+// The z-march applies to dense 3-D grids with nx % 4 == 0 (16-byte rows),
+// 16-byte aligned bases and planes at least one box wide.
+static bool lin_march_applicable(const Geom &g, const void *phi0, const void *vel) {
+  return g.nz > 1 && g.nx % 4 == 0 && g.nx >= 8 && g.ny >= 4 && ((uintptr_t)phi0 % 16) == 0 &&
+         ((uintptr_t)vel % 16) == 0;
+}
+
+int launch_sl_lin_f32(const Geom &g, const float *phi0, const float *vel, double dt, const int *band, long long npts,
+                      int backtrace, float *phi, int *flags, cudaStream_t st) {
+  const float dth0 = (float)(dt / g.hx), dth1 = (float)(dt / g.hy), dth2 = (float)(dt / g.hz);
+  const bool mid = backtrace == DCELL_MIDPOINT;
+  if (!band && lin_march_applicable(g, phi0, vel)) {
+    static bool configured = false;
+    if (!configured) {
+      DCELL_CUDA_CHECK(cudaFuncSetAttribute(lin::sl_lin_march_kernel<DCELL_EULER>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, lin::kSmem));
+      DCELL_CUDA_CHECK(cudaFuncSetAttribute(lin::sl_lin_march_kernel<DCELL_MIDPOINT>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, lin::kSmem));
+      configured = true;
+    }
+    CUtensorMap tm_phi, tm_vel;
+    if (make_tensor_map_3d(&tm_phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, phi0, (uint64_t)g.nx, (uint64_t)g.ny,
+                           (uint64_t)g.nz, lin::PW, lin::PH, 1, 4) &&
+        make_tensor_map_3d(&tm_vel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel, 3ull * g.nx, (uint64_t)g.ny,
+                           (uint64_t)g.nz, lin::VW, lin::PH, 1, 4)) {
+      lin::MarchGrid mg;
+      mg.ncx = (g.nx + lin::TX - 1) / lin::TX;
+      const int ncy = (g.ny + lin::TY - 1) / lin::TY;
+      mg.units = mg.ncx * ncy * g.nz;
+      int dev = 0, sms = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const int grid = std::min(3 * sms, mg.units);
+      auto kern = mid ? lin::sl_lin_march_kernel<DCELL_MIDPOINT> : lin::sl_lin_march_kernel<DCELL_EULER>;
+      kern<<<grid, lin::kThreads, lin::kSmem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0, dth1, dth2, phi, flags);
+      return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+    }
+    // no tensor maps (driver entry point unavailable): the gather form below
+  }
+  const int n = (int)npts;
+  int blocks = (n + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  if (g.nz == 1) {
+    if (mid) lin::sl_lin_gather_kernel<DCELL_MIDPOINT, 2><<<blocks, 256, 0, st>>>(g, phi0, vel, dth0, dth1, dth2, band, n, phi, flags);
+    else lin::sl_lin_gather_kernel<DCELL_EULER, 2><<<blocks, 256, 0, st>>>(g, phi0, vel, dth0, dth1, dth2, band, n, phi, flags);
+  } else {
+    if (mid) lin::sl_lin_gather_kernel<DCELL_MIDPOINT, 3><<<blocks, 256, 0, st>>>(g, phi0, vel, dth0, dth1, dth2, band, n, phi, flags);
+    else lin::sl_lin_gather_kernel<DCELL_EULER, 3><<<blocks, 256, 0, st>>>(g, phi0, vel, dth0, dth1, dth2, band, n, phi, flags);
+  }
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}

@@ -34,6 +34,7 @@
 #include <cuda_bf16.h>
 
 #include "dcell_common.cuh"
+#include "dcell_tma.cuh"
 #include "dcell_kernels.h"
 #include "sl_device.cuh"
 
@@ -46,11 +47,6 @@ constexpr int kK = 128;          // K: stencil entry j contributes hi_j at K = 2
 constexpr int kTmemCols = 128;   // A: 64 columns (one packed hi|lo word per stencil entry), D: 64 columns
 constexpr int kBBytes = kCoef * kK * 2;  // B: 64 rows x 128 K of bf16, B[n][2j] = B[n][2j+1] = M[n][j]
 constexpr int kDynSmem = 56 * 1024;      // caps residency at 4 CTAs/SM = 512 TMEM columns
-constexpr unsigned kWaitLimit = 1u << 20;  // bounded mbarrier polls (a normal MMA completes in microseconds)
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
 
 // Shared-memory matrix descriptor, K-major, no swizzle: 8-row x 16-byte core
 // matrices; LBO = byte stride between K-adjacent core matrices, SBO = byte
@@ -68,49 +64,6 @@ __host__ __device__ constexpr uint32_t instr_desc_bf16(int M, int N) {
 // Byte offset of element (row n, k) of a K-major no-swizzle operand with K = 128.
 __device__ __forceinline__ int b_offset(int n, int k) {
   return (((n >> 3) * (kK / 8) + (k >> 3)) * 128) + (n & 7) * 16 + (k & 7) * 2;
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-// Bounded wait for phase `parity` of the mbarrier; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (unsigned it = 0; it < kWaitLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-// Bounded wait that lets the hardware suspend the thread until the phase
-// completes (or `kSleepNs` pass) instead of spinning: pipeline waits inside
-// the brick kernel, where warps routinely wait a few hundred cycles.  At most
-// kSleepLimit rounds (well under a second in all).
-constexpr uint32_t kSleepNs = 20000;
-constexpr unsigned kSleepLimit = 1u << 15;
-__device__ __forceinline__ bool mbar_wait_sleep(uint64_t *bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (unsigned it = 0; it < kSleepLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity), "r"(kSleepNs)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
 }
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -457,20 +410,6 @@ __global__ void __launch_bounds__(kTile, 4) sl_tc_split_kernel(Geom g, const uin
 // elements (16-byte rule); nothing starts a store at a negative coordinate.
 // Points whose departure (or midpoint) leaves the box -- per-component
 // CFL >= 1 -- take the global-memory path.
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-// 3-D tiled TMA load (no multicast) of the box at (c0, c1, c2) into shared memory
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, int c0, int c1, int c2,
-                                            uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
-      "[%5];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
-      : "memory");
-}
-
 struct BrickGrid {
   int nbx, nby, nbz;  // bricks of this launch per axis
   int bz0;            // z brick index of the launch's first brick (z-slab launches)
@@ -558,10 +497,6 @@ __device__ __forceinline__ bool replicate_pass(uint32_t *box, int axis, const in
     box[base + dst * inner] = box[base + src * inner];
   }
   return true;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // The global-memory path for one point of a brick warp that left its boxes:
@@ -1442,7 +1377,7 @@ static EncodeTiledFn encode_tiled() {
 }
 
 // 3-D tiled map over a row-major array (x fastest) of `elem` bytes per value.
-static bool make_map(CUtensorMap *m, CUtensorMapDataType type, const void *base, uint64_t dx, uint64_t dy,
+bool make_tensor_map_3d(CUtensorMap *m, CUtensorMapDataType type, const void *base, uint64_t dx, uint64_t dy,
                      uint64_t dz, uint32_t bx, uint32_t by, uint32_t bz, uint32_t elem) {
   EncodeTiledFn fn = encode_tiled();
   if (!fn) return false;
@@ -1480,9 +1415,9 @@ static int launch_brick(const Geom &g, const uint32_t *phi0s, const float *vel, 
     configured = true;
   }
   CUtensorMap tm_phi, tm_vel;
-  if (!make_map(&tm_phi, CU_TENSOR_MAP_DATA_TYPE_UINT32, phi0s, (uint64_t)g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
+  if (!make_tensor_map_3d(&tm_phi, CU_TENSOR_MAP_DATA_TYPE_UINT32, phi0s, (uint64_t)g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
                 S::PX, S::PY, S::PZ, 4) ||
-      !make_map(&tm_vel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel, 3ull * g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
+      !make_tensor_map_3d(&tm_vel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel, 3ull * g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
                 3 * S::VX, S::VY, S::VZ, 4)) {
     dcell_set_error(DCELL_ERR_CUDA, "cuTensorMapEncodeTiled failed for the TMA brick path");
     return DCELL_ERR_CUDA;

@@ -50,6 +50,48 @@ def test_linear_fp32_vs_reference(golden, cuda, case):
     assert np.abs(out - g["phi"]).max() <= 4e-7 * scale
 
 
+def _random_case(shape, cfl, dev, seed=3):
+    """Smooth-ish FP32 phi and a random MAC velocity whose largest component
+    moves cfl cells per unit step (dt = h = 1)."""
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    nz, ny, nx = shape
+    z, y, x = torch.meshgrid(torch.arange(nz), torch.arange(ny), torch.arange(nx), indexing="ij")
+    phi = (torch.sin(0.37 * x) + torch.cos(0.29 * y) * torch.sin(0.41 * z) + 0.1 * torch.rand(shape, generator=g))
+    vel = (torch.rand(shape + (3,), generator=g) * 2 - 1) * cfl
+    return phi.float().to(dev).contiguous(), vel.float().to(dev).contiguous()
+
+
+@pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
+@pytest.mark.parametrize("shape,cfl", [((9, 20, 36), 0.5), ((40, 24, 64), 0.9), ((16, 16, 32), 3.0), ((3, 5, 8), 0.5),
+                                       ((70, 9, 96), 1.7)])
+def test_linear_fp32_march_equals_gather(cuda, backtrace, shape, cfl):
+    """FP32 trilinear step: the TMA z-march of dense grids (partial tiles,
+    short grids, and departures beyond the staged box at CFL 1.7 and 3, which
+    take the warp's global path) gives the same bits as the global-gather
+    form run on a band that lists every point."""
+    phi, vel = _random_case(shape, cfl, cuda)
+    dense = L.sl_step(phi, vel, 1.0, 1.0, interp="linear", backtrace=backtrace)
+    band = fields.band_of(torch.zeros_like(phi), 1.0, margin=0).to(cuda)
+    assert band.shape[0] == phi.numel()
+    banded = L.sl_step(phi, vel, 1.0, 1.0, band=band, interp="linear", backtrace=backtrace,
+                       out=torch.full_like(phi, float("nan")))
+    torch.cuda.synchronize()
+    assert torch.equal(dense, banded)
+
+
+@pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
+def test_linear_fp32_dense_vs_fp64(cuda, backtrace):
+    """Dense 64^3 sphere in the deformation field (FP32-representable
+    inputs): the FP32 step within FP32 rounding of the FP64 reference-order
+    step (Euler: the reference's own arithmetic; midpoint: its FP64 form)."""
+    N = 64
+    h, phi, vel, dt = _sphere_case(N, cuda)
+    p32, v32 = phi.float().contiguous(), vel.float().contiguous()
+    ref = L.sl_step(p32.double(), v32.double(), dt, h, interp="linear", backtrace=backtrace)
+    out = L.sl_step(p32, v32, dt, h, interp="linear", backtrace=backtrace).double()
+    assert float((out - ref).abs().max()) <= 4e-7 * float(ref.abs().max())
+
+
 def test_rk2_half_full_fp64_bit_exact(golden, cuda):
     """AdvectRK2.c: HalfStep(dt/2, u^n) then FullStep(dt, u^{n+1/2}) from the same phi0."""
     g = golden("sl3d_rk2")
