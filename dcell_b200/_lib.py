@@ -20,8 +20,10 @@ FLAG_DEPARTURE_CLAMPED, FLAG_NONFINITE, FLAG_CAPACITY, FLAG_WAIT_TIMEOUT, FLAG_B
 FLAG_UNSETTLED = 32
 FLAG_PARTICLE_OUTSIDE = 64
 
+GATHER_FORM = 0x100  # OR'ed into interp: the global-gather form on dense FP32 grids
 INTERP = {"linear": LINEAR, "cubic": CUBIC_PLAIN, "cubic_plain": CUBIC_PLAIN, "cubic_separable": CUBIC_SEPARABLE,
-          "cubic_tc": CUBIC_TC}
+          "cubic_tc": CUBIC_TC, "linear_gather": LINEAR | GATHER_FORM,
+          "cubic_plain_gather": CUBIC_PLAIN | GATHER_FORM, "cubic_separable_gather": CUBIC_SEPARABLE | GATHER_FORM}
 BACKTRACE = {"euler": EULER, "midpoint": MIDPOINT}
 
 

@@ -64,6 +64,8 @@ DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, co
   int rc = check_geom(g);
   if (rc) return rc;
   if (dtype != DCELL_F32 && dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "dtype must be DCELL_F32 or DCELL_F64");
+  const bool gather = (interp & DCELL_GATHER_FORM) != 0;
+  interp &= ~DCELL_GATHER_FORM;
   if (interp < DCELL_LINEAR || interp > DCELL_CUBIC_TC) FAIL(DCELL_ERR_ARG, "unknown interpolation %d", interp);
   if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
   if (!phi0 || !vel || !phi) FAIL(DCELL_ERR_ARG, "phi0, vel and phi must be device pointers");
@@ -73,14 +75,15 @@ DCELL_API int dcell_sl_step(const dcell_geom *g, int dtype, const void *phi0, co
   const long long npts = band ? (long long)nband : grid_points(g);
   if (npts == 0) return DCELL_OK;
   cudaStream_t st = (cudaStream_t)stream;
-  if (interp == DCELL_LINEAR) return launch_sl_linear(G, dtype, phi0, vel, dt, band, npts, backtrace, phi, flags, st);
+  if (interp == DCELL_LINEAR)
+    return launch_sl_linear(G, dtype, phi0, vel, dt, band, npts, backtrace, phi, flags, st, gather);
   if (interp == DCELL_CUBIC_TC) {
     if (dtype != DCELL_F32) FAIL(DCELL_ERR_UNSUPPORTED, "DCELL_CUBIC_TC computes in FP32 only");
     if (G.nz == 1) FAIL(DCELL_ERR_UNSUPPORTED, "DCELL_CUBIC_TC is 3D only");
     return launch_sl_tc(G, (const float *)phi0, (const float *)vel, dt, band, npts, backtrace, (float *)phi, flags,
                         st);
   }
-  return launch_sl_cubic(G, dtype, phi0, vel, dt, band, npts, interp, backtrace, phi, flags, st);
+  return launch_sl_cubic(G, dtype, phi0, vel, dt, band, npts, interp, backtrace, phi, flags, st, gather);
 }
 
 DCELL_API int dcell_split_bf16(const dcell_geom *g, const float *phi, unsigned int *split, void *stream) {

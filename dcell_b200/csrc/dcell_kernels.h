@@ -14,12 +14,14 @@ bool make_tensor_map_3d(CUtensorMap *m, CUtensorMapDataType type, const void *ba
                         uint64_t dz, uint32_t bx, uint32_t by, uint32_t bz, uint32_t elem);
 
 int launch_sl_linear(const dcell::Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
-                     long long npts, int backtrace, void *phi, int *flags, cudaStream_t st);
+                     long long npts, int backtrace, void *phi, int *flags, cudaStream_t st, bool gather = false);
 // FP32 trilinear step (sl_lin.cu): TMA z-march on dense 3-D grids, gathers otherwise
 int launch_sl_lin_f32(const dcell::Geom &g, const float *phi0, const float *vel, double dt, const int *band,
-                      long long npts, int backtrace, float *phi, int *flags, cudaStream_t st);
+                      long long npts, int backtrace, float *phi, int *flags, cudaStream_t st, bool gather = false);
+// gather: the global-gather form even where the brick-staged one applies
 int launch_sl_cubic(const dcell::Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
-                    long long npts, int interp, int backtrace, void *phi, int *flags, cudaStream_t st);
+                    long long npts, int interp, int backtrace, void *phi, int *flags, cudaStream_t st,
+                    bool gather = false);
 int launch_sl_tc(const dcell::Geom &g, const float *phi0, const float *vel, double dt, const int *band,
                  long long npts, int backtrace, float *phi, int *flags, cudaStream_t st);
 

@@ -14,6 +14,13 @@
 // Band structure and backtrace follow LevelSetAdvectSL_2D/_3D
 // (LevelSetMethod/AdvectSL.c:23-89).  The FP64 instantiation of PLAIN is
 // the GPU FP64 oracle used to measure errors on grids too large for the CPU.
+//
+// Two data paths: global gathers (one thread per point; bands, FP64, 2-D)
+// and, for dense FP32 3-D grids, the bricks of the tensor-core stepper
+// (brick_stage.cuh: TMA-staged boxes, edge replication, the same departure
+// code) with the two forms evaluated on CUDA cores -- the equal-data-movement
+// comparison for the tensor-core contraction.
+#include "brick_stage.cuh"
 #include "dcell_common.cuh"
 #include "dcell_kernels.h"
 #include "sl_device.cuh"
@@ -21,28 +28,58 @@
 
 namespace dcell {
 
+// Coefficients with the 1331 non-zeros of M = C (x) C (x) C, then Horner per
+// axis: the polynomial of stencil s (s[x + 4y + 16z]) at fraction f.
+template <typename T>
+__device__ __forceinline__ T plain_eval3(const T *s, const T f[3]) {
+  T a[64];
+  DCELL_CR_COEFS3(s, a);
+  // p = sum a[i + 4j + 16k] x^i y^j z^k, Horner per axis
+  T pz = T(0);
+#pragma unroll
+  for (int k = 3; k >= 0; --k) {
+    T py = T(0);
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+      const T *r = a + 4 * j + 16 * k;
+      const T px = ((r[3] * f[0] + r[2]) * f[0] + r[1]) * f[0] + r[0];
+      py = py * f[1] + px;
+    }
+    pz = pz * f[2] + py;
+  }
+  return pz;
+}
+
+// 4-tap Catmull-Rom weights per axis applied to stencil s: 64 + 16 + 4
+// multiply-adds.
+template <typename T>
+__device__ __forceinline__ T separable_eval3(const T *s, const T f[3]) {
+  T wx[4], wy[4], wz[4];
+  cr_weights<T>(f[0], wx);
+  cr_weights<T>(f[1], wy);
+  cr_weights<T>(f[2], wz);
+  T acc = T(0);
+#pragma unroll
+  for (int z = 0; z < 4; ++z) {
+    T accy = T(0);
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+      T accx = T(0);
+#pragma unroll
+      for (int x = 0; x < 4; ++x) accx += wx[x] * s[x + 4 * y + 16 * z];
+      accy += wy[y] * accx;
+    }
+    acc += wz[z] * accy;
+  }
+  return acc;
+}
+
 template <typename T, int DIM>
 __device__ __forceinline__ T cubic_plain(const Geom &g, const T *__restrict__ phi0, const int c[3], const T f[3]) {
   if (DIM == 3) {
     T s[64];
     gather_stencil<T, 3>(g, phi0, c, s);
-    // a = M s with M = C (x) C (x) C: the 1331 non-zeros as straight-line code
-    T a[64];
-    DCELL_CR_COEFS3(s, a);
-    // p = sum a[i + 4j + 16k] x^i y^j z^k, Horner per axis
-    T pz = T(0);
-#pragma unroll
-    for (int k = 3; k >= 0; --k) {
-      T py = T(0);
-#pragma unroll
-      for (int j = 3; j >= 0; --j) {
-        const T *r = a + 4 * j + 16 * k;
-        const T px = ((r[3] * f[0] + r[2]) * f[0] + r[1]) * f[0] + r[0];
-        py = py * f[1] + px;
-      }
-      pz = pz * f[2] + py;
-    }
-    return pz;
+    return plain_eval3<T>(s, f);
   } else {
     T s[16];
     gather_stencil<T, 2>(g, phi0, c, s);
@@ -61,39 +98,21 @@ __device__ __forceinline__ T cubic_plain(const Geom &g, const T *__restrict__ ph
 
 template <typename T, int DIM>
 __device__ __forceinline__ T cubic_separable(const Geom &g, const T *__restrict__ phi0, const int c[3], const T f[3]) {
+  T s[DIM == 3 ? 64 : 16];
+  gather_stencil<T, DIM>(g, phi0, c, s);
+  if (DIM == 3) return separable_eval3<T>(s, f);
   T wx[4], wy[4];
   cr_weights<T>(f[0], wx);
   cr_weights<T>(f[1], wy);
-  T s[DIM == 3 ? 64 : 16];
-  gather_stencil<T, DIM>(g, phi0, c, s);
-  if (DIM == 3) {
-    T wz[4];
-    cr_weights<T>(f[2], wz);
-    T acc = T(0);
+  T acc = T(0);
 #pragma unroll
-    for (int z = 0; z < 4; ++z) {
-      T accy = T(0);
+  for (int y = 0; y < 4; ++y) {
+    T accx = T(0);
 #pragma unroll
-      for (int y = 0; y < 4; ++y) {
-        T accx = T(0);
-#pragma unroll
-        for (int x = 0; x < 4; ++x) accx += wx[x] * s[x + 4 * y + 16 * z];
-        accy += wy[y] * accx;
-      }
-      acc += wz[z] * accy;
-    }
-    return acc;
-  } else {
-    T acc = T(0);
-#pragma unroll
-    for (int y = 0; y < 4; ++y) {
-      T accx = T(0);
-#pragma unroll
-      for (int x = 0; x < 4; ++x) accx += wx[x] * s[x + 4 * y];
-      acc += wy[y] * accx;
-    }
-    return acc;
+    for (int x = 0; x < 4; ++x) accx += wx[x] * s[x + 4 * y];
+    acc += wy[y] * accx;
   }
+  return acc;
 }
 
 template <typename T, int DIM, bool SEPARABLE>
@@ -116,6 +135,117 @@ __global__ void __launch_bounds__(256) sl_cubic_kernel(Geom g, const T *__restri
   }
   if (clamped && band) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);  // dense grids: the edge is the domain boundary
   if (bad) raise_flag(flags, FLAG_BAD_BAND);
+}
+
+// Brick-staged CUDA-core step (dense FP32 3-D grids, nx % 4 == 0): the
+// tensor-core stepper's 32 x 4 x 8 bricks and TMA boxes (phi staged as FP32
+// here), double-buffered, edge-replicated, departures by brick_depart; the
+// coefficient solve and evaluation on CUDA cores (PLAIN: the 1331 non-zeros
+// and Horner; SEPARABLE: 4-tap weights).  256 threads: warp w owns tile row
+// w & 3 and brick planes 4 (w >> 2) .. 4 (w >> 2) + 3, two points per step
+// (the same (x, y) in consecutive planes), two steps per brick.  A warp whose
+// stencils leave the boxes takes the global path for that step.  Thread 0
+// issues the loads; one CTA barrier per brick frees its buffer.  Bounded
+// waits; on a timeout the CTA raises FLAG_WAIT_TIMEOUT, waits (bounded) for
+// its loads in flight and leaves.
+constexpr int kCcThreads = 256;
+
+template <int BT, bool SEP>
+__global__ void __launch_bounds__(kCcThreads, 2)
+    sl_cc_brick_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel, Geom g,
+                       BrickGrid bg, const float *__restrict__ phi0, const float *__restrict__ vel, float dt,
+                       float *__restrict__ phi, int *flags) {
+  using S = BrickBox<2>;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *const buf0 = smem, *const buf1 = smem + S::BufBytes;
+  uint64_t *const tbar = reinterpret_cast<uint64_t *>(smem + 2 * S::BufBytes);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    mbar_init(&tbar[0], 1);
+    mbar_init(&tbar[1], 1);
+  }
+  __syncthreads();
+  const int nbricks = bg.nbx * bg.nby * bg.nbz;
+  const int nmine = (int)blockIdx.x < nbricks ? (nbricks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  int issued[2] = {nmine > 0 ? 1 : 0, nmine > 1 ? 1 : 0};  // loads per buffer (thread 0 issues them)
+  if (tid == 0) {
+    if (nmine > 0) issue_brick<S>(bg, blockIdx.x, buf0, &tm_phi, &tm_vel, &tbar[0]);
+    if (nmine > 1) issue_brick<S>(bg, blockIdx.x + gridDim.x, buf1, &tm_phi, &tm_vel, &tbar[1]);
+  }
+  const float dth[3] = {dt / (float)g.hx, dt / (float)g.hy, dt / (float)g.hz};
+  const float hdth[3] = {-0.5f * dth[0], -0.5f * dth[1], -0.5f * dth[2]};
+  const int nn[3] = {g.nx, g.ny, g.nz};
+  const int ly = warp & 3, zg = warp >> 2;
+  int consumed[2] = {0, 0};
+  bool err = false;
+  for (int k = 0; k < nmine; ++k) {
+    const int bs = k & 1;
+    uint8_t *const cbuf = bs ? buf1 : buf0;
+    const bool ok = mbar_wait_sleep(&tbar[bs], (uint32_t)(k >> 1) & 1u);
+    if (__syncthreads_or(!ok)) {
+      err = true;
+      break;
+    }
+    ++consumed[bs];
+    int x0, y0, z0;
+    brick_origin<S>(bg, (int)blockIdx.x + k * (int)gridDim.x, x0, y0, z0);
+    if (x0 < 4 || x0 + S::PX - 4 > g.nx || y0 < 2 || y0 + S::PY - 2 > g.ny || z0 < 2 || z0 + S::PZ - 2 > g.nz) {
+      const int op[3] = {x0 - 4, y0 - 2, z0 - 2}, ov[3] = {x0 - 4, y0 - 1, z0 - 1};
+      for (int axis = 0; axis < 3; ++axis) {
+        replicate_pass<S::PX, S::PY, S::PZ, 1>(reinterpret_cast<uint32_t *>(cbuf), axis, op, nn, kCcThreads);
+        replicate_pass<S::VX, S::VY, S::VZ, 3>(reinterpret_cast<uint32_t *>(cbuf + S::PhiBytes), axis, ov, nn,
+                                               kCcThreads);
+        __syncthreads();
+      }
+    }
+    const float *pbox = reinterpret_cast<const float *>(cbuf);
+    const float *vbox = reinterpret_cast<const float *>(cbuf + S::PhiBytes);
+    const int x = min(x0 + lane, g.nx - 1), y = min(y0 + ly, g.ny - 1);
+    const bool xy_valid = x0 + lane < g.nx && y0 + ly < g.ny;
+#pragma unroll 1
+    for (int st = 0; st < 2; ++st) {
+      const int zl = 4 * zg + 2 * st;  // brick-local plane of point 0
+      float f[2][3];
+      int soff[2];
+      const bool in = brick_depart<BT, S, 2>(vbox, x - x0 + 4, y - y0 + 1, zl + 1, x - x0 + 4, y - y0 + 2, zl + 2,
+                                             dth, hdth, f, soff);
+      float v[2];
+      if (__all_sync(0xffffffffu, in)) {
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          float sv[64];
+          const float *q = pbox + soff[p];
+#pragma unroll
+          for (int e = 0; e < 64; ++e) sv[e] = q[((e >> 4) * S::PY + ((e >> 2) & 3)) * S::PX + (e & 3)];
+          v[p] = SEP ? separable_eval3<float>(sv, f[p]) : plain_eval3<float>(sv, f[p]);
+        }
+      } else {
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          int c[3];
+          float fg[3];
+          departure_cell<float, 3>(g, vel, dth, BT, x, y, min(z0 + zl + p, g.nz - 1), c, fg);
+          v[p] = SEP ? cubic_separable<float, 3>(g, phi0, c, fg) : cubic_plain<float, 3>(g, phi0, c, fg);
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        const int z = z0 + zl + p;
+        if (xy_valid && z < g.nz) phi[(z * g.ny + y) * g.nx + x] = v[p];
+      }
+    }
+    __syncthreads();  // the buffer read for the last time
+    if (k + 2 < nmine) {
+      if (tid == 0) issue_brick<S>(bg, (int)blockIdx.x + (k + 2) * (int)gridDim.x, cbuf, &tm_phi, &tm_vel, &tbar[bs]);
+      ++issued[bs];
+    }
+  }
+  if (err && tid == 0) {
+    // the load still in flight per buffer, if any
+    for (int b = 0; b < 2; ++b)
+      if (issued[b] > consumed[b]) mbar_wait(&tbar[b], (uint32_t)(issued[b] - 1) & 1u);
+    raise_flag(flags, FLAG_WAIT_TIMEOUT);
+  }
 }
 
 // Trilinear sample on the production gather (batched linear mode).
@@ -199,8 +329,54 @@ static void cubic_dispatch(const Geom &g, const T *phi0, const T *vel, T dt, con
   }
 }
 
+// Brick-staged CUDA-core step; false when the grid does not admit it or no
+// tensor maps could be made (the caller then runs the gather form).
+static bool launch_cc_brick(const Geom &g, const float *phi0, const float *vel, double dt, int interp, int backtrace,
+                            float *phi, int *flags, cudaStream_t st) {
+  using S = BrickBox<2>;
+  constexpr int smem = 2 * S::BufBytes + 16;
+  if (!tc_brick_applicable(g, phi0, vel)) return false;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(sl_cc_brick_kernel<DCELL_EULER, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess ||
+        cudaFuncSetAttribute(sl_cc_brick_kernel<DCELL_EULER, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess ||
+        cudaFuncSetAttribute(sl_cc_brick_kernel<DCELL_MIDPOINT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess ||
+        cudaFuncSetAttribute(sl_cc_brick_kernel<DCELL_MIDPOINT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess)
+      return false;
+    configured = true;
+  }
+  CUtensorMap tm_phi, tm_vel;
+  if (!make_tensor_map_3d(&tm_phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, phi0, (uint64_t)g.nx, (uint64_t)g.ny,
+                          (uint64_t)g.nz, S::PX, S::PY, S::PZ, 4) ||
+      !make_tensor_map_3d(&tm_vel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel, 3ull * g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
+                          3 * S::VX, S::VY, S::VZ, 4))
+    return false;
+  BrickGrid bg;
+  bg.nbx = (g.nx + S::BX - 1) / S::BX;
+  bg.nby = (g.ny + S::BY - 1) / S::BY;
+  bg.nbz = (g.nz + S::BZ - 1) / S::BZ;
+  bg.bz0 = 0;
+  const long long nbricks = (long long)bg.nbx * bg.nby * bg.nbz;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)(nbricks < 2LL * sms ? nbricks : 2LL * sms);
+  const bool mid = backtrace == DCELL_MIDPOINT, sep = interp == DCELL_CUBIC_SEPARABLE;
+  auto kern = mid ? (sep ? sl_cc_brick_kernel<DCELL_MIDPOINT, true> : sl_cc_brick_kernel<DCELL_MIDPOINT, false>)
+                  : (sep ? sl_cc_brick_kernel<DCELL_EULER, true> : sl_cc_brick_kernel<DCELL_EULER, false>);
+  kern<<<grid, kCcThreads, smem, st>>>(tm_phi, tm_vel, g, bg, phi0, vel, (float)dt, phi, flags);
+  return true;
+}
+
 int launch_sl_cubic(const Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
-                    long long npts, int interp, int backtrace, void *phi, int *flags, cudaStream_t st) {
+                    long long npts, int interp, int backtrace, void *phi, int *flags, cudaStream_t st, bool gather) {
+  if (dtype == DCELL_F32 && !band && g.nz > 1 && !gather &&
+      launch_cc_brick(g, (const float *)phi0, (const float *)vel, dt, interp, backtrace, (float *)phi, flags, st))
+    return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
   if (dtype == DCELL_F64)
     cubic_dispatch<double>(g, (const double *)phi0, (const double *)vel, dt, band, npts, interp, backtrace,
                            (double *)phi, flags, st);

@@ -1171,14 +1171,14 @@ static inline int grid_for(long long n, int threads) {
 }
 
 int launch_sl_linear(const Geom &g, int dtype, const void *phi0, const void *vel, double dt, const int *band,
-                     long long npts, int backtrace, void *phi, int *flags, cudaStream_t st) {
+                     long long npts, int backtrace, void *phi, int *flags, cudaStream_t st, bool gather) {
   const int threads = 256, blocks = grid_for(npts, threads);
   const bool is2d = g.nz == 1;
   // FP32 runs the fast unit (sl_lin.cu); this one keeps the reference's
   // FP64 operation order
   if (dtype == DCELL_F32)
     return launch_sl_lin_f32(g, (const float *)phi0, (const float *)vel, dt, band, npts, backtrace, (float *)phi,
-                             flags, st);
+                             flags, st, gather);
   if (is2d)
     sl_linear_kernel<double, 2><<<blocks, threads, 0, st>>>(g, (const double *)phi0, (const double *)vel, dt, band,
                                                             npts, backtrace, (double *)phi, flags);

@@ -24,6 +24,8 @@
 // the global-gather kernel with the same arithmetic.
 #include <math.h>
 
+#include <stdlib.h>
+
 #include <algorithm>
 
 #include "dcell_common.cuh"
@@ -34,18 +36,27 @@
 namespace dcell {
 namespace lin {
 
-constexpr int TX = 32, TY = 8;             // points of one plane per CTA (one warp per row)
-constexpr int kThreads = TX * TY;
+constexpr int TX = 32;                     // points of a tile row (one warp)
 constexpr int HX = 4, HY = 2;              // box halo (x: 4 keeps TMA x coordinates 16-byte aligned)
 constexpr int PW = TX + 2 * HX;            // 40 phi values per box row
-constexpr int PH = TY + 2 * HY;            // 12 box rows
 constexpr int VW = 3 * PW;                 // 120 velocity values per box row (u, v, w interleaved)
-constexpr int kPlanePhi = PW * PH;         // floats of one staged phi plane (1920 B)
-constexpr int kPlaneVel = VW * PH;         // floats of one staged velocity plane (5760 B)
-constexpr int kRing = 8;                   // ring slots: planes z-2 .. z+2 in use, three ahead
-constexpr int kPlaneBytes = 4 * (kPlanePhi + kPlaneVel);
-constexpr int kSmem = kRing * kPlaneBytes + kRing * 8;  // + one mbarrier per slot
-static_assert((4 * kPlanePhi) % 128 == 0 && (4 * kPlaneVel) % 128 == 0, "staged planes stay 128-byte aligned");
+constexpr int kRing = 8;                   // ring slots: planes z-2 .. z+2 in use, up to three ahead
+
+// A tile of TX x TY points per plane: TY consumer warps (one tile row each)
+// and one producer warp.  The staged planes are (TY + 4) box rows high.
+template <int TY_>
+struct MarchShape {
+  static constexpr int TY = TY_;
+  static constexpr int PH = TY + 2 * HY;
+  static constexpr int PlanePhi = PW * PH;  // floats of one staged phi plane
+  static constexpr int PlaneVel = VW * PH;  // floats of one staged velocity plane
+  static constexpr int PlaneBytes = 4 * (PlanePhi + PlaneVel);
+  static constexpr int Threads = 32 * (TY + 1);
+  static constexpr int Smem = kRing * PlaneBytes + 2 * kRing * 8;  // + full / empty mbarrier per slot
+  static constexpr int CtasPerSm = (228 * 1024) / (Smem + 1024) < 4 ? (228 * 1024) / (Smem + 1024) : 4;
+  static_assert((4 * PlanePhi) % 128 == 0 && (4 * PlaneVel) % 128 == 0, "staged planes stay 128-byte aligned");
+  static_assert(CtasPerSm >= 1, "ring too large for one CTA");
+};
 static_assert((kRing & (kRing - 1)) == 0 && kRing >= 8, "ring slot of plane p is (p + kRing) & (kRing - 1)");
 
 // phi0 / velocity through global memory, indices clamped into the grid (the
@@ -72,6 +83,7 @@ struct GlobalAcc {
 // grid-clamped position lies in the box the read equals the global clamped
 // read; any other index still reads inside the ring (a value that the caller
 // discards, since lin_point then reports the point as outside the box).
+template <class S>
 struct BoxAcc {
   const float *phis;  // ring of phi planes
   const float *vels;  // ring of velocity planes
@@ -80,15 +92,15 @@ struct BoxAcc {
   int rlo, rhi;       // box rows that hold grid rows
   __device__ __forceinline__ BoxAcc(const float *p, const float *v, int x0, int y0, int nx, int ny)
       : phis(p), vels(v), bx(x0 - HX), by(y0 - HY), clo(max(HX - x0, 0)), chi(min(nx - 1 - (x0 - HX), PW - 1)),
-        rlo(max(HY - y0, 0)), rhi(min(ny - 1 - (y0 - HY), PH - 1)) {}
+        rlo(max(HY - y0, 0)), rhi(min(ny - 1 - (y0 - HY), S::PH - 1)) {}
   __device__ __forceinline__ int col(int i) const { return clampi(i - bx, clo, chi); }
   __device__ __forceinline__ int row(int j) const { return clampi(j - by, rlo, rhi); }
   __device__ __forceinline__ static int slot(int k) { return (k + kRing) & (kRing - 1); }
   __device__ __forceinline__ float phi(int i, int j, int k) const {
-    return phis[slot(k) * kPlanePhi + row(j) * PW + col(i)];
+    return phis[slot(k) * S::PlanePhi + row(j) * PW + col(i)];
   }
   __device__ __forceinline__ float v(int i, int j, int k, int d) const {
-    return vels[slot(k) * kPlaneVel + row(j) * VW + 3 * col(i) + d];
+    return vels[slot(k) * S::PlaneVel + row(j) * VW + 3 * col(i) + d];
   }
 };
 
@@ -191,100 +203,115 @@ struct MarchGrid {
 };
 
 // Dense 3-D march (see the head of the file).  CTA b owns units
-// [b U / G, (b+1) U / G) in order: z-runs of one tile, a new run (ring
-// restart) where the range crosses into the next tile.  Thread 0 issues the
-// loads; all threads wait on the slot's mbarrier before a plane's first use;
-// one CTA barrier per plane releases the slot of plane z-2, which thread 0
-// then refills with plane z+6.  Warps whose points read outside the staged
-// box (per-axis displacement >= 2, or a midpoint offset >= 1) take the
-// global path for that plane.  Every wait is bounded; on a timeout the CTA
-// raises FLAG_WAIT_TIMEOUT, waits (bounded) for its loads in flight and
-// leaves.
-template <int BT>
-__global__ void __launch_bounds__(kThreads, 3)
+// [b U / G, (b+1) U / G) in order: z-runs of one tile, a new run where the
+// range crosses into the next tile.  A producer warp loads every plane a run
+// reads (zs-2 .. ze+1) into the ring, each one once the slot's previous plane
+// is released; the TY consumer warps wait on a slot's `full` mbarrier before
+// a plane's first use, compute their row of the plane, and release plane z-2
+// on its `empty` mbarrier after plane z (the last planes of a run at its
+// end).  No CTA barrier in the loop: warps drift up to a few planes apart.
+// Warps whose points read outside the staged box (per-axis displacement
+// >= 2, or a midpoint offset >= 1) take the global path for that plane.
+// Every wait is bounded; a warp that gives up raises FLAG_WAIT_TIMEOUT and
+// leaves (the others then give up at their next wait), and the producer
+// waits (bounded) for its last load per slot before the CTA ends.
+template <int BT, int TY>
+__global__ void __launch_bounds__(MarchShape<TY>::Threads, MarchShape<TY>::CtasPerSm)
     sl_lin_march_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel,
                         Geom g, MarchGrid mg, const float *__restrict__ phi0, const float *__restrict__ vel, float dth0,
                         float dth1, float dth2, float *__restrict__ phi, int *flags) {
+  using S = MarchShape<TY>;
   extern __shared__ __align__(1024) uint8_t smem[];
   float *const phis = reinterpret_cast<float *>(smem);
-  float *const vels = phis + kRing * kPlanePhi;
-  uint64_t *const full = reinterpret_cast<uint64_t *>(smem + kRing * kPlaneBytes);
-  const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5;
+  float *const vels = phis + kRing * S::PlanePhi;
+  uint64_t *const full = reinterpret_cast<uint64_t *>(smem + kRing * S::PlaneBytes);
+  uint64_t *const empty = full + kRing;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0)
-    for (int s = 0; s < kRing; ++s) mbar_init(&full[s], 1);
+    for (int s = 0; s < kRing; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], TY);
+    }
   __syncthreads();
 
+  const int U = mg.units, G = (int)gridDim.x, b = (int)blockIdx.x;
+  const int ubeg = (int)((long long)U * b / G), uend = (int)((long long)U * (b + 1) / G);
+
+  if (warp == TY) {  // ---------------- producer ----------------
+    if (lane == 0) {
+      uint32_t used = 0, epar = 0, lastpar = 0;  // per slot: loaded once, next empty phase, phase of the last load
+      bool err = false;
+      for (int u = ubeg; u < uend && !err;) {
+        const int tile = u / g.nz, zs = u - tile * g.nz, ze = min(g.nz, zs + (uend - u));
+        u += ze - zs;
+        const int x0 = (tile % mg.ncx) * TX, y0 = (tile / mg.ncx) * TY;
+        for (int p = zs - 2; p <= ze + 1; ++p) {
+          const int s = BoxAcc<S>::slot(p), pz = clampi(p, 0, g.nz - 1);
+          const uint32_t bit = 1u << s;
+          if (used & bit) {
+            if (!mbar_wait(&empty[s], (epar & bit) ? 1u : 0u)) {
+              err = true;
+              break;
+            }
+            epar ^= bit;
+            lastpar ^= bit;
+          }
+          used |= bit;
+          fence_proxy_async();  // the consumers' reads of the slot before these writes
+          mbar_expect_tx(&full[s], (uint32_t)S::PlaneBytes);
+          tma_load_3d(phis + s * S::PlanePhi, &tm_phi, x0 - HX, y0 - HY, pz, &full[s]);
+          tma_load_3d(vels + s * S::PlaneVel, &tm_vel, 3 * (x0 - HX), y0 - HY, pz, &full[s]);
+        }
+      }
+      // nothing may still be in flight when the CTA's shared memory goes away
+      bool ok = true;
+      for (int s = 0; s < kRing; ++s)
+        if (used & (1u << s)) ok &= mbar_wait(&full[s], (lastpar >> s) & 1u);
+      if (err || !ok) raise_flag(flags, FLAG_WAIT_TIMEOUT);
+    }
+    return;
+  }
+  // ---------------- consumers: warp = tile row ----------------
   const float dth[3] = {dth0, dth1, dth2};
   const float hdth[3] = {-0.5f * dth0, -0.5f * dth1, -0.5f * dth2};
   const GlobalAcc<3> gacc{phi0, vel, g.nx, g.ny, g.nz};
-  const int U = mg.units, G = (int)gridDim.x, b = (int)blockIdx.x;
-  const int ubeg = (int)((long long)U * b / G), uend = (int)((long long)U * (b + 1) / G);
-  uint32_t parity = 0;         // bit s: phase of slot s's next completion (same in every thread)
-  int issued = 0, waited = 0;  // planes of the current run loaded / waited for, up to (exclusive)
+  uint32_t fpar = 0;  // bit s: phase of slot s's next full completion
   bool err = false;
-
-  auto issue = [&](int x0, int y0, int p) {  // thread 0: plane p of the tile at (x0, y0) into its slot
-    const int s = BoxAcc::slot(p), pz = clampi(p, 0, g.nz - 1);
-    mbar_expect_tx(&full[s], (uint32_t)kPlaneBytes);
-    tma_load_3d(phis + s * kPlanePhi, &tm_phi, x0 - HX, y0 - HY, pz, &full[s]);
-    tma_load_3d(vels + s * kPlaneVel, &tm_vel, 3 * (x0 - HX), y0 - HY, pz, &full[s]);
-  };
-
   for (int u = ubeg; u < uend && !err;) {
-    const int tile = u / g.nz, zs = u - tile * g.nz;
-    const int ze = min(g.nz, zs + (uend - u));
+    const int tile = u / g.nz, zs = u - tile * g.nz, ze = min(g.nz, zs + (uend - u));
     u += ze - zs;
     const int x0 = (tile % mg.ncx) * TX, y0 = (tile / mg.ncx) * TY;
-    const int last = ze + 1;                      // the last plane this run reads (ze - 1 + 2)
-    const int head = min(zs + kRing - 3, last);   // the prologue loads planes zs - 2 .. head
-    if (tid == 0) {
-      fence_proxy_async();  // earlier reads of the ring before these writes
-      for (int p = zs - 2; p <= head; ++p) issue(x0, y0, p);
-    }
-    issued = head + 1;
-    waited = zs - 2;
-    const BoxAcc bacc(phis, vels, x0, y0, g.nx, g.ny);
-    const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
-    const bool store = x0 + lx < g.nx && y0 + ly < g.ny;
+    const BoxAcc<S> bacc(phis, vels, x0, y0, g.nx, g.ny);
+    const int x = min(x0 + lane, g.nx - 1), y = min(y0 + warp, g.ny - 1);
+    const bool store = x0 + lane < g.nx && y0 + warp < g.ny;
+    int waited = zs - 2;
     for (int z = zs; z < ze; ++z) {
-      for (; !err && waited <= z + 2; ++waited) {  // planes up to z + 2 present
-        const int s = BoxAcc::slot(waited);
-        if (!mbar_wait_sleep(&full[s], (parity >> s) & 1u)) {
+      for (; waited <= z + 2; ++waited) {  // planes up to z + 2 present
+        const int s = BoxAcc<S>::slot(waited);
+        const bool ok = mbar_wait_sleep(&full[s], (fpar >> s) & 1u);
+        if (!__all_sync(0xffffffffu, ok)) {
           err = true;
           break;
         }
-        parity ^= 1u << s;
+        fpar ^= 1u << s;
       }
-      // (after a timeout the ring holds stale values: reads stay in bounds,
-      // the results are discarded with the flag raised)
+      if (err) break;
       bool in;
       int c[3];
       float f[3];
       float v = lin_point<BT, 3>(bacc, x, y, z, dth, hdth, in, c, f);
       if (!__all_sync(0xffffffffu, in)) v = lin_point<BT, 3>(gacc, x, y, z, dth, hdth, in, c, f);
       if (store) phi[(z * g.ny + y) * g.nx + x] = v;
-      if (__syncthreads_or(err)) {  // also: slot of plane z - 2 read for the last time
-        err = true;
-        break;
-      }
-      if (issued <= last) {  // refill that slot with plane z + 6
-        if (tid == 0) {
-          fence_proxy_async();
-          issue(x0, y0, issued);
-        }
-        ++issued;
-      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[BoxAcc<S>::slot(z - 2)]);  // plane z - 2 read for the last time
+    }
+    if (!err) {
+      __syncwarp();
+      if (lane == 0)
+        for (int p = max(ze - 2, zs - 2); p <= ze + 1; ++p) mbar_arrive(&empty[BoxAcc<S>::slot(p)]);
     }
   }
-  if (err && tid == 0) {
-    // loads still in flight: planes [waited, issued) of the run that stopped
-    for (int p = waited; p < issued; ++p) {
-      const int s = BoxAcc::slot(p);
-      if (!mbar_wait(&full[s], (parity >> s) & 1u)) break;
-      parity ^= 1u << s;
-    }
-    raise_flag(flags, FLAG_WAIT_TIMEOUT);
-  }
+  if (err && lane == 0) raise_flag(flags, FLAG_WAIT_TIMEOUT);
 }
 
 }  // namespace lin
@@ -299,36 +326,58 @@ static bool lin_march_applicable(const Geom &g, const void *phi0, const void *ve
          ((uintptr_t)vel % 16) == 0;
 }
 
+// Tile rows of the z-march: 8 (three CTAs per SM) or 16 (two);
+// DCELL_LIN_TILE_ROWS overrides the default.
+static int lin_tile_rows() {
+  static int rows = 0;
+  if (!rows) {
+    rows = 8;
+    if (const char *e = getenv("DCELL_LIN_TILE_ROWS")) rows = atoi(e) == 16 ? 16 : 8;
+  }
+  return rows;
+}
+
+// Launches the march; false when no tensor maps could be made.
+template <int TY>
+static bool launch_march(const Geom &g, const float *phi0, const float *vel, float dth0, float dth1, float dth2,
+                         bool mid, float *phi, int *flags, cudaStream_t st) {
+  using S = lin::MarchShape<TY>;
+  static bool configured = false;
+  if (!configured) {
+    if (cudaFuncSetAttribute(lin::sl_lin_march_kernel<DCELL_EULER, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             S::Smem) != cudaSuccess ||
+        cudaFuncSetAttribute(lin::sl_lin_march_kernel<DCELL_MIDPOINT, TY>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, S::Smem) != cudaSuccess)
+      return false;
+    configured = true;
+  }
+  CUtensorMap tm_phi, tm_vel;
+  if (!make_tensor_map_3d(&tm_phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, phi0, (uint64_t)g.nx, (uint64_t)g.ny,
+                          (uint64_t)g.nz, lin::PW, S::PH, 1, 4) ||
+      !make_tensor_map_3d(&tm_vel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel, 3ull * g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
+                          lin::VW, S::PH, 1, 4))
+    return false;
+  lin::MarchGrid mg;
+  mg.ncx = (g.nx + lin::TX - 1) / lin::TX;
+  const int ncy = (g.ny + TY - 1) / TY;
+  mg.units = mg.ncx * ncy * g.nz;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::min(S::CtasPerSm * sms, mg.units);
+  auto kern = mid ? lin::sl_lin_march_kernel<DCELL_MIDPOINT, TY> : lin::sl_lin_march_kernel<DCELL_EULER, TY>;
+  kern<<<grid, S::Threads, S::Smem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0, dth1, dth2, phi, flags);
+  return true;
+}
+
 int launch_sl_lin_f32(const Geom &g, const float *phi0, const float *vel, double dt, const int *band, long long npts,
-                      int backtrace, float *phi, int *flags, cudaStream_t st) {
+                      int backtrace, float *phi, int *flags, cudaStream_t st, bool gather) {
   const float dth0 = (float)(dt / g.hx), dth1 = (float)(dt / g.hy), dth2 = (float)(dt / g.hz);
   const bool mid = backtrace == DCELL_MIDPOINT;
-  if (!band && lin_march_applicable(g, phi0, vel)) {
-    static bool configured = false;
-    if (!configured) {
-      DCELL_CUDA_CHECK(cudaFuncSetAttribute(lin::sl_lin_march_kernel<DCELL_EULER>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, lin::kSmem));
-      DCELL_CUDA_CHECK(cudaFuncSetAttribute(lin::sl_lin_march_kernel<DCELL_MIDPOINT>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, lin::kSmem));
-      configured = true;
-    }
-    CUtensorMap tm_phi, tm_vel;
-    if (make_tensor_map_3d(&tm_phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, phi0, (uint64_t)g.nx, (uint64_t)g.ny,
-                           (uint64_t)g.nz, lin::PW, lin::PH, 1, 4) &&
-        make_tensor_map_3d(&tm_vel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel, 3ull * g.nx, (uint64_t)g.ny,
-                           (uint64_t)g.nz, lin::VW, lin::PH, 1, 4)) {
-      lin::MarchGrid mg;
-      mg.ncx = (g.nx + lin::TX - 1) / lin::TX;
-      const int ncy = (g.ny + lin::TY - 1) / lin::TY;
-      mg.units = mg.ncx * ncy * g.nz;
-      int dev = 0, sms = 148;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      const int grid = std::min(3 * sms, mg.units);
-      auto kern = mid ? lin::sl_lin_march_kernel<DCELL_MIDPOINT> : lin::sl_lin_march_kernel<DCELL_EULER>;
-      kern<<<grid, lin::kThreads, lin::kSmem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0, dth1, dth2, phi, flags);
+  if (!band && !gather && lin_march_applicable(g, phi0, vel)) {
+    if (lin_tile_rows() == 16 ? launch_march<16>(g, phi0, vel, dth0, dth1, dth2, mid, phi, flags, st)
+                              : launch_march<8>(g, phi0, vel, dth0, dth1, dth2, mid, phi, flags, st))
       return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
-    }
     // no tensor maps (driver entry point unavailable): the gather form below
   }
   const int n = (int)npts;

@@ -65,6 +65,14 @@ enum {
                                 GEMM with FP32 accumulation (3D, FP32 only) */
 };
 
+/* OR'ed into interp: run the global-gather form of DCELL_LINEAR /
+ * DCELL_CUBIC_PLAIN / DCELL_CUBIC_SEPARABLE on a dense FP32 3D grid (one
+ * thread per point, every value gathered from global memory) instead of its
+ * shared-memory-staged form (TMA z-march for LINEAR, TMA bricks for the two
+ * cubic forms).  Both forms give the same results; the flag exists to compare
+ * their data paths. */
+#define DCELL_GATHER_FORM 0x100
+
 /* departure-point backtrace */
 enum {
   DCELL_EULER = 0,    /* S = X - V(X) dt/h, V at the arrival point (AdvectSL.c:44-47, :78-82) */
@@ -124,7 +132,8 @@ DCELL_API int dcell_version(void);
  * skipped and raise DCELL_FLAG_BAD_BAND.  Grids are limited to
  * 3 * points < 2^31.  flags (optional int on the device) receives
  * DCELL_FLAG_* bits.  DCELL_CUBIC_TC requires dtype F32 and a 3D
- * grid. */
+ * grid.  Dense FP32 3D grids with nx % 4 == 0 and 16-byte aligned arrays run
+ * the shared-memory-staged forms unless interp carries DCELL_GATHER_FORM. */
 #define DCELL_FLAG_DEPARTURE_CLAMPED 1
 #define DCELL_FLAG_NONFINITE 2
 #define DCELL_FLAG_CAPACITY 4

@@ -18,8 +18,12 @@
  *   OrthogonalProjection2D/3D   LevelSetMethod/OrthogonalProjection*.c
  *   TricubicInverse.h           (64 Catmull-Rom coefficients of a 4^3 stencil)
  *   particle level set          LevelSetMethod/ParticleLS.c, ParticleLS2D.c, ParticleLS3D.c
+ *   GridWrite                   Common/Serialize.c:23 (PETSc binary viewer in the shim)
+ *   LevelSetWriteIrregularNodeList  LevelSetMethod/IrregularNodes.c:224
+ *   ArrayWrite                  Common/Array.c:134
  */
 #include <stdlib.h>
+#include <string.h>
 #include "LevelSetMethod.h"
 #include "LSM_private.h"
 
@@ -398,4 +402,55 @@ DREF_EXPORT void dref_rand48_get(unsigned short *s) {
 DREF_EXPORT void dref_rand48_set(const unsigned short *s) {
   unsigned short t[3] = {s[0], s[1], s[2]};
   seed48(t);
+}
+
+/* ---------------------------------------------------------------------------
+ * Output in the reference's file formats, through its own writers. */
+void dcell_shim_set_dirs(const char *wd, const char *tmp);
+
+/* directories of DCellGetWorkingDirectory (grids, node lists) and PetscGetTmp (Arrays) */
+DREF_EXPORT void dref_set_dirs(const char *wd, const char *tmp) { dcell_shim_set_dirs(wd, tmp); }
+
+/* GridWrite (Common/Serialize.c:23) of a grid, named first (GridSetName,
+ * Common/Grid.c:162, which also restarts the grid's .pos / .size files) when
+ * its name differs */
+static int named_write(Grid g, const char *name, int t) {
+  if (strcmp(g->name, name)) {
+    int e = GridSetName(g, name);
+    if (e) return e;
+  }
+  return GridWrite(g, t);
+}
+DREF_EXPORT int dref_grid_write(void *h, const char *name, int t) { return named_write(((LevelSet)h)->phi, name, t); }
+/* the same for a velocity grid (dof 2 / 3) */
+DREF_EXPORT int dref_vel_write(void *v, const char *name, int t) { return named_write((Grid)v, name, t); }
+
+/* The surface quantities of every irregular node (normal n and curvature k,
+ * computed as dref_get_irregular's with_surface export does) stored in the
+ * nodes, so that the node-list writer has non-zero values to write. */
+DREF_EXPORT int dref_set_surface(void *h) {
+  LevelSet ls = (LevelSet)h;
+  int len = ArrayLength(ls->irregularNodes);
+  double *rows = (double *)malloc(sizeof(double) * 18 * (size_t)(len > 0 ? len : 1));
+  if (!rows) return PETSC_ERR_MEM;
+  dref_get_irregular(h, rows, 1);
+  IrregularNode *nodes = (IrregularNode *)ArrayGetData(ls->irregularNodes);
+  for (int i = 0; i < len; ++i) {
+    nodes[i].nx = rows[18 * i + 14];
+    nodes[i].ny = rows[18 * i + 15];
+    nodes[i].nz = rows[18 * i + 16];
+    nodes[i].k = rows[18 * i + 17];
+  }
+  free(rows);
+  return len;
+}
+
+/* LevelSetWriteIrregularNodeList (IrregularNodes.c:224-246) */
+DREF_EXPORT int dref_write_irregular(void *h, int idx) { return LevelSetWriteIrregularNodeList((LevelSet)h, idx); }
+
+/* ArrayWrite (Array.c:134-150) of the particle Array (ParticleLSWriteParticles' call) */
+DREF_EXPORT int dref_pls_write(void *h, int t) {
+  LevelSet ls = (LevelSet)h;
+  if (!ls->pls) return 1;
+  return ArrayWrite(ls->pls->particles, t);
 }

@@ -75,6 +75,14 @@ def lib(path=PATH):
         L.dref_rand48_get.restype = None
         L.dref_rand48_set.argtypes = [vp]
         L.dref_rand48_set.restype = None
+        if hasattr(L, "dref_grid_write"):  # the reference's writers (Common/Serialize.c, IrregularNodes.c, Array.c)
+            L.dref_set_dirs.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+            L.dref_set_dirs.restype = None
+            L.dref_grid_write.argtypes = [vp, ctypes.c_char_p, i]
+            L.dref_vel_write.argtypes = [vp, ctypes.c_char_p, i]
+            L.dref_set_surface.argtypes = [vp]
+            L.dref_write_irregular.argtypes = [vp, i]
+            L.dref_pls_write.argtypes = [vp, i]
         if hasattr(L, "dref_advect_mac"):  # the reference-only library (shim/mac)
             L.dref_advect_mac.argtypes = [vp, vp, vp, vp, vp, vp, vp, d, vp]
         _LIBS[path] = L
@@ -218,6 +226,31 @@ class RefLevelSet:
 
     def reinitialize(self):
         assert self.L.dref_reinitialize(self.h) == 0
+
+    # output through the reference's own writers, into `wd` (grids, node
+    # lists: DCellGetWorkingDirectory) and `tmp` (Arrays: PetscGetTmp)
+    def set_output_dirs(self, wd, tmp):
+        self.L.dref_set_dirs(wd.encode(), tmp.encode())
+
+    def grid_write(self, name, t):
+        """GridSetName + GridWrite (Common/Serialize.c:23-55) of phi."""
+        assert self.L.dref_grid_write(self.h, name.encode(), int(t)) == 0
+
+    def velocity_write(self, name, t):
+        """GridWrite of the velocity grid set by set_velocity (dof 2 / 3)."""
+        assert self.L.dref_vel_write(self._vel, name.encode(), int(t)) == 0
+
+    def set_surface(self):
+        """Store the node normals and curvature in the irregular nodes."""
+        return self.L.dref_set_surface(self.h)
+
+    def write_irregular(self, idx):
+        """LevelSetWriteIrregularNodeList (IrregularNodes.c:224-246)."""
+        assert self.L.dref_write_irregular(self.h, int(idx)) == 0
+
+    def write_particles(self, t):
+        """ArrayWrite (Common/Array.c:134-150) of the particle Array."""
+        assert self.L.dref_pls_write(self.h, int(t)) == 0
 
     def get_velocity(self, global_field):
         """LevelSetGetVelocity (Advect.c:145-192) from a one-process Global

@@ -63,10 +63,31 @@ PetscErrorCode VecCopy(Vec x, Vec y) {
   return 0;
 }
 
+/* File viewers.  PETSc is absent, so its binary format is restated from its
+ * documentation: big-endian values; a Vec is the class id 1211214 (int32),
+ * its length (int32), then its values; a binary viewer opened for writing
+ * creates `<name>.info` beside the file, into which VecView writes
+ * "-vecload_block_size <bs>" for a block size above one. */
+struct dcell_shim_viewer {
+  FILE *f;    /* the file */
+  FILE *info; /* binary viewers: <name>.info */
+  int binary;
+};
+
+static void put_be(FILE *f, const void *p, size_t elem, size_t n) {
+  const unsigned char *b = (const unsigned char *)p;
+  for (size_t i = 0; i < n; ++i)
+    for (size_t k = 0; k < elem; ++k) fputc(b[i * elem + (elem - 1 - k)], f);
+}
+
 PetscErrorCode VecView(Vec v, PetscViewer w) {
-  (void)v;
-  (void)w;
-  return 0;
+  struct dcell_shim_viewer *sv = (struct dcell_shim_viewer *)w;
+  if (!sv || !sv->binary) return 0;
+  const int head[2] = {1211214, v->n};
+  put_be(sv->f, head, sizeof(int), 2);
+  put_be(sv->f, v->array, sizeof(double), (size_t)v->n);
+  if (v->bs > 1 && sv->info) fprintf(sv->info, "-vecload_block_size %d\n", v->bs);
+  return ferror(sv->f) ? dcell_shim_error(66, "VecView: write failed") : 0;
 }
 
 /* 2-d table: one block holding m row pointers; a[i] = array + (i-ms)*n - ns. */
@@ -139,24 +160,99 @@ PetscErrorCode VecRestoreArray4d(Vec x, PetscInt m, PetscInt n, PetscInt p, Pets
   return 0;
 }
 
-PetscErrorCode PetscViewerDestroy(PetscViewer *v) { if (v) *v = NULL; return 0; }
+PetscErrorCode PetscViewerDestroy(PetscViewer *v) {
+  if (v && *v) {
+    struct dcell_shim_viewer *sv = (struct dcell_shim_viewer *)*v;
+    if (sv->f) fclose(sv->f);
+    if (sv->info) fclose(sv->info);
+    free(sv);
+  }
+  if (v) *v = NULL;
+  return 0;
+}
+static PetscErrorCode open_viewer(const char *name, int binary, PetscViewer *v) {
+  struct dcell_shim_viewer *sv = (struct dcell_shim_viewer *)calloc(1, sizeof(*sv));
+  if (!sv) return PETSC_ERR_MEM;
+  sv->binary = binary;
+  sv->f = fopen(name, binary ? "wb" : "w");
+  if (!sv->f) {
+    free(sv);
+    return dcell_shim_error(65, "cannot open %s", name);
+  }
+  if (binary) {
+    char info[PETSC_MAX_PATH_LEN];
+    snprintf(info, sizeof info, "%s.info", name);
+    sv->info = fopen(info, "w");
+  }
+  *v = sv;
+  return 0;
+}
 PetscErrorCode PetscViewerBinaryOpen(MPI_Comm c, const char *name, PetscFileMode m, PetscViewer *v) {
-  (void)c; (void)name; (void)m; *v = NULL; return 0;
+  (void)c;
+  if (m != FILE_MODE_WRITE) return dcell_shim_error(56, "PetscViewerBinaryOpen: only FILE_MODE_WRITE is supported");
+  return open_viewer(name, 1, v);
 }
 PetscErrorCode PetscViewerASCIIOpen(MPI_Comm c, const char *name, PetscViewer *v) {
-  (void)c; (void)name; *v = NULL; return 0;
+  (void)c;
+  return open_viewer(name, 0, v);
 }
-PetscErrorCode PetscViewerASCIIPrintf(PetscViewer v, const char *fmt, ...) { (void)v; (void)fmt; return 0; }
+PetscErrorCode PetscViewerASCIIPrintf(PetscViewer v, const char *fmt, ...) {
+  struct dcell_shim_viewer *sv = (struct dcell_shim_viewer *)v;
+  if (!sv) return 0;
+  va_list ap;
+  va_start(ap, fmt);
+  vfprintf(sv->f, fmt, ap);
+  va_end(ap);
+  fflush(sv->f);
+  return 0;
+}
 PetscErrorCode PetscViewerBinaryWrite(PetscViewer v, void *d, PetscInt n, PetscDataType t, PetscBool tmp) {
-  (void)v; (void)d; (void)n; (void)t; (void)tmp; return 0;
+  struct dcell_shim_viewer *sv = (struct dcell_shim_viewer *)v;
+  (void)tmp;
+  if (!sv) return 0;
+  if (t == PETSC_DOUBLE) put_be(sv->f, d, sizeof(double), (size_t)n);
+  else if (t == PETSC_INT) put_be(sv->f, d, sizeof(int), (size_t)n);
+  else fwrite(d, 1, (size_t)n, sv->f);
+  return 0;
 }
-PetscErrorCode PetscGetTmp(MPI_Comm c, char *dir, size_t len) { (void)c; snprintf(dir, len, "/tmp"); return 0; }
-PetscErrorCode PetscGetWorkingDirectory(char *dir, size_t len) { snprintf(dir, len, "."); return 0; }
-PetscErrorCode PetscBinaryOpen(const char *name, PetscFileMode m, int *fd) { (void)name; (void)m; *fd = -1; return 0; }
+/* Output directories of the reference's writers: DCellGetWorkingDirectory
+ * (grids, node lists) and PetscGetTmp (Array files); set by the driver. */
+static char g_wd[PETSC_MAX_PATH_LEN] = ".";
+static char g_tmp[PETSC_MAX_PATH_LEN] = "/tmp";
+void dcell_shim_set_dirs(const char *wd, const char *tmp) {
+  if (wd) snprintf(g_wd, sizeof g_wd, "%s", wd);
+  if (tmp) snprintf(g_tmp, sizeof g_tmp, "%s", tmp);
+}
+PetscErrorCode PetscGetTmp(MPI_Comm c, char *dir, size_t len) { (void)c; snprintf(dir, len, "%s", g_tmp); return 0; }
+PetscErrorCode PetscGetWorkingDirectory(char *dir, size_t len) { snprintf(dir, len, "%s", g_wd); return 0; }
+/* PetscBinaryOpen / Write / Close over a FILE * kept in a small table. */
+static FILE *g_bin[16];
+PetscErrorCode PetscBinaryOpen(const char *name, PetscFileMode m, int *fd) {
+  if (m != FILE_MODE_WRITE) return dcell_shim_error(56, "PetscBinaryOpen: only FILE_MODE_WRITE is supported");
+  for (int i = 0; i < 16; ++i)
+    if (!g_bin[i]) {
+      g_bin[i] = fopen(name, "wb");
+      if (!g_bin[i]) return dcell_shim_error(65, "cannot open %s", name);
+      *fd = i;
+      return 0;
+    }
+  return dcell_shim_error(55, "PetscBinaryOpen: too many open files");
+}
 PetscErrorCode PetscBinaryWrite(int fd, void *p, PetscInt n, PetscDataType t, PetscBool tmp) {
-  (void)fd; (void)p; (void)n; (void)t; (void)tmp; return 0;
+  (void)tmp;
+  if (fd < 0 || fd >= 16 || !g_bin[fd]) return dcell_shim_error(62, "PetscBinaryWrite: bad descriptor");
+  if (t == PETSC_DOUBLE) put_be(g_bin[fd], p, sizeof(double), (size_t)n);
+  else if (t == PETSC_INT) put_be(g_bin[fd], p, sizeof(int), (size_t)n);
+  else fwrite(p, 1, (size_t)n, g_bin[fd]);
+  return 0;
 }
-PetscErrorCode PetscBinaryClose(int fd) { (void)fd; return 0; }
+PetscErrorCode PetscBinaryClose(int fd) {
+  if (fd >= 0 && fd < 16 && g_bin[fd]) {
+    fclose(g_bin[fd]);
+    g_bin[fd] = NULL;
+  }
+  return 0;
+}
 PetscErrorCode MatView(Mat m, PetscViewer v) { (void)m; (void)v; return 0; }
 int MPI_Comm_rank(MPI_Comm c, int *rank) { (void)c; *rank = 0; return 0; }
 
@@ -245,6 +341,8 @@ PetscErrorCode PetscRandomDestroy(PetscRandom *r) {
  * oracle does not build (GA gather glue, file output). */
 typedef struct _Array *Array;
 PetscErrorCode GAGather(int ga, Array c, Array v) { (void)ga; (void)c; (void)v; return 1; }
-PetscErrorCode DCellGetWorkingDirectory(char *wd) { strcpy(wd, "."); return 0; }
-typedef struct _Grid *Grid;
-PetscErrorCode GridWrite(Grid g, int t) { (void)g; (void)t; return 0; }
+/* The reference's own DCellGetWorkingDirectory (Common/Serialize.c:9-19)
+ * caches the directory in a `static const` array, which gcc places in
+ * read-only memory; its object's definition is weakened at link time and this
+ * one, returning the same directory (PetscGetWorkingDirectory's), is used. */
+PetscErrorCode DCellGetWorkingDirectory(char *wd) { return PetscGetWorkingDirectory(wd, PETSC_MAX_PATH_LEN); }

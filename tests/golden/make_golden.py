@@ -11,6 +11,7 @@ reference saw.
 
     python tests/golden/make_golden.py        # needs oracle/_ref/libdcell_ref.so
     python tests/golden/make_golden.py mac    # only mac.npz
+    python tests/golden/make_golden.py writer # only writer.npz
 """
 from __future__ import annotations
 
@@ -215,12 +216,79 @@ def run_mac():
     return res
 
 
+def run_writer():
+    """The reference's own writers, into a scratch directory: GridWrite
+    (Common/Serialize.c:23-55; two writes of one grid, so .pos / .size hold two
+    lines; a velocity grid of dof 3 and one of dof 2), the node lists of a 3D
+    and a 2D level set (LevelSetWriteIrregularNodeList,
+    IrregularNodes.c:145-246; nodes from the reference's own irregular-node
+    pass with normals and curvature stored in them) and a particle Array
+    (ArrayWrite, Common/Array.c:134-150).  Stored: the inputs, and every file's
+    bytes under "file:<name>"."""
+    import tempfile
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        wd, tmp = os.path.join(d, "wd"), os.path.join(d, "tmp")
+        os.makedirs(wd)
+        os.makedirs(tmp)
+        # 3D: a sphere (cell units) on a 16 x 18 x 20 (z, y, x) box at origin (-3, 2, 1)
+        phi3, vel3, band3 = sphere_case((16, 18, 20), (-3, 2, 1), 0.1, (6.3, 10.6, 8.4), 4.7, seed=21)
+        ls = R.RefLevelSet.create(0.1, (-3, 2, 1), phi3.shape)
+        ls.set_output_dirs(wd, tmp)
+        ls.set_phi(phi3)
+        ls.set_band(band3)
+        ls.update_irregular()
+        ls.set_surface()
+        nodes3 = ls.nodes_no_update(ls.update_irregular(), surface=True)
+        ls.set_surface()
+        ls.grid_write("ls3", 0)
+        ls.set_phi(f32(phi3 * 0.5))
+        ls.grid_write("ls3", 1)
+        ls.set_phi(phi3)
+        ls.write_irregular(2)
+        ls.set_velocity(vel3)
+        ls.velocity_write("vel3", 4)
+        ls.close()
+        # 2D: a circle on a 26 x 30 (y, x) box at origin (5, -4)
+        phi2, vel2, band2 = circle_case((26, 30), (5, -4), (18.3, 8.6), 6.2, seed=22)
+        ls = R.RefLevelSet.create(0.1, (5, -4), phi2.shape)
+        ls.set_output_dirs(wd, tmp)
+        ls.set_phi(phi2)
+        ls.set_band(band2)
+        n2 = ls.update_irregular()
+        ls.set_surface()
+        nodes2 = ls.nodes_no_update(n2, surface=True)
+        ls.grid_write("ls2", 7)
+        ls.write_irregular(0)
+        ls.set_velocity(vel2)
+        ls.velocity_write("vel2", 1)
+        ls.close()
+        # particles: the reference's own 2D seeding of a circle
+        ls = R.RefLevelSet.circle(1.0 / 24, (0.4512, 0.5371), 0.1)
+        ls.set_output_dirs(wd, tmp)
+        ls.pls_init()
+        parts = ls.particles()
+        ls.write_particles(3)
+        ls.close()
+        for sub, base in (("wd", wd), ("tmp", tmp)):
+            for name in sorted(os.listdir(base)):
+                with open(os.path.join(base, name), "rb") as f:
+                    out[f"file:{sub}/{name}"] = np.frombuffer(f.read(), dtype=np.uint8)
+    out.update(phi3=phi3, vel3=vel3, nodes3=nodes3, phi2=phi2, vel2=vel2, nodes2=nodes2, particles=parts)
+    return out
+
+
 def main(only=None):
     assert R.available(), "build oracle/_ref first: make -C oracle ref REF=<reference tree>"
     if only == "mac":
         np.savez_compressed(os.path.join(OUT, "mac.npz"), **run_mac())
         print("mac.npz written to", OUT)
         return
+    if only == "writer":
+        np.savez_compressed(os.path.join(OUT, "writer.npz"), **run_writer())
+        print("writer.npz written to", OUT)
+        return
+    np.savez_compressed(os.path.join(OUT, "writer.npz"), **run_writer())
     np.savez_compressed(os.path.join(OUT, "mac.npz"), **run_mac())
     # fast-marching reinitialisation: a sphere and a circle as the reference's
     # own initialisers build them (off-grid centres, no symmetric ties)

@@ -52,18 +52,29 @@ def test_tc_bricks_equal_gather_path(wl32, cuda):
 @pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
 def test_linear_fp32_march_equals_gather_and_fp64(wl32, cuda, backtrace):
     """FP32 trilinear step at 256^3: the TMA z-march equals the global-gather
-    form (a band of every point) bit for bit, and the FP64 reference-order
-    step within FP32 rounding."""
+    form bit for bit, and the FP64 reference-order step within FP32
+    rounding."""
     phi, vel = wl32
     dense = L.sl_step(phi, vel, DT, H, interp="linear", backtrace=backtrace)
-    band = fields.band_of(torch.zeros_like(phi), 1.0, margin=0).to(cuda)
-    banded = L.sl_step(phi, vel, DT, H, band=band, interp="linear", backtrace=backtrace,
-                       out=torch.full_like(phi, float("nan")))
+    gathered = L.sl_step(phi, vel, DT, H, interp="linear_gather", backtrace=backtrace,
+                         out=torch.full_like(phi, float("nan")))
     torch.cuda.synchronize()
-    assert torch.equal(dense, banded)
-    del banded, band
+    assert torch.equal(dense, gathered)
+    del gathered
     ref = L.sl_step(phi.double(), vel.double(), DT, H, interp="linear", backtrace=backtrace)
     assert float((dense.double() - ref).abs().max()) <= 4e-7 * float(ref.abs().max())
+
+
+@pytest.mark.parametrize("interp", ["cubic_plain", "cubic_separable"])
+def test_cubic_fp32_bricks_equal_gather(wl32, cuda, interp):
+    """FP32 tricubic step at 256^3 (midpoint): the brick-staged CUDA-core
+    form equals the global-gather form bit for bit."""
+    phi, vel = wl32
+    staged = L.sl_step(phi, vel, DT, H, interp=interp, backtrace="midpoint")
+    gathered = L.sl_step(phi, vel, DT, H, interp=interp + "_gather", backtrace="midpoint",
+                         out=torch.full_like(phi, float("nan")))
+    torch.cuda.synchronize()
+    assert torch.equal(staged, gathered)
 
 
 def test_tc_error_budget_against_fp64(wl32, cuda):

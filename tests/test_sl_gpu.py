@@ -61,22 +61,30 @@ def _random_case(shape, cfl, dev, seed=3):
     return phi.float().to(dev).contiguous(), vel.float().to(dev).contiguous()
 
 
+@pytest.mark.parametrize("interp", ["linear", "cubic_plain", "cubic_separable"])
 @pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
-@pytest.mark.parametrize("shape,cfl", [((9, 20, 36), 0.5), ((40, 24, 64), 0.9), ((16, 16, 32), 3.0), ((3, 5, 8), 0.5),
-                                       ((70, 9, 96), 1.7)])
-def test_linear_fp32_march_equals_gather(cuda, backtrace, shape, cfl):
-    """FP32 trilinear step: the TMA z-march of dense grids (partial tiles,
-    short grids, and departures beyond the staged box at CFL 1.7 and 3, which
-    take the warp's global path) gives the same bits as the global-gather
-    form run on a band that lists every point."""
+@pytest.mark.parametrize("shape,cfl", [((9, 20, 36), 0.5), ((40, 24, 64), 0.9), ((24, 16, 44), 3.0), ((3, 5, 8), 0.5),
+                                       ((70, 9, 96), 1.7), ((12, 8, 40), 0.5)])
+def test_fp32_staged_form_equals_gather_form(cuda, interp, backtrace, shape, cfl):
+    """Dense FP32 steps: the shared-memory-staged forms (TMA z-march for the
+    trilinear step, TMA bricks for the two cubic forms) give the same bits as
+    their global-gather forms -- on partial tiles and bricks, grids smaller
+    than a box, and departures beyond the staged boxes at CFL 1.7 and 3 (the
+    warps' global path).  The linear gather form also equals the band form
+    run on a band that lists every point."""
     phi, vel = _random_case(shape, cfl, cuda)
-    dense = L.sl_step(phi, vel, 1.0, 1.0, interp="linear", backtrace=backtrace)
-    band = fields.band_of(torch.zeros_like(phi), 1.0, margin=0).to(cuda)
-    assert band.shape[0] == phi.numel()
-    banded = L.sl_step(phi, vel, 1.0, 1.0, band=band, interp="linear", backtrace=backtrace,
-                       out=torch.full_like(phi, float("nan")))
+    staged = L.sl_step(phi, vel, 1.0, 1.0, interp=interp, backtrace=backtrace)
+    gathered = L.sl_step(phi, vel, 1.0, 1.0, interp=interp + "_gather", backtrace=backtrace,
+                         out=torch.full_like(phi, float("nan")))
     torch.cuda.synchronize()
-    assert torch.equal(dense, banded)
+    assert torch.equal(staged, gathered)
+    if interp == "linear":
+        band = fields.band_of(torch.zeros_like(phi), 1.0, margin=0).to(cuda)
+        assert band.shape[0] == phi.numel()
+        banded = L.sl_step(phi, vel, 1.0, 1.0, band=band, interp=interp, backtrace=backtrace,
+                           out=torch.full_like(phi, float("nan")))
+        torch.cuda.synchronize()
+        assert torch.equal(staged, banded)
 
 
 @pytest.mark.parametrize("backtrace", ["euler", "midpoint"])

@@ -2,13 +2,17 @@
 23-55), LevelSetWriteIrregularNodeList (LevelSetMethod/IrregularNodes.c:
 145-246), the particle ArrayWrite (Common/Array.c:133-150).
 
-Pinning: the reference's own reader of .Real64 files
+Pinning: tests/golden/writer.npz holds the bytes of every file the
+reference's OWN writers produced (run by tests/golden/make_golden.py through
+oracle/_ref; PETSc's binary viewer, absent here, is its documented format in
+the shim: big-endian values, Vec class id 1211214 and length, `.info` with
+the block size) together with their inputs -- the writer must reproduce each
+file byte for byte from the same inputs, host forms here and device forms on
+the GPU.  The reference's own reader of .Real64 files
 (Visualization/DCellVTK.py: skip two int32 header words, read big-endian
-FP64) reads our grids back exactly; the header is PETSc's binary Vec header
-(class id 1211214, length); node rows follow the reference's row layouts
-field by field; the particle file is the Array's raw records.  The host forms
-run here; the device forms must write the same bytes (GPU tests), including
-when the caller overwrites the device data right after the call."""
+FP64) also reads the grids back exactly.  The device forms must write the
+same bytes even when the caller overwrites the device data right after the
+call."""
 import os
 
 import numpy as np
@@ -36,6 +40,59 @@ def _nodes(n, dim, seed=3):
     a["k"] = rng.uniform(-2, 2, size=n)
     a["d"] = rng.uniform(0, 1, size=n)
     return a
+
+
+def _rows_to_nodes(rows):
+    """18-column node rows (pos, axis, shift, signCenter, signFace, d, X, op,
+    n, k) -> NODE_DTYPE records."""
+    a = np.zeros(len(rows), dtype=_lib.NODE_DTYPE)
+    a["pos"], a["axis"], a["shift"] = rows[:, 0:3], rows[:, 3], rows[:, 4]
+    a["signCenter"], a["signFace"], a["d"] = rows[:, 5], rows[:, 6], rows[:, 7]
+    a["X"], a["op"], a["n"], a["k"] = rows[:, 8:11], rows[:, 11:14], rows[:, 14:17], rows[:, 17]
+    return a
+
+
+def _write_like_reference(w, g, arrays):
+    """The golden sequence of writes (tests/golden/make_golden.py
+    run_writer) through writer `w`; `arrays(x)` makes each input the form to
+    write (numpy here, device tensors on the GPU)."""
+    w.grid("ls3", 0, arrays(g["phi3"]), 0.1, (-3, 2, 1))
+    w.grid("ls3", 1, arrays(g["phi3"] * 0.5), 0.1, (-3, 2, 1))
+    w.irregular_nodes("ls3", 2, *_nodes_arg(arrays, g["nodes3"]), dim=3)
+    w.grid("vel3", 4, arrays(g["vel3"]), 0.1, (-3, 2, 1), dof=3)
+    w.grid("ls2", 7, arrays(g["phi2"]), 0.1, (5, -4))
+    w.irregular_nodes("ls2", 0, *_nodes_arg(arrays, g["nodes2"]), dim=2)
+    w.grid("vel2", 1, arrays(g["vel2"]), 0.1, (5, -4), dof=2)
+    w.particles("particles", 3, arrays(g["particles"]))
+
+
+def _nodes_arg(arrays, rows):
+    nodes = _rows_to_nodes(rows)
+    a = arrays(nodes)
+    if isinstance(a, np.ndarray):
+        return a, len(nodes)
+    import torch
+    return a, torch.tensor([len(nodes)], dtype=torch.int32, device=a.device)
+
+
+def _compare_with_reference_files(g, wd, tmp):
+    files = [k for k in g if k.startswith("file:")]
+    assert len(files) == 23
+    for k in files:
+        sub, name = k[5:].split("/", 1)
+        path = os.path.join(wd if sub == "wd" else tmp, name)
+        assert os.path.exists(path), name
+        assert open(path, "rb").read() == g[k].tobytes(), name
+
+
+def test_files_equal_the_reference_writers_bytes(golden, tmp_path):
+    """Host forms: every file of the reference's own writers, byte for byte."""
+    g = golden("writer")
+    wd, tmp = str(tmp_path / "wd"), str(tmp_path / "tmp")
+    os.makedirs(tmp)
+    with Writer(wd, tmpdir=tmp) as w:
+        _write_like_reference(w, g, lambda x: x)
+    _compare_with_reference_files(g, wd, tmp)
 
 
 def test_grid_files(tmp_path):
@@ -101,6 +158,24 @@ def test_particle_array_and_errors(tmp_path):
 
 # ---------------------------------------------------------------------------
 # GPU: device snapshots write the same bytes
+
+@pytest.mark.gpu
+def test_gpu_device_files_equal_the_reference_writers_bytes(golden, tmp_path, cuda):
+    """Device forms (FP64 device grids, node records and particles on the
+    device): every file of the reference's own writers, byte for byte."""
+    import torch
+    g = golden("writer")
+    wd, tmp = str(tmp_path / "wd"), str(tmp_path / "tmp")
+    os.makedirs(tmp)
+
+    def dev(x):
+        if x.dtype.names:  # node records: raw bytes on the device
+            return torch.from_numpy(np.frombuffer(x.tobytes(), dtype=np.uint8).copy()).to(cuda)
+        return torch.as_tensor(np.ascontiguousarray(x), dtype=torch.float64, device=cuda)
+    with Writer(wd, tmpdir=tmp) as w:
+        _write_like_reference(w, g, dev)
+    _compare_with_reference_files(g, wd, tmp)
+
 
 @pytest.mark.gpu
 def test_gpu_device_writes_equal_host_writes(tmp_path, cuda):
