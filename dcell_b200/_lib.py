@@ -119,6 +119,7 @@ def lib():
     L.dcell_sl_adjoint.argtypes = [G, i, vp, vp, d, i, i, vp, vp, vp, vp]
     L.dcell_split_bf16.argtypes = [G, vp, vp, vp]
     L.dcell_sl_step_tc_split.argtypes = [G, vp, vp, d, vp, i, i, vp, vp, vp, vp]
+    L.dcell_sl_step_tc_split_planes.argtypes = [G, vp, vp, d, i, i, i, vp, vp, vp, vp]
     L.dcell_batch_plan.argtypes = [vp, i, i, i, i, vp, i, vp]
     L.dcell_batch_sl_step.argtypes = [vp, i, vp, i, i, i, i, i, vp, vp, vp, i, i, vp, vp]
     L.dcell_batch_sl_step_tc_split.argtypes = [vp, i, vp, i, vp, vp, i, vp, vp, vp, vp]
@@ -161,7 +162,7 @@ def lib():
                  "dcell_tc_gemm_check", "dcell_wait_timeout_check",
                  "dcell_sl_adjoint", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",
                  "dcell_batch_sl_step_tc_split",
-                 "dcell_sl_step_tc_split", "dcell_pls_advect", "dcell_pls_correct", "dcell_pls_adjust_radii",
+                 "dcell_sl_step_tc_split", "dcell_sl_step_tc_split_planes", "dcell_pls_advect", "dcell_pls_correct", "dcell_pls_adjust_radii",
                  "dcell_pls_seed", "dcell_pls_reseed", "dcell_ls_pls_advect", "dcell_ls_pls_correct",
                  "dcell_ls_pls_adjust_radii", "dcell_ls_pls_seed", "dcell_ls_pls_reseed", "dcell_advect_mac",
                  "dcell_ls_advect_mac"):

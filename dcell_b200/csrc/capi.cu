@@ -109,6 +109,29 @@ DCELL_API int dcell_sl_step_tc_split(const dcell_geom *g, const unsigned int *ph
                             (cudaStream_t)stream);
 }
 
+DCELL_API int dcell_sl_step_tc_split_planes(const dcell_geom *g, const unsigned int *phi0_split, const float *vel,
+                                            double dt, int z_begin, int z_end, int backtrace, float *phi,
+                                            unsigned int *phi_split, int *flags, void *stream) {
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (g->n[2] < 2) FAIL(DCELL_ERR_UNSUPPORTED, "the tensor-core step is 3D only");
+  if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+  if (!phi0_split || !vel || !phi) FAIL(DCELL_ERR_ARG, "phi0_split, vel and phi must be device pointers");
+  if (!(dt == dt)) FAIL(DCELL_ERR_NONFINITE, "dt is NaN");
+  const int nz = g->n[2], bz = tc_slab_planes();
+  if (z_begin < 0 || z_end > nz || z_begin > z_end)
+    FAIL(DCELL_ERR_ARG, "plane range [%d, %d) outside the grid's %d planes", z_begin, z_end, nz);
+  if (z_begin % bz || (z_end % bz && z_end != nz))
+    FAIL(DCELL_ERR_ARG, "plane range [%d, %d) not aligned to %d-plane bricks", z_begin, z_end, bz);
+  const dcell::Geom G = dcell::to_geom(g);
+  if (!tc_brick_applicable(G, phi0_split, vel))
+    FAIL(DCELL_ERR_UNSUPPORTED, "plane ranges need the dense brick path (nx %% 4 == 0, 16-byte aligned arrays, "
+                                "at least one brick box per axis)");
+  if (z_begin == z_end) return DCELL_OK;
+  return launch_sl_tc_split_planes(G, phi0_split, vel, dt, backtrace, phi, phi_split, flags, (cudaStream_t)stream,
+                                   z_begin / bz, (z_end - z_begin + bz - 1) / bz);
+}
+
 DCELL_API int dcell_sl_adjoint(const dcell_geom *g, int dtype, const void *phi0, const void *vel, double dt,
                                int interp, int backtrace, const void *grad_phi, void *grad_phi0, void *grad_vel,
                                void *stream) {

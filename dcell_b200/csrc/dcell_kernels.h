@@ -40,6 +40,11 @@ int tc_slab_planes();
 bool tc_brick_applicable(const dcell::Geom &g, const void *phi0s, const void *vel);
 int launch_sl_tc_slab(const dcell::Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace,
                       float *phi, int *flags, cudaStream_t st, const TcSlab &slab);
+// z bricks [bz0, bz0 + nbz) of the dense split-state step (tc_slab_planes()
+// planes each), no gate
+int launch_sl_tc_split_planes(const dcell::Geom &g, const uint32_t *phi0s, const float *vel, double dt,
+                              int backtrace, float *phi, uint32_t *phis, int *flags, cudaStream_t st, int bz0,
+                              int nbz);
 int launch_sl_tc_split(const dcell::Geom &g, const uint32_t *phi0s, const float *vel, double dt, const int *band,
                        long long npts, int backtrace, float *phi, uint32_t *phis, int *flags, cudaStream_t st);
 int launch_batch_tc(const dcell_cell *cells, const dcell_tile *tiles, int ntiles, int tx, int ty, int ctas_per_sm,

@@ -11,8 +11,15 @@
 //   dL/dU_a = gbar[X] dI/dS_a(S) (-dt/h_a)                (departure point)
 //   dL/du  += dU/du^T dL/dU  through V(X) (Euler) or V(Xm) and, for the
 //            midpoint, through Xm's dependence on V(X).
-// Accumulation uses global atomics (RED): results agree with any ordering to
-// rounding but are not bitwise reproducible in FP32.  Floors of the
+// Accumulation uses global atomics (RED), warp-aggregated: a warp's 32
+// lanes are consecutive arrival points of one grid row, and wherever the
+// departure (or midpoint) cells of its contributing lanes are one row of
+// consecutive cells, the contributions that land on one target -- the
+// stencils of neighbouring lanes overlap in x -- are summed with shuffles
+// first (a sliding window along the row), so each target of a stencil row
+// gets one atomic per warp instead of one per lane: 35 instead of 128 per
+// row of a tricubic stencil.  Other warps add per lane.  Results agree with
+// any ordering to rounding but are not bitwise reproducible.  Floors of the
 // departure cell are treated as constants (the interpolants are continuous,
 // the tricubic one C1).
 #include "dcell_common.cuh"
@@ -45,6 +52,44 @@ __device__ __forceinline__ void weights(T t, T w[4], T dw[4]) {
 
 __device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Warp-aggregated scatter of one stencil row.  Lane L holds v[i] (i < W) for
+// the targets m = L + i of a row whose target m lives at dst + stride *
+// clamp(m0 + m, 0, n - 1), dst and m0 the same in every lane: the sliding
+// sums value(m) = sum_i v[i](lane m - i) for m = 0 .. 31 + W - 1 go out as
+// one atomic each (lane m adds value(m); lanes 0 .. W - 2 add the tail m =
+// 32 + lane), zero sums skipped.  Called by the whole warp.
+template <int W, typename T>
+__device__ __forceinline__ void warp_row_scatter(const T v[W], T *dst, int m0, int n, int stride, int lane) {
+  T s = v[0];
+#pragma unroll
+  for (int i = 1; i < W; ++i) {
+    const T u = __shfl_up_sync(kFull, v[i], i);
+    if (lane >= i) s += u;
+  }
+  if (s != T(0)) atomic_add(dst + (long long)stride * clampi(m0 + lane, 0, n - 1), s);
+  T t = T(0);
+#pragma unroll
+  for (int i = 1; i < W; ++i) {  // value(32 + lane) = sum_{i > lane} v[i](lane 32 + lane - i)
+    const int src = 32 + lane - i;
+    const T u = __shfl_sync(kFull, v[i], src & 31);
+    if (src <= 31) t += u;
+  }
+  if (lane < W - 1 && t != T(0)) atomic_add(dst + (long long)stride * clampi(m0 + 32 + lane, 0, n - 1), t);
+}
+
+// Whether the contributing lanes (active) of the warp share the values a, b
+// and have c - lane equal (their cells are consecutive along the row); the
+// common c - lane goes to c0.
+__device__ __forceinline__ bool warp_row(unsigned active, int a, int b, int c, int lane, int &c0) {
+  const int ref = __ffs(active) - 1;
+  const int ra = __shfl_sync(kFull, a, ref), rb = __shfl_sync(kFull, b, ref);
+  c0 = __shfl_sync(kFull, c - lane, ref);
+  const bool ok = !((active >> lane) & 1u) || (a == ra && b == rb && c - lane == c0);
+  return __all_sync(kFull, ok);
+}
 
 // Trilinear MAC interpolation of component d at node + dl, its weights'
 // gradient wrt position, and the 8 face indices (clamped).
@@ -91,11 +136,18 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
   const long long npts = (long long)g.nx * g.ny * g.nz;
   const T dth[3] = {dt / (T)g.hx, dt / (T)g.hy, dt / (T)g.hz};
   const int sy = g.nx, sz = g.nx * g.ny;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npts;
-       q += (long long)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  // whole warps step together (the scatters are warp-collective); lanes past
+  // the grid's end compute the last point and contribute nothing
+  for (long long wq = blockIdx.x * (long long)blockDim.x + threadIdx.x - lane; wq < npts;
+       wq += (long long)gridDim.x * blockDim.x) {
+    const long long q = wq + lane < npts ? wq + lane : npts - 1;
     const int x = (int)(q % g.nx), y = (int)((q / g.nx) % g.ny), z = (int)(q / sz);
-    const T gb = gphi[q];
-    if (gb == T(0)) continue;
+    const T gb = wq + lane < npts ? gphi[q] : T(0);
+    const unsigned active = __ballot_sync(kFull, gb != T(0));
+    if (!active) continue;
+    const bool on = (active >> lane) & 1u;  // this lane contributes
+    const int ref = __ffs(active) - 1;      // a contributing lane: rows of the warp-wide scatters
     // ---- forward recomputation of the departure point
     T V0[3];
     mac_vel_node<T, 3>(g, vel, x, y, z, V0);
@@ -122,7 +174,6 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
     weights<T, CUBIC>(f[0], wx, dwx);
     weights<T, CUBIC>(f[1], wy, dwy);
     weights<T, CUBIC>(f[2], wz, dwz);
-    // ---- transpose scatter into dL/dphi0 and the interpolant's gradient
     int xi[4], yo[4], zo[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -130,6 +181,7 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
       yo[i] = clampi(c[1] - 1 + i, 0, g.ny - 1) * sy;
       zo[i] = clampi(c[2] - 1 + i, 0, g.nz - 1) * sz;
     }
+    // ---- the interpolant's gradient at S
     T gS[3] = {0, 0, 0};
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -140,14 +192,33 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           if (!CUBIC && (i == 0 || i == 3)) continue;
-          const int p = zo[k] + yo[j] + xi[i];
-          atomic_add(gphi0 + p, gb * wx[i] * wy[j] * wz[k]);
-          const T v = phi0[p];
+          const T v = phi0[zo[k] + yo[j] + xi[i]];
           gS[0] += dwx[i] * wy[j] * wz[k] * v;
           gS[1] += wx[i] * dwy[j] * wz[k] * v;
           gS[2] += wx[i] * wy[j] * dwz[k] * v;
         }
       }
+    }
+    // ---- transpose scatter into dL/dphi0
+    constexpr int I0 = CUBIC ? 0 : 1, W = CUBIC ? 4 : 2;
+    int cx0;
+    if (warp_row(active, c[1], c[2], c[0], lane, cx0)) {
+#pragma unroll
+      for (int k = I0; k < I0 + W; ++k)
+#pragma unroll
+        for (int j = I0; j < I0 + W; ++j) {
+          T v[W];
+#pragma unroll
+          for (int i = 0; i < W; ++i) v[i] = on ? gb * wx[I0 + i] * wy[j] * wz[k] : T(0);
+          warp_row_scatter<W, T>(v, gphi0 + __shfl_sync(kFull, zo[k] + yo[j], ref), cx0 - 1 + I0, g.nx, 1, lane);
+        }
+    } else if (on) {
+#pragma unroll
+      for (int k = I0; k < I0 + W; ++k)
+#pragma unroll
+        for (int j = I0; j < I0 + W; ++j)
+#pragma unroll
+          for (int i = I0; i < I0 + W; ++i) atomic_add(gphi0 + zo[k] + yo[j] + xi[i], gb * wx[i] * wy[j] * wz[k]);
     }
     // ---- velocity sensitivity: dL/dU_a = gb dI/dS_a (-dt/h_a)
     T gU[3];
@@ -155,11 +226,30 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
     for (int a = 0; a < 3; ++a) gU[a] = gb * gS[a] * (-dth[a]);
     T gV0[3] = {gU[0], gU[1], gU[2]};  // Euler: U = V(X)
     if (backtrace == DCELL_MIDPOINT) {
-      // U_a = sum_e w8[a][e] u_a[idx[a][e]]
+      // U_a = sum_e w8[a][e] u_a[idx[a][e]], e = i + 2j + 4k over the 2^3
+      // corners of the midpoint cell b_a (x of corner i of lane L at
+      // idx / 3 % nx = clamp(b_a.x + i))
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
+      for (int a = 0; a < 3; ++a) {
+        const int q0 = idx[a][0] / 3;  // corner (0, 0, 0), clamped
+        const int bx = q0 % g.nx, byz = q0 / g.nx;
+        const int bxu = (idx[a][1] / 3) % g.nx;  // corner (1, 0, 0): bx + 1 clamped
+        int bx0;
+        // one row when the contributing lanes share the corner rows and their
+        // corners are consecutive, unclamped cells
+        const bool interior = bxu == bx + 1;
+        if (__all_sync(kFull, interior || !on) && warp_row(active, byz, 0, bx, lane, bx0)) {
 #pragma unroll
-        for (int e = 0; e < 8; ++e) atomic_add(gvel + idx[a][e], gU[a] * w8[a][e]);
+          for (int jk = 0; jk < 4; ++jk) {
+            const T v[2] = {on ? gU[a] * w8[a][2 * jk] : T(0), on ? gU[a] * w8[a][2 * jk + 1] : T(0)};
+            const int row = idx[a][2 * jk] / 3 - bx;  // corner (0, j, k) row start, this lane
+            warp_row_scatter<2, T>(v, gvel + 3 * (long long)__shfl_sync(kFull, row, ref) + a, bx0, g.nx, 3, lane);
+          }
+        } else if (on) {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) atomic_add(gvel + idx[a][e], gU[a] * w8[a][e]);
+        }
+      }
       // through Xm = X + d(V(X)):  dL/dd_b = sum_a gU_a J[a][b];  d_b = -(dt/2h_b) V0_b
 #pragma unroll
       for (int b = 0; b < 3; ++b) {
@@ -169,12 +259,23 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
         gV0[b] = acc * (T(-0.5) * dth[b]);
       }
     }
-    if (backtrace == DCELL_EULER || backtrace == DCELL_MIDPOINT) {
-      // V0_a = (u_a[node] + u_a[node + e_a]) / 2  (upper face clamped at the edge)
-      const int qn = (z * g.ny + y) * g.nx + x;
-      const int up[3] = {x + 1 < g.nx ? 1 : 0, y + 1 < g.ny ? g.nx : 0, z + 1 < g.nz ? sz : 0};
+    // V0_a = (u_a[node] + u_a[node + e_a]) / 2  (upper face clamped at the edge):
+    // the u faces of a row of nodes overlap between neighbouring lanes
+    const int qn = (z * g.ny + y) * g.nx + x;
+    const int up[3] = {x + 1 < g.nx ? 1 : 0, y + 1 < g.ny ? g.nx : 0, z + 1 < g.nz ? sz : 0};
+    int x0;
+    if (warp_row(active, y, z, x, lane, x0)) {
+      const T hv = on ? T(0.5) * gV0[0] : T(0);
+      const T v[2] = {hv, hv};
+      warp_row_scatter<2, T>(v, gvel + 3 * (long long)__shfl_sync(kFull, (z * g.ny + y) * g.nx, ref), x0, g.nx, 3,
+                             lane);
+    } else if (on) {
+      atomic_add(gvel + 3 * qn, T(0.5) * gV0[0]);
+      atomic_add(gvel + 3 * (qn + up[0]), T(0.5) * gV0[0]);
+    }
+    if (on) {
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
+      for (int a = 1; a < 3; ++a) {
         atomic_add(gvel + 3 * qn + a, T(0.5) * gV0[a]);
         atomic_add(gvel + 3 * (qn + up[a]) + a, T(0.5) * gV0[a]);
       }

@@ -1282,6 +1282,12 @@ int launch_sl_tc_slab(const Geom &g, const uint32_t *phi0s, const float *vel, do
   return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, nullptr, flags, st, &slab);
 }
 
+int launch_sl_tc_split_planes(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace,
+                              float *phi, uint32_t *phis, int *flags, cudaStream_t st, int bz0, int nbz) {
+  const TcSlab slab{bz0, nbz, nullptr, 0.f};
+  return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st, &slab);
+}
+
 int launch_wait_timeout_check(int *result, cudaStream_t st) {
   tc::wait_timeout_check_kernel<<<1, 32, 0, st>>>(result);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;

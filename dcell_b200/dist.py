@@ -21,15 +21,17 @@ Two decompositions of the level-set transport step:
   LevelSetMethod/Advect.c:145-192), and each owner assembles its boxes with
   zeros outside the field.
 
-The per-slab / per-cell step is a callable (default: the CUDA kernels via
-dcell_b200.levelset.sl_step), so the same host logic runs on GPUs with NCCL
+The per-slab / per-cell step is a callable (default: the CUDA kernels --
+the split-state tensor-core brick stepper for slabs, stepping a plane range
+so that the interior overlaps the halo exchange, and the batched brick
+stepper for a rank's cells), so the same host logic runs on GPUs with NCCL
 and in CPU tests with gloo.
 """
 from __future__ import annotations
 
 import math
 from dataclasses import dataclass
-from typing import Callable, List, Sequence
+from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 import torch
@@ -54,6 +56,67 @@ def allreduce_diagnostics(volume: float, maxvel: float, device="cpu"):
     dist.all_reduce(v, op=dist.ReduceOp.SUM)
     dist.all_reduce(m, op=dist.ReduceOp.MAX)
     return float(v.item()), float(m.item())
+
+
+def cells_steps(phis: Sequence[torch.Tensor], vels: Sequence[torch.Tensor], hs, dt: float, nsteps: int,
+                advance: Optional[Callable] = None, diagnose: Optional[Callable] = None, device="cuda",
+                diag_every: int = 1):
+    """The reference's cells-over-ranks loop (DWorld/DCellsArray.c:50-64: each
+    rank advects its own cells, then a barrier) for one process per GPU.
+
+    Cells (the same list on every rank) are assigned largest-first
+    (partition_cells); this rank advances its share `nsteps` times and, every
+    `diag_every` steps, all-reduces the diagnostics of its cells (enclosed
+    volume sum, max |V| / h for the CFL count) -- the only collective.
+
+    advance(phis, vels, hs, dt, k) -> the phis of this rank's cells after k
+    steps; the default packs them into one CellBatch and runs the split-state
+    tensor-core brick stepper over all of them, one launch per step
+    (CellBatch.step_tc_split).  diagnose(phis, vels, hs) -> (volume, vmax)
+    of a list of cells (default: FP64 smoothed-Heaviside volume on the
+    device, eps = 1.5 h_x).  Returns (this rank's cell indices, their final
+    phis, [(step, volume sum, max |V| / h)] identical on every rank)."""
+    rank, world = dist.get_rank(), dist.get_world_size()
+    parts = partition_cells([int(p.numel()) for p in phis], world)
+    mine = parts[rank]
+    hs = np.broadcast_to(np.asarray(hs, dtype=np.float64).reshape(-1, 3) if np.ndim(hs) > 1 else
+                         np.asarray(hs, dtype=np.float64), (len(phis), 3))
+    my_phis, my_vels, my_hs = [phis[i] for i in mine], [vels[i] for i in mine], hs[mine]
+    advance = advance or _batch_advance(device)
+    diagnose = diagnose or _device_diagnostics
+    diags = []
+    done = 0
+    while done < nsteps:
+        k = min(diag_every, nsteps - done)
+        my_phis = advance(my_phis, my_vels, my_hs, dt, k) if my_phis else my_phis
+        done += k
+        vol, vmax = diagnose(my_phis, my_vels, my_hs) if my_phis else (0.0, 0.0)
+        v, m = allreduce_diagnostics(vol, vmax, device=device if dist.get_backend() == "nccl" else "cpu")
+        diags.append((done, v, m))
+    return mine, my_phis, diags
+
+
+def _batch_advance(device):
+    """This rank's cells in one CellBatch, split-state bricks, one launch per step."""
+    def advance(phis, vels, hs, dt, k):
+        from .batch import CellBatch
+        b = CellBatch(phis, vels, hs, dt, device=device)
+        sa, sb = b.split(), torch.empty(b.npoints, dtype=torch.int32, device=b.device)
+        out = torch.empty_like(b.phi)
+        for _ in range(k):
+            b.step_tc_split(sa, out, sb)
+            sa, sb = sb, sa
+        return [b.cell_view(out, i).clone() for i in range(b.ncells)]
+    return advance
+
+
+def _device_diagnostics(phis, vels, hs):
+    from .levelset import volume
+    vol, vmax = 0.0, 0.0
+    for p, v, h in zip(phis, vels, hs):
+        vol += float(volume(p.contiguous(), tuple(h), 1.5 * float(h[0])).item())
+        vmax = max(vmax, max(float(v[..., d].abs().max()) / float(h[d]) for d in range(3)))
+    return vol, vmax
 
 
 def halo_for(max_w: float, dt: float, hz: float, cubic: bool = True) -> int:
@@ -85,10 +148,11 @@ class Slab:
     def interior(self, local):
         return local[self.z0 - self.lo:self.z1 - self.lo]
 
-    def exchange(self, local: torch.Tensor):
-        """Refresh the halo planes of `local` from the z-neighbours."""
-        ops = []
-        bufs = []
+    def exchange_start(self, local: torch.Tensor):
+        """Post the halo exchange of `local` with the z-neighbours (my edge
+        planes out, their edge planes into my halo planes); returns what
+        exchange_finish needs.  The interior planes may be read meanwhile."""
+        ops, bufs = [], []
         lo_in, hi_in = self.z0 - self.lo, self.z1 - self.lo
         if self.rank > 0:  # my first planes -> lower neighbour's upper halo; its last planes -> my lower halo
             send = local[lo_in:lo_in + (self.z0 - self.lo)].contiguous()
@@ -101,15 +165,42 @@ class Slab:
             recv = torch.empty_like(local[hi_in:])
             ops += [dist.P2POp(dist.isend, send, self.rank + 1), dist.P2POp(dist.irecv, recv, self.rank + 1)]
             bufs.append((hi_in, recv))
-        if ops:
-            for req in dist.batch_isend_irecv(ops):
-                req.wait()
+        reqs = dist.batch_isend_irecv(ops) if ops else []
+        return reqs, bufs
+
+    def exchange_finish(self, local: torch.Tensor, pending):
+        reqs, bufs = pending
+        for req in reqs:
+            req.wait()
         for start, recv in bufs:
             local[start:start + recv.shape[0]] = recv
         return local
 
+    def exchange(self, local: torch.Tensor):
+        """Refresh the halo planes of `local` from the z-neighbours."""
+        return self.exchange_finish(local, self.exchange_start(local))
+
+    def step_ranges(self, reach: int, align: int = 1):
+        """Local plane ranges of one overlapped step: (interior, edges).  The
+        interior range reads no halo plane (its departures reach `reach`
+        planes), so it can step while the exchange is in flight; the edge
+        ranges step after it.  Ranges are widened to multiples of `align`
+        (the local grid's last plane ends the last range) and together cover
+        the owned planes [z0 - lo, z1 - lo)."""
+        n = self.hi - self.lo
+        lo_in, hi_in = self.z0 - self.lo, self.z1 - self.lo
+        up = lambda v: min(n, -(-v // align) * align)  # noqa: E731
+        down = lambda v: (v // align) * align  # noqa: E731
+        a, b = up(lo_in + reach), down(hi_in - reach)
+        start, end = down(lo_in), up(hi_in)
+        if a >= b:  # too thin to overlap: everything after the exchange
+            return None, [(start, end)]
+        return (a, b), [r for r in ((start, a), (b, end)) if r[1] > r[0]]
+
 
 def default_stepper(interp="cubic_tc", backtrace="midpoint"):
+    """Whole-array stepper over the CUDA kernels: step(phi0, vel, dt, h,
+    origin) -> phi."""
     from .levelset import sl_step
 
     def step(phi0, vel, dt, h, origin):
@@ -119,12 +210,57 @@ def default_stepper(interp="cubic_tc", backtrace="midpoint"):
 
 def slab_steps(slab: Slab, phi_local: torch.Tensor, vel_local: torch.Tensor, dts: Sequence[float], h,
                stepper: Callable):
-    """Advance this rank's slab by len(dts) steps with a halo exchange before
-    each; returns the local array (interior planes valid)."""
+    """Advance this rank's slab by len(dts) steps with a blocking halo
+    exchange before each (whole-array stepper); returns the local array
+    (interior planes valid)."""
     x = phi_local
     for dt in dts:
         slab.exchange(x)
         x = stepper(x, vel_local, dt, h, (0, 0, slab.lo))
+    return x
+
+
+class SplitStateSlab:
+    """The dense split-state tensor-core stepper on a z-slab (the benchmark's
+    brick kernel): the state carried between steps is the packed BF16 hi/lo
+    words, so only they cross the halo exchange (4 bytes per halo point); the
+    FP32 phi of each step is a side output.  step(x_in, vel, dt, h, origin,
+    z_begin, z_end, x_out) advances local planes [z_begin, z_end) (multiples
+    of the 8-plane brick depth) into x_out and self.phi."""
+
+    align = 8
+
+    def __init__(self, shape, device, backtrace="midpoint"):
+        self.phi = torch.empty(shape, dtype=torch.float32, device=device)
+        self.backtrace = backtrace
+
+    def __call__(self, x_in, vel, dt, h, origin, z_begin, z_end, x_out):
+        from .levelset import sl_step_tc_split_planes
+        sl_step_tc_split_planes(x_in, vel, dt, h, z_begin, z_end, self.phi, x_out, origin=origin,
+                                backtrace=self.backtrace)
+
+
+def slab_steps_overlapped(slab: Slab, state: torch.Tensor, vel_local: torch.Tensor, dts: Sequence[float], h,
+                          stepper: Callable, reach: int, align: int = 1):
+    """Advance this rank's slab by len(dts) steps, each overlapping its halo
+    exchange with the interior planes: post the exchange of the state's edge
+    planes, step the planes that read no halo plane (`reach` = the planes a
+    departure reaches), wait, step the planes next to the halos.  `stepper`
+    advances a plane range: stepper(x_in, vel, dt, h, origin, z_begin, z_end,
+    x_out).  On GPUs the exchange runs on NCCL's stream while the interior
+    kernel runs on the compute stream.  Returns the final state (interior
+    planes valid)."""
+    x, y = state, torch.empty_like(state)
+    inner, edges = slab.step_ranges(reach, align)
+    origin = (0, 0, slab.lo)
+    for dt in dts:
+        pending = slab.exchange_start(x)
+        if inner:
+            stepper(x, vel_local, dt, h, origin, inner[0], inner[1], y)
+        slab.exchange_finish(x, pending)
+        for a, b in edges:
+            stepper(x, vel_local, dt, h, origin, a, b, y)
+        x, y = y, x
     return x
 
 

@@ -111,6 +111,22 @@ def sl_step_tc_split(phi0_split: torch.Tensor, vel: torch.Tensor, dt: float, h, 
     return out, out_split
 
 
+def sl_step_tc_split_planes(phi0_split: torch.Tensor, vel: torch.Tensor, dt: float, h, z_begin: int, z_end: int,
+                            out: torch.Tensor, out_split: Optional[torch.Tensor] = None, origin=(0, 0, 0),
+                            backtrace="midpoint", flags: Optional[torch.Tensor] = None):
+    """The split-state tensor-core step on arrival planes [z_begin, z_end)
+    only (multiples of the 8-plane brick depth, or z_end = nz): writes those
+    planes of out / out_split, reads phi0_split wherever their departures
+    reach (dcell_sl_step_tc_split_planes)."""
+    _require_cuda(phi0_split, vel, out, out_split, flags)
+    g = geom(phi0_split.shape, h, origin)
+    check(lib().dcell_sl_step_tc_split_planes(ctypes.byref(g), _ptr(phi0_split), _ptr(vel), float(dt), int(z_begin),
+                                              int(z_end),
+                                              BACKTRACE[backtrace] if isinstance(backtrace, str) else int(backtrace),
+                                              _ptr(out), _ptr(out_split), _ptr(flags), _stream()))
+    return out, out_split
+
+
 def nodes_to_numpy(raw: torch.Tensor, count: int) -> np.ndarray:
     """Device node buffer (uint8, 120 B/node) -> numpy structured array."""
     n = int(count)

@@ -158,6 +158,18 @@ DCELL_API int dcell_sl_step_tc_split(const dcell_geom *g, const unsigned int *ph
                                      const int *band, int nband, int backtrace, float *phi, unsigned int *phi_split,
                                      int *flags, void *stream);
 
+/* dcell_sl_step_tc_split on the arrival planes [z_begin, z_end) only (dense
+ * grid, no band): the form a z-slab owner uses to step its interior planes
+ * while its halo planes are still in flight, then the planes next to the
+ * halos.  z_begin and z_end are multiples of the brick depth, 8 planes (z_end
+ * may also be nz); the brick path must apply (nx % 4 == 0, 16-byte aligned
+ * arrays, a grid at least one brick box wide per axis), else
+ * DCELL_ERR_UNSUPPORTED.  Planes outside the range are not written.  No
+ * reference counterpart: the reference never splits one level set. */
+DCELL_API int dcell_sl_step_tc_split_planes(const dcell_geom *g, const unsigned int *phi0_split, const float *vel,
+                                            double dt, int z_begin, int z_end, int backtrace, float *phi,
+                                            unsigned int *phi_split, int *flags, void *stream);
+
 /* Adjoint of one dense 3D SL step (dcell_sl_step with band == NULL): given
  * grad_phi = dL/dphi, ACCUMULATES dL/dphi0 into grad_phi0 and dL/dvel into
  * grad_vel (same layouts as phi0 / vel; zero them first for a fresh

@@ -88,6 +88,37 @@ def test_fp32_staged_form_equals_gather_form(cuda, interp, backtrace, shape, cfl
 
 
 @pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
+def test_split_state_plane_ranges_equal_the_full_step(cuda, backtrace):
+    """dcell_sl_step_tc_split_planes over brick-aligned plane ranges (the
+    overlapped z-slab form: interior first, then the planes next to the
+    halos, here on one GPU) gives the full dense step's phi and split words
+    bit for bit, and writes nothing outside its ranges."""
+    from dcell_b200 import dist as D
+    phi, vel = _random_case((43, 24, 64), 0.9, cuda, seed=5)
+    spl = L.split_bf16(phi)
+    full, fspl = L.sl_step_tc_split(spl, vel, 1.0, 1.0, backtrace=backtrace, out_split=torch.empty_like(spl))
+    out = torch.full_like(phi, float("nan"))
+    ospl = torch.full_like(spl, -1)
+    L.sl_step_tc_split_planes(spl, vel, 1.0, 1.0, 8, 24, out, ospl, backtrace=backtrace)
+    torch.cuda.synchronize()
+    assert torch.equal(out[8:24], full[8:24]) and torch.equal(ospl[8:24], fspl[8:24])
+    assert bool(out[:8].isnan().all()) and bool(out[24:].isnan().all()) and bool((ospl[24:] == -1).all())
+    L.sl_step_tc_split_planes(spl, vel, 1.0, 1.0, 0, 8, out, ospl, backtrace=backtrace)
+    L.sl_step_tc_split_planes(spl, vel, 1.0, 1.0, 24, 43, out, ospl, backtrace=backtrace)
+    torch.cuda.synchronize()
+    assert torch.equal(out, full) and torch.equal(ospl, fspl)
+    # the slab stepper over one rank's ranges (no neighbours: no exchange)
+    st = D.SplitStateSlab(phi.shape, cuda, backtrace)
+    slab = D.Slab(phi.shape[0], 1, 0, 3)
+    inner, edges = slab.step_ranges(3, D.SplitStateSlab.align)
+    y = torch.empty_like(spl)
+    for a, b in ([inner] if inner else []) + edges:
+        st(spl, vel, 1.0, 1.0, (0, 0, 0), a, b, y)
+    torch.cuda.synchronize()
+    assert torch.equal(st.phi, full) and torch.equal(y, fspl)
+
+
+@pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
 def test_linear_fp32_dense_vs_fp64(cuda, backtrace):
     """Dense 64^3 sphere in the deformation field (FP32-representable
     inputs): the FP32 step within FP32 rounding of the FP64 reference-order
