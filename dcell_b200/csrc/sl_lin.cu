@@ -78,12 +78,14 @@ struct GlobalAcc {
 
 // The staged ring: box origin (bx, by) = (x0 - 4, y0 - 2) of the tile; plane
 // p of the grid sits in slot (p + kRing) & (kRing - 1) and holds plane
-// clamp(p, 0, nz - 1) (the z clamping is done by the load).  Columns and rows
-// are clamped into the grid and into the box in one step: for an index whose
-// grid-clamped position lies in the box the read equals the global clamped
-// read; any other index still reads inside the ring (a value that the caller
-// discards, since lin_point then reports the point as outside the box).
-template <class S>
+// clamp(p, 0, nz - 1) (the z clamping is done by the load).  CLAMP (tiles
+// whose box crosses the grid's x or y edge): columns and rows are clamped
+// into the grid and into the box in one step, so a read at any index stays
+// in the ring and equals the global clamped read wherever the grid-clamped
+// position lies in the box.  Without CLAMP (the box inside the grid) indices
+// map straight into the box: lin_point reads only indices it has checked to
+// lie in the box.
+template <class S, bool CLAMP>
 struct BoxAcc {
   const float *phis;  // ring of phi planes
   const float *vels;  // ring of velocity planes
@@ -93,8 +95,8 @@ struct BoxAcc {
   __device__ __forceinline__ BoxAcc(const float *p, const float *v, int x0, int y0, int nx, int ny)
       : phis(p), vels(v), bx(x0 - HX), by(y0 - HY), clo(max(HX - x0, 0)), chi(min(nx - 1 - (x0 - HX), PW - 1)),
         rlo(max(HY - y0, 0)), rhi(min(ny - 1 - (y0 - HY), S::PH - 1)) {}
-  __device__ __forceinline__ int col(int i) const { return clampi(i - bx, clo, chi); }
-  __device__ __forceinline__ int row(int j) const { return clampi(j - by, rlo, rhi); }
+  __device__ __forceinline__ int col(int i) const { return CLAMP ? clampi(i - bx, clo, chi) : i - bx; }
+  __device__ __forceinline__ int row(int j) const { return CLAMP ? clampi(j - by, rlo, rhi) : j - by; }
   __device__ __forceinline__ static int slot(int k) { return (k + kRing) & (kRing - 1); }
   __device__ __forceinline__ float phi(int i, int j, int k) const {
     return phis[slot(k) * S::PlanePhi + row(j) * PW + col(i)];
@@ -105,26 +107,31 @@ struct BoxAcc {
 };
 
 // One arrival point (local indices x, y, z): node velocity, optional
-// midpoint velocity, departure, bi/trilinear phi0.  dth = dt / h per axis,
-// hdth = -dt / (2 h).  `in` reports whether every value read lies within
-// the staged box of the point's tile (|midpoint offset| < 1 and departure
-// offset in [-2, 2) per axis); c, f: the departure cell (local) and fraction.
-template <int BT, int DIM, class A>
-__device__ __forceinline__ float lin_point(const A &acc, int x, int y, int z, const float dth[3], const float hdth[3],
-                                           bool &in, int c[3], float f[3]) {
+// midpoint velocity, departure, bi/trilinear phi0, into `out`; c, f: the
+// departure cell (local) and fraction.  dth = dt / h per axis, hdth = -dt /
+// (2 h).  VOTE (staged boxes; called by whole warps): before the midpoint
+// velocity and before phi0 are read, the warp checks that every lane's reads
+// stay in the staged box (|midpoint offset| < 1, departure offset in [-2, 2)
+// per axis) and returns false, with nothing read, where one does not; the
+// node velocity always lies in the box.  The arithmetic is the same either
+// way, so a warp redone through global memory gives the same bits.
+template <int BT, int DIM, bool VOTE, class A>
+__device__ __forceinline__ bool lin_point(const A &acc, int x, int y, int z, const float dth[3], const float hdth[3],
+                                          float &out, int c[3], float f[3]) {
   const int X[3] = {x, y, z};
   float U[3];
   U[0] = face_mean(acc.v(x, y, z, 0), acc.v(x + 1, y, z, 0));
   U[1] = face_mean(acc.v(x, y, z, 1), acc.v(x, y + 1, z, 1));
   U[2] = DIM == 3 ? face_mean(acc.v(x, y, z, 2), acc.v(x, y, z + 1, 2)) : 0.f;
-  in = true;
   if (BT == DCELL_MIDPOINT) {
     float dl[3];
+    bool near = true;
 #pragma unroll
     for (int a = 0; a < DIM; ++a) {
       dl[a] = rmul(U[a], hdth[a]);
-      in = in && fabsf(dl[a]) < 1.f;
+      near = near && fabsf(dl[a]) < 1.f;
     }
+    if (VOTE && !__all_sync(0xffffffffu, near)) return false;
     float V[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
@@ -151,6 +158,7 @@ __device__ __forceinline__ float lin_point(const A &acc, int x, int y, int z, co
   }
   c[2] = z;
   f[2] = 0.f;
+  bool in = true;
 #pragma unroll
   for (int a = 0; a < DIM; ++a) {
     const float t = rmul(-U[a], dth[a]);
@@ -159,12 +167,15 @@ __device__ __forceinline__ float lin_point(const A &acc, int x, int y, int z, co
     c[a] = X[a] + (int)fl;
     f[a] = __fsub_rn(t, fl);
   }
+  if (VOTE && !__all_sync(0xffffffffu, in)) return false;
   if (DIM == 3)
-    return trilerp(acc.phi(c[0], c[1], c[2]), acc.phi(c[0] + 1, c[1], c[2]), acc.phi(c[0], c[1] + 1, c[2]),
-                   acc.phi(c[0] + 1, c[1] + 1, c[2]), acc.phi(c[0], c[1], c[2] + 1), acc.phi(c[0] + 1, c[1], c[2] + 1),
-                   acc.phi(c[0], c[1] + 1, c[2] + 1), acc.phi(c[0] + 1, c[1] + 1, c[2] + 1), f);
-  return bilerp(acc.phi(c[0], c[1], 0), acc.phi(c[0] + 1, c[1], 0), acc.phi(c[0], c[1] + 1, 0),
-                acc.phi(c[0] + 1, c[1] + 1, 0), f[0], f[1]);
+    out = trilerp(acc.phi(c[0], c[1], c[2]), acc.phi(c[0] + 1, c[1], c[2]), acc.phi(c[0], c[1] + 1, c[2]),
+                  acc.phi(c[0] + 1, c[1] + 1, c[2]), acc.phi(c[0], c[1], c[2] + 1), acc.phi(c[0] + 1, c[1], c[2] + 1),
+                  acc.phi(c[0], c[1] + 1, c[2] + 1), acc.phi(c[0] + 1, c[1] + 1, c[2] + 1), f);
+  else
+    out = bilerp(acc.phi(c[0], c[1], 0), acc.phi(c[0] + 1, c[1], 0), acc.phi(c[0], c[1] + 1, 0),
+                 acc.phi(c[0] + 1, c[1] + 1, 0), f[0], f[1]);
+  return true;
 }
 
 // Global-gather form: one thread per arrival point of the band (or of the
@@ -186,10 +197,11 @@ __global__ void __launch_bounds__(256) sl_lin_gather_kernel(Geom g, const float 
       bad = true;
       continue;
     }
-    bool in;
     int c[3];
     float f[3];
-    phi[(z * g.ny + y) * g.nx + x] = lin_point<BT, DIM>(acc, x, y, z, dth, hdth, in, c, f);
+    float v;
+    lin_point<BT, DIM, false>(acc, x, y, z, dth, hdth, v, c, f);
+    phi[(z * g.ny + y) * g.nx + x] = v;
 #pragma unroll
     for (int a = 0; a < DIM; ++a) clamped |= c[a] < 0 || c[a] + (f[a] > 0.f ? 1 : 0) > n[a] - 1;
   }
@@ -198,23 +210,62 @@ __global__ void __launch_bounds__(256) sl_lin_gather_kernel(Geom g, const float 
 }
 
 struct MarchGrid {
-  int ncx;    // tiles per row of tiles (x)
-  int units;  // tiles x planes: unit u = tile * nz + z
+  int ncx;     // tiles per row of tiles (x)
+  int ntiles;  // tiles per plane
+  int seglen;  // planes per z-segment
+  int units;   // segments x tiles: unit u = segment (u / ntiles) of tile (u % ntiles)
 };
 
-// Dense 3-D march (see the head of the file).  CTA b owns units
-// [b U / G, (b+1) U / G) in order: z-runs of one tile, a new run where the
-// range crosses into the next tile.  A producer warp loads every plane a run
-// reads (zs-2 .. ze+1) into the ring, each one once the slot's previous plane
-// is released; the TY consumer warps wait on a slot's `full` mbarrier before
-// a plane's first use, compute their row of the plane, and release plane z-2
-// on its `empty` mbarrier after plane z (the last planes of a run at its
-// end).  No CTA barrier in the loop: warps drift up to a few planes apart.
-// Warps whose points read outside the staged box (per-axis displacement
-// >= 2, or a midpoint offset >= 1) take the global path for that plane.
-// Every wait is bounded; a warp that gives up raises FLAG_WAIT_TIMEOUT and
-// leaves (the others then give up at their next wait), and the producer
-// waits (bounded) for its last load per slot before the CTA ends.
+// One z-run of a tile on the consumer side: planes [zs, ze) of the tile at
+// (x0, y0), the staged ring read through accessor A (clamped at the grid's x
+// / y edges, or not); warps whose reads would leave the box redo the plane
+// through global memory.  Returns false when a wait gave up.
+template <int BT, class S, class A>
+__device__ __forceinline__ bool march_run(const A &bacc, const GlobalAcc<3> &gacc, const Geom &g, int x0, int y0,
+                                          int zs, int ze, int lane, int warp, const float dth[3], const float hdth[3],
+                                          uint64_t *full, uint64_t *empty, uint32_t &fpar, float *__restrict__ phi) {
+  const int x = min(x0 + lane, g.nx - 1), y = min(y0 + warp, g.ny - 1);
+  const bool store = x0 + lane < g.nx && y0 + warp < g.ny;
+  int waited = zs - 2;
+  for (int z = zs; z < ze; ++z) {
+    for (; waited <= z + 2; ++waited) {  // planes up to z + 2 present
+      const int s = BoxAcc<S, false>::slot(waited);
+      const bool ok = mbar_wait_sleep(&full[s], (fpar >> s) & 1u);
+      if (!__all_sync(0xffffffffu, ok)) return false;
+      fpar ^= 1u << s;
+    }
+    int c[3];
+    float f[3];
+    float v;
+    if (!lin_point<BT, 3, true>(bacc, x, y, z, dth, hdth, v, c, f))
+      lin_point<BT, 3, false>(gacc, x, y, z, dth, hdth, v, c, f);
+    if (store) phi[(z * g.ny + y) * g.nx + x] = v;
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[BoxAcc<S, false>::slot(z - 2)]);  // plane z - 2 read for the last time
+  }
+  __syncwarp();
+  if (lane == 0)
+    for (int p = max(ze - 2, zs - 2); p <= ze + 1; ++p) mbar_arrive(&empty[BoxAcc<S, false>::slot(p)]);
+  return true;
+}
+
+// Dense 3-D march (see the head of the file).  Work units are z-segments of
+// `seglen` planes of one tile, numbered segment-major (all tiles of a
+// segment, then the next segment), and CTA b takes units b, b + G, b + 2G,
+// ...: the CTAs in flight work on neighbouring tiles of the same segment at
+// the same time, so the halo rows their boxes share come from L2, and a
+// segment's boundary planes, reloaded by the next segment's unit one round
+// later, too.  Per unit a producer warp loads every plane the unit reads
+// (zs-2 .. ze+1) into the ring, each one once the slot's previous plane is
+// released; the TY consumer warps wait on a slot's `full` mbarrier before a
+// plane's first use, compute their row of the plane, and release plane z-2
+// on its `empty` mbarrier after plane z (the unit's last planes at its end).
+// No CTA barrier in the loop: warps drift up to a few planes apart.  Warps
+// whose points read outside the staged box (per-axis displacement >= 2, or a
+// midpoint offset >= 1) take the global path for that plane.  Every wait is
+// bounded; a warp that gives up raises FLAG_WAIT_TIMEOUT and leaves (the
+// others then give up at their next wait), and the producer waits (bounded)
+// for its last load per slot before the CTA ends.
 template <int BT, int TY>
 __global__ void __launch_bounds__(MarchShape<TY>::Threads, MarchShape<TY>::CtasPerSm)
     sl_lin_march_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel,
@@ -234,19 +285,16 @@ __global__ void __launch_bounds__(MarchShape<TY>::Threads, MarchShape<TY>::CtasP
     }
   __syncthreads();
 
-  const int U = mg.units, G = (int)gridDim.x, b = (int)blockIdx.x;
-  const int ubeg = (int)((long long)U * b / G), uend = (int)((long long)U * (b + 1) / G);
-
   if (warp == TY) {  // ---------------- producer ----------------
     if (lane == 0) {
       uint32_t used = 0, epar = 0, lastpar = 0;  // per slot: loaded once, next empty phase, phase of the last load
       bool err = false;
-      for (int u = ubeg; u < uend && !err;) {
-        const int tile = u / g.nz, zs = u - tile * g.nz, ze = min(g.nz, zs + (uend - u));
-        u += ze - zs;
+      for (int u = blockIdx.x; u < mg.units && !err; u += gridDim.x) {
+        const int seg = u / mg.ntiles, tile = u - seg * mg.ntiles;
+        const int zs = seg * mg.seglen, ze = min(g.nz, zs + mg.seglen);
         const int x0 = (tile % mg.ncx) * TX, y0 = (tile / mg.ncx) * TY;
         for (int p = zs - 2; p <= ze + 1; ++p) {
-          const int s = BoxAcc<S>::slot(p), pz = clampi(p, 0, g.nz - 1);
+          const int s = BoxAcc<S, false>::slot(p), pz = clampi(p, 0, g.nz - 1);
           const uint32_t bit = 1u << s;
           if (used & bit) {
             if (!mbar_wait(&empty[s], (epar & bit) ? 1u : 0u)) {
@@ -276,42 +324,19 @@ __global__ void __launch_bounds__(MarchShape<TY>::Threads, MarchShape<TY>::CtasP
   const float hdth[3] = {-0.5f * dth0, -0.5f * dth1, -0.5f * dth2};
   const GlobalAcc<3> gacc{phi0, vel, g.nx, g.ny, g.nz};
   uint32_t fpar = 0;  // bit s: phase of slot s's next full completion
-  bool err = false;
-  for (int u = ubeg; u < uend && !err;) {
-    const int tile = u / g.nz, zs = u - tile * g.nz, ze = min(g.nz, zs + (uend - u));
-    u += ze - zs;
+  bool ok = true;
+  for (int u = blockIdx.x; u < mg.units && ok; u += gridDim.x) {
+    const int seg = u / mg.ntiles, tile = u - seg * mg.ntiles;
+    const int zs = seg * mg.seglen, ze = min(g.nz, zs + mg.seglen);
     const int x0 = (tile % mg.ncx) * TX, y0 = (tile / mg.ncx) * TY;
-    const BoxAcc<S> bacc(phis, vels, x0, y0, g.nx, g.ny);
-    const int x = min(x0 + lane, g.nx - 1), y = min(y0 + warp, g.ny - 1);
-    const bool store = x0 + lane < g.nx && y0 + warp < g.ny;
-    int waited = zs - 2;
-    for (int z = zs; z < ze; ++z) {
-      for (; waited <= z + 2; ++waited) {  // planes up to z + 2 present
-        const int s = BoxAcc<S>::slot(waited);
-        const bool ok = mbar_wait_sleep(&full[s], (fpar >> s) & 1u);
-        if (!__all_sync(0xffffffffu, ok)) {
-          err = true;
-          break;
-        }
-        fpar ^= 1u << s;
-      }
-      if (err) break;
-      bool in;
-      int c[3];
-      float f[3];
-      float v = lin_point<BT, 3>(bacc, x, y, z, dth, hdth, in, c, f);
-      if (!__all_sync(0xffffffffu, in)) v = lin_point<BT, 3>(gacc, x, y, z, dth, hdth, in, c, f);
-      if (store) phi[(z * g.ny + y) * g.nx + x] = v;
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[BoxAcc<S>::slot(z - 2)]);  // plane z - 2 read for the last time
-    }
-    if (!err) {
-      __syncwarp();
-      if (lane == 0)
-        for (int p = max(ze - 2, zs - 2); p <= ze + 1; ++p) mbar_arrive(&empty[BoxAcc<S>::slot(p)]);
-    }
+    if (x0 >= HX && x0 - HX + PW <= g.nx && y0 >= HY && y0 - HY + S::PH <= g.ny)
+      ok = march_run<BT, S>(BoxAcc<S, false>(phis, vels, x0, y0, g.nx, g.ny), gacc, g, x0, y0, zs, ze, lane, warp, dth,
+                            hdth, full, empty, fpar, phi);
+    else
+      ok = march_run<BT, S>(BoxAcc<S, true>(phis, vels, x0, y0, g.nx, g.ny), gacc, g, x0, y0, zs, ze, lane, warp, dth,
+                            hdth, full, empty, fpar, phi);
   }
-  if (err && lane == 0) raise_flag(flags, FLAG_WAIT_TIMEOUT);
+  if (!ok && lane == 0) raise_flag(flags, FLAG_WAIT_TIMEOUT);
 }
 
 }  // namespace lin
@@ -337,6 +362,17 @@ static int lin_tile_rows() {
   return rows;
 }
 
+// Planes per z-segment (work unit) of the march: 16; DCELL_LIN_SEGMENT
+// overrides it (4 .. 256).
+static int lin_segment_planes() {
+  static int planes = 0;
+  if (!planes) {
+    planes = 16;
+    if (const char *e = getenv("DCELL_LIN_SEGMENT")) planes = std::max(4, std::min(256, atoi(e)));
+  }
+  return planes;
+}
+
 // Launches the march; false when no tensor maps could be made.
 template <int TY>
 static bool launch_march(const Geom &g, const float *phi0, const float *vel, float dth0, float dth1, float dth2,
@@ -359,12 +395,15 @@ static bool launch_march(const Geom &g, const float *phi0, const float *vel, flo
     return false;
   lin::MarchGrid mg;
   mg.ncx = (g.nx + lin::TX - 1) / lin::TX;
-  const int ncy = (g.ny + TY - 1) / TY;
-  mg.units = mg.ncx * ncy * g.nz;
+  mg.ntiles = mg.ncx * ((g.ny + TY - 1) / TY);
+  mg.seglen = std::min(lin_segment_planes(), g.nz);
+  mg.units = mg.ntiles * ((g.nz + mg.seglen - 1) / mg.seglen);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = std::min(S::CtasPerSm * sms, mg.units);
+  // rounds of at most one resident wave; the grid evens the units over them
+  const int slots = S::CtasPerSm * sms, rounds = (mg.units + slots - 1) / slots;
+  const int grid = (mg.units + rounds - 1) / rounds;
   auto kern = mid ? lin::sl_lin_march_kernel<DCELL_MIDPOINT, TY> : lin::sl_lin_march_kernel<DCELL_EULER, TY>;
   kern<<<grid, S::Threads, S::Smem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0, dth1, dth2, phi, flags);
   return true;
