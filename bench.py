@@ -392,6 +392,41 @@ def e2e_rate(phi, vel, h, dt, K, torch):
                                              "pinned, no compute"}}
 
 
+def e2e_resident_rate(phi, vel, h, dt, K, torch):
+    """The reference's LevelSetAdvectAndReinit loop (Advect.c:33-50) through
+    the C ABI with the level set resident on the device
+    (dcell_ls_resident_*): phi (cell units, as after the reference's fast
+    marching) and its band go up once before the timed region; every step
+    uploads its velocity from pinned FP32 host memory (12 B per point) and
+    reads back the step's diagnostics (max |V| and the CFL counters), and
+    runs the split-BF16 tensor-core step, the CFL increment, the
+    irregular-node list and, when the CFL count passes 3 (the reference's
+    default), the device reinitialisation; phi comes down once at the end,
+    inside the timed region.  Host clock around the synchronous calls."""
+    from dcell_b200 import fields
+    from dcell_b200 import levelset as L
+    N = phi.shape[0]
+    n = N ** 3
+    cells = (phi.double() * N).contiguous()
+    band = fields.band_of(cells, 6.0, margin=3)
+    vhost = vel.float().cpu().pin_memory()
+    r = L.ResidentLevelSet(cells.cpu().numpy(), h, band=band.cpu().numpy(), precision="f32", CFLthres=3.0)
+    r.advect_and_reinit(vhost, dt_at(0, dt), "cubic_tc", "midpoint", dense=True)  # warm-up (buffers)
+    reinits = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in range(K):
+        reinits += r.advect_and_reinit(vhost, dt_at(s + 1, dt), "cubic_tc", "midpoint", dense=True).reinitialized
+    out, _ = r.get()
+    t = time.perf_counter() - t0
+    r.close()
+    return n * K / t, {"h2d_bytes_per_step": n * 12, "d2h_bytes_per_step": 16 + n * 8 / K, "steps": K,
+                       "reinitialisations": reinits,
+                       "how": "dcell_ls_resident_advect_and_reinit per step (FP32 host velocity up, diagnostics "
+                              "down; split-BF16 TC step, CFL increment, irregular nodes, device reinitialisation at "
+                              "CFL count > 3), phi down once at the end; host clock"}
+
+
 def error_check(L, torch, phi, vel, h, dt):
     a = L.sl_step_tc_split(L.split_bf16(phi), vel, dt_at(0, dt), h, backtrace="midpoint")[0].double()
     ref = L.sl_step(phi.double(), vel.double(), dt_at(0, dt), h, interp="cubic_plain", backtrace="midpoint")
@@ -535,16 +570,23 @@ def main():
         # and PCIe); the slowest rank's rate sets the job's
         if dist:
             dist.barrier()
-        e2e, by = e2e_rate(phi, vel, h, dt, min(K, 5), torch)
+        e2e_rt, by = e2e_rate(phi, vel, h, dt, min(K, 5), torch)
+        e2e, by_res = e2e_resident_rate(phi, vel, h, dt, 10, torch)
         if dist:
-            t = torch.tensor([e2e], device=dev)
+            t = torch.tensor([e2e, e2e_rt], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MIN)
-            e2e = float(t.item())
+            e2e, e2e_rt = float(t[0].item()), float(t[1].item())
         if rank == 0:
-            line["e2e"] = {"value": e2e * world, "unit": "updates/s", **by,
-                           "how": "dcell_ls_advect_sl (C ABI) on pinned FP64 host buffers, FP32 TC compute, "
-                                  "host clock around synchronous calls, every rank at once, the slowest rank's "
-                                  "rate times the ranks"}
+            # the headline end-to-end form: the reference's time loop with the
+            # level set resident on the device; beside it the one-call round
+            # trip of phi0 and velocity up, phi down (FP64 host buffers)
+            line["e2e"] = {"value": e2e * world, "unit": "updates/s",
+                           "h2d_bytes_per_step": by_res["h2d_bytes_per_step"],
+                           "d2h_bytes_per_step": by_res["d2h_bytes_per_step"], "resident_loop": by_res,
+                           "round_trip": {"value": e2e_rt * world, "unit": "updates/s", **by,
+                                          "how": "dcell_ls_advect_sl (C ABI) on pinned FP64 host buffers, FP32 TC "
+                                                 "compute, host clock around synchronous calls"},
+                           "ranks": "every rank at once, the slowest rank's rate times the ranks"}
             if world == 1:
                 rate, npts, t = cpu_oracle_rate(phi, vel, h, dt, nplanes=24, threads=1)
                 line["cpu_baseline"] = {"value": rate, "unit": "updates/s", "cores": 1, "kind": "port",

@@ -51,6 +51,13 @@ class PlsParams(ctypes.Structure):
                 ("l_max", ctypes.c_int)]
 
 
+class LsLoop(ctypes.Structure):
+    """struct dcell_ls_loop: the loop counters of struct _LevelSet (LevelSetMethod.h:10-26)."""
+    _fields_ = [("CFLcount", ctypes.c_double), ("CFLthres", ctypes.c_double), ("maxVel", ctypes.c_double),
+                ("bandWidth", ctypes.c_double), ("AdvectCount", ctypes.c_int), ("AdvectThres", ctypes.c_int),
+                ("reinitialized", ctypes.c_int), ("band", ctypes.c_int)]
+
+
 NODE_DTYPE = np.dtype([("pos", "<i4", 3), ("axis", "<i4"), ("shift", "<i4"), ("signCenter", "<i4"),
                        ("signFace", "<i4"), ("pad", "<i4"), ("d", "<f8"), ("X", "<f8", 3), ("op", "<f8", 3),
                        ("n", "<f8", 3), ("k", "<f8")])
@@ -117,6 +124,9 @@ def lib():
     L.dcell_tc_gemm_check.argtypes = [vp, vp, vp, vp]
     L.dcell_wait_timeout_check.argtypes = [vp, vp]
     L.dcell_sl_adjoint.argtypes = [G, i, vp, vp, d, i, i, vp, vp, vp, vp]
+    L.dcell_ls_resident_set.argtypes = [vp, G, vp, vp, i, i]
+    L.dcell_ls_resident_advect_and_reinit.argtypes = [vp, G, vp, i, d, i, i, i, ctypes.POINTER(LsLoop)]
+    L.dcell_ls_resident_get.argtypes = [vp, G, vp, vp, i, vp]
     L.dcell_split_bf16.argtypes = [G, vp, vp, vp]
     L.dcell_sl_step_tc_split.argtypes = [G, vp, vp, d, vp, i, i, vp, vp, vp, vp]
     L.dcell_sl_step_tc_split_planes.argtypes = [G, vp, vp, d, i, i, i, vp, vp, vp, vp]
@@ -160,7 +170,8 @@ def lib():
                  "dcell_ls_update_irregular_nodes", "dcell_ls_max_velocity", "dcell_ls_reinitialize",
                  "dcell_ls_advect_sl_rk2_half", "dcell_ls_advect_sl_rk2_full",
                  "dcell_tc_gemm_check", "dcell_wait_timeout_check",
-                 "dcell_sl_adjoint", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",
+                 "dcell_sl_adjoint", "dcell_ls_resident_set", "dcell_ls_resident_advect_and_reinit",
+                 "dcell_ls_resident_get", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",
                  "dcell_batch_sl_step_tc_split",
                  "dcell_sl_step_tc_split", "dcell_sl_step_tc_split_planes", "dcell_pls_advect", "dcell_pls_correct", "dcell_pls_adjust_radii",
                  "dcell_pls_seed", "dcell_pls_reseed", "dcell_ls_pls_advect", "dcell_ls_pls_correct",

@@ -9,6 +9,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "dcell_common.cuh"
@@ -489,11 +490,42 @@ struct DevBuf {
     cap = bytes;
     return DCELL_OK;
   }
+  // grow to `bytes`, keeping the first `keep` bytes (copied on `st`)
+  int grow_keep(size_t bytes, size_t keep, cudaStream_t st) {
+    if (bytes <= cap) return DCELL_OK;
+    void *q = nullptr;
+    if (cudaMalloc(&q, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      FAIL(DCELL_ERR_NOMEM, "cudaMalloc of %zu bytes failed", bytes);
+    }
+    if (p && keep) DCELL_CUDA_CHECK(cudaMemcpyAsync(q, p, keep < cap ? keep : cap, cudaMemcpyDeviceToDevice, st));
+    if (p) {
+      cudaStreamSynchronize(st);
+      cudaFree(p);
+    }
+    p = q;
+    cap = bytes;
+    return DCELL_OK;
+  }
   void release() {
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
   }
+};
+
+// A level set kept on the device across steps (dcell_ls_resident_*): phi
+// (two buffers, stepped ping-pong) in the set precision, its packed split
+// words for the FP32 tensor-core step, the band, the irregular nodes of the
+// current phi, the velocity of the last step.
+struct Resident {
+  bool on = false;
+  dcell_geom g{};
+  int precision = DCELL_F64;
+  int cur = 0;          // phi[cur] / split[cur] hold the level set
+  bool split_ok = false;  // split[cur] is the split of phi[cur]
+  int nband = 0, ncap = 0;
+  DevBuf phi[2], split[2], vel, vel64, band, nodes, scratch, small;
 };
 
 struct dcell_session {
@@ -504,6 +536,7 @@ struct dcell_session {
   DevBuf gates;
   DevBuf phi0_64, vel_64, phi_64, phi0_32, vel_32, phi_32, stage32, band, vals, nodes, scratch, small, parts, split;
   std::vector<double> host_vals;
+  Resident res;
 };
 
 #define ENSURE(buf, bytes)             \
@@ -572,6 +605,10 @@ DCELL_API int dcell_session_destroy(dcell_session *s) {
   cudaStreamSynchronize(s->stream);
   for (DevBuf *b : {&s->phi0_64, &s->vel_64, &s->phi_64, &s->phi0_32, &s->vel_32, &s->phi_32, &s->stage32, &s->band, &s->vals,
                     &s->nodes, &s->scratch, &s->small, &s->parts, &s->split, &s->gates})
+    b->release();
+  Resident &r = s->res;
+  for (DevBuf *b : {&r.phi[0], &r.phi[1], &r.split[0], &r.split[1], &r.vel, &r.vel64, &r.band, &r.nodes, &r.scratch,
+                    &r.small})
     b->release();
   for (cudaEvent_t e : s->ev_in) cudaEventDestroy(e);
   for (cudaEvent_t e : s->ev_out) cudaEventDestroy(e);
@@ -1212,6 +1249,212 @@ DCELL_API int dcell_ls_pls_reseed(dcell_session *s, const dcell_geom *g, const d
                                   long long n, long long capacity, long long *count) {
   if (n < 0) FAIL(DCELL_ERR_ARG, "n must be >= 0");
   return ls_pls_seed_common(s, g, phi, band, nband, prm, rng, particles, n, capacity, count);
+}
+
+// ---------------------------------------------------------------------------
+// Device-resident level set: LevelSetAdvectAndReinit (Advect.c:33-50) step
+// after step with phi, its band and irregular nodes kept on the device.
+
+static bool same_geom(const dcell_geom *a, const dcell_geom *b) {
+  return a->n[0] == b->n[0] && a->n[1] == b->n[1] && a->n[2] == b->n[2] && a->p[0] == b->p[0] &&
+         a->p[1] == b->p[1] && a->p[2] == b->p[2] && a->h[0] == b->h[0] && a->h[1] == b->h[1] && a->h[2] == b->h[2];
+}
+
+// The irregular nodes of phi[cur] over the band (LevelSetUpdateIrregularNodeList);
+// the count stays on the device (small + 4).
+static int resident_nodes(dcell_session *s) {
+  Resident &r = s->res;
+  cudaStream_t st = s->stream;
+  int *dflags = (int *)r.small.p, *dcount = dflags + 1;
+  const size_t sb = irregular_scratch_bytes(r.nband);
+  ENSURE(r.scratch, sb);
+  return dcell_irregular_nodes(&r.g, r.precision, r.phi[r.cur].p, (const int *)r.band.p, r.nband, 0,
+                               (dcell_irregular_node *)r.nodes.p, r.ncap, dcount, r.scratch.p, sb, dflags, st);
+}
+
+// Node capacity for a band of nband points (sign changes at a band point's
+// faces and its projection node), grown keeping the current nodes (the next
+// step's max |V| reads them); the band buffer holds any band of the grid.
+static int resident_sizes(dcell_session *s, int nband) {
+  Resident &r = s->res;
+  const long long n = grid_points(&r.g);
+  const int want = (int)std::min<long long>(8LL * nband + 1024, 8LL * n + 1024);
+  int rc = r.nodes.grow_keep((size_t)want * sizeof(dcell_irregular_node),
+                             (size_t)r.ncap * sizeof(dcell_irregular_node), s->stream);
+  if (rc) return rc;
+  if (want > r.ncap) r.ncap = want;
+  ENSURE(r.band, (size_t)(n > 0 ? n : 1) * 3 * sizeof(int));
+  ENSURE(r.small, 256);
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_ls_resident_set(dcell_session *s, const dcell_geom *g, const double *phi, const int *band,
+                                    int nband, int precision) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  int rc = check_geom(g);
+  if (rc) return rc;
+  if (!phi || (nband > 0 && !band) || nband < 0) FAIL(DCELL_ERR_ARG, "phi (and band when nband > 0) are required");
+  if (precision != DCELL_F32 && precision != DCELL_F64) FAIL(DCELL_ERR_ARG, "precision must be F32 or F64");
+  if (nband > 0 && (rc = check_band_host(g, band, nband))) return rc;
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  Resident &r = s->res;
+  r.on = false;
+  r.g = *g;
+  r.precision = precision;
+  r.cur = 0;
+  r.nband = nband;
+  r.ncap = 0;
+  const long long n = grid_points(g);
+  cudaStream_t st = s->stream;
+  const size_t es = precision == DCELL_F32 ? sizeof(float) : sizeof(double);
+  ENSURE(r.phi[0], n * es);
+  ENSURE(r.phi[1], n * es);
+  if ((rc = resident_sizes(s, nband))) return rc;
+  if (precision == DCELL_F32) {
+    ENSURE(s->phi_64, n * sizeof(double));
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(s->phi_64.p, phi, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    if ((rc = launch_convert(s->phi_64.p, DCELL_F64, r.phi[0].p, DCELL_F32, n, st))) return rc;
+  } else {
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(r.phi[0].p, phi, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
+  if (nband > 0)
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(r.band.p, band, (size_t)nband * 3 * sizeof(int), cudaMemcpyHostToDevice, st));
+  r.split_ok = false;
+  DCELL_CUDA_CHECK(cudaMemsetAsync(r.small.p, 0, 256, st));
+  if ((rc = resident_nodes(s))) return rc;
+  int hf = 0;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(&hf, r.small.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  r.on = true;
+  return session_flags_status(s, hf);
+}
+
+DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_geom *g, const void *vel,
+                                                  int vel_dtype, double dt, int interp, int backtrace, int dense,
+                                                  dcell_ls_loop *loop) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  Resident &r = s->res;
+  if (!r.on) FAIL(DCELL_ERR_ARG, "no resident level set: call dcell_ls_resident_set first");
+  if (!g || !same_geom(g, &r.g)) FAIL(DCELL_ERR_ARG, "geometry differs from the resident level set's");
+  if (!vel || !loop) FAIL(DCELL_ERR_ARG, "vel and loop are required");
+  if (vel_dtype != DCELL_F32 && vel_dtype != DCELL_F64) FAIL(DCELL_ERR_ARG, "vel_dtype must be F32 or F64");
+  if (interp < DCELL_LINEAR || interp > DCELL_CUBIC_TC) FAIL(DCELL_ERR_ARG, "unknown interpolation %d", interp);
+  if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+  if (!(dt == dt)) FAIL(DCELL_ERR_NONFINITE, "dt is NaN");
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long n = grid_points(g);
+  const int dof = g->n[2] > 1 ? 3 : 2;
+  const dcell::Geom G = dcell::to_geom(g);
+  int rc;
+  int *dflags = (int *)r.small.p, *dcount = dflags + 1;
+  double *dmax = (double *)((char *)r.small.p + 64);
+  DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
+  // the step's velocity (the only per-step upload)
+  const size_t ves = r.precision == DCELL_F32 ? sizeof(float) : sizeof(double);
+  ENSURE(r.vel, n * dof * ves);
+  if (vel_dtype == r.precision) {
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(r.vel.p, vel, n * dof * ves, cudaMemcpyHostToDevice, st));
+  } else {
+    const size_t ies = vel_dtype == DCELL_F32 ? sizeof(float) : sizeof(double);
+    ENSURE(r.vel64, n * dof * ies);
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(r.vel64.p, vel, n * dof * ies, cudaMemcpyHostToDevice, st));
+    if ((rc = launch_convert(r.vel64.p, vel_dtype, r.vel.p, r.precision, n * dof, st))) return rc;
+  }
+  // LevelSetCFLIncrement (Advect.c:54-66) needs max |V| at the current
+  // nodes; the reference takes it after the advection, from the nodes of the
+  // level set before this step -- the same nodes, queued here
+  if ((rc = dcell_max_velocity(g, r.precision, r.vel.p, (const dcell_irregular_node *)r.nodes.p, dcount, r.ncap, dmax,
+                               st)))
+    return rc;
+  // GridCopy (phi0 <- phi) and the SL step: phi[nxt] from phi[cur]
+  const int cur = r.cur, nxt = 1 - cur;
+  const bool use_band = !dense && r.nband > 0;
+  if (r.precision == DCELL_F32 && interp == DCELL_CUBIC_TC && !use_band && G.nz > 1) {
+    ENSURE(r.split[0], n * sizeof(uint32_t));
+    ENSURE(r.split[1], n * sizeof(uint32_t));
+    if (!r.split_ok && (rc = launch_split_bf16((const float *)r.phi[cur].p, (uint32_t *)r.split[cur].p, n, st)))
+      return rc;
+    rc = launch_sl_tc_split(G, (const uint32_t *)r.split[cur].p, (const float *)r.vel.p, dt, nullptr, n, backtrace,
+                            (float *)r.phi[nxt].p, (uint32_t *)r.split[nxt].p, dflags, st);
+    r.split_ok = true;
+  } else {
+    if (use_band)  // band points only: the others keep phi's values
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(r.phi[nxt].p, r.phi[cur].p, n * ves, cudaMemcpyDeviceToDevice, st));
+    rc = dcell_sl_step(g, r.precision, r.phi[cur].p, r.vel.p, dt, use_band ? (const int *)r.band.p : nullptr,
+                       use_band ? r.nband : 0, interp, backtrace, r.phi[nxt].p, dflags, st);
+    r.split_ok = false;
+  }
+  if (rc) return rc;
+  r.cur = nxt;
+  // LevelSetUpdateIrregularNodeList of the new phi
+  if ((rc = resident_nodes(s))) return rc;
+  double maxvel = 0.0;
+  int hf = 0;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(&maxvel, dmax, sizeof(double), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(&hf, dflags, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  if ((rc = session_flags_status(s, hf & ~DCELL_FLAG_DEPARTURE_CLAMPED))) return rc;
+  loop->maxVel = maxvel;
+  loop->CFLcount += dt * maxvel / g->h[0];
+  loop->AdvectCount++;
+  loop->reinitialized = 0;
+  if (loop->AdvectCount > loop->AdvectThres || loop->CFLcount > loop->CFLthres) {
+    // LevelSetReinitialize on the device (the bucketed march), new band
+    loop->CFLcount = 0;
+    loop->AdvectCount = 0;
+    int nn = 0;
+    DCELL_CUDA_CHECK(cudaMemcpy(&nn, dcount, sizeof(int), cudaMemcpyDeviceToHost));
+    if (nn > r.ncap) nn = r.ncap;
+    const size_t sb = dcell_reinit_scratch_bytes(g, r.precision);
+    ENSURE(r.scratch, sb);
+    int *dband_count = dflags + 2;
+    if ((rc = dcell_reinitialize(g, r.precision, r.phi[r.cur].p, (const dcell_irregular_node *)r.nodes.p, nn,
+                                 loop->bandWidth, 0.0, (int *)r.band.p, (int)n, dband_count, r.scratch.p, sb, dflags,
+                                 st)))
+      return rc;
+    int hv[3] = {0, 0, 0};
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(hv, dflags, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+    if ((rc = session_flags_status(s, hv[0] & ~DCELL_FLAG_DEPARTURE_CLAMPED))) return rc;
+    r.nband = hv[2];
+    r.split_ok = false;
+    if ((rc = resident_sizes(s, r.nband))) return rc;
+    loop->reinitialized = 1;
+  }
+  loop->band = r.nband;
+  return (hf & DCELL_FLAG_DEPARTURE_CLAMPED) && use_band
+             ? (dcell_set_error(DCELL_ERR_DEPARTURE, "a departure point left the grid; its sample was clamped"),
+                DCELL_ERR_DEPARTURE)
+             : DCELL_OK;
+}
+
+DCELL_API int dcell_ls_resident_get(dcell_session *s, const dcell_geom *g, double *phi, int *band, int capacity,
+                                    int *nband) {
+  if (!s) FAIL(DCELL_ERR_ARG, "session is NULL");
+  Resident &r = s->res;
+  if (!r.on) FAIL(DCELL_ERR_ARG, "no resident level set: call dcell_ls_resident_set first");
+  if (!g || !same_geom(g, &r.g)) FAIL(DCELL_ERR_ARG, "geometry differs from the resident level set's");
+  if (capacity < 0 || (capacity > 0 && !band)) FAIL(DCELL_ERR_ARG, "invalid band buffer");
+  DCELL_CUDA_CHECK(cudaSetDevice(s->device));
+  cudaStream_t st = s->stream;
+  const long long n = grid_points(g);
+  int rc;
+  if (phi) {
+    if (r.precision == DCELL_F32) {
+      ENSURE(s->phi_64, n * sizeof(double));
+      if ((rc = launch_convert(r.phi[r.cur].p, DCELL_F32, s->phi_64.p, DCELL_F64, n, st))) return rc;
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(phi, s->phi_64.p, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    } else {
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(phi, r.phi[r.cur].p, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+  }
+  const int ncopy = r.nband < capacity ? r.nband : capacity;
+  if (ncopy > 0)
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(band, r.band.p, (size_t)ncopy * 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  if (nband) *nband = r.nband;
+  return DCELL_OK;
 }
 
 }  // extern "C"

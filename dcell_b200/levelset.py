@@ -418,6 +418,70 @@ def LevelSetReinitializeGPU(ls: LevelSet, bucket: float = 1.0 / 64):
     ls.band = reinitialize(ls.phi, raw, count, ls.bandWidth, bucket, ls.origin, flags=ls.flags)
 
 
+class ResidentLevelSet:
+    """A level set kept on the device across LevelSetAdvectAndReinit steps
+    (Advect.c:33-50) through the host-buffer C ABI (dcell_ls_resident_*):
+    phi and its band go up once, each step uploads only its velocity.
+
+        r = ResidentLevelSet(phi_host, h, origin, band_host, precision="f32")
+        for s in range(steps):
+            r.advect_and_reinit(vel_host, dt, interp="cubic_tc", backtrace="midpoint")
+        phi_host, band_host = r.get()
+    """
+
+    def __init__(self, phi: np.ndarray, h, origin=(0, 0, 0), band=None, precision="f64", device: int = 0,
+                 bandWidth: float = 6.0, CFLthres: float = 3.0, AdvectThres: int = 1000):
+        self.shape = tuple(phi.shape)
+        self.g = geom(self.shape, h, origin)
+        self.s = ctypes.c_void_p()
+        check(lib().dcell_session_create(int(device), ctypes.byref(self.s)))
+        self.loop = _lib.LsLoop(CFLcount=0.0, CFLthres=float(CFLthres), maxVel=0.0, bandWidth=float(bandWidth),
+                                AdvectCount=0, AdvectThres=int(AdvectThres), reinitialized=0, band=0)
+        p = np.ascontiguousarray(phi, dtype=np.float64)
+        b = np.ascontiguousarray(band if band is not None else np.zeros((0, 3)), dtype=np.int32).reshape(-1, 3)
+        self.precision = _lib.F32 if precision in ("f32", _lib.F32) else _lib.F64
+        check(lib().dcell_ls_resident_set(self.s, ctypes.byref(self.g), p.ctypes.data_as(ctypes.c_void_p),
+                                          b.ctypes.data_as(ctypes.c_void_p), b.shape[0], self.precision))
+
+    def advect_and_reinit(self, vel, dt: float, interp="linear", backtrace="euler", dense: bool = False):
+        """One step; vel a host array (numpy or CPU tensor, FP32 or FP64,
+        (..., dof) in the reference's layout).  Returns the loop counters."""
+        v = vel.numpy() if isinstance(vel, torch.Tensor) else vel
+        v = np.ascontiguousarray(v)
+        vdt = _lib.F32 if v.dtype == np.float32 else _lib.F64
+        if vdt == _lib.F64:
+            v = np.ascontiguousarray(v, dtype=np.float64)
+        ptr = ctypes.c_void_p(vel.data_ptr()) if isinstance(vel, torch.Tensor) and vel.is_contiguous() and \
+            vel.dtype in (torch.float32, torch.float64) else v.ctypes.data_as(ctypes.c_void_p)
+        check(lib().dcell_ls_resident_advect_and_reinit(
+            self.s, ctypes.byref(self.g), ptr, vdt, float(dt), INTERP[interp] if isinstance(interp, str) else
+            int(interp), BACKTRACE[backtrace] if isinstance(backtrace, str) else int(backtrace), int(dense),
+            ctypes.byref(self.loop)))
+        return self.loop
+
+    def get(self):
+        """(phi (FP64 host array), band (nb, 3) int32)."""
+        phi = np.empty(self.shape, dtype=np.float64)
+        n = ctypes.c_int()
+        check(lib().dcell_ls_resident_get(self.s, ctypes.byref(self.g), phi.ctypes.data_as(ctypes.c_void_p), None, 0,
+                                          ctypes.byref(n)))
+        band = np.empty((max(n.value, 1), 3), dtype=np.int32)
+        check(lib().dcell_ls_resident_get(self.s, ctypes.byref(self.g), None, band.ctypes.data_as(ctypes.c_void_p),
+                                          n.value, ctypes.byref(n)))
+        return phi, band[: n.value]
+
+    def close(self):
+        if self.s:
+            lib().dcell_session_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def status(ls: LevelSet) -> int:
     """Read and clear the device status flags of ``ls`` (DCELL_FLAG_* bits)."""
     v = int(ls.flags.item())

@@ -442,6 +442,39 @@ DCELL_API int dcell_session_destroy(dcell_session *s);
 DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const double *phi0, const double *vel, const int *band,
                        int nband, double dt, int interp, int backtrace, int precision, double *phi);
 
+/* Device-resident level set: the reference's LevelSetAdvectAndReinit loop
+ * (LevelSetMethod/Advect.c:33-50, called once per time step by DCell's
+ * ls->Advect slot) without the round trip of phi through host memory.
+ * dcell_ls_resident_set uploads phi (reference Grid layout, FP64 host) and
+ * its band once and computes its irregular nodes; each
+ * dcell_ls_resident_advect_and_reinit call then uploads only the step's
+ * velocity (host, FP32 or FP64 by vel_dtype: FP32 halves the bytes) and runs
+ * on the device GridCopy (phi0 <- phi), LevelSetAdvectSL (dense when `dense`
+ * or no band, else the band points), LevelSetCFLIncrement (max |V| over the
+ * irregular nodes of the level set before the step, Advect.c:54-111),
+ * LevelSetUpdateIrregularNodeList, and, when loop->AdvectCount >
+ * loop->AdvectThres or loop->CFLcount > loop->CFLthres, the reinitialisation
+ * (dcell_reinitialize's bucketed march, band width loop->bandWidth) that
+ * replaces phi's band; the counters live in `loop` as in struct _LevelSet.
+ * dcell_ls_resident_get downloads phi (FP64) and the band where the host
+ * needs them (output, or a CPU fast marching instead of the device one).
+ * precision: the arithmetic (DCELL_F32 with DCELL_CUBIC_TC on a dense 3D grid
+ * carries the split state between steps, as dcell_sl_step_tc_split).  One
+ * resident level set per session; dcell_ls_resident_set replaces it. */
+typedef struct dcell_ls_loop {
+  double CFLcount, CFLthres, maxVel, bandWidth; /* struct _LevelSet's fields (LevelSetMethod.h:10-26) */
+  int AdvectCount, AdvectThres;
+  int reinitialized; /* out: 1 when this step reinitialised */
+  int band;          /* out: band points after the step */
+} dcell_ls_loop;
+DCELL_API int dcell_ls_resident_set(dcell_session *s, const dcell_geom *g, const double *phi, const int *band,
+                                    int nband, int precision);
+DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_geom *g, const void *vel,
+                                                  int vel_dtype, double dt, int interp, int backtrace, int dense,
+                                                  dcell_ls_loop *loop);
+DCELL_API int dcell_ls_resident_get(dcell_session *s, const dcell_geom *g, double *phi, int *band, int capacity,
+                                    int *nband);
+
 /* LevelSetAdvectSLRK2HalfStep / LevelSetAdvectSLRK2FullStep (AdvectRK2.c:
  * 5-26) on host arrays in one call each: the half step first copies phi into
  * phi0 (GridCopy), then both advect phi from phi0 as dcell_ls_advect_sl does

@@ -1,0 +1,84 @@
+"""The device-resident LevelSetAdvectAndReinit loop (dcell_ls_resident_*,
+LevelSetMethod/Advect.c:33-50): phi, band and irregular nodes stay on the
+device between steps, only the velocity goes up.  Checked against the same
+loop run step by step through the device API (levelset.LevelSetAdvectAndReinit
+with the GPU reinitialisation hook): same phi bits, bands, counters."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from dcell_b200 import _lib, fields
+from dcell_b200 import levelset as L
+
+
+def test_resident_argument_errors():
+    """No resident level set, a different geometry, bad dtypes: status codes,
+    no device work."""
+    lib = _lib.lib()
+    g = _lib.geom((8, 8, 8), 0.1)
+    loop = _lib.LsLoop()
+    dummy = ctypes.c_void_p(64)
+    assert lib.dcell_ls_resident_advect_and_reinit(None, ctypes.byref(g), dummy, 0, 0.1, 0, 0, 0,
+                                                   ctypes.byref(loop)) == _lib.ERR_ARG
+    assert lib.dcell_ls_resident_set(None, ctypes.byref(g), dummy, None, 0, 0) == _lib.ERR_ARG
+    assert lib.dcell_ls_resident_get(None, ctypes.byref(g), None, None, 0, None) == _lib.ERR_ARG
+
+
+def _case(N, dev):
+    h = 1.0 / N
+    phi = (fields.sphere_sdf(N, center=(0.5, 0.45, 0.55), r=0.2, device=dev) * N).contiguous()  # cell units
+    vel = fields.deformation_velocity(N, device=dev).contiguous()
+    band = fields.band_of(phi, 6.0, margin=3)
+    return h, phi, vel, band
+
+
+@pytest.mark.gpu
+def test_resident_loop_equals_the_device_api_loop(cuda):
+    """8 steps, FP64 linear Euler on the band, CFL threshold 1 so that the
+    reinitialisation runs inside the loop: the resident loop gives the device
+    API loop's phi and band bit for bit, and the same counters each step."""
+    N = 48
+    h, phi, vel, band = _case(N, cuda)
+    dt = 0.9 * h
+    ls = L.LevelSetCreate(h, (0, 0, 0), (N, N, N), dtype=torch.float64, device=cuda)
+    ls.phi.copy_(phi)
+    ls.band = band.to(cuda)
+    ls.CFLthres = 1.0
+    ls.Reinitialize = L.LevelSetReinitializeGPU
+    L.LevelSetUpdateIrregularNodeList(ls)
+    r = L.ResidentLevelSet(phi.cpu().numpy(), h, band=band.numpy(), precision="f64", CFLthres=1.0)
+    vhost = vel.cpu().numpy()
+    reinits = 0
+    for s in range(8):
+        L.LevelSetAdvectAndReinit(ls, vel, dt)
+        loop = r.advect_and_reinit(vhost, dt)
+        assert loop.AdvectCount == ls.AdvectCount and loop.CFLcount == ls.CFLcount and loop.maxVel == ls.maxVel
+        reinits += loop.reinitialized
+    assert reinits >= 2
+    got, gband = r.get()
+    r.close()
+    assert np.array_equal(got, ls.phi.cpu().numpy())
+    assert np.array_equal(gband, ls.band.cpu().numpy())
+
+
+@pytest.mark.gpu
+def test_resident_tc_loop_equals_split_state_steps(cuda):
+    """FP32, dense, split-BF16 tensor-core steps with FP32 host velocity: the
+    resident loop's phi after 5 steps equals 5 dcell_sl_step_tc_split steps
+    (the split state carried between them) bit for bit."""
+    N = 64
+    h, phi, vel, band = _case(N, cuda)
+    dt = 0.5 * h
+    r = L.ResidentLevelSet(phi.cpu().numpy(), h, band=band.numpy(), precision="f32", CFLthres=1e9)
+    v32 = vel.float().contiguous()
+    vhost = v32.cpu().numpy()
+    spl = L.split_bf16(phi.float().contiguous())
+    out = None
+    for s in range(5):
+        r.advect_and_reinit(vhost, dt, interp="cubic_tc", backtrace="midpoint", dense=True)
+        out, spl = L.sl_step_tc_split(spl, v32, dt, h, backtrace="midpoint", out_split=torch.empty_like(spl))
+    got, _ = r.get()
+    r.close()
+    assert np.array_equal(got, out.double().cpu().numpy())
