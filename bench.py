@@ -9,9 +9,14 @@ every one of the 16,777,216 grid points is updated.  Inputs are synthetic
 (formulas), resident in HBM, larger than L2 (no flush needed).
 
 Also measured in the same run: the plain FP32 CUDA-core step (1331-nnz
-coefficient form) and the separable FP32 step, the error of the TC step vs
-the FP64 GPU oracle in the |phi| < 3h band, the end-to-end rate through the
-reference-facing C ABI with FP64 host buffers, and the CPU oracle port.
+coefficient form) and the separable FP32 step, each as global gathers and on
+the tensor-core stepper's TMA bricks; the trilinear FP32 step (the
+reference's own mode) against the HBM roofline; the error of the TC step vs
+the FP64 GPU oracle in the |phi| < 3h band, one step and over the field's
+whole period; the end-to-end rate through the reference-facing C ABI (the
+reference's LevelSetAdvectAndReinit loop with the level set resident on the
+device, and the one-call round trip of FP64 host buffers); the CPU oracle
+port.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -537,8 +542,13 @@ def main():
             "gpu_launches": K, "clocks": clk.summary()}
 
     if not args.no_extras:
-        ms_pl = timed_steps(L, torch, phi, vel, h, dt, "cubic_plain", K, W)
-        ms_sep = timed_steps(L, torch, phi, vel, h, dt, "cubic_separable", K, W)
+        # CUDA-core comparators in both data paths: global gathers (one thread
+        # per point) and the tensor-core stepper's TMA bricks (equal data
+        # movement, evaluation on CUDA cores)
+        ms_pl = timed_steps(L, torch, phi, vel, h, dt, "cubic_plain_gather", K, W)
+        ms_sep = timed_steps(L, torch, phi, vel, h, dt, "cubic_separable_gather", K, W)
+        ms_pl_b = timed_steps(L, torch, phi, vel, h, dt, "cubic_plain", K, W)
+        ms_sep_b = timed_steps(L, torch, phi, vel, h, dt, "cubic_separable", K, W)
         ms_tc_unsplit = timed_steps(L, torch, phi, vel, h, dt, "cubic_tc", K, W)
         ms_lin = timed_steps(L, torch, phi, vel, h, dt, "linear", K, W)
         ms_lin_e = timed_steps(L, torch, phi, vel, h, dt, "linear", K, W, backtrace="euler")
@@ -550,10 +560,16 @@ def main():
         line["comparators"] = {
             "plain_fp32_updates_per_s": n * K / (ms_pl / 1e3),
             "separable_fp32_updates_per_s": n * K / (ms_sep / 1e3),
+            "plain_fp32_brick_updates_per_s": n * K / (ms_pl_b / 1e3),
+            "separable_fp32_brick_updates_per_s": n * K / (ms_sep_b / 1e3),
             "linear_fp32_updates_per_s": n * K / (ms_lin / 1e3),
             "tc_unsplit_state_updates_per_s": n * K / (ms_tc_unsplit / 1e3),
             "tc_over_plain_fp32": ms_pl / ms_tc,
             "tc_over_separable_fp32": ms_sep / ms_tc,
+            "tc_over_plain_fp32_brick": ms_pl_b / ms_tc,
+            "tc_over_separable_fp32_brick": ms_sep_b / ms_tc,
+            "forms": "plain/separable: global-gather form (one thread per point, the scope's plain FP32 CUDA SL "
+                     "step); *_brick: the same arithmetic on the tensor-core stepper's TMA-staged bricks",
             # the reference's own mode (trilinear, Euler backtrace) and its
             # midpoint form: TMA z-march, HBM-bound
             "linear_fp32": {"euler": hbm_leg(ms_lin_e), "midpoint": hbm_leg(ms_lin),
