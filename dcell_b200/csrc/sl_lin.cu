@@ -37,24 +37,35 @@ namespace dcell {
 namespace lin {
 
 constexpr int TX = 32;                     // points of a tile row (one warp)
-constexpr int HX = 4, HY = 2;              // box halo (x: 4 keeps TMA x coordinates 16-byte aligned)
+constexpr int HX = 4, HY = 2;              // phi box halo (x: 4 keeps TMA x coordinates 16-byte aligned)
 constexpr int PW = TX + 2 * HX;            // 40 phi values per box row
-constexpr int VW = 3 * PW;                 // 120 velocity values per box row (u, v, w interleaved)
 constexpr int kRing = 8;                   // ring slots: planes z-2 .. z+2 in use, up to three ahead
 
 // A tile of TX x TY points per plane: TY consumer warps (one tile row each)
-// and one producer warp.  The staged planes are (TY + 4) box rows high.
-template <int TY_>
+// and one producer warp.  The phi box is [x0-4, x0+36) x [y0-2, y0+TY+2).
+// The velocity box holds what the backtrace reads: the faces around the
+// nodes for Euler, [x0, x0+36) x [y0, y0+TY+1) (36 points keep the row a
+// multiple of 16 bytes), and the midpoint's trilinear corners within one
+// cell of the nodes as well, [x0-4, x0+36) x [y0-1, y0+TY+2).  Planes start
+// on 128-byte boundaries.
+template <int TY_, int BT>
 struct MarchShape {
   static constexpr int TY = TY_;
   static constexpr int PH = TY + 2 * HY;
-  static constexpr int PlanePhi = PW * PH;  // floats of one staged phi plane
-  static constexpr int PlaneVel = VW * PH;  // floats of one staged velocity plane
-  static constexpr int PlaneBytes = 4 * (PlanePhi + PlaneVel);
+  static constexpr int VX0 = BT == DCELL_MIDPOINT ? -4 : 0;   // velocity box x origin - x0
+  static constexpr int VY0 = BT == DCELL_MIDPOINT ? -1 : 0;   // velocity box y origin - y0
+  static constexpr int VXN = BT == DCELL_MIDPOINT ? 40 : 36;  // velocity box points per row
+  static constexpr int VH = BT == DCELL_MIDPOINT ? TY + 3 : TY + 1;
+  static constexpr int VW = 3 * VXN;                            // velocity floats per box row
+  static constexpr int PlanePhi = PW * PH;                      // floats of one staged phi plane
+  static constexpr int PlaneVel = (VW * VH + 31) / 32 * 32;     // floats of one staged velocity plane (padded)
+  static constexpr int VelBoxBytes = 4 * VW * VH;               // bytes a velocity load writes
+  static constexpr int PlaneBytes = 4 * PlanePhi + VelBoxBytes;  // transaction bytes per plane
   static constexpr int Threads = 32 * (TY + 1);
-  static constexpr int Smem = kRing * PlaneBytes + 2 * kRing * 8;  // + full / empty mbarrier per slot
+  static constexpr int Smem = kRing * 4 * (PlanePhi + PlaneVel) + 2 * kRing * 8;  // + full / empty mbarriers
   static constexpr int CtasPerSm = (228 * 1024) / (Smem + 1024) < 4 ? (228 * 1024) / (Smem + 1024) : 4;
   static_assert((4 * PlanePhi) % 128 == 0 && (4 * PlaneVel) % 128 == 0, "staged planes stay 128-byte aligned");
+  static_assert((4 * VW) % 16 == 0 && (4 * PW) % 16 == 0, "box rows are multiples of 16 bytes");
   static_assert(CtasPerSm >= 1, "ring too large for one CTA");
 };
 static_assert((kRing & (kRing - 1)) == 0 && kRing >= 8, "ring slot of plane p is (p + kRing) & (kRing - 1)");
@@ -89,20 +100,27 @@ template <class S, bool CLAMP>
 struct BoxAcc {
   const float *phis;  // ring of phi planes
   const float *vels;  // ring of velocity planes
-  int bx, by;         // box origin (grid coordinates)
-  int clo, chi;       // box columns that hold grid columns: [max(-bx, 0), min(nx - 1 - bx, PW - 1)]
-  int rlo, rhi;       // box rows that hold grid rows
+  int bx, by;         // phi box origin (grid coordinates)
+  int vbx, vby;       // velocity box origin
+  int clo, chi;       // phi box columns that hold grid columns: [max(-bx, 0), min(nx - 1 - bx, PW - 1)]
+  int rlo, rhi;       // phi box rows that hold grid rows
+  int vclo, vchi, vrlo, vrhi;  // the same for the velocity box
   __device__ __forceinline__ BoxAcc(const float *p, const float *v, int x0, int y0, int nx, int ny)
-      : phis(p), vels(v), bx(x0 - HX), by(y0 - HY), clo(max(HX - x0, 0)), chi(min(nx - 1 - (x0 - HX), PW - 1)),
-        rlo(max(HY - y0, 0)), rhi(min(ny - 1 - (y0 - HY), S::PH - 1)) {}
+      : phis(p), vels(v), bx(x0 - HX), by(y0 - HY), vbx(x0 + S::VX0), vby(y0 + S::VY0),
+        clo(max(HX - x0, 0)), chi(min(nx - 1 - (x0 - HX), PW - 1)), rlo(max(HY - y0, 0)),
+        rhi(min(ny - 1 - (y0 - HY), S::PH - 1)), vclo(max(-(x0 + S::VX0), 0)),
+        vchi(min(nx - 1 - (x0 + S::VX0), S::VXN - 1)), vrlo(max(-(y0 + S::VY0), 0)),
+        vrhi(min(ny - 1 - (y0 + S::VY0), S::VH - 1)) {}
   __device__ __forceinline__ int col(int i) const { return CLAMP ? clampi(i - bx, clo, chi) : i - bx; }
   __device__ __forceinline__ int row(int j) const { return CLAMP ? clampi(j - by, rlo, rhi) : j - by; }
+  __device__ __forceinline__ int vcol(int i) const { return CLAMP ? clampi(i - vbx, vclo, vchi) : i - vbx; }
+  __device__ __forceinline__ int vrow(int j) const { return CLAMP ? clampi(j - vby, vrlo, vrhi) : j - vby; }
   __device__ __forceinline__ static int slot(int k) { return (k + kRing) & (kRing - 1); }
   __device__ __forceinline__ float phi(int i, int j, int k) const {
     return phis[slot(k) * S::PlanePhi + row(j) * PW + col(i)];
   }
   __device__ __forceinline__ float v(int i, int j, int k, int d) const {
-    return vels[slot(k) * S::PlaneVel + row(j) * VW + 3 * col(i) + d];
+    return vels[slot(k) * S::PlaneVel + vrow(j) * S::VW + 3 * vcol(i) + d];
   }
 };
 
@@ -267,15 +285,15 @@ __device__ __forceinline__ bool march_run(const A &bacc, const GlobalAcc<3> &gac
 // others then give up at their next wait), and the producer waits (bounded)
 // for its last load per slot before the CTA ends.
 template <int BT, int TY>
-__global__ void __launch_bounds__(MarchShape<TY>::Threads, MarchShape<TY>::CtasPerSm)
+__global__ void __launch_bounds__(MarchShape<TY, BT>::Threads, MarchShape<TY, BT>::CtasPerSm)
     sl_lin_march_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel,
                         Geom g, MarchGrid mg, const float *__restrict__ phi0, const float *__restrict__ vel, float dth0,
                         float dth1, float dth2, float *__restrict__ phi, int *flags) {
-  using S = MarchShape<TY>;
+  using S = MarchShape<TY, BT>;
   extern __shared__ __align__(1024) uint8_t smem[];
   float *const phis = reinterpret_cast<float *>(smem);
   float *const vels = phis + kRing * S::PlanePhi;
-  uint64_t *const full = reinterpret_cast<uint64_t *>(smem + kRing * S::PlaneBytes);
+  uint64_t *const full = reinterpret_cast<uint64_t *>(smem + kRing * 4 * (S::PlanePhi + S::PlaneVel));
   uint64_t *const empty = full + kRing;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0)
@@ -308,7 +326,7 @@ __global__ void __launch_bounds__(MarchShape<TY>::Threads, MarchShape<TY>::CtasP
           fence_proxy_async();  // the consumers' reads of the slot before these writes
           mbar_expect_tx(&full[s], (uint32_t)S::PlaneBytes);
           tma_load_3d(phis + s * S::PlanePhi, &tm_phi, x0 - HX, y0 - HY, pz, &full[s]);
-          tma_load_3d(vels + s * S::PlaneVel, &tm_vel, 3 * (x0 - HX), y0 - HY, pz, &full[s]);
+          tma_load_3d(vels + s * S::PlaneVel, &tm_vel, 3 * (x0 + S::VX0), y0 + S::VY0, pz, &full[s]);
         }
       }
       // nothing may still be in flight when the CTA's shared memory goes away
@@ -329,7 +347,8 @@ __global__ void __launch_bounds__(MarchShape<TY>::Threads, MarchShape<TY>::CtasP
     const int seg = u / mg.ntiles, tile = u - seg * mg.ntiles;
     const int zs = seg * mg.seglen, ze = min(g.nz, zs + mg.seglen);
     const int x0 = (tile % mg.ncx) * TX, y0 = (tile / mg.ncx) * TY;
-    if (x0 >= HX && x0 - HX + PW <= g.nx && y0 >= HY && y0 - HY + S::PH <= g.ny)
+    if (x0 >= HX && x0 - HX + PW <= g.nx && y0 >= HY && y0 - HY + S::PH <= g.ny && x0 + S::VX0 >= 0 &&
+        x0 + S::VX0 + S::VXN <= g.nx && y0 + S::VY0 >= 0 && y0 + S::VY0 + S::VH <= g.ny)
       ok = march_run<BT, S>(BoxAcc<S, false>(phis, vels, x0, y0, g.nx, g.ny), gacc, g, x0, y0, zs, ze, lane, warp, dth,
                             hdth, full, empty, fpar, phi);
     else
@@ -373,17 +392,15 @@ static int lin_segment_planes() {
   return planes;
 }
 
-// Launches the march; false when no tensor maps could be made.
-template <int TY>
-static bool launch_march(const Geom &g, const float *phi0, const float *vel, float dth0, float dth1, float dth2,
-                         bool mid, float *phi, int *flags, cudaStream_t st) {
-  using S = lin::MarchShape<TY>;
+// The march with backtrace BT; false when no tensor maps could be made.
+template <int TY, int BT>
+static bool launch_march_bt(const Geom &g, const float *phi0, const float *vel, float dth0, float dth1, float dth2,
+                            float *phi, int *flags, cudaStream_t st) {
+  using S = lin::MarchShape<TY, BT>;
   static bool configured = false;
   if (!configured) {
-    if (cudaFuncSetAttribute(lin::sl_lin_march_kernel<DCELL_EULER, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             S::Smem) != cudaSuccess ||
-        cudaFuncSetAttribute(lin::sl_lin_march_kernel<DCELL_MIDPOINT, TY>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, S::Smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(lin::sl_lin_march_kernel<BT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::Smem) !=
+        cudaSuccess)
       return false;
     configured = true;
   }
@@ -391,7 +408,7 @@ static bool launch_march(const Geom &g, const float *phi0, const float *vel, flo
   if (!make_tensor_map_3d(&tm_phi, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, phi0, (uint64_t)g.nx, (uint64_t)g.ny,
                           (uint64_t)g.nz, lin::PW, S::PH, 1, 4) ||
       !make_tensor_map_3d(&tm_vel, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel, 3ull * g.nx, (uint64_t)g.ny, (uint64_t)g.nz,
-                          lin::VW, S::PH, 1, 4))
+                          S::VW, S::VH, 1, 4))
     return false;
   lin::MarchGrid mg;
   mg.ncx = (g.nx + lin::TX - 1) / lin::TX;
@@ -404,9 +421,17 @@ static bool launch_march(const Geom &g, const float *phi0, const float *vel, flo
   // rounds of at most one resident wave; the grid evens the units over them
   const int slots = S::CtasPerSm * sms, rounds = (mg.units + slots - 1) / slots;
   const int grid = (mg.units + rounds - 1) / rounds;
-  auto kern = mid ? lin::sl_lin_march_kernel<DCELL_MIDPOINT, TY> : lin::sl_lin_march_kernel<DCELL_EULER, TY>;
-  kern<<<grid, S::Threads, S::Smem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0, dth1, dth2, phi, flags);
+  lin::sl_lin_march_kernel<BT, TY><<<grid, S::Threads, S::Smem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0, dth1,
+                                                                       dth2, phi, flags);
   return true;
+}
+
+// Launches the march; false when no tensor maps could be made.
+template <int TY>
+static bool launch_march(const Geom &g, const float *phi0, const float *vel, float dth0, float dth1, float dth2,
+                         bool mid, float *phi, int *flags, cudaStream_t st) {
+  return mid ? launch_march_bt<TY, DCELL_MIDPOINT>(g, phi0, vel, dth0, dth1, dth2, phi, flags, st)
+             : launch_march_bt<TY, DCELL_EULER>(g, phi0, vel, dth0, dth1, dth2, phi, flags, st);
 }
 
 int launch_sl_lin_f32(const Geom &g, const float *phi0, const float *vel, double dt, const int *band, long long npts,
