@@ -133,6 +133,10 @@ def lib():
     L.dcell_batch_plan.argtypes = [vp, i, i, i, i, vp, i, vp]
     L.dcell_batch_sl_step.argtypes = [vp, i, vp, i, i, i, i, i, vp, vp, vp, i, i, vp, vp]
     L.dcell_batch_sl_step_tc_split.argtypes = [vp, i, vp, i, vp, vp, i, vp, vp, vp, vp]
+    L.dcell_batch_tma_maps_bytes.argtypes = [i]
+    L.dcell_batch_tma_maps_bytes.restype = sz
+    L.dcell_batch_tma_maps.argtypes = [vp, i, vp, vp, vp, vp]
+    L.dcell_batch_sl_step_tc_split_tma.argtypes = [vp, i, vp, i, vp, vp, vp, i, vp, vp, vp, vp]
     ll, P = ctypes.c_longlong, ctypes.POINTER(PlsParams)
     L.dcell_pls_default_params.argtypes = [i, P]
     L.dcell_pls_default_params.restype = None
@@ -172,7 +176,7 @@ def lib():
                  "dcell_tc_gemm_check", "dcell_wait_timeout_check",
                  "dcell_sl_adjoint", "dcell_ls_resident_set", "dcell_ls_resident_advect_and_reinit",
                  "dcell_ls_resident_get", "dcell_batch_plan", "dcell_batch_sl_step", "dcell_split_bf16",
-                 "dcell_batch_sl_step_tc_split",
+                 "dcell_batch_sl_step_tc_split", "dcell_batch_tma_maps", "dcell_batch_sl_step_tc_split_tma",
                  "dcell_sl_step_tc_split", "dcell_sl_step_tc_split_planes", "dcell_pls_advect", "dcell_pls_correct", "dcell_pls_adjust_radii",
                  "dcell_pls_seed", "dcell_pls_reseed", "dcell_ls_pls_advect", "dcell_ls_pls_correct",
                  "dcell_ls_pls_adjust_radii", "dcell_ls_pls_seed", "dcell_ls_pls_reseed", "dcell_advect_mac",

@@ -43,13 +43,21 @@ def _stream():
 class CellBatch:
     """A packed batch of 3D cell grids (FP32) on one device."""
 
-    def __init__(self, phis: Sequence[torch.Tensor], vels: Sequence[torch.Tensor], hs, dts, device="cuda"):
+    def __init__(self, phis: Sequence[torch.Tensor], vels: Sequence[torch.Tensor], hs, dts, device="cuda",
+                 padded: bool = False):
+        """padded: rows padded to multiples of 4 points (the extra columns
+        hold copies of each cell's last column) for the TMA-staged batched
+        split-state step (step_tc_split_tma); the other steps need the
+        unpadded packing."""
         if len(phis) != len(vels):
             raise DcellError(_lib.ERR_ARG, "one velocity per cell")
         self.device = torch.device(device)
         self.ncells = len(phis)
+        self.padded = bool(padded)
         self.shapes = [tuple(int(v) for v in p.shape) for p in phis]
-        sizes = [int(np.prod(s)) for s in self.shapes]
+        # stored shapes: the padded row length in x
+        self.stored = [(s[0], s[1], (s[2] + 3) // 4 * 4 if padded else s[2]) for s in self.shapes]
+        sizes = [int(np.prod(s)) for s in self.stored]
         self.offsets = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
         self.npoints = int(sum(sizes))
         if 3 * self.npoints >= 2 ** 31:
@@ -60,11 +68,19 @@ class CellBatch:
             o, n = int(self.offsets[i]), sizes[i]
             if tuple(v.shape) != self.shapes[i] + (3,):
                 raise DcellError(_lib.ERR_ARG, f"cell {i}: velocity shape {tuple(v.shape)}")
-            self.phi[o:o + n] = p.reshape(-1).to(self.device, torch.float32)
-            self.vel[3 * o:3 * (o + n)] = v.reshape(-1).to(self.device, torch.float32)
+            nx, sx = self.shapes[i][2], self.stored[i][2]
+            pp = p.to(self.device, torch.float32)
+            vv = v.to(self.device, torch.float32)
+            if sx > nx:  # pad columns: copies of the last column
+                pp = torch.cat([pp, pp[..., -1:].expand(*pp.shape[:2], sx - nx)], dim=2)
+                vv = torch.cat([vv, vv[..., -1:, :].expand(*vv.shape[:2], sx - nx, 3)], dim=2)
+            self.phi[o:o + n] = pp.reshape(-1)
+            self.vel[3 * o:3 * (o + n)] = vv.reshape(-1)
         cells = np.zeros(self.ncells, dtype=CELL_DTYPE)
         cells["offset"] = self.offsets
         cells["n"] = [(s[2], s[1], s[0]) for s in self.shapes]
+        if padded:
+            cells["pad"] = [s[2] for s in self.stored]
         hs = np.broadcast_to(np.asarray(hs, dtype=np.float64).reshape(-1, 3) if np.ndim(hs) > 1 else
                              np.asarray(hs, dtype=np.float64), (self.ncells, 3))
         cells["h"] = hs
@@ -73,6 +89,11 @@ class CellBatch:
         self.cells = torch.as_tensor(cells.view(np.uint8), device=self.device)
         self._plans = {}
         self.tuned = {}
+
+    def _unpadded(self):
+        if self.padded:
+            raise DcellError(_lib.ERR_ARG, "this step reads the unpadded packing: use step_tc_split_tma on a "
+                                           "padded batch")
 
     # ------------------------------------------------------------------
     def plan(self, tile):
@@ -93,6 +114,7 @@ class CellBatch:
 
     def step(self, phi0, phi, interp="cubic_tc", backtrace="midpoint", tile=None, ctas_per_sm=None, flags=None):
         """One SL step of every cell: phi <- SL(phi0) in one persistent launch."""
+        self._unpadded()
         mode = INTERP[interp] if isinstance(interp, str) else int(interp)
         if tile is None or ctas_per_sm is None:
             t, c = self.tuned.get((mode, BACKTRACE[backtrace] if isinstance(backtrace, str) else backtrace),
@@ -108,6 +130,7 @@ class CellBatch:
 
     def step_per_cell(self, phi0, phi, interp="cubic_tc", backtrace="midpoint"):
         """The comparator: one dcell_sl_step launch per cell."""
+        self._unpadded()
         mode = INTERP[interp] if isinstance(interp, str) else int(interp)
         bt = BACKTRACE[backtrace] if isinstance(backtrace, str) else int(backtrace)
         L = lib()
@@ -133,6 +156,7 @@ class CellBatch:
         """One split-state tensor-core step of every cell in ONE launch over
         bricks of 32 x 4 x 8 points (dcell_batch_sl_step_tc_split): phi and
         phi_split (the next step's input) receive the new state."""
+        self._unpadded()
         bricks, n = self.plan(self.BRICK)
         check(lib().dcell_batch_sl_step_tc_split(_vp(self.cells), self.ncells, _vp(bricks), n, _vp(phi0_split),
                                                  _vp(self.vel), BACKTRACE[backtrace] if isinstance(backtrace, str)
@@ -142,6 +166,7 @@ class CellBatch:
 
     def step_tc_split_per_cell(self, phi0_split, phi, phi_split, backtrace="midpoint"):
         """The comparator: dcell_sl_step_tc_split launched once per cell."""
+        self._unpadded()
         bt = BACKTRACE[backtrace] if isinstance(backtrace, str) else int(backtrace)
         L = lib()
         st = _stream()
@@ -156,8 +181,34 @@ class CellBatch:
         return phi, phi_split
 
     def cell_view(self, flat, i):
-        o, s = int(self.offsets[i]), self.shapes[i]
-        return flat[o:o + int(np.prod(s))].view(s)
+        """Cell i's grid in a packed array (its real columns when padded)."""
+        o, st = int(self.offsets[i]), self.stored[i]
+        return flat[o:o + int(np.prod(st))].view(st)[..., :self.shapes[i][2]]
+
+    def step_tc_split_tma(self, phi0_split, phi, phi_split, backtrace="midpoint", flags=None):
+        """One split-state tensor-core step of every cell of a padded batch
+        in ONE launch over bricks of 32 x 4 x 8 points, the boxes staged by
+        TMA with a tensor map per cell (dcell_batch_sl_step_tc_split_tma);
+        the maps of each (phi0_split, velocity) buffer pair are built once."""
+        if not self.padded:
+            raise DcellError(_lib.ERR_ARG, "the TMA-staged batched step needs CellBatch(..., padded=True)")
+        bricks, n = self.plan(self.BRICK)
+        key = (phi0_split.data_ptr(), self.vel.data_ptr())
+        maps = self._maps.get(key) if hasattr(self, "_maps") else None
+        if maps is None:
+            if not hasattr(self, "_maps"):
+                self._maps = {}
+            maps = torch.empty(int(lib().dcell_batch_tma_maps_bytes(self.ncells)), dtype=torch.uint8,
+                               device=self.device)
+            check(lib().dcell_batch_tma_maps(self.cells_host.ctypes.data_as(ctypes.c_void_p), self.ncells,
+                                             _vp(phi0_split), _vp(self.vel), _vp(maps), _stream()))
+            self._maps[key] = maps
+        check(lib().dcell_batch_sl_step_tc_split_tma(_vp(self.cells), self.ncells, _vp(bricks), n, _vp(maps),
+                                                     _vp(phi0_split), _vp(self.vel),
+                                                     BACKTRACE[backtrace] if isinstance(backtrace, str)
+                                                     else int(backtrace), _vp(phi), _vp(phi_split),
+                                                     _vp(flags) if flags is not None else None, _stream()))
+        return phi, phi_split
 
     # ------------------------------------------------------------------
     def autotune(self, interp="cubic_tc", backtrace="midpoint", candidates=None, ctas=None, reps=3, cache=None):

@@ -466,6 +466,35 @@ DCELL_API int dcell_batch_sl_step_tc_split(const dcell_cell *cells, int ncells, 
                             (cudaStream_t)stream);
 }
 
+DCELL_API size_t dcell_batch_tma_maps_bytes(int ncells) { return ncells > 0 ? (size_t)ncells * 256 : 0; }
+
+DCELL_API int dcell_batch_tma_maps(const dcell_cell *cells, int ncells, const unsigned int *phi0_split,
+                                   const float *vel, void *maps, void *stream) {
+  if (ncells < 0) FAIL(DCELL_ERR_ARG, "ncells must be >= 0");
+  if (ncells == 0) return DCELL_OK;
+  if (!cells || !phi0_split || !vel || !maps) FAIL(DCELL_ERR_ARG, "cells, phi0_split, vel and maps are required");
+  if (((uintptr_t)maps % 64) || ((uintptr_t)phi0_split % 16) || ((uintptr_t)vel % 16))
+    FAIL(DCELL_ERR_ARG, "maps must be 64-byte aligned, phi0_split and vel 16-byte aligned");
+  std::vector<unsigned char> host((size_t)ncells * 256);
+  int rc = batch_tma_maps_host(cells, ncells, phi0_split, vel, host.data());
+  if (rc) return rc;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(maps, host.data(), host.size(), cudaMemcpyHostToDevice, (cudaStream_t)stream));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize((cudaStream_t)stream));  // the staging vector goes out of scope
+  return DCELL_OK;
+}
+
+DCELL_API int dcell_batch_sl_step_tc_split_tma(const dcell_cell *cells, int ncells, const dcell_tile *bricks,
+                                               int nbricks, const void *maps, const unsigned int *phi0_split,
+                                               const float *vel, int backtrace, float *phi, unsigned int *phi_split,
+                                               int *flags, void *stream) {
+  if (ncells < 0 || nbricks < 0) FAIL(DCELL_ERR_ARG, "ncells and nbricks must be >= 0");
+  if (nbricks > 0 && (!cells || !bricks || !maps || !phi0_split || !vel || !phi || !phi_split))
+    FAIL(DCELL_ERR_ARG, "cells, bricks, maps, phi0_split, vel, phi and phi_split are required");
+  if (backtrace != DCELL_EULER && backtrace != DCELL_MIDPOINT) FAIL(DCELL_ERR_ARG, "unknown backtrace %d", backtrace);
+  return launch_batch_brick_tma(cells, bricks, nbricks, maps, phi0_split, vel, backtrace, phi, phi_split, flags,
+                                (cudaStream_t)stream);
+}
+
 DCELL_API int dcell_tc_gemm_check(const float *a, float *d, int *flags, void *stream) {
   if (!a || !d) FAIL(DCELL_ERR_ARG, "a and d are required");
   return launch_tc_gemm_check(a, d, flags, (cudaStream_t)stream);

@@ -28,6 +28,12 @@ int launch_sl_tc(const dcell::Geom &g, const float *phi0, const float *vel, doub
 int launch_split_bf16(const float *phi, uint32_t *out, long long n, cudaStream_t st);
 int launch_batch_brick(const dcell_cell *cells, const dcell_tile *bricks, int nbricks, const uint32_t *phi0s,
                        const float *vel, int backtrace, float *phi, uint32_t *phis, int *flags, cudaStream_t st);
+// Padded-cell batches staged by TMA: tensor maps encoded on the host (two
+// per cell, `out` holds 2 * ncells CUtensorMap), then the batched brick step.
+int batch_tma_maps_host(const dcell_cell *cells, int ncells, const uint32_t *phi0s, const float *vel, void *out);
+int launch_batch_brick_tma(const dcell_cell *cells, const dcell_tile *bricks, int nbricks, const void *maps,
+                           const uint32_t *phi0s, const float *vel, int backtrace, float *phi, uint32_t *phis,
+                           int *flags, cudaStream_t st);
 // One z-slab of the dense split-state tensor-core step: z bricks [bz0, bz0 +
 // nbz) of tc_slab_planes() planes each, gated on max |w| (FP32 bits at
 // gate_maxw) * dt / h_z <= gate_limit.

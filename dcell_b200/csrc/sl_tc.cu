@@ -982,6 +982,261 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<2>::CtasPerSm)
   if (warp == 0) tmem_dealloc(c.tmem, S::TmemCols);
 }
 
+// Batched split-state stepper over the bricks of many cells, the boxes
+// staged by TMA as in sl_tc_brick_kernel.  The cells are packed with padded
+// rows (dcell_cell.pad = the row length in points, a multiple of 4; cell
+// offsets multiples of 4 points) whose pad columns hold copies of the cell's
+// last column, so every cell is a dense grid of its padded width whose extra
+// columns read as the clamped edge: a TMA map per cell (maps[2 c] the split
+// words, maps[2 c + 1] the velocity, built by dcell_batch_tma_maps), the
+// dense kernel's boxes, edge replication and departures, and the clamped
+// global path all see the cell's own values.  Arrival points are clamped to
+// the cell's columns; lanes over the pad columns store the stepped last
+// column there, which keeps the pads copies.  Per cell the real points get
+// the bits of dcell_sl_step_tc_split on the unpadded cell.
+struct CellBrickP {
+  CellBrick b;  // geometry: g.nx = the padded row length
+  int nxl;      // the cell's columns
+};
+
+__device__ __forceinline__ CellBrickP cell_brick_padded(const dcell_cell *__restrict__ cells,
+                                                        const dcell_tile *__restrict__ bricks, int b) {
+  CellBrickP r;
+  r.b = cell_brick(cells, bricks, b);
+  const dcell_cell C = cells[bricks[b].cell];
+  r.nxl = C.n[0];
+  if (C.pad > C.n[0]) r.b.g.nx = C.pad;
+  return r;
+}
+
+template <int BT>
+__global__ void __launch_bounds__(kBrickThreads, BrickShape<2>::CtasPerSm)
+    batch_brick_tma_kernel(const dcell_cell *__restrict__ cells, const dcell_tile *__restrict__ bricks, int nbricks,
+                           const CUtensorMap *__restrict__ maps, const uint32_t *__restrict__ phi0s,
+                           const float *__restrict__ vel, float *__restrict__ phi, uint32_t *__restrict__ phis,
+                           int *flags) {
+  constexpr int P = 2;
+  using S = BrickShape<P>;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t *sB = smem;
+  uint8_t *const buf0 = smem + kBBytes, *const buf1 = smem + kBBytes + S::BufBytes;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kBBytes + 2 * S::BufBytes);
+  uint64_t *const unused = bars + 0;  // setup() initialises one MMA barrier; this kernel uses its own
+  uint64_t *const afull = bars + 1, *const dfull = bars + 2, *const tbar = bars + 3, *const fixbar = bars + 5;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 6);
+  if (threadIdx.x == 0) {
+    mbar_init(afull, 4);
+    mbar_init(dfull, 1);
+    mbar_init(&tbar[0], 1);
+    mbar_init(&tbar[1], 1);
+    mbar_init(fixbar, kTile);
+  }
+  Ctx c;
+  setup(sB, unused, tmem_slot, c, S::TmemCols);  // B operand, TMEM; ends with a CTA barrier
+
+  const int nmine = (int)blockIdx.x < nbricks ? (nbricks - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const int nsteps = 4 * nmine;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool err = false;
+  // both boxes of the k-th brick of this CTA into `buf` (one thread)
+  auto issue = [&](int k, uint8_t *buf, uint64_t *bar) {
+    const dcell_tile T = bricks[(int)blockIdx.x + k * (int)gridDim.x];
+    fence_proxy_async();
+    mbar_expect_tx(bar, (uint32_t)S::BufBytes);
+    tma_load_3d(buf, maps + 2 * T.cell, T.x0 - 4, T.y0 - 2, T.z0 - 2, bar);
+    tma_load_3d(buf + S::PhiBytes, maps + 2 * T.cell + 1, 3 * (T.x0 - 4), T.y0 - 1, T.z0 - 1, bar);
+  };
+
+  if (warp == 4) {  // ---------------- issuer ----------------
+    if (lane == 0) {
+      int tma_issued[2] = {0, 0}, mma_issued = 0;
+      if (nmine > 0) {
+        issue(0, buf0, &tbar[0]);
+        tma_issued[0] = 1;
+      }
+      if (nmine > 1) {
+        issue(1, buf1, &tbar[1]);
+        tma_issued[1] = 1;
+      }
+      constexpr uint32_t idesc = instr_desc_bf16(kTile, kCoef);
+      for (int j = 0; j < nsteps && !err; ++j) {
+        if (!mbar_wait(afull, (uint32_t)j & 1u)) { err = true; break; }
+        fence_after();
+#pragma unroll
+        for (int st = 0; st < P; ++st)
+#pragma unroll
+          for (int kk = 0; kk < kK / 16; ++kk)
+            mma_bf16(c.tmem + 128 * st + 64, c.tmem + 128 * st + (uint32_t)(kk * 8),
+                     c.bdesc + (uint64_t)((kk * 256) >> 4), idesc, kk > 0 ? 1u : 0u);
+        mma_commit(dfull);
+        ++mma_issued;
+        const int k = j >> 2;
+        if ((j & 3) == 3 && k + 2 < nmine) {  // brick k read for the last time: refill with brick k+2
+          issue(k + 2, k & 1 ? buf1 : buf0, k & 1 ? &tbar[1] : &tbar[0]);
+          ++tma_issued[k & 1];
+        }
+      }
+      bool ok = true;
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        if (tma_issued[b]) ok &= mbar_wait(&tbar[b], (uint32_t)(tma_issued[b] - 1) & 1u);
+      if (mma_issued) ok &= mbar_wait(dfull, (uint32_t)(mma_issued - 1) & 1u);
+      if (err || !ok) raise_flag(flags, FLAG_WAIT_TIMEOUT);
+    }
+  } else {  // ---------------- compute warps ----------------
+    const int lx = lane, ly = warp;
+    uint32_t fixphase = 0;
+    // Boxes of brick k staged (and edge-replicated where they cross the cell's padded grid).
+    auto open_brick = [&](int k, CellBrickP &B) -> bool {
+      const bool odd = k & 1;
+      if (!mbar_wait_sleep(odd ? &tbar[1] : &tbar[0], (uint32_t)(k >> 1) & 1u)) return false;
+      B = cell_brick_padded(cells, bricks, (int)blockIdx.x + k * (int)gridDim.x);
+      const Geom &g = B.b.g;
+      const int x0 = B.b.x0, y0 = B.b.y0, z0 = B.b.z0;
+      if (x0 < 4 || x0 + S::PX - 4 > g.nx || y0 < 2 || y0 + S::PY - 2 > g.ny || z0 < 2 || z0 + S::PZ - 2 > g.nz) {
+        uint8_t *cbuf = odd ? buf1 : buf0;
+        const int op[3] = {x0 - 4, y0 - 2, z0 - 2}, ov[3] = {x0 - 4, y0 - 1, z0 - 1};
+        const int nn[3] = {g.nx, g.ny, g.nz};
+        for (int axis = 0; axis < 3; ++axis) {
+          const bool a =
+              replicate_pass<S::PX, S::PY, S::PZ, 1>(reinterpret_cast<uint32_t *>(cbuf), axis, op, nn, kTile);
+          const bool b = replicate_pass<S::VX, S::VY, S::VZ, 3>(reinterpret_cast<uint32_t *>(cbuf + S::PhiBytes),
+                                                                axis, ov, nn, kTile);
+          if (!(a || b)) continue;
+          fence_proxy_async();  // generic writes before a later TMA refill
+          mbar_arrive(fixbar);
+          const bool ok = mbar_wait_sleep(fixbar, fixphase);
+          fixphase ^= 1u;
+          if (!ok) return false;
+        }
+      }
+      return true;
+    };
+    // Departures of step j's P points; lanes over the cell's pad columns (and
+    // past its last column) compute the last column
+    auto depart = [&](int j, const CellBrickP &B, float f[P][3], int soff[P]) -> bool {
+      const float *vbox = reinterpret_cast<const float *>(((j >> 2) & 1 ? buf1 : buf0) + S::PhiBytes);
+      const int x = min(B.b.x0 + lx, B.nxl - 1), y = min(B.b.y0 + ly, B.b.g.ny - 1);
+      const int zl = P * (j & 3);
+      const bool in = brick_depart<BT, S, P>(vbox, x - B.b.x0 + 4, y - B.b.y0 + 1, zl + 1, x - B.b.x0 + 4,
+                                             y - B.b.y0 + 2, zl + 2, B.b.dth, B.b.hdth, f, soff);
+      return __all_sync(0xffffffffu, in);
+    };
+
+    CellBrickP B;
+    float f[P][3];
+    int soff[P];
+    bool boxed = true;
+    if (nsteps > 0) {
+      err = !open_brick(0, B);
+      if (__any_sync(0xffffffffu, err)) err = true;
+      else boxed = depart(0, B, f, soff);
+    }
+    for (int j = 0; j < nsteps && !err; ++j) {
+      const int k = j >> 2;
+      const uint32_t *ps = phi0s + B.b.off;
+      const float *vs = vel + 3 * B.b.off;
+      // a: A rows of the P points into their stages, then this warp's arrival
+      bool stacked = boxed;
+#pragma unroll
+      for (int p = 1; p < P; ++p) stacked = stacked && soff[p] == soff[0] + p * S::PX * S::PY;
+      if (__all_sync(0xffffffffu, stacked)) {
+        const uint32_t *q = reinterpret_cast<const uint32_t *>(k & 1 ? buf1 : buf0) + soff[0];
+        uint32_t v[16 * (P + 3)];
+#pragma unroll
+        for (int e = 0; e < 16 * (P + 3); ++e) v[e] = q[((e >> 4) * S::PY + ((e >> 2) & 3)) * S::PX + (e & 3)];
+#pragma unroll
+        for (int p = 0; p < P; ++p)
+#pragma unroll
+          for (int q16 = 0; q16 < 4; ++q16) tmem_st16(c.tmem + c.lane_off + 128 * p + 16 * q16, v + 16 * (p + q16));
+      } else {
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          if (boxed) {
+            uint32_t w[64];
+            const uint32_t *q = reinterpret_cast<const uint32_t *>(k & 1 ? buf1 : buf0) + soff[p];
+#pragma unroll
+            for (int e = 0; e < 64; ++e) w[e] = q[((e >> 4) * S::PY + ((e >> 2) & 3)) * S::PX + (e & 3)];
+            __syncwarp();
+            tmem_st32(c.tmem + c.lane_off + 128 * p, w);
+            tmem_st32(c.tmem + c.lane_off + 128 * p + 32, w + 32);
+          } else {  // the warp left its boxes: departure and gathers from global memory
+            const int x = min(B.b.x0 + lx, B.nxl - 1), y = min(B.b.y0 + ly, B.b.g.ny - 1);
+            const int z = min(B.b.z0 + P * (j & 3) + p, B.b.g.nz - 1);
+            const float3 r = brick_rows_global(B.b.g, ps, vs, B.b.dth[0], B.b.dth[1], B.b.dth[2], BT, x, y, z,
+                                               c.tmem + c.lane_off + 128 * p);
+            f[p][0] = r.x;
+            f[p][1] = r.y;
+            f[p][2] = r.z;
+          }
+        }
+      }
+      tmem_wait_st();
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(afull);
+      // b: next step's departures while the tensor core works
+      CellBrickP Bn = B;
+      float fn[P][3];
+      int soffn[P];
+      bool boxedn = true;
+      if (j + 1 < nsteps) {
+        if (((j + 1) & 3) == 0) err = !open_brick(k + 1, Bn);
+        if (__any_sync(0xffffffffu, err)) err = true;
+        else boxedn = depart(j + 1, Bn, fn, soffn);
+      }
+      // c: coefficients -> values, two points at a time
+      const Geom &g = B.b.g;
+      const int y = min(B.b.y0 + ly, g.ny - 1);
+      const int xs = B.b.x0 + lx;  // the column stored: pad columns take the last column's value
+      const bool xy_valid = xs < g.nx && B.b.y0 + ly < g.ny;
+      const int zr = B.b.z0 + P * (j & 3);
+      const int plane = g.nx * g.ny;
+      const long long p0 = B.b.off + ((long long)min(zr, g.nz - 1) * g.ny + y) * g.nx + min(xs, g.nx - 1);
+      const bool ok = mbar_wait_sleep(dfull, (uint32_t)j & 1u);
+      if (__any_sync(0xffffffffu, !ok)) { err = true; break; }
+      fence_after();
+      {
+        float ca[64], cb[64];
+        tmem_ld32f(c.tmem + c.lane_off + 64, ca);
+        tmem_ld32f(c.tmem + c.lane_off + 128 + 64, cb);
+        tmem_ld32f(c.tmem + c.lane_off + 96, ca + 32);
+        tmem_ld32f(c.tmem + c.lane_off + 128 + 96, cb + 32);
+        tmem_wait_ld_tied(ca, cb);
+        tmem_wait_ld_tied(ca + 32, cb + 32);  // completes nothing more: ties the other halves
+        float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
+#pragma unroll
+        for (int kz = 3; kz >= 0; --kz) {
+          va = fmaf(va, f[0][2], horner_slice(ca + 16 * kz, f[0]));
+          vb = fmaf(vb, f[1][2], horner_slice(cb + 16 * kz, f[1]));
+        }
+        if (xy_valid && zr < g.nz) {
+          phi[p0] = va;
+          phis[p0] = pack_split(va);
+        }
+        if (xy_valid && zr + 1 < g.nz) {
+          phi[p0 + plane] = vb;
+          phis[p0 + plane] = pack_split(vb);
+        }
+      }
+      fence_before();
+      B = Bn;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        f[p][0] = fn[p][0]; f[p][1] = fn[p][1]; f[p][2] = fn[p][2];
+        soff[p] = soffn[p];
+      }
+      boxed = boxedn;
+    }
+    if (err) raise_flag(flags, FLAG_WAIT_TIMEOUT);
+  }
+  __syncwarp();  // the issuer warp's other lanes wait here for lane 0
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0) tmem_dealloc(c.tmem, S::TmemCols);
+}
+
 // Batched cells: a persistent CTA walks a packed queue of 128-point tiles
 // (tx x ty x tz boxes of one cell's grid) over many uneven cell grids.
 __global__ void __launch_bounds__(kTile, 4) batch_tc_kernel(const dcell_cell *__restrict__ cells,
@@ -1141,6 +1396,52 @@ int launch_batch_brick(const dcell_cell *cells, const dcell_tile *bricks, int nb
   auto kern = backtrace == DCELL_MIDPOINT ? tc::batch_brick_kernel<DCELL_MIDPOINT> : tc::batch_brick_kernel<DCELL_EULER>;
   kern<<<grid, tc::kBrickThreads, S::DynSmem, st>>>(cells, bricks, nbricks, phi0s, vel, phi, phis, flags);
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int launch_batch_brick_tma(const dcell_cell *cells, const dcell_tile *bricks, int nbricks, const void *maps,
+                           const uint32_t *phi0s, const float *vel, int backtrace, float *phi, uint32_t *phis,
+                           int *flags, cudaStream_t st) {
+  using S = tc::BrickShape<2>;
+  static bool configured = false;
+  if (!configured) {
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::batch_brick_tma_kernel<DCELL_EULER>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, S::DynSmem));
+    DCELL_CUDA_CHECK(cudaFuncSetAttribute(tc::batch_brick_tma_kernel<DCELL_MIDPOINT>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, S::DynSmem));
+    configured = true;
+  }
+  if (nbricks <= 0) return DCELL_OK;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = S::CtasPerSm * sms < nbricks ? S::CtasPerSm * sms : nbricks;
+  auto kern = backtrace == DCELL_MIDPOINT ? tc::batch_brick_tma_kernel<DCELL_MIDPOINT>
+                                          : tc::batch_brick_tma_kernel<DCELL_EULER>;
+  kern<<<grid, tc::kBrickThreads, S::DynSmem, st>>>(cells, bricks, nbricks, (const CUtensorMap *)maps, phi0s, vel,
+                                                      phi, phis, flags);
+  return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
+}
+
+int batch_tma_maps_host(const dcell_cell *cells, int ncells, const uint32_t *phi0s, const float *vel, void *out) {
+  using S = tc::BrickShape<2>;
+  CUtensorMap *m = (CUtensorMap *)out;
+  for (int c = 0; c < ncells; ++c) {
+    const dcell_cell &C = cells[c];
+    const int sx = C.pad > C.n[0] ? C.pad : C.n[0];
+    if (sx % 4 || C.offset % 4 || C.n[1] < 1 || C.n[2] < 2) {
+      dcell_set_error(DCELL_ERR_ARG, "cell %d: rows of %d points at offset %lld: TMA needs rows and offsets that are "
+                                     "multiples of 4 points, and a 3D cell", c, sx, C.offset);
+      return DCELL_ERR_ARG;
+    }
+    if (!make_tensor_map_3d(&m[2 * c], CU_TENSOR_MAP_DATA_TYPE_UINT32, phi0s + C.offset, (uint64_t)sx,
+                            (uint64_t)C.n[1], (uint64_t)C.n[2], S::PX, S::PY, S::PZ, 4) ||
+        !make_tensor_map_3d(&m[2 * c + 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vel + 3 * C.offset, 3ull * sx,
+                            (uint64_t)C.n[1], (uint64_t)C.n[2], 3 * S::VX, S::VY, S::VZ, 4)) {
+      dcell_set_error(DCELL_ERR_CUDA, "cuTensorMapEncodeTiled failed for cell %d", c);
+      return DCELL_ERR_CUDA;
+    }
+  }
+  return DCELL_OK;
 }
 
 int launch_split_bf16(const float *phi, uint32_t *out, long long n, cudaStream_t st) {

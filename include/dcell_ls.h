@@ -361,7 +361,7 @@ DCELL_API int dcell_pls_reseed(const dcell_geom *g, int dtype, const void *phi, 
 typedef struct dcell_cell {
   long long offset;
   int n[3];
-  int pad;
+  int pad; /* 0, or the padded row length of dcell_batch_sl_step_tc_split_tma's packing */
   double h[3];
   double dt;
 } dcell_cell;
@@ -401,6 +401,24 @@ DCELL_API int dcell_batch_sl_step_tc_split(const dcell_cell *cells, int ncells, 
                                            int nbricks, const unsigned int *phi0_split, const float *vel,
                                            int backtrace, float *phi, unsigned int *phi_split, int *flags,
                                            void *stream);
+
+/* The same batched split-state step with the boxes staged by TMA (the dense
+ * kernel's data path), for cells packed with padded rows: cell.pad = the
+ * row length in points (a multiple of 4, >= n[0]; its extra columns hold
+ * copies of the cell's last column in phi0_split and vel), cell.offset a
+ * multiple of 4.  maps: dcell_batch_tma_maps_bytes(ncells) bytes of device
+ * memory filled by dcell_batch_tma_maps for these very phi0_split and vel
+ * arrays (a tensor map per cell and array; build once per buffer pair).  The
+ * step writes every real point with the bits dcell_sl_step_tc_split gives the
+ * unpadded cell, and the pad columns with copies of the new last column, so
+ * its output feeds the next step.  No reference counterpart (batching). */
+DCELL_API size_t dcell_batch_tma_maps_bytes(int ncells);
+DCELL_API int dcell_batch_tma_maps(const dcell_cell *cells, int ncells, const unsigned int *phi0_split,
+                                   const float *vel, void *maps, void *stream);
+DCELL_API int dcell_batch_sl_step_tc_split_tma(const dcell_cell *cells, int ncells, const dcell_tile *bricks,
+                                               int nbricks, const void *maps, const unsigned int *phi0_split,
+                                               const float *vel, int backtrace, float *phi, unsigned int *phi_split,
+                                               int *flags, void *stream);
 
 /* One explicit first-order conservative upwind step of phi on MAC faces:
  * LevelSetAdvectMAC (2D) / LevelSetAdvectMAC_3D, LevelSetMethod/AdvectMAC.c:

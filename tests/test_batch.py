@@ -125,3 +125,35 @@ def test_batched_split_bricks_equal_per_cell_split_steps(cuda, backtrace):
             assert torch.equal(a_phi, c_phi)
             assert torch.equal(a_s, c_s)
             xa, xc = a_s.clone(), c_s.clone()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("backtrace", ["midpoint", "euler"])
+def test_tma_batched_split_bricks_equal_per_cell_split_steps(cuda, backtrace):
+    """The TMA-staged batched step on a padded batch (rows padded to 4
+    points, pad columns copies of each cell's last column, a tensor map per
+    cell) gives every cell's real points the bits of dcell_sl_step_tc_split
+    on that cell alone, and keeps the pad columns copies of the new last
+    column, over three consecutive steps, also at 3x the CFL (the global
+    fallback)."""
+    from dcell_b200.batch import CellBatch, c4_workload
+    phis, vels, hs, dt = c4_workload(ncells=10, emin=5, emax=70, seed=11, device=cuda)
+    assert any(p.shape[2] % 4 for p in phis)
+    for scale in (1.0, 3.0):
+        dts = dt * scale
+        ref = CellBatch(phis, vels, hs, dts, device=cuda)
+        b = CellBatch(phis, vels, hs, dts, device=cuda, padded=True)
+        xr, xb = ref.split(), b.split()
+        r_phi, r_s = torch.empty_like(ref.phi), torch.empty_like(xr)
+        b_phi, b_s = torch.empty_like(b.phi), torch.empty_like(xb)
+        for _ in range(3):
+            ref.step_tc_split_per_cell(xr, r_phi, r_s, backtrace)
+            b.step_tc_split_tma(xb, b_phi, b_s, backtrace)
+            torch.cuda.synchronize()
+            for i in range(b.ncells):
+                assert torch.equal(b.cell_view(b_phi, i), ref.cell_view(r_phi, i)), i
+                assert torch.equal(b.cell_view(b_s, i), ref.cell_view(r_s, i)), i
+                full = b_s[int(b.offsets[i]):int(b.offsets[i]) + int(np.prod(b.stored[i]))].view(b.stored[i])
+                nx = b.shapes[i][2]
+                assert torch.equal(full[..., nx:], full[..., nx - 1:nx].expand_as(full[..., nx:])), i
+            xr, xb = r_s.clone(), b_s.clone()

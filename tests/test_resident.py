@@ -44,11 +44,11 @@ def test_resident_loop_equals_the_device_api_loop(cuda):
     dt = 0.9 * h
     ls = L.LevelSetCreate(h, (0, 0, 0), (N, N, N), dtype=torch.float64, device=cuda)
     ls.phi.copy_(phi)
-    ls.band = band.to(cuda)
+    ls.band = band.to(cuda).contiguous()
     ls.CFLthres = 1.0
     ls.Reinitialize = L.LevelSetReinitializeGPU
     L.LevelSetUpdateIrregularNodeList(ls)
-    r = L.ResidentLevelSet(phi.cpu().numpy(), h, band=band.numpy(), precision="f64", CFLthres=1.0)
+    r = L.ResidentLevelSet(phi.cpu().numpy(), h, band=band.cpu().numpy(), precision="f64", CFLthres=1.0)
     vhost = vel.cpu().numpy()
     reinits = 0
     for s in range(8):
@@ -71,7 +71,7 @@ def test_resident_tc_loop_equals_split_state_steps(cuda):
     N = 64
     h, phi, vel, band = _case(N, cuda)
     dt = 0.5 * h
-    r = L.ResidentLevelSet(phi.cpu().numpy(), h, band=band.numpy(), precision="f32", CFLthres=1e9)
+    r = L.ResidentLevelSet(phi.cpu().numpy(), h, band=band.cpu().numpy(), precision="f32", CFLthres=1e9)
     v32 = vel.float().contiguous()
     vhost = v32.cpu().numpy()
     spl = L.split_bf16(phi.float().contiguous())
