@@ -19,7 +19,9 @@ c3  the same field at 256^3 over the whole period (t = 0 .. T): the
     split-state TC and plain FP32 trajectories at t = T.
 c4  512 cells, edges U{32..96} (seeded), ellipsoids in 8-mode divergence-free
     Fourier velocities, 20 steps: one persistent CUDA-graph launch per step
-    with autotuned tiles vs one launch per cell.
+    with autotuned tiles vs one launch per cell; the split-state bricks of
+    all cells in one launch per step, staged by cp.async and, over a padded
+    packing, by TMA.
 vel velocity acquisition of 512 cells' boxes (edges U{32..96}, some
     straddling the domain edge) from a 512^3 fluid field [z][y][x][c] (FP32,
     c = CELL_CENTER, U, V, W) in one dcell_velocity_boxes launch: time,
@@ -275,6 +277,27 @@ def run_c4(dev="cuda", ncells=512, steps=20):
                                     "equal_to_per_cell": bool(torch.equal(pa, pc)),
                                     "how": "dcell_batch_sl_step_tc_split, one launch per step over bricks of all "
                                            "cells, split state, CUDA events"}
+    # the same over a padded packing with the boxes staged by TMA (a tensor
+    # map per cell); the real points must equal the unpadded run's
+    bp = CellBatch(phis, vels, hs, dt, device=dev, padded=True)
+    sp = bp.split()
+    xp, yp, pp = sp.clone(), torch.empty_like(sp), torch.empty_like(bp.phi)
+    bp.step_tc_split_tma(xp, pp, yp)  # warm-up (tensor maps of both buffers)
+    bp.step_tc_split_tma(yp, pp, xp)
+    xp.copy_(sp)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        bp.step_tc_split_tma(xp, pp, yp)
+        xp, yp = yp, xp
+    e1.record()
+    torch.cuda.synchronize()
+    ms_tma = e0.elapsed_time(e1)
+    same = all(torch.equal(bp.cell_view(pp, i), b.cell_view(pa, i)) for i in range(b.ncells))
+    res["cubic_tc_split_bricks_tma"] = {"ms": ms_tma, "updates_per_s": b.npoints * steps / (ms_tma / 1e3),
+                                        "stored_points": bp.npoints, "equal_to_unpadded": same,
+                                        "how": "dcell_batch_sl_step_tc_split_tma, rows padded to 4 points, TMA "
+                                               "boxes through a tensor map per cell, CUDA events"}
     return res
 
 
