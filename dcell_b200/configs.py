@@ -35,6 +35,8 @@ reinit  narrow-band reinitialisation (bucketed fast marching) of the
 io  output: phi of the 256^3 workload (FP32) written 10 times in the
     reference's .Real64 format by the asynchronous writer -- the time the
     compute stream spends on each snapshot, and the drain rate to disk.
+steps  K dense steps of one SL form at 256^3 (--interp, --backtrace, --steps):
+    the command the kernel profiles capture.
 c5  128^3, 50 midpoint steps, velocity from 16 learnable Fourier
     coefficients, loss sum (H_eps(phi_T) - H_eps(phi_target))^2: hand-written
     adjoint (checkpoints every 10) vs FP64 central differences (delta 1e-3)
@@ -608,13 +610,39 @@ def run_c5(N=128, steps=50, every=10, dev="cuda", fd_modes=16):
     return res
 
 
+def run_steps(N=256, interp="cubic_tc", backtrace="midpoint", steps=4, dev="cuda"):
+    """`steps` dense steps of one form of the SL step (any `interp` name of
+    levelset.sl_step, "_gather" forms included) on the benchmark's N^3
+    workload (sphere in the deformation field, FP32, dt at CFL 0.5), the
+    same input each step; CUDA events.  The command the kernel profiles
+    capture."""
+    h, phi0, vel = _deformation(N, dev)
+    phi, v = phi0.float().contiguous(), vel.float().contiguous()
+    del phi0, vel
+    dt = fields.cfl_dt((2.0, 1.0, 1.0), h)
+    out = torch.empty_like(phi)
+    e0, e1 = _events()
+    L.sl_step(phi, v, dt, h, interp=interp, backtrace=backtrace, out=out)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        L.sl_step(phi, v, dt, h, interp=interp, backtrace=backtrace, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"grid": [N] * 3, "interp": interp, "backtrace": backtrace, "steps": steps, "ms_per_step": ms,
+            "updates_per_s": N ** 3 / (ms / 1e3)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("which", nargs="?", default="all")
     ap.add_argument("--out", default=None)
     ap.add_argument("--grid", type=int, default=None, help="vel: edge of the fluid field (512); pls: grid edge (256)")
     ap.add_argument("--cells", type=int, default=512, help="vel: number of cell boxes; c4: number of cells")
-    ap.add_argument("--steps", type=int, default=20, help="c4: steps per timed run")
+    ap.add_argument("--steps", type=int, default=20, help="c4, steps: steps per timed run")
+    ap.add_argument("--interp", default="cubic_tc", help="steps: the SL form (levelset.sl_step interp name)")
+    ap.add_argument("--backtrace", default="midpoint", help="steps: euler or midpoint")
     a = ap.parse_args()
     todo = ["c1", "c2", "c3", "c4", "c5"] if a.which == "all" else a.which.split(",")
     results = {}
@@ -624,6 +652,7 @@ def main():
                       run_pls(a.grid or 256) if c == "pls" else run_io(a.grid or 256) if c == "io" else
                       run_reinit(a.grid or 256) if c == "reinit" else run_mac(a.grid or 256) if c == "mac" else
                       run_nodes(a.grid or 256) if c == "nodes" else run_c4(ncells=a.cells, steps=a.steps) if c == "c4" else
+                      run_steps(a.grid or 256, a.interp, a.backtrace, a.steps) if c == "steps" else
                       globals()[f"run_{c}"]())
         results[c]["wall_s"] = time.time() - t0
         print(json.dumps({c: results[c]}, default=float), flush=True)

@@ -238,36 +238,28 @@ struct MarchGrid {
 // (x0, y0), the staged ring read through accessor A (clamped at the grid's x
 // / y edges, or not); warps whose reads would leave the box redo the plane
 // through global memory.  Returns false when a wait gave up.
-template <int BT, class S, int PZ, class A>
+template <int BT, class S, class A>
 __device__ __forceinline__ bool march_run(const A &bacc, const GlobalAcc<3> &gacc, const Geom &g, int x0, int y0,
                                           int zs, int ze, int lane, int warp, const float dth[3], const float hdth[3],
                                           uint64_t *full, uint64_t *empty, uint32_t &fpar, float *__restrict__ phi) {
   const int x = min(x0 + lane, g.nx - 1), y = min(y0 + warp, g.ny - 1);
   const bool store = x0 + lane < g.nx && y0 + warp < g.ny;
   int waited = zs - 2;
-  for (int z = zs; z < ze; z += PZ) {  // PZ planes per round: z .. zn - 1
-    const int zn = min(z + PZ, ze);
-    for (; waited <= zn + 1; ++waited) {  // planes up to zn + 1 present
+  for (int z = zs; z < ze; ++z) {
+    for (; waited <= z + 2; ++waited) {  // planes up to z + 2 present
       const int s = BoxAcc<S, false>::slot(waited);
       const bool ok = mbar_wait_sleep(&full[s], (fpar >> s) & 1u);
       if (!__all_sync(0xffffffffu, ok)) return false;
       fpar ^= 1u << s;
     }
-#pragma unroll
-    for (int q = 0; q < PZ; ++q) {
-      const int zq = z + q;
-      if (zq < zn) {  // warp-uniform
-        int c[3];
-        float f[3];
-        float v;
-        if (!lin_point<BT, 3, true>(bacc, x, y, zq, dth, hdth, v, c, f))
-          lin_point<BT, 3, false>(gacc, x, y, zq, dth, hdth, v, c, f);
-        if (store) phi[(zq * g.ny + y) * g.nx + x] = v;
-      }
-    }
+    int c[3];
+    float f[3];
+    float v;
+    if (!lin_point<BT, 3, true>(bacc, x, y, z, dth, hdth, v, c, f))
+      lin_point<BT, 3, false>(gacc, x, y, z, dth, hdth, v, c, f);
+    if (store) phi[(z * g.ny + y) * g.nx + x] = v;
     __syncwarp();
-    if (lane == 0)  // planes z - 2 .. zn - 3 read for the last time
-      for (int q = z - 2; q < zn - 2; ++q) mbar_arrive(&empty[BoxAcc<S, false>::slot(q)]);
+    if (lane == 0) mbar_arrive(&empty[BoxAcc<S, false>::slot(z - 2)]);  // plane z - 2 read for the last time
   }
   __syncwarp();
   if (lane == 0)
@@ -292,7 +284,7 @@ __device__ __forceinline__ bool march_run(const A &bacc, const GlobalAcc<3> &gac
 // bounded; a warp that gives up raises FLAG_WAIT_TIMEOUT and leaves (the
 // others then give up at their next wait), and the producer waits (bounded)
 // for its last load per slot before the CTA ends.
-template <int BT, int TY, int PZ>
+template <int BT, int TY>
 __global__ void __launch_bounds__(MarchShape<TY, BT>::Threads, MarchShape<TY, BT>::CtasPerSm)
     sl_lin_march_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel,
                         Geom g, MarchGrid mg, const float *__restrict__ phi0, const float *__restrict__ vel, float dth0,
@@ -322,8 +314,8 @@ __global__ void __launch_bounds__(MarchShape<TY, BT>::Threads, MarchShape<TY, BT
         for (int p = zs - 2; p <= ze + 1; ++p) {
           const int s = BoxAcc<S, false>::slot(p), pz = clampi(p, 0, g.nz - 1);
           const uint32_t bit = 1u << s;
-          if (used & bit) {
-            if (!mbar_wait(&empty[s], (epar & bit) ? 1u : 0u)) {
+          if (used & bit) {  // suspend-hinted: a polling producer would take issue slots from the consumers
+            if (!mbar_wait_sleep(&empty[s], (epar & bit) ? 1u : 0u)) {
               err = true;
               break;
             }
@@ -357,11 +349,11 @@ __global__ void __launch_bounds__(MarchShape<TY, BT>::Threads, MarchShape<TY, BT
     const int x0 = (tile % mg.ncx) * TX, y0 = (tile / mg.ncx) * TY;
     if (x0 >= HX && x0 - HX + PW <= g.nx && y0 >= HY && y0 - HY + S::PH <= g.ny && x0 + S::VX0 >= 0 &&
         x0 + S::VX0 + S::VXN <= g.nx && y0 + S::VY0 >= 0 && y0 + S::VY0 + S::VH <= g.ny)
-      ok = march_run<BT, S, PZ>(BoxAcc<S, false>(phis, vels, x0, y0, g.nx, g.ny), gacc, g, x0, y0, zs, ze, lane,
-                                warp, dth, hdth, full, empty, fpar, phi);
+      ok = march_run<BT, S>(BoxAcc<S, false>(phis, vels, x0, y0, g.nx, g.ny), gacc, g, x0, y0, zs, ze, lane, warp, dth,
+                            hdth, full, empty, fpar, phi);
     else
-      ok = march_run<BT, S, PZ>(BoxAcc<S, true>(phis, vels, x0, y0, g.nx, g.ny), gacc, g, x0, y0, zs, ze, lane, warp,
-                                dth, hdth, full, empty, fpar, phi);
+      ok = march_run<BT, S>(BoxAcc<S, true>(phis, vels, x0, y0, g.nx, g.ny), gacc, g, x0, y0, zs, ze, lane, warp, dth,
+                            hdth, full, empty, fpar, phi);
   }
   if (!ok && lane == 0) raise_flag(flags, FLAG_WAIT_TIMEOUT);
 }
@@ -401,28 +393,14 @@ static int lin_segment_planes() {
 }
 
 // The march with backtrace BT; false when no tensor maps could be made.
-// Planes per consumer round of the march: 2 (the two points of a thread
-// share the loop's waits and releases and a face of their velocity);
-// DCELL_LIN_PLANES_PER_ROUND=1 selects one.
-static int lin_round_planes() {
-  static int planes = 0;
-  if (!planes) {
-    planes = 2;
-    if (const char *e = getenv("DCELL_LIN_PLANES_PER_ROUND")) planes = atoi(e) == 1 ? 1 : 2;
-  }
-  return planes;
-}
-
 template <int TY, int BT>
 static bool launch_march_bt(const Geom &g, const float *phi0, const float *vel, float dth0, float dth1, float dth2,
                             float *phi, int *flags, cudaStream_t st) {
   using S = lin::MarchShape<TY, BT>;
   static bool configured = false;
   if (!configured) {
-    if (cudaFuncSetAttribute(lin::sl_lin_march_kernel<BT, TY, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             S::Smem) != cudaSuccess ||
-        cudaFuncSetAttribute(lin::sl_lin_march_kernel<BT, TY, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             S::Smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(lin::sl_lin_march_kernel<BT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::Smem) !=
+        cudaSuccess)
       return false;
     configured = true;
   }
@@ -443,8 +421,8 @@ static bool launch_march_bt(const Geom &g, const float *phi0, const float *vel, 
   // rounds of at most one resident wave; the grid evens the units over them
   const int slots = S::CtasPerSm * sms, rounds = (mg.units + slots - 1) / slots;
   const int grid = (mg.units + rounds - 1) / rounds;
-  auto kern = lin_round_planes() == 2 ? lin::sl_lin_march_kernel<BT, TY, 2> : lin::sl_lin_march_kernel<BT, TY, 1>;
-  kern<<<grid, S::Threads, S::Smem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0, dth1, dth2, phi, flags);
+  lin::sl_lin_march_kernel<BT, TY><<<grid, S::Threads, S::Smem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0, dth1,
+                                                                       dth2, phi, flags);
   return true;
 }
 
