@@ -15,13 +15,14 @@
 // global-memory paths below give the same bits.
 //
 // Dense 3-D grids (nx % 4 == 0) march z-columns through a plane ring staged
-// by TMA: a CTA of 256 threads owns a 32 x 8 tile of every plane of a z-run,
-// and keeps planes z-2 .. z+5 of phi0 (40 x 12 floats, halo 4 | 2) and of the
-// interleaved velocity (120 x 12 floats) in an 8-slot ring; each plane is
-// loaded once as it enters the window, three planes ahead of its first use.
-// Per point: 6 (Euler) or 6 + 24 (midpoint) velocity and 8 phi0 values from
-// shared memory, one coalesced store.  Bands, 2-D grids and other shapes run
-// the global-gather kernel with the same arithmetic.
+// by TMA: a CTA owns a 32 x TY tile (TY = 8 for Euler, 16 for the midpoint)
+// of every plane of a z-run, each consumer warp two of its rows, and keeps
+// planes z-2 .. z+5 of phi0 (40 x (TY+4) floats, halo 4 | 2) and of the
+// interleaved velocity in an 8-slot ring; each plane is loaded once as it
+// enters the window, three planes ahead of its first use.  Per point: 6
+// (Euler) or 6 + 24 (midpoint) velocity and 8 phi0 values from shared memory,
+// one coalesced store.  Bands, 2-D grids and other shapes run the
+// global-gather kernel with the same arithmetic.
 #include <math.h>
 
 #include <stdlib.h>
@@ -41,16 +42,19 @@ constexpr int HX = 4, HY = 2;              // phi box halo (x: 4 keeps TMA x coo
 constexpr int PW = TX + 2 * HX;            // 40 phi values per box row
 constexpr int kRing = 8;                   // ring slots: planes z-2 .. z+2 in use, up to three ahead
 
-// A tile of TX x TY points per plane: TY consumer warps (one tile row each)
-// and one producer warp.  The phi box is [x0-4, x0+36) x [y0-2, y0+TY+2).
+// A tile of TX x TY points per plane: TY / RW consumer warps (RW adjacent
+// tile rows each) and one producer warp.  The phi box is [x0-4, x0+36) x
+// [y0-2, y0+TY+2).
 // The velocity box holds what the backtrace reads: the faces around the
 // nodes for Euler, [x0, x0+36) x [y0, y0+TY+1) (36 points keep the row a
 // multiple of 16 bytes), and the midpoint's trilinear corners within one
 // cell of the nodes as well, [x0-4, x0+36) x [y0-1, y0+TY+2).  Planes start
 // on 128-byte boundaries.
-template <int TY_, int BT>
+template <int TY_, int BT, int RW_>
 struct MarchShape {
   static constexpr int TY = TY_;
+  static constexpr int RW = RW_;      // tile rows per consumer warp
+  static constexpr int Warps = TY / RW;  // consumer warps
   static constexpr int PH = TY + 2 * HY;
   static constexpr int VX0 = BT == DCELL_MIDPOINT ? -4 : 0;   // velocity box x origin - x0
   static constexpr int VY0 = BT == DCELL_MIDPOINT ? -1 : 0;   // velocity box y origin - y0
@@ -61,12 +65,13 @@ struct MarchShape {
   static constexpr int PlaneVel = (VW * VH + 31) / 32 * 32;     // floats of one staged velocity plane (padded)
   static constexpr int VelBoxBytes = 4 * VW * VH;               // bytes a velocity load writes
   static constexpr int PlaneBytes = 4 * PlanePhi + VelBoxBytes;  // transaction bytes per plane
-  static constexpr int Threads = 32 * (TY + 1);
+  static constexpr int Threads = 32 * (Warps + 1);
   static constexpr int Smem = kRing * 4 * (PlanePhi + PlaneVel) + 2 * kRing * 8;  // + full / empty mbarriers
   static constexpr int CtasPerSm = (228 * 1024) / (Smem + 1024) < 4 ? (228 * 1024) / (Smem + 1024) : 4;
   static_assert((4 * PlanePhi) % 128 == 0 && (4 * PlaneVel) % 128 == 0, "staged planes stay 128-byte aligned");
   static_assert((4 * VW) % 16 == 0 && (4 * PW) % 16 == 0, "box rows are multiples of 16 bytes");
   static_assert(CtasPerSm >= 1, "ring too large for one CTA");
+  static_assert(TY % RW == 0, "whole rows per consumer warp");
 };
 static_assert((kRing & (kRing - 1)) == 0 && kRing >= 8, "ring slot of plane p is (p + kRing) & (kRing - 1)");
 
@@ -94,7 +99,7 @@ struct GlobalAcc {
 // into the grid and into the box in one step, so a read at any index stays
 // in the ring and equals the global clamped read wherever the grid-clamped
 // position lies in the box.  Without CLAMP (the box inside the grid) indices
-// map straight into the box: lin_point reads only indices it has checked to
+// map straight into the box: lin_points reads only indices it has checked to
 // lie in the box.
 template <class S, bool CLAMP>
 struct BoxAcc {
@@ -124,75 +129,94 @@ struct BoxAcc {
   }
 };
 
-// One arrival point (local indices x, y, z): node velocity, optional
-// midpoint velocity, departure, bi/trilinear phi0, into `out`; c, f: the
-// departure cell (local) and fraction.  dth = dt / h per axis, hdth = -dt /
-// (2 h).  VOTE (staged boxes; called by whole warps): before the midpoint
-// velocity and before phi0 are read, the warp checks that every lane's reads
-// stay in the staged box (|midpoint offset| < 1, departure offset in [-2, 2)
-// per axis) and returns false, with nothing read, where one does not; the
-// node velocity always lies in the box.  The arithmetic is the same either
-// way, so a warp redone through global memory gives the same bits.
-template <int BT, int DIM, bool VOTE, class A>
-__device__ __forceinline__ bool lin_point(const A &acc, int x, int y, int z, const float dth[3], const float hdth[3],
-                                          float &out, int c[3], float f[3]) {
-  const int X[3] = {x, y, z};
-  float U[3];
-  U[0] = face_mean(acc.v(x, y, z, 0), acc.v(x + 1, y, z, 0));
-  U[1] = face_mean(acc.v(x, y, z, 1), acc.v(x, y + 1, z, 1));
-  U[2] = DIM == 3 ? face_mean(acc.v(x, y, z, 2), acc.v(x, y, z + 1, 2)) : 0.f;
+// R arrival points of one thread (local indices x, y[r], z): node velocity,
+// optional midpoint velocity, departure, bi/trilinear phi0, into out[r]; c,
+// f: the departure cells (local) and fractions.  dth = dt / h per axis,
+// hdth = -dt / (2 h).  Each phase runs over all R points before the next, so
+// their loads overlap.  VOTE (staged boxes; called by whole warps): before
+// the midpoint velocity and before phi0 are read, the warp checks that every
+// lane's reads of all R points stay in the staged box (|midpoint offset| <
+// 1, departure offset in [-2, 2) per axis) and returns false, with nothing
+// read, where one does not; the node velocity always lies in the box.  The
+// arithmetic is the same either way, so a warp redone through global memory
+// gives the same bits.
+template <int BT, int DIM, bool VOTE, int R, class A>
+__device__ __forceinline__ bool lin_points(const A &acc, int x, const int y[R], int z, const float dth[3],
+                                           const float hdth[3], float out[R], int c[R][3], float f[R][3]) {
+  float U[R][3];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    U[r][0] = face_mean(acc.v(x, y[r], z, 0), acc.v(x + 1, y[r], z, 0));
+    U[r][1] = face_mean(acc.v(x, y[r], z, 1), acc.v(x, y[r] + 1, z, 1));
+    U[r][2] = DIM == 3 ? face_mean(acc.v(x, y[r], z, 2), acc.v(x, y[r], z + 1, 2)) : 0.f;
+  }
   if (BT == DCELL_MIDPOINT) {
-    float dl[3];
+    float dl[R][3];
     bool near = true;
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) {
-      dl[a] = rmul(U[a], hdth[a]);
-      near = near && fabsf(dl[a]) < 1.f;
-    }
-    if (VOTE && !__all_sync(0xffffffffu, near)) return false;
-    float V[3] = {0.f, 0.f, 0.f};
+    for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      int b[3] = {0, 0, z};
-      float s[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) {  // the component's own axis carries the half-cell stagger
-        const float t = a == d ? __fadd_rn(dl[a], 0.5f) : dl[a];
-        const float fl = floorf(t);
-        b[a] = X[a] + (int)fl;
-        s[a] = __fsub_rn(t, fl);
+      for (int a = 0; a < DIM; ++a) {
+        dl[r][a] = rmul(U[r][a], hdth[a]);
+        near = near && fabsf(dl[r][a]) < 1.f;
       }
-      if (DIM == 3)
-        V[d] = trilerp(acc.v(b[0], b[1], b[2], d), acc.v(b[0] + 1, b[1], b[2], d), acc.v(b[0], b[1] + 1, b[2], d),
-                       acc.v(b[0] + 1, b[1] + 1, b[2], d), acc.v(b[0], b[1], b[2] + 1, d),
-                       acc.v(b[0] + 1, b[1], b[2] + 1, d), acc.v(b[0], b[1] + 1, b[2] + 1, d),
-                       acc.v(b[0] + 1, b[1] + 1, b[2] + 1, d), s);
-      else
-        V[d] = bilerp(acc.v(b[0], b[1], 0, d), acc.v(b[0] + 1, b[1], 0, d), acc.v(b[0], b[1] + 1, 0, d),
-                      acc.v(b[0] + 1, b[1] + 1, 0, d), s[0], s[1]);
-    }
+    if (VOTE && !__all_sync(0xffffffffu, near)) return false;
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) U[a] = V[a];
+    for (int r = 0; r < R; ++r) {
+      const int X[3] = {x, y[r], z};
+      float V[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        int b[3] = {0, 0, z};
+        float s[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {  // the component's own axis carries the half-cell stagger
+          const float t = a == d ? __fadd_rn(dl[r][a], 0.5f) : dl[r][a];
+          const float fl = floorf(t);
+          b[a] = X[a] + (int)fl;
+          s[a] = __fsub_rn(t, fl);
+        }
+        if (DIM == 3)
+          V[d] = trilerp(acc.v(b[0], b[1], b[2], d), acc.v(b[0] + 1, b[1], b[2], d), acc.v(b[0], b[1] + 1, b[2], d),
+                         acc.v(b[0] + 1, b[1] + 1, b[2], d), acc.v(b[0], b[1], b[2] + 1, d),
+                         acc.v(b[0] + 1, b[1], b[2] + 1, d), acc.v(b[0], b[1] + 1, b[2] + 1, d),
+                         acc.v(b[0] + 1, b[1] + 1, b[2] + 1, d), s);
+        else
+          V[d] = bilerp(acc.v(b[0], b[1], 0, d), acc.v(b[0] + 1, b[1], 0, d), acc.v(b[0], b[1] + 1, 0, d),
+                        acc.v(b[0] + 1, b[1] + 1, 0, d), s[0], s[1]);
+      }
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) U[r][a] = V[a];
+    }
   }
-  c[2] = z;
-  f[2] = 0.f;
   bool in = true;
 #pragma unroll
-  for (int a = 0; a < DIM; ++a) {
-    const float t = rmul(-U[a], dth[a]);
-    in = in && t >= -2.f && t < 2.f;
-    const float fl = floorf(t);
-    c[a] = X[a] + (int)fl;
-    f[a] = __fsub_rn(t, fl);
+  for (int r = 0; r < R; ++r) {
+    const int X[3] = {x, y[r], z};
+    c[r][2] = z;
+    f[r][2] = 0.f;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      const float t = rmul(-U[r][a], dth[a]);
+      in = in && t >= -2.f && t < 2.f;
+      const float fl = floorf(t);
+      c[r][a] = X[a] + (int)fl;
+      f[r][a] = __fsub_rn(t, fl);
+    }
   }
   if (VOTE && !__all_sync(0xffffffffu, in)) return false;
-  if (DIM == 3)
-    out = trilerp(acc.phi(c[0], c[1], c[2]), acc.phi(c[0] + 1, c[1], c[2]), acc.phi(c[0], c[1] + 1, c[2]),
-                  acc.phi(c[0] + 1, c[1] + 1, c[2]), acc.phi(c[0], c[1], c[2] + 1), acc.phi(c[0] + 1, c[1], c[2] + 1),
-                  acc.phi(c[0], c[1] + 1, c[2] + 1), acc.phi(c[0] + 1, c[1] + 1, c[2] + 1), f);
-  else
-    out = bilerp(acc.phi(c[0], c[1], 0), acc.phi(c[0] + 1, c[1], 0), acc.phi(c[0], c[1] + 1, 0),
-                 acc.phi(c[0] + 1, c[1] + 1, 0), f[0], f[1]);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int *C = c[r];
+    if (DIM == 3)
+      out[r] = trilerp(acc.phi(C[0], C[1], C[2]), acc.phi(C[0] + 1, C[1], C[2]), acc.phi(C[0], C[1] + 1, C[2]),
+                       acc.phi(C[0] + 1, C[1] + 1, C[2]), acc.phi(C[0], C[1], C[2] + 1),
+                       acc.phi(C[0] + 1, C[1], C[2] + 1), acc.phi(C[0], C[1] + 1, C[2] + 1),
+                       acc.phi(C[0] + 1, C[1] + 1, C[2] + 1), f[r]);
+    else
+      out[r] = bilerp(acc.phi(C[0], C[1], 0), acc.phi(C[0] + 1, C[1], 0), acc.phi(C[0], C[1] + 1, 0),
+                      acc.phi(C[0] + 1, C[1] + 1, 0), f[r][0], f[r][1]);
+  }
   return true;
 }
 
@@ -215,13 +239,14 @@ __global__ void __launch_bounds__(256) sl_lin_gather_kernel(Geom g, const float 
       bad = true;
       continue;
     }
-    int c[3];
-    float f[3];
-    float v;
-    lin_point<BT, DIM, false>(acc, x, y, z, dth, hdth, v, c, f);
-    phi[(z * g.ny + y) * g.nx + x] = v;
+    int c[1][3];
+    float f[1][3];
+    float v[1];
+    const int yy[1] = {y};
+    lin_points<BT, DIM, false, 1>(acc, x, yy, z, dth, hdth, v, c, f);
+    phi[(z * g.ny + y) * g.nx + x] = v[0];
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) clamped |= c[a] < 0 || c[a] + (f[a] > 0.f ? 1 : 0) > n[a] - 1;
+    for (int a = 0; a < DIM; ++a) clamped |= c[0][a] < 0 || c[0][a] + (f[0][a] > 0.f ? 1 : 0) > n[a] - 1;
   }
   if (bad) raise_flag(flags, FLAG_BAD_BAND);
   if (clamped && band) raise_flag(flags, FLAG_DEPARTURE_CLAMPED);  // dense grids: the edge is the domain boundary
@@ -242,8 +267,15 @@ template <int BT, class S, class A>
 __device__ __forceinline__ bool march_run(const A &bacc, const GlobalAcc<3> &gacc, const Geom &g, int x0, int y0,
                                           int zs, int ze, int lane, int warp, const float dth[3], const float hdth[3],
                                           uint64_t *full, uint64_t *empty, uint32_t &fpar, float *__restrict__ phi) {
-  const int x = min(x0 + lane, g.nx - 1), y = min(y0 + warp, g.ny - 1);
-  const bool store = x0 + lane < g.nx && y0 + warp < g.ny;
+  const int x = min(x0 + lane, g.nx - 1);
+  int y[S::RW];
+  bool store[S::RW];
+#pragma unroll
+  for (int r = 0; r < S::RW; ++r) {  // the warp's rows: y0 + RW * warp + r
+    const int yr = y0 + S::RW * warp + r;
+    y[r] = min(yr, g.ny - 1);
+    store[r] = x0 + lane < g.nx && yr < g.ny;
+  }
   int waited = zs - 2;
   for (int z = zs; z < ze; ++z) {
     for (; waited <= z + 2; ++waited) {  // planes up to z + 2 present
@@ -252,12 +284,14 @@ __device__ __forceinline__ bool march_run(const A &bacc, const GlobalAcc<3> &gac
       if (!__all_sync(0xffffffffu, ok)) return false;
       fpar ^= 1u << s;
     }
-    int c[3];
-    float f[3];
-    float v;
-    if (!lin_point<BT, 3, true>(bacc, x, y, z, dth, hdth, v, c, f))
-      lin_point<BT, 3, false>(gacc, x, y, z, dth, hdth, v, c, f);
-    if (store) phi[(z * g.ny + y) * g.nx + x] = v;
+    int c[S::RW][3];
+    float f[S::RW][3];
+    float v[S::RW];
+    if (!lin_points<BT, 3, true, S::RW>(bacc, x, y, z, dth, hdth, v, c, f))
+      lin_points<BT, 3, false, S::RW>(gacc, x, y, z, dth, hdth, v, c, f);
+#pragma unroll
+    for (int r = 0; r < S::RW; ++r)
+      if (store[r]) phi[(z * g.ny + y[r]) * g.nx + x] = v[r];
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[BoxAcc<S, false>::slot(z - 2)]);  // plane z - 2 read for the last time
   }
@@ -275,8 +309,8 @@ __device__ __forceinline__ bool march_run(const A &bacc, const GlobalAcc<3> &gac
 // segment's boundary planes, reloaded by the next segment's unit one round
 // later, too.  Per unit a producer warp loads every plane the unit reads
 // (zs-2 .. ze+1) into the ring, each one once the slot's previous plane is
-// released; the TY consumer warps wait on a slot's `full` mbarrier before a
-// plane's first use, compute their row of the plane, and release plane z-2
+// released; the TY / RW consumer warps wait on a slot's `full` mbarrier
+// before a plane's first use, compute their rows of the plane, release plane z-2
 // on its `empty` mbarrier after plane z (the unit's last planes at its end).
 // No CTA barrier in the loop: warps drift up to a few planes apart.  Warps
 // whose points read outside the staged box (per-axis displacement >= 2, or a
@@ -284,12 +318,12 @@ __device__ __forceinline__ bool march_run(const A &bacc, const GlobalAcc<3> &gac
 // bounded; a warp that gives up raises FLAG_WAIT_TIMEOUT and leaves (the
 // others then give up at their next wait), and the producer waits (bounded)
 // for its last load per slot before the CTA ends.
-template <int BT, int TY>
-__global__ void __launch_bounds__(MarchShape<TY, BT>::Threads, MarchShape<TY, BT>::CtasPerSm)
+template <int BT, int TY, int RW>
+__global__ void __launch_bounds__(MarchShape<TY, BT, RW>::Threads, MarchShape<TY, BT, RW>::CtasPerSm)
     sl_lin_march_kernel(const __grid_constant__ CUtensorMap tm_phi, const __grid_constant__ CUtensorMap tm_vel,
                         Geom g, MarchGrid mg, const float *__restrict__ phi0, const float *__restrict__ vel, float dth0,
                         float dth1, float dth2, float *__restrict__ phi, int *flags) {
-  using S = MarchShape<TY, BT>;
+  using S = MarchShape<TY, BT, RW>;
   extern __shared__ __align__(1024) uint8_t smem[];
   float *const phis = reinterpret_cast<float *>(smem);
   float *const vels = phis + kRing * S::PlanePhi;
@@ -299,11 +333,11 @@ __global__ void __launch_bounds__(MarchShape<TY, BT>::Threads, MarchShape<TY, BT
   if (tid == 0)
     for (int s = 0; s < kRing; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], TY);
+      mbar_init(&empty[s], S::Warps);
     }
   __syncthreads();
 
-  if (warp == TY) {  // ---------------- producer ----------------
+  if (warp == S::Warps) {  // ---------------- producer ----------------
     if (lane == 0) {
       uint32_t used = 0, epar = 0, lastpar = 0;  // per slot: loaded once, next empty phase, phase of the last load
       bool err = false;
@@ -337,7 +371,7 @@ __global__ void __launch_bounds__(MarchShape<TY, BT>::Threads, MarchShape<TY, BT
     }
     return;
   }
-  // ---------------- consumers: warp = tile row ----------------
+  // ---------------- consumers: warp w = tile rows RW w .. RW w + RW - 1 ----------------
   const float dth[3] = {dth0, dth1, dth2};
   const float hdth[3] = {-0.5f * dth0, -0.5f * dth1, -0.5f * dth2};
   const GlobalAcc<3> gacc{phi0, vel, g.nx, g.ny, g.nz};
@@ -370,15 +404,21 @@ static bool lin_march_applicable(const Geom &g, const void *phi0, const void *ve
          ((uintptr_t)vel % 16) == 0;
 }
 
-// Tile rows of the z-march: 8 (three CTAs per SM) or 16 (two);
-// DCELL_LIN_TILE_ROWS overrides the default.
-static int lin_tile_rows() {
-  static int rows = 0;
-  if (!rows) {
-    rows = 8;
-    if (const char *e = getenv("DCELL_LIN_TILE_ROWS")) rows = atoi(e) == 16 ? 16 : 8;
+// Tile rows of the z-march: 8 for Euler, 16 for the midpoint backtrace (the
+// faster of the two at 256^3); DCELL_LIN_TILE_ROWS (8 or 16) overrides both.
+static int lin_tile_rows(bool mid) {
+  if (const char *e = getenv("DCELL_LIN_TILE_ROWS")) return atoi(e) == 16 ? 16 : 8;
+  return mid ? 16 : 8;
+}
+
+// Tile rows per consumer warp: 2; DCELL_LIN_ROWS_PER_WARP (1, 2 or 4)
+// overrides it.
+static int lin_rows_per_warp() {
+  if (const char *e = getenv("DCELL_LIN_ROWS_PER_WARP")) {
+    const int r = atoi(e);
+    return r == 1 || r == 4 ? r : 2;
   }
-  return rows;
+  return 2;
 }
 
 // Planes per z-segment (work unit) of the march: 16; DCELL_LIN_SEGMENT
@@ -393,13 +433,13 @@ static int lin_segment_planes() {
 }
 
 // The march with backtrace BT; false when no tensor maps could be made.
-template <int TY, int BT>
+template <int TY, int RW, int BT>
 static bool launch_march_bt(const Geom &g, const float *phi0, const float *vel, float dth0, float dth1, float dth2,
                             float *phi, int *flags, cudaStream_t st) {
-  using S = lin::MarchShape<TY, BT>;
+  using S = lin::MarchShape<TY, BT, RW>;
   static bool configured = false;
   if (!configured) {
-    if (cudaFuncSetAttribute(lin::sl_lin_march_kernel<BT, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::Smem) !=
+    if (cudaFuncSetAttribute(lin::sl_lin_march_kernel<BT, TY, RW>, cudaFuncAttributeMaxDynamicSharedMemorySize, S::Smem) !=
         cudaSuccess)
       return false;
     configured = true;
@@ -421,17 +461,27 @@ static bool launch_march_bt(const Geom &g, const float *phi0, const float *vel, 
   // rounds of at most one resident wave; the grid evens the units over them
   const int slots = S::CtasPerSm * sms, rounds = (mg.units + slots - 1) / slots;
   const int grid = (mg.units + rounds - 1) / rounds;
-  lin::sl_lin_march_kernel<BT, TY><<<grid, S::Threads, S::Smem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0, dth1,
-                                                                       dth2, phi, flags);
+  lin::sl_lin_march_kernel<BT, TY, RW><<<grid, S::Threads, S::Smem, st>>>(tm_phi, tm_vel, g, mg, phi0, vel, dth0,
+                                                                           dth1, dth2, phi, flags);
   return true;
 }
 
 // Launches the march; false when no tensor maps could be made.
-template <int TY>
+template <int TY, int RW>
 static bool launch_march(const Geom &g, const float *phi0, const float *vel, float dth0, float dth1, float dth2,
                          bool mid, float *phi, int *flags, cudaStream_t st) {
-  return mid ? launch_march_bt<TY, DCELL_MIDPOINT>(g, phi0, vel, dth0, dth1, dth2, phi, flags, st)
-             : launch_march_bt<TY, DCELL_EULER>(g, phi0, vel, dth0, dth1, dth2, phi, flags, st);
+  return mid ? launch_march_bt<TY, RW, DCELL_MIDPOINT>(g, phi0, vel, dth0, dth1, dth2, phi, flags, st)
+             : launch_march_bt<TY, RW, DCELL_EULER>(g, phi0, vel, dth0, dth1, dth2, phi, flags, st);
+}
+
+template <int TY>
+static bool launch_march_rows(const Geom &g, const float *phi0, const float *vel, float dth0, float dth1, float dth2,
+                              bool mid, float *phi, int *flags, cudaStream_t st) {
+  switch (lin_rows_per_warp()) {
+    case 1: return launch_march<TY, 1>(g, phi0, vel, dth0, dth1, dth2, mid, phi, flags, st);
+    case 4: return launch_march<TY, 4>(g, phi0, vel, dth0, dth1, dth2, mid, phi, flags, st);
+    default: return launch_march<TY, 2>(g, phi0, vel, dth0, dth1, dth2, mid, phi, flags, st);
+  }
 }
 
 int launch_sl_lin_f32(const Geom &g, const float *phi0, const float *vel, double dt, const int *band, long long npts,
@@ -439,8 +489,8 @@ int launch_sl_lin_f32(const Geom &g, const float *phi0, const float *vel, double
   const float dth0 = (float)(dt / g.hx), dth1 = (float)(dt / g.hy), dth2 = (float)(dt / g.hz);
   const bool mid = backtrace == DCELL_MIDPOINT;
   if (!band && !gather && lin_march_applicable(g, phi0, vel)) {
-    if (lin_tile_rows() == 16 ? launch_march<16>(g, phi0, vel, dth0, dth1, dth2, mid, phi, flags, st)
-                              : launch_march<8>(g, phi0, vel, dth0, dth1, dth2, mid, phi, flags, st))
+    if (lin_tile_rows(mid) == 16 ? launch_march_rows<16>(g, phi0, vel, dth0, dth1, dth2, mid, phi, flags, st)
+                              : launch_march_rows<8>(g, phi0, vel, dth0, dth1, dth2, mid, phi, flags, st))
       return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
     // no tensor maps (driver entry point unavailable): the gather form below
   }
