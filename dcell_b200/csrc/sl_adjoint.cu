@@ -11,17 +11,25 @@
 //   dL/dU_a = gbar[X] dI/dS_a(S) (-dt/h_a)                (departure point)
 //   dL/du  += dU/du^T dL/dU  through V(X) (Euler) or V(Xm) and, for the
 //            midpoint, through Xm's dependence on V(X).
-// Accumulation uses global atomics (RED), warp-aggregated: a warp's 32
-// lanes are consecutive arrival points of one grid row, and wherever the
-// departure (or midpoint) cells of its contributing lanes are one row of
-// consecutive cells, the contributions that land on one target -- the
-// stencils of neighbouring lanes overlap in x -- are summed with shuffles
-// first (a sliding window along the row), so each target of a stencil row
-// gets one atomic per warp instead of one per lane: 35 instead of 128 per
-// row of a tricubic stencil.  Other warps add per lane.  Results agree with
-// any ordering to rounding but are not bitwise reproducible.  Floors of the
-// departure cell are treated as constants (the interpolants are continuous,
-// the tricubic one C1).
+// Accumulation uses global atomics (RED), one per lane and target by
+// default.  The warp-aggregated form is built too (DCELL_ADJOINT_AGGREGATE =
+// phi, vel or all): a warp's 32 lanes are consecutive arrival points of one
+// grid row, and wherever the departure (or midpoint) cells of its
+// contributing lanes are one row of consecutive cells, the contributions
+// that land on one target -- the stencils of neighbouring lanes overlap in
+// x -- are summed with shuffles first (a sliding window along the row), so
+// each target of a stencil row gets one atomic per warp instead of one per
+// lane: 35 instead of 128 per row of a tricubic stencil.  Other warps add per
+// lane.  On the 128^3 differentiation workload the shuffles cost more than
+// the atomics they save (FP32 backward 13.9 ms per lane, 15.9 ms
+// aggregated), hence the default.  Results agree with any ordering to
+// rounding but are not bitwise reproducible.  Floors of the departure cell
+// are treated as constants (the interpolants are continuous, the tricubic
+// one C1).
+#include <stdlib.h>
+
+#include <string>
+
 #include "dcell_common.cuh"
 #include "dcell_kernels.h"
 #include "sl_device.cuh"
@@ -129,7 +137,9 @@ __device__ __forceinline__ T mac_component(const Geom &g, const T *__restrict__ 
   return val;
 }
 
-template <typename T, bool CUBIC>
+// AGG_PHI / AGG_VEL: warp-aggregate the dL/dphi0 / the velocity scatters
+// (per-lane atomics otherwise).
+template <typename T, bool CUBIC, bool AGG_PHI, bool AGG_VEL>
 __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__restrict__ phi0, const T *__restrict__ vel,
                                                          T dt, int backtrace, const T *__restrict__ gphi,
                                                          T *__restrict__ gphi0, T *__restrict__ gvel) {
@@ -202,7 +212,7 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
     // ---- transpose scatter into dL/dphi0
     constexpr int I0 = CUBIC ? 0 : 1, W = CUBIC ? 4 : 2;
     int cx0;
-    if (warp_row(active, c[1], c[2], c[0], lane, cx0)) {
+    if (AGG_PHI && warp_row(active, c[1], c[2], c[0], lane, cx0)) {
 #pragma unroll
       for (int k = I0; k < I0 + W; ++k)
 #pragma unroll
@@ -233,12 +243,17 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
       for (int a = 0; a < 3; ++a) {
         const int q0 = idx[a][0] / 3;  // corner (0, 0, 0), clamped
         const int bx = q0 % g.nx, byz = q0 / g.nx;
+        const int byz11 = idx[a][6] / 3 / g.nx;  // row of corner (0, 1, 1), clamped
         const int bxu = (idx[a][1] / 3) % g.nx;  // corner (1, 0, 0): bx + 1 clamped
         int bx0;
         // one row when the contributing lanes share the corner rows and their
-        // corners are consecutive, unclamped cells
+        // corners are consecutive, unclamped cells.  The rows of corners
+        // (0, 0, 0) and (0, 1, 1) fix clamp(by), clamp(by + 1), clamp(bz)
+        // and clamp(bz + 1), hence all four corner rows: at a y or z edge
+        // lanes whose midpoint cells differ there can share the first row
+        // alone.
         const bool interior = bxu == bx + 1;
-        if (__all_sync(kFull, interior || !on) && warp_row(active, byz, 0, bx, lane, bx0)) {
+        if (AGG_VEL && __all_sync(kFull, interior || !on) && warp_row(active, byz, byz11, bx, lane, bx0)) {
 #pragma unroll
           for (int jk = 0; jk < 4; ++jk) {
             const T v[2] = {on ? gU[a] * w8[a][2 * jk] : T(0), on ? gU[a] * w8[a][2 * jk + 1] : T(0)};
@@ -264,7 +279,7 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
     const int qn = (z * g.ny + y) * g.nx + x;
     const int up[3] = {x + 1 < g.nx ? 1 : 0, y + 1 < g.ny ? g.nx : 0, z + 1 < g.nz ? sz : 0};
     int x0;
-    if (warp_row(active, y, z, x, lane, x0)) {
+    if (AGG_VEL && warp_row(active, y, z, x, lane, x0)) {
       const T hv = on ? T(0.5) * gV0[0] : T(0);
       const T v[2] = {hv, hv};
       warp_row_scatter<2, T>(v, gvel + 3 * (long long)__shfl_sync(kFull, (z * g.ny + y) * g.nx, ref), x0, g.nx, 3,
@@ -287,30 +302,47 @@ __global__ void __launch_bounds__(256) sl_adjoint_kernel(Geom g, const T *__rest
 
 using namespace dcell;
 
+// Which scatters are warp-aggregated: DCELL_ADJOINT_AGGREGATE = none, phi,
+// vel or all (default none: per-lane atomics measured faster).
+static int adjoint_aggregate() {
+  const char *e = getenv("DCELL_ADJOINT_AGGREGATE");
+  if (!e) return 0;
+  const std::string v(e);
+  return v == "none" ? 0 : v == "phi" ? 1 : v == "vel" ? 2 : 3;
+}
+
+template <typename T, bool CUBIC>
+static void launch_adjoint_t(int agg, int blocks, const Geom &g, const T *phi0, const T *vel, T dt, int backtrace,
+                             const T *gphi, T *gphi0, T *gvel, cudaStream_t st) {
+  switch (agg) {
+    case 0: sl_adjoint_kernel<T, CUBIC, false, false><<<blocks, 256, 0, st>>>(g, phi0, vel, dt, backtrace, gphi, gphi0, gvel); break;
+    case 1: sl_adjoint_kernel<T, CUBIC, true, false><<<blocks, 256, 0, st>>>(g, phi0, vel, dt, backtrace, gphi, gphi0, gvel); break;
+    case 2: sl_adjoint_kernel<T, CUBIC, false, true><<<blocks, 256, 0, st>>>(g, phi0, vel, dt, backtrace, gphi, gphi0, gvel); break;
+    default: sl_adjoint_kernel<T, CUBIC, true, true><<<blocks, 256, 0, st>>>(g, phi0, vel, dt, backtrace, gphi, gphi0, gvel);
+  }
+}
+
 int launch_sl_adjoint(const Geom &g, int dtype, const void *phi0, const void *vel, double dt, int interp,
                       int backtrace, const void *gphi, void *gphi0, void *gvel, cudaStream_t st) {
   const long long n = (long long)g.nx * g.ny * g.nz;
   long long blocks = (n + 255) / 256;
   if (blocks > 148LL * 16) blocks = 148LL * 16;
   const bool cubic = interp != DCELL_LINEAR;
+  const int agg = adjoint_aggregate();
   if (dtype == DCELL_F64) {
     if (cubic)
-      sl_adjoint_kernel<double, true><<<(int)blocks, 256, 0, st>>>(g, (const double *)phi0, (const double *)vel, dt,
-                                                                   backtrace, (const double *)gphi, (double *)gphi0,
-                                                                   (double *)gvel);
+      launch_adjoint_t<double, true>(agg, (int)blocks, g, (const double *)phi0, (const double *)vel, dt, backtrace,
+                                     (const double *)gphi, (double *)gphi0, (double *)gvel, st);
     else
-      sl_adjoint_kernel<double, false><<<(int)blocks, 256, 0, st>>>(g, (const double *)phi0, (const double *)vel, dt,
-                                                                    backtrace, (const double *)gphi, (double *)gphi0,
-                                                                    (double *)gvel);
+      launch_adjoint_t<double, false>(agg, (int)blocks, g, (const double *)phi0, (const double *)vel, dt, backtrace,
+                                      (const double *)gphi, (double *)gphi0, (double *)gvel, st);
   } else {
     if (cubic)
-      sl_adjoint_kernel<float, true><<<(int)blocks, 256, 0, st>>>(g, (const float *)phi0, (const float *)vel,
-                                                                  (float)dt, backtrace, (const float *)gphi,
-                                                                  (float *)gphi0, (float *)gvel);
+      launch_adjoint_t<float, true>(agg, (int)blocks, g, (const float *)phi0, (const float *)vel, (float)dt, backtrace,
+                                    (const float *)gphi, (float *)gphi0, (float *)gvel, st);
     else
-      sl_adjoint_kernel<float, false><<<(int)blocks, 256, 0, st>>>(g, (const float *)phi0, (const float *)vel,
-                                                                   (float)dt, backtrace, (const float *)gphi,
-                                                                   (float *)gphi0, (float *)gvel);
+      launch_adjoint_t<float, false>(agg, (int)blocks, g, (const float *)phi0, (const float *)vel, (float)dt,
+                                     backtrace, (const float *)gphi, (float *)gphi0, (float *)gvel, st);
   }
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }

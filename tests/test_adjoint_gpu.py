@@ -15,10 +15,13 @@ def _dot(a, b):
     return float((a.double() * b.double()).sum())
 
 
+@pytest.mark.parametrize("aggregate", ["none", "all"])
 @pytest.mark.parametrize("interp", ["linear", "cubic_separable"])
 @pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
-def test_single_step_adjoint_identity(cuda, interp, backtrace):
-    """<SL'(phi0) dphi + SL_vel dvel, gbar> == <dphi, gphi0> + <dvel, gvel> (FP64, tiny steps)."""
+def test_single_step_adjoint_identity(cuda, interp, backtrace, aggregate, monkeypatch):
+    """<SL'(phi0) dphi + SL_vel dvel, gbar> == <dphi, gphi0> + <dvel, gvel> (FP64, tiny steps),
+    with per-lane and with warp-aggregated scatters."""
+    monkeypatch.setenv("DCELL_ADJOINT_AGGREGATE", aggregate)
     N = 24
     h = 1.0 / N
     torch.manual_seed(0)
@@ -36,6 +39,34 @@ def test_single_step_adjoint_identity(cuda, interp, backtrace):
         lhs = _dot((fp - fm) / (2 * eps), gbar)
         rhs = _dot(dphi, gphi0) + _dot(dvel, gvel)
         assert abs(lhs - rhs) <= 1e-6 * max(abs(lhs), 1.0), (lhs, rhs)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("interp", ["linear", "cubic_separable"])
+def test_aggregated_scatters_equal_per_lane_atomics(cuda, interp, dtype, monkeypatch):
+    """The warp-aggregated scatters (phi0, velocity, both) give the per-lane
+    atomics' gradients up to summation order, over a partial last warp
+    (nx = 45) and 3x the CFL number (departures off the warp's row)."""
+    nz, ny, nx = 20, 24, 45
+    h = 1.0 / 48
+    k, a, ph = fields.fourier_modes(4, 11)
+    for cfl in (0.3, 3.0):
+        phi0 = fields.sphere_sdf(48, center=(0.5, 0.5, 0.5), r=0.25, device=cuda)[:nz, :ny, :nx].contiguous().to(dtype)
+        vel = fields.fourier_velocity((48, 48, 48), np.full(4, 0.05), (k, a, ph), device=cuda)[:nz, :ny, :nx]
+        vel = vel.contiguous().to(dtype)
+        gbar = torch.randn(phi0.shape, generator=torch.Generator().manual_seed(3), dtype=torch.float64).to(cuda, dtype)
+        gbar[gbar.abs() < 0.3] = 0  # lanes that contribute nothing
+        dt = cfl * h / float(vel.abs().max())
+        res = {}
+        for mode in ("none", "phi", "vel", "all"):
+            monkeypatch.setenv("DCELL_ADJOINT_AGGREGATE", mode)
+            gphi0, gvel = torch.zeros_like(phi0), torch.zeros_like(vel)
+            sl_adjoint(phi0, vel, dt, h, gbar, gphi0, gvel, interp, "midpoint")
+            res[mode] = (gphi0.double(), gvel.double())
+        tol = 1e-12 if dtype == torch.float64 else 1e-5
+        for mode in ("phi", "vel", "all"):
+            for got, ref in zip(res[mode], res["none"]):
+                assert float((got - ref).abs().max()) <= tol * float(ref.abs().max()), (mode, cfl)
 
 
 def _c5(N, nsteps, dtype, cuda):
