@@ -87,6 +87,23 @@ def test_fp32_staged_form_equals_gather_form(cuda, interp, backtrace, shape, cfl
         assert torch.equal(staged, banded)
 
 
+@pytest.mark.parametrize("rows,per_warp", [(8, 1), (8, 2), (16, 2), (16, 4)])
+@pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
+def test_linear_march_shapes_equal_gather_form(cuda, backtrace, rows, per_warp, monkeypatch):
+    """Every tile shape of the FP32 trilinear z-march (tile rows, rows per
+    consumer warp) gives the gather form's bits: partial tiles in x and y,
+    and departures beyond the staged box (CFL 3)."""
+    monkeypatch.setenv("DCELL_LIN_TILE_ROWS", str(rows))
+    monkeypatch.setenv("DCELL_LIN_ROWS_PER_WARP", str(per_warp))
+    for shape, cfl in (((40, 24, 64), 0.9), ((21, 37, 44), 3.0)):
+        phi, vel = _random_case(shape, cfl, cuda)
+        staged = L.sl_step(phi, vel, 1.0, 1.0, interp="linear", backtrace=backtrace)
+        gathered = L.sl_step(phi, vel, 1.0, 1.0, interp="linear_gather", backtrace=backtrace,
+                             out=torch.full_like(phi, float("nan")))
+        torch.cuda.synchronize()
+        assert torch.equal(staged, gathered), (shape, cfl)
+
+
 @pytest.mark.parametrize("backtrace", ["euler", "midpoint"])
 def test_split_state_plane_ranges_equal_the_full_step(cuda, backtrace):
     """dcell_sl_step_tc_split_planes over brick-aligned plane ranges (the
