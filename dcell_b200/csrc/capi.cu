@@ -657,23 +657,35 @@ DCELL_API int dcell_session_destroy(dcell_session *s) {
 // in them); otherwise it leaves its slab, and once all inputs are present
 // the whole grid is stepped again and copied down (identical results either
 // way: the same kernel on the same inputs).
-static int ls_advect_tc_pipelined(dcell_session *s, const dcell_geom *g, const double *phi0, const double *vel,
-                                  double dt, int backtrace, double *phi) {
-  constexpr int kHalo = 6, kSlabs = 8;
-  const dcell::Geom G = dcell::to_geom(g);
-  const long long plane = (long long)G.nx * G.ny, n = plane * G.nz;
-  cudaStream_t st = s->stream;
+// Slabs and halo of the z-slab pipelines: a slab's step starts once the
+// planes up to its top + kPipeHalo are on the device, and runs only if max
+// |w| dt / h_z over those planes is at most kPipeHalo - 3.
+constexpr int kPipeHalo = 6, kPipeSlabs = 8;
+
+// the session's two copy streams and kPipeSlabs events per direction
+static int ensure_copy_streams(dcell_session *s) {
   if (!s->h2d) {
     DCELL_CUDA_CHECK(cudaStreamCreateWithFlags(&s->h2d, cudaStreamNonBlocking));
     DCELL_CUDA_CHECK(cudaStreamCreateWithFlags(&s->d2h, cudaStreamNonBlocking));
   }
-  while ((int)s->ev_in.size() < kSlabs) {
+  while ((int)s->ev_in.size() < kPipeSlabs) {
     cudaEvent_t a, b;
     DCELL_CUDA_CHECK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
     DCELL_CUDA_CHECK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
     s->ev_in.push_back(a);
     s->ev_out.push_back(b);
   }
+  return DCELL_OK;
+}
+
+static int ls_advect_tc_pipelined(dcell_session *s, const dcell_geom *g, const double *phi0, const double *vel,
+                                  double dt, int backtrace, double *phi) {
+  constexpr int kHalo = kPipeHalo, kSlabs = kPipeSlabs;
+  const dcell::Geom G = dcell::to_geom(g);
+  const long long plane = (long long)G.nx * G.ny, n = plane * G.nz;
+  cudaStream_t st = s->stream;
+  int rc;
+  if ((rc = ensure_copy_streams(s))) return rc;
   ENSURE(s->phi0_64, n * sizeof(double));
   ENSURE(s->vel_64, n * 3 * sizeof(double));
   ENSURE(s->phi_64, n * sizeof(double));
@@ -686,7 +698,6 @@ static int ls_advect_tc_pipelined(dcell_session *s, const dcell_geom *g, const d
   double *p64 = (double *)s->phi0_64.p, *v64 = (double *)s->vel_64.p, *o64 = (double *)s->phi_64.p;
   float *p32 = (float *)s->phi0_32.p, *v32 = (float *)s->vel_32.p, *o32 = (float *)s->phi_32.p;
   uint32_t *w = (uint32_t *)s->split.p;
-  int rc;
   // every stream starts after the work this session queued before
   cudaEvent_t start = s->ev_out[kSlabs - 1];
   DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
@@ -720,7 +731,7 @@ static int ls_advect_tc_pipelined(dcell_session *s, const dcell_geom *g, const d
     slab.nbz = b1 - b0;
     slab.gate_maxw = gates + k;
     slab.gate_limit = (float)(kHalo - 3);
-    if ((rc = launch_sl_tc_slab(G, w, v32, dt, backtrace, o32, dflags, st, slab))) return rc;
+    if ((rc = launch_sl_tc_slab(G, w, v32, dt, backtrace, o32, nullptr, dflags, st, slab))) return rc;
     const long long oz = z0 * plane, mz = (z1 - z0) * plane;
     if ((rc = launch_convert(o32 + oz, DCELL_F32, o64 + oz, DCELL_F64, mz, st))) return rc;
     DCELL_CUDA_CHECK(cudaEventRecord(s->ev_out[k], st));
@@ -1379,27 +1390,90 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
   int *dflags = (int *)r.small.p, *dcount = dflags + 1;
   double *dmax = (double *)((char *)r.small.p + 64);
   DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
-  // the step's velocity (the only per-step upload)
   const size_t ves = r.precision == DCELL_F32 ? sizeof(float) : sizeof(double);
+  const size_t ies = vel_dtype == DCELL_F32 ? sizeof(float) : sizeof(double);
   ENSURE(r.vel, n * dof * ves);
-  if (vel_dtype == r.precision) {
-    DCELL_CUDA_CHECK(cudaMemcpyAsync(r.vel.p, vel, n * dof * ves, cudaMemcpyHostToDevice, st));
+  if (vel_dtype != r.precision) ENSURE(r.vel64, n * dof * ies);
+  const int cur = r.cur, nxt = 1 - cur;
+  const bool use_band = !dense && r.nband > 0;
+  const bool dense_tc = r.precision == DCELL_F32 && interp == DCELL_CUBIC_TC && !use_band && G.nz > 1;
+  // The dense tensor-core step on deep grids overlaps the velocity upload:
+  // plane chunks go up on the copy stream and each z-slab is stepped once
+  // the planes it can read are present (the gate of ls_advect_tc_pipelined:
+  // a slab whose departures could reach planes not yet present is left, and
+  // the whole grid is stepped again below).
+  const bool pipelined = dense_tc && G.nz >= 4 * tc_slab_planes() &&
+                         tc_brick_applicable(G, (const void *)256, (const void *)256);
+  bool redo_possible = false;
+  if (pipelined) {
+    if ((rc = ensure_copy_streams(s))) return rc;
+    ENSURE(r.split[0], n * sizeof(uint32_t));
+    ENSURE(r.split[1], n * sizeof(uint32_t));
+    ENSURE(s->gates, kPipeSlabs * sizeof(int));
+    int *gates = (int *)s->gates.p;
+    if (!r.split_ok && (rc = launch_split_bf16((const float *)r.phi[cur].p, (uint32_t *)r.split[cur].p, n, st)))
+      return rc;
+    DCELL_CUDA_CHECK(cudaMemsetAsync(gates, 0, kPipeSlabs * sizeof(int), st));
+    cudaEvent_t start = s->ev_out[kPipeSlabs - 1];
+    DCELL_CUDA_CHECK(cudaEventRecord(start, st));  // the upload starts after this session's earlier work
+    DCELL_CUDA_CHECK(cudaStreamWaitEvent(s->h2d, start, 0));
+    const long long plane = (long long)G.nx * G.ny;
+    const int BZ = tc_slab_planes(), nbz = (G.nz + BZ - 1) / BZ, per = (nbz + kPipeSlabs - 1) / kPipeSlabs;
+    float *v32 = (float *)r.vel.p;
+    int have = 0;
+    for (int k = 0; k < kPipeSlabs; ++k) {
+      const int b0 = k * per, b1 = b0 + per < nbz ? b0 + per : nbz;
+      if (b0 >= b1) break;
+      const int z1 = b1 * BZ < G.nz ? b1 * BZ : G.nz;
+      const int need = z1 + kPipeHalo < G.nz ? z1 + kPipeHalo : G.nz;
+      if (need > have) {  // the next chunk of velocity planes
+        const long long o = have * plane * dof, m = (need - have) * plane * dof;
+        if (vel_dtype == r.precision) {
+          DCELL_CUDA_CHECK(cudaMemcpyAsync(v32 + o, (const float *)vel + o, m * sizeof(float), cudaMemcpyHostToDevice,
+                                           s->h2d));
+        } else {
+          double *v64 = (double *)r.vel64.p;
+          DCELL_CUDA_CHECK(cudaMemcpyAsync(v64 + o, (const double *)vel + o, m * sizeof(double),
+                                           cudaMemcpyHostToDevice, s->h2d));
+          if ((rc = launch_convert(v64 + o, DCELL_F64, v32 + o, DCELL_F32, m, s->h2d))) return rc;
+        }
+        have = need;
+      }
+      DCELL_CUDA_CHECK(cudaEventRecord(s->ev_in[k], s->h2d));
+      DCELL_CUDA_CHECK(cudaStreamWaitEvent(st, s->ev_in[k], 0));
+      if ((rc = launch_max_abs_component(v32, have * plane, 3, 2, gates + k, st))) return rc;
+      TcSlab slab;
+      slab.bz0 = b0;
+      slab.nbz = b1 - b0;
+      slab.gate_maxw = gates + k;
+      slab.gate_limit = (float)(kPipeHalo - 3);
+      if ((rc = launch_sl_tc_slab(G, (const uint32_t *)r.split[cur].p, v32, dt, backtrace, (float *)r.phi[nxt].p,
+                                  (uint32_t *)r.split[nxt].p, dflags, st, slab)))
+        return rc;
+    }
+    // the last slab waited for the last chunk: every velocity plane is present on st from here
+    redo_possible = true;
+    r.split_ok = true;
   } else {
-    const size_t ies = vel_dtype == DCELL_F32 ? sizeof(float) : sizeof(double);
-    ENSURE(r.vel64, n * dof * ies);
-    DCELL_CUDA_CHECK(cudaMemcpyAsync(r.vel64.p, vel, n * dof * ies, cudaMemcpyHostToDevice, st));
-    if ((rc = launch_convert(r.vel64.p, vel_dtype, r.vel.p, r.precision, n * dof, st))) return rc;
+    // the step's velocity (the only per-step upload)
+    if (vel_dtype == r.precision) {
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(r.vel.p, vel, n * dof * ves, cudaMemcpyHostToDevice, st));
+    } else {
+      DCELL_CUDA_CHECK(cudaMemcpyAsync(r.vel64.p, vel, n * dof * ies, cudaMemcpyHostToDevice, st));
+      if ((rc = launch_convert(r.vel64.p, vel_dtype, r.vel.p, r.precision, n * dof, st))) return rc;
+    }
   }
   // LevelSetCFLIncrement (Advect.c:54-66) needs max |V| at the current
   // nodes; the reference takes it after the advection, from the nodes of the
-  // level set before this step -- the same nodes, queued here
+  // level set before this step -- the same nodes, queued here (before the
+  // node pass of the new level set overwrites them)
   if ((rc = dcell_max_velocity(g, r.precision, r.vel.p, (const dcell_irregular_node *)r.nodes.p, dcount, r.ncap, dmax,
                                st)))
     return rc;
   // GridCopy (phi0 <- phi) and the SL step: phi[nxt] from phi[cur]
-  const int cur = r.cur, nxt = 1 - cur;
-  const bool use_band = !dense && r.nband > 0;
-  if (r.precision == DCELL_F32 && interp == DCELL_CUBIC_TC && !use_band && G.nz > 1) {
+  if (pipelined) {
+    rc = DCELL_OK;  // stepped above
+  } else if (dense_tc) {
     ENSURE(r.split[0], n * sizeof(uint32_t));
     ENSURE(r.split[1], n * sizeof(uint32_t));
     if (!r.split_ok && (rc = launch_split_bf16((const float *)r.phi[cur].p, (uint32_t *)r.split[cur].p, n, st)))
@@ -1423,6 +1497,18 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
   DCELL_CUDA_CHECK(cudaMemcpyAsync(&maxvel, dmax, sizeof(double), cudaMemcpyDeviceToHost, st));
   DCELL_CUDA_CHECK(cudaMemcpyAsync(&hf, dflags, sizeof(int), cudaMemcpyDeviceToHost, st));
   DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  if (redo_possible && (hf & dcell::FLAG_PIPELINE_REDO)) {
+    // a slab was left: step the whole grid with every plane present (the
+    // same kernel on the same inputs), then the node pass again
+    DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
+    if ((rc = launch_sl_tc_split(G, (const uint32_t *)r.split[cur].p, (const float *)r.vel.p, dt, nullptr, n,
+                                 backtrace, (float *)r.phi[nxt].p, (uint32_t *)r.split[nxt].p, dflags, st)))
+      return rc;
+    if ((rc = resident_nodes(s))) return rc;
+    DCELL_CUDA_CHECK(cudaMemcpyAsync(&hf, dflags, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  }
+  hf &= ~dcell::FLAG_PIPELINE_REDO;
   if ((rc = session_flags_status(s, hf & ~DCELL_FLAG_DEPARTURE_CLAMPED))) return rc;
   loop->maxVel = maxvel;
   loop->CFLcount += dt * maxvel / g->h[0];

@@ -44,8 +44,10 @@ struct TcSlab {
 };
 int tc_slab_planes();
 bool tc_brick_applicable(const dcell::Geom &g, const void *phi0s, const void *vel);
+// z bricks [slab.bz0, slab.bz0 + slab.nbz) of the dense split-state step,
+// gated (see TcSlab); phis (nullable) receives the stepped split words
 int launch_sl_tc_slab(const dcell::Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace,
-                      float *phi, int *flags, cudaStream_t st, const TcSlab &slab);
+                      float *phi, uint32_t *phis, int *flags, cudaStream_t st, const TcSlab &slab);
 // z bricks [bz0, bz0 + nbz) of the dense split-state step (tc_slab_planes()
 // planes each), no gate
 int launch_sl_tc_split_planes(const dcell::Geom &g, const uint32_t *phi0s, const float *vel, double dt,

@@ -1579,8 +1579,8 @@ int launch_sl_tc_brick(const Geom &g, const uint32_t *phi0s, const float *vel, d
 int tc_slab_planes() { return tc::BrickShape<2>::BZ; }
 
 int launch_sl_tc_slab(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
-                      int *flags, cudaStream_t st, const TcSlab &slab) {
-  return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, nullptr, flags, st, &slab);
+                      uint32_t *phis, int *flags, cudaStream_t st, const TcSlab &slab) {
+  return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st, &slab);
 }
 
 int launch_sl_tc_split_planes(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace,

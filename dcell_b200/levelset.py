@@ -459,12 +459,26 @@ class ResidentLevelSet:
             ctypes.byref(self.loop)))
         return self.loop
 
-    def get(self):
-        """(phi (FP64 host array), band (nb, 3) int32)."""
-        phi = np.empty(self.shape, dtype=np.float64)
+    def get(self, out=None):
+        """(phi (FP64 host array), band (nb, 3) int32).  `out`: a C-contiguous
+        FP64 host array (numpy, or a CPU tensor, pinned for the full copy
+        rate) of the grid's shape that receives phi; a new array otherwise."""
+        if out is None:
+            phi = np.empty(self.shape, dtype=np.float64)
+            ptr = phi.ctypes.data_as(ctypes.c_void_p)
+        else:
+            phi = out
+            if isinstance(out, torch.Tensor):
+                if out.device.type != "cpu" or out.dtype != torch.float64 or not out.is_contiguous() or \
+                        tuple(out.shape) != self.shape:
+                    raise ValueError("out must be a contiguous CPU float64 tensor of the grid's shape")
+                ptr = ctypes.c_void_p(out.data_ptr())
+            else:
+                if out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"] or tuple(out.shape) != self.shape:
+                    raise ValueError("out must be a C-contiguous float64 array of the grid's shape")
+                ptr = out.ctypes.data_as(ctypes.c_void_p)
         n = ctypes.c_int()
-        check(lib().dcell_ls_resident_get(self.s, ctypes.byref(self.g), phi.ctypes.data_as(ctypes.c_void_p), None, 0,
-                                          ctypes.byref(n)))
+        check(lib().dcell_ls_resident_get(self.s, ctypes.byref(self.g), ptr, None, 0, ctypes.byref(n)))
         band = np.empty((max(n.value, 1), 3), dtype=np.int32)
         check(lib().dcell_ls_resident_get(self.s, ctypes.byref(self.g), None, band.ctypes.data_as(ctypes.c_void_p),
                                           n.value, ctypes.byref(n)))

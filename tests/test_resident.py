@@ -64,16 +64,21 @@ def test_resident_loop_equals_the_device_api_loop(cuda):
 
 
 @pytest.mark.gpu
-def test_resident_tc_loop_equals_split_state_steps(cuda):
-    """FP32, dense, split-BF16 tensor-core steps with FP32 host velocity: the
-    resident loop's phi after 5 steps equals 5 dcell_sl_step_tc_split steps
-    (the split state carried between them) bit for bit."""
+@pytest.mark.parametrize("vel_dtype", ["f32", "f64"])
+@pytest.mark.parametrize("cfl", [0.5, 4.0])
+def test_resident_tc_loop_equals_split_state_steps(cuda, cfl, vel_dtype):
+    """FP32, dense, split-BF16 tensor-core steps with FP32 or FP64 host
+    velocity: the resident loop's phi after 5 steps equals 5
+    dcell_sl_step_tc_split steps (the split state carried between them) bit
+    for bit.  At 64^3 the loop steps z-slabs while the velocity planes go up;
+    at 4x the CFL number the slabs' gate leaves them and the whole grid is
+    stepped again once every plane is present."""
     N = 64
     h, phi, vel, band = _case(N, cuda)
-    dt = 0.5 * h
+    dt = cfl * h
     r = L.ResidentLevelSet(phi.cpu().numpy(), h, band=band.cpu().numpy(), precision="f32", CFLthres=1e9)
     v32 = vel.float().contiguous()
-    vhost = v32.cpu().numpy()
+    vhost = v32.cpu().numpy() if vel_dtype == "f32" else v32.double().cpu().numpy()
     spl = L.split_bf16(phi.float().contiguous())
     out = None
     for s in range(5):
