@@ -477,7 +477,9 @@ DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const do
  * dcell_ls_resident_get downloads phi (FP64) and the band where the host
  * needs them (output, or a CPU fast marching instead of the device one).
  * precision: the arithmetic (DCELL_F32 with DCELL_CUBIC_TC on a dense 3D grid
- * carries the split state between steps, as dcell_sl_step_tc_split).  One
+ * carries the split state between steps, as dcell_sl_step_tc_split; on grids
+ * of at least 32 planes the velocity then goes up in plane chunks while
+ * z-slabs already step, with the bits of the unpipelined step).  One
  * resident level set per session; dcell_ls_resident_set replaces it. */
 typedef struct dcell_ls_loop {
   double CFLcount, CFLthres, maxVel, bandWidth; /* struct _LevelSet's fields (LevelSetMethod.h:10-26) */
