@@ -659,7 +659,9 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
       const bool xy_valid = x0 + lx < g.nx && y0 + ly < g.ny;
       const int zr = z0 + P * (j & 3);
       const int p0 = (min(zr, g.nz - 1) * g.ny + y) * g.nx + x;
-      const bool ok = mbar_wait_sleep(dfull, (uint32_t)j & 1u);
+      // polled, not suspend-hinted: the warp resumes as the MMAs complete
+      // (0.3978 against 0.3995 ms per 256^3 step, alternating runs)
+      const bool ok = mbar_wait(dfull, (uint32_t)j & 1u);
       if (__any_sync(0xffffffffu, !ok)) { err = true; break; }
       fence_after();
 #pragma unroll
