@@ -441,6 +441,52 @@ def e2e_resident_rate(phi, vel, h, dt, K, torch):
                               "one reinitialisation; host clock"}
 
 
+def c4_rates(torch, dev, steps=20, sample_cells=48):
+    """C4 (512 cells of 32..96 points per axis, ellipsoids in their own
+    Fourier velocities, midpoint tricubic steps): the GPU's TMA-staged
+    split-state bricks of all cells, one launch per step (CUDA events, 20
+    steps), against the FP64 oracle restatement of the same tricubic/midpoint
+    step on a sample of the cells with one host thread per core (the
+    reference advects its cells rank by rank; its SL has no tricubic form)."""
+    import numpy as np
+
+    import oracle
+    from dcell_b200.batch import CellBatch, c4_workload
+    phis, vels, hs, dt = c4_workload(ncells=512, device=dev)
+    bp = CellBatch(phis, vels, hs, dt, device=dev, padded=True)
+    sp = bp.split()
+    x, y, p = sp.clone(), torch.empty_like(sp), torch.empty_like(bp.phi)
+    bp.step_tc_split_tma(x, p, y)  # warm-up (tensor maps of both buffers)
+    bp.step_tc_split_tma(y, p, x)
+    x.copy_(sp)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        bp.step_tc_split_tma(x, p, y)
+        x, y = y, x
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    idx = np.linspace(0, len(phis) - 1, sample_cells).astype(int)
+    cells = [(phis[i].double().cpu().numpy(), vels[i].double().cpu().numpy(), hs[i]) for i in idx]
+    threads = os.cpu_count() or 1
+    from concurrent.futures import ThreadPoolExecutor
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:  # ctypes releases the GIL
+        list(ex.map(lambda c: oracle.sl_step(c[0], c[1], dt, c[2], interp="cubic", backtrace="midpoint"), cells))
+    t = time.perf_counter() - t0
+    npts = int(sum(c[0].size for c in cells))
+    gpu = bp.npoints * steps / (ms / 1e3)
+    cpu = npts / t
+    return {"cells": len(phis), "points_per_step": int(bp.npoints), "steps": steps,
+            "gpu": {"ms": ms, "updates_per_s": gpu, "how": "dcell_batch_sl_step_tc_split_tma, CUDA events"},
+            "cpu_baseline": {"value": cpu, "unit": "updates/s", "cores": threads, "kind": "port",
+                             "sample": f"{sample_cells} of the 512 cells ({npts} points), one step each, one host "
+                                       f"thread per core, {t:.1f} s"},
+            "gpu_over_cpu": gpu / cpu}
+
+
 def error_check(L, torch, phi, vel, h, dt):
     a = L.sl_step_tc_split(L.split_bf16(phi), vel, dt_at(0, dt), h, backtrace="midpoint")[0].double()
     ref = L.sl_step(phi.double(), vel.double(), dt_at(0, dt), h, interp="cubic_plain", backtrace="midpoint")
@@ -620,6 +666,8 @@ def main():
                 ref_lin = reference_linear_rate(phi, vel, h, dt, nplanes=24)
                 if ref_lin:
                     line["cpu_baseline"]["reference_linear_advectsl_updates_per_s"] = ref_lin
+            if world == 1:
+                line["c4"] = c4_rates(torch, dev)
             # narrow-band reinitialisation of the same sphere (cell units), GPU vs the reference's heap FMM
             rphi, rband, raw, count = reinit_case(torch, args.size, dev)
             ms64, y64, b64 = timed_reinit(torch, rphi, raw, count, torch.float64)
