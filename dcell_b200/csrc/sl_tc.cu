@@ -475,6 +475,7 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
                        float *__restrict__ phi, uint32_t *__restrict__ phis, int *flags, const int *gate_maxw,
                        float gate_limit) {
   using S = BrickShape<P>;
+  static_assert(P == 2, "the step loop holds two points' coefficients per thread");
   // z-slab launches: run only if the staged planes bound every departure
   // (max |w| dt / h_z over them within gate_limit); otherwise leave the slab
   // to a full-grid step once all planes are present
@@ -611,23 +612,15 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
       }
     };
 
-    int x0 = 0, y0 = 0, z0 = 0;
-    float f[P][3];
-    int soff[P];
-    bool boxed = true;
-    if (nsteps > 0) {
-      err = !open_brick(0, x0, y0, z0);
-      if (__any_sync(0xffffffffu, err)) err = true;
-      else boxed = depart(0, x0, y0, z0, f, soff);
-    }
-    for (int j = 0; j < nsteps && !err; ++j) {
-      const int k = j >> 2;
-      // a: A rows of the P points into their stages, then this warp's arrival
-      bool stacked = boxed;
+    // A rows of step s (points of brick (bx, by, bz), departures ff / so)
+    // into their stages; the warp's 4 x 4 x (P+3) union is gathered once
+    // when its stencils are stacked plane over plane (the usual case)
+    auto stage_step = [&](int s, int bx, int by, int bz, bool bxd, int so[P], float ff[P][3]) {
+      bool stacked = bxd;
 #pragma unroll
-      for (int p = 1; p < P; ++p) stacked = stacked && soff[p] == soff[0] + p * S::PX * S::PY;
+      for (int p = 1; p < P; ++p) stacked = stacked && so[p] == so[0] + p * S::PX * S::PY;
       if (__all_sync(0xffffffffu, stacked)) {
-        const uint32_t *q = reinterpret_cast<const uint32_t *>(k & 1 ? buf1 : buf0) + soff[0];
+        const uint32_t *q = reinterpret_cast<const uint32_t *>((s >> 2) & 1 ? buf1 : buf0) + so[0];
         uint32_t v[16 * (P + 3)];
 #pragma unroll
         for (int e = 0; e < 16 * (P + 3); ++e) v[e] = q[((e >> 4) * S::PY + ((e >> 2) & 3)) * S::PX + (e & 3)];
@@ -638,70 +631,94 @@ __global__ void __launch_bounds__(kBrickThreads, BrickShape<P>::CtasPerSm)
             tmem_st16(c.tmem + c.lane_off + 128 * p + 16 * q16, v + 16 * (p + q16));
       } else {
 #pragma unroll
-        for (int p = 0; p < P; ++p) stage_rows(j, x0, y0, z0, boxed, soff[p], f[p], p);
+        for (int p = 0; p < P; ++p) stage_rows(s, bx, by, bz, bxd, so[p], ff[p], p);
       }
+    };
+
+    // Step j's points (brick origin x0.., departures f / soff) and step
+    // j+1's (x1.., f1 / soff1): step j+1's A rows go in as soon as step j's
+    // MMAs are done, so its MMAs run while step j is evaluated and step
+    // j+2's departures are computed.
+    int x0 = 0, y0 = 0, z0 = 0, x1 = 0, y1 = 0, z1 = 0;
+    float f[P][3], f1[P][3];
+    int soff[P], soff1[P];
+    bool boxed = true, boxed1 = true;
+    if (nsteps > 0) {
+      err = !open_brick(0, x0, y0, z0);
+      if (__any_sync(0xffffffffu, err)) err = true;
+      else boxed = depart(0, x0, y0, z0, f, soff);
+    }
+    if (nsteps > 0 && !err) {
+      stage_step(0, x0, y0, z0, boxed, soff, f);
       tmem_wait_st();
       fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(afull);
-      // b: next step's departures while the tensor core works
-      int nx0 = x0, ny0 = y0, nz0 = z0;
-      float fn[P][3];
-      int soffn[P];
-      bool boxedn = true;
-      if (j + 1 < nsteps) {
-        if (((j + 1) & 3) == 0) err = !open_brick(k + 1, nx0, ny0, nz0);
-        if (__any_sync(0xffffffffu, err)) err = true;
-        else boxedn = depart(j + 1, nx0, ny0, nz0, fn, soffn);
-      }
-      // c: coefficients -> values, two points at a time, two z-slices per TMEM load round
+      x1 = x0; y1 = y0; z1 = z0;
+      if (nsteps > 1) boxed1 = depart(1, x1, y1, z1, f1, soff1);  // step 1 lies in brick 0
+    }
+    for (int j = 0; j < nsteps && !err; ++j) {
       const int x = min(x0 + lx, g.nx - 1), y = min(y0 + ly, g.ny - 1);
       const bool xy_valid = x0 + lx < g.nx && y0 + ly < g.ny;
       const int zr = z0 + P * (j & 3);
       const int p0 = (min(zr, g.nz - 1) * g.ny + y) * g.nx + x;
       // polled, not suspend-hinted: the warp resumes as the MMAs complete
-      // (0.3978 against 0.3995 ms per 256^3 step, alternating runs)
       const bool ok = mbar_wait(dfull, (uint32_t)j & 1u);
       if (__any_sync(0xffffffffu, !ok)) { err = true; break; }
       fence_after();
-#pragma unroll
-      for (int pp = 0; pp < P; pp += 2) {
-        // both points' 64 coefficients in one TMEM load round
-        float ca[64], cb[64];
-        tmem_ld32f(c.tmem + c.lane_off + 128 * pp + 96, ca + 32);
-        tmem_ld32f(c.tmem + c.lane_off + 128 * (pp + 1) + 96, cb + 32);
-        tmem_wait_ld_tied(ca + 32, cb + 32);
-        tmem_ld32f(c.tmem + c.lane_off + 128 * pp + 64, ca);
-        tmem_ld32f(c.tmem + c.lane_off + 128 * (pp + 1) + 64, cb);
-        float va = 0.f, vb = 0.f;  // horner3 order: slices k = 3 .. 0
-#pragma unroll
-        for (int kz = 3; kz >= 2; --kz) {
-          va = fmaf(va, f[pp][2], horner_slice(ca + 16 * kz, f[pp]));
-          vb = fmaf(vb, f[pp + 1][2], horner_slice(cb + 16 * kz, f[pp + 1]));
-        }
-        tmem_wait_ld_tied(ca, cb);
-#pragma unroll
-        for (int kz = 1; kz >= 0; --kz) {
-          va = fmaf(va, f[pp][2], horner_slice(ca + 16 * kz, f[pp]));
-          vb = fmaf(vb, f[pp + 1][2], horner_slice(cb + 16 * kz, f[pp + 1]));
-        }
-        if (xy_valid && zr + pp < g.nz) {
-          phi[p0 + pp * plane] = va;
-          if (SPLIT) phis[p0 + pp * plane] = pack_split(va);
-        }
-        if (xy_valid && zr + pp + 1 < g.nz) {
-          phi[p0 + (pp + 1) * plane] = vb;
-          if (SPLIT) phis[p0 + (pp + 1) * plane] = pack_split(vb);
-        }
+      // step j's MMAs have read their A rows: step j+1's replace them
+      const bool more = j + 1 < nsteps;
+      if (more) stage_step(j + 1, x1, y1, z1, boxed1, soff1, f1);
+      // step j's coefficients into registers before step j+1's MMAs overwrite them
+      float ca[64], cb[64];
+      tmem_ld32f(c.tmem + c.lane_off + 96, ca + 32);
+      tmem_ld32f(c.tmem + c.lane_off + 128 + 96, cb + 32);
+      tmem_ld32f(c.tmem + c.lane_off + 64, ca);
+      tmem_ld32f(c.tmem + c.lane_off + 128 + 64, cb);
+      tmem_wait_ld_tied(ca + 32, cb + 32);
+      tmem_wait_ld_tied(ca, cb);  // (the first wait completed all four loads; this one ties the rest)
+      if (more) {
+        tmem_wait_st();
+        fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(afull);
       }
-      fence_before();
-      x0 = nx0; y0 = ny0; z0 = nz0;
+      // step j's values (horner3 order: slices k = 3 .. 0)
+      float va = 0.f, vb = 0.f;
+#pragma unroll
+      for (int kz = 3; kz >= 0; --kz) {
+        va = fmaf(va, f[0][2], horner_slice(ca + 16 * kz, f[0]));
+        vb = fmaf(vb, f[1][2], horner_slice(cb + 16 * kz, f[1]));
+      }
+      if (xy_valid && zr < g.nz) {
+        phi[p0] = va;
+        if (SPLIT) phis[p0] = pack_split(va);
+      }
+      if (xy_valid && zr + 1 < g.nz) {
+        phi[p0 + plane] = vb;
+        if (SPLIT) phis[p0 + plane] = pack_split(vb);
+      }
+      // step j+2's departures while step j+1's MMAs run
+      int x2 = x1, y2 = y1, z2 = z1;
+      float f2[P][3];
+      int soff2[P];
+      bool boxed2 = true;
+      if (j + 2 < nsteps) {
+        if (((j + 2) & 3) == 0) err = !open_brick((j + 2) >> 2, x2, y2, z2);
+        if (__any_sync(0xffffffffu, err)) err = true;
+        else boxed2 = depart(j + 2, x2, y2, z2, f2, soff2);
+      }
+      x0 = x1; y0 = y1; z0 = z1;
+      x1 = x2; y1 = y2; z1 = z2;
 #pragma unroll
       for (int p = 0; p < P; ++p) {
-        f[p][0] = fn[p][0]; f[p][1] = fn[p][1]; f[p][2] = fn[p][2];
-        soff[p] = soffn[p];
+        f[p][0] = f1[p][0]; f[p][1] = f1[p][1]; f[p][2] = f1[p][2];
+        soff[p] = soff1[p];
+        f1[p][0] = f2[p][0]; f1[p][1] = f2[p][1]; f1[p][2] = f2[p][2];
+        soff1[p] = soff2[p];
       }
-      boxed = boxedn;
+      boxed = boxed1;
+      boxed1 = boxed2;
     }
     if (err) raise_flag(flags, FLAG_WAIT_TIMEOUT);
   }
@@ -1562,19 +1579,8 @@ static int launch_brick(const Geom &g, const uint32_t *phi0s, const float *vel, 
   return cudaGetLastError() == cudaSuccess ? DCELL_OK : DCELL_ERR_CUDA;
 }
 
-// Points per thread of the brick kernel: 2 (two CTAs per SM) or 4 (one CTA
-// per SM, deeper z columns).  DCELL_TC_BRICK_POINTS overrides the default;
-// grids too shallow for the 4-point box use 2.
-static int brick_points(const Geom &g) {
-  int p = 2;
-  if (const char *e = getenv("DCELL_TC_BRICK_POINTS")) p = atoi(e) == 4 ? 4 : 2;
-  if (p == 4 && g.nz < tc::BrickShape<4>::PZ) p = 2;
-  return p;
-}
-
 int launch_sl_tc_brick(const Geom &g, const uint32_t *phi0s, const float *vel, double dt, int backtrace, float *phi,
                        uint32_t *phis, int *flags, cudaStream_t st) {
-  if (brick_points(g) == 4) return launch_brick<4>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st, nullptr);
   return launch_brick<2>(g, phi0s, vel, dt, backtrace, phi, phis, flags, st, nullptr);
 }
 

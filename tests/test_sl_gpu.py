@@ -360,17 +360,14 @@ def test_tc_split_band_mode_and_multistep(cuda):
     assert float(err.max()) <= 1e-5, float(err.max())
 
 
-@pytest.mark.parametrize("points", [2, 4])
 @pytest.mark.parametrize("shape", [(40, 48, 64), (37, 45, 68), (12, 8, 40), (20, 8, 40)])
 @pytest.mark.parametrize("cfl_scale", [1.0, 3.0])
-def test_tc_brick_path_equals_gather_path(cuda, cfl_scale, shape, points, monkeypatch):
+def test_tc_brick_path_equals_gather_path(cuda, cfl_scale, shape):
     """Dense split-state steps on grids with nx % 4 == 0 run the TMA-staged
-    brick kernel (2 or 4 points per thread; grids too shallow for the 4-point
-    box use 2); a band listing every point runs the global-gather kernel.
+    brick kernel; a band listing every point runs the global-gather kernel.
     Both must give the same bits (3x the CFL exercises the brick fallbacks;
     the odd shapes end in partial bricks on every axis, the smallest are one
-    brick box deep)."""
-    monkeypatch.setenv("DCELL_TC_BRICK_POINTS", str(points))
+    brick deep, so a CTA's first step is also its last brick's)."""
     nz, ny, nx = shape
     h = 1.0 / 64
     phi = fields.sphere_sdf(72, device=cuda)[:nz, :ny, :nx].contiguous().float()
