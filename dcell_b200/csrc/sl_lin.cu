@@ -129,6 +129,98 @@ struct BoxAcc {
   }
 };
 
+// Paired FP32 (fma.rn.f32x2 / add / mul): two points of one thread advance
+// together, each lane rounding exactly as the scalar helpers of
+// sl_device.cuh do (explicit round-to-nearest, no contraction), so a pair
+// gives the bits of two scalar evaluations.
+__device__ __forceinline__ float2 pair(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 s) {  // a + s (b - a)
+  return __ffma2_rn(s, __fadd2_rn(b, make_float2(-a.x, -a.y)), a);
+}
+__device__ __forceinline__ float2 trilerp2(float2 v000, float2 v100, float2 v010, float2 v110, float2 v001,
+                                           float2 v101, float2 v011, float2 v111, const float2 s[3]) {
+  return lerp2(lerp2(lerp2(v000, v100, s[0]), lerp2(v010, v110, s[0]), s[1]),
+               lerp2(lerp2(v001, v101, s[0]), lerp2(v011, v111, s[0]), s[1]), s[2]);
+}
+__device__ __forceinline__ float2 face_mean2(float2 a, float2 b) {  // 0.5 a + (0.5 b), as face_mean
+  return __ffma2_rn(pair(0.5f, 0.5f), a, __fmul2_rn(pair(0.5f, 0.5f), b));
+}
+
+// lin_points for two points of one thread on a 3-D grid (rows y[0], y[1]):
+// the same operations in the same order, the two points' floating-point
+// steps paired.
+template <int BT, bool VOTE, class A>
+__device__ __forceinline__ bool lin_points_pair(const A &acc, int x, const int y[2], int z, const float dth[3],
+                                                const float hdth[3], float out[2], int c[2][3], float f[2][3]) {
+  const int y0 = y[0], y1 = y[1];
+  float2 U[3];
+  U[0] = face_mean2(pair(acc.v(x, y0, z, 0), acc.v(x, y1, z, 0)), pair(acc.v(x + 1, y0, z, 0), acc.v(x + 1, y1, z, 0)));
+  U[1] = face_mean2(pair(acc.v(x, y0, z, 1), acc.v(x, y1, z, 1)), pair(acc.v(x, y0 + 1, z, 1), acc.v(x, y1 + 1, z, 1)));
+  U[2] = face_mean2(pair(acc.v(x, y0, z, 2), acc.v(x, y1, z, 2)), pair(acc.v(x, y0, z + 1, 2), acc.v(x, y1, z + 1, 2)));
+  const int X0[3] = {x, y0, z}, X1[3] = {x, y1, z};
+  if (BT == DCELL_MIDPOINT) {
+    float2 dl[3];
+    bool near = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      dl[a] = __fmul2_rn(U[a], pair(hdth[a], hdth[a]));
+      near = near && fabsf(dl[a].x) < 1.f && fabsf(dl[a].y) < 1.f;
+    }
+    if (VOTE && !__all_sync(0xffffffffu, near)) return false;
+    float2 V[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      int b0[3], b1[3];
+      float2 s[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {  // the component's own axis carries the half-cell stagger
+        const float2 t = a == d ? __fadd2_rn(dl[a], pair(0.5f, 0.5f)) : dl[a];
+        const float fl0 = floorf(t.x), fl1 = floorf(t.y);
+        b0[a] = X0[a] + (int)fl0;
+        b1[a] = X1[a] + (int)fl1;
+        s[a] = __fadd2_rn(t, pair(-fl0, -fl1));
+      }
+      V[d] = trilerp2(pair(acc.v(b0[0], b0[1], b0[2], d), acc.v(b1[0], b1[1], b1[2], d)),
+                      pair(acc.v(b0[0] + 1, b0[1], b0[2], d), acc.v(b1[0] + 1, b1[1], b1[2], d)),
+                      pair(acc.v(b0[0], b0[1] + 1, b0[2], d), acc.v(b1[0], b1[1] + 1, b1[2], d)),
+                      pair(acc.v(b0[0] + 1, b0[1] + 1, b0[2], d), acc.v(b1[0] + 1, b1[1] + 1, b1[2], d)),
+                      pair(acc.v(b0[0], b0[1], b0[2] + 1, d), acc.v(b1[0], b1[1], b1[2] + 1, d)),
+                      pair(acc.v(b0[0] + 1, b0[1], b0[2] + 1, d), acc.v(b1[0] + 1, b1[1], b1[2] + 1, d)),
+                      pair(acc.v(b0[0], b0[1] + 1, b0[2] + 1, d), acc.v(b1[0], b1[1] + 1, b1[2] + 1, d)),
+                      pair(acc.v(b0[0] + 1, b0[1] + 1, b0[2] + 1, d), acc.v(b1[0] + 1, b1[1] + 1, b1[2] + 1, d)), s);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) U[a] = V[a];
+  }
+  bool in = true;
+  float2 fr[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float2 t = __fmul2_rn(pair(-U[a].x, -U[a].y), pair(dth[a], dth[a]));
+    in = in && t.x >= -2.f && t.x < 2.f && t.y >= -2.f && t.y < 2.f;
+    const float fl0 = floorf(t.x), fl1 = floorf(t.y);
+    c[0][a] = X0[a] + (int)fl0;
+    c[1][a] = X1[a] + (int)fl1;
+    fr[a] = __fadd2_rn(t, pair(-fl0, -fl1));
+    f[0][a] = fr[a].x;
+    f[1][a] = fr[a].y;
+  }
+  if (VOTE && !__all_sync(0xffffffffu, in)) return false;
+  const int *C0 = c[0], *C1 = c[1];
+  const float2 v = trilerp2(pair(acc.phi(C0[0], C0[1], C0[2]), acc.phi(C1[0], C1[1], C1[2])),
+                            pair(acc.phi(C0[0] + 1, C0[1], C0[2]), acc.phi(C1[0] + 1, C1[1], C1[2])),
+                            pair(acc.phi(C0[0], C0[1] + 1, C0[2]), acc.phi(C1[0], C1[1] + 1, C1[2])),
+                            pair(acc.phi(C0[0] + 1, C0[1] + 1, C0[2]), acc.phi(C1[0] + 1, C1[1] + 1, C1[2])),
+                            pair(acc.phi(C0[0], C0[1], C0[2] + 1), acc.phi(C1[0], C1[1], C1[2] + 1)),
+                            pair(acc.phi(C0[0] + 1, C0[1], C0[2] + 1), acc.phi(C1[0] + 1, C1[1], C1[2] + 1)),
+                            pair(acc.phi(C0[0], C0[1] + 1, C0[2] + 1), acc.phi(C1[0], C1[1] + 1, C1[2] + 1)),
+                            pair(acc.phi(C0[0] + 1, C0[1] + 1, C0[2] + 1), acc.phi(C1[0] + 1, C1[1] + 1, C1[2] + 1)),
+                            fr);
+  out[0] = v.x;
+  out[1] = v.y;
+  return true;
+}
+
 // R arrival points of one thread (local indices x, y[r], z): node velocity,
 // optional midpoint velocity, departure, bi/trilinear phi0, into out[r]; c,
 // f: the departure cells (local) and fractions.  dth = dt / h per axis,
@@ -287,8 +379,13 @@ __device__ __forceinline__ bool march_run(const A &bacc, const GlobalAcc<3> &gac
     int c[S::RW][3];
     float f[S::RW][3];
     float v[S::RW];
-    if (!lin_points<BT, 3, true, S::RW>(bacc, x, y, z, dth, hdth, v, c, f))
-      lin_points<BT, 3, false, S::RW>(gacc, x, y, z, dth, hdth, v, c, f);
+    if constexpr (S::RW == 2) {  // two rows per warp: the points' arithmetic in f32x2 pairs
+      if (!lin_points_pair<BT, true>(bacc, x, y, z, dth, hdth, v, c, f))
+        lin_points_pair<BT, false>(gacc, x, y, z, dth, hdth, v, c, f);
+    } else {
+      if (!lin_points<BT, 3, true, S::RW>(bacc, x, y, z, dth, hdth, v, c, f))
+        lin_points<BT, 3, false, S::RW>(gacc, x, y, z, dth, hdth, v, c, f);
+    }
 #pragma unroll
     for (int r = 0; r < S::RW; ++r)
       if (store[r]) phi[(z * g.ny + y[r]) * g.nx + x] = v[r];
