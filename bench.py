@@ -155,13 +155,13 @@ def timed_steps(L, torch, phi, vel, h, dt, interp, K, W, dist=None, backtrace="m
     return e0.elapsed_time(e1)
 
 
-def timed_tc_split(L, torch, phi, vel, h, dt, K, W, dist=None):
+def timed_tc_split(L, torch, phi, vel, h, dt, K, W, dist=None, backtrace="midpoint"):
     """The headline loop: split-BF16 tensor-core steps on a split-state level
     set (each step writes phi and its packed BF16 split for the next step)."""
     a, b = phi.clone(), torch.empty_like(phi)
     sa, sb = L.split_bf16(phi), torch.empty(phi.shape, dtype=torch.int32, device=phi.device)
     for s in range(W):
-        L.sl_step_tc_split(sa, vel, dt_at(s, dt), h, backtrace="midpoint", out=b, out_split=sb)
+        L.sl_step_tc_split(sa, vel, dt_at(s, dt), h, backtrace=backtrace, out=b, out_split=sb)
         a, b, sa, sb = b, a, sb, sa
     if dist:
         dist.barrier()
@@ -170,7 +170,7 @@ def timed_tc_split(L, torch, phi, vel, h, dt, K, W, dist=None):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
     for s in range(K):
-        L.sl_step_tc_split(sa, vel, dt_at(W + s, dt), h, backtrace="midpoint", out=b, out_split=sb)
+        L.sl_step_tc_split(sa, vel, dt_at(W + s, dt), h, backtrace=backtrace, out=b, out_split=sb)
         a, b, sa, sb = b, a, sb, sa
     e1.record(st)
     torch.cuda.synchronize()
@@ -607,6 +607,11 @@ def main():
         ms_tc_unsplit = timed_steps(L, torch, phi, vel, h, dt, "cubic_tc", K, W)
         ms_lin = timed_steps(L, torch, phi, vel, h, dt, "linear", K, W)
         ms_lin_e = timed_steps(L, torch, phi, vel, h, dt, "linear", K, W, backtrace="euler")
+        # the reference's own backtrace (AdvectSL.c:56-89: S = X - V dt / h)
+        ms_tc_e = timed_tc_split(L, torch, phi, vel, h, dt, K, W, backtrace="euler")
+        ms_pl_e = timed_steps(L, torch, phi, vel, h, dt, "cubic_plain_gather", K, W, backtrace="euler")
+        ms_sep_e = timed_steps(L, torch, phi, vel, h, dt, "cubic_separable_gather", K, W, backtrace="euler")
+        ms_sep_b_e = timed_steps(L, torch, phi, vel, h, dt, "cubic_separable", K, W, backtrace="euler")
 
         def hbm_leg(ms):  # one dense FP32 step: 20 algorithmic bytes per update
             t = ms / K / 1e3
@@ -628,7 +633,13 @@ def main():
             # the reference's own mode (trilinear, Euler backtrace) and its
             # midpoint form: TMA z-march, HBM-bound
             "linear_fp32": {"euler": hbm_leg(ms_lin_e), "midpoint": hbm_leg(ms_lin),
-                            "kernel": "sl_lin_march_kernel"}}
+                            "kernel": "sl_lin_march_kernel"},
+            # the same forms with the reference's own (Euler) backtrace
+            "euler_backtrace": {"tc_ms_per_step": ms_tc_e / K, "plain_fp32_ms_per_step": ms_pl_e / K,
+                                "separable_fp32_ms_per_step": ms_sep_e / K,
+                                "separable_fp32_brick_ms_per_step": ms_sep_b_e / K,
+                                "tc_over_plain_fp32": ms_pl_e / ms_tc_e, "tc_over_separable_fp32": ms_sep_e / ms_tc_e,
+                                "tc_over_separable_fp32_brick": ms_sep_b_e / ms_tc_e}}
         line["accuracy"] = error_check(L, torch, phi, vel, h, dt)
         if world == 1:
             # the whole period of the field (t = 0 .. T): one-step error of the
