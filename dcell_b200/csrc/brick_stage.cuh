@@ -5,7 +5,7 @@
 // thread's points from the staged boxes.
 //
 // A CTA walks bricks of 32 x 4 x 4P arrival points, P = points each thread
-// carries per step along z (2 or 4).  For each brick two tiled TMA loads stage
+// carries per step along z (2).  For each brick two tiled TMA loads stage
 // the 32-bit phi words of the box [x0-4, x0+36) x [y0-2, y0+6) x [z0-2,
 // z0+4P+2) and the interleaved velocity of [x0-4, x0+36) x [y0-1, y0+5) x
 // [z0-1, z0+4P+1) in shared memory, completion tracked by an mbarrier's

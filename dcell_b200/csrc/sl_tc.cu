@@ -440,16 +440,18 @@ __device__ __noinline__ float3 brick_rows_global(Geom g, const uint32_t *__restr
 // Dense-grid stepper over TMA-staged bricks.
 //
 // Each CTA owns bricks blockIdx.x, blockIdx.x + gridDim.x, ... (32 x 4 x 4P
-// points, 4 steps each); their boxes are double-buffered with the next brick
-// in flight.  Four compute warps carry P points per thread and step -- the
-// same (x, y) in P consecutive z planes -- held in P TMEM stages (A | D, 128
-// columns each); a fifth warp only issues the MMAs and the TMA loads.  Warps
-// are decoupled by mbarriers, not CTA barriers:
+// points, P = 2, 4 steps each); their boxes are double-buffered with the next
+// brick in flight.  Four compute warps carry P points per thread and step --
+// the same (x, y) in P consecutive z planes -- held in P TMEM stages (A | D,
+// 128 columns each); a fifth warp only issues the MMAs and the TMA loads.
+// Warps are decoupled by mbarriers, not CTA barriers:
 //
-//   compute warp, step j:
-//     a. A rows of the P points -> their stages, arrive on afull
-//     b. departures of step j+1's points (overlaps the MMAs)
-//     c. wait dfull: coefficients -> values, two points evaluated together
+//   compute warp, step j (step j+1's departures are known from step j-1):
+//     1. wait dfull: step j's MMAs are done
+//     2. A rows of step j+1's points -> the stages (step j's rows are read)
+//     3. step j's coefficients -> registers, then arrive on afull (step j+1)
+//     4. step j's values evaluated and stored
+//     5. departures of step j+2's points (overlaps step j+1's MMAs)
 //   issuer, step j: wait afull (all four warps), every stage's MMAs, commit to
 //     dfull; after a brick's last step, refill that brick's buffer with the
 //     brick two ahead.
@@ -457,11 +459,11 @@ __device__ __noinline__ float3 brick_rows_global(Geom g, const uint32_t *__restr
 // When every lane's P stencils are stacked one plane apart (the usual case:
 // the points depart from vertically adjacent cells) the warp gathers their
 // 4 x 4 x (P+3) union once.  A stage's A columns are rewritten only after the
-// writing warp saw the MMAs complete (c of the step before); D columns are
-// overwritten only after every warp arrived on afull for the next step, which
-// each does after reading D.  A buffer is refilled only after afull of its
-// brick's last step: every warp has then gathered from it for the last time
-// (its departures were computed one step earlier).  Every wait is bounded; a
+// writing warp saw the MMAs that read them complete (1); D columns are
+// overwritten only after every warp has read them and arrived for the next
+// step (3).  A buffer is refilled only after afull of its brick's last step:
+// every warp has then gathered from it for the last time (its departures were
+// computed before).  Every wait is bounded; a
 // warp that gives up raises FLAG_WAIT_TIMEOUT and leaves, and the others then
 // give up at their next wait.  Before the CTA ends, the issuer waits for its
 // last TMA load per buffer and its last commit.  SPLIT: also write the
