@@ -555,6 +555,10 @@ struct Resident {
   bool split_ok = false;  // split[cur] is the split of phi[cur]
   int nband = 0, ncap = 0;
   DevBuf phi[2], split[2], vel, vel64, band, nodes, scratch, small;
+  bool reinit_pending = false;  // a step triggered the reinitialisation; it runs before the level set is next used
+  double reinit_bw = 0.0;       // its band width
+  int *reinit_hv = nullptr;     // pinned: its flags, -, band points
+  cudaEvent_t reinit_ev = nullptr;
 };
 
 struct dcell_session {
@@ -639,6 +643,8 @@ DCELL_API int dcell_session_destroy(dcell_session *s) {
   for (DevBuf *b : {&r.phi[0], &r.phi[1], &r.split[0], &r.split[1], &r.vel, &r.vel64, &r.band, &r.nodes, &r.scratch,
                     &r.small})
     b->release();
+  if (r.reinit_hv) cudaFreeHost(r.reinit_hv);
+  if (r.reinit_ev) cudaEventDestroy(r.reinit_ev);
   for (cudaEvent_t e : s->ev_in) cudaEventDestroy(e);
   for (cudaEvent_t e : s->ev_out) cudaEventDestroy(e);
   if (s->h2d) cudaStreamDestroy(s->h2d);
@@ -1314,18 +1320,62 @@ static int resident_nodes(dcell_session *s) {
 
 // Node capacity for a band of nband points (sign changes at a band point's
 // faces and its projection node), grown keeping the current nodes (the next
-// step's max |V| reads them); the band buffer holds any band of the grid.
+// step's max |V| reads them), with a quarter of headroom so that a band that
+// grows a little after a reinitialisation does not reallocate every time;
+// the band buffer holds any band of the grid.
 static int resident_sizes(dcell_session *s, int nband) {
   Resident &r = s->res;
   const long long n = grid_points(&r.g);
-  const int want = (int)std::min<long long>(8LL * nband + 1024, 8LL * n + 1024);
-  int rc = r.nodes.grow_keep((size_t)want * sizeof(dcell_irregular_node),
-                             (size_t)r.ncap * sizeof(dcell_irregular_node), s->stream);
-  if (rc) return rc;
-  if (want > r.ncap) r.ncap = want;
+  const long long most = 8LL * n + 1024;
+  const long long need = std::min<long long>(8LL * nband + 1024, most);
+  if (need > r.ncap) {
+    const int want = (int)std::min<long long>(need + need / 4, most);
+    int rc = r.nodes.grow_keep((size_t)want * sizeof(dcell_irregular_node),
+                               (size_t)r.ncap * sizeof(dcell_irregular_node), s->stream);
+    if (rc) return rc;
+    r.ncap = want;
+  }
   ENSURE(r.band, (size_t)(n > 0 ? n : 1) * 3 * sizeof(int));
   ENSURE(r.small, 256);
   return DCELL_OK;
+}
+
+// LevelSetReinitialize on the device (the bucketed march, band width bw),
+// seeded by the current irregular nodes, enqueued on the session stream with
+// its counters copied back behind it; reinit_ev marks the end.  The session
+// stream holds nothing else of this call yet, so reading the node count is
+// a short wait.
+static int resident_reinit_enqueue(dcell_session *s, double bw) {
+  Resident &r = s->res;
+  cudaStream_t st = s->stream;
+  const dcell_geom *g = &r.g;
+  const long long n = grid_points(g);
+  int *dflags = (int *)r.small.p, *dcount = dflags + 1;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(r.reinit_hv, dcount, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
+  int nn = r.reinit_hv[0];
+  if (nn > r.ncap) nn = r.ncap;
+  const size_t sb = dcell_reinit_scratch_bytes(g, r.precision);
+  ENSURE(r.scratch, sb);
+  int rc = dcell_reinitialize(g, r.precision, r.phi[r.cur].p, (const dcell_irregular_node *)r.nodes.p, nn, bw, 0.0,
+                              (int *)r.band.p, (int)n, dflags + 2, r.scratch.p, sb, dflags, st);
+  if (rc) return rc;
+  DCELL_CUDA_CHECK(cudaMemcpyAsync(r.reinit_hv, dflags, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+  DCELL_CUDA_CHECK(cudaEventRecord(r.reinit_ev, st));
+  r.split_ok = false;
+  r.reinit_pending = false;
+  return DCELL_OK;
+}
+
+// Waits for the enqueued reinitialisation alone (later work on the stream
+// may still run), takes its band and grows the node buffer for it.
+static int resident_reinit_finish(dcell_session *s) {
+  Resident &r = s->res;
+  DCELL_CUDA_CHECK(cudaEventSynchronize(r.reinit_ev));
+  int rc = session_flags_status(s, r.reinit_hv[0] & ~DCELL_FLAG_DEPARTURE_CLAMPED);
+  if (rc) return rc;
+  r.nband = r.reinit_hv[2];
+  return resident_sizes(s, r.nband);
 }
 
 DCELL_API int dcell_ls_resident_set(dcell_session *s, const dcell_geom *g, const double *phi, const int *band,
@@ -1339,6 +1389,9 @@ DCELL_API int dcell_ls_resident_set(dcell_session *s, const dcell_geom *g, const
   DCELL_CUDA_CHECK(cudaSetDevice(s->device));
   Resident &r = s->res;
   r.on = false;
+  r.reinit_pending = false;
+  if (!r.reinit_hv) DCELL_CUDA_CHECK(cudaMallocHost((void **)&r.reinit_hv, 4 * sizeof(int)));
+  if (!r.reinit_ev) DCELL_CUDA_CHECK(cudaEventCreateWithFlags(&r.reinit_ev, cudaEventDisableTiming));
   r.g = *g;
   r.precision = precision;
   r.cur = 0;
@@ -1390,6 +1443,19 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
   int *dflags = (int *)r.small.p, *dcount = dflags + 1;
   double *dmax = (double *)((char *)r.small.p + 64);
   DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
+  // the reinitialisation the last step triggered runs first; with the
+  // pipelined upload below it overlaps this step's velocity copy
+  // the velocity upload (on the copy stream, when pipelined) needs only the
+  // session's earlier work done, not this call's reinitialisation
+  if ((rc = ensure_copy_streams(s))) return rc;
+  cudaEvent_t start = s->ev_out[kPipeSlabs - 1];
+  DCELL_CUDA_CHECK(cudaEventRecord(start, st));
+  bool reinit_open = r.reinit_pending;  // enqueued, its band not yet taken
+  if (reinit_open && (rc = resident_reinit_enqueue(s, r.reinit_bw))) return rc;
+  if (reinit_open && !dense) {  // the band step below needs the new band first
+    if ((rc = resident_reinit_finish(s))) return rc;
+    reinit_open = false;
+  }
   const size_t ves = r.precision == DCELL_F32 ? sizeof(float) : sizeof(double);
   const size_t ies = vel_dtype == DCELL_F32 ? sizeof(float) : sizeof(double);
   ENSURE(r.vel, n * dof * ves);
@@ -1406,7 +1472,6 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
                          tc_brick_applicable(G, (const void *)256, (const void *)256);
   bool redo_possible = false;
   if (pipelined) {
-    if ((rc = ensure_copy_streams(s))) return rc;
     ENSURE(r.split[0], n * sizeof(uint32_t));
     ENSURE(r.split[1], n * sizeof(uint32_t));
     ENSURE(s->gates, kPipeSlabs * sizeof(int));
@@ -1414,8 +1479,6 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
     if (!r.split_ok && (rc = launch_split_bf16((const float *)r.phi[cur].p, (uint32_t *)r.split[cur].p, n, st)))
       return rc;
     DCELL_CUDA_CHECK(cudaMemsetAsync(gates, 0, kPipeSlabs * sizeof(int), st));
-    cudaEvent_t start = s->ev_out[kPipeSlabs - 1];
-    DCELL_CUDA_CHECK(cudaEventRecord(start, st));  // the upload starts after this session's earlier work
     DCELL_CUDA_CHECK(cudaStreamWaitEvent(s->h2d, start, 0));
     const long long plane = (long long)G.nx * G.ny;
     const int BZ = tc_slab_planes(), nbz = (G.nz + BZ - 1) / BZ, per = (nbz + kPipeSlabs - 1) / kPipeSlabs;
@@ -1454,7 +1517,12 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
     // the last slab waited for the last chunk: every velocity plane is present on st from here
     redo_possible = true;
     r.split_ok = true;
-  } else {
+  }
+  if (reinit_open) {  // its band sizes the node pass (and the upload, when pipelined, is already on its way)
+    if ((rc = resident_reinit_finish(s))) return rc;
+    reinit_open = false;
+  }
+  if (!pipelined) {
     // the step's velocity (the only per-step upload)
     if (vel_dtype == r.precision) {
       DCELL_CUDA_CHECK(cudaMemcpyAsync(r.vel.p, vel, n * dof * ves, cudaMemcpyHostToDevice, st));
@@ -1515,26 +1583,14 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
   loop->AdvectCount++;
   loop->reinitialized = 0;
   if (loop->AdvectCount > loop->AdvectThres || loop->CFLcount > loop->CFLthres) {
-    // LevelSetReinitialize on the device (the bucketed march), new band
+    // LevelSetReinitialize (the device's bucketed march, new band), from
+    // this step's nodes: it runs before the level set is next used -- at the
+    // start of the next call, under its velocity upload, or in
+    // dcell_ls_resident_get
     loop->CFLcount = 0;
     loop->AdvectCount = 0;
-    int nn = 0;
-    DCELL_CUDA_CHECK(cudaMemcpy(&nn, dcount, sizeof(int), cudaMemcpyDeviceToHost));
-    if (nn > r.ncap) nn = r.ncap;
-    const size_t sb = dcell_reinit_scratch_bytes(g, r.precision);
-    ENSURE(r.scratch, sb);
-    int *dband_count = dflags + 2;
-    if ((rc = dcell_reinitialize(g, r.precision, r.phi[r.cur].p, (const dcell_irregular_node *)r.nodes.p, nn,
-                                 loop->bandWidth, 0.0, (int *)r.band.p, (int)n, dband_count, r.scratch.p, sb, dflags,
-                                 st)))
-      return rc;
-    int hv[3] = {0, 0, 0};
-    DCELL_CUDA_CHECK(cudaMemcpyAsync(hv, dflags, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
-    DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
-    if ((rc = session_flags_status(s, hv[0] & ~DCELL_FLAG_DEPARTURE_CLAMPED))) return rc;
-    r.nband = hv[2];
-    r.split_ok = false;
-    if ((rc = resident_sizes(s, r.nband))) return rc;
+    r.reinit_pending = true;
+    r.reinit_bw = loop->bandWidth;
     loop->reinitialized = 1;
   }
   loop->band = r.nband;
@@ -1555,6 +1611,9 @@ DCELL_API int dcell_ls_resident_get(dcell_session *s, const dcell_geom *g, doubl
   cudaStream_t st = s->stream;
   const long long n = grid_points(g);
   int rc;
+  if (r.reinit_pending) {  // the reinitialisation the last step triggered
+    if ((rc = resident_reinit_enqueue(s, r.reinit_bw)) || (rc = resident_reinit_finish(s))) return rc;
+  }
   if (phi) {
     if (r.precision == DCELL_F32) {
       ENSURE(s->phi_64, n * sizeof(double));

@@ -474,6 +474,11 @@ DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const do
  * loop->AdvectThres or loop->CFLcount > loop->CFLthres, the reinitialisation
  * (dcell_reinitialize's bucketed march, band width loop->bandWidth) that
  * replaces phi's band; the counters live in `loop` as in struct _LevelSet.
+ * The reinitialisation a step triggers (loop->reinitialized = 1) runs before
+ * the level set is next used -- first thing in the next call, where it
+ * overlaps that step's velocity upload, or in dcell_ls_resident_get -- so
+ * loop->band reports the band before it; the results are those of running
+ * it at the end of the step.
  * dcell_ls_resident_get downloads phi (FP64) and the band where the host
  * needs them (output, or a CPU fast marching instead of the device one).
  * precision: the arithmetic (DCELL_F32 with DCELL_CUBIC_TC on a dense 3D grid
@@ -484,8 +489,8 @@ DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const do
 typedef struct dcell_ls_loop {
   double CFLcount, CFLthres, maxVel, bandWidth; /* struct _LevelSet's fields (LevelSetMethod.h:10-26) */
   int AdvectCount, AdvectThres;
-  int reinitialized; /* out: 1 when this step reinitialised */
-  int band;          /* out: band points after the step */
+  int reinitialized; /* out: 1 when this step triggered the reinitialisation */
+  int band;          /* out: band points after the step (before a reinitialisation it triggered) */
 } dcell_ls_loop;
 DCELL_API int dcell_ls_resident_set(dcell_session *s, const dcell_geom *g, const double *phi, const int *band,
                                     int nband, int precision);

@@ -87,3 +87,45 @@ def test_resident_tc_loop_equals_split_state_steps(cuda, cfl, vel_dtype):
     got, _ = r.get()
     r.close()
     assert np.array_equal(got, out.double().cpu().numpy())
+
+
+@pytest.mark.gpu
+def test_resident_tc_loop_with_reinitialisation(cuda):
+    """FP32 dense split-BF16 steps at 64^3 (the velocity upload overlapped with
+    z-slab steps) with a CFL threshold low enough that the loop reinitialises
+    twice.  The reinitialisation a step triggers runs at the start of the next
+    call, under its upload, or in get(); phi, band and counters equal a
+    step-by-step device loop that reinitialises at the end of the triggering
+    step (split state carried, re-split after each reinitialisation)."""
+    N = 64
+    h, phi, vel, band = _case(N, cuda)
+    dt = 0.5 * h
+    v32 = vel.float().contiguous()
+    r = L.ResidentLevelSet(phi.cpu().numpy(), h, band=band.cpu().numpy(), precision="f32", CFLthres=1.0)
+    vhost = v32.cpu().numpy()
+    p = phi.float().contiguous()
+    b = band.to(cuda).contiguous()
+    spl = L.split_bf16(p)
+    raw, count = L.irregular_nodes(p, h, b, with_surface=False)
+    cfl, reinits = 0.0, 0
+    for s in range(10):
+        loop = r.advect_and_reinit(vhost, dt, interp="cubic_tc", backtrace="midpoint", dense=True)
+        p, spl = L.sl_step_tc_split(spl, v32, dt, h, backtrace="midpoint", out_split=torch.empty_like(spl))
+        maxvel = float(L.max_velocity(v32, h, raw, count).item())
+        cfl += dt * maxvel / h
+        raw, count = L.irregular_nodes(p, h, b, with_surface=False)
+        assert loop.maxVel == maxvel
+        if cfl > 1.0:
+            cfl = 0.0
+            reinits += 1
+            b = L.reinitialize(p, raw, count, 6.0)
+            spl = L.split_bf16(p)
+            assert loop.reinitialized == 1
+        else:
+            assert loop.reinitialized == 0
+        assert loop.CFLcount == cfl
+    assert reinits >= 2
+    got, gband = r.get()
+    r.close()
+    assert np.array_equal(got, p.double().cpu().numpy())
+    assert np.array_equal(gband, b.cpu().numpy())
