@@ -555,6 +555,7 @@ struct Resident {
   bool split_ok = false;  // split[cur] is the split of phi[cur]
   int nband = 0, ncap = 0;
   DevBuf phi[2], split[2], vel, vel64, band, nodes, scratch, small;
+  bool nodes_pending = false;   // the irregular nodes of phi[cur] are due (the node pass of the last step)
   bool reinit_pending = false;  // a step triggered the reinitialisation; it runs before the level set is next used
   double reinit_bw = 0.0;       // its band width
   int *reinit_hv = nullptr;     // pinned: its flags, -, band points
@@ -712,7 +713,7 @@ static int ls_advect_tc_pipelined(dcell_session *s, const dcell_geom *g, const d
   DCELL_CUDA_CHECK(cudaStreamWaitEvent(s->h2d, start, 0));
   const int BZ = tc_slab_planes();
   const int nbz = (G.nz + BZ - 1) / BZ, per = (nbz + kSlabs - 1) / kSlabs;
-  int have = 0, nslab = 0;  // planes present on the device
+  int have = 0, gated = 0, nslab = 0;  // planes present on the device, planes in the gate's max
   for (int k = 0; k < kSlabs; ++k) {
     const int b0 = k * per, b1 = b0 + per < nbz ? b0 + per : nbz;
     if (b0 >= b1) break;
@@ -730,12 +731,17 @@ static int ls_advect_tc_pipelined(dcell_session *s, const dcell_geom *g, const d
     }
     DCELL_CUDA_CHECK(cudaEventRecord(s->ev_in[k], s->h2d));
     DCELL_CUDA_CHECK(cudaStreamWaitEvent(st, s->ev_in[k], 0));
-    // the gate: max |w| over every plane present bounds the departures of this slab
-    if ((rc = launch_max_abs_component(v32, have * plane, 3, 2, gates + k, st))) return rc;
+    // the gate: max |w| over every plane present bounds the departures of
+    // this slab (a running max: each chunk's planes once)
+    if (have > gated) {
+      if ((rc = launch_max_abs_component(v32 + 3 * gated * plane, (have - gated) * plane, 3, 2, gates, st)))
+        return rc;
+      gated = have;
+    }
     TcSlab slab;
     slab.bz0 = b0;
     slab.nbz = b1 - b0;
-    slab.gate_maxw = gates + k;
+    slab.gate_maxw = gates;
     slab.gate_limit = (float)(kHalo - 3);
     if ((rc = launch_sl_tc_slab(G, w, v32, dt, backtrace, o32, nullptr, dflags, st, slab))) return rc;
     const long long oz = z0 * plane, mz = (z1 - z0) * plane;
@@ -1340,6 +1346,17 @@ static int resident_sizes(dcell_session *s, int nband) {
   return DCELL_OK;
 }
 
+// The node pass a step leaves due (LevelSetUpdateIrregularNodeList of the
+// new level set), enqueued on the session stream: the next call runs it
+// first, under its velocity upload, before the max |V| and a
+// reinitialisation read the nodes.
+static int resident_nodes_due(dcell_session *s) {
+  Resident &r = s->res;
+  if (!r.nodes_pending) return DCELL_OK;
+  r.nodes_pending = false;
+  return resident_nodes(s);
+}
+
 // LevelSetReinitialize on the device (the bucketed march, band width bw),
 // seeded by the current irregular nodes, enqueued on the session stream with
 // its counters copied back behind it; reinit_ev marks the end.  The session
@@ -1389,6 +1406,7 @@ DCELL_API int dcell_ls_resident_set(dcell_session *s, const dcell_geom *g, const
   DCELL_CUDA_CHECK(cudaSetDevice(s->device));
   Resident &r = s->res;
   r.on = false;
+  r.nodes_pending = false;
   r.reinit_pending = false;
   if (!r.reinit_hv) DCELL_CUDA_CHECK(cudaMallocHost((void **)&r.reinit_hv, 4 * sizeof(int)));
   if (!r.reinit_ev) DCELL_CUDA_CHECK(cudaEventCreateWithFlags(&r.reinit_ev, cudaEventDisableTiming));
@@ -1450,6 +1468,7 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
   if ((rc = ensure_copy_streams(s))) return rc;
   cudaEvent_t start = s->ev_out[kPipeSlabs - 1];
   DCELL_CUDA_CHECK(cudaEventRecord(start, st));
+  if ((rc = resident_nodes_due(s))) return rc;  // the last step's node pass
   bool reinit_open = r.reinit_pending;  // enqueued, its band not yet taken
   if (reinit_open && (rc = resident_reinit_enqueue(s, r.reinit_bw))) return rc;
   if (reinit_open && !dense) {  // the band step below needs the new band first
@@ -1483,7 +1502,7 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
     const long long plane = (long long)G.nx * G.ny;
     const int BZ = tc_slab_planes(), nbz = (G.nz + BZ - 1) / BZ, per = (nbz + kPipeSlabs - 1) / kPipeSlabs;
     float *v32 = (float *)r.vel.p;
-    int have = 0;
+    int have = 0, gated = 0;  // planes present on the device, planes in the gate's max
     for (int k = 0; k < kPipeSlabs; ++k) {
       const int b0 = k * per, b1 = b0 + per < nbz ? b0 + per : nbz;
       if (b0 >= b1) break;
@@ -1504,11 +1523,15 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
       }
       DCELL_CUDA_CHECK(cudaEventRecord(s->ev_in[k], s->h2d));
       DCELL_CUDA_CHECK(cudaStreamWaitEvent(st, s->ev_in[k], 0));
-      if ((rc = launch_max_abs_component(v32, have * plane, 3, 2, gates + k, st))) return rc;
+      if (have > gated) {  // the gate's running max over the planes present
+        if ((rc = launch_max_abs_component(v32 + 3 * gated * plane, (have - gated) * plane, 3, 2, gates, st)))
+          return rc;
+        gated = have;
+      }
       TcSlab slab;
       slab.bz0 = b0;
       slab.nbz = b1 - b0;
-      slab.gate_maxw = gates + k;
+      slab.gate_maxw = gates;
       slab.gate_limit = (float)(kPipeHalo - 3);
       if ((rc = launch_sl_tc_slab(G, (const uint32_t *)r.split[cur].p, v32, dt, backtrace, (float *)r.phi[nxt].p,
                                   (uint32_t *)r.split[nxt].p, dflags, st, slab)))
@@ -1558,8 +1581,9 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
   }
   if (rc) return rc;
   r.cur = nxt;
-  // LevelSetUpdateIrregularNodeList of the new phi
-  if ((rc = resident_nodes(s))) return rc;
+  // LevelSetUpdateIrregularNodeList of the new phi: due, it runs first in the
+  // next call (under its upload) or before a reinitialisation
+  r.nodes_pending = true;
   double maxvel = 0.0;
   int hf = 0;
   DCELL_CUDA_CHECK(cudaMemcpyAsync(&maxvel, dmax, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1567,12 +1591,11 @@ DCELL_API int dcell_ls_resident_advect_and_reinit(dcell_session *s, const dcell_
   DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
   if (redo_possible && (hf & dcell::FLAG_PIPELINE_REDO)) {
     // a slab was left: step the whole grid with every plane present (the
-    // same kernel on the same inputs), then the node pass again
+    // same kernel on the same inputs)
     DCELL_CUDA_CHECK(cudaMemsetAsync(dflags, 0, sizeof(int), st));
     if ((rc = launch_sl_tc_split(G, (const uint32_t *)r.split[cur].p, (const float *)r.vel.p, dt, nullptr, n,
                                  backtrace, (float *)r.phi[nxt].p, (uint32_t *)r.split[nxt].p, dflags, st)))
       return rc;
-    if ((rc = resident_nodes(s))) return rc;
     DCELL_CUDA_CHECK(cudaMemcpyAsync(&hf, dflags, sizeof(int), cudaMemcpyDeviceToHost, st));
     DCELL_CUDA_CHECK(cudaStreamSynchronize(st));
   }
@@ -1611,8 +1634,10 @@ DCELL_API int dcell_ls_resident_get(dcell_session *s, const dcell_geom *g, doubl
   cudaStream_t st = s->stream;
   const long long n = grid_points(g);
   int rc;
-  if (r.reinit_pending) {  // the reinitialisation the last step triggered
-    if ((rc = resident_reinit_enqueue(s, r.reinit_bw)) || (rc = resident_reinit_finish(s))) return rc;
+  if (r.reinit_pending) {  // the reinitialisation the last step triggered, from that step's nodes
+    if ((rc = resident_nodes_due(s)) || (rc = resident_reinit_enqueue(s, r.reinit_bw)) ||
+        (rc = resident_reinit_finish(s)))
+      return rc;
   }
   if (phi) {
     if (r.precision == DCELL_F32) {

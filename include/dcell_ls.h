@@ -474,11 +474,13 @@ DCELL_API int dcell_ls_advect_sl(dcell_session *s, const dcell_geom *g, const do
  * loop->AdvectThres or loop->CFLcount > loop->CFLthres, the reinitialisation
  * (dcell_reinitialize's bucketed march, band width loop->bandWidth) that
  * replaces phi's band; the counters live in `loop` as in struct _LevelSet.
- * The reinitialisation a step triggers (loop->reinitialized = 1) runs before
- * the level set is next used -- first thing in the next call, where it
- * overlaps that step's velocity upload, or in dcell_ls_resident_get -- so
- * loop->band reports the band before it; the results are those of running
- * it at the end of the step.
+ * The node pass of the step's new level set, and the reinitialisation a
+ * step triggers (loop->reinitialized = 1), run before their results are
+ * next used -- first thing in the next call, where they overlap that step's
+ * velocity upload, or (the reinitialisation) in dcell_ls_resident_get -- so
+ * loop->band reports the band before the reinitialisation and an error of
+ * the node pass is returned by the next call; the results are those of
+ * running both at the end of the step.
  * dcell_ls_resident_get downloads phi (FP64) and the band where the host
  * needs them (output, or a CPU fast marching instead of the device one).
  * precision: the arithmetic (DCELL_F32 with DCELL_CUBIC_TC on a dense 3D grid
