@@ -4,6 +4,7 @@ device between steps, only the velocity goes up.  Checked against the same
 loop run step by step through the device API (levelset.LevelSetAdvectAndReinit
 with the GPU reinitialisation hook): same phi bits, bands, counters."""
 import ctypes
+import math
 
 import numpy as np
 import pytest
@@ -129,3 +130,36 @@ def test_resident_tc_loop_with_reinitialisation(cuda):
     r.close()
     assert np.array_equal(got, p.double().cpu().numpy())
     assert np.array_equal(gband, b.cpu().numpy())
+
+
+@pytest.mark.gpu
+def test_resident_loop_2d_equals_the_device_api_loop(cuda):
+    """The 2D loop (Zalesak's disk in cell units, rigid rotation, FP64
+    bilinear Euler on the band, CFL threshold 1 so that it reinitialises
+    inside the loop): the resident loop's phi, band and counters equal the
+    device API loop's, bit for bit."""
+    N = 128
+    h = 1.0 / N
+    phi = (fields.slotted_disk_sdf(N, device=cuda) * N).contiguous()
+    vel = fields.rotation_velocity_2d(N, device=cuda).contiguous()
+    band = fields.band_of(phi, 6.0, margin=3)
+    dt = 0.5 * h / math.pi
+    ls = L.LevelSetCreate(h, (0, 0, 0), (N, N, 1), dtype=torch.float64, device=cuda)
+    ls.phi.copy_(phi)
+    ls.band = band.to(cuda).contiguous()
+    ls.CFLthres = 1.0
+    ls.Reinitialize = L.LevelSetReinitializeGPU
+    L.LevelSetUpdateIrregularNodeList(ls)
+    r = L.ResidentLevelSet(phi.cpu().numpy(), h, band=band.cpu().numpy(), precision="f64", CFLthres=1.0)
+    vhost = vel.cpu().numpy()
+    reinits = 0
+    for s in range(12):
+        L.LevelSetAdvectAndReinit(ls, vel, dt)
+        loop = r.advect_and_reinit(vhost, dt)
+        assert loop.AdvectCount == ls.AdvectCount and loop.CFLcount == ls.CFLcount and loop.maxVel == ls.maxVel
+        reinits += loop.reinitialized
+    assert reinits >= 2
+    got, gband = r.get()
+    r.close()
+    assert np.array_equal(got, ls.phi.cpu().numpy())
+    assert np.array_equal(gband, ls.band.cpu().numpy())
